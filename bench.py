@@ -1,0 +1,312 @@
+"""Benchmark of the collective-coordinate energy+gradient hot path on B200.
+
+Workload: 3D stealthy CC configuration, N = 2000 points uniform in a periodic cube of side N^(1/3) (unit density),
+chi = 0.45, the CLI's Type 0 k-set (M = 2724 half-space k-vectors, v(k) = 1): one STEP is one FP64 energy + Cartesian
+forces evaluation of one configuration. Synthetic seeded inputs (no dataset exists for this workload).
+
+  value : evaluations/s with positions resident in HBM. The evaluations run round-robin over a pool of distinct
+          configurations larger than L2 (so no step re-reads cached inputs), replayed from CUDA graphs of the two
+          kernels per step, timed with CUDA events on the launching stream.
+  e2e   : the same metric through the C ABI with host buffers (cc_set_positions + cc_energy_grad: host->device copy
+          of the step's positions and device->host read of E and F inside the timed region), wall clock.
+  roofline: the dominant kernel's algorithmic FLOPs ((17 + 2d) per particle-k pair and evaluation: 8 in the rho
+          kernel, 9 + 2d in the force kernel) / its CUDA-event duration, against the FP64 FMA peak measured in the
+          same run by an FMA-chain probe kernel (MEASURED_PEAKS.json has no FP64 figure).
+  cpu_baseline: the reference's own ShiftedCCPotential (Energy + AllForce, oracle/_ref) on the host cores.
+
+--impl reference times that reference CPU path alone on the same workload and prints its line.
+Multi-GPU: replicas only (independent configurations per rank, no collective on the data path).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+D, N, CHI = 3, 2000, 0.45
+SIDE = N ** (1.0 / 3.0)
+METRIC = "CC energy+grad evals/s"
+UNIT = "evals/s"
+WORKLOAD = "3D stealthy CC ground-state evaluation: N=2000 uniform in a periodic cube (unit density), chi=0.45, " \
+           "M=2724 half-space k (v=1), FP64 energy + Cartesian forces"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--warmup", type=int, default=500)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--pool", type=int, default=3072, help="distinct configurations cycled through (> L2)")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons while running."""
+
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "samples": len(rows), "reasons": sorted(reasons)}
+
+
+def cpu_reference_rate(seconds, steps=None, warmup=1):
+    """The reference's Direct path (oracle/_ref): evaluations/s on all host cores for this workload."""
+    import oracle
+    if not oracle.ref_available():
+        raise RuntimeError("oracle/_ref/libccref.so is not built")
+    import modules_b200 as cc
+    modes, V = cc.stealthy_kset(D, np.eye(D) * SIDE, N, CHI)
+    cores = os.cpu_count() or 1
+    ref = oracle.Ref(D, np.eye(D) * SIDE, V, modes=modes, nthreads=cores)
+    rng = np.random.default_rng(99)
+    pool = [rng.random((N, D)) for _ in range(4)]
+    for i in range(warmup):
+        ref.set_positions(pool[i % 4])
+        ref.eval()
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        ref.set_positions(pool[n % 4])
+        ref.eval()
+        n += 1
+        el = time.perf_counter() - t0
+        if (steps is not None and n >= steps) or (steps is None and el >= seconds and n >= 3):
+            break
+    return n / el, cores, n, el
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    rate, cores, n, el = cpu_reference_rate(None, steps=args.steps, warmup=args.warmup)
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / n, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded uniform positions)",
+            "config": {"workload": WORKLOAD, "N": N, "d": D, "chi": CHI, "M": 2724},
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": f"{n} evaluations (SetConfiguration+Energy+AllForce), {el:.1f} s"},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+
+    import modules_b200 as cc
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    prec = cc.PREC_FP64 if args.precision == "fp64" else cc.PREC_MIXED
+    basis = np.eye(D) * SIDE
+    modes, V = cc.stealthy_kset(D, basis, N, CHI)
+    M = len(V)
+    pot = cc.CCPotential(D, basis, modes, V)
+    P = args.pool
+    rng = np.random.default_rng(1234 + rank)
+    host_pool = rng.random((P, N, D))
+    dev = torch.device("cuda", local)
+    pool = torch.tensor(host_pool, dtype=torch.float64, device=dev)
+    E = torch.zeros(P, dtype=torch.float64, device=dev)
+    F = torch.zeros_like(pool)
+    side = torch.cuda.Stream(device=dev)
+
+    def step(i, stream):
+        j = i % P
+        pot.energy_grad_device(N, pool[j].data_ptr(), E[j:j + 1].data_ptr(), F[j].data_ptr(), precision=prec,
+                               stream=stream)
+
+    # warm-up (also allocates the library's work buffers before any capture)
+    with torch.cuda.stream(side):
+        for i in range(max(args.warmup, 3)):
+            step(i, side.cuda_stream)
+    torch.cuda.synchronize()
+
+    # CUDA graphs of G consecutive steps covering the pool
+    G = 128
+    graphs = []
+    for g0 in range(0, P, G):
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=side):
+            cs = torch.cuda.current_stream().cuda_stream
+            for i in range(g0, min(P, g0 + G)):
+                step(i, cs)
+        graphs.append(g)
+    torch.cuda.synchronize()
+
+    def run_steps(K, stream):
+        done = 0
+        gi = 0
+        while done + G <= K:
+            graphs[gi % len(graphs)].replay()
+            gi += 1
+            done += G
+        with torch.cuda.stream(stream):
+            while done < K:
+                step(done, stream.cuda_stream)
+                done += 1
+
+    with torch.cuda.stream(side):
+        run_steps(min(args.warmup, 4 * G) + G, side)
+    torch.cuda.synchronize()
+
+    K = args.steps
+    clocks = Clocks(local)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(side):
+        t_start.record(side)
+        run_steps(K, side)
+        t_end.record(side)
+    torch.cuda.synchronize()
+    ms = t_start.elapsed_time(t_end)
+    clk = clocks.stop()
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * K / (ms / 1e3)
+
+    # per-kernel CUDA-event timing pass (same steps, launched directly, events on the launching stream)
+    KT = min(max(K, 200), 4000)
+    pot.set_timing(True)
+    with torch.cuda.stream(side):
+        for i in range(KT):
+            step(i, side.cuda_stream)
+    rho_ms, force_ms, nt = pot.get_timing()
+    pot.set_timing(False)
+    pairs = N * M
+    rho_flops, force_flops = 8.0 * pairs, (9.0 + 2 * D) * pairs
+    t_rho, t_force = rho_ms / nt, force_ms / nt
+    peak = cc.probe_fma_peak(cc.PREC_FP64 if prec == cc.PREC_FP64 else cc.PREC_MIXED)
+    if t_force >= t_rho:
+        dom, fl, tk = "cc_force_kernel", force_flops, t_force
+    else:
+        dom, fl, tk = "cc_rho_kernel", rho_flops, t_rho
+    achieved = fl / (tk * 1e-3) / 1e12
+
+    # end to end through the C ABI with host buffers
+    KE = K
+    host_F = np.zeros((N, D))
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for i in range(KE):
+        pot.set_configuration(host_pool[i % P])
+        e_, _ = pot.energy_and_forces(precision=prec)
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * KE / e2e_s
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            rate, cores, n, el = cpu_reference_rate(args.cpu_seconds)
+            cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
+                   "sample": f"{n} evaluations of the same workload (SetConfiguration+Energy+AllForce, "
+                             f"reference Direct path, OpenMP over {cores} threads), {el:.1f} s"}
+        except Exception as exc:  # the baseline is a report, never a reason to drop the GPU line
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"unavailable: {exc}"}
+
+    info = pot.plan_info(N)
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
+                "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if prec == cc.PREC_FP64 else "f32-recurrence/f64-accumulate",
+                "data": "synthetic (seeded uniform positions, random k-set of the CLI rule)",
+                "config": {"workload": WORKLOAD, "N": N, "d": D, "chi": CHI, "M": M, "pairs_per_eval": pairs,
+                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                           "l2": f"inputs larger than L2: {P} distinct configurations "
+                                 f"({P * N * D * 8 / 1e6:.0f} MB) cycled round-robin",
+                           "graphs": f"CUDA graphs of {G} steps", "segment_len": info["L"],
+                           "segments": info["nseg"], "rho_splits": info["nsplit"], "force_splits": info["nksplit"]},
+                "pairs_per_s": value * pairs,
+                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": N * D * 8,
+                        "d2h_bytes_per_step": N * D * 8 + 8},
+                "gpu_launches": 2 * K,
+                "roofline": {"bound": "fp64_fma" if prec == cc.PREC_FP64 else "fp32_fma", "kernel": dom,
+                             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                             "peak_source": "measured in this run: FMA-chain probe kernel (cc_probe_fma_peak)",
+                             "flops_per_launch": fl, "launch_ms": tk, "traffic": None,
+                             "kernel_ms": {"cc_rho_kernel": t_rho, "cc_force_kernel": t_force}},
+                "clocks": clk, "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    del graphs
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

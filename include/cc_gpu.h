@@ -1,0 +1,133 @@
+/* cc_gpu.h — C ABI of the B200 collective-coordinate (CC) potential library (libccgpu.so).
+ *
+ * The library evaluates, on one GPU, the stealthy collective-coordinate potential of a periodic point pattern:
+ *   rho(k)   = sum_j exp(i k.r_j)                              over the constraint set {k, V(k)},
+ *   Phi      = sum_k V(k) |rho(k)|^2 / Volume + Shift,
+ *   F_j      = -dPhi/dr_j = (2/Volume) sum_k V(k) Im(conj(rho(k)) exp(i k.r_j)) k,
+ *   S(k)     = |rho(k)|^2 / N.
+ * Every k must lie on the reciprocal lattice of the cell: k = sum_e n_e b_e with integer n. Positions are given as
+ * fractional (relative) coordinates s in the cell basis, r = sum_i s_i a_i, and wrapped into [0,1) the way the
+ * reference's Configuration::Insert wraps them.
+ *
+ * Conventions: every call returns an int status (CC_OK = 0, negative on error); no exception crosses the ABI. Host
+ * buffers are copied in and out; a handle owns its device buffers and one CUDA stream. Calls on one handle are not
+ * thread-safe (as one reference potential object is not), distinct handles are independent.
+ *
+ * Reference interfaces replaced (paths within the reference project):
+ *   cc_create / cc_create_cartesian   ShiftedCCPotential(dim) + constraints/AddConstraint + Shift
+ *                                     (potential/CollectiveCoordinatePotential.h:84-117, :1318-1331)
+ *   cc_set_positions                  ShiftedCCPotential::SetConfiguration (:1457-1463), which binds a Configuration
+ *                                     built by Configuration::Insert (core/PeriodicCellList.h:517-538)
+ *   cc_energy_grad                    Energy() then AllForce() (:1351-1372, :1434-1448), i.e. the bitwise contract of
+ *                                     CombinedEnergyForce::EnergyAndAllForce (potential/CombinedEnergyForce.h)
+ *   cc_rho                            GetRho() / RhoReal, RhoImag (:1255-1314)
+ *   cc_force_one                      Force(result, i) (:1377-1394)
+ *   cc_structure_factor               StructureFactor(config, k) (pairstat/StructureFactor.cpp:56-65)
+ *   cc_objective                      Objective, Switch 0 (potential/StructureOptimization.cpp:447-536)
+ */
+#ifndef CC_GPU_H
+#define CC_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+	CC_OK = 0,
+	CC_ERR_ARG = -1,          /* invalid argument (null pointer, bad size, dimension outside 1..3, NaN input) */
+	CC_ERR_OOM = -2,          /* device or host allocation failed */
+	CC_ERR_CUDA = -3,         /* a CUDA call failed; cc_last_error() has the message */
+	CC_ERR_TIMEOUT = -4,      /* a bounded device wait ran out */
+	CC_ERR_NONLATTICE = -5,   /* a Cartesian k is not on the reciprocal lattice of the cell */
+	CC_ERR_STATE = -6,        /* call order: e.g. energy requested before positions were set */
+	CC_ERR_NOGPU = -7         /* no CUDA device is visible: the library has no CPU path */
+};
+
+enum {
+	CC_PREC_FP64 = 0,   /* FP64 seeds, FP64 recurrences, FP64 sums */
+	CC_PREC_MIXED = 1   /* FP64 argument reduction, FP32 seeds and recurrences, FP64 tile partials and sums */
+};
+
+typedef struct cc_handle cc_handle;
+
+/* Message of the last failed call on this thread (static storage, never NULL). */
+const char *cc_last_error(void);
+
+/* 1 if a CUDA device is usable, 0 otherwise. */
+int cc_device_available(void);
+
+/* Create a potential. d in 1..3; basis: d rows of d doubles, row i = basis vector a_i of the cell;
+ * modes: M x d integers n (k = sum_e n_e b_e, b the reciprocal basis, b_e . a_i = 2 pi delta_ei); V: M weights;
+ * shift: added to the energy. Modes may repeat, be zero or negative, in any order. M may be 0. */
+int cc_create(int d, const double *basis, int64_t M, const int32_t *modes, const double *V, double shift,
+              cc_handle **out);
+
+/* As cc_create with Cartesian k (M x d). Each k is mapped to n_e = k.a_e / (2 pi); CC_ERR_NONLATTICE if some n_e is
+ * not within 1e-9 (relative to max(1,|n_e|)) of an integer. */
+int cc_create_cartesian(int d, const double *basis, int64_t M, const double *k, const double *V, double shift,
+                        cc_handle **out);
+
+int cc_destroy(cc_handle *h);
+
+/* Number of constraints, dimension, volume and the integer modes (M x d) of a handle. */
+int cc_info(const cc_handle *h, int64_t *M, int *d, double *volume, int32_t *modes);
+
+/* Real offset added to every Re rho(k) (the reference's HAVETWOFIXEDPARTICLES build adds 2). Default 0. */
+int cc_set_rho_offset(cc_handle *h, double offset);
+
+/* Bind N particles at fractional coordinates frac (N x d, host). N may be 0. */
+int cc_set_positions(cc_handle *h, int64_t N, const double *frac);
+
+/* Energy and Cartesian forces (N x d, host; F may be NULL) of the bound positions. precision: CC_PREC_*. */
+int cc_energy_grad(cc_handle *h, double *E, double *F, int precision);
+
+/* rho(k) of the bound positions in constraint order (host arrays of M). */
+int cc_rho(cc_handle *h, double *re, double *im, int precision);
+
+/* Force on particle i of the bound positions (d doubles), from the last cc_energy_grad. */
+int cc_force_one(cc_handle *h, int64_t i, double *f);
+
+/* S(k) = |rho(k)|^2 / N of the bound positions at K integer modes (K x d), host output S (K). */
+int cc_structure_factor(cc_handle *h, int64_t K, const int32_t *modes, double *S, int precision);
+
+/* The structure optimiser's Switch-0 objective: x = rescale * fractional coordinates (N*d), returns the energy in
+ * *f and, if grad is not NULL, grad[i*d+j] = -F_i . a_j / rescale. */
+int cc_objective(cc_handle *h, int64_t N, const double *x, double rescale, double *f, double *grad, int precision);
+
+/* Device-resident evaluation: d_frac (N x d, device), outputs d_E (1 double) and d_F (N x d Cartesian, may be
+ * NULL) and d_gfrac (N x d gradient of the energy with respect to the fractional coordinates, may be NULL), all on
+ * the device, enqueued on `stream` (a cudaStream_t; NULL = the handle's stream). No host synchronisation. */
+int cc_energy_grad_device(cc_handle *h, int64_t N, const double *d_frac, double *d_E, double *d_F, double *d_gfrac,
+                          int precision, void *stream);
+
+/* Generate the stealthy k-set of the reference's CLI (GeneratePotential Type 0..3): the half-space reciprocal
+ * vectors (first nonzero index > 0) sorted by |k|, the first ceil(chi*N*d) of them plus the rest of the last shell;
+ * V = 1 (type 0), acos(x)-x*sqrt(1-x^2) (1), (1-x)^6 (2), (1-x)^2 (3) with x = |k|/K, K the first excluded |k|.
+ * Writes at most cap modes; *M receives the count (CC_ERR_ARG if cap is too small, *M then holds the need). */
+int cc_kset_stealthy(int d, const double *basis, int64_t N, double chi, int type, int64_t cap, int32_t *modes,
+                     double *V, int64_t *M);
+
+/* --- measurement support (no counterpart in the reference) --------------------------------------------------- */
+
+/* on = 1: every following evaluation on this handle records CUDA events around its rho and force kernels (on the
+ * stream they run on); cc_get_timing synchronises and returns the summed kernel times in ms and the number of
+ * evaluations timed since timing was switched on, then clears the record. */
+int cc_set_timing(cc_handle *h, int on);
+int cc_get_timing(cc_handle *h, double *rho_ms, double *force_ms, int64_t *evals);
+
+/* Launch configuration chosen for N particles: the rho kernel's particle splits and the force kernel's segment
+ * splits, the segment length L and the number of segments (for reports). */
+int cc_plan_info(const cc_handle *h, int64_t N, int *L, int64_t *nseg, int *nsplit, int *nksplit);
+
+/* Measure the device's FMA throughput (TFLOP/s, 2 flops per FMA) of independent FMA chains in FP64
+ * (precision = CC_PREC_FP64) or FP32 (CC_PREC_MIXED), timed with CUDA events: the roofline peak of this path. */
+int cc_probe_fma_peak(int precision, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CC_GPU_H */

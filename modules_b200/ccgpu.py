@@ -1,0 +1,235 @@
+"""ctypes binding of libccgpu.so (include/cc_gpu.h).
+
+``CCPotential`` mirrors the reference's ShiftedCCPotential (potential/CollectiveCoordinatePotential.h): a constraint
+set {k, V(k)} plus Shift, bound to one configuration at a time (SetConfiguration), with Energy / AllForce / Force /
+GetRho and the structure optimiser's objective. Errors raise ``CCError`` carrying the ABI status code, as the
+reference's setters raise std::invalid_argument / std::logic_error.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+_STATUS = {0: "CC_OK", -1: "CC_ERR_ARG", -2: "CC_ERR_OOM", -3: "CC_ERR_CUDA", -4: "CC_ERR_TIMEOUT",
+           -5: "CC_ERR_NONLATTICE", -6: "CC_ERR_STATE", -7: "CC_ERR_NOGPU"}
+
+
+class CCError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{_STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def library_path():
+    return os.path.join(_HERE, "libccgpu.so")
+
+
+_vp = ctypes.c_void_p
+_i64 = ctypes.c_int64
+_d = ctypes.c_double
+_i = ctypes.c_int
+
+_SIGS = {
+    "cc_last_error": (ctypes.c_char_p, []),
+    "cc_device_available": (_i, []),
+    "cc_create": (_i, [_i, _vp, _i64, _vp, _vp, _d, ctypes.POINTER(_vp)]),
+    "cc_create_cartesian": (_i, [_i, _vp, _i64, _vp, _vp, _d, ctypes.POINTER(_vp)]),
+    "cc_destroy": (_i, [_vp]),
+    "cc_info": (_i, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i), ctypes.POINTER(_d), _vp]),
+    "cc_set_rho_offset": (_i, [_vp, _d]),
+    "cc_set_positions": (_i, [_vp, _i64, _vp]),
+    "cc_energy_grad": (_i, [_vp, ctypes.POINTER(_d), _vp, _i]),
+    "cc_rho": (_i, [_vp, _vp, _vp, _i]),
+    "cc_force_one": (_i, [_vp, _i64, _vp]),
+    "cc_structure_factor": (_i, [_vp, _i64, _vp, _vp, _i]),
+    "cc_objective": (_i, [_vp, _i64, _vp, _d, ctypes.POINTER(_d), _vp, _i]),
+    "cc_energy_grad_device": (_i, [_vp, _i64, _vp, _vp, _vp, _vp, _i, _vp]),
+    "cc_kset_stealthy": (_i, [_i, _vp, _i64, _d, _i, _i64, _vp, _vp, ctypes.POINTER(_i64)]),
+    "cc_set_timing": (_i, [_vp, _i]),
+    "cc_get_timing": (_i, [_vp, ctypes.POINTER(_d), ctypes.POINTER(_d), ctypes.POINTER(_i64)]),
+    "cc_plan_info": (_i, [_vp, _i64, ctypes.POINTER(_i), ctypes.POINTER(_i64), ctypes.POINTER(_i),
+                          ctypes.POINTER(_i)]),
+    "cc_probe_fma_peak": (_i, [_i, ctypes.POINTER(_d)]),
+}
+
+
+def load_library():
+    """Load libccgpu.so (building it first if it is missing and nvcc is present). Raises if it cannot be loaded."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = library_path()
+    if not os.path.exists(path):
+        from . import build
+        build.build()
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise CCError(rc, load_library().cc_last_error().decode())
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_vp) if a is not None else None
+
+
+def device_available():
+    return bool(load_library().cc_device_available())
+
+
+def stealthy_kset(d, basis, N, chi, type_=0):
+    """The reference CLI's stealthy k-set (GeneratePotential Type 0..3): (modes int32 M x d, V float64 M)."""
+    lib = load_library()
+    basis = np.ascontiguousarray(basis, dtype=np.float64).reshape(d, d)
+    M = _i64(0)
+    rc = lib.cc_kset_stealthy(d, _ptr(basis), N, chi, type_, 0, None, None, ctypes.byref(M))
+    if rc not in (0, -1):
+        _check(rc)
+    modes = np.zeros((max(M.value, 1), d), np.int32)
+    V = np.zeros(max(M.value, 1))
+    _check(lib.cc_kset_stealthy(d, _ptr(basis), N, chi, type_, M.value, _ptr(modes), _ptr(V), ctypes.byref(M)))
+    return modes[:M.value], V[:M.value]
+
+
+def probe_fma_peak(precision=PREC_FP64):
+    """Measured FMA throughput of the device in TFLOP/s (FP64 or FP32 chains)."""
+    t = _d()
+    _check(load_library().cc_probe_fma_peak(precision, ctypes.byref(t)))
+    return t.value
+
+
+class CCPotential:
+    """GPU ShiftedCCPotential over a cell ``basis`` (rows a_i) with integer ``modes`` (k = sum_e n_e b_e)."""
+
+    def __init__(self, d, basis, modes=None, V=None, shift=0.0, kcart=None):
+        self._lib = load_library()
+        self.d = int(d)
+        self.basis = np.ascontiguousarray(basis, dtype=np.float64).reshape(self.d, self.d)
+        h = _vp()
+        if kcart is not None:
+            kc = np.ascontiguousarray(kcart, dtype=np.float64).reshape(-1, self.d)
+            V = np.ascontiguousarray(V, dtype=np.float64).reshape(-1)
+            _check(self._lib.cc_create_cartesian(self.d, _ptr(self.basis), len(V), _ptr(kc), _ptr(V), shift,
+                                                 ctypes.byref(h)))
+        else:
+            modes = np.ascontiguousarray(modes, dtype=np.int32).reshape(-1, self.d)
+            V = np.ascontiguousarray(V, dtype=np.float64).reshape(-1)
+            if len(V) != len(modes):
+                raise ValueError("modes and V differ in length")
+            _check(self._lib.cc_create(self.d, _ptr(self.basis), len(V), _ptr(modes), _ptr(V), shift,
+                                       ctypes.byref(h)))
+        self._h = h
+        self.M = len(V)
+        self.N = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.cc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self):
+        M, d, vol = _i64(), _i(), _d()
+        modes = np.zeros((max(self.M, 1), self.d), np.int32)
+        _check(self._lib.cc_info(self._h, ctypes.byref(M), ctypes.byref(d), ctypes.byref(vol), _ptr(modes)))
+        return modes[:M.value], vol.value
+
+    def set_rho_offset(self, off):
+        _check(self._lib.cc_set_rho_offset(self._h, float(off)))
+
+    def set_configuration(self, frac):
+        frac = np.ascontiguousarray(frac, dtype=np.float64).reshape(-1, self.d)
+        _check(self._lib.cc_set_positions(self._h, len(frac), _ptr(frac)))
+        self.N = len(frac)
+
+    SetConfiguration = set_configuration
+
+    def energy_and_forces(self, precision=PREC_FP64, forces=True):
+        E = _d()
+        F = np.zeros((max(self.N or 0, 1), self.d)) if forces else None
+        _check(self._lib.cc_energy_grad(self._h, ctypes.byref(E), _ptr(F) if forces else None, precision))
+        return (E.value, F[: self.N]) if forces else (E.value, None)
+
+    def energy(self, precision=PREC_FP64):
+        return self.energy_and_forces(precision, forces=False)[0]
+
+    Energy = energy
+
+    def all_force(self, precision=PREC_FP64):
+        return self.energy_and_forces(precision)[1]
+
+    AllForce = all_force
+
+    def force(self, i):
+        f = np.zeros(self.d)
+        _check(self._lib.cc_force_one(self._h, int(i), _ptr(f)))
+        return f
+
+    Force = force
+
+    def rho(self, precision=PREC_FP64):
+        re = np.zeros(max(self.M, 1))
+        im = np.zeros(max(self.M, 1))
+        _check(self._lib.cc_rho(self._h, _ptr(re), _ptr(im), precision))
+        return re[: self.M], im[: self.M]
+
+    GetRho = rho
+
+    def structure_factor(self, modes, precision=PREC_FP64):
+        modes = np.ascontiguousarray(modes, dtype=np.int32).reshape(-1, self.d)
+        S = np.zeros(max(len(modes), 1))
+        _check(self._lib.cc_structure_factor(self._h, len(modes), _ptr(modes), _ptr(S), precision))
+        return S[: len(modes)]
+
+    def objective(self, x, rescale, grad=True, precision=PREC_FP64):
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+        n = len(x) // self.d
+        f = _d()
+        g = np.zeros(max(len(x), 1)) if grad else None
+        _check(self._lib.cc_objective(self._h, n, _ptr(x), rescale, ctypes.byref(f), _ptr(g) if grad else None,
+                                      precision))
+        self.N = n
+        return (f.value, g[: len(x)]) if grad else f.value
+
+    def set_timing(self, on):
+        _check(self._lib.cc_set_timing(self._h, 1 if on else 0))
+
+    def get_timing(self):
+        """(rho kernel ms, force kernel ms, evaluations) summed since set_timing(True)."""
+        r, f, n = _d(), _d(), _i64()
+        _check(self._lib.cc_get_timing(self._h, ctypes.byref(r), ctypes.byref(f), ctypes.byref(n)))
+        return r.value, f.value, n.value
+
+    def plan_info(self, N):
+        L, nseg, ns, nk = _i(), _i64(), _i(), _i()
+        _check(self._lib.cc_plan_info(self._h, int(N), ctypes.byref(L), ctypes.byref(nseg), ctypes.byref(ns),
+                                      ctypes.byref(nk)))
+        return dict(L=L.value, nseg=nseg.value, nsplit=ns.value, nksplit=nk.value)
+
+    def energy_grad_device(self, N, d_frac, d_E, d_F=None, d_gfrac=None, precision=PREC_FP64, stream=None):
+        """Enqueue one evaluation on device pointers (ints); no synchronisation."""
+        _check(self._lib.cc_energy_grad_device(self._h, int(N), _vp(d_frac), _vp(d_E), _vp(d_F) if d_F else None,
+                                               _vp(d_gfrac) if d_gfrac else None, precision,
+                                               _vp(stream) if stream else None))

@@ -1,0 +1,873 @@
+// cc_capi.cu — the C ABI of libccgpu.so (declared in include/cc_gpu.h): handles, k-set planning, launches.
+//
+// A handle holds the constraint set of one ShiftedCCPotential (potential/CollectiveCoordinatePotential.h:84-117)
+// planned into lattice-line segments (see cc_kernels.cuh), the cell (volume, reciprocal basis) and the device
+// buffers of the bound positions. One evaluation is two kernel launches on the handle's stream:
+//   cc_rho_kernel   -> rho per slot, u = V conj(rho), the energy (and rho in mode order on request);
+//   cc_force_kernel -> Cartesian forces and/or the gradient in fractional coordinates.
+// There is no CPU path: without a CUDA device every call that computes returns CC_ERR_NOGPU.
+#include "../../include/cc_gpu.h"
+#include "cc_kernels.cuh"
+#include "cc_plan.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_err = "";
+
+int fail(int code, const std::string &msg)
+{
+	g_err = msg;
+	return code;
+}
+
+#define CC_CUDA(call)                                                                                         \
+	do {                                                                                                      \
+		cudaError_t e_ = (call);                                                                              \
+		if (e_ != cudaSuccess)                                                                                \
+			return fail(CC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));                    \
+	} while (0)
+
+constexpr int kWarps = 8;
+constexpr int kChunk = 64;
+constexpr int kSegChunk = 64;
+
+// ---------------------------------------------------------------------------------------------------------------
+// device-side k-set: a Plan uploaded
+// ---------------------------------------------------------------------------------------------------------------
+struct DevKSet {
+	cc::Plan plan;
+	cc::Seg *segs = nullptr;
+	double *slotV = nullptr;
+	int *mode_slot = nullptr;
+	double *modeV = nullptr;
+	double2 *rho_slot = nullptr;
+	double2 *u_slot = nullptr;
+	double2 *rho_mode = nullptr;
+	unsigned *counters = nullptr;   // ngroups + 1
+	double2 *partial = nullptr;     // nsplit_cap * nslot
+	size_t partial_cap = 0;         // in double2 elements
+
+	void release()
+	{
+		cudaFree(segs);
+		cudaFree(slotV);
+		cudaFree(mode_slot);
+		cudaFree(modeV);
+		cudaFree(rho_slot);
+		cudaFree(u_slot);
+		cudaFree(rho_mode);
+		cudaFree(counters);
+		cudaFree(partial);
+		*this = DevKSet();
+	}
+};
+
+template <class T> int dev_alloc(T **p, size_t n)
+{
+	*p = nullptr;
+	if (n == 0)
+		n = 1;
+	cudaError_t e = cudaMalloc(reinterpret_cast<void **>(p), n * sizeof(T));
+	if (e != cudaSuccess)
+		return fail(e == cudaErrorMemoryAllocation ? CC_ERR_OOM : CC_ERR_CUDA,
+		            std::string("cudaMalloc: ") + cudaGetErrorString(e));
+	return CC_OK;
+}
+
+int upload_kset(DevKSet &k, const cc::Plan &plan)
+{
+	k.release();
+	k.plan = plan;
+	int rc;
+	const size_t nseg = plan.segs.size(), nslot = plan.slotV.size(), M = plan.mode_slot.size();
+	if ((rc = dev_alloc(&k.segs, nseg)) || (rc = dev_alloc(&k.slotV, nslot)) || (rc = dev_alloc(&k.mode_slot, M)) ||
+	    (rc = dev_alloc(&k.modeV, M)) || (rc = dev_alloc(&k.rho_slot, nslot)) || (rc = dev_alloc(&k.u_slot, nslot)) ||
+	    (rc = dev_alloc(&k.rho_mode, M)) || (rc = dev_alloc(&k.counters, plan.ngroups + 1)))
+		return rc;
+	CC_CUDA(cudaMemcpy(k.segs, plan.segs.data(), nseg * sizeof(cc::Seg), cudaMemcpyHostToDevice));
+	CC_CUDA(cudaMemcpy(k.slotV, plan.slotV.data(), nslot * sizeof(double), cudaMemcpyHostToDevice));
+	CC_CUDA(cudaMemcpy(k.mode_slot, plan.mode_slot.data(), M * sizeof(int), cudaMemcpyHostToDevice));
+	CC_CUDA(cudaMemcpy(k.modeV, plan.modeV.data(), M * sizeof(double), cudaMemcpyHostToDevice));
+	CC_CUDA(cudaMemset(k.counters, 0, (plan.ngroups + 1) * sizeof(unsigned)));
+	return CC_OK;
+}
+
+}  // namespace
+
+struct cc_handle {
+	int d = 0;
+	double basis[9] = {0};
+	double recip[9] = {0};
+	double volume = 0;
+	double shift = 0;
+	double rho_offset = 0;
+	std::vector<int32_t> modes;
+	std::vector<double> V;
+	DevKSet main;
+	DevKSet sk;                     // k-set of the last cc_structure_factor call
+	std::vector<int32_t> sk_modes;
+	cudaStream_t stream = nullptr;
+	int64_t N = -1;                 // bound particle count, -1 before cc_set_positions
+	size_t ncap = 0;                // capacity of the per-particle buffers
+	double *d_frac = nullptr, *d_F = nullptr, *d_gfrac = nullptr, *d_partialG = nullptr;
+	size_t partialG_cap = 0;
+	unsigned *d_fcounters = nullptr;
+	double *d_E = nullptr;
+	double *h_pin = nullptr;        // pinned staging of N*d doubles (+1 for E)
+	size_t pin_cap = 0;
+	std::vector<double> lastF;      // forces of the last cc_energy_grad
+	bool lastF_valid = false;
+	bool timing = false;            // cc_set_timing
+	std::vector<cudaEvent_t> ev;    // 3 events per timed evaluation
+	size_t ev_used = 0;
+};
+
+namespace {
+
+// ---------------------------------------------------------------------------------------------------------------
+// launch configuration
+// ---------------------------------------------------------------------------------------------------------------
+struct Launch {
+	int nsplit, per_split;          // rho
+	int nksplit, segs_per_split;    // force
+};
+
+int sm_count()
+{
+	static int n = 0;
+	if (n == 0) {
+		int dev = 0;
+		cudaGetDevice(&dev);
+		if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+			n = 148;
+	}
+	return n;
+}
+
+Launch choose_launch(const cc::Plan &p, int64_t N)
+{
+	Launch l;
+	const int target = sm_count() * 3;   // resident blocks of 256 threads at the rho kernel's shared memory
+	// rho: enough particle splits to fill the chip, each split at least 2 particles per warp
+	int ns = std::max(1, (target + p.ngroups - 1) / std::max(1, p.ngroups));
+	ns = (int)std::min<int64_t>(ns, std::max<int64_t>(1, N / (2 * kWarps)));
+	l.per_split = (int)std::max<int64_t>(1, (N + ns - 1) / ns);
+	l.nsplit = N > 0 ? (int)((N + l.per_split - 1) / l.per_split) : 1;
+	// force: split the segments when there are too few particle groups
+	const int nseg = (int)p.segs.size();
+	const int64_t pg = (N + 31) / 32;
+	int nk = (int)std::max<int64_t>(1, (target + pg - 1) / std::max<int64_t>(1, pg));
+	nk = std::min(nk, std::max(1, nseg / (2 * kWarps)));
+	l.segs_per_split = std::max(1, (nseg + nk - 1) / nk);
+	l.nksplit = std::max(1, (nseg + l.segs_per_split - 1) / l.segs_per_split);
+	return l;
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// kernel dispatch
+// ---------------------------------------------------------------------------------------------------------------
+template <int D, int L, bool MIXED> int launch_rho_t(const cc::RhoArgs &a, int nsplit, cudaStream_t st)
+{
+	typedef cc::RhoSmem<D, L, kWarps, kChunk, MIXED> Lay;
+	auto kern = cc::cc_rho_kernel<D, L, kWarps, kChunk, MIXED>;
+	static bool attr = false;
+	if (!attr) {
+		CC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::bytes));
+		attr = true;
+	}
+	kern<<<dim3(a.ngroups, nsplit), kWarps * 32, Lay::bytes, st>>>(a);
+	CC_CUDA(cudaGetLastError());
+	return CC_OK;
+}
+
+template <int D, int L, bool MIXED> int launch_force_t(const cc::ForceArgs &a, int64_t N, cudaStream_t st)
+{
+	auto kern = cc::cc_force_kernel<D, L, kWarps, kSegChunk, MIXED>;
+	kern<<<dim3((unsigned)((N + 31) / 32), a.nksplit), kWarps * 32, 0, st>>>(a);
+	CC_CUDA(cudaGetLastError());
+	return CC_OK;
+}
+
+template <int D> int launch_rho_d(const cc::RhoArgs &a, int L, bool mixed, int nsplit, cudaStream_t st)
+{
+	if (L == 8)
+		return mixed ? launch_rho_t<D, 8, true>(a, nsplit, st) : launch_rho_t<D, 8, false>(a, nsplit, st);
+	return mixed ? launch_rho_t<D, 16, true>(a, nsplit, st) : launch_rho_t<D, 16, false>(a, nsplit, st);
+}
+template <int D> int launch_force_d(const cc::ForceArgs &a, int L, bool mixed, int64_t N, cudaStream_t st)
+{
+	if (L == 8)
+		return mixed ? launch_force_t<D, 8, true>(a, N, st) : launch_force_t<D, 8, false>(a, N, st);
+	return mixed ? launch_force_t<D, 16, true>(a, N, st) : launch_force_t<D, 16, false>(a, N, st);
+}
+
+int launch_rho(int d, const cc::RhoArgs &a, int L, bool mixed, int nsplit, cudaStream_t st)
+{
+	switch (d) {
+	case 1: return launch_rho_d<1>(a, L, mixed, nsplit, st);
+	case 2: return launch_rho_d<2>(a, L, mixed, nsplit, st);
+	default: return launch_rho_d<3>(a, L, mixed, nsplit, st);
+	}
+}
+int launch_force(int d, const cc::ForceArgs &a, int L, bool mixed, int64_t N, cudaStream_t st)
+{
+	switch (d) {
+	case 1: return launch_force_d<1>(a, L, mixed, N, st);
+	case 2: return launch_force_d<2>(a, L, mixed, N, st);
+	default: return launch_force_d<3>(a, L, mixed, N, st);
+	}
+}
+
+__global__ void set_scalar_kernel(double *p, double v) { *p = v; }
+
+// ---------------------------------------------------------------------------------------------------------------
+// buffers
+// ---------------------------------------------------------------------------------------------------------------
+int ensure_particles(cc_handle *h, int64_t N)
+{
+	const size_t need = (size_t)std::max<int64_t>(N, 1);
+	if (need > h->ncap) {
+		cudaFree(h->d_frac);
+		cudaFree(h->d_F);
+		cudaFree(h->d_gfrac);
+		cudaFree(h->d_fcounters);
+		h->d_frac = h->d_F = h->d_gfrac = nullptr;
+		h->d_fcounters = nullptr;
+		h->ncap = 0;
+		h->N = -1;   // the bound positions do not survive a reallocation
+		h->lastF_valid = false;
+		int rc;
+		if ((rc = dev_alloc(&h->d_frac, need * h->d)) || (rc = dev_alloc(&h->d_F, need * h->d)) ||
+		    (rc = dev_alloc(&h->d_gfrac, need * h->d)) || (rc = dev_alloc(&h->d_fcounters, (need + 31) / 32)))
+			return rc;
+		CC_CUDA(cudaMemset(h->d_fcounters, 0, ((need + 31) / 32) * sizeof(unsigned)));
+		h->ncap = need;
+	}
+	const size_t pin = need * h->d + 2;
+	if (pin > h->pin_cap) {
+		cudaFreeHost(h->h_pin);
+		h->h_pin = nullptr;
+		h->pin_cap = 0;
+		cudaError_t e = cudaMallocHost(reinterpret_cast<void **>(&h->h_pin), pin * sizeof(double));
+		if (e != cudaSuccess)
+			return fail(CC_ERR_OOM, std::string("cudaMallocHost: ") + cudaGetErrorString(e));
+		h->pin_cap = pin;
+	}
+	return CC_OK;
+}
+
+int ensure_partial(DevKSet &k, size_t elems)
+{
+	if (elems <= k.partial_cap)
+		return CC_OK;
+	cudaFree(k.partial);
+	k.partial = nullptr;
+	k.partial_cap = 0;
+	int rc = dev_alloc(&k.partial, elems);
+	if (rc)
+		return rc;
+	k.partial_cap = elems;
+	return CC_OK;
+}
+
+int ensure_partialG(cc_handle *h, size_t elems)
+{
+	if (elems <= h->partialG_cap)
+		return CC_OK;
+	cudaFree(h->d_partialG);
+	h->d_partialG = nullptr;
+	h->partialG_cap = 0;
+	int rc = dev_alloc(&h->d_partialG, elems);
+	if (rc)
+		return rc;
+	h->partialG_cap = elems;
+	return CC_OK;
+}
+
+// rho pass of k-set `k` over N device positions; writes the energy to d_E (weights of k's plan).
+int run_rho(cc_handle *h, DevKSet &k, int64_t N, const double *d_frac, double *d_E, bool want_rho_mode, bool mixed,
+            const Launch &l, cudaStream_t st)
+{
+	const cc::Plan &p = k.plan;
+	if (p.ngroups == 0) {
+		set_scalar_kernel<<<1, 1, 0, st>>>(d_E, h->shift);
+		CC_CUDA(cudaGetLastError());
+		return CC_OK;
+	}
+	int rc = ensure_partial(k, (size_t)l.nsplit * p.nslot);
+	if (rc)
+		return rc;
+	cc::RhoArgs a;
+	a.frac = d_frac;
+	a.N = (int)N;
+	a.per_split = N > 0 ? l.per_split : 0;
+	a.nsplit = N > 0 ? l.nsplit : 1;
+	a.segs = k.segs;
+	a.ngroups = p.ngroups;
+	a.nslot = p.nslot;
+	a.partial = k.partial;
+	a.counters = k.counters;
+	a.rho_slot = k.rho_slot;
+	a.slotV = k.slotV;
+	a.u_slot = k.u_slot;
+	a.mode_slot = k.mode_slot;
+	a.modeV = k.modeV;
+	a.M = (int)p.mode_slot.size();
+	a.rho_offset = h->rho_offset;
+	a.inv_vol = 1.0 / h->volume;
+	a.shift = h->shift;
+	a.E_out = d_E;
+	a.rho_mode = want_rho_mode ? k.rho_mode : nullptr;
+	return launch_rho(h->d, a, p.L, mixed, a.nsplit, st);
+}
+
+int run_force(cc_handle *h, int64_t N, const double *d_frac, double *d_F, double *d_gfrac, bool mixed,
+              const Launch &l, cudaStream_t st)
+{
+	const cc::Plan &p = h->main.plan;
+	if (N == 0)
+		return CC_OK;
+	if (p.ngroups == 0) {
+		if (d_F)
+			CC_CUDA(cudaMemsetAsync(d_F, 0, sizeof(double) * N * h->d, st));
+		if (d_gfrac)
+			CC_CUDA(cudaMemsetAsync(d_gfrac, 0, sizeof(double) * N * h->d, st));
+		return CC_OK;
+	}
+	if (l.nksplit > 1) {
+		int rc = ensure_partialG(h, (size_t)l.nksplit * N * h->d);
+		if (rc)
+			return rc;
+	}
+	cc::ForceArgs a;
+	a.frac = d_frac;
+	a.N = (int)N;
+	a.segs = h->main.segs;
+	a.nseg = (int)p.segs.size();
+	a.segs_per_split = l.segs_per_split;
+	a.nksplit = l.nksplit;
+	a.u_slot = h->main.u_slot;
+	a.partialG = h->d_partialG;
+	a.counters = h->d_fcounters;
+	for (int i = 0; i < 9; i++)
+		a.recip[i] = h->recip[i];
+	a.fscale = 2.0 / h->volume;
+	a.F_out = d_F;
+	a.gfrac_out = d_gfrac;
+	return launch_force(h->d, a, p.L, mixed, N, st);
+}
+
+int check_handle(const cc_handle *h)
+{
+	if (!h)
+		return fail(CC_ERR_ARG, "null handle");
+	return CC_OK;
+}
+
+int check_prec(int precision)
+{
+	if (precision != CC_PREC_FP64 && precision != CC_PREC_MIXED)
+		return fail(CC_ERR_ARG, "precision must be CC_PREC_FP64 or CC_PREC_MIXED");
+	return CC_OK;
+}
+
+int device_ok()
+{
+	int n = 0;
+	if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0)
+		return fail(CC_ERR_NOGPU, "no CUDA device is visible; libccgpu has no CPU path");
+	return CC_OK;
+}
+
+int create_common(int d, const double *basis, int64_t M, const int32_t *modes, const double *V, double shift,
+                  cc_handle **out)
+{
+	if (!out)
+		return fail(CC_ERR_ARG, "out is null");
+	*out = nullptr;
+	if (d < 1 || d > 3)
+		return fail(CC_ERR_ARG, "dimension must be 1, 2 or 3");
+	if (!basis || M < 0 || (M > 0 && (!modes || !V)))
+		return fail(CC_ERR_ARG, "null basis/modes/V or negative M");
+	if (M > (int64_t)1 << 30)
+		return fail(CC_ERR_ARG, "too many constraints");
+	int rc = device_ok();
+	if (rc)
+		return rc;
+	cc_handle *h = new cc_handle();
+	h->d = d;
+	for (int i = 0; i < d * d; i++)
+		h->basis[i] = basis[i];
+	if (!cc::cell_geometry(d, h->basis, &h->volume, h->recip)) {
+		delete h;
+		return fail(CC_ERR_ARG, "degenerate cell basis");
+	}
+	h->shift = shift;
+	h->modes.assign(modes, modes + M * d);
+	h->V.assign(V, V + M);
+	for (int64_t m = 0; m < M; m++)
+		if (!std::isfinite(V[m])) {
+			delete h;
+			return fail(CC_ERR_ARG, "non-finite weight V");
+		}
+	cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+	if (e != cudaSuccess) {
+		delete h;
+		return fail(CC_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+	}
+	cc::Plan plan = cc::build_plan(d, M, modes, V, 0);
+	if ((rc = upload_kset(h->main, plan)) || (rc = dev_alloc(&h->d_E, 2))) {
+		cc_destroy(h);
+		return rc;
+	}
+	*out = h;
+	return CC_OK;
+}
+
+cudaEvent_t next_event(cc_handle *h)
+{
+	if (h->ev_used == h->ev.size()) {
+		cudaEvent_t e;
+		if (cudaEventCreate(&e) != cudaSuccess)
+			return nullptr;
+		h->ev.push_back(e);
+	}
+	return h->ev[h->ev_used++];
+}
+
+int eval_device(cc_handle *h, int64_t N, const double *d_frac, double *d_E, double *d_F, double *d_gfrac,
+                bool want_rho_mode, int precision, cudaStream_t st)
+{
+	const bool mixed = precision == CC_PREC_MIXED;
+	const Launch l = choose_launch(h->main.plan, N);
+	cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
+	if (h->timing && h->ev_used + 3 <= 3 * 100000) {
+		e0 = next_event(h);
+		e1 = next_event(h);
+		e2 = next_event(h);
+		if (e0 && e1 && e2)
+			CC_CUDA(cudaEventRecord(e0, st));
+	}
+	int rc = run_rho(h, h->main, N, d_frac, d_E, want_rho_mode, mixed, l, st);
+	if (rc)
+		return rc;
+	if (e1)
+		CC_CUDA(cudaEventRecord(e1, st));
+	if (d_F || d_gfrac)
+		rc = run_force(h, N, d_frac, d_F, d_gfrac, mixed, l, st);
+	if (e2)
+		CC_CUDA(cudaEventRecord(e2, st));
+	return rc;
+}
+
+template <typename T> __global__ void fma_probe_kernel(T *out, int iters, T a, T b)
+{
+	T x[8];
+#pragma unroll
+	for (int k = 0; k < 8; k++)
+		x[k] = (T)(threadIdx.x + k) * (T)1e-3;
+	for (int i = 0; i < iters; i++) {
+#pragma unroll
+		for (int k = 0; k < 8; k++)
+			x[k] = fma(x[k], a, b);
+	}
+	T s = 0;
+#pragma unroll
+	for (int k = 0; k < 8; k++)
+		s += x[k];
+	if (s == (T)-1.2345)
+		out[0] = s;
+}
+
+template <typename T> int probe_peak(double *tflops)
+{
+	T *out = nullptr;
+	if (int rc = dev_alloc(&out, 1))
+		return rc;
+	const int blocks = sm_count() * 8, threads = 256, iters = 1 << 14;
+	cudaEvent_t a, b;
+	CC_CUDA(cudaEventCreate(&a));
+	CC_CUDA(cudaEventCreate(&b));
+	float best = 1e30f;
+	for (int rep = 0; rep < 6; rep++) {
+		CC_CUDA(cudaEventRecord(a));
+		fma_probe_kernel<T><<<blocks, threads>>>(out, iters, (T)0.9999999, (T)1e-7);
+		CC_CUDA(cudaEventRecord(b));
+		CC_CUDA(cudaEventSynchronize(b));
+		float ms = 0;
+		CC_CUDA(cudaEventElapsedTime(&ms, a, b));
+		if (rep > 0)
+			best = std::min(best, ms);
+	}
+	cudaEventDestroy(a);
+	cudaEventDestroy(b);
+	cudaFree(out);
+	*tflops = 2.0 * 8.0 * iters * (double)blocks * threads / (best * 1e-3) / 1e12;
+	return CC_OK;
+}
+
+}  // namespace
+
+// ===============================================================================================================
+// C ABI
+// ===============================================================================================================
+extern "C" {
+
+const char *cc_last_error(void) { return g_err.c_str(); }
+
+int cc_device_available(void)
+{
+	int n = 0;
+	return (cudaGetDeviceCount(&n) == cudaSuccess && n > 0) ? 1 : 0;
+}
+
+int cc_create(int d, const double *basis, int64_t M, const int32_t *modes, const double *V, double shift,
+              cc_handle **out)
+{
+	return create_common(d, basis, M, modes, V, shift, out);
+}
+
+int cc_create_cartesian(int d, const double *basis, int64_t M, const double *k, const double *V, double shift,
+                        cc_handle **out)
+{
+	if (d < 1 || d > 3 || !basis || M < 0 || (M > 0 && !k))
+		return fail(CC_ERR_ARG, "invalid arguments");
+	std::vector<int32_t> modes((size_t)M * d);
+	if (!cc::cartesian_to_modes(d, basis, M, k, modes.data()))
+		return fail(CC_ERR_NONLATTICE, "a Cartesian k is not on the reciprocal lattice of the cell");
+	return create_common(d, basis, M, modes.data(), V, shift, out);
+}
+
+int cc_destroy(cc_handle *h)
+{
+	if (!h)
+		return CC_OK;
+	if (h->stream)
+		cudaStreamSynchronize(h->stream);
+	h->main.release();
+	h->sk.release();
+	cudaFree(h->d_frac);
+	cudaFree(h->d_F);
+	cudaFree(h->d_gfrac);
+	cudaFree(h->d_partialG);
+	cudaFree(h->d_fcounters);
+	cudaFree(h->d_E);
+	cudaFreeHost(h->h_pin);
+	for (cudaEvent_t e : h->ev)
+		cudaEventDestroy(e);
+	if (h->stream)
+		cudaStreamDestroy(h->stream);
+	delete h;
+	return CC_OK;
+}
+
+int cc_info(const cc_handle *h, int64_t *M, int *d, double *volume, int32_t *modes)
+{
+	if (int rc = check_handle(h))
+		return rc;
+	if (M)
+		*M = (int64_t)h->V.size();
+	if (d)
+		*d = h->d;
+	if (volume)
+		*volume = h->volume;
+	if (modes)
+		std::memcpy(modes, h->modes.data(), h->modes.size() * sizeof(int32_t));
+	return CC_OK;
+}
+
+int cc_set_rho_offset(cc_handle *h, double offset)
+{
+	if (int rc = check_handle(h))
+		return rc;
+	if (!std::isfinite(offset))
+		return fail(CC_ERR_ARG, "offset must be finite");
+	h->rho_offset = offset;
+	h->lastF_valid = false;
+	return CC_OK;
+}
+
+int cc_set_positions(cc_handle *h, int64_t N, const double *frac)
+{
+	if (int rc = check_handle(h))
+		return rc;
+	if (N < 0 || (N > 0 && !frac) || N > ((int64_t)1 << 31) - 64)
+		return fail(CC_ERR_ARG, "invalid particle count or null positions");
+	if (int rc = ensure_particles(h, N))
+		return rc;
+	const int d = h->d;
+	for (int64_t i = 0; i < N * d; i++) {
+		const double x = frac[i];
+		if (!std::isfinite(x))
+			return fail(CC_ERR_ARG, "non-finite fractional coordinate");
+		// wrap into [0,1) as Configuration::Insert does (floor twice)
+		double s = x - std::floor(x);
+		s -= std::floor(s);
+		h->h_pin[i] = s;
+	}
+	if (N > 0) {
+		CC_CUDA(cudaMemcpyAsync(h->d_frac, h->h_pin, sizeof(double) * N * d, cudaMemcpyHostToDevice, h->stream));
+		CC_CUDA(cudaStreamSynchronize(h->stream));
+	}
+	h->N = N;
+	h->lastF_valid = false;
+	return CC_OK;
+}
+
+int cc_energy_grad(cc_handle *h, double *E, double *F, int precision)
+{
+	if (int rc = check_handle(h))
+		return rc;
+	if (int rc = check_prec(precision))
+		return rc;
+	if (h->N < 0)
+		return fail(CC_ERR_STATE, "positions not set");
+	if (!E)
+		return fail(CC_ERR_ARG, "E is null");
+	const int64_t N = h->N;
+	if (int rc = eval_device(h, N, h->d_frac, h->d_E, F ? h->d_F : nullptr, nullptr, false, precision, h->stream))
+		return rc;
+	CC_CUDA(cudaMemcpyAsync(h->h_pin, h->d_E, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+	if (F && N > 0)
+		CC_CUDA(cudaMemcpyAsync(h->h_pin + 2, h->d_F, sizeof(double) * N * h->d, cudaMemcpyDeviceToHost, h->stream));
+	CC_CUDA(cudaStreamSynchronize(h->stream));
+	*E = h->h_pin[0];
+	if (F && N > 0) {
+		std::memcpy(F, h->h_pin + 2, sizeof(double) * N * h->d);
+		h->lastF.assign(F, F + N * h->d);
+		h->lastF_valid = true;
+	}
+	return CC_OK;
+}
+
+int cc_energy_grad_device(cc_handle *h, int64_t N, const double *d_frac, double *d_E, double *d_F, double *d_gfrac,
+                          int precision, void *stream)
+{
+	if (int rc = check_handle(h))
+		return rc;
+	if (int rc = check_prec(precision))
+		return rc;
+	if (N < 0 || (N > 0 && !d_frac) || !d_E)
+		return fail(CC_ERR_ARG, "invalid device arguments");
+	if ((size_t)std::max<int64_t>(N, 1) > h->ncap)
+		if (int rc = ensure_particles(h, N))
+			return rc;
+	cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+	return eval_device(h, N, d_frac, d_E, d_F, d_gfrac, false, precision, st);
+}
+
+int cc_rho(cc_handle *h, double *re, double *im, int precision)
+{
+	if (int rc = check_handle(h))
+		return rc;
+	if (int rc = check_prec(precision))
+		return rc;
+	if (h->N < 0)
+		return fail(CC_ERR_STATE, "positions not set");
+	const int64_t N = h->N;
+	const size_t M = h->V.size();
+	const Launch l = choose_launch(h->main.plan, N);
+	if (int rc = run_rho(h, h->main, N, h->d_frac, h->d_E, true, precision == CC_PREC_MIXED, l, h->stream))
+		return rc;
+	if (M == 0)
+		return CC_OK;
+	std::vector<double2> tmp(M);
+	CC_CUDA(cudaMemcpyAsync(tmp.data(), h->main.rho_mode, sizeof(double2) * M, cudaMemcpyDeviceToHost, h->stream));
+	CC_CUDA(cudaStreamSynchronize(h->stream));
+	for (size_t m = 0; m < M; m++) {
+		if (re)
+			re[m] = tmp[m].x;
+		if (im)
+			im[m] = tmp[m].y;
+	}
+	return CC_OK;
+}
+
+int cc_force_one(cc_handle *h, int64_t i, double *f)
+{
+	if (int rc = check_handle(h))
+		return rc;
+	if (h->N < 0)
+		return fail(CC_ERR_STATE, "positions not set");
+	if (i < 0 || i >= h->N || !f)
+		return fail(CC_ERR_ARG, "particle index out of range");
+	if (!h->lastF_valid) {
+		std::vector<double> F((size_t)h->N * h->d);
+		double E;
+		if (int rc = cc_energy_grad(h, &E, F.data(), CC_PREC_FP64))
+			return rc;
+	}
+	for (int e = 0; e < h->d; e++)
+		f[e] = h->lastF[(size_t)i * h->d + e];
+	return CC_OK;
+}
+
+int cc_structure_factor(cc_handle *h, int64_t K, const int32_t *modes, double *S, int precision)
+{
+	if (int rc = check_handle(h))
+		return rc;
+	if (int rc = check_prec(precision))
+		return rc;
+	if (h->N < 0)
+		return fail(CC_ERR_STATE, "positions not set");
+	if (K < 0 || (K > 0 && (!modes || !S)))
+		return fail(CC_ERR_ARG, "invalid k list");
+	if (K == 0)
+		return CC_OK;
+	const int64_t N = h->N;
+	if (N == 0) {
+		for (int64_t q = 0; q < K; q++)
+			S[q] = std::nan("");
+		return CC_OK;
+	}
+	std::vector<int32_t> key(modes, modes + K * h->d);
+	if (key != h->sk_modes || h->sk.segs == nullptr) {
+		std::vector<double> ones((size_t)K, 1.0);
+		cc::Plan plan = cc::build_plan(h->d, K, modes, ones.data(), 0);
+		if (int rc = upload_kset(h->sk, plan))
+			return rc;
+		h->sk_modes = key;
+	}
+	const Launch l = choose_launch(h->sk.plan, N);
+	const double save_off = h->rho_offset;
+	h->rho_offset = 0.0;   // S(k) of the particles themselves (StructureFactor has no fixed-particle offset)
+	int rc = run_rho(h, h->sk, N, h->d_frac, h->d_E + 1, true, precision == CC_PREC_MIXED, l, h->stream);
+	h->rho_offset = save_off;
+	if (rc)
+		return rc;
+	std::vector<double2> tmp((size_t)K);
+	CC_CUDA(cudaMemcpyAsync(tmp.data(), h->sk.rho_mode, sizeof(double2) * K, cudaMemcpyDeviceToHost, h->stream));
+	CC_CUDA(cudaStreamSynchronize(h->stream));
+	for (int64_t q = 0; q < K; q++)
+		S[q] = (tmp[q].x * tmp[q].x + tmp[q].y * tmp[q].y) / (double)N;
+	return CC_OK;
+}
+
+int cc_objective(cc_handle *h, int64_t N, const double *x, double rescale, double *f, double *grad, int precision)
+{
+	if (int rc = check_handle(h))
+		return rc;
+	if (!x || !f || N < 0 || !(rescale != 0.0))
+		return fail(CC_ERR_ARG, "invalid objective arguments");
+	const int d = h->d;
+	// A NaN first variable makes the reference's objective return MaxEnergy with a zero gradient.
+	if (N > 0 && x[0] != x[0]) {
+		*f = 1e10;
+		if (grad)
+			std::fill(grad, grad + N * d, 0.0);
+		return CC_OK;
+	}
+	if (int rc = ensure_particles(h, N))
+		return rc;
+	for (int64_t i = 0; i < N * d; i++) {
+		if (!std::isfinite(x[i]))
+			return fail(CC_ERR_ARG, "non-finite variable");
+		double s = x[i] / rescale;
+		s -= std::floor(s);
+		s -= std::floor(s);
+		h->h_pin[i] = s;
+	}
+	if (N > 0)
+		CC_CUDA(cudaMemcpyAsync(h->d_frac, h->h_pin, sizeof(double) * N * d, cudaMemcpyHostToDevice, h->stream));
+	h->N = N;
+	h->lastF_valid = false;
+	if (int rc = eval_device(h, N, h->d_frac, h->d_E, nullptr, grad ? h->d_gfrac : nullptr, false, precision,
+	                         h->stream))
+		return rc;
+	CC_CUDA(cudaMemcpyAsync(h->h_pin, h->d_E, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+	if (grad && N > 0)
+		CC_CUDA(cudaMemcpyAsync(h->h_pin + 2, h->d_gfrac, sizeof(double) * N * d, cudaMemcpyDeviceToHost,
+		                        h->stream));
+	CC_CUDA(cudaStreamSynchronize(h->stream));
+	*f = h->h_pin[0];
+	if (grad)
+		for (int64_t i = 0; i < N * d; i++)
+			grad[i] = h->h_pin[2 + i] / rescale;
+	return CC_OK;
+}
+
+int cc_set_timing(cc_handle *h, int on)
+{
+	if (int rc = check_handle(h))
+		return rc;
+	h->timing = on != 0;
+	h->ev_used = 0;
+	return CC_OK;
+}
+
+int cc_get_timing(cc_handle *h, double *rho_ms, double *force_ms, int64_t *evals)
+{
+	if (int rc = check_handle(h))
+		return rc;
+	CC_CUDA(cudaDeviceSynchronize());
+	double r = 0, f = 0;
+	for (size_t i = 0; i + 3 <= h->ev_used; i += 3) {
+		float a = 0, b = 0;
+		CC_CUDA(cudaEventElapsedTime(&a, h->ev[i], h->ev[i + 1]));
+		CC_CUDA(cudaEventElapsedTime(&b, h->ev[i + 1], h->ev[i + 2]));
+		r += a;
+		f += b;
+	}
+	if (rho_ms)
+		*rho_ms = r;
+	if (force_ms)
+		*force_ms = f;
+	if (evals)
+		*evals = (int64_t)(h->ev_used / 3);
+	h->ev_used = 0;
+	return CC_OK;
+}
+
+int cc_plan_info(const cc_handle *h, int64_t N, int *L, int64_t *nseg, int *nsplit, int *nksplit)
+{
+	if (int rc = check_handle(h))
+		return rc;
+	const Launch l = choose_launch(h->main.plan, N);
+	if (L)
+		*L = h->main.plan.L;
+	if (nseg)
+		*nseg = (int64_t)h->main.plan.segs.size();
+	if (nsplit)
+		*nsplit = l.nsplit;
+	if (nksplit)
+		*nksplit = l.nksplit;
+	return CC_OK;
+}
+
+int cc_probe_fma_peak(int precision, double *tflops)
+{
+	if (int rc = check_prec(precision))
+		return rc;
+	if (!tflops)
+		return fail(CC_ERR_ARG, "tflops is null");
+	if (int rc = device_ok())
+		return rc;
+	return precision == CC_PREC_FP64 ? probe_peak<double>(tflops) : probe_peak<float>(tflops);
+}
+
+int cc_kset_stealthy(int d, const double *basis, int64_t N, double chi, int type, int64_t cap, int32_t *modes,
+                     double *V, int64_t *M)
+{
+	if (d < 1 || d > 3 || !basis || N < 0 || !(chi >= 0) || type < 0 || type > 3 || !M || cap < 0 ||
+	    (cap > 0 && (!modes || !V)))
+		return fail(CC_ERR_ARG, "invalid k-set arguments");
+	std::vector<int32_t> mv;
+	std::vector<double> vv;
+	if (!cc::stealthy_kset(d, basis, N, chi, type, mv, vv))
+		return fail(CC_ERR_ARG, "degenerate cell basis or k-set too large");
+	*M = (int64_t)vv.size();
+	if (*M > cap)
+		return fail(CC_ERR_ARG, "cap too small for the k-set");
+	std::memcpy(modes, mv.data(), mv.size() * sizeof(int32_t));
+	std::memcpy(V, vv.data(), vv.size() * sizeof(double));
+	return CC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,185 @@
+"""ORACLE — test infrastructure only (tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg).
+
+Two CPU checkers of the collective-coordinate path:
+  * ``Ref``  — the reference's own ShiftedCCPotential / LuksanPLIS compiled from its sources (oracle/_ref/libccref.so,
+    built by oracle/Makefile where the reference tree is present);
+  * ``port`` — the plain-C restatement oracle/cc_oracle.c (oracle/_build/libccoracle.so), pinned to the reference by
+    tests/test_oracle.py and the golden vectors in tests/golden/.
+Nothing on the product path imports this package.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_LIB = os.path.join(HERE, "_ref", "libccref.so")
+PORT_LIB = os.path.join(HERE, "_build", "libccoracle.so")
+REFERENCE_TREE = os.environ.get("CC_REFERENCE_TREE", "/root/reference")
+
+_vp = ctypes.c_void_p
+_l = ctypes.c_long
+_d = ctypes.c_double
+
+
+def build(ref=True):
+    """Build the port (always) and the reference oracle (when the reference tree is present)."""
+    subprocess.run(["make", "-s", "-C", HERE, "port"], check=True)
+    if ref and os.path.isdir(REFERENCE_TREE):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REFERENCE_TREE}"], check=True)
+
+
+def _p(a):
+    return a.ctypes.data_as(_vp) if a is not None else None
+
+
+_REF = None
+_PORT = None
+
+
+def ref_available():
+    return os.path.exists(REF_LIB)
+
+
+def ref_lib():
+    global _REF
+    if _REF is None:
+        lib = ctypes.CDLL(REF_LIB)
+        lib.ccref_create.restype = _vp
+        lib.ccref_create.argtypes = [ctypes.c_int, _vp, _l, _vp, _vp, _vp, _d, ctypes.c_int]
+        lib.ccref_destroy.argtypes = [_vp]
+        lib.ccref_kcart.argtypes = [_vp, _vp]
+        lib.ccref_volume.restype = _d
+        lib.ccref_volume.argtypes = [_vp]
+        lib.ccref_reciprocal.argtypes = [_vp, _vp]
+        lib.ccref_set_positions.argtypes = [_vp, _l, _vp]
+        lib.ccref_eval.argtypes = [_vp, ctypes.POINTER(_d), _vp, _vp, _vp]
+        lib.ccref_force_one.argtypes = [_vp, _l, _vp]
+        lib.ccref_cartesian.argtypes = [_vp, _vp]
+        lib.ccref_structure_factor.argtypes = [_vp, _l, _vp, _vp]
+        lib.ccref_minimize.restype = _d
+        lib.ccref_minimize.argtypes = [_vp, _l, _vp, _d, _l, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_l)]
+        lib.ccref_kset_cli.restype = _l
+        lib.ccref_kset_cli.argtypes = [ctypes.c_int, _vp, _l, _d, ctypes.c_int, _l, _vp, _vp]
+        _REF = lib
+    return _REF
+
+
+def port_lib():
+    global _PORT
+    if _PORT is None:
+        if not os.path.exists(PORT_LIB):
+            build(ref=False)
+        lib = ctypes.CDLL(PORT_LIB)
+        lib.cco_eval.restype = _d
+        lib.cco_eval.argtypes = [ctypes.c_int, _vp, _l, _vp, _l, _vp, _vp, _d, _vp, _vp, _vp]
+        lib.cco_sk.argtypes = [ctypes.c_int, _vp, _l, _vp, _l, _vp, _vp]
+        lib.cco_volume.restype = _d
+        lib.cco_volume.argtypes = [ctypes.c_int, _vp]
+        _PORT = lib
+    return _PORT
+
+
+def lattice_k(basis, modes):
+    """Cartesian k = sum_e n_e b_e with b = 2 pi inv(A)^T (A rows = basis vectors)."""
+    basis = np.asarray(basis, np.float64)
+    B = 2 * np.pi * np.linalg.inv(basis).T
+    return np.asarray(modes, np.float64) @ B
+
+
+class Ref:
+    """The reference's ShiftedCCPotential (Direct backend) over a cell; modes or Cartesian k."""
+
+    def __init__(self, d, basis, V, modes=None, kcart=None, shift=0.0, nthreads=None):
+        self.lib = ref_lib()
+        self.d = d
+        self.basis = np.ascontiguousarray(basis, np.float64).reshape(d, d)
+        V = np.ascontiguousarray(V, np.float64)
+        self.M = len(V)
+        m = np.ascontiguousarray(modes, np.int32) if modes is not None else None
+        k = np.ascontiguousarray(kcart, np.float64) if kcart is not None else None
+        nt = nthreads or os.cpu_count() or 1
+        self.h = self.lib.ccref_create(d, _p(self.basis), self.M, _p(m), _p(k), _p(V), shift, nt)
+        if not self.h:
+            raise ValueError("ccref_create failed")
+        self.N = 0
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.ccref_destroy(self.h)
+            self.h = None
+
+    def kcart(self):
+        out = np.zeros((max(self.M, 1), self.d))
+        self.lib.ccref_kcart(self.h, _p(out))
+        return out[: self.M]
+
+    def volume(self):
+        return self.lib.ccref_volume(self.h)
+
+    def set_positions(self, frac):
+        frac = np.ascontiguousarray(frac, np.float64).reshape(-1, self.d)
+        self.N = len(frac)
+        self.lib.ccref_set_positions(self.h, self.N, _p(frac))
+
+    def eval(self, forces=True):
+        E = _d()
+        F = np.zeros((max(self.N, 1), self.d)) if forces else None
+        re = np.zeros(max(self.M, 1))
+        im = np.zeros(max(self.M, 1))
+        self.lib.ccref_eval(self.h, ctypes.byref(E), _p(F), _p(re), _p(im))
+        return E.value, (F[: self.N] if forces else None), re[: self.M], im[: self.M]
+
+    def force_one(self, i):
+        f = np.zeros(self.d)
+        self.lib.ccref_force_one(self.h, i, _p(f))
+        return f
+
+    def structure_factor(self, kcart):
+        kcart = np.ascontiguousarray(kcart, np.float64).reshape(-1, self.d)
+        S = np.zeros(max(len(kcart), 1))
+        self.lib.ccref_structure_factor(self.h, len(kcart), _p(kcart), _p(S))
+        return S[: len(kcart)]
+
+    def minimize(self, frac, emin=-1.0, maxeval=5000, history=40, fast=0):
+        x = np.ascontiguousarray(frac, np.float64).reshape(-1, self.d).copy()
+        ev = _l()
+        E = self.lib.ccref_minimize(self.h, len(x), _p(x), emin, maxeval, history, fast, ctypes.byref(ev))
+        return E, x, ev.value
+
+
+def ref_kset(d, basis, N, chi, type_=0, cap=400000):
+    lib = ref_lib()
+    basis = np.ascontiguousarray(basis, np.float64).reshape(d, d)
+    modes = np.zeros((cap, d), np.int32)
+    V = np.zeros(cap)
+    M = lib.ccref_kset_cli(d, _p(basis), N, chi, type_, cap, _p(modes), _p(V))
+    if M < 0:
+        raise ValueError("cap too small")
+    return modes[:M].copy(), V[:M].copy()
+
+
+def port_eval(d, basis, frac, kcart, V, shift=0.0):
+    """The C restatement: (E, F, re, im)."""
+    lib = port_lib()
+    basis = np.ascontiguousarray(basis, np.float64).reshape(d, d)
+    frac = np.ascontiguousarray(frac, np.float64).reshape(-1, d)
+    kcart = np.ascontiguousarray(kcart, np.float64).reshape(-1, d)
+    V = np.ascontiguousarray(V, np.float64)
+    N, M = len(frac), len(V)
+    F = np.zeros((max(N, 1), d))
+    re = np.zeros(max(M, 1))
+    im = np.zeros(max(M, 1))
+    E = lib.cco_eval(d, _p(basis), N, _p(frac), M, _p(kcart), _p(V), shift, _p(F), _p(re), _p(im))
+    return E, F[:N], re[:M], im[:M]
+
+
+def port_sk(d, basis, frac, kcart):
+    lib = port_lib()
+    basis = np.ascontiguousarray(basis, np.float64).reshape(d, d)
+    frac = np.ascontiguousarray(frac, np.float64).reshape(-1, d)
+    kcart = np.ascontiguousarray(kcart, np.float64).reshape(-1, d)
+    S = np.zeros(max(len(kcart), 1))
+    lib.cco_sk(d, _p(basis), len(frac), _p(frac), len(kcart), _p(kcart), _p(S))
+    return S[: len(kcart)]
