@@ -110,6 +110,27 @@ int cc_energy_grad_device(cc_handle *h, int64_t N, const double *d_frac, double 
 int cc_kset_stealthy(int d, const double *basis, int64_t N, double chi, int type, int64_t cap, int32_t *modes,
                      double *V, int64_t *M);
 
+/* --- allocation-free evaluation (no counterpart in the reference) -----------------------------------------------
+ * For callers that cannot allocate GPU memory: code running while a CUDA graph is captured (cudaMalloc is refused
+ * under global-mode capture) and processes whose memory manager owns the device's memory. They cannot create a
+ * cc_handle (cc_create allocates). cc_energy_noalloc allocates nothing, on the device or the host: the caller passes
+ * every input and output in its own device memory, and the only scratch is a fixed array of
+ * CC_NOALLOC_SCRATCH_BYTES inside the library, which every GPU that loads the library holds until the process exits.
+ *   d, basis (host, d x d), M modes (device, M x d int32), V (device, M), shift, N fractional positions (device,
+ *   N x d); outputs: d_E (device, 1 double) = sum_m V_m |rho_m|^2 / volume + shift and, if not NULL, d_rho (device,
+ *   M complex doubles as re,im pairs) in mode order. Work is enqueued on `stream` (cudaStream_t, NULL = legacy).
+ * Limits: M <= CC_NOALLOC_MAX_MODES, N <= CC_NOALLOC_MAX_PARTICLES, else CC_ERR_ARG (see cc_noalloc_last_error).
+ * The first call on each device looks up the scratch array's device address (and may load the kernel), so make it
+ * before any stream capture, with that device current. All calls share the one scratch array and each call leaves
+ * its contents behind (the call clears what must start at zero): calls whose work overlaps on the GPU, e.g. on
+ * two streams at once, race and must be serialised by the caller. */
+#define CC_NOALLOC_SCRATCH_BYTES (16u << 20)
+#define CC_NOALLOC_MAX_MODES 262144
+#define CC_NOALLOC_MAX_PARTICLES (1 << 30)
+int cc_energy_noalloc(int d, const double *basis, int64_t M, const int32_t *d_modes, const double *d_V, double shift,
+                      int64_t N, const double *d_frac, double *d_E, double *d_rho, void *stream);
+const char *cc_noalloc_last_error(void);
+
 /* --- measurement support (no counterpart in the reference) --------------------------------------------------- */
 
 /* on = 1: every following evaluation on this handle records CUDA events around its rho and force kernels (on the

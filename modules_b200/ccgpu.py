@@ -56,6 +56,8 @@ _SIGS = {
     "cc_plan_info": (_i, [_vp, _i64, ctypes.POINTER(_i), ctypes.POINTER(_i64), ctypes.POINTER(_i),
                           ctypes.POINTER(_i)]),
     "cc_probe_fma_peak": (_i, [_i, ctypes.POINTER(_d)]),
+    "cc_energy_noalloc": (_i, [_i, _vp, _i64, _vp, _vp, _d, _i64, _vp, _vp, _vp, _vp]),
+    "cc_noalloc_last_error": (ctypes.c_char_p, []),
 }
 
 
