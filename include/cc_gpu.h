@@ -131,15 +131,27 @@ int cc_energy_noalloc(int d, const double *basis, int64_t M, const int32_t *d_mo
                       int64_t N, const double *d_frac, double *d_E, double *d_rho, void *stream);
 const char *cc_noalloc_last_error(void);
 
+/* --- execution path (no counterpart in the reference) ---------------------------------------------------------
+ * CC_PATH_SPLIT (default): three kernels per evaluation (rho, split reduction + energy, forces) chained by
+ * programmatic dependent launch. CC_PATH_FUSED: problems whose per-particle phase tables fit 64 MiB per layout run
+ * as ONE cooperative kernel per evaluation (phases separated by grid barriers whose waits are bounded; larger ones
+ * still take the split path). Results agree to rounding; each path repeats bitwise. */
+enum { CC_PATH_SPLIT = 0, CC_PATH_FUSED = 1 };
+int cc_set_path(cc_handle *h, int path);
+
+/* Synchronise the device and report CC_ERR_TIMEOUT if a bounded grid-barrier wait of an earlier device-path
+ * evaluation ran out (the error is then cleared). Host-path calls check this themselves. */
+int cc_check_device_error(cc_handle *h);
+
 /* --- measurement support (no counterpart in the reference) --------------------------------------------------- */
 
-/* on = 1: every following evaluation on this handle records CUDA events around its rho and force kernels (on the
- * stream they run on); cc_get_timing synchronises and returns the summed kernel times in ms and the number of
- * evaluations timed since timing was switched on, then clears the record. */
+/* on = 1: every following evaluation on this handle records CUDA events around its rho, reduce and force kernels
+ * (on the stream they run on); cc_get_timing synchronises and returns the summed kernel times in ms and the number
+ * of evaluations timed since timing was switched on, then clears the record. */
 int cc_set_timing(cc_handle *h, int on);
-int cc_get_timing(cc_handle *h, double *rho_ms, double *force_ms, int64_t *evals);
+int cc_get_timing(cc_handle *h, double *rho_ms, double *reduce_ms, double *force_ms, int64_t *evals);
 
-/* Launch configuration chosen for N particles: the rho kernel's particle splits and the force kernel's segment
+/* Launch configuration chosen for N particles: the rho kernel's particle splits and the force kernel's unit
  * splits, the segment length L and the number of segments (for reports). */
 int cc_plan_info(const cc_handle *h, int64_t N, int *L, int64_t *nseg, int *nsplit, int *nksplit);
 

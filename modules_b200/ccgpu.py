@@ -52,10 +52,12 @@ _SIGS = {
     "cc_energy_grad_device": (_i, [_vp, _i64, _vp, _vp, _vp, _vp, _i, _vp]),
     "cc_kset_stealthy": (_i, [_i, _vp, _i64, _d, _i, _i64, _vp, _vp, ctypes.POINTER(_i64)]),
     "cc_set_timing": (_i, [_vp, _i]),
-    "cc_get_timing": (_i, [_vp, ctypes.POINTER(_d), ctypes.POINTER(_d), ctypes.POINTER(_i64)]),
+    "cc_get_timing": (_i, [_vp, ctypes.POINTER(_d), ctypes.POINTER(_d), ctypes.POINTER(_d), ctypes.POINTER(_i64)]),
     "cc_plan_info": (_i, [_vp, _i64, ctypes.POINTER(_i), ctypes.POINTER(_i64), ctypes.POINTER(_i),
                           ctypes.POINTER(_i)]),
     "cc_probe_fma_peak": (_i, [_i, ctypes.POINTER(_d)]),
+    "cc_set_path": (_i, [_vp, _i]),
+    "cc_check_device_error": (_i, [_vp]),
     "cc_energy_noalloc": (_i, [_i, _vp, _i64, _vp, _vp, _d, _i64, _vp, _vp, _vp, _vp]),
     "cc_noalloc_last_error": (ctypes.c_char_p, []),
 }
@@ -215,14 +217,21 @@ class CCPotential:
         self.N = n
         return (f.value, g[: len(x)]) if grad else f.value
 
+    def set_path(self, path):
+        """0 = the three-kernel split path (default), 1 = one fused cooperative kernel when the tables fit."""
+        _check(self._lib.cc_set_path(self._h, int(path)))
+
+    def check_device_error(self):
+        _check(self._lib.cc_check_device_error(self._h))
+
     def set_timing(self, on):
         _check(self._lib.cc_set_timing(self._h, 1 if on else 0))
 
     def get_timing(self):
-        """(rho kernel ms, force kernel ms, evaluations) summed since set_timing(True)."""
-        r, f, n = _d(), _d(), _i64()
-        _check(self._lib.cc_get_timing(self._h, ctypes.byref(r), ctypes.byref(f), ctypes.byref(n)))
-        return r.value, f.value, n.value
+        """(rho kernel ms, reduce kernel ms, force kernel ms, evaluations) summed since set_timing(True)."""
+        r, q, f, n = _d(), _d(), _d(), _i64()
+        _check(self._lib.cc_get_timing(self._h, ctypes.byref(r), ctypes.byref(q), ctypes.byref(f), ctypes.byref(n)))
+        return r.value, q.value, f.value, n.value
 
     def plan_info(self, N):
         L, nseg, ns, nk = _i(), _i64(), _i(), _i()

@@ -7,6 +7,7 @@
 //   cc_force_kernel -> Cartesian forces and/or the gradient in fractional coordinates.
 // There is no CPU path: without a CUDA device every call that computes returns CC_ERR_NOGPU.
 #include "../../include/cc_gpu.h"
+#include "cc_fused.cuh"
 #include "cc_kernels.cuh"
 #include "cc_plan.h"
 
@@ -34,37 +35,52 @@ int fail(int code, const std::string &msg)
 			return fail(CC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));                    \
 	} while (0)
 
-constexpr int kWarps = 8;
-constexpr int kChunk = 64;
-constexpr int kSegChunk = 64;
 
 // ---------------------------------------------------------------------------------------------------------------
 // device-side k-set: a Plan uploaded
 // ---------------------------------------------------------------------------------------------------------------
+struct DevSplits {
+	int want = 0;
+	cc::ForceSplits host;
+	int *kstart = nullptr;
+	cc::TabSpec *kspec = nullptr;
+};
+
 struct DevKSet {
 	cc::Plan plan;
 	cc::Seg *segs = nullptr;
+	cc::TabSpec *rspec = nullptr;
+	int *bstart = nullptr;
+	cc::TabSpec *bspec = nullptr;
 	double *slotV = nullptr;
 	int *mode_slot = nullptr;
-	double *modeV = nullptr;
 	double2 *rho_slot = nullptr;
 	double2 *u_slot = nullptr;
 	double2 *rho_mode = nullptr;
-	unsigned *counters = nullptr;   // ngroups + 1
-	double2 *partial = nullptr;     // nsplit_cap * nslot
+	double *eblock = nullptr;       // one per reduce block
+	unsigned *ticket = nullptr;
+	double2 *partial = nullptr;     // partial rows * nslot
 	size_t partial_cap = 0;         // in double2 elements
+	std::vector<DevSplits> splits;  // force splits per requested count
 
 	void release()
 	{
 		cudaFree(segs);
+		cudaFree(rspec);
+		cudaFree(bstart);
+		cudaFree(bspec);
 		cudaFree(slotV);
 		cudaFree(mode_slot);
-		cudaFree(modeV);
 		cudaFree(rho_slot);
 		cudaFree(u_slot);
 		cudaFree(rho_mode);
-		cudaFree(counters);
+		cudaFree(eblock);
+		cudaFree(ticket);
 		cudaFree(partial);
+		for (DevSplits &f : splits) {
+			cudaFree(f.kstart);
+			cudaFree(f.kspec);
+		}
 		*this = DevKSet();
 	}
 };
@@ -81,21 +97,29 @@ template <class T> int dev_alloc(T **p, size_t n)
 	return CC_OK;
 }
 
+template <class T> int upload(T **p, const std::vector<T> &v)
+{
+	if (int rc = dev_alloc(p, v.size()))
+		return rc;
+	if (!v.empty())
+		CC_CUDA(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+	return CC_OK;
+}
+
 int upload_kset(DevKSet &k, const cc::Plan &plan)
 {
 	k.release();
 	k.plan = plan;
 	int rc;
-	const size_t nseg = plan.segs.size(), nslot = plan.slotV.size(), M = plan.mode_slot.size();
-	if ((rc = dev_alloc(&k.segs, nseg)) || (rc = dev_alloc(&k.slotV, nslot)) || (rc = dev_alloc(&k.mode_slot, M)) ||
-	    (rc = dev_alloc(&k.modeV, M)) || (rc = dev_alloc(&k.rho_slot, nslot)) || (rc = dev_alloc(&k.u_slot, nslot)) ||
-	    (rc = dev_alloc(&k.rho_mode, M)) || (rc = dev_alloc(&k.counters, plan.ngroups + 1)))
+	const size_t nslot = plan.slotV.size(), M = plan.mode_slot.size();
+	const size_t nred = (nslot + 31) / 32;
+	if ((rc = upload(&k.segs, plan.segs)) || (rc = upload(&k.rspec, plan.rspec)) || (rc = upload(&k.slotV, plan.slotV)) ||
+	    (rc = upload(&k.bstart, plan.bstart)) || (rc = upload(&k.bspec, plan.bspec)) ||
+	    (rc = upload(&k.mode_slot, plan.mode_slot)) || (rc = dev_alloc(&k.rho_slot, nslot)) ||
+	    (rc = dev_alloc(&k.u_slot, nslot)) || (rc = dev_alloc(&k.rho_mode, M)) || (rc = dev_alloc(&k.eblock, nred)) ||
+	    (rc = dev_alloc(&k.ticket, 1)))
 		return rc;
-	CC_CUDA(cudaMemcpy(k.segs, plan.segs.data(), nseg * sizeof(cc::Seg), cudaMemcpyHostToDevice));
-	CC_CUDA(cudaMemcpy(k.slotV, plan.slotV.data(), nslot * sizeof(double), cudaMemcpyHostToDevice));
-	CC_CUDA(cudaMemcpy(k.mode_slot, plan.mode_slot.data(), M * sizeof(int), cudaMemcpyHostToDevice));
-	CC_CUDA(cudaMemcpy(k.modeV, plan.modeV.data(), M * sizeof(double), cudaMemcpyHostToDevice));
-	CC_CUDA(cudaMemset(k.counters, 0, (plan.ngroups + 1) * sizeof(unsigned)));
+	CC_CUDA(cudaMemset(k.ticket, 0, sizeof(unsigned)));
 	return CC_OK;
 }
 
@@ -124,6 +148,17 @@ struct cc_handle {
 	size_t pin_cap = 0;
 	std::vector<double> lastF;      // forces of the last cc_energy_grad
 	bool lastF_valid = false;
+	// fused (cooperative) path
+	cc::TabSpec gspec;
+	void *d_tabP = nullptr, *d_tabE = nullptr;
+	size_t tab_cap = 0;             // bytes of each table buffer
+	unsigned *d_bar = nullptr;      // grid barrier words (arrivals, generation, error)
+	double *d_eblockF = nullptr;
+	int eblockF_cap = 0;
+	double2 *d_partialF = nullptr;
+	size_t partialF_cap = 0;
+	std::vector<std::pair<int, int *> > kstarts;   // even segment splits per count
+	bool use_fused = false;         // cc_set_path
 	bool timing = false;            // cc_set_timing
 	std::vector<cudaEvent_t> ev;    // 3 events per timed evaluation
 	size_t ev_used = 0;
@@ -135,8 +170,8 @@ namespace {
 // launch configuration
 // ---------------------------------------------------------------------------------------------------------------
 struct Launch {
-	int nsplit, per_split;          // rho
-	int nksplit, segs_per_split;    // force
+	int nsplit, per_split, csize, chunk;   // rho: particle splits (a multiple of the cluster size)
+	int want_force;                       // force: requested number of segment splits
 };
 
 int sm_count()
@@ -151,81 +186,148 @@ int sm_count()
 	return n;
 }
 
-Launch choose_launch(const cc::Plan &p, int64_t N)
+constexpr size_t kRhoTabBudget = 48 * 1024;   // shared memory for one chunk of rho tables
+
+Launch choose_launch(const cc::Plan &p, int64_t N, bool mixed)
 {
 	Launch l;
-	const int target = sm_count() * 3;   // resident blocks of 256 threads at the rho kernel's shared memory
-	// rho: enough particle splits to fill the chip, each split at least 2 particles per warp
-	int ns = std::max(1, (target + p.ngroups - 1) / std::max(1, p.ngroups));
-	ns = (int)std::min<int64_t>(ns, std::max<int64_t>(1, N / (2 * kWarps)));
+	const int target = sm_count() * 4;   // resident 256-thread blocks
+	// rho: particle splits to fill the chip, at least 2 particles per block; clusters of up to 8 splits
+	const int ng = std::max(1, p.nbgroups());
+	int ns = std::max(1, (target + ng - 1) / ng);
+	ns = (int)std::min<int64_t>(ns, std::max<int64_t>(1, N / 2));
+	ns = std::min(ns, 4096);
+	l.csize = ns >= 8 ? 8 : ns >= 4 ? 4 : ns >= 2 ? 2 : 1;
+	ns = (ns + l.csize - 1) / l.csize * l.csize;
 	l.per_split = (int)std::max<int64_t>(1, (N + ns - 1) / ns);
-	l.nsplit = N > 0 ? (int)((N + l.per_split - 1) / l.per_split) : 1;
+	l.nsplit = ns;
+	const size_t esz = mixed ? sizeof(float2) : sizeof(double2);
+	l.chunk = (int)std::max<size_t>(8, std::min<size_t>(64, kRhoTabBudget / (esz * std::max(1, p.block_max_row | 1))));
 	// force: split the segments when there are too few particle groups
-	const int nseg = (int)p.segs.size();
-	const int64_t pg = (N + 31) / 32;
-	int nk = (int)std::max<int64_t>(1, (target + pg - 1) / std::max<int64_t>(1, pg));
-	nk = std::min(nk, std::max(1, nseg / (2 * kWarps)));
-	l.segs_per_split = std::max(1, (nseg + nk - 1) / nk);
-	l.nksplit = std::max(1, (nseg + l.segs_per_split - 1) / l.segs_per_split);
+	const int64_t pg = std::max<int64_t>(1, (N + 31) / 32);
+	l.want_force = (int)std::max<int64_t>(1, std::min<int64_t>((target + pg - 1) / pg, 1024));
 	return l;
 }
 
 // ---------------------------------------------------------------------------------------------------------------
 // kernel dispatch
 // ---------------------------------------------------------------------------------------------------------------
-template <int D, int L, bool MIXED> int launch_rho_t(const cc::RhoArgs &a, int nsplit, cudaStream_t st)
+// Launch with programmatic stream serialization: the kernel may be scheduled while the previous kernel on the stream
+// drains; it calls cudaGridDependencySynchronize() before it reads that kernel's results.
+template <typename Kern, typename Arg>
+cudaError_t launch_pdl(Kern kern, dim3 grid, dim3 block, size_t smem, cudaStream_t st, const Arg &a)
 {
-	typedef cc::RhoSmem<D, L, kWarps, kChunk, MIXED> Lay;
-	auto kern = cc::cc_rho_kernel<D, L, kWarps, kChunk, MIXED>;
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = grid;
+	cfg.blockDim = block;
+	cfg.dynamicSmemBytes = smem;
+	cfg.stream = st;
+	cudaLaunchAttribute attr[1];
+	attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+	attr[0].val.programmaticStreamSerializationAllowed = 1;
+	cfg.attrs = attr;
+	cfg.numAttrs = 1;
+	return cudaLaunchKernelEx(&cfg, kern, a);
+}
+template <typename C> size_t rho_smem(int row, int chunk, int L)
+{
+	return std::max((size_t)chunk * (row | 1) * sizeof(C), (size_t)cc::kRhoWarps * 32 * L * sizeof(double2));
+}
+template <typename C> size_t force_smem(int row, int d)
+{
+	return std::max((size_t)row * 32 * sizeof(C), (size_t)cc::kForceWarps * 32 * d * sizeof(double));
+}
+
+template <int D, int L, bool MIXED> int launch_rho_t(const cc::RhoArgs &a, int ngroups, int nsplit, int csize, int row,
+                                                     cudaStream_t st)
+{
+	typedef typename std::conditional<MIXED, float2, double2>::type C;
+	auto kern = cc::cc_rho_kernel<D, L, MIXED>;
 	static bool attr = false;
 	if (!attr) {
-		CC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::bytes));
+		CC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                             (int)rho_smem<C>(cc::kMaxRow, 64, L)));
 		attr = true;
 	}
-	kern<<<dim3(a.ngroups, nsplit), kWarps * 32, Lay::bytes, st>>>(a);
-	CC_CUDA(cudaGetLastError());
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = dim3(ngroups, nsplit);
+	cfg.blockDim = dim3(cc::kRhoThreads);
+	cfg.dynamicSmemBytes = rho_smem<C>(row, a.chunk, L);
+	cfg.stream = st;
+	cudaLaunchAttribute attrs[2];
+	attrs[0].id = cudaLaunchAttributeClusterDimension;
+	attrs[0].val.clusterDim.x = 1;
+	attrs[0].val.clusterDim.y = csize;
+	attrs[0].val.clusterDim.z = 1;
+	attrs[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+	attrs[1].val.programmaticStreamSerializationAllowed = 1;
+	cfg.attrs = attrs;
+	cfg.numAttrs = 2;
+	CC_CUDA(cudaLaunchKernelEx(&cfg, kern, a));
 	return CC_OK;
 }
 
-template <int D, int L, bool MIXED> int launch_force_t(const cc::ForceArgs &a, int64_t N, cudaStream_t st)
+template <int D, int L, bool MIXED> int launch_force_t(const cc::ForceArgs &a, int64_t N, int row, cudaStream_t st)
 {
-	auto kern = cc::cc_force_kernel<D, L, kWarps, kSegChunk, MIXED>;
-	kern<<<dim3((unsigned)((N + 31) / 32), a.nksplit), kWarps * 32, 0, st>>>(a);
-	CC_CUDA(cudaGetLastError());
+	typedef typename std::conditional<MIXED, float2, double2>::type C;
+	auto kern = cc::cc_force_kernel<D, L, MIXED>;
+	static bool attr = false;
+	if (!attr) {
+		CC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                             (int)force_smem<C>(cc::kMaxRow, D)));
+		attr = true;
+	}
+	CC_CUDA(launch_pdl(kern, dim3((unsigned)((N + 31) / 32), a.nksplit), dim3(cc::kForceThreads), force_smem<C>(row, D),
+	                   st, a));
 	return CC_OK;
 }
 
-template <int D> int launch_rho_d(const cc::RhoArgs &a, int L, bool mixed, int nsplit, cudaStream_t st)
+template <int D> int launch_rho_d(const cc::RhoArgs &a, bool mixed, int ngroups, int nsplit, int csize, int row,
+                                  cudaStream_t st)
 {
-	if (L == 8)
-		return mixed ? launch_rho_t<D, 8, true>(a, nsplit, st) : launch_rho_t<D, 8, false>(a, nsplit, st);
-	return mixed ? launch_rho_t<D, 16, true>(a, nsplit, st) : launch_rho_t<D, 16, false>(a, nsplit, st);
+	return mixed ? launch_rho_t<D, 8, true>(a, ngroups, nsplit, csize, row, st)
+	             : launch_rho_t<D, 8, false>(a, ngroups, nsplit, csize, row, st);
 }
-template <int D> int launch_force_d(const cc::ForceArgs &a, int L, bool mixed, int64_t N, cudaStream_t st)
+template <int D> int launch_force_d(const cc::ForceArgs &a, bool mixed, int64_t N, int row, cudaStream_t st)
 {
-	if (L == 8)
-		return mixed ? launch_force_t<D, 8, true>(a, N, st) : launch_force_t<D, 8, false>(a, N, st);
-	return mixed ? launch_force_t<D, 16, true>(a, N, st) : launch_force_t<D, 16, false>(a, N, st);
+	return mixed ? launch_force_t<D, 8, true>(a, N, row, st) : launch_force_t<D, 8, false>(a, N, row, st);
 }
 
-int launch_rho(int d, const cc::RhoArgs &a, int L, bool mixed, int nsplit, cudaStream_t st)
+int launch_rho(int d, const cc::RhoArgs &a, bool mixed, int ngroups, int nsplit, int csize, int row, cudaStream_t st)
 {
 	switch (d) {
-	case 1: return launch_rho_d<1>(a, L, mixed, nsplit, st);
-	case 2: return launch_rho_d<2>(a, L, mixed, nsplit, st);
-	default: return launch_rho_d<3>(a, L, mixed, nsplit, st);
+	case 1: return launch_rho_d<1>(a, mixed, ngroups, nsplit, csize, row, st);
+	case 2: return launch_rho_d<2>(a, mixed, ngroups, nsplit, csize, row, st);
+	default: return launch_rho_d<3>(a, mixed, ngroups, nsplit, csize, row, st);
 	}
 }
-int launch_force(int d, const cc::ForceArgs &a, int L, bool mixed, int64_t N, cudaStream_t st)
+int launch_force(int d, const cc::ForceArgs &a, bool mixed, int64_t N, int row, cudaStream_t st)
 {
 	switch (d) {
-	case 1: return launch_force_d<1>(a, L, mixed, N, st);
-	case 2: return launch_force_d<2>(a, L, mixed, N, st);
-	default: return launch_force_d<3>(a, L, mixed, N, st);
+	case 1: return launch_force_d<1>(a, mixed, N, row, st);
+	case 2: return launch_force_d<2>(a, mixed, N, row, st);
+	default: return launch_force_d<3>(a, mixed, N, row, st);
 	}
 }
 
-__global__ void set_scalar_kernel(double *p, double v) { *p = v; }
+// force splits for `want`, uploaded once and cached on the k-set
+int get_splits(DevKSet &k, int want, const DevSplits **out)
+{
+	for (const DevSplits &f : k.splits)
+		if (f.want == want) {
+			*out = &f;
+			return CC_OK;
+		}
+	DevSplits f;
+	f.want = want;
+	f.host = cc::force_splits(k.plan, want);
+	int rc;
+	if ((rc = upload(&f.kstart, f.host.start)) || (rc = upload(&f.kspec, f.host.spec)))
+		return rc;
+	k.splits.push_back(f);
+	*out = &k.splits.back();
+	return CC_OK;
+}
 
 // ---------------------------------------------------------------------------------------------------------------
 // buffers
@@ -291,41 +393,56 @@ int ensure_partialG(cc_handle *h, size_t elems)
 	return CC_OK;
 }
 
-// rho pass of k-set `k` over N device positions; writes the energy to d_E (weights of k's plan).
+// rho pass of k-set `k` over N device positions: rho per slot, u, and the energy into d_E.
 int run_rho(cc_handle *h, DevKSet &k, int64_t N, const double *d_frac, double *d_E, bool want_rho_mode, bool mixed,
-            const Launch &l, cudaStream_t st)
+            const Launch &l, cudaStream_t st, cudaEvent_t after_rho = nullptr)
 {
 	const cc::Plan &p = k.plan;
-	if (p.ngroups == 0) {
-		set_scalar_kernel<<<1, 1, 0, st>>>(d_E, h->shift);
+	if (p.nslot == 0) {
+		cc::cc_set_scalar_kernel<<<1, 1, 0, st>>>(d_E, h->shift);
 		CC_CUDA(cudaGetLastError());
 		return CC_OK;
 	}
-	int rc = ensure_partial(k, (size_t)l.nsplit * p.nslot);
-	if (rc)
+	const int nsplit = N > 0 ? l.nsplit : 1;
+	const int csize = N > 0 ? l.csize : 1;
+	const int rows = nsplit / csize;
+	if (int rc = ensure_partial(k, (size_t)rows * p.nslot))
 		return rc;
 	cc::RhoArgs a;
 	a.frac = d_frac;
 	a.N = (int)N;
 	a.per_split = N > 0 ? l.per_split : 0;
-	a.nsplit = N > 0 ? l.nsplit : 1;
+	a.chunk = l.chunk;
 	a.segs = k.segs;
-	a.ngroups = p.ngroups;
+	a.bstart = k.bstart;
+	a.bspec = k.bspec;
+	a.nseg = (int)p.segs.size();
 	a.nslot = p.nslot;
 	a.partial = k.partial;
-	a.counters = k.counters;
-	a.rho_slot = k.rho_slot;
-	a.slotV = k.slotV;
-	a.u_slot = k.u_slot;
-	a.mode_slot = k.mode_slot;
-	a.modeV = k.modeV;
-	a.M = (int)p.mode_slot.size();
-	a.rho_offset = h->rho_offset;
-	a.inv_vol = 1.0 / h->volume;
-	a.shift = h->shift;
-	a.E_out = d_E;
-	a.rho_mode = want_rho_mode ? k.rho_mode : nullptr;
-	return launch_rho(h->d, a, p.L, mixed, a.nsplit, st);
+	if (int rc = launch_rho(h->d, a, mixed, p.nbgroups(), nsplit, csize, p.block_max_row, st))
+		return rc;
+	if (after_rho)
+		CC_CUDA(cudaEventRecord(after_rho, st));
+	cc::ReduceArgs r;
+	r.partial = k.partial;
+	r.nsplit = rows;
+	r.nslot = p.nslot;
+	r.slotV = k.slotV;
+	r.rho_offset = h->rho_offset;
+	r.rho_slot = k.rho_slot;
+	r.u_slot = k.u_slot;
+	r.eblock = k.eblock;
+	r.ticket = k.ticket;
+	r.inv_vol = 1.0 / h->volume;
+	r.shift = h->shift;
+	r.E_out = d_E;
+	CC_CUDA(launch_pdl(cc::cc_reduce_kernel, dim3((p.nslot + 31) / 32), dim3(cc::kRedThreads), 0, st, r));
+	if (want_rho_mode && !p.mode_slot.empty()) {
+		const int M = (int)p.mode_slot.size();
+		cc::cc_gather_rho_kernel<<<(M + 255) / 256, 256, 0, st>>>(k.rho_slot, k.mode_slot, M, k.rho_mode);
+		CC_CUDA(cudaGetLastError());
+	}
+	return CC_OK;
 }
 
 int run_force(cc_handle *h, int64_t N, const double *d_frac, double *d_F, double *d_gfrac, bool mixed,
@@ -334,15 +451,19 @@ int run_force(cc_handle *h, int64_t N, const double *d_frac, double *d_F, double
 	const cc::Plan &p = h->main.plan;
 	if (N == 0)
 		return CC_OK;
-	if (p.ngroups == 0) {
+	if (p.nslot == 0) {
 		if (d_F)
 			CC_CUDA(cudaMemsetAsync(d_F, 0, sizeof(double) * N * h->d, st));
 		if (d_gfrac)
 			CC_CUDA(cudaMemsetAsync(d_gfrac, 0, sizeof(double) * N * h->d, st));
 		return CC_OK;
 	}
-	if (l.nksplit > 1) {
-		int rc = ensure_partialG(h, (size_t)l.nksplit * N * h->d);
+	const DevSplits *f = nullptr;
+	if (int rc = get_splits(h->main, l.want_force, &f))
+		return rc;
+	const int nk = f->host.count();
+	if (nk > 1) {
+		int rc = ensure_partialG(h, (size_t)nk * N * h->d);
 		if (rc)
 			return rc;
 	}
@@ -350,10 +471,11 @@ int run_force(cc_handle *h, int64_t N, const double *d_frac, double *d_F, double
 	a.frac = d_frac;
 	a.N = (int)N;
 	a.segs = h->main.segs;
-	a.nseg = (int)p.segs.size();
-	a.segs_per_split = l.segs_per_split;
-	a.nksplit = l.nksplit;
+	a.kstart = f->kstart;
+	a.kspec = f->kspec;
+	a.nksplit = nk;
 	a.u_slot = h->main.u_slot;
+	a.nseg = (int)p.segs.size();
 	a.partialG = h->d_partialG;
 	a.counters = h->d_fcounters;
 	for (int i = 0; i < 9; i++)
@@ -361,7 +483,184 @@ int run_force(cc_handle *h, int64_t N, const double *d_frac, double *d_F, double
 	a.fscale = 2.0 / h->volume;
 	a.F_out = d_F;
 	a.gfrac_out = d_gfrac;
-	return launch_force(h->d, a, p.L, mixed, N, st);
+	return launch_force(h->d, a, mixed, N, f->host.max_row, st);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// fused path: one cooperative launch per evaluation (tables in global memory, grid barriers)
+// ---------------------------------------------------------------------------------------------------------------
+constexpr size_t kFusedTabCap = 64u << 20;   // bytes per table layout: beyond this the three-kernel path runs
+
+bool fused_eligible(const cc_handle *h, int64_t N, bool mixed)
+{
+	if (N <= 0 || h->main.plan.nslot == 0)
+		return false;
+	const size_t esz = mixed ? sizeof(float2) : sizeof(double2);
+	const size_t Npad = (size_t)(N + 31) / 32 * 32;
+	return (size_t)((h->gspec.row | 1)) * Npad * esz <= kFusedTabCap;
+}
+
+template <int D, int L, bool MIXED> int fused_grid(int *grid)
+{
+	static int per_sm = -1;
+	if (per_sm < 0) {
+		CC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cc::cc_fused_kernel<D, L, MIXED>,
+		                                                     cc::kFusedThreads, 0));
+		if (per_sm < 1)
+			return fail(CC_ERR_CUDA, "fused kernel cannot be resident");
+	}
+	*grid = per_sm * sm_count();
+	return CC_OK;
+}
+
+template <int D, int L, bool MIXED> int launch_fused_t(cc::FusedArgs &a, int grid, cudaStream_t st)
+{
+	void *args[] = {&a};
+	CC_CUDA(cudaLaunchCooperativeKernel((const void *)cc::cc_fused_kernel<D, L, MIXED>, dim3(grid),
+	                                    dim3(cc::kFusedThreads), args, 0, st));
+	return CC_OK;
+}
+
+int fused_grid_d(int d, bool mixed, int *grid)
+{
+	switch (d) {
+	case 1: return mixed ? fused_grid<1, 8, true>(grid) : fused_grid<1, 8, false>(grid);
+	case 2: return mixed ? fused_grid<2, 8, true>(grid) : fused_grid<2, 8, false>(grid);
+	default: return mixed ? fused_grid<3, 8, true>(grid) : fused_grid<3, 8, false>(grid);
+	}
+}
+
+int launch_fused(int d, bool mixed, cc::FusedArgs &a, int grid, cudaStream_t st)
+{
+	switch (d) {
+	case 1: return mixed ? launch_fused_t<1, 8, true>(a, grid, st) : launch_fused_t<1, 8, false>(a, grid, st);
+	case 2: return mixed ? launch_fused_t<2, 8, true>(a, grid, st) : launch_fused_t<2, 8, false>(a, grid, st);
+	default: return mixed ? launch_fused_t<3, 8, true>(a, grid, st) : launch_fused_t<3, 8, false>(a, grid, st);
+	}
+}
+
+int get_kstart(cc_handle *h, int nks, int **out)
+{
+	for (auto &kv : h->kstarts)
+		if (kv.first == nks) {
+			*out = kv.second;
+			return CC_OK;
+		}
+	const int nseg = (int)h->main.plan.segs.size();
+	std::vector<int> ks(nks + 1);
+	for (int k = 0; k <= nks; k++)
+		ks[k] = (int)((int64_t)nseg * k / nks);
+	int *d = nullptr;
+	if (int rc = upload(&d, ks))
+		return rc;
+	h->kstarts.push_back(std::make_pair(nks, d));
+	*out = d;
+	return CC_OK;
+}
+
+template <class T> int grow(T **p, size_t &cap, size_t n)
+{
+	if (n <= cap)
+		return CC_OK;
+	cudaFree(*p);
+	*p = nullptr;
+	cap = 0;
+	if (int rc = dev_alloc(p, n))
+		return rc;
+	cap = n;
+	return CC_OK;
+}
+
+int run_fused(cc_handle *h, int64_t N, const double *d_frac, double *d_E, double *d_F, double *d_gfrac, bool mixed,
+              cudaStream_t st)
+{
+	const cc::Plan &p = h->main.plan;
+	int grid = 0;
+	if (int rc = fused_grid_d(h->d, mixed, &grid))
+		return rc;
+	const size_t esz = mixed ? sizeof(float2) : sizeof(double2);
+	const int Npad = (int)((N + 31) / 32 * 32);
+	const int rowP = h->gspec.row | 1;
+	const size_t tab_bytes = std::max((size_t)rowP * Npad, (size_t)h->gspec.row * Npad) * esz;
+	if (tab_bytes > h->tab_cap) {
+		cudaFree(h->d_tabP);
+		cudaFree(h->d_tabE);
+		h->d_tabP = h->d_tabE = nullptr;
+		h->tab_cap = 0;
+		unsigned char *a = nullptr, *b = nullptr;
+		int rc;
+		if ((rc = dev_alloc(&a, tab_bytes)) || (rc = dev_alloc(&b, tab_bytes)))
+			return rc;
+		h->d_tabP = a;
+		h->d_tabE = b;
+		h->tab_cap = tab_bytes;
+	}
+	const int ng = p.ngroups();
+	int nsplit = std::max(1, (2 * grid + ng - 1) / ng);
+	nsplit = (int)std::min<int64_t>(nsplit, std::max<int64_t>(1, N / 16));
+	const int per_split = (int)((N + nsplit - 1) / nsplit);
+	nsplit = (int)((N + per_split - 1) / per_split);
+	const int pg = (int)((N + 31) / 32);
+	const int nseg = (int)p.segs.size();
+	int nks = std::max(1, (2 * grid + pg - 1) / pg);
+	nks = std::min(nks, std::max(1, nseg / 64));
+	int *kstart = nullptr;
+	size_t eb_cap = (size_t)h->eblockF_cap;
+	if (int rc = get_kstart(h, nks, &kstart))
+		return rc;
+	if (int rc = grow(&h->d_eblockF, eb_cap, (size_t)grid))
+		return rc;
+	h->eblockF_cap = (int)eb_cap;
+	if (int rc = grow(&h->d_partialF, h->partialF_cap, (size_t)nsplit * p.nslot))
+		return rc;
+	if (nks > 1)
+		if (int rc = ensure_partialG(h, (size_t)nks * N * h->d))
+			return rc;
+	cc::FusedArgs a;
+	a.frac = d_frac;
+	a.N = (int)N;
+	a.segs = h->main.segs;
+	a.ngroups = ng;
+	a.nseg = nseg;
+	a.nslot = p.nslot;
+	a.slotV = h->main.slotV;
+	a.rho_offset = h->rho_offset;
+	a.inv_vol = 1.0 / h->volume;
+	a.shift = h->shift;
+	a.spec = h->gspec;
+	a.tabP = h->d_tabP;
+	a.tabE = h->d_tabE;
+	a.Npad = Npad;
+	a.nsplit = nsplit;
+	a.per_split = per_split;
+	a.partial = h->d_partialF;
+	a.rho_slot = h->main.rho_slot;
+	a.u_slot = h->main.u_slot;
+	a.eblock = h->d_eblockF;
+	a.kstart = kstart;
+	a.nksplit = nks;
+	a.partialG = h->d_partialG;
+	a.fcounters = h->d_fcounters;
+	for (int i = 0; i < 9; i++)
+		a.recip[i] = h->recip[i];
+	a.fscale = 2.0 / h->volume;
+	a.F_out = d_F;
+	a.gfrac_out = d_gfrac;
+	a.E_out = d_E;
+	a.bar = h->d_bar;
+	return launch_fused(h->d, mixed, a, grid, st);
+}
+
+// A grid barrier of an earlier fused launch that ran out of time leaves its error word set: report it and reset.
+int check_barrier(cc_handle *h)
+{
+	unsigned w[3] = {0, 0, 0};
+	CC_CUDA(cudaMemcpy(w, h->d_bar, sizeof(w), cudaMemcpyDeviceToHost));
+	if (w[2] != 0u) {
+		CC_CUDA(cudaMemset(h->d_bar, 0, 3 * sizeof(unsigned)));
+		return fail(CC_ERR_TIMEOUT, "a grid barrier wait ran out in the fused evaluation kernel");
+	}
+	return CC_OK;
 }
 
 int check_handle(const cc_handle *h)
@@ -422,8 +721,10 @@ int create_common(int d, const double *basis, int64_t M, const int32_t *modes, c
 		delete h;
 		return fail(CC_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
 	}
-	cc::Plan plan = cc::build_plan(d, M, modes, V, 0);
-	if ((rc = upload_kset(h->main, plan)) || (rc = dev_alloc(&h->d_E, 2))) {
+	cc::Plan plan = cc::build_plan(d, M, modes, V, 8);
+	h->gspec = cc::global_spec(plan);
+	if ((rc = upload_kset(h->main, plan)) || (rc = dev_alloc(&h->d_E, 2)) || (rc = dev_alloc(&h->d_bar, 4)) ||
+	    (rc = (cudaMemset(h->d_bar, 0, 4 * sizeof(unsigned)) == cudaSuccess ? CC_OK : CC_ERR_CUDA))) {
 		cc_destroy(h);
 		return rc;
 	}
@@ -446,24 +747,37 @@ int eval_device(cc_handle *h, int64_t N, const double *d_frac, double *d_E, doub
                 bool want_rho_mode, int precision, cudaStream_t st)
 {
 	const bool mixed = precision == CC_PREC_MIXED;
-	const Launch l = choose_launch(h->main.plan, N);
-	cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
-	if (h->timing && h->ev_used + 3 <= 3 * 100000) {
+	const Launch l = choose_launch(h->main.plan, N, mixed);
+	cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
+	if (h->timing && h->ev_used + 4 <= 4 * 100000) {
 		e0 = next_event(h);
 		e1 = next_event(h);
 		e2 = next_event(h);
-		if (e0 && e1 && e2)
-			CC_CUDA(cudaEventRecord(e0, st));
+		e3 = next_event(h);
+		if (!(e0 && e1 && e2 && e3))
+			return fail(CC_ERR_CUDA, "cudaEventCreate failed");
+		CC_CUDA(cudaEventRecord(e0, st));
 	}
-	int rc = run_rho(h, h->main, N, d_frac, d_E, want_rho_mode, mixed, l, st);
+	if (!want_rho_mode && h->use_fused && fused_eligible(h, N, mixed)) {
+		// one cooperative launch: the whole evaluation is reported as the force interval
+		if (e1)
+			CC_CUDA(cudaEventRecord(e1, st));
+		if (e2)
+			CC_CUDA(cudaEventRecord(e2, st));
+		int rc = run_fused(h, N, d_frac, d_E, d_F, d_gfrac, mixed, st);
+		if (e3)
+			CC_CUDA(cudaEventRecord(e3, st));
+		return rc;
+	}
+	int rc = run_rho(h, h->main, N, d_frac, d_E, want_rho_mode, mixed, l, st, e1);
 	if (rc)
 		return rc;
-	if (e1)
-		CC_CUDA(cudaEventRecord(e1, st));
-	if (d_F || d_gfrac)
-		rc = run_force(h, N, d_frac, d_F, d_gfrac, mixed, l, st);
 	if (e2)
 		CC_CUDA(cudaEventRecord(e2, st));
+	if (d_F || d_gfrac)
+		rc = run_force(h, N, d_frac, d_F, d_gfrac, mixed, l, st);
+	if (e3)
+		CC_CUDA(cudaEventRecord(e3, st));
 	return rc;
 }
 
@@ -560,6 +874,13 @@ int cc_destroy(cc_handle *h)
 	cudaFree(h->d_fcounters);
 	cudaFree(h->d_E);
 	cudaFreeHost(h->h_pin);
+	cudaFree(h->d_tabP);
+	cudaFree(h->d_tabE);
+	cudaFree(h->d_bar);
+	cudaFree(h->d_eblockF);
+	cudaFree(h->d_partialF);
+	for (auto &kv : h->kstarts)
+		cudaFree(kv.second);
 	for (cudaEvent_t e : h->ev)
 		cudaEventDestroy(e);
 	if (h->stream)
@@ -638,6 +959,8 @@ int cc_energy_grad(cc_handle *h, double *E, double *F, int precision)
 	if (F && N > 0)
 		CC_CUDA(cudaMemcpyAsync(h->h_pin + 2, h->d_F, sizeof(double) * N * h->d, cudaMemcpyDeviceToHost, h->stream));
 	CC_CUDA(cudaStreamSynchronize(h->stream));
+	if (int rc = check_barrier(h))
+		return rc;
 	*E = h->h_pin[0];
 	if (F && N > 0) {
 		std::memcpy(F, h->h_pin + 2, sizeof(double) * N * h->d);
@@ -673,7 +996,7 @@ int cc_rho(cc_handle *h, double *re, double *im, int precision)
 		return fail(CC_ERR_STATE, "positions not set");
 	const int64_t N = h->N;
 	const size_t M = h->V.size();
-	const Launch l = choose_launch(h->main.plan, N);
+	const Launch l = choose_launch(h->main.plan, N, precision == CC_PREC_MIXED);
 	if (int rc = run_rho(h, h->main, N, h->d_frac, h->d_E, true, precision == CC_PREC_MIXED, l, h->stream))
 		return rc;
 	if (M == 0)
@@ -730,12 +1053,12 @@ int cc_structure_factor(cc_handle *h, int64_t K, const int32_t *modes, double *S
 	std::vector<int32_t> key(modes, modes + K * h->d);
 	if (key != h->sk_modes || h->sk.segs == nullptr) {
 		std::vector<double> ones((size_t)K, 1.0);
-		cc::Plan plan = cc::build_plan(h->d, K, modes, ones.data(), 0);
+		cc::Plan plan = cc::build_plan(h->d, K, modes, ones.data(), 8);
 		if (int rc = upload_kset(h->sk, plan))
 			return rc;
 		h->sk_modes = key;
 	}
-	const Launch l = choose_launch(h->sk.plan, N);
+	const Launch l = choose_launch(h->sk.plan, N, precision == CC_PREC_MIXED);
 	const double save_off = h->rho_offset;
 	h->rho_offset = 0.0;   // S(k) of the particles themselves (StructureFactor has no fixed-particle offset)
 	int rc = run_rho(h, h->sk, N, h->d_frac, h->d_E + 1, true, precision == CC_PREC_MIXED, l, h->stream);
@@ -786,11 +1109,31 @@ int cc_objective(cc_handle *h, int64_t N, const double *x, double rescale, doubl
 		CC_CUDA(cudaMemcpyAsync(h->h_pin + 2, h->d_gfrac, sizeof(double) * N * d, cudaMemcpyDeviceToHost,
 		                        h->stream));
 	CC_CUDA(cudaStreamSynchronize(h->stream));
+	if (int rc = check_barrier(h))
+		return rc;
 	*f = h->h_pin[0];
 	if (grad)
 		for (int64_t i = 0; i < N * d; i++)
 			grad[i] = h->h_pin[2 + i] / rescale;
 	return CC_OK;
+}
+
+int cc_set_path(cc_handle *h, int path)
+{
+	if (int rc = check_handle(h))
+		return rc;
+	if (path != CC_PATH_SPLIT && path != CC_PATH_FUSED)
+		return fail(CC_ERR_ARG, "path must be CC_PATH_SPLIT or CC_PATH_FUSED");
+	h->use_fused = path == CC_PATH_FUSED;
+	return CC_OK;
+}
+
+int cc_check_device_error(cc_handle *h)
+{
+	if (int rc = check_handle(h))
+		return rc;
+	CC_CUDA(cudaDeviceSynchronize());
+	return check_barrier(h);
 }
 
 int cc_set_timing(cc_handle *h, int on)
@@ -802,25 +1145,29 @@ int cc_set_timing(cc_handle *h, int on)
 	return CC_OK;
 }
 
-int cc_get_timing(cc_handle *h, double *rho_ms, double *force_ms, int64_t *evals)
+int cc_get_timing(cc_handle *h, double *rho_ms, double *reduce_ms, double *force_ms, int64_t *evals)
 {
 	if (int rc = check_handle(h))
 		return rc;
 	CC_CUDA(cudaDeviceSynchronize());
-	double r = 0, f = 0;
-	for (size_t i = 0; i + 3 <= h->ev_used; i += 3) {
-		float a = 0, b = 0;
+	double r = 0, q = 0, f = 0;
+	for (size_t i = 0; i + 4 <= h->ev_used; i += 4) {
+		float a = 0, b = 0, c = 0;
 		CC_CUDA(cudaEventElapsedTime(&a, h->ev[i], h->ev[i + 1]));
 		CC_CUDA(cudaEventElapsedTime(&b, h->ev[i + 1], h->ev[i + 2]));
+		CC_CUDA(cudaEventElapsedTime(&c, h->ev[i + 2], h->ev[i + 3]));
 		r += a;
-		f += b;
+		q += b;
+		f += c;
 	}
 	if (rho_ms)
 		*rho_ms = r;
+	if (reduce_ms)
+		*reduce_ms = q;
 	if (force_ms)
 		*force_ms = f;
 	if (evals)
-		*evals = (int64_t)(h->ev_used / 3);
+		*evals = (int64_t)(h->ev_used / 4);
 	h->ev_used = 0;
 	return CC_OK;
 }
@@ -829,15 +1176,15 @@ int cc_plan_info(const cc_handle *h, int64_t N, int *L, int64_t *nseg, int *nspl
 {
 	if (int rc = check_handle(h))
 		return rc;
-	const Launch l = choose_launch(h->main.plan, N);
+	const Launch l = choose_launch(h->main.plan, N, false);
 	if (L)
 		*L = h->main.plan.L;
 	if (nseg)
-		*nseg = (int64_t)h->main.plan.segs.size();
+		*nseg = h->main.plan.real_segs;
 	if (nsplit)
 		*nsplit = l.nsplit;
 	if (nksplit)
-		*nksplit = l.nksplit;
+		*nksplit = (int)cc::force_splits(h->main.plan, l.want_force).count();
 	return CC_OK;
 }
 

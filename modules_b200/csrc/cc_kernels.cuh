@@ -1,41 +1,51 @@
 // cc_kernels.cuh — sm_100a kernels of the collective-coordinate (CC) potential.
 //
-// Work decomposition. The constraint modes n (integer k-lattice indices) are grouped on the host into SEGMENTS: up
-// to L modes that share every index but the last and whose last index runs start, start+1, ..., start+len-1 (a piece
-// of a lattice line). For one particle with fractional coordinates s, the phases of a segment are
-//     z_r = exp(2 pi i n_r.s) = z_0 * w^r,   z_0 = exp(2 pi i (prefix.s' + start s_last)),  w = exp(2 pi i s_last),
-// so one seed (an exactly reduced sincospi) gives L phases through complex multiplications, which are FMA work.
-// A segment owns L consecutive SLOTS; slot values are the per-segment rho partials, and every input mode maps to
-// one slot (repeated modes share it). Empty slots (r >= len, padding segments) carry weight 0.
+// Work decomposition. The constraint modes n (integer k-lattice indices) are grouped on the host into SEGMENTS of
+// L = 8 modes that share every index but the last and whose last index runs start, start+1, ... (a piece of a lattice
+// line). For a particle with fractional coordinates s the phases of a segment are
+//     z_r = exp(2 pi i n_r.s) = z_0 w^r,   w = exp(2 pi i s_last),
+// so after one seed z_0 every further phase is one complex multiplication (FMA work). Seeds come from per-particle
+// PHASE TABLES built in shared memory for the block's particles: T_e(m) = exp(2 pi i m s_e) over the index range the
+// block's segments use, either in full or as coarse (stride 8) x fine (0..7) factors; each 8-entry block of a table
+// starts from an exactly reduced FP64 sincospi and continues by at most 7 FP64 complex multiplications, so table
+// entries are accurate to a few ulp whatever the index. A seed is then 2-3 complex products of table entries.
 //
-// rho pass (cc_rho_kernel): one lane per segment, a block = 32 segments (its GROUP) x WARPS warps that stride over
-// the block's particle range; particles are staged in shared memory and read as warp-wide broadcasts. The warps'
-// accumulators are summed in a fixed order, written as the block's partial, and the last block of each group (an
-// atomic ticket, no waiting) sums the partials of all particle splits in split order. The last group overall forms
-// the energy sum over modes in mode order. Every sum has a fixed order, so results repeat bitwise.
+// Exact argument reduction: n.s mod 1 is formed from the rounded product and its exact FMA residual, with the integer
+// part removed by rint, so the phase carries ~1e-16 of a turn of error for any |n| (the reference forms k.r in
+// Cartesian coordinates, whose rounding grows with |k.r|).
 //
-// force pass (cc_force_kernel): one lane per particle, a block = 32 particles x WARPS warps that stride over the
-// block's segment range; segment descriptors and weights u = V conj(rho) are staged in shared memory and read as
-// broadcasts. Per segment the lane accumulates S0 = sum_r t_r and S1 = sum_r r t_r with t_r = Im(u_r z_r); the
-// integer-index gradient is g += S0 * (prefix, start) + (0.., S1). Cartesian force F = (2/V) sum_e g_e b_e; the
-// gradient in fractional coordinates is dPhi/ds_e = -(2/V) 2 pi g_e.
+// Per evaluation (FP64 or mixed):
+//   cc_rho_kernel    grid (rho groups x particle splits), 512 threads = one segment per thread; all warps of a block
+//                    walk the block's particles (tables staged per chunk of 32 particles, read as broadcasts).
+//                    Writes per-split partial sums of every slot.
+//   cc_reduce_kernel sums the splits of every slot in split order (8 chunks in parallel, combined in chunk order),
+//                    forms rho, u = V conj(rho) and the energy (block partials summed in block order by the last
+//                    block, which takes an atomic ticket and never waits).
+//   cc_force_kernel  grid (particle groups of 32 x segment splits), 512 threads = 32 particles (lanes) x 16 warps
+//                    striding over the split's segments unit by unit (a unit = up to 64 segments with its own tables).
+//                    Per segment: S0 = sum_r t_r, S1 = sum_r r t_r with t_r = Im(u_r z_r); the integer-index gradient
+//                    is g += S0 (prefix, start) + (0, S1). Splits are summed in split order by the last block of each
+//                    particle group. Cartesian F = (2/V) sum_e g_e b_e; dPhi/ds_e = -(2/V) 2 pi g_e.
+// Every sum has a fixed order, so results repeat bitwise.
 //
-// Precision. FP64 path: phases from an exact argument reduction of n.s modulo 1 (two-product with FMA, integer parts
-// removed by rint), FP64 sincospi seeds, FP64 recurrences and sums. Mixed path: the same FP64 reduction, then FP32
-// sincospi seeds and FP32 recurrences; per-lane FP32 sums are flushed into FP64 accumulators every SUB particles
-// (rho) or every segment (force), and all cross-lane sums are FP64.
+// Mixed precision: tables are built in FP64 and rounded to FP32; seeds, recurrences and per-segment sums run in
+// FP32; per-thread rho sums are flushed to FP64 every 16 particles, per-segment force sums are added to FP64; all
+// cross-thread sums are FP64.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <cooperative_groups.h>
 #include <type_traits>
 
 #include "cc_plan.h"
 
 namespace cc {
 
+namespace cg = cooperative_groups;
 
 // ---------------------------------------------------------------------------------------------------------------
-// exact fractional phase: t = (sum_e n_e s_e) mod 1, in [-1/2, 1/2]
+// exact fractional phase
 // ---------------------------------------------------------------------------------------------------------------
 __device__ __forceinline__ void acc_phase(int n, double s, double &hi, double &lo)
 {
@@ -45,6 +55,7 @@ __device__ __forceinline__ void acc_phase(int n, double s, double &hi, double &l
 	hi = __dadd_rn(hi, __dsub_rn(p, rint(p)));        // exact: fractional part of the rounded product
 }
 
+// (n . s) mod 1 in [-1/2, 1/2] for a segment's first mode
 template <int D>
 __device__ __forceinline__ double seg_phase(const Seg &g, const double *s)
 {
@@ -58,178 +69,272 @@ __device__ __forceinline__ double seg_phase(const Seg &g, const double *s)
 	return __dsub_rn(t, rint(t));
 }
 
+// (m s) mod 1 in [-1/2, 1/2]
+__device__ __forceinline__ double phase1(int m, double s)
+{
+	double hi = 0.0, lo = 0.0;
+	acc_phase(m, s, hi, lo);
+	const double t = __dadd_rn(hi, lo);
+	return __dsub_rn(t, rint(t));
+}
+
 __device__ __forceinline__ double2 cmul(double2 a, double2 b)
 {
 	return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
 }
-__device__ __forceinline__ float2 cmulf(float2 a, float2 b)
+__device__ __forceinline__ float2 cmul(float2 a, float2 b)
 {
 	return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
 
-// exp(2 pi i t) for t in [-1/2, 1/2] (or [0,1)): (cos, sin)
+// exp(2 pi i t): (cos, sin)
 __device__ __forceinline__ double2 expi2pi(double t)
 {
 	double s, c;
 	sincospi(2.0 * t, &s, &c);
 	return make_double2(c, s);
 }
-__device__ __forceinline__ float2 expi2pif(double t)
+
+template <typename C> __device__ __forceinline__ C to_c(double2 z);
+template <> __device__ __forceinline__ double2 to_c<double2>(double2 z) { return z; }
+template <> __device__ __forceinline__ float2 to_c<float2>(double2 z) { return make_float2((float)z.x, (float)z.y); }
+
+// ---------------------------------------------------------------------------------------------------------------
+// phase tables
+// ---------------------------------------------------------------------------------------------------------------
+// Build the tables of `cnt` particles (fractional coordinates frac[(first + i) * D + axis], i < nvalid; rows of the
+// remaining particles get the tables of s = 0) into tab. Entry k of particle i lives at tab[i * pstride + k * estride].
+// One work item = up to 8 consecutive entries of one run.
+template <int D, typename C>
+__device__ __forceinline__ void build_tables(const TabSpec &sp, const double *__restrict__ frac, int64_t first,
+                                             int cnt, int nvalid, C *tab, int pstride, int estride, int tid,
+                                             int nthreads)
 {
-	float s, c;
-	sincospif(2.0f * (float)t, &s, &c);
-	return make_float2(c, s);
+	const int total = cnt * sp.items;
+	for (int t = tid; t < total; t += nthreads) {
+		const int i = t / sp.items;
+		int k = t - i * sp.items;
+		int r = 0;
+		int nb = (sp.run[0].count + 7) >> 3;
+		while (k >= nb) {
+			k -= nb;
+			r++;
+			nb = (sp.run[r].count + 7) >> 3;
+		}
+		const TabRun &run = sp.run[r];
+		const double s = (i < nvalid) ? frac[(first + i) * D + run.axis] : 0.0;
+		const int k0 = k * 8;
+		double2 z = expi2pi(phase1(run.m0 + run.stride * k0, s));
+		const double2 step = expi2pi(phase1(run.stride, s));
+		const int k1 = min(run.count, k0 + 8);
+		C *dst = tab + (size_t)i * pstride;
+		for (int kk = k0; kk < k1; kk++) {
+			dst[(run.off + kk) * estride] = to_c<C>(z);
+			z = cmul(z, step);
+		}
+	}
 }
 
-template <typename T> struct Cx;
-template <> struct Cx<double> {
-	typedef double2 type;
-	static __device__ __forceinline__ double2 expi(double t) { return expi2pi(t); }
-	static __device__ __forceinline__ double2 mul(double2 a, double2 b) { return cmul(a, b); }
-	static __device__ __forceinline__ double2 zero() { return make_double2(0.0, 0.0); }
-};
-template <> struct Cx<float> {
-	typedef float2 type;
-	static __device__ __forceinline__ float2 expi(double t) { return expi2pif(t); }
-	static __device__ __forceinline__ float2 mul(float2 a, float2 b) { return cmulf(a, b); }
-	static __device__ __forceinline__ float2 zero() { return make_float2(0.0f, 0.0f); }
+// Table indices of a segment's seed: z_0 = prod_e T_e(index_e).
+struct SeedIdx {
+	int a[3], b[3];   // axis e: entry a[e] (full) or a[e] * b[e] (coarse x fine, b[e] >= 0)
+	int w;            // entry of the recurrence step exp(2 pi i s_last)
 };
 
-// ---------------------------------------------------------------------------------------------------------------
-// parameters
-// ---------------------------------------------------------------------------------------------------------------
-struct RhoArgs {
-	const double *frac;       // N x D fractional coordinates in [0,1)
-	int N;
-	int per_split;            // particles per block (blockIdx.y)
-	int nsplit;
-	const Seg *segs;          // ngroups*32 segments
-	int ngroups;
-	int nslot;                // ngroups*32*L
-	double2 *partial;         // [nsplit][nslot]
-	unsigned *counters;       // [ngroups + 1], zero between launches
-	double2 *rho_slot;        // [nslot]
-	const double *slotV;      // [nslot] summed weight of the modes in the slot
-	double2 *u_slot;          // [nslot] u = slotV * conj(rho)
-	const int *mode_slot;     // [M]
-	const double *modeV;      // [M]
-	int M;
-	double rho_offset;        // added to Re rho of every slot
-	double inv_vol, shift;
-	double *E_out;            // energy (device scalar)
-	double2 *rho_mode;        // [M] rho in mode order, or nullptr
-};
+template <int D>
+__device__ __forceinline__ SeedIdx seed_index(const TabSpec &sp, const Seg &g)
+{
+	SeedIdx x;
+	int v[3] = {g.p0, g.p1, 0};
+	v[D - 1] = g.start;
+#pragma unroll
+	for (int e = 0; e < D; e++) {
+		const int m = v[e] - sp.lo[e];
+		if (sp.full[e]) {
+			x.a[e] = sp.offc[e] + m;
+			x.b[e] = -1;
+		} else {
+			x.a[e] = sp.offc[e] + (m >> 3);
+			x.b[e] = sp.offf[e] + (m & 7);
+		}
+	}
+	x.w = sp.offf[D - 1] + 1;
+	return x;
+}
 
-struct ForceArgs {
-	const double *frac;       // N x D
-	int N;
-	const Seg *segs;
-	int nseg;                 // ngroups*32
-	int segs_per_split;
-	int nksplit;
-	const double2 *u_slot;    // [nseg*L]
-	double *partialG;         // [nksplit][N][D], only for nksplit > 1
-	unsigned *counters;       // [ceil(N/32)], zero between launches
-	double recip[9];          // reciprocal basis, row e = b_e (Cartesian)
-	double fscale;            // 2 / Volume
-	double *F_out;            // N x D Cartesian forces, or nullptr
-	double *gfrac_out;        // N x D dPhi/ds, or nullptr
-};
+template <int D, typename C>
+__device__ __forceinline__ C seed_from(const C *row, int estride, const SeedIdx &x)
+{
+	C z = row[x.a[D - 1] * estride];
+	if (x.b[D - 1] >= 0)
+		z = cmul(z, row[x.b[D - 1] * estride]);
+#pragma unroll
+	for (int e = 0; e < D - 1; e++) {
+		C t = row[x.a[e] * estride];
+		if (x.b[e] >= 0)
+			t = cmul(t, row[x.b[e] * estride]);
+		z = cmul(z, t);
+	}
+	return z;
+}
+
+// The same from tables in global memory written earlier in the same launch: loads go to L2 (ld.global.cg), never
+// to a possibly stale L1 line.
+template <int D, typename C>
+__device__ __forceinline__ C seed_from_l2(const C *row, size_t estride, const SeedIdx &x)
+{
+	C z = __ldcg(row + x.a[D - 1] * estride);
+	if (x.b[D - 1] >= 0)
+		z = cmul(z, __ldcg(row + x.b[D - 1] * estride));
+#pragma unroll
+	for (int e = 0; e < D - 1; e++) {
+		C t = __ldcg(row + x.a[e] * estride);
+		if (x.b[e] >= 0)
+			t = cmul(t, __ldcg(row + x.b[e] * estride));
+		z = cmul(z, t);
+	}
+	return z;
+}
+
+// Cartesian force F = fscale * sum_e g_e b_e and fractional gradient -fscale * 2 pi * g of particle j.
+template <int D>
+__device__ __forceinline__ void write_force_out(double *F_out, double *gfrac_out, const double *recip, double fscale,
+                                                int j, const double *g)
+{
+	if (F_out) {
+#pragma unroll
+		for (int c = 0; c < D; c++) {
+			double f = 0.0;
+#pragma unroll
+			for (int e = 0; e < D; e++)
+				f = fma(g[e], recip[e * D + c], f);
+			F_out[(size_t)j * D + c] = fscale * f;
+		}
+	}
+	if (gfrac_out) {
+		const double gs = -fscale * 6.283185307179586476925286766559;
+#pragma unroll
+		for (int e = 0; e < D; e++)
+			gfrac_out[(size_t)j * D + e] = gs * g[e];
+	}
+}
 
 // ---------------------------------------------------------------------------------------------------------------
 // rho pass
 // ---------------------------------------------------------------------------------------------------------------
-// dynamic shared memory layout of cc_rho_kernel (16-byte aligned pieces)
-template <int D, int L, int WARPS, int CHUNK, bool MIXED>
-struct RhoSmem {
-	static constexpr size_t al(size_t x) { return (x + 15) & ~size_t(15); }
-	static constexpr size_t off_s = 0;
-	static constexpr size_t off_w = al(sizeof(double) * CHUNK * D);
-	static constexpr size_t off_red = al(off_w + (MIXED ? sizeof(float2) : sizeof(double2)) * CHUNK);
-	static constexpr size_t bytes = al(off_red + sizeof(double2) * WARPS * 32 * L);
+struct RhoArgs {
+	const double *frac;       // N x D fractional coordinates
+	int N;
+	int per_split;            // particles per block (blockIdx.y)
+	int chunk;                // particles whose tables are staged at once
+	const Seg *segs;          // ngroups * 32 (padding segments have len 0)
+	const int *bstart;        // nbgroups + 1: rho groups (warps) of each block group
+	const TabSpec *bspec;     // nbgroups
+	int nseg, nslot;          // nseg = ngroups * 32, nslot = nseg * L
+	double2 *partial;         // [nsplit / cluster][nslot]
 };
 
-// per-particle recurrence step w = exp(2 pi i s_last): computed in FP64 and rounded for the mixed path
-template <typename R> __device__ __forceinline__ typename Cx<R>::type step_w(double s);
-template <> __device__ __forceinline__ double2 step_w<double>(double s) { return expi2pi(s); }
-template <> __device__ __forceinline__ float2 step_w<float>(double s)
-{
-	const double2 w = expi2pi(s);
-	return make_float2((float)w.x, (float)w.y);
-}
+constexpr int kRhoWarps = 8;
+constexpr int kRhoThreads = kRhoWarps * 32;
 
-template <int D, int L, int WARPS, int CHUNK, bool MIXED>
-__global__ void __launch_bounds__(WARPS * 32) cc_rho_kernel(RhoArgs a)
+// Grid (nbgroups, nsplit), clusters of `csize` blocks along y (the particle splits of one block group). Warp w of a
+// block owns the 32 segments of rho group bstart[g] + w (one per lane) and walks every particle of the block's split;
+// the tables of a chunk of particles are built once for the block group's spec and shared by all warps. The cluster's
+// blocks are added in rank order through distributed shared memory into one partial row.
+template <int D, int L, bool MIXED>
+__global__ void __launch_bounds__(kRhoThreads, 3) cc_rho_kernel(RhoArgs a)
 {
-	typedef typename std::conditional<MIXED, float, double>::type R;
-	typedef typename Cx<R>::type C;
-	constexpr int SUB = 32;   // mixed: FP32 partial sums are flushed to FP64 after this many particles per lane
-
+	typedef typename std::conditional<MIXED, float2, double2>::type C;
+	constexpr int SUB = 16;
 	extern __shared__ __align__(16) unsigned char smem[];
-	typedef RhoSmem<D, L, WARPS, CHUNK, MIXED> Lay;
-	double *sh_s = reinterpret_cast<double *>(smem + Lay::off_s);     // CHUNK*D
-	C *sh_w = reinterpret_cast<C *>(smem + Lay::off_w);               // CHUNK
-	double2 *sh_red = reinterpret_cast<double2 *>(smem + Lay::off_red); // WARPS*32*L
-	__shared__ int sh_last;
+	C *tab = reinterpret_cast<C *>(smem);             // chunk x row (particle-major)
+	double2 *red = reinterpret_cast<double2 *>(smem); // after the loop: kRhoWarps x L x 32
+	__shared__ TabSpec sp;
 
+	cg::cluster_group cluster = cg::this_cluster();
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	const int group = blockIdx.x, split = blockIdx.y;
-	const Seg sg = a.segs[group * 32 + lane];
-	const int j0 = split * a.per_split;
+	const int bg = blockIdx.x, split = blockIdx.y;
+	if (threadIdx.x == 0)
+		sp = a.bspec[bg];
+	const int g0 = a.bstart[bg], nwg = a.bstart[bg + 1] - g0;
+	const bool active = warp < nwg;
+	const int q = (g0 + (active ? warp : 0)) * 32 + lane;
+	const Seg sg = a.segs[q];
+	const int j0 = min(a.N, split * a.per_split);
 	const int j1 = min(a.N, j0 + a.per_split);
-
-	double2 acc[L];
+	cudaGridDependencySynchronize();   // inputs of this step are complete (programmatic dependent launch)
+	__syncthreads();
+	const int row = sp.row | 1;        // odd row stride: consecutive particles' rows start in different banks
+	SeedIdx ix = seed_index<D>(sp, sg);
+	if (sg.len == 0 || !active) {
+		// padding lanes read entry 0 of every table (always present)
 #pragma unroll
-	for (int r = 0; r < L; r++)
-		acc[r] = make_double2(0.0, 0.0);
-	C accf[L];
-	int since_flush = 0;
-	if (MIXED) {
-#pragma unroll
-		for (int r = 0; r < L; r++)
-			accf[r] = Cx<R>::zero();
+		for (int e = 0; e < 3; e++) {
+			ix.a[e] = 0;
+			ix.b[e] = -1;
+		}
 	}
 
-	for (int cj = j0; cj < j1; cj += CHUNK) {
-		const int cnt = min(CHUNK, j1 - cj);
-		__syncthreads();
-		for (int i = threadIdx.x; i < cnt; i += WARPS * 32) {
+	double2 acc[L];
+	C accf[L];
 #pragma unroll
-			for (int e = 0; e < D; e++)
-				sh_s[i * D + e] = a.frac[(size_t)(cj + i) * D + e];
-			sh_w[i] = step_w<R>(a.frac[(size_t)(cj + i) * D + D - 1]);
+	for (int r = 0; r < L; r++) {
+		acc[r] = make_double2(0.0, 0.0);
+		accf[r].x = 0;
+		accf[r].y = 0;
+	}
+	int since_flush = 0;
+
+	for (int cj = j0; cj < j1; cj += a.chunk) {
+		const int cnt = min(a.chunk, j1 - cj);
+		if (cj != j0)
+			__syncthreads();
+		build_tables<D, C>(sp, a.frac, cj, cnt, cnt, tab, row, 1, threadIdx.x, kRhoThreads);
+		__syncthreads();
+		if (!active)
+			continue;
+		int i = 0;
+		for (; i + 1 < cnt; i += 2) {
+			const C *r0 = tab + i * row, *r1 = r0 + row;
+			C z0 = seed_from<D, C>(r0, 1, ix), z1 = seed_from<D, C>(r1, 1, ix);
+			const C w0 = r0[ix.w], w1 = r1[ix.w];
+#pragma unroll
+			for (int r = 0; r < L; r++) {
+				if (MIXED) {
+					accf[r].x += z0.x + z1.x;
+					accf[r].y += z0.y + z1.y;
+				} else {
+					acc[r].x += (double)z0.x + (double)z1.x;
+					acc[r].y += (double)z0.y + (double)z1.y;
+				}
+				z0 = cmul(z0, w0);
+				z1 = cmul(z1, w1);
+			}
+			if (MIXED && (since_flush += 2) >= SUB) {
+				since_flush = 0;
+#pragma unroll
+				for (int r = 0; r < L; r++) {
+					acc[r].x += (double)accf[r].x;
+					acc[r].y += (double)accf[r].y;
+					accf[r].x = 0;
+					accf[r].y = 0;
+				}
+			}
 		}
-		__syncthreads();
-		for (int i = warp; i < cnt; i += WARPS) {
-			double s[D];
+		if (i < cnt) {
+			const C *r0 = tab + i * row;
+			C z0 = seed_from<D, C>(r0, 1, ix);
+			const C w0 = r0[ix.w];
 #pragma unroll
-			for (int e = 0; e < D; e++)
-				s[e] = sh_s[i * D + e];
-			const C w = sh_w[i];
-			C z = Cx<R>::expi(seg_phase<D>(sg, s));
-			if (MIXED) {
-#pragma unroll
-				for (int r = 0; r < L; r++) {
-					accf[r].x += z.x;
-					accf[r].y += z.y;
-					z = Cx<R>::mul(z, w);
+			for (int r = 0; r < L; r++) {
+				if (MIXED) {
+					accf[r].x += z0.x;
+					accf[r].y += z0.y;
+				} else {
+					acc[r].x += (double)z0.x;
+					acc[r].y += (double)z0.y;
 				}
-				if (++since_flush == SUB) {
-					since_flush = 0;
-#pragma unroll
-					for (int r = 0; r < L; r++) {
-						acc[r].x += (double)accf[r].x;
-						acc[r].y += (double)accf[r].y;
-						accf[r] = Cx<R>::zero();
-					}
-				}
-			} else {
-#pragma unroll
-				for (int r = 0; r < L; r++) {
-					acc[r].x += (double)z.x;
-					acc[r].y += (double)z.y;
-					z = Cx<R>::mul(z, w);
-				}
+				z0 = cmul(z0, w0);
 			}
 		}
 	}
@@ -240,166 +345,244 @@ __global__ void __launch_bounds__(WARPS * 32) cc_rho_kernel(RhoArgs a)
 			acc[r].y += (double)accf[r].y;
 		}
 	}
+	cudaTriggerProgrammaticLaunchCompletion();   // the next kernel may be scheduled; it waits for this grid
 
-	// fixed-order sum over the block's warps
+	// this block's sums, layout [warp][r][lane], then the cluster's blocks in rank order
 	__syncthreads();
+	if (active) {
 #pragma unroll
-	for (int r = 0; r < L; r++)
-		sh_red[(warp * 32 + lane) * L + r] = acc[r];
-	__syncthreads();
-	const size_t gbase = (size_t)group * 32 * L;
-	for (int q = threadIdx.x; q < 32 * L; q += WARPS * 32) {
-		double2 t = sh_red[q];
-		for (int w = 1; w < WARPS; w++) {
-			const double2 v = sh_red[w * 32 * L + q];
+		for (int r = 0; r < L; r++)
+			red[(warp * L + r) * 32 + lane] = acc[r];
+	}
+	cluster.sync();
+	const int cs = (int)cluster.num_blocks();
+	const int rank = (int)cluster.block_rank();
+	const int total = nwg * L * 32;
+	const int per = (total + cs - 1) / cs;
+	const size_t out_row = (size_t)(split / cs) * a.nslot;
+	for (int e = rank * per + threadIdx.x; e < min(total, (rank + 1) * per); e += kRhoThreads) {
+		const int w = e / (L * 32), r = (e / 32) % L, ln = e & 31;
+		double2 t = make_double2(0.0, 0.0);
+		for (int k = 0; k < cs; k++) {
+			const double2 *rs = cluster.map_shared_rank(red, k);
+			const double2 v = rs[e];
 			t.x += v.x;
 			t.y += v.y;
 		}
-		a.partial[(size_t)split * a.nslot + gbase + q] = t;
+		a.partial[out_row + (size_t)r * a.nseg + (g0 + w) * 32 + ln] = t;
 	}
+	cluster.sync();
+}
 
-	// the last block of this group sums the partials of every split, in split order
-	__threadfence();
-	__syncthreads();
-	if (threadIdx.x == 0)
-		sh_last = (atomicAdd(&a.counters[group], 1u) == (unsigned)(a.nsplit - 1));
-	__syncthreads();
-	if (!sh_last)
-		return;
-	__threadfence();
-	for (int q = threadIdx.x; q < 32 * L; q += WARPS * 32) {
-		double2 t = __ldcg(&a.partial[gbase + q]);
-		for (int sp = 1; sp < a.nsplit; sp++) {
-			const double2 v = __ldcg(&a.partial[(size_t)sp * a.nslot + gbase + q]);
+// ---------------------------------------------------------------------------------------------------------------
+// split reduction, u = V conj(rho), energy
+// ---------------------------------------------------------------------------------------------------------------
+struct ReduceArgs {
+	const double2 *partial;   // [nsplit][nslot]
+	int nsplit, nslot;
+	const double *slotV;
+	double rho_offset;        // added to Re rho of every slot
+	double2 *rho_slot, *u_slot;
+	double *eblock;           // [gridDim.x]
+	unsigned *ticket;         // 1, zero between launches
+	double inv_vol, shift;
+	double *E_out;
+};
+
+constexpr int kRedThreads = 256;   // 32 slots x 8 split chunks
+
+static __global__ void __launch_bounds__(kRedThreads) cc_reduce_kernel(ReduceArgs a)
+{
+	__shared__ double2 sh[8][32];
+	__shared__ int sh_last;
+	const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
+	const int slot = blockIdx.x * 32 + lane;
+	const int per = (a.nsplit + 7) >> 3;
+	cudaGridDependencySynchronize();
+	cudaTriggerProgrammaticLaunchCompletion();
+	const int s0 = min(a.nsplit, c * per), s1 = min(a.nsplit, s0 + per);
+	double2 t = make_double2(0.0, 0.0);
+	if (slot < a.nslot) {
+		int sp = s0;
+		for (; sp + 4 <= s1; sp += 4) {
+			const double2 v0 = __ldcg(&a.partial[(size_t)sp * a.nslot + slot]);
+			const double2 v1 = __ldcg(&a.partial[(size_t)(sp + 1) * a.nslot + slot]);
+			const double2 v2 = __ldcg(&a.partial[(size_t)(sp + 2) * a.nslot + slot]);
+			const double2 v3 = __ldcg(&a.partial[(size_t)(sp + 3) * a.nslot + slot]);
+			t.x += v0.x;
+			t.y += v0.y;
+			t.x += v1.x;
+			t.y += v1.y;
+			t.x += v2.x;
+			t.y += v2.y;
+			t.x += v3.x;
+			t.y += v3.y;
+		}
+		for (; sp < s1; sp++) {
+			const double2 v = __ldcg(&a.partial[(size_t)sp * a.nslot + slot]);
 			t.x += v.x;
 			t.y += v.y;
 		}
-		t.x += a.rho_offset;
-		a.rho_slot[gbase + q] = t;
-		const double v = a.slotV[gbase + q];
-		a.u_slot[gbase + q] = make_double2(v * t.x, -v * t.y);
 	}
-	if (threadIdx.x == 0)
-		a.counters[group] = 0u;
-
-	// the last group overall forms the energy in mode order
+	sh[c][lane] = t;
+	__syncthreads();
+	if (c == 0) {
+		double2 rho = sh[0][lane];
+#pragma unroll
+		for (int k = 1; k < 8; k++) {
+			rho.x += sh[k][lane].x;
+			rho.y += sh[k][lane].y;
+		}
+		double e = 0.0;
+		if (slot < a.nslot) {
+			rho.x += a.rho_offset;
+			a.rho_slot[slot] = rho;
+			const double v = a.slotV[slot];
+			a.u_slot[slot] = make_double2(v * rho.x, -v * rho.y);
+			e = v * (rho.x * rho.x + rho.y * rho.y);
+		}
+#pragma unroll
+		for (int o = 16; o > 0; o >>= 1)
+			e += __shfl_down_sync(0xffffffffu, e, o);
+		if (lane == 0)
+			a.eblock[blockIdx.x] = e;
+	}
 	__threadfence();
 	__syncthreads();
 	if (threadIdx.x == 0)
-		sh_last = (atomicAdd(&a.counters[a.ngroups], 1u) == (unsigned)(a.ngroups - 1));
+		sh_last = (atomicAdd(a.ticket, 1u) == gridDim.x - 1);
 	__syncthreads();
-	if (!sh_last)
+	if (!sh_last || c != 0)
 		return;
 	__threadfence();
 	double e = 0.0;
-	for (int m = threadIdx.x; m < a.M; m += WARPS * 32) {
-		const double2 rho = __ldcg(&a.rho_slot[a.mode_slot[m]]);
-		e += a.modeV[m] * (rho.x * rho.x + rho.y * rho.y);
-		if (a.rho_mode)
-			a.rho_mode[m] = rho;
-	}
-	__syncthreads();
-	double *sh_e = reinterpret_cast<double *>(sh_red);
-	sh_e[threadIdx.x] = e;
-	__syncthreads();
-	for (int stride = WARPS * 16; stride > 0; stride >>= 1) {
-		if (threadIdx.x < stride)
-			sh_e[threadIdx.x] += sh_e[threadIdx.x + stride];
-		__syncthreads();
-	}
-	if (threadIdx.x == 0) {
-		*a.E_out = sh_e[0] * a.inv_vol + a.shift;
-		a.counters[a.ngroups] = 0u;
+	for (int b = lane; b < (int)gridDim.x; b += 32)
+		e += __ldcg(&a.eblock[b]);
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1)
+		e += __shfl_down_sync(0xffffffffu, e, o);
+	if (lane == 0) {
+		*a.E_out = e * a.inv_vol + a.shift;
+		*a.ticket = 0u;
 	}
 }
+
+// rho in input-mode order (repeated modes read their shared slot)
+static __global__ void cc_gather_rho_kernel(const double2 *__restrict__ rho_slot, const int *__restrict__ mode_slot, int M,
+                                     double2 *__restrict__ rho_mode)
+{
+	const int m = blockIdx.x * blockDim.x + threadIdx.x;
+	if (m < M)
+		rho_mode[m] = rho_slot[mode_slot[m]];
+}
+
+// E = shift when there is no constraint
+static __global__ void cc_set_scalar_kernel(double *p, double v) { *p = v; }
 
 // ---------------------------------------------------------------------------------------------------------------
 // force pass
 // ---------------------------------------------------------------------------------------------------------------
+struct ForceArgs {
+	const double *frac;       // N x D
+	int N;
+	const Seg *segs;
+	const int *kstart;        // nksplit + 1: segment range of each split
+	const TabSpec *kspec;     // nksplit
+	int nksplit;
+	const double2 *u_slot;    // [nslot], slot of (segment q, step r) = r * nseg + q
+	int nseg;
+	double *partialG;         // [nksplit][N][D], only for nksplit > 1
+	unsigned *counters;       // [ceil(N/32)], zero between launches
+	double recip[9];          // reciprocal basis, row e = b_e (Cartesian)
+	double fscale;            // 2 / Volume
+	double *F_out;            // N x D Cartesian forces, or nullptr
+	double *gfrac_out;        // N x D dPhi/ds, or nullptr
+};
+
+constexpr int kForceWarps = 8;
+constexpr int kForceThreads = kForceWarps * 32;
+
 template <int D>
 __device__ __forceinline__ void write_force(const ForceArgs &a, int j, const double *g)
 {
-	if (a.F_out) {
-#pragma unroll
-		for (int c = 0; c < D; c++) {
-			double f = 0.0;
-#pragma unroll
-			for (int e = 0; e < D; e++)
-				f = fma(g[e], a.recip[e * D + c], f);
-			a.F_out[(size_t)j * D + c] = a.fscale * f;
-		}
-	}
-	if (a.gfrac_out) {
-		const double gs = -a.fscale * 6.283185307179586476925286766559;
-#pragma unroll
-		for (int e = 0; e < D; e++)
-			a.gfrac_out[(size_t)j * D + e] = gs * g[e];
-	}
+	write_force_out<D>(a.F_out, a.gfrac_out, a.recip, a.fscale, j, g);
 }
 
-template <int D, int L, int WARPS, int SEGCHUNK, bool MIXED>
-__global__ void __launch_bounds__(WARPS * 32) cc_force_kernel(ForceArgs a)
+// Grid (ceil(N/32), nksplit). Block = 32 particles (lanes) x 8 warps striding over the split's segments; the tables of
+// the block's particles for the split are built once (entry-major, so a warp reads 32 consecutive entries).
+template <int D, int L, bool MIXED>
+__global__ void __launch_bounds__(kForceThreads, 2) cc_force_kernel(ForceArgs a)
 {
 	typedef typename std::conditional<MIXED, float, double>::type R;
-	typedef typename Cx<R>::type C;
-	__shared__ Seg sh_seg[SEGCHUNK];
-	__shared__ C sh_u[SEGCHUNK * L];
-	__shared__ double sh_g[WARPS * 32 * D];
+	typedef typename std::conditional<MIXED, float2, double2>::type C;
+	extern __shared__ __align__(16) unsigned char smem[];
+	C *tab = reinterpret_cast<C *>(smem);            // row x 32, entry-major
+	double *sh_g = reinterpret_cast<double *>(smem); // reused after the loop: kForceWarps x 32 x D
+	__shared__ TabSpec sp;
 	__shared__ int sh_last;
 
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	const int j = blockIdx.x * 32 + lane;
+	const int pbase = blockIdx.x * 32;
+	const int j = pbase + lane;
+	const int nvalid = min(32, a.N - pbase);
 	const int ks = blockIdx.y;
-	const int q0 = ks * a.segs_per_split;
-	const int q1 = min(a.nseg, q0 + a.segs_per_split);
-
-	double s[D];
-#pragma unroll
-	for (int e = 0; e < D; e++)
-		s[e] = (j < a.N) ? a.frac[(size_t)j * D + e] : 0.0;
-	const C w = step_w<R>(s[D - 1]);
+	const int q0 = a.kstart[ks], q1 = a.kstart[ks + 1];
+	if (threadIdx.x == 0)
+		sp = a.kspec[ks];
+	cudaGridDependencySynchronize();   // u of this step is complete
+	__syncthreads();
+	build_tables<D, C>(sp, a.frac, pbase, 32, nvalid, tab, 1, 32, threadIdx.x, kForceThreads);
+	__syncthreads();
 
 	double g[D];
 #pragma unroll
 	for (int e = 0; e < D; e++)
 		g[e] = 0.0;
-
-	for (int cq = q0; cq < q1; cq += SEGCHUNK) {
-		const int cnt = min(SEGCHUNK, q1 - cq);
-		__syncthreads();
-		for (int i = threadIdx.x; i < cnt; i += WARPS * 32)
-			sh_seg[i] = a.segs[cq + i];
-		for (int i = threadIdx.x; i < cnt * L; i += WARPS * 32) {
-			const double2 u = a.u_slot[(size_t)cq * L + i];
-			if (MIXED)
-				reinterpret_cast<float2 *>(sh_u)[i] = make_float2((float)u.x, (float)u.y);
-			else
-				reinterpret_cast<double2 *>(sh_u)[i] = u;
-		}
-		__syncthreads();
-		for (int q = warp; q < cnt; q += WARPS) {
-			const Seg sg = sh_seg[q];
-			if (sg.len == 0)
-				continue;
-			C z = Cx<R>::expi(seg_phase<D>(sg, s));
-			R S0 = 0, S1 = 0;
+	// software pipeline: the next segment's descriptor and weights are loaded while this one is computed
+	int q = q0 + warp;
+	Seg nsg = {0, 0, 0, 0};
+	double2 nu[L];
+	if (q < q1) {
+		nsg = a.segs[q];
 #pragma unroll
-			for (int r = 0; r < L; r++) {
-				const C u = sh_u[q * L + r];
-				const R t = u.x * z.y + u.y * z.x;
-				S0 += t;
-				S1 = fma((R)r, t, S1);
-				z = Cx<R>::mul(z, w);
-			}
-			const double S0d = (double)S0;
-			if (D >= 2)
-				g[0] = fma(S0d, (double)sg.p0, g[0]);
-			if (D >= 3)
-				g[1] = fma(S0d, (double)sg.p1, g[1]);
-			g[D - 1] = fma(S0d, (double)sg.start, g[D - 1] + (double)S1);
+		for (int r = 0; r < L; r++)
+			nu[r] = __ldg(a.u_slot + q + (size_t)r * a.nseg);
+	}
+	for (; q < q1; q += kForceWarps) {
+		const Seg sgm = nsg;
+		C uu[L];
+#pragma unroll
+		for (int r = 0; r < L; r++)
+			uu[r] = to_c<C>(nu[r]);
+		const int qn = q + kForceWarps;
+		if (qn < q1) {
+			nsg = a.segs[qn];
+#pragma unroll
+			for (int r = 0; r < L; r++)
+				nu[r] = __ldg(a.u_slot + qn + (size_t)r * a.nseg);
 		}
+		if (sgm.len == 0)   // padding segment of a rho group: weight 0, no table entries
+			continue;
+		const SeedIdx ix = seed_index<D>(sp, sgm);
+		C z = seed_from<D, C>(tab + lane, 32, ix);
+		const C w = tab[ix.w * 32 + lane];
+		R S0 = 0, S1 = 0;
+#pragma unroll
+		for (int r = 0; r < L; r++) {
+			const R t = uu[r].x * z.y + uu[r].y * z.x;
+			S0 += t;
+			S1 = fma((R)r, t, S1);
+			z = cmul(z, w);
+		}
+		const double S0d = (double)S0;
+		if (D >= 2)
+			g[0] = fma(S0d, (double)sgm.p0, g[0]);
+		if (D >= 3)
+			g[1] = fma(S0d, (double)sgm.p1, g[1]);
+		g[D - 1] = fma(S0d, (double)sgm.start, g[D - 1] + (double)S1);
 	}
 
+	cudaTriggerProgrammaticLaunchCompletion();
 	// fixed-order sum over the block's warps
 	__syncthreads();
 #pragma unroll
@@ -412,7 +595,7 @@ __global__ void __launch_bounds__(WARPS * 32) cc_force_kernel(ForceArgs a)
 #pragma unroll
 	for (int e = 0; e < D; e++) {
 		t[e] = sh_g[lane * D + e];
-		for (int w2 = 1; w2 < WARPS; w2++)
+		for (int w2 = 1; w2 < kForceWarps; w2++)
 			t[e] += sh_g[(w2 * 32 + lane) * D + e];
 	}
 	if (a.nksplit == 1) {
@@ -434,15 +617,15 @@ __global__ void __launch_bounds__(WARPS * 32) cc_force_kernel(ForceArgs a)
 		return;
 	__threadfence();
 	if (j < a.N) {
-		double u[D];
+		double v[D];
 #pragma unroll
 		for (int e = 0; e < D; e++)
-			u[e] = __ldcg(&a.partialG[(size_t)j * D + e]);
+			v[e] = __ldcg(&a.partialG[(size_t)j * D + e]);
 		for (int k2 = 1; k2 < a.nksplit; k2++)
 #pragma unroll
 			for (int e = 0; e < D; e++)
-				u[e] += __ldcg(&a.partialG[((size_t)k2 * a.N + j) * D + e]);
-		write_force<D>(a, j, u);
+				v[e] += __ldcg(&a.partialG[((size_t)k2 * a.N + j) * D + e]);
+		write_force<D>(a, j, v);
 	}
 	if (lane == 0)
 		a.counters[blockIdx.x] = 0u;

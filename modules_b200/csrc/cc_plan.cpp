@@ -25,23 +25,55 @@ struct ModeLess {
 	}
 };
 
-int64_t count_segments(int d, const std::vector<std::array<int32_t, 3> > &u, int L)
+// Index ranges of a set of segments, per axis (prefix axes: p0, p1; last axis: segment starts).
+struct Ranges {
+	int lo[3], hi[3];
+	bool empty = true;
+	void add(int d, const Seg &s)
+	{
+		int v[3] = {s.p0, s.p1, 0};
+		v[d - 1] = s.start;
+		for (int e = 0; e < d; e++) {
+			if (empty || v[e] < lo[e])
+				lo[e] = v[e];
+			if (empty || v[e] > hi[e])
+				hi[e] = v[e];
+		}
+		empty = false;
+	}
+};
+
+TabSpec make_spec(int d, const Ranges &r)
 {
-	int64_t nseg = 0;
-	int len = 0;
-	for (size_t i = 0; i < u.size(); i++) {
-		bool cont = i > 0 && len < L && u[i][d - 1] == u[i - 1][d - 1] + 1;
-		for (int e = 0; e + 1 < d && cont; e++)
-			cont = u[i][e] == u[i - 1][e];
-		if (cont) {
-			len++;
+	TabSpec t = {};
+	int off = 0;
+	for (int e = 0; e < d; e++) {
+		const int range = r.hi[e] - r.lo[e] + 1;
+		t.lo[e] = r.lo[e];
+		if (e < d - 1 && range <= kFullMax) {
+			t.full[e] = 1;
+			t.offc[e] = off;
+			t.run[t.nrun++] = TabRun{e, 1, r.lo[e], range, off};
+			off += range;
 		} else {
-			nseg++;
-			len = 1;
+			const int nc = (range + 7) / 8;
+			t.full[e] = 0;
+			t.offc[e] = off;
+			t.run[t.nrun++] = TabRun{e, 8, r.lo[e], nc, off};
+			off += nc;
+			t.offf[e] = off;
+			t.run[t.nrun++] = TabRun{e, 1, 0, 8, off};
+			off += 8;
 		}
 	}
-	return (nseg + 31) / 32 * 32;
+	t.row = off;
+	t.items = 0;
+	for (int i = 0; i < t.nrun; i++)
+		t.items += (t.run[i].count + 7) / 8;
+	return t;
 }
+
+int spec_row(int d, const Ranges &r) { return make_spec(d, r).row; }
 
 }  // namespace
 
@@ -69,11 +101,8 @@ Plan build_plan(int d, int64_t M, const int32_t *modes, const double *V, int L)
 		mode_u[m] = (int64_t)u.size() - 1;
 	}
 	p.unique_modes = (int64_t)u.size();
-	if (L == 0) {
-		// seed (~45 FP64 instructions) + L recurrence steps (~7) per segment and particle
-		const int64_t n8 = count_segments(d, u, 8), n16 = count_segments(d, u, 16);
-		L = (n8 * (45 + 7 * 8) <= n16 * (45 + 7 * 16)) ? 8 : 16;
-	}
+	if (L <= 0)
+		L = 8;
 	p.L = L;
 	std::vector<int64_t> u_slot(u.size());
 	int len = 0;
@@ -95,10 +124,64 @@ Plan build_plan(int d, int64_t M, const int32_t *modes, const double *V, int L)
 		}
 		u_slot[i] = (int64_t)(p.segs.size() - 1) * L + (len - 1);
 	}
-	while (p.segs.size() % 32)
-		p.segs.push_back(Seg{0, 0, 0, 0});
-	p.ngroups = (int)(p.segs.size() / 32);
-	p.nslot = p.ngroups * 32 * L;
+	// rho groups: up to 32 consecutive segments whose tables fit kMaxRow entries, padded to 32
+	std::vector<Seg> raw;
+	raw.swap(p.segs);
+	p.real_segs = (int64_t)raw.size();
+	std::vector<int64_t> where(raw.size());
+	size_t i0 = 0;
+	while (i0 < raw.size()) {
+		Ranges r;
+		size_t j = i0;
+		while (j < raw.size() && (int)(j - i0) < kGroupSegs) {
+			Ranges t = r;
+			t.add(d, raw[j]);
+			if (j > i0 && spec_row(d, t) > kMaxRow)
+				break;
+			r = t;
+			j++;
+		}
+		for (size_t k = i0; k < j; k++) {
+			where[k] = (int64_t)p.segs.size();
+			p.segs.push_back(raw[k]);
+		}
+		while (p.segs.size() % kGroupSegs)
+			p.segs.push_back(Seg{0, 0, 0, 0});
+		p.rspec.push_back(make_spec(d, r));
+		p.rho_max_row = std::max(p.rho_max_row, p.rspec.back().row);
+		i0 = j;
+	}
+	// slot of (segment q, step r) = r * nseg + q: a warp's 32 segments are contiguous for every r
+	const int64_t nseg = (int64_t)p.segs.size();
+	for (size_t i = 0; i < u.size(); i++) {
+		const int64_t seg = u_slot[i] / L, r = u_slot[i] % L;
+		u_slot[i] = r * nseg + where[(size_t)seg];
+	}
+	// block groups: up to kBlockGroups consecutive rho groups whose joint tables fit kMaxRow entries
+	{
+		const int ng = p.ngroups();
+		int g = 0;
+		while (g < ng) {
+			Ranges r;
+			int h = g;
+			while (h < ng && h - g < kBlockGroups) {
+				Ranges t = r;
+				for (int q = h * kGroupSegs; q < (h + 1) * kGroupSegs; q++)
+					if (p.segs[q].len > 0)
+						t.add(d, p.segs[q]);
+				if (h > g && spec_row(d, t) > kMaxRow)
+					break;
+				r = t;
+				h++;
+			}
+			p.bstart.push_back(g);
+			p.bspec.push_back(make_spec(d, r));
+			p.block_max_row = std::max(p.block_max_row, p.bspec.back().row);
+			g = h;
+		}
+		p.bstart.push_back(ng);
+	}
+	p.nslot = (int)p.segs.size() * L;
 	p.slotV.assign((size_t)p.nslot, 0.0);
 	for (size_t i = 0; i < u.size(); i++)
 		p.slotV[(size_t)u_slot[i]] = uV[i];
@@ -107,6 +190,62 @@ Plan build_plan(int d, int64_t M, const int32_t *modes, const double *V, int L)
 	for (int64_t m = 0; m < M; m++)
 		p.mode_slot[(size_t)m] = (int)u_slot[(size_t)mode_u[(size_t)m]];
 	return p;
+}
+
+TabSpec global_spec(const Plan &p)
+{
+	Ranges r;
+	for (const Seg &s : p.segs)
+		if (s.len > 0)
+			r.add(p.d, s);
+	if (r.empty) {
+		Seg z = {0, 0, 0, 1};
+		r.add(p.d, z);
+	}
+	return make_spec(p.d, r);
+}
+
+ForceSplits force_splits(const Plan &p, int want)
+{
+	ForceSplits f;
+	const int nseg = (int)p.segs.size();
+	want = std::max(1, std::min(want, std::max(1, (int)p.real_segs)));
+	const int64_t target = (p.real_segs + want - 1) / want;   // real segments per split
+	int i = 0;
+	while (i < nseg) {
+		Ranges r;
+		int j = i, real = 0;
+		while (j < nseg) {
+			if (p.segs[j].len == 0) {   // padding: no table entries
+				j++;
+				continue;
+			}
+			if (real >= target)
+				break;
+			Ranges t = r;
+			t.add(p.d, p.segs[j]);
+			if (real > 0 && spec_row(p.d, t) > kMaxRow)
+				break;
+			r = t;
+			real++;
+			j++;
+		}
+		if (real == 0)   // trailing padding only: attach to the previous split
+		{
+			if (!f.start.empty()) {
+				i = nseg;
+				break;
+			}
+			Seg z = {0, 0, 0, 1};
+			r.add(p.d, z);
+		}
+		f.start.push_back(i);
+		f.spec.push_back(make_spec(p.d, r));
+		f.max_row = std::max(f.max_row, f.spec.back().row);
+		i = j;
+	}
+	f.start.push_back(nseg);
+	return f;
 }
 
 bool cell_geometry(int d, const double *a, double *volume, double *recip)

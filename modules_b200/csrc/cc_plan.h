@@ -1,32 +1,79 @@
-// cc_plan.h — host-side planning of the CC kernels: lattice-line segments, cell geometry, the stealthy k-set.
+// cc_plan.h — host-side planning of the CC kernels: lattice-line segments, phase-table specs, cell geometry and the
+// stealthy k-set.
 #pragma once
 #include <cstdint>
 #include <vector>
 
 namespace cc {
 
-// A piece of a lattice line of modes (see cc_kernels.cuh): modes (p0, p1, start + r) for r < len, d = 3;
-// (p0, start + r) for d = 2; (start + r) for d = 1.
+// A piece of a lattice line of modes (see cc_kernels.cuh): modes (p0, p1, start + r) for r < len when d = 3;
+// (p0, start + r) when d = 2; (start + r) when d = 1.
 struct alignas(16) Seg {
 	int p0, p1;
 	int start;
 	int len;
 };
 
-struct Plan {
-	int d = 0;
-	int L = 16;                   // slots per segment (8 or 16)
-	int ngroups = 0;              // segments / 32
-	int nslot = 0;                // ngroups * 32 * L
-	std::vector<Seg> segs;        // ngroups * 32, padding segments have len 0
-	std::vector<double> slotV;    // nslot: summed weight of the modes of each slot
-	std::vector<int> mode_slot;   // M: slot of each input mode
-	std::vector<double> modeV;    // M: input weights
-	int64_t unique_modes = 0;
+// One run of a per-particle phase table: entries off .. off+count-1 of a particle's row hold
+// exp(2 pi i (m0 + stride k) s_axis), k = 0 .. count-1.
+struct TabRun {
+	int axis, stride, m0, count, off;
 };
 
-// Group M modes (M x d integers) into segments of at most L slots; L = 0 chooses 8 or 16 by a work estimate.
+// The phase tables a group of segments needs, per particle. Axis e is looked up either in a FULL table (full[e] = 1:
+// T(m) = row[offc[e] + m - lo[e]]) or as COARSE x FINE (full[e] = 0: T(m) = row[offc[e] + (m-lo[e])/8] *
+// row[offf[e] + (m-lo[e])%8]). The last axis is always coarse x fine; its fine entry 1 is the recurrence step.
+struct TabSpec {
+	TabRun run[6];
+	int nrun;
+	int row;        // entries per particle
+	int items;      // sum over runs of ceil(count / 8): table-building work items per particle
+	int lo[3], full[3], offc[3], offf[3];
+};
+
+struct Plan {
+	int d = 0;
+	int L = 8;                        // slots per segment
+	std::vector<Seg> segs;            // ngroups * 32: rho groups of 32 segments, padded with len = 0 segments
+	int nslot = 0;                    // segs.size() * L; slot of (segment q, step r) = r * segs.size() + q
+	std::vector<double> slotV;        // nslot: summed weight of the modes of each slot (0 for empty slots)
+	std::vector<int> mode_slot;       // M: slot of each input mode
+	std::vector<double> modeV;        // M: input weights
+	int64_t unique_modes = 0;
+	int64_t real_segs = 0;            // segments with len > 0
+	std::vector<TabSpec> rspec;       // one table spec per rho group
+	int rho_max_row = 0;
+	int ngroups() const { return (int)rspec.size(); }
+	// block groups of the split rho kernel: warp groups [bstart[b], bstart[b+1]) (at most kBlockGroups) that share
+	// one table spec
+	std::vector<int> bstart;
+	std::vector<TabSpec> bspec;
+	int block_max_row = 0;
+	int nbgroups() const { return (int)bspec.size(); }
+};
+
+// A split of the segments for the force pass: segments [start[k], start[k+1]) share the table spec spec[k].
+struct ForceSplits {
+	std::vector<int> start;
+	std::vector<TabSpec> spec;
+	int max_row = 0;
+	int count() const { return (int)spec.size(); }
+};
+
+constexpr int kGroupSegs = 32;     // segments per rho group (one per lane)
+constexpr int kBlockGroups = 8;    // rho groups (warps) per block of the split rho kernel
+constexpr int kMaxRow = 128;       // table entries per particle and group/split
+constexpr int kFullMax = 48;       // prefix axes with a range up to this many indices get a full table
+
+// Group M modes (M x d integers) into segments of L slots, in rho groups of 32 segments.
 Plan build_plan(int d, int64_t M, const int32_t *modes, const double *V, int L);
+
+// One table spec covering every segment of the plan (full tables for prefix axes up to kFullMax indices, coarse x
+// fine otherwise); its row may exceed kMaxRow.
+TabSpec global_spec(const Plan &p);
+
+// Cut the plan's segments into at least `want` force splits of similar size whose tables fit kMaxRow entries.
+ForceSplits force_splits(const Plan &p, int want);
 
 // |det| of the basis (rows a_i) and the reciprocal basis rows b_e with b_e . a_i = 2 pi delta_ei.
 bool cell_geometry(int d, const double *basis, double *volume, double *recip);
