@@ -97,6 +97,38 @@ int cc_structure_factor(cc_handle *h, int64_t K, const int32_t *modes, double *S
  * *f and, if grad is not NULL, grad[i*d+j] = -F_i . a_j / rescale. */
 int cc_objective(cc_handle *h, int64_t N, const double *x, double rescale, double *f, double *grad, int precision);
 
+/* --- structure optimisation (L-BFGS on the device) --------------------------------------------------------------
+ * Replaces the structure optimiser's L-BFGS loop (RelaxStructure_NLOPT / _inner / _Emin,
+ * potential/StructureOptimization.cpp:881-1090, with NLopt's or LuksanPLIS's L-BFGS, potential/LuksanPLIS.cpp:1668-)
+ * for the Switch-0 objective (particle coordinates only). The variables are the fractional coordinates; positions,
+ * gradient, the m correction pairs and every dot product stay on the device (FP64). The method is L-BFGS in the compact
+ * representation (Byrd, Nocedal & Schnabel 1994) with Armijo backtracking; iterates are not NLopt's bit for bit. */
+enum {
+	CC_PREC_SCHEDULE = 2        /* cc_minimize: mixed precision until E/N <= switch_energy_per_particle, then FP64 */
+};
+typedef struct {
+	int history;                /* correction pairs m (1..64), default 40 as the reference's LBFGSHistory */
+	int64_t max_evals;          /* evaluation limit, default 100000 */
+	double stopval;             /* stop when E <= stopval, default -1e300 (the ground state: 1e-20 * N) */
+	double gtol;                /* stop when max |dE/ds| <= gtol, default 0 */
+	double ftol;                /* stop after 3 accepted steps with E decreasing by <= ftol |E|, default 1e-15 */
+	int precision;              /* CC_PREC_FP64 (default), CC_PREC_MIXED or CC_PREC_SCHEDULE */
+	double switch_energy_per_particle;   /* CC_PREC_SCHEDULE threshold, default 1e-12 */
+	int iters_per_check;        /* iterations per host status check (one CUDA graph replay), default 32 */
+} cc_lbfgs_opts;
+
+typedef struct {
+	double E;                   /* FP64 energy of the returned configuration */
+	int64_t evals, iters;
+	int status;                 /* 1 stop value, 2 gradient, 3 evaluation limit, 4 line search, 5 relative change */
+} cc_lbfgs_result;
+
+int cc_lbfgs_defaults(cc_lbfgs_opts *opts);
+
+/* Minimise the energy from the fractional start frac (N x d, host), which receives the result wrapped into [0,1).
+ * The handle's bound positions become the result. */
+int cc_minimize(cc_handle *h, int64_t N, double *frac, const cc_lbfgs_opts *opts, cc_lbfgs_result *result);
+
 /* Device-resident evaluation: d_frac (N x d, device), outputs d_E (1 double) and d_F (N x d Cartesian, may be
  * NULL) and d_gfrac (N x d gradient of the energy with respect to the fractional coordinates, may be NULL), all on
  * the device, enqueued on `stream` (a cudaStream_t; NULL = the handle's stream). No host synchronisation. */

@@ -35,6 +35,19 @@ _i64 = ctypes.c_int64
 _d = ctypes.c_double
 _i = ctypes.c_int
 
+class LbfgsOpts(ctypes.Structure):
+    _fields_ = [("history", ctypes.c_int), ("max_evals", ctypes.c_int64), ("stopval", ctypes.c_double),
+                ("gtol", ctypes.c_double), ("ftol", ctypes.c_double), ("precision", ctypes.c_int),
+                ("switch_energy_per_particle", ctypes.c_double), ("iters_per_check", ctypes.c_int)]
+
+
+class LbfgsResult(ctypes.Structure):
+    _fields_ = [("E", ctypes.c_double), ("evals", ctypes.c_int64), ("iters", ctypes.c_int64),
+                ("status", ctypes.c_int)]
+
+
+PREC_SCHEDULE = 2
+
 _SIGS = {
     "cc_last_error": (ctypes.c_char_p, []),
     "cc_device_available": (_i, []),
@@ -56,6 +69,8 @@ _SIGS = {
     "cc_plan_info": (_i, [_vp, _i64, ctypes.POINTER(_i), ctypes.POINTER(_i64), ctypes.POINTER(_i),
                           ctypes.POINTER(_i)]),
     "cc_probe_fma_peak": (_i, [_i, ctypes.POINTER(_d)]),
+    "cc_lbfgs_defaults": (_i, [ctypes.POINTER(LbfgsOpts)]),
+    "cc_minimize": (_i, [_vp, _i64, _vp, ctypes.POINTER(LbfgsOpts), ctypes.POINTER(LbfgsResult)]),
     "cc_set_path": (_i, [_vp, _i]),
     "cc_check_device_error": (_i, [_vp]),
     "cc_energy_noalloc": (_i, [_i, _vp, _i64, _vp, _vp, _d, _i64, _vp, _vp, _vp, _vp]),
@@ -216,6 +231,22 @@ class CCPotential:
                                       precision))
         self.N = n
         return (f.value, g[: len(x)]) if grad else f.value
+
+    def minimize(self, frac, stopval=None, history=40, max_evals=100000, precision=PREC_FP64, gtol=0.0,
+                 ftol=1e-15, switch_energy_per_particle=1e-12, iters_per_check=32):
+        """Device-resident L-BFGS from the fractional start `frac`; returns (frac, E, evals, iters, status)."""
+        o = LbfgsOpts()
+        _check(self._lib.cc_lbfgs_defaults(ctypes.byref(o)))
+        o.history, o.max_evals, o.precision = history, max_evals, precision
+        o.gtol, o.ftol, o.switch_energy_per_particle, o.iters_per_check = gtol, ftol, switch_energy_per_particle, \
+            iters_per_check
+        if stopval is not None:
+            o.stopval = stopval
+        x = np.ascontiguousarray(frac, dtype=np.float64).reshape(-1, self.d).copy()
+        r = LbfgsResult()
+        _check(self._lib.cc_minimize(self._h, len(x), _ptr(x), ctypes.byref(o), ctypes.byref(r)))
+        self.N = len(x)
+        return x, r.E, r.evals, r.iters, r.status
 
     def set_path(self, path):
         """0 = the three-kernel split path (default), 1 = one fused cooperative kernel when the tables fit."""

@@ -9,6 +9,7 @@
 #include "../../include/cc_gpu.h"
 #include "cc_fused.cuh"
 #include "cc_kernels.cuh"
+#include "cc_lbfgs.cuh"
 #include "cc_plan.h"
 
 #include <algorithm>
@@ -159,6 +160,7 @@ struct cc_handle {
 	size_t partialF_cap = 0;
 	std::vector<std::pair<int, int *> > kstarts;   // even segment splits per count
 	bool use_fused = false;         // cc_set_path
+	const int *d_skip = nullptr;    // evaluations do nothing while *d_skip != 0 (set by cc_minimize)
 	bool timing = false;            // cc_set_timing
 	std::vector<cudaEvent_t> ev;    // 3 events per timed evaluation
 	size_t ev_used = 0;
@@ -419,6 +421,7 @@ int run_rho(cc_handle *h, DevKSet &k, int64_t N, const double *d_frac, double *d
 	a.nseg = (int)p.segs.size();
 	a.nslot = p.nslot;
 	a.partial = k.partial;
+	a.skip = h->d_skip;
 	if (int rc = launch_rho(h->d, a, mixed, p.nbgroups(), nsplit, csize, p.block_max_row, st))
 		return rc;
 	if (after_rho)
@@ -436,6 +439,7 @@ int run_rho(cc_handle *h, DevKSet &k, int64_t N, const double *d_frac, double *d
 	r.inv_vol = 1.0 / h->volume;
 	r.shift = h->shift;
 	r.E_out = d_E;
+	r.skip = h->d_skip;
 	CC_CUDA(launch_pdl(cc::cc_reduce_kernel, dim3((p.nslot + 31) / 32), dim3(cc::kRedThreads), 0, st, r));
 	if (want_rho_mode && !p.mode_slot.empty()) {
 		const int M = (int)p.mode_slot.size();
@@ -483,6 +487,7 @@ int run_force(cc_handle *h, int64_t N, const double *d_frac, double *d_F, double
 	a.fscale = 2.0 / h->volume;
 	a.F_out = d_F;
 	a.gfrac_out = d_gfrac;
+	a.skip = h->d_skip;
 	return launch_force(h->d, a, mixed, N, f->host.max_row, st);
 }
 
@@ -758,7 +763,7 @@ int eval_device(cc_handle *h, int64_t N, const double *d_frac, double *d_E, doub
 			return fail(CC_ERR_CUDA, "cudaEventCreate failed");
 		CC_CUDA(cudaEventRecord(e0, st));
 	}
-	if (!want_rho_mode && h->use_fused && fused_eligible(h, N, mixed)) {
+	if (!want_rho_mode && h->use_fused && !h->d_skip && fused_eligible(h, N, mixed)) {
 		// one cooperative launch: the whole evaluation is reported as the force interval
 		if (e1)
 			CC_CUDA(cudaEventRecord(e1, st));
@@ -1197,6 +1202,201 @@ int cc_probe_fma_peak(int precision, double *tflops)
 	if (int rc = device_ok())
 		return rc;
 	return precision == CC_PREC_FP64 ? probe_peak<double>(tflops) : probe_peak<float>(tflops);
+}
+
+int cc_lbfgs_defaults(cc_lbfgs_opts *o)
+{
+	if (!o)
+		return fail(CC_ERR_ARG, "opts is null");
+	o->history = 40;
+	o->max_evals = 100000;
+	o->stopval = -1e300;
+	o->gtol = 0.0;
+	o->ftol = 1e-15;
+	o->precision = CC_PREC_FP64;
+	o->switch_energy_per_particle = 1e-12;
+	o->iters_per_check = 32;
+	return CC_OK;
+}
+
+namespace {
+
+struct LbBuffers {
+	double *x = nullptr, *g = nullptr, *d = nullptr, *xt = nullptr, *gt = nullptr, *S = nullptr, *Y = nullptr;
+	double *part = nullptr;
+	cc::LbState *st = nullptr;
+	cc::LbInst *inst = nullptr;
+	void release()
+	{
+		cudaFree(x);
+		cudaFree(g);
+		cudaFree(d);
+		cudaFree(xt);
+		cudaFree(gt);
+		cudaFree(S);
+		cudaFree(Y);
+		cudaFree(part);
+		cudaFree(st);
+		cudaFree(inst);
+		*this = LbBuffers();
+	}
+};
+
+// one iteration: evaluation at x_trial, dot products, solve, update
+int lb_iteration(cc_handle *h, int64_t N, LbBuffers &b, int n, int nblk, int prec, cudaStream_t st)
+{
+	if (int rc = eval_device(h, N, b.xt, &b.st->Et, nullptr, b.gt, false, prec, st))
+		return rc;
+	cc::lb_dots_kernel<<<dim3(nblk, 1), cc::kLbThreads, 0, st>>>(b.inst, nblk);
+	cc::lb_solve_kernel<<<1, cc::kLbSolveThreads, 0, st>>>(b.inst, nblk);
+	cc::lb_update_kernel<<<dim3((n + cc::kLbThreads - 1) / cc::kLbThreads, 1), cc::kLbThreads, 0, st>>>(b.inst);
+	CC_CUDA(cudaGetLastError());
+	return CC_OK;
+}
+
+int lb_graph(cc_handle *h, int64_t N, LbBuffers &b, int n, int nblk, int prec, int iters, cudaGraphExec_t *out)
+{
+	cudaGraph_t g = nullptr;
+	CC_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+	int rc = CC_OK;
+	for (int i = 0; i < iters && rc == CC_OK; i++)
+		rc = lb_iteration(h, N, b, n, nblk, prec, h->stream);
+	cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+	if (rc)
+		return rc;
+	if (e != cudaSuccess)
+		return fail(CC_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+	e = cudaGraphInstantiate(out, g, 0);
+	cudaGraphDestroy(g);
+	if (e != cudaSuccess)
+		return fail(CC_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+	return CC_OK;
+}
+
+}  // namespace
+
+int cc_minimize(cc_handle *h, int64_t N, double *frac, const cc_lbfgs_opts *opts, cc_lbfgs_result *result)
+{
+	if (int rc = check_handle(h))
+		return rc;
+	cc_lbfgs_opts o;
+	cc_lbfgs_defaults(&o);
+	if (opts)
+		o = *opts;
+	if (N < 1 || !frac || o.history < 1 || o.history > cc::kLbMaxHist || o.iters_per_check < 1 ||
+	    (o.precision != CC_PREC_FP64 && o.precision != CC_PREC_MIXED && o.precision != CC_PREC_SCHEDULE))
+		return fail(CC_ERR_ARG, "invalid minimisation arguments");
+	if ((int64_t)N * h->d > (1 << 30))
+		return fail(CC_ERR_ARG, "too many variables");
+	const int d = h->d, n = (int)(N * d), m = o.history;
+	const int nblk = std::max(1, std::min(148, n / 2048));
+	LbBuffers b;
+	int rc;
+	if ((rc = dev_alloc(&b.x, n)) || (rc = dev_alloc(&b.g, n)) || (rc = dev_alloc(&b.d, n)) || (rc = dev_alloc(&b.xt, n)) ||
+	    (rc = dev_alloc(&b.gt, n)) || (rc = dev_alloc(&b.S, (size_t)m * n)) || (rc = dev_alloc(&b.Y, (size_t)m * n)) ||
+	    (rc = dev_alloc(&b.part, (size_t)nblk * cc::lb_ndots(m))) || (rc = dev_alloc(&b.st, 1)) ||
+	    (rc = dev_alloc(&b.inst, 1)) || (rc = ensure_particles(h, N))) {
+		b.release();
+		return rc;
+	}
+	auto cleanup = [&](int code) {
+		h->d_skip = nullptr;
+		b.release();
+		return code;
+	};
+	std::vector<double> x0((size_t)n);
+	for (int i = 0; i < n; i++) {
+		if (!std::isfinite(frac[i]))
+			return cleanup(fail(CC_ERR_ARG, "non-finite start"));
+		double v = frac[i] - std::floor(frac[i]);
+		x0[i] = v - std::floor(v);
+	}
+	CC_CUDA(cudaMemcpy(b.x, x0.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+	CC_CUDA(cudaMemcpy(b.xt, x0.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+	CC_CUDA(cudaMemset(b.g, 0, sizeof(double) * n));
+	CC_CUDA(cudaMemset(b.d, 0, sizeof(double) * n));
+	cc::LbInst inst;
+	inst.n = n;
+	inst.x = b.x;
+	inst.g = b.g;
+	inst.d = b.d;
+	inst.xt = b.xt;
+	inst.gt = b.gt;
+	inst.S = b.S;
+	inst.Y = b.Y;
+	inst.part = b.part;
+	inst.st = b.st;
+	CC_CUDA(cudaMemcpy(b.inst, &inst, sizeof(inst), cudaMemcpyHostToDevice));
+	// warm-up evaluations allocate the evaluation's work buffers before any capture
+	const bool sched = o.precision == CC_PREC_SCHEDULE;
+	const int prec0 = (o.precision == CC_PREC_FP64) ? CC_PREC_FP64 : CC_PREC_MIXED;
+	if ((rc = eval_device(h, N, b.xt, b.part, nullptr, b.gt, false, prec0, h->stream)) ||
+	    (sched && (rc = eval_device(h, N, b.xt, b.part, nullptr, b.gt, false, CC_PREC_FP64, h->stream))))
+		return cleanup(rc);
+	CC_CUDA(cudaStreamSynchronize(h->stream));
+	// state: a virtual previous point of infinite energy, so the first evaluation is always accepted
+	cc::LbState s0;
+	std::memset(&s0, 0, sizeof(s0));
+	s0.E = INFINITY;
+	s0.gamma = 1.0;
+	s0.stopval = o.stopval;
+	s0.gtol = o.gtol;
+	s0.ftol = o.ftol;
+	s0.max_evals = o.max_evals;
+	s0.m = m;
+	s0.newslot = -1;
+	CC_CUDA(cudaMemcpy(b.st, &s0, sizeof(s0), cudaMemcpyHostToDevice));
+	h->d_skip = &b.st->status;
+	cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+	auto destroy_graphs = [&]() {
+		for (auto &ge : gexec)
+			if (ge)
+				cudaGraphExecDestroy(ge);
+	};
+	if ((rc = lb_graph(h, N, b, n, nblk, prec0, o.iters_per_check, &gexec[0])) ||
+	    (sched && (rc = lb_graph(h, N, b, n, nblk, CC_PREC_FP64, o.iters_per_check, &gexec[1])))) {
+		destroy_graphs();
+		return cleanup(rc);
+	}
+	int stage = 0;
+	cc::LbState hs;
+	const int64_t max_rounds = o.max_evals / o.iters_per_check + 2;
+	for (int64_t round = 0; round < max_rounds; round++) {
+		cudaError_t e = cudaGraphLaunch(gexec[stage], h->stream);
+		if (e == cudaSuccess)
+			e = cudaMemcpyAsync(&hs, b.st, sizeof(hs), cudaMemcpyDeviceToHost, h->stream);
+		if (e == cudaSuccess)
+			e = cudaStreamSynchronize(h->stream);
+		if (e != cudaSuccess) {
+			destroy_graphs();
+			return cleanup(fail(CC_ERR_CUDA, std::string("minimisation: ") + cudaGetErrorString(e)));
+		}
+		if (hs.status != cc::kLbRunning)
+			break;
+		if (sched && stage == 0 && std::isfinite(hs.E) && hs.E <= o.switch_energy_per_particle * (double)N)
+			stage = 1;
+	}
+	destroy_graphs();
+	h->d_skip = nullptr;
+	// result: the last accepted point, wrapped into [0,1), and its FP64 energy
+	CC_CUDA(cudaMemcpy(x0.data(), b.x, sizeof(double) * n, cudaMemcpyDeviceToHost));
+	for (int i = 0; i < n; i++) {
+		double v = x0[i] - std::floor(x0[i]);
+		frac[i] = v - std::floor(v);
+	}
+	b.release();
+	if ((rc = cc_set_positions(h, N, frac)))
+		return rc;
+	double E = 0.0;
+	if ((rc = cc_energy_grad(h, &E, nullptr, CC_PREC_FP64)))
+		return rc;
+	if (result) {
+		result->E = E;
+		result->evals = hs.evals;
+		result->iters = hs.iters;
+		result->status = hs.status == cc::kLbRunning ? cc::kLbMaxEval : hs.status;
+	}
+	return CC_OK;
 }
 
 int cc_kset_stealthy(int d, const double *basis, int64_t N, double chi, int type, int64_t cap, int32_t *modes,

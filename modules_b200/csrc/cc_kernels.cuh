@@ -232,6 +232,7 @@ struct RhoArgs {
 	const TabSpec *bspec;     // nbgroups
 	int nseg, nslot;          // nseg = ngroups * 32, nslot = nseg * L
 	double2 *partial;         // [nsplit / cluster][nslot]
+	const int *skip;          // if not null and nonzero, the launch does nothing (a finished minimisation)
 };
 
 constexpr int kRhoWarps = 8;
@@ -263,6 +264,8 @@ __global__ void __launch_bounds__(kRhoThreads, 3) cc_rho_kernel(RhoArgs a)
 	const int j0 = min(a.N, split * a.per_split);
 	const int j1 = min(a.N, j0 + a.per_split);
 	cudaGridDependencySynchronize();   // inputs of this step are complete (programmatic dependent launch)
+	if (a.skip && *a.skip)             // uniform over the grid: no block reaches a cluster barrier
+		return;
 	__syncthreads();
 	const int row = sp.row | 1;        // odd row stride: consecutive particles' rows start in different banks
 	SeedIdx ix = seed_index<D>(sp, sg);
@@ -387,6 +390,7 @@ struct ReduceArgs {
 	unsigned *ticket;         // 1, zero between launches
 	double inv_vol, shift;
 	double *E_out;
+	const int *skip;
 };
 
 constexpr int kRedThreads = 256;   // 32 slots x 8 split chunks
@@ -400,6 +404,8 @@ static __global__ void __launch_bounds__(kRedThreads) cc_reduce_kernel(ReduceArg
 	const int per = (a.nsplit + 7) >> 3;
 	cudaGridDependencySynchronize();
 	cudaTriggerProgrammaticLaunchCompletion();
+	if (a.skip && *a.skip)
+		return;
 	const int s0 = min(a.nsplit, c * per), s1 = min(a.nsplit, s0 + per);
 	double2 t = make_double2(0.0, 0.0);
 	if (slot < a.nslot) {
@@ -497,6 +503,7 @@ struct ForceArgs {
 	double fscale;            // 2 / Volume
 	double *F_out;            // N x D Cartesian forces, or nullptr
 	double *gfrac_out;        // N x D dPhi/ds, or nullptr
+	const int *skip;
 };
 
 constexpr int kForceWarps = 8;
@@ -530,6 +537,8 @@ __global__ void __launch_bounds__(kForceThreads, 2) cc_force_kernel(ForceArgs a)
 	if (threadIdx.x == 0)
 		sp = a.kspec[ks];
 	cudaGridDependencySynchronize();   // u of this step is complete
+	if (a.skip && *a.skip)
+		return;
 	__syncthreads();
 	build_tables<D, C>(sp, a.frac, pbase, 32, nvalid, tab, 1, 32, threadIdx.x, kForceThreads);
 	__syncthreads();

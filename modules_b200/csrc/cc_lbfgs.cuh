@@ -1,0 +1,348 @@
+// cc_lbfgs.cuh — device-resident limited-memory BFGS for the collective-coordinate energy.
+//
+// Method: L-BFGS (Nocedal 1980) in the compact representation of Byrd, Nocedal and Schnabel (1994): with the m most
+// recent pairs S = [s_i], Y = [y_i] (oldest first), R = upper triangle of S^T Y, D = diag(s_i^T y_i) and
+// gamma = s^T y / y^T y of the newest pair,
+//     H g = gamma g + S w1 + gamma Y w2,   t = R^-1 (S^T g),  w2 = -t,  w1 = R^-T ((D + gamma Y^T Y) t - gamma Y^T g),
+// which needs two passes over the history per iteration (the dot products S^T g, Y^T g, ... and the combination),
+// both parallel over the n = N d variables, instead of the 2m dependent dot products of the two-loop recursion.
+// Line search: Armijo backtracking (c1 = 1e-4) with a safeguarded quadratic step; a pair enters the history only if
+// s^T y > 0. Variables are the fractional coordinates; the gradient is dPhi/ds from the force kernel.
+//
+// One iteration on the device (every instance of a batch at once, blockIdx.y = instance):
+//   evaluation at x_trial -> E_t, g_t;  lb_dots: block partials of the dot products;
+//   lb_solve (one block per instance): totals in block order, accept / reject, history matrices, the small solves,
+//     the next step length and the stop tests;  lb_update: history insert, x, g, the new direction and x_trial.
+// Every sum has a fixed order, so a run repeats bitwise.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cc {
+
+constexpr int kLbMaxHist = 64;
+constexpr int kLbThreads = 256;
+
+enum LbStatus {
+	kLbRunning = 0,
+	kLbStopval = 1,    // energy at or below the stop value
+	kLbGtol = 2,       // max |g| at or below gtol
+	kLbMaxEval = 3,    // evaluation limit
+	kLbLineSearch = 4, // line search found no decrease
+	kLbFtol = 5        // relative energy change below ftol on 3 consecutive accepted steps
+};
+
+struct LbState {
+	// energies and step
+	double E, Et, alpha, gd, gamma;
+	double stopval, gtol, ftol;
+	int64_t max_evals, evals, iters;
+	int m, count, head;     // history size, pairs stored, ring slot of the oldest pair
+	int status, accepted, rejects, small_steps;
+	int newslot;            // ring slot the update kernel fills with the accepted pair, or -1
+	double gmax;            // max |g| at x
+	double gg;              // g.g at x
+	double w[2 * kLbMaxHist];
+	double SY[kLbMaxHist * kLbMaxHist];   // SY[i * m + j] = s_i . y_j (ring slots)
+	double YY[kLbMaxHist * kLbMaxHist];   // YY[i * m + j] = y_i . y_j
+	double Sg[kLbMaxHist], Yg[kLbMaxHist];// S^T g, Y^T g at x (ring slots)
+};
+
+struct LbInst {
+	int n;                  // variables
+	double *x, *g, *d, *xt, *gt;
+	double *S, *Y;          // [m][n] ring
+	double *part;           // [nblk][kLbDots]
+	LbState *st;
+};
+
+// dot products per block. For each used ring slot i: s_i.gt, y_i.gt, s_i.y', y_i.y', y_i.s' with the candidate pair
+// s' = xt - x, y' = gt - g; then gt.d, gt.gt, s'.y', y'.y', y'.gt, max|gt|. Differences are formed before the
+// products, so s'.y' and the history cross terms carry no cancellation.
+__host__ __device__ constexpr int lb_ndots(int m) { return 5 * m + 6; }
+
+__global__ void __launch_bounds__(kLbThreads) lb_dots_kernel(const LbInst *insts, int nblk)
+{
+	const LbInst in = insts[blockIdx.y];
+	const LbState *st = in.st;
+	if (st->status != kLbRunning)
+		return;
+	const int m = st->m, nd = lb_ndots(m);
+	const int per = (in.n + nblk - 1) / nblk;
+	const int j0 = blockIdx.x * per, j1 = min(in.n, j0 + per);
+	__shared__ double red[kLbThreads / 32][5 * kLbMaxHist + 6];
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	const int count = st->count;
+	double a[6] = {0, 0, 0, 0, 0, 0};
+	for (int j = j0 + threadIdx.x; j < j1; j += kLbThreads) {
+		const double gt = in.gt[j], yj = gt - in.g[j], sj = in.xt[j] - in.x[j];
+		a[0] += gt * in.d[j];
+		a[1] += gt * gt;
+		a[2] += sj * yj;
+		a[3] += yj * yj;
+		a[4] += yj * gt;
+		a[5] = fmax(a[5], fabs(gt));
+	}
+#pragma unroll
+	for (int k = 0; k < 5; k++)
+		for (int o = 16; o > 0; o >>= 1)
+			a[k] += __shfl_down_sync(0xffffffffu, a[k], o);
+	for (int o = 16; o > 0; o >>= 1)
+		a[5] = fmax(a[5], __shfl_down_sync(0xffffffffu, a[5], o));
+	if (lane == 0)
+		for (int k = 0; k < 6; k++)
+			red[warp][5 * kLbMaxHist + k] = a[k];
+	for (int i = 0; i < count; i++) {
+		const double *s = in.S + (size_t)i * in.n, *y = in.Y + (size_t)i * in.n;
+		double b[5] = {0, 0, 0, 0, 0};
+		for (int j = j0 + threadIdx.x; j < j1; j += kLbThreads) {
+			const double gt = in.gt[j], yn = gt - in.g[j], sn = in.xt[j] - in.x[j];
+			const double si = s[j], yi = y[j];
+			b[0] += si * gt;
+			b[1] += yi * gt;
+			b[2] += si * yn;
+			b[3] += yi * yn;
+			b[4] += yi * sn;
+		}
+#pragma unroll
+		for (int k = 0; k < 5; k++)
+			for (int o = 16; o > 0; o >>= 1)
+				b[k] += __shfl_down_sync(0xffffffffu, b[k], o);
+		if (lane == 0)
+			for (int k = 0; k < 5; k++)
+				red[warp][5 * i + k] = b[k];
+	}
+	__syncthreads();
+	double *out = in.part + (size_t)blockIdx.x * nd;
+	for (int k = threadIdx.x; k < nd; k += kLbThreads) {
+		const int src = k < 5 * m ? k : 5 * kLbMaxHist + (k - 5 * m);
+		if (k < 5 * m && k / 5 >= count) {
+			out[k] = 0.0;
+			continue;
+		}
+		double t = red[0][src];
+		for (int w = 1; w < kLbThreads / 32; w++)
+			t = (k == nd - 1) ? fmax(t, red[w][src]) : t + red[w][src];
+		out[k] = t;
+	}
+}
+
+// ring slot of the c-th oldest pair
+__device__ __forceinline__ int lb_slot(const LbState *st, int c) { return (st->head + c) % st->m; }
+
+// warp-wide sum with a fixed tree (every lane gets the total)
+__device__ __forceinline__ double lb_warp_sum(double v)
+{
+	for (int o = 16; o > 0; o >>= 1)
+		v += __shfl_xor_sync(0xffffffffu, v, o);
+	return v;
+}
+
+constexpr int kLbSolveThreads = 256;
+
+// One block per instance: block totals of the dot products (parallel over the products, blocks summed in order),
+// accept / reject and the step length (thread 0), history matrices (parallel over slots), the triangular solves of
+// the compact form (warp 0, lanes split every inner sum), g.d of the new direction and the stop tests.
+__global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const LbInst *insts, int nblk)
+{
+	const LbInst in = insts[blockIdx.x];
+	LbState *st = in.st;
+	if (st->status != kLbRunning)
+		return;
+	__shared__ double tot[5 * kLbMaxHist + 6];
+	__shared__ double Sg[kLbMaxHist], Yg[kLbMaxHist], t[kLbMaxHist], q[kLbMaxHist], w1[kLbMaxHist];
+	__shared__ int sh_accept, sh_newslot, sh_k;
+	const int m = st->m, nd = lb_ndots(m);
+	for (int k = threadIdx.x; k < nd; k += kLbSolveThreads) {
+		double v = in.part[k];
+		for (int b = 1; b < nblk; b++)
+			v = (k == nd - 1) ? fmax(v, in.part[(size_t)b * nd + k]) : v + in.part[(size_t)b * nd + k];
+		tot[k] = v;
+	}
+	__syncthreads();
+	const double gtd = tot[5 * m], gtgt = tot[5 * m + 1], sy = tot[5 * m + 2], yy = tot[5 * m + 3],
+	             ygt = tot[5 * m + 4], gtmax = tot[5 * m + 5];
+	const int count = st->count;
+	if (threadIdx.x == 0) {
+		st->evals++;
+		const double alpha = st->alpha, E = st->E, Et = st->Et, gd = st->gd;
+		const bool finite = isfinite(Et) && isfinite(gtgt);
+		const bool armijo = finite && Et <= E + 1e-4 * alpha * gd;
+		sh_accept = armijo;
+		if (!armijo) {
+			// backtrack: safeguarded quadratic model of the energy along d
+			double a2 = 0.5 * alpha;
+			if (finite) {
+				const double den = 2.0 * (Et - E - gd * alpha);
+				if (den > 0)
+					a2 = -gd * alpha * alpha / den;
+				a2 = fmin(fmax(a2, 0.1 * alpha), 0.5 * alpha);
+			}
+			st->alpha = a2;
+			st->accepted = 0;
+			st->rejects++;
+			if (st->rejects > 60 || a2 < 1e-300)
+				st->status = kLbLineSearch;
+			else if (st->evals >= st->max_evals)
+				st->status = kLbMaxEval;
+		} else {
+			st->accepted = 1;
+			st->rejects = 0;
+			st->iters++;
+			const double dE = E - Et;
+			st->small_steps = (isfinite(E) && dE <= st->ftol * fabs(E)) ? st->small_steps + 1 : 0;
+			const bool keep = sy > 1e-300 && yy > 0 && isfinite(sy) && isfinite(yy);
+			int newslot = -1;
+			if (keep) {
+				newslot = count < m ? (st->head + count) % m : st->head;
+				if (count < m)
+					st->count = count + 1;
+				else
+					st->head = (st->head + 1) % m;
+				st->gamma = sy / yy;
+			}
+			sh_newslot = newslot;
+			st->newslot = newslot;
+			st->E = Et;
+			st->gmax = gtmax;
+			st->gg = gtgt;
+			if (Et <= st->stopval)
+				st->status = kLbStopval;
+			else if (gtmax <= st->gtol)
+				st->status = kLbGtol;
+			else if (st->small_steps >= 3)
+				st->status = kLbFtol;
+			else if (st->evals >= st->max_evals)
+				st->status = kLbMaxEval;
+		}
+	}
+	__syncthreads();
+	if (!sh_accept)
+		return;
+	const int newslot = sh_newslot;
+	// history products at the new point (ring slots), the new pair's rows and columns of S^T Y and Y^T Y
+	for (int i = threadIdx.x; i < count; i += kLbSolveThreads) {
+		if (i == newslot)   // the oldest pair, replaced by the new one below
+			continue;
+		Sg[i] = tot[5 * i];
+		Yg[i] = tot[5 * i + 1];
+		if (newslot >= 0) {
+			st->SY[i * m + newslot] = tot[5 * i + 2];
+			st->SY[newslot * m + i] = tot[5 * i + 4];
+			st->YY[i * m + newslot] = tot[5 * i + 3];
+			st->YY[newslot * m + i] = tot[5 * i + 3];
+		}
+	}
+	if (threadIdx.x == 0 && newslot >= 0) {
+		st->SY[newslot * m + newslot] = sy;
+		st->YY[newslot * m + newslot] = yy;
+		Sg[newslot] = st->alpha * gtd;   // s'.gt with s' = alpha d (alpha of this accepted step)
+		Yg[newslot] = ygt;
+	}
+	__syncthreads();
+	const int k = st->count, head = st->head;
+	const double gam = k > 0 ? st->gamma : 1.0;
+	for (int i = threadIdx.x; i < k; i += kLbSolveThreads) {
+		st->Sg[i] = Sg[i];
+		st->Yg[i] = Yg[i];
+	}
+	// compact-form solves on warp 0 (chronological index a <-> ring slot (head + a) % m)
+	if (threadIdx.x < 32) {
+		const int lane = threadIdx.x;
+		// t = R^-1 S^T g, R[a][b] = s_a . y_b (a <= b): backward substitution
+		for (int a = k - 1; a >= 0; a--) {
+			const int ia = (head + a) % m;
+			double v = 0.0;
+			for (int b = a + 1 + lane; b < k; b += 32)
+				v += st->SY[ia * m + (head + b) % m] * t[b];
+			v = lb_warp_sum(v);
+			if (lane == 0)
+				t[a] = (Sg[ia] - v) / st->SY[ia * m + ia];
+			__syncwarp();
+		}
+		// q = D t + gamma Y^T Y t - gamma Y^T g
+		for (int a = lane; a < k; a += 32) {
+			const int ia = (head + a) % m;
+			double v = 0.0;
+			for (int b = 0; b < k; b++)
+				v += st->YY[ia * m + (head + b) % m] * t[b];
+			q[a] = st->SY[ia * m + ia] * t[a] + gam * v - gam * Yg[ia];
+		}
+		__syncwarp();
+		// w1 = R^-T q: forward substitution
+		for (int a = 0; a < k; a++) {
+			const int ia = (head + a) % m;
+			double v = 0.0;
+			for (int b = lane; b < a; b += 32)
+				v += st->SY[((head + b) % m) * m + ia] * w1[b];
+			v = lb_warp_sum(v);
+			if (lane == 0)
+				w1[a] = (q[a] - v) / st->SY[ia * m + ia];
+			__syncwarp();
+		}
+		// store per ring slot: w[slot] = w1, w[kLbMaxHist + slot] = -gamma t; g.d of d = -(gamma g + S w1 + gamma Y w2)
+		double gdn = 0.0;
+		for (int a = lane; a < k; a += 32) {
+			const int ia = (head + a) % m;
+			st->w[ia] = w1[a];
+			st->w[kLbMaxHist + ia] = -gam * t[a];
+			gdn += w1[a] * Sg[ia] - gam * t[a] * Yg[ia];
+		}
+		gdn = lb_warp_sum(gdn);
+		if (lane == 0) {
+			gdn = -(gam * gtgt + gdn);
+			int kk = k;
+			st->gamma = gam;
+			if (!(gdn < 0) || !isfinite(gdn)) {
+				// not a descent direction: drop the history (and the pair just formed), restart from steepest descent
+				gdn = -gtgt;
+				st->count = 0;
+				st->head = 0;
+				st->gamma = 1.0;
+				st->newslot = -1;
+				kk = 0;
+			}
+			st->gd = gdn;
+			// first step of a fresh history: at most 1e-2 of a cell per coordinate; afterwards the unit step
+			st->alpha = (kk == 0) ? fmin(1.0, 1e-2 / fmax(gtmax, 1e-300)) : 1.0;
+		}
+	}
+}
+
+// accept: insert the pair, move x and g; then d = -(gamma g + S w1 + gamma Y w2) and x_trial = x + alpha d.
+// reject: x_trial = x + alpha d.
+__global__ void __launch_bounds__(kLbThreads) lb_update_kernel(const LbInst *insts)
+{
+	const LbInst in = insts[blockIdx.y];
+	const LbState *st = in.st;
+	if (st->status != kLbRunning && !(st->accepted && st->status != kLbLineSearch))
+		return;
+	const int j = blockIdx.x * kLbThreads + threadIdx.x;
+	if (j >= in.n)
+		return;
+	const int m = st->m;
+	if (st->accepted) {
+		const int newslot = st->newslot;
+		const double gt = in.gt[j];
+		if (newslot >= 0 && st->status == kLbRunning) {
+			// s = x_trial - x exactly as stepped; y = gt - g (a finished run stores no pair, so a repeated
+			// launch after the end only repeats the idempotent x = x_trial, g = gt)
+			in.S[(size_t)newslot * in.n + j] = in.xt[j] - in.x[j];
+			in.Y[(size_t)newslot * in.n + j] = gt - in.g[j];
+		}
+		in.x[j] = in.xt[j];
+		in.g[j] = gt;
+		if (st->status != kLbRunning)
+			return;
+		double v = st->gamma * gt;
+		for (int c = 0; c < st->count; c++) {
+			const int i = lb_slot(st, c);
+			v += st->w[i] * in.S[(size_t)i * in.n + j] + st->w[kLbMaxHist + i] * in.Y[(size_t)i * in.n + j];
+		}
+		in.d[j] = -v;
+	}
+	(void)m;
+	in.xt[j] = in.x[j] + st->alpha * in.d[j];
+}
+
+}  // namespace cc
