@@ -106,10 +106,11 @@ int cc_objective(cc_handle *h, int64_t N, const double *x, double rescale, doubl
 enum {
 	CC_PREC_SCHEDULE = 2        /* cc_minimize: mixed precision until E/N <= switch_energy_per_particle, then FP64 */
 };
+#define CC_STOPVAL_GROUND_STATE (-1.0)
 typedef struct {
 	int history;                /* correction pairs m (1..64), default 40 as the reference's LBFGSHistory */
 	int64_t max_evals;          /* evaluation limit, default 100000 */
-	double stopval;             /* stop when E <= stopval, default -1e300 (the ground state: 1e-20 * N) */
+	double stopval;             /* stop when E <= stopval, default -1e300; CC_STOPVAL_GROUND_STATE: E <= 1e-20 N */
 	double gtol;                /* stop when max |dE/ds| <= gtol, default 0 */
 	double ftol;                /* stop after 3 accepted steps with E decreasing by <= ftol |E|, default 1e-15 */
 	int precision;              /* CC_PREC_FP64 (default), CC_PREC_MIXED or CC_PREC_SCHEDULE */
@@ -128,6 +129,53 @@ int cc_lbfgs_defaults(cc_lbfgs_opts *opts);
 /* Minimise the energy from the fractional start frac (N x d, host), which receives the result wrapped into [0,1).
  * The handle's bound positions become the result. */
 int cc_minimize(cc_handle *h, int64_t N, double *frac, const cc_lbfgs_opts *opts, cc_lbfgs_result *result);
+
+/* --- batches of independent configurations (no counterpart in the reference, which evaluates one at a time) ---
+ * A batch holds `count` instances, each an existing handle (its cell, constraint set, Shift) with a fixed particle
+ * count N[i]. One evaluation of the batch is one cooperative kernel launch per dimension present (work items of all
+ * instances share the persistent grid); a batched minimisation runs every instance's L-BFGS at once, and instances
+ * that have finished are skipped item by item. The handles must outlive the batch. */
+typedef struct cc_batch cc_batch;
+int cc_batch_create(int count, cc_handle *const *handles, const int64_t *N, cc_batch **out);
+int cc_batch_destroy(cc_batch *b);
+/* Bind positions (host, frac[i] is N[i] x d_i) to the batch's device buffers. */
+int cc_batch_set_positions(cc_batch *b, const double *const *frac);
+/* Evaluate every instance at its bound positions: energies E[count] and, if F is not NULL, forces F[i] (host). */
+int cc_batch_energy_grad(cc_batch *b, double *E, double *const *F, int precision);
+/* The same, enqueued on `stream` with results left on the device (no host synchronisation). */
+int cc_batch_eval_device(cc_batch *b, int precision, void *stream);
+/* Minimise every instance from its bound positions; frac[i] (host) receives the results, results[i] the outcomes. */
+int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opts, cc_lbfgs_result *results);
+
+/* --- ground-state server with continuous batching (no counterpart in the reference) ------------------------------
+ * Each request is a stealthy configuration in a periodic cube of unit density (side N^(1/d)): the CLI's k-set for
+ * (d, N, chi) with weights vtype (0: v = 1, 3: v = (1 - |k|/K)^2, as cc_kset_stealthy), a start frac0 (N x d) and an
+ * arrival time in seconds after the call starts. The server minimises every request to Phi/N < 1e-20 (FP64), admitting
+ * arrived requests while a slot is free and their device memory fits hbm_budget, and running all admitted requests
+ * together, iters_per_round L-BFGS iterations per round; finished requests leave between rounds. */
+typedef struct {
+	int d;
+	int64_t N;
+	double chi;
+	int vtype;
+	const double *frac0;
+	double arrival_s;
+	int64_t max_evals;          /* 0: 100000 */
+} cc_request;
+typedef struct {
+	double E;                   /* energy at the end (FP64) */
+	int64_t evals;
+	int status;                 /* as cc_lbfgs_result.status */
+	double t_admit, t_done;     /* seconds after the call started */
+} cc_request_result;
+typedef struct {
+	size_t hbm_budget;          /* bytes for the admitted requests, default 16 GiB */
+	int max_slots;              /* admitted requests at most, default 256 */
+	int iters_per_round;        /* default 16 */
+	int history;                /* L-BFGS pairs, default 40 */
+} cc_serve_opts;
+int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *opts, cc_request_result *results, double *wall_s);
+const char *cc_serve_last_error(void);
 
 /* Device-resident evaluation: d_frac (N x d, device), outputs d_E (1 double) and d_F (N x d Cartesian, may be
  * NULL) and d_gfrac (N x d gradient of the energy with respect to the fractional coordinates, may be NULL), all on

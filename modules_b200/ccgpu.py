@@ -46,7 +46,23 @@ class LbfgsResult(ctypes.Structure):
                 ("status", ctypes.c_int)]
 
 
+class ServeRequest(ctypes.Structure):
+    _fields_ = [("d", ctypes.c_int), ("N", ctypes.c_int64), ("chi", ctypes.c_double), ("vtype", ctypes.c_int),
+                ("frac0", ctypes.c_void_p), ("arrival_s", ctypes.c_double), ("max_evals", ctypes.c_int64)]
+
+
+class ServeResult(ctypes.Structure):
+    _fields_ = [("E", ctypes.c_double), ("evals", ctypes.c_int64), ("status", ctypes.c_int),
+                ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double)]
+
+
+class ServeOpts(ctypes.Structure):
+    _fields_ = [("hbm_budget", ctypes.c_size_t), ("max_slots", ctypes.c_int), ("iters_per_round", ctypes.c_int),
+                ("history", ctypes.c_int)]
+
+
 PREC_SCHEDULE = 2
+STOPVAL_GROUND_STATE = -1.0
 
 _SIGS = {
     "cc_last_error": (ctypes.c_char_p, []),
@@ -71,6 +87,15 @@ _SIGS = {
     "cc_probe_fma_peak": (_i, [_i, ctypes.POINTER(_d)]),
     "cc_lbfgs_defaults": (_i, [ctypes.POINTER(LbfgsOpts)]),
     "cc_minimize": (_i, [_vp, _i64, _vp, ctypes.POINTER(LbfgsOpts), ctypes.POINTER(LbfgsResult)]),
+    "cc_batch_create": (_i, [_i, ctypes.POINTER(_vp), ctypes.POINTER(_i64), ctypes.POINTER(_vp)]),
+    "cc_batch_destroy": (_i, [_vp]),
+    "cc_batch_set_positions": (_i, [_vp, ctypes.POINTER(_vp)]),
+    "cc_batch_energy_grad": (_i, [_vp, _vp, ctypes.POINTER(_vp), _i]),
+    "cc_batch_eval_device": (_i, [_vp, _i, _vp]),
+    "cc_batch_minimize": (_i, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(LbfgsOpts), ctypes.POINTER(LbfgsResult)]),
+    "cc_serve": (_i, [ctypes.POINTER(ServeRequest), _i, ctypes.POINTER(ServeOpts), ctypes.POINTER(ServeResult),
+                      ctypes.POINTER(_d)]),
+    "cc_serve_last_error": (ctypes.c_char_p, []),
     "cc_set_path": (_i, [_vp, _i]),
     "cc_check_device_error": (_i, [_vp]),
     "cc_energy_noalloc": (_i, [_i, _vp, _i64, _vp, _vp, _d, _i64, _vp, _vp, _vp, _vp]),
@@ -275,3 +300,87 @@ class CCPotential:
         _check(self._lib.cc_energy_grad_device(self._h, int(N), _vp(d_frac), _vp(d_E), _vp(d_F) if d_F else None,
                                                _vp(d_gfrac) if d_gfrac else None, precision,
                                                _vp(stream) if stream else None))
+
+
+class CCBatch:
+    """Many independent configurations evaluated (and minimised) together: one cooperative launch per dimension."""
+
+    def __init__(self, pots, N):
+        self._lib = load_library()
+        self.pots = list(pots)
+        self.N = [int(n) for n in N]
+        hs = (_vp * len(self.pots))(*[p.handle for p in self.pots])
+        ns = (_i64 * len(self.N))(*self.N)
+        b = _vp()
+        _check(self._lib.cc_batch_create(len(self.pots), hs, ns, ctypes.byref(b)))
+        self._b = b
+
+    def close(self):
+        if getattr(self, "_b", None):
+            self._lib.cc_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._b
+
+    def _arrays(self, fracs):
+        arrs = [np.ascontiguousarray(f, dtype=np.float64).reshape(n, p.d).copy()
+                for f, n, p in zip(fracs, self.N, self.pots)]
+        return arrs, (_vp * len(arrs))(*[a.ctypes.data_as(_vp) for a in arrs])
+
+    def set_positions(self, fracs):
+        arrs, ptrs = self._arrays(fracs)
+        _check(self._lib.cc_batch_set_positions(self._b, ptrs))
+
+    def energy_and_forces(self, precision=PREC_FP64, forces=True):
+        E = np.zeros(len(self.pots))
+        F = [np.zeros((n, p.d)) for n, p in zip(self.N, self.pots)]
+        fp = (_vp * len(F))(*[f.ctypes.data_as(_vp) for f in F]) if forces else None
+        _check(self._lib.cc_batch_energy_grad(self._b, E.ctypes.data_as(_vp), fp, precision))
+        return (E, F) if forces else (E, None)
+
+    def eval_device(self, precision=PREC_FP64, stream=None):
+        _check(self._lib.cc_batch_eval_device(self._b, precision, _vp(stream) if stream else None))
+
+    def minimize(self, fracs, stopval=STOPVAL_GROUND_STATE, history=40, max_evals=100000, precision=PREC_FP64,
+                 gtol=0.0, ftol=1e-15, switch_energy_per_particle=1e-12, iters_per_check=32):
+        """Minimise every instance from fracs[i]; returns (list of frac, E array, evals, iters, status arrays)."""
+        self.set_positions(fracs)
+        arrs, ptrs = self._arrays(fracs)
+        o = LbfgsOpts()
+        _check(self._lib.cc_lbfgs_defaults(ctypes.byref(o)))
+        o.history, o.max_evals, o.precision, o.stopval = history, max_evals, precision, stopval
+        o.gtol, o.ftol, o.switch_energy_per_particle, o.iters_per_check = gtol, ftol, switch_energy_per_particle, \
+            iters_per_check
+        res = (LbfgsResult * len(arrs))()
+        _check(self._lib.cc_batch_minimize(self._b, ptrs, ctypes.byref(o), res))
+        return (arrs, np.array([r.E for r in res]), np.array([r.evals for r in res]),
+                np.array([r.iters for r in res]), np.array([r.status for r in res]))
+
+
+def serve(requests, hbm_budget=16 << 30, max_slots=256, iters_per_round=16, history=40):
+    """Run the continuous-batching ground-state server on `requests`, a list of dicts with keys d, N, chi, vtype,
+    frac0 (N x d array), arrival_s. Returns (list of result dicts, wall seconds)."""
+    lib = load_library()
+    keep = []
+    reqs = (ServeRequest * len(requests))()
+    for i, r in enumerate(requests):
+        f = np.ascontiguousarray(r["frac0"], dtype=np.float64).reshape(int(r["N"]), int(r["d"]))
+        keep.append(f)
+        reqs[i] = ServeRequest(int(r["d"]), int(r["N"]), float(r["chi"]), int(r.get("vtype", 0)),
+                               f.ctypes.data_as(_vp), float(r.get("arrival_s", 0.0)), int(r.get("max_evals", 0)))
+    opts = ServeOpts(hbm_budget, max_slots, iters_per_round, history)
+    res = (ServeResult * len(requests))()
+    wall = _d()
+    rc = lib.cc_serve(reqs, len(requests), ctypes.byref(opts), res, ctypes.byref(wall))
+    if rc != 0:
+        raise CCError(rc, lib.cc_serve_last_error().decode())
+    out = [dict(E=x.E, evals=x.evals, status=x.status, t_admit=x.t_admit, t_done=x.t_done) for x in res]
+    return out, wall.value

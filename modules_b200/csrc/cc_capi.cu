@@ -7,6 +7,7 @@
 //   cc_force_kernel -> Cartesian forces and/or the gradient in fractional coordinates.
 // There is no CPU path: without a CUDA device every call that computes returns CC_ERR_NOGPU.
 #include "../../include/cc_gpu.h"
+#include "cc_batch.cuh"
 #include "cc_fused.cuh"
 #include "cc_kernels.cuh"
 #include "cc_lbfgs.cuh"
@@ -14,6 +15,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -104,6 +106,13 @@ template <class T> int upload(T **p, const std::vector<T> &v)
 		return rc;
 	if (!v.empty())
 		CC_CUDA(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+	return CC_OK;
+}
+
+template <class T> int upload_into(T *p, const std::vector<T> &v)
+{
+	if (!v.empty())
+		CC_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
 	return CC_OK;
 }
 
@@ -1339,7 +1348,7 @@ int cc_minimize(cc_handle *h, int64_t N, double *frac, const cc_lbfgs_opts *opts
 	std::memset(&s0, 0, sizeof(s0));
 	s0.E = INFINITY;
 	s0.gamma = 1.0;
-	s0.stopval = o.stopval;
+	s0.stopval = o.stopval == CC_STOPVAL_GROUND_STATE ? 1e-20 * (double)N : o.stopval;
 	s0.gtol = o.gtol;
 	s0.ftol = o.ftol;
 	s0.max_evals = o.max_evals;
@@ -1396,6 +1405,500 @@ int cc_minimize(cc_handle *h, int64_t N, double *frac, const cc_lbfgs_opts *opts
 		result->iters = hs.iters;
 		result->status = hs.status == cc::kLbRunning ? cc::kLbMaxEval : hs.status;
 	}
+	return CC_OK;
+}
+
+}  // extern "C"
+
+// ===============================================================================================================
+// batches
+// ===============================================================================================================
+namespace {
+
+// carve 256-byte aligned pieces out of one device allocation
+struct Arena {
+	unsigned char *base = nullptr;
+	size_t used = 0, cap = 0;
+	size_t take(size_t bytes)
+	{
+		const size_t off = used;
+		used += (bytes + 255) / 256 * 256;
+		return off;
+	}
+	template <class T> T *at(size_t off) { return reinterpret_cast<T *>(base + off); }
+};
+
+struct BatchGroup {
+	int D = 0;
+	std::vector<int> members;            // instance indices
+	cc::BInst *d_inst = nullptr;         // evaluation descriptors (batch positions)
+	cc::BInst *d_inst_lb = nullptr;      // minimisation descriptors (L-BFGS trial points)
+	int *d_pre = nullptr;                // 4 x (B + 1)
+	int total[4] = {0, 0, 0, 0};
+};
+
+}  // namespace
+
+struct cc_batch {
+	std::vector<cc_handle *> h;
+	std::vector<int64_t> N;
+	std::vector<cc::BInst> inst;         // host copies (evaluation descriptors)
+	std::vector<BatchGroup> groups;
+	Arena arena;
+	std::vector<size_t> off_frac, off_F, off_E;
+	cudaStream_t stream = nullptr;
+	unsigned *d_bar = nullptr;
+};
+
+namespace {
+
+template <int D, bool MIXED> int batch_grid(int *grid)
+{
+	static int per_sm = -1;
+	if (per_sm < 0) {
+		CC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cc::cc_batch_kernel<D, 8, MIXED>,
+		                                                     cc::kFusedThreads, 0));
+		if (per_sm < 1)
+			return fail(CC_ERR_CUDA, "batch kernel cannot be resident");
+	}
+	*grid = per_sm * sm_count();
+	return CC_OK;
+}
+
+template <int D, bool MIXED> int batch_launch_t(cc::BatchArgs &a, cudaStream_t st)
+{
+	int grid = 0;
+	if (int rc = batch_grid<D, MIXED>(&grid))
+		return rc;
+	void *args[] = {&a};
+	CC_CUDA(cudaLaunchCooperativeKernel((const void *)cc::cc_batch_kernel<D, 8, MIXED>, dim3(grid),
+	                                    dim3(cc::kFusedThreads), args, 0, st));
+	return CC_OK;
+}
+
+int batch_launch(int D, bool mixed, cc::BatchArgs &a, cudaStream_t st)
+{
+	switch (D) {
+	case 1: return mixed ? batch_launch_t<1, true>(a, st) : batch_launch_t<1, false>(a, st);
+	case 2: return mixed ? batch_launch_t<2, true>(a, st) : batch_launch_t<2, false>(a, st);
+	default: return mixed ? batch_launch_t<3, true>(a, st) : batch_launch_t<3, false>(a, st);
+	}
+}
+
+// evaluate every group with the given descriptors (lb = the minimisation's)
+int batch_eval(cc_batch *b, bool lb, int precision, cudaStream_t st)
+{
+	const bool mixed = precision == CC_PREC_MIXED;
+	for (BatchGroup &g : b->groups) {
+		cc::BatchArgs a;
+		a.inst = lb ? g.d_inst_lb : g.d_inst;
+		a.B = (int)g.members.size();
+		for (int k = 0; k < 4; k++)
+			a.pre[k] = g.d_pre + k * (a.B + 1);
+		a.bar = b->d_bar;
+		if (int rc = batch_launch(g.D, mixed, a, st))
+			return rc;
+	}
+	return CC_OK;
+}
+
+int batch_check_barrier(cc_batch *b)
+{
+	unsigned w[3] = {0, 0, 0};
+	CC_CUDA(cudaMemcpy(w, b->d_bar, sizeof(w), cudaMemcpyDeviceToHost));
+	if (w[2] != 0u) {
+		CC_CUDA(cudaMemset(b->d_bar, 0, 3 * sizeof(unsigned)));
+		return fail(CC_ERR_TIMEOUT, "a grid barrier wait ran out in the batch kernel");
+	}
+	return CC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cc_batch_create(int count, cc_handle *const *handles, const int64_t *N, cc_batch **out)
+{
+	if (!out || count < 1 || !handles || !N)
+		return fail(CC_ERR_ARG, "invalid batch arguments");
+	*out = nullptr;
+	for (int i = 0; i < count; i++)
+		if (!handles[i] || N[i] < 1 || N[i] > (1 << 26) || handles[i]->main.plan.nslot == 0)
+			return fail(CC_ERR_ARG, "every instance needs a handle with constraints and 1 <= N <= 2^26");
+	cc_batch *b = new cc_batch();
+	b->h.assign(handles, handles + count);
+	b->N.assign(N, N + count);
+	b->inst.resize(count);
+	// sizes
+	std::vector<size_t> o_tabP(count), o_tabE(count), o_part(count), o_u(count), o_ep(count), o_pg(count), o_fc(count);
+	b->off_frac.resize(count);
+	b->off_F.resize(count);
+	b->off_E.resize(count);
+	for (int i = 0; i < count; i++) {
+		cc_handle *h = handles[i];
+		const cc::Plan &p = h->main.plan;
+		const int64_t n = N[i];
+		const int Npad = (int)((n + 31) / 32 * 32);
+		const int rowP = h->gspec.row | 1;
+		const int nsplit = (int)((n + cc::kBatchSplit - 1) / cc::kBatchSplit);
+		const int nks = std::max(1, (int)(p.segs.size() + cc::kBatchSegs - 1) / cc::kBatchSegs);
+		b->off_frac[i] = b->arena.take(sizeof(double) * n * h->d);
+		b->off_F[i] = b->arena.take(sizeof(double) * n * h->d);
+		b->off_E[i] = b->arena.take(sizeof(double));
+		o_tabP[i] = b->arena.take(sizeof(double2) * (size_t)rowP * Npad);
+		o_tabE[i] = b->arena.take(sizeof(double2) * (size_t)h->gspec.row * Npad);
+		o_part[i] = b->arena.take(sizeof(double2) * (size_t)nsplit * p.nslot);
+		o_u[i] = b->arena.take(sizeof(double2) * p.nslot);
+		o_ep[i] = b->arena.take(sizeof(double) * ((p.nslot + 255) / 256));
+		o_pg[i] = b->arena.take(sizeof(double) * (size_t)nks * n * h->d);
+		o_fc[i] = b->arena.take(sizeof(unsigned) * ((n + 31) / 32));
+	}
+	int rc;
+	if ((rc = dev_alloc(&b->arena.base, b->arena.used)) || (rc = dev_alloc(&b->d_bar, 4))) {
+		cc_batch_destroy(b);
+		return rc;
+	}
+	b->arena.cap = b->arena.used;
+	if (cudaMemset(b->arena.base, 0, b->arena.used) != cudaSuccess || cudaMemset(b->d_bar, 0, 16) != cudaSuccess ||
+	    cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+		cc_batch_destroy(b);
+		return fail(CC_ERR_CUDA, "batch initialisation failed");
+	}
+	for (int i = 0; i < count; i++) {
+		cc_handle *h = handles[i];
+		const cc::Plan &p = h->main.plan;
+		cc::BInst &in = b->inst[i];
+		std::memset(&in, 0, sizeof(in));
+		in.frac = b->arena.at<double>(b->off_frac[i]);
+		in.E_out = b->arena.at<double>(b->off_E[i]);
+		in.F_out = b->arena.at<double>(b->off_F[i]);
+		in.gfrac_out = nullptr;
+		in.status = nullptr;
+		in.N = (int)N[i];
+		in.Npad = (int)((N[i] + 31) / 32 * 32);
+		in.segs = h->main.segs;
+		in.ngroups = p.ngroups();
+		in.nseg = (int)p.segs.size();
+		in.nslot = p.nslot;
+		in.slotV = h->main.slotV;
+		in.rho_offset = h->rho_offset;
+		in.inv_vol = 1.0 / h->volume;
+		in.shift = h->shift;
+		in.spec = h->gspec;
+		in.tabP = b->arena.at<void>(o_tabP[i]);
+		in.tabE = b->arena.at<void>(o_tabE[i]);
+		in.nsplit = (int)((N[i] + cc::kBatchSplit - 1) / cc::kBatchSplit);
+		in.partial = b->arena.at<double2>(o_part[i]);
+		in.u_slot = b->arena.at<double2>(o_u[i]);
+		in.epart = b->arena.at<double>(o_ep[i]);
+		in.nechunk = (p.nslot + 255) / 256;
+		in.nks = std::max(1, (int)(p.segs.size() + cc::kBatchSegs - 1) / cc::kBatchSegs);
+		in.partialG = b->arena.at<double>(o_pg[i]);
+		in.fcounters = b->arena.at<unsigned>(o_fc[i]);
+		for (int k = 0; k < 9; k++)
+			in.recip[k] = h->recip[k];
+		in.fscale = 2.0 / h->volume;
+	}
+	// one group per dimension
+	for (int D = 1; D <= 3; D++) {
+		BatchGroup g;
+		g.D = D;
+		for (int i = 0; i < count; i++)
+			if (handles[i]->d == D)
+				g.members.push_back(i);
+		if (g.members.empty())
+			continue;
+		const int B = (int)g.members.size();
+		std::vector<int> pre(4 * (B + 1), 0);
+		std::vector<cc::BInst> gi;
+		for (int k = 0; k < B; k++) {
+			const cc::BInst &in = b->inst[g.members[k]];
+			const int c[4] = {(in.N * in.spec.items + cc::kFusedThreads - 1) / cc::kFusedThreads, in.ngroups * in.nsplit,
+			                  in.nechunk, ((in.N + 31) / 32) * in.nks};
+			for (int ph = 0; ph < 4; ph++)
+				pre[ph * (B + 1) + k + 1] = pre[ph * (B + 1) + k] + c[ph];
+			gi.push_back(in);
+		}
+		for (int ph = 0; ph < 4; ph++)
+			g.total[ph] = pre[ph * (B + 1) + B];
+		if ((rc = upload(&g.d_inst, gi)) || (rc = upload(&g.d_pre, pre)) || (rc = dev_alloc(&g.d_inst_lb, B))) {
+			b->groups.push_back(g);
+			cc_batch_destroy(b);
+			return rc;
+		}
+		b->groups.push_back(g);
+	}
+	*out = b;
+	return CC_OK;
+}
+
+int cc_batch_destroy(cc_batch *b)
+{
+	if (!b)
+		return CC_OK;
+	if (b->stream)
+		cudaStreamSynchronize(b->stream);
+	for (BatchGroup &g : b->groups) {
+		cudaFree(g.d_inst);
+		cudaFree(g.d_inst_lb);
+		cudaFree(g.d_pre);
+	}
+	cudaFree(b->arena.base);
+	cudaFree(b->d_bar);
+	if (b->stream)
+		cudaStreamDestroy(b->stream);
+	delete b;
+	return CC_OK;
+}
+
+int cc_batch_set_positions(cc_batch *b, const double *const *frac)
+{
+	if (!b || !frac)
+		return fail(CC_ERR_ARG, "invalid batch arguments");
+	for (size_t i = 0; i < b->h.size(); i++) {
+		const size_t n = (size_t)b->N[i] * b->h[i]->d;
+		std::vector<double> w(n);
+		for (size_t k = 0; k < n; k++) {
+			if (!std::isfinite(frac[i][k]))
+				return fail(CC_ERR_ARG, "non-finite fractional coordinate");
+			double v = frac[i][k] - std::floor(frac[i][k]);
+			w[k] = v - std::floor(v);
+		}
+		CC_CUDA(cudaMemcpyAsync(b->arena.at<double>(b->off_frac[i]), w.data(), sizeof(double) * n,
+		                        cudaMemcpyHostToDevice, b->stream));
+		CC_CUDA(cudaStreamSynchronize(b->stream));
+	}
+	return CC_OK;
+}
+
+int cc_batch_eval_device(cc_batch *b, int precision, void *stream)
+{
+	if (!b)
+		return fail(CC_ERR_ARG, "null batch");
+	if (int rc = check_prec(precision))
+		return rc;
+	return batch_eval(b, false, precision, stream ? static_cast<cudaStream_t>(stream) : b->stream);
+}
+
+int cc_batch_energy_grad(cc_batch *b, double *E, double *const *F, int precision)
+{
+	if (!b || !E)
+		return fail(CC_ERR_ARG, "invalid batch arguments");
+	if (int rc = cc_batch_eval_device(b, precision, b->stream))
+		return rc;
+	CC_CUDA(cudaStreamSynchronize(b->stream));
+	if (int rc = batch_check_barrier(b))
+		return rc;
+	for (size_t i = 0; i < b->h.size(); i++) {
+		CC_CUDA(cudaMemcpy(&E[i], b->arena.at<double>(b->off_E[i]), sizeof(double), cudaMemcpyDeviceToHost));
+		if (F && F[i])
+			CC_CUDA(cudaMemcpy(F[i], b->arena.at<double>(b->off_F[i]), sizeof(double) * b->N[i] * b->h[i]->d,
+			                   cudaMemcpyDeviceToHost));
+	}
+	return CC_OK;
+}
+
+int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opts, cc_lbfgs_result *results)
+{
+	if (!b || !frac)
+		return fail(CC_ERR_ARG, "invalid batch arguments");
+	cc_lbfgs_opts o;
+	cc_lbfgs_defaults(&o);
+	if (opts)
+		o = *opts;
+	if (o.history < 1 || o.history > cc::kLbMaxHist || o.iters_per_check < 1 ||
+	    (o.precision != CC_PREC_FP64 && o.precision != CC_PREC_MIXED && o.precision != CC_PREC_SCHEDULE))
+		return fail(CC_ERR_ARG, "invalid minimisation options");
+	const int count = (int)b->h.size(), m = o.history;
+	int maxn = 0;
+	for (int i = 0; i < count; i++)
+		maxn = std::max(maxn, (int)(b->N[i] * b->h[i]->d));
+	const int nblk = std::max(1, std::min(32, maxn / 2048));
+	// L-BFGS buffers of every instance in one allocation
+	Arena ar;
+	std::vector<size_t> ox(count), og(count), od(count), oxt(count), ogt(count), oS(count), oY(count), op(count),
+	    ost(count);
+	for (int i = 0; i < count; i++) {
+		const size_t n = (size_t)b->N[i] * b->h[i]->d;
+		ox[i] = ar.take(8 * n);
+		og[i] = ar.take(8 * n);
+		od[i] = ar.take(8 * n);
+		oxt[i] = ar.take(8 * n);
+		ogt[i] = ar.take(8 * n);
+		oS[i] = ar.take(8 * n * m);
+		oY[i] = ar.take(8 * n * m);
+		op[i] = ar.take(8 * (size_t)nblk * cc::lb_ndots(m));
+		ost[i] = ar.take(sizeof(cc::LbState));
+	}
+	cc::LbInst *d_lb = nullptr;
+	int rc;
+	if ((rc = dev_alloc(&ar.base, ar.used)) || (rc = dev_alloc(&d_lb, count))) {
+		cudaFree(ar.base);
+		return rc;
+	}
+	auto cleanup = [&](int code) {
+		cudaFree(ar.base);
+		cudaFree(d_lb);
+		return code;
+	};
+	std::vector<cc::LbInst> lbi(count);
+	cc::LbState s0;
+	std::memset(&s0, 0, sizeof(s0));
+	s0.E = INFINITY;
+	s0.gamma = 1.0;
+	s0.gtol = o.gtol;
+	s0.ftol = o.ftol;
+	s0.max_evals = o.max_evals;
+	s0.m = m;
+	s0.newslot = -1;
+	for (int i = 0; i < count; i++) {
+		const size_t n = (size_t)b->N[i] * b->h[i]->d;
+		cc::LbInst &l = lbi[i];
+		l.n = (int)n;
+		l.x = ar.at<double>(ox[i]);
+		l.g = ar.at<double>(og[i]);
+		l.d = ar.at<double>(od[i]);
+		l.xt = ar.at<double>(oxt[i]);
+		l.gt = ar.at<double>(ogt[i]);
+		l.S = ar.at<double>(oS[i]);
+		l.Y = ar.at<double>(oY[i]);
+		l.part = ar.at<double>(op[i]);
+		l.st = ar.at<cc::LbState>(ost[i]);
+		std::vector<double> x0(n);
+		for (size_t k = 0; k < n; k++) {
+			if (!std::isfinite(frac[i][k]))
+				return cleanup(fail(CC_ERR_ARG, "non-finite start"));
+			double v = frac[i][k] - std::floor(frac[i][k]);
+			x0[k] = v - std::floor(v);
+		}
+		CC_CUDA(cudaMemcpy(l.x, x0.data(), 8 * n, cudaMemcpyHostToDevice));
+		CC_CUDA(cudaMemcpy(l.xt, x0.data(), 8 * n, cudaMemcpyHostToDevice));
+		CC_CUDA(cudaMemset(l.g, 0, 8 * n));
+		CC_CUDA(cudaMemset(l.d, 0, 8 * n));
+		s0.stopval = o.stopval == CC_STOPVAL_GROUND_STATE ? 1e-20 * (double)b->N[i] : o.stopval;
+		CC_CUDA(cudaMemcpy(l.st, &s0, sizeof(s0), cudaMemcpyHostToDevice));
+	}
+	if ((rc = upload_into(d_lb, lbi)))
+		return cleanup(rc);
+	// minimisation descriptors: evaluate at x_trial into the L-BFGS buffers, skip finished instances
+	for (BatchGroup &g : b->groups) {
+		std::vector<cc::BInst> gi;
+		for (int i : g.members) {
+			cc::BInst in = b->inst[i];
+			in.frac = lbi[i].xt;
+			in.E_out = &lbi[i].st->Et;
+			in.gfrac_out = lbi[i].gt;
+			in.F_out = nullptr;
+			in.status = &lbi[i].st->status;
+			gi.push_back(in);
+		}
+		CC_CUDA(cudaMemcpy(g.d_inst_lb, gi.data(), sizeof(cc::BInst) * gi.size(), cudaMemcpyHostToDevice));
+	}
+	cudaStream_t st = b->stream;
+	const bool sched = o.precision == CC_PREC_SCHEDULE;
+	const int prec0 = o.precision == CC_PREC_FP64 ? CC_PREC_FP64 : CC_PREC_MIXED;
+	auto iteration = [&](int prec) -> int {
+		if (int r2 = batch_eval(b, true, prec, st))
+			return r2;
+		cc::lb_dots_kernel<<<dim3(nblk, count), cc::kLbThreads, 0, st>>>(d_lb, nblk);
+		cc::lb_solve_kernel<<<count, cc::kLbSolveThreads, 0, st>>>(d_lb, nblk);
+		cc::lb_update_kernel<<<dim3((maxn + cc::kLbThreads - 1) / cc::kLbThreads, count), cc::kLbThreads, 0, st>>>(d_lb);
+		CC_CUDA(cudaGetLastError());
+		return CC_OK;
+	};
+	auto make_graph = [&](int prec, cudaGraphExec_t *out) -> int {
+		cudaGraph_t g = nullptr;
+		CC_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+		int r2 = CC_OK;
+		for (int k = 0; k < o.iters_per_check && r2 == CC_OK; k++)
+			r2 = iteration(prec);
+		cudaError_t e = cudaStreamEndCapture(st, &g);
+		if (r2)
+			return r2;
+		if (e != cudaSuccess)
+			return fail(CC_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+		e = cudaGraphInstantiate(out, g, 0);
+		cudaGraphDestroy(g);
+		if (e != cudaSuccess)
+			return fail(CC_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+		return CC_OK;
+	};
+	cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+	auto destroy_graphs = [&]() {
+		for (auto &ge : gexec)
+			if (ge)
+				cudaGraphExecDestroy(ge);
+	};
+	// warm-up: make sure the cooperative kernels' occupancy is queried before capture
+	int tmp = 0;
+	for (BatchGroup &g : b->groups)
+		if ((rc = (prec0 == CC_PREC_MIXED ? (g.D == 1 ? batch_grid<1, true>(&tmp) : g.D == 2 ? batch_grid<2, true>(&tmp)
+		                                                                                       : batch_grid<3, true>(&tmp))
+		                                  : (g.D == 1 ? batch_grid<1, false>(&tmp) : g.D == 2 ? batch_grid<2, false>(&tmp)
+		                                                                                       : batch_grid<3, false>(&tmp)))) ||
+		    (sched && (rc = (g.D == 1 ? batch_grid<1, false>(&tmp) : g.D == 2 ? batch_grid<2, false>(&tmp)
+		                                                                      : batch_grid<3, false>(&tmp)))))
+			return cleanup(rc);
+	if ((rc = make_graph(prec0, &gexec[0])) || (sched && (rc = make_graph(CC_PREC_FP64, &gexec[1])))) {
+		destroy_graphs();
+		return cleanup(rc);
+	}
+	std::vector<cc::LbState> hs(count);
+	int stage = 0;
+	const int64_t max_rounds = o.max_evals / o.iters_per_check + 2;
+	for (int64_t round = 0; round < max_rounds; round++) {
+		cudaError_t e = cudaGraphLaunch(gexec[stage], st);
+		if (e == cudaSuccess)
+			e = cudaStreamSynchronize(st);
+		if (e != cudaSuccess) {
+			destroy_graphs();
+			return cleanup(fail(CC_ERR_CUDA, std::string("batch minimisation: ") + cudaGetErrorString(e)));
+		}
+		if ((rc = batch_check_barrier(b))) {
+			destroy_graphs();
+			return cleanup(rc);
+		}
+		bool running = false, all_low = true;
+		for (int i = 0; i < count; i++) {
+			CC_CUDA(cudaMemcpyAsync(&hs[i], lbi[i].st, offsetof(cc::LbState, w), cudaMemcpyDeviceToHost, st));
+		}
+		CC_CUDA(cudaStreamSynchronize(st));
+		for (int i = 0; i < count; i++) {
+			running |= hs[i].status == cc::kLbRunning;
+			if (hs[i].status == cc::kLbRunning && !(std::isfinite(hs[i].E) &&
+			                                         hs[i].E <= o.switch_energy_per_particle * (double)b->N[i]))
+				all_low = false;
+		}
+		if (!running)
+			break;
+		if (sched && stage == 0 && all_low)
+			stage = 1;
+	}
+	destroy_graphs();
+	// results: positions wrapped into [0,1), FP64 energies of the results (one batched evaluation)
+	std::vector<const double *> fr(count);
+	for (int i = 0; i < count; i++) {
+		const size_t n = (size_t)b->N[i] * b->h[i]->d;
+		CC_CUDA(cudaMemcpy(frac[i], lbi[i].x, 8 * n, cudaMemcpyDeviceToHost));
+		for (size_t k = 0; k < n; k++) {
+			double v = frac[i][k] - std::floor(frac[i][k]);
+			frac[i][k] = v - std::floor(v);
+		}
+		fr[i] = frac[i];
+	}
+	cleanup(CC_OK);
+	if ((rc = cc_batch_set_positions(b, fr.data())))
+		return rc;
+	std::vector<double> E(count);
+	if ((rc = cc_batch_energy_grad(b, E.data(), nullptr, CC_PREC_FP64)))
+		return rc;
+	if (results)
+		for (int i = 0; i < count; i++) {
+			results[i].E = E[i];
+			results[i].evals = hs[i].evals;
+			results[i].iters = hs[i].iters;
+			results[i].status = hs[i].status == cc::kLbRunning ? cc::kLbMaxEval : hs[i].status;
+		}
 	return CC_OK;
 }
 

@@ -61,7 +61,7 @@ struct LbInst {
 // products, so s'.y' and the history cross terms carry no cancellation.
 __host__ __device__ constexpr int lb_ndots(int m) { return 5 * m + 6; }
 
-__global__ void __launch_bounds__(kLbThreads) lb_dots_kernel(const LbInst *insts, int nblk)
+static __global__ void __launch_bounds__(kLbThreads) lb_dots_kernel(const LbInst *insts, int nblk)
 {
 	const LbInst in = insts[blockIdx.y];
 	const LbState *st = in.st;
@@ -143,7 +143,7 @@ constexpr int kLbSolveThreads = 256;
 // One block per instance: block totals of the dot products (parallel over the products, blocks summed in order),
 // accept / reject and the step length (thread 0), history matrices (parallel over slots), the triangular solves of
 // the compact form (warp 0, lanes split every inner sum), g.d of the new direction and the stop tests.
-__global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const LbInst *insts, int nblk)
+static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const LbInst *insts, int nblk)
 {
 	const LbInst in = insts[blockIdx.x];
 	LbState *st = in.st;
@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const LbInst 
 
 // accept: insert the pair, move x and g; then d = -(gamma g + S w1 + gamma Y w2) and x_trial = x + alpha d.
 // reject: x_trial = x + alpha d.
-__global__ void __launch_bounds__(kLbThreads) lb_update_kernel(const LbInst *insts)
+static __global__ void __launch_bounds__(kLbThreads) lb_update_kernel(const LbInst *insts)
 {
 	const LbInst in = insts[blockIdx.y];
 	const LbState *st = in.st;

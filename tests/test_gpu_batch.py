@@ -1,0 +1,63 @@
+"""Batches of uneven configurations in one launch per dimension: same results as each configuration alone."""
+import numpy as np
+import pytest
+
+from conftest import load_golden, scales
+
+pytestmark = pytest.mark.gpu
+
+
+def _instances(gpu, specs, seed=11):
+    rng = np.random.default_rng(seed)
+    pots, N, fracs = [], [], []
+    for d, n, chi, typ in specs:
+        basis = np.eye(d) * n ** (1.0 / d)
+        modes, V = gpu.stealthy_kset(d, basis, n, chi, typ)
+        pots.append(gpu.CCPotential(d, basis, modes, V))
+        N.append(n)
+        fracs.append(rng.random((n, d)))
+    return pots, N, fracs
+
+
+SPECS = [(2, 200, 0.3, 3), (3, 300, 0.12, 3), (2, 1000, 0.45, 3), (3, 700, 0.25, 3), (2, 64, 0.40, 0),
+         (3, 2000, 0.45, 0)]
+
+
+def test_batch_matches_each_instance(gpu):
+    pots, N, fracs = _instances(gpu, SPECS)
+    batch = gpu.CCBatch(pots, N)
+    batch.set_positions(fracs)
+    E, F = batch.energy_and_forces()
+    for p, f, e, fb in zip(pots, fracs, E, F):
+        p.set_configuration(f)
+        e1, f1 = p.energy_and_forces()
+        assert abs(e - e1) <= 1e-10 * abs(e1)
+        assert np.abs(fb - f1).max() <= 1e-10 * np.abs(f1).max()
+
+
+def test_batch_golden_parity(gpu):
+    """A batch of the golden cases (1D-3D, skew cells, repeated modes) against the reference's results."""
+    names = ["lattice_1d", "lattice_2d_skew", "lattice_3d_skew", "weighted_3d_n300", "stealthy_3d_n2000"]
+    recs = [load_golden(n) for n in names]
+    pots = [gpu.CCPotential(int(r["d"]), r["basis"], r["modes"], r["V"], float(r["shift"])) for r in recs]
+    batch = gpu.CCBatch(pots, [len(r["frac"]) for r in recs])
+    batch.set_positions([r["frac"] for r in recs])
+    E, F = batch.energy_and_forces()
+    for r, e, f in zip(recs, E, F):
+        s = scales(r)
+        assert abs(e - float(r["E"])) <= 1e-10 * abs(float(r["E"])) + 1e-13 * s["energy"]
+        assert np.abs(f - r["F"]).max() <= 1e-10 * s["force"]
+
+
+def test_batch_minimize_same_alone_and_in_mix(gpu):
+    """Continuous batching must not change results: an instance minimised in a mixed batch ends bitwise where it
+    ends when minimised alone, and every instance reaches its ground state (Phi/N < 1e-20)."""
+    pots, N, fracs = _instances(gpu, SPECS[:5], seed=3)
+    batch = gpu.CCBatch(pots, N)
+    xs, E, evals, iters, status = batch.minimize(fracs)
+    print("batch:", [f"{e / n:.1e}" for e, n in zip(E, N)], evals.tolist())
+    assert np.all(E / np.array(N) < 1e-20)
+    for k in (0, 3):
+        alone = gpu.CCBatch([pots[k]], [N[k]])
+        xa, Ea, ea, ia, sa = alone.minimize([fracs[k]])
+        assert np.array_equal(xa[0], xs[k]) and Ea[0] == E[k] and ea[0] == evals[k]
