@@ -35,6 +35,9 @@ D, N, CHI = 3, 2000, 0.45
 SIDE = N ** (1.0 / 3.0)
 METRIC = "CC energy+grad evals/s"
 UNIT = "evals/s"
+# DRAM bytes (read + write) per launch of the kernels on this workload, from one ncu capture
+# (profiles/cc_kernels_3d_n2000_ncu.md: dram__bytes_read.sum + dram__bytes_write.sum)
+NCU_TRAFFIC_BYTES = {"cc_force_kernel": 0.137e6, "cc_rho_kernel": 0.078e6, "cc_reduce_kernel": 2.163e6}
 WORKLOAD = "3D stealthy CC ground-state evaluation: N=2000 uniform in a periodic cube (unit density), chi=0.45, " \
            "M=2724 half-space k (v=1), FP64 energy + Cartesian forces"
 
@@ -49,6 +52,10 @@ def parse():
     ap.add_argument("--pool", type=int, default=3072, help="distinct configurations cycled through (> L2)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched / ground-state / served measurements")
+    ap.add_argument("--batch", type=int, default=512, help="instances of the batched uneven workload")
+    ap.add_argument("--gs-instances", type=int, default=48, help="instances of the ground-states/s comparison")
+    ap.add_argument("--served", type=int, default=300, help="requests of the served sample")
     return ap.parse_args()
 
 
@@ -139,6 +146,99 @@ def run_reference(args):
                              "sample": f"{n} evaluations (SetConfiguration+Energy+AllForce), {el:.1f} s"},
             "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def batched_workload(cc, count, seed=2024):
+    """512 independent stealthy configurations: d in {2,3}, N log-uniform in [200, 5000], chi U[0.10, 0.49],
+    v(k) = (1 - |k|/K)^2 (GeneratePotential Type 3), unit density, uniform random positions."""
+    rng = np.random.default_rng(seed)
+    pots, Ns, fracs, pairs = [], [], [], 0
+    for _ in range(count):
+        d = int(rng.choice([2, 3]))
+        n = int(round(np.exp(rng.uniform(np.log(200), np.log(5000)))))
+        chi = float(rng.uniform(0.10, 0.49))
+        basis = np.eye(d) * n ** (1.0 / d)
+        modes, V = cc.stealthy_kset(d, basis, n, chi, 3)
+        pots.append(cc.CCPotential(d, basis, modes, V))
+        Ns.append(n)
+        fracs.append(rng.random((n, d)))
+        pairs += n * len(V)
+    return pots, Ns, fracs, pairs
+
+
+def run_extras(args, cc, torch):
+    out = {}
+    # batched uneven instances: one batched energy+gradient step, CUDA-event timed, inputs resident
+    pots, Ns, fracs, pairs = batched_workload(cc, args.batch)
+    batch = cc.CCBatch(pots, Ns)
+    batch.set_positions(fracs)
+    st = torch.cuda.Stream()
+    with torch.cuda.stream(st):
+        for _ in range(3):
+            batch.eval_device(stream=st.cuda_stream)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 10
+    with torch.cuda.stream(st):
+        a.record(st)
+        for _ in range(reps):
+            batch.eval_device(stream=st.cuda_stream)
+        b.record(st)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    out["batched"] = {"workload": f"{args.batch} instances, d in {{2,3}}, N log-uniform [200,5000], chi U[0.10,0.49], "
+                                  "v=(1-|k|/K)^2, FP64", "ms_per_step": ms, "instance_evals_per_s": args.batch / (ms / 1e3),
+                      "pairs_per_s": pairs / (ms / 1e3), "launches_per_step": 2}
+    del batch
+    # ground states per second: the plain single-configuration FP64 path, one instance after another, against the
+    # batched minimisation of the same instances (mixed precision until E/N <= 1e-10, then FP64)
+    rng = np.random.default_rng(77)
+    gpots, gN, gfr = [], [], []
+    for _ in range(args.gs_instances):
+        d = int(rng.choice([2, 3]))
+        n = int(round(np.exp(rng.uniform(np.log(200), np.log(1000)))))
+        chi = float(rng.uniform(0.10, 0.40))
+        basis = np.eye(d) * n ** (1.0 / d)
+        modes, V = cc.stealthy_kset(d, basis, n, chi, 3)
+        gpots.append(cc.CCPotential(d, basis, modes, V))
+        gN.append(n)
+        gfr.append(rng.random((n, d)))
+    t0 = time.perf_counter()
+    plain_E = []
+    for p, f, n in zip(gpots, gfr, gN):
+        x, E, ev, it, stt = p.minimize(f, stopval=1e-20 * n)
+        plain_E.append(E / n)
+    t_plain = time.perf_counter() - t0
+    gb = cc.CCBatch(gpots, gN)
+    t0 = time.perf_counter()
+    xs, E, ev, it, stt = gb.minimize(gfr, precision=cc.PREC_SCHEDULE, switch_energy_per_particle=1e-10)
+    t_batch = time.perf_counter() - t0
+    epp = E / np.array(gN)
+    out["ground_states"] = {
+        "workload": f"{args.gs_instances} instances, d in {{2,3}}, N log-uniform [200,1000], chi U[0.10,0.40], "
+                    "v=(1-|k|/K)^2, to Phi/N < 1e-20",
+        "plain_fp64_per_s": args.gs_instances / t_plain, "batched_schedule_per_s": args.gs_instances / t_batch,
+        "speedup": t_plain / t_batch, "reached": int((epp < 1e-20).sum()),
+        "max_E_per_particle_batched": float(epp.max()), "max_E_per_particle_plain": float(max(plain_E))}
+    del gb
+    # served stream (a bounded sample of the 10000-request workload)
+    rng = np.random.default_rng(99)
+    reqs, t = [], 0.0
+    rate = 60.0
+    for _ in range(args.served):
+        t += rng.exponential(1.0 / rate)
+        d = int(rng.choice([2, 3]))
+        n = int(np.clip(np.exp(rng.normal(np.log(1000), 0.6)), 100, 4000))
+        chi = float(rng.uniform(0.05, 0.40))
+        reqs.append(dict(d=d, N=n, chi=chi, vtype=int(rng.choice([0, 3])), frac0=rng.random((n, d)), arrival_s=t))
+    res, wall = cc.serve(reqs, iters_per_round=16)
+    lat = np.array([r["t_done"] - q["arrival_s"] for r, q in zip(res, reqs)])
+    ok = np.array([r["E"] / q["N"] < 1e-20 for r, q in zip(res, reqs)])
+    out["served"] = {"workload": f"{args.served} requests, Poisson arrivals at {rate:.0f}/s, d in {{2,3}}, N log-normal "
+                                 "(median 1000, clipped to [100,4000]), chi U[0.05,0.40], v in {1,(1-|k|/K)^2}",
+                     "ground_states_per_s": len(reqs) / wall, "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                     "p99_ms": float(np.percentile(lat, 99) * 1e3), "reached": int(ok.sum()), "wall_s": wall}
+    return out
 
 
 def run_ours(args):
@@ -284,6 +384,12 @@ def run_ours(args):
                    "sample": f"unavailable: {exc}"}
 
     info = pot.plan_info(N)
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        try:
+            extras = run_extras(args, cc, torch)
+        except Exception as exc:   # extras are reports; never drop the headline line
+            extras = {"extras_error": str(exc)[:300]}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
                 "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -302,10 +408,12 @@ def run_ours(args):
                 "roofline": {"bound": "fp64_fma" if prec == cc.PREC_FP64 else "fp32_fma", "kernel": dom,
                              "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                              "peak_source": "measured in this run: FMA-chain probe kernel (cc_probe_fma_peak)",
-                             "flops_per_launch": fl, "launch_ms": tk, "traffic": None,
+                             "flops_per_launch": fl, "launch_ms": tk, "traffic": NCU_TRAFFIC_BYTES.get(dom),
+                             "traffic_unit": "bytes per launch (ncu capture)",
                              "kernel_ms": {"cc_rho_kernel": t_rho, "cc_reduce_kernel": t_red,
                                            "cc_force_kernel": t_force}},
                 "clocks": clk, "cpu_baseline": cpu}
+        line.update(extras)
         print(json.dumps(line), flush=True)
     del graphs
     if world > 1:

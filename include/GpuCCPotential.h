@@ -1,0 +1,170 @@
+/* GpuCCPotential.h — drop-in GPU replacement for the reference's ShiftedCCPotential (header-only C++ adapter).
+ *
+ * Include it in code built against the reference (it needs potential/CollectiveCoordinatePotential.h and
+ * potential/CombinedEnergyForce.h on the include path) and link libccgpu.so. The class derives from ShiftedCCPotential
+ * (potential/CollectiveCoordinatePotential.h:53-1497) and CombinedEnergyForce (potential/CombinedEnergyForce.h), so the
+ * structure optimiser's Objective (potential/StructureOptimization.cpp:447-536) finds EnergyAndAllForce by
+ * dynamic_cast and makes one GPU evaluation per step; MD/MC drivers call Energy / AllForce / Force as before.
+ *
+ * Contract kept from the reference:
+ *   - constraints / Shift are the public members of ShiftedCCPotential; a change is seen at the next evaluation;
+ *     every k must lie on the reciprocal lattice of the bound cell (std::invalid_argument otherwise);
+ *   - SetConfiguration binds a Configuration the caller keeps alive (non-owning), invalidating cached results;
+ *   - EnergyAndAllForce equals Energy() followed by AllForce() bitwise (both read one cached GPU evaluation);
+ *   - GetRho fills RhoReal / RhoImag and sets RhoValid;
+ *   - one object is not evaluated from several threads at once.
+ * Errors of the C ABI become std::invalid_argument (CC_ERR_ARG, CC_ERR_NONLATTICE), std::logic_error (CC_ERR_STATE)
+ * or std::runtime_error (the rest).
+ */
+#ifndef GPU_CC_POTENTIAL_H
+#define GPU_CC_POTENTIAL_H
+
+#include "CollectiveCoordinatePotential.h"
+#include "CombinedEnergyForce.h"
+#include "cc_gpu.h"
+
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+class GpuCCPotential : public ShiftedCCPotential, public CombinedEnergyForce
+{
+	cc_handle *handle_ = nullptr;
+	std::vector<double> kcopy_, vcopy_, basis_;   // the constraint set and cell the handle was built from
+	double shift_copy_ = 0.0;
+	std::vector<double> frac_, forces_;
+	double energy_ = 0.0;
+	bool positions_dirty_ = true, result_valid_ = false;
+	int precision_ = CC_PREC_FP64;
+
+	static void Check(int rc)
+	{
+		if (rc == CC_OK)
+			return;
+		const std::string msg = std::string("GpuCCPotential: ") + cc_last_error();
+		if (rc == CC_ERR_ARG || rc == CC_ERR_NONLATTICE)
+			throw std::invalid_argument(msg);
+		if (rc == CC_ERR_STATE)
+			throw std::logic_error(msg);
+		throw std::runtime_error(msg);
+	}
+
+	const Configuration &Bound() const { return *this->pConfig; }
+
+	// (Re)create the handle when the constraints, Shift or the cell changed; upload positions when dirty.
+	void Sync()
+	{
+		if (this->pConfig == nullptr)
+			throw std::logic_error("GpuCCPotential: no configuration bound");
+		const Configuration &c = Bound();
+		const int d = this->Dimension;
+		std::vector<double> basis(d * d), k, V;
+		for (int i = 0; i < d; i++)
+			for (int j = 0; j < d; j++)
+				basis[i * d + j] = c.GetBasisVector(i).x[j];
+		k.reserve(this->constraints.size() * d);
+		for (const auto &q : this->constraints) {
+			for (int j = 0; j < d; j++)
+				k.push_back(q.k.x[j]);
+			V.push_back(q.V);
+		}
+		if (!handle_ || k != kcopy_ || V != vcopy_ || basis != basis_ || this->Shift != shift_copy_) {
+			cc_destroy(handle_);
+			handle_ = nullptr;
+			Check(cc_create_cartesian(d, basis.data(), (int64_t)V.size(), k.data(), V.data(), this->Shift, &handle_));
+			kcopy_.swap(k);
+			vcopy_.swap(V);
+			basis_.swap(basis);
+			shift_copy_ = this->Shift;
+			positions_dirty_ = true;
+		}
+		if (positions_dirty_) {
+			const size_t n = c.NumParticle();
+			frac_.resize(n * d);
+			for (size_t i = 0; i < n; i++)
+				for (int j = 0; j < d; j++)
+					frac_[i * d + j] = c.GetRelativeCoordinates(i).x[j];
+			Check(cc_set_positions(handle_, (int64_t)n, frac_.data()));
+			positions_dirty_ = false;
+			result_valid_ = false;
+		}
+	}
+
+	void Evaluate()
+	{
+		Sync();
+		if (result_valid_)
+			return;
+		forces_.assign(frac_.size(), 0.0);
+		Check(cc_energy_grad(handle_, &energy_, forces_.empty() ? nullptr : forces_.data(), precision_));
+		result_valid_ = true;
+	}
+
+public:
+	explicit GpuCCPotential(DimensionType dimension) : ShiftedCCPotential(dimension) {}
+	explicit GpuCCPotential(const ShiftedCCPotential &src) : ShiftedCCPotential(src) {}
+	GpuCCPotential(const GpuCCPotential &) = delete;
+	GpuCCPotential &operator=(const GpuCCPotential &) = delete;
+	virtual ~GpuCCPotential() { cc_destroy(handle_); }
+
+	/* CC_PREC_FP64 (default, the reference's arithmetic to rounding) or CC_PREC_MIXED. */
+	void SetPrecision(int precision)
+	{
+		precision_ = precision;
+		result_valid_ = false;
+	}
+
+	virtual void SetConfiguration(const Configuration &Position)
+	{
+		ShiftedCCPotential::SetConfiguration(Position);
+		positions_dirty_ = true;
+		result_valid_ = false;
+	}
+
+	virtual void GetRho(void)
+	{
+		Sync();
+		const size_t M = this->constraints.size();
+		this->RhoReal.resize(M);
+		this->RhoImag.resize(M);
+		Check(cc_rho(handle_, this->RhoReal.data(), this->RhoImag.data(), precision_));
+		this->RhoValid = true;
+	}
+
+	virtual double Energy()
+	{
+		Evaluate();
+		return energy_;
+	}
+
+	virtual void AllForce(std::vector<GeometryVector> &results)
+	{
+		Evaluate();
+		const int d = this->Dimension;
+		const size_t n = frac_.size() / d;
+		results.assign(n, GeometryVector(d));
+		for (size_t i = 0; i < n; i++)
+			for (int j = 0; j < d; j++)
+				results[i].x[j] = forces_[i * d + j];
+	}
+
+	virtual void Force(GeometryVector &result, size_t i)
+	{
+		Evaluate();
+		const int d = this->Dimension;
+		if (i >= frac_.size() / d)
+			throw std::out_of_range("GpuCCPotential::Force: particle index out of range");
+		result = GeometryVector(d);
+		for (int j = 0; j < d; j++)
+			result.x[j] = forces_[i * d + j];
+	}
+
+	virtual double EnergyAndAllForce(std::vector<GeometryVector> &forces)
+	{
+		AllForce(forces);
+		return energy_;
+	}
+};
+
+#endif

@@ -147,6 +147,15 @@ int cc_batch_eval_device(cc_batch *b, int precision, void *stream);
 /* Minimise every instance from its bound positions; frac[i] (host) receives the results, results[i] the outcomes. */
 int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opts, cc_lbfgs_result *results);
 
+/* --- Monte Carlo moves ----------------------------------------------------------------------------------------------
+ * Replace ShiftedCCPotential_ForMC::TryMove / AcceptMove (potential/CollectiveCoordinatePotential.h:1906-1957): the
+ * energy change when one particle moves from s_prev to s_after (fractional coordinates, d doubles each), in O(M)
+ * from rho(k) of the bound positions, which the first call computes and AcceptMove then keeps current. The handle's
+ * bound positions are not changed (the caller moves its particle, as the reference's MC drivers do).
+ * AcceptMove without a pending trial returns CC_ERR_STATE. */
+int cc_mc_try_move(cc_handle *h, const double *s_prev, const double *s_after, double *dE);
+int cc_mc_accept_move(cc_handle *h);
+
 /* --- ground-state server with continuous batching (no counterpart in the reference) ------------------------------
  * Each request is a stealthy configuration in a periodic cube of unit density (side N^(1/d)): the CLI's k-set for
  * (d, N, chi) with weights vtype (0: v = 1, 3: v = (1 - |k|/K)^2, as cc_kset_stealthy), a start frac0 (N x d) and an
@@ -226,8 +235,9 @@ int cc_check_device_error(cc_handle *h);
 /* --- measurement support (no counterpart in the reference) --------------------------------------------------- */
 
 /* on = 1: every following evaluation on this handle records CUDA events around its rho, reduce and force kernels
- * (on the stream they run on); cc_get_timing synchronises and returns the summed kernel times in ms and the number
- * of evaluations timed since timing was switched on, then clears the record. */
+ * (on the stream they run on), also inside a stream capture (the events become graph nodes); cc_get_timing
+ * synchronises and returns the summed kernel times in ms and the number of evaluations timed since timing was
+ * switched on, then clears the record. Switching timing off keeps the record. */
 int cc_set_timing(cc_handle *h, int on);
 int cc_get_timing(cc_handle *h, double *rho_ms, double *reduce_ms, double *force_ms, int64_t *evals);
 

@@ -96,6 +96,8 @@ _SIGS = {
     "cc_serve": (_i, [ctypes.POINTER(ServeRequest), _i, ctypes.POINTER(ServeOpts), ctypes.POINTER(ServeResult),
                       ctypes.POINTER(_d)]),
     "cc_serve_last_error": (ctypes.c_char_p, []),
+    "cc_mc_try_move": (_i, [_vp, _vp, _vp, ctypes.POINTER(_d)]),
+    "cc_mc_accept_move": (_i, [_vp]),
     "cc_set_path": (_i, [_vp, _i]),
     "cc_check_device_error": (_i, [_vp]),
     "cc_energy_noalloc": (_i, [_i, _vp, _i64, _vp, _vp, _d, _i64, _vp, _vp, _vp, _vp]),
@@ -272,6 +274,21 @@ class CCPotential:
         _check(self._lib.cc_minimize(self._h, len(x), _ptr(x), ctypes.byref(o), ctypes.byref(r)))
         self.N = len(x)
         return x, r.E, r.evals, r.iters, r.status
+
+    def try_move(self, s_prev, s_after):
+        """Energy change of moving one particle from s_prev to s_after (fractional), as ForMC::TryMove."""
+        a = np.ascontiguousarray(s_prev, dtype=np.float64).reshape(self.d)
+        b = np.ascontiguousarray(s_after, dtype=np.float64).reshape(self.d)
+        dE = _d()
+        _check(self._lib.cc_mc_try_move(self._h, _ptr(a), _ptr(b), ctypes.byref(dE)))
+        return dE.value
+
+    TryMove = try_move
+
+    def accept_move(self):
+        _check(self._lib.cc_mc_accept_move(self._h))
+
+    AcceptMove = accept_move
 
     def set_path(self, path):
         """0 = the three-kernel split path (default), 1 = one fused cooperative kernel when the tables fit."""

@@ -23,6 +23,7 @@ struct BInst {
 	const double *frac;       // N x D
 	double *E_out, *gfrac_out, *F_out;   // outputs (F_out / gfrac_out may be null)
 	const int *status;        // skip the instance when *status != 0 (null: never)
+	const int *stage;         // skip the instance when *stage differs from the launch's stage (null: never)
 	int N, Npad;
 	const Seg *segs;
 	int ngroups, nseg, nslot;
@@ -62,7 +63,11 @@ __device__ __forceinline__ int batch_find(const int *pre, int B, int item)
 	return lo;
 }
 
-__device__ __forceinline__ bool batch_skip(const BInst &in) { return in.status && *(volatile const int *)in.status; }
+__device__ __forceinline__ bool batch_skip(const BInst &in, int launch_stage)
+{
+	return (in.status && *(volatile const int *)in.status) ||
+	       (in.stage && *(volatile const int *)in.stage != launch_stage);
+}
 
 template <int D, int L, bool MIXED>
 __global__ void __launch_bounds__(kFusedThreads, 2) cc_batch_kernel(BatchArgs a)
@@ -81,7 +86,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2) cc_batch_kernel(BatchArgs a)
 		for (int it = blockIdx.x; it < items; it += gridDim.x) {
 			const int b = batch_find(a.pre[0], a.B, it);
 			const BInst &in = a.inst[b];
-			if (batch_skip(in))
+			if (batch_skip(in, MIXED ? 0 : 1))
 				continue;
 			const TabSpec &sp = in.spec;
 			const int rowP = sp.row | 1;
@@ -122,7 +127,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2) cc_batch_kernel(BatchArgs a)
 		for (int it = blockIdx.x; it < items; it += gridDim.x) {
 			const int b = batch_find(a.pre[1], a.B, it);
 			const BInst &in = a.inst[b];
-			if (batch_skip(in))
+			if (batch_skip(in, MIXED ? 0 : 1))
 				continue;
 			const int local = it - a.pre[1][b];
 			const int group = local % in.ngroups, split = local / in.ngroups;
@@ -191,7 +196,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2) cc_batch_kernel(BatchArgs a)
 		for (int it = blockIdx.x; it < items; it += gridDim.x) {
 			const int b = batch_find(a.pre[2], a.B, it);
 			const BInst &in = a.inst[b];
-			if (batch_skip(in))
+			if (batch_skip(in, MIXED ? 0 : 1))
 				continue;
 			const int chunk = it - a.pre[2][b];
 			const int slot = chunk * kFusedThreads + threadIdx.x;
@@ -232,7 +237,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2) cc_batch_kernel(BatchArgs a)
 		for (int it = blockIdx.x; it < items; it += gridDim.x) {
 			const int b = batch_find(a.pre[3], a.B, it);
 			const BInst &in = a.inst[b];
-			if (batch_skip(in))
+			if (batch_skip(in, MIXED ? 0 : 1))
 				continue;
 			const int local = it - a.pre[3][b];
 			const int pgroups = (in.N + 31) / 32;

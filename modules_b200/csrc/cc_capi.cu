@@ -169,6 +169,12 @@ struct cc_handle {
 	size_t partialF_cap = 0;
 	std::vector<std::pair<int, int *> > kstarts;   // even segment splits per count
 	bool use_fused = false;         // cc_set_path
+	// Monte Carlo: rho in mode order of the bound positions, the trial rho and the device modes
+	int32_t *d_modes = nullptr;
+	double *d_modeV = nullptr;
+	double2 *d_rho_trial = nullptr, *d_rho_cur = nullptr;
+	double *d_mc_part = nullptr;
+	bool mc_valid = false, mc_pending = false;
 	const int *d_skip = nullptr;    // evaluations do nothing while *d_skip != 0 (set by cc_minimize)
 	bool timing = false;            // cc_set_timing
 	std::vector<cudaEvent_t> ev;    // 3 events per timed evaluation
@@ -195,6 +201,15 @@ int sm_count()
 			n = 148;
 	}
 	return n;
+}
+
+// Record a timing event; inside a stream capture it must be an external record node to carry a timestamp.
+cudaError_t record_timing(cudaEvent_t e, cudaStream_t st)
+{
+	cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+	if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusActive)
+		return cudaEventRecordWithFlags(e, st, cudaEventRecordExternal);
+	return cudaEventRecord(e, st);
 }
 
 constexpr size_t kRhoTabBudget = 48 * 1024;   // shared memory for one chunk of rho tables
@@ -434,7 +449,7 @@ int run_rho(cc_handle *h, DevKSet &k, int64_t N, const double *d_frac, double *d
 	if (int rc = launch_rho(h->d, a, mixed, p.nbgroups(), nsplit, csize, p.block_max_row, st))
 		return rc;
 	if (after_rho)
-		CC_CUDA(cudaEventRecord(after_rho, st));
+		CC_CUDA(record_timing(after_rho, st));
 	cc::ReduceArgs r;
 	r.partial = k.partial;
 	r.nsplit = rows;
@@ -770,28 +785,28 @@ int eval_device(cc_handle *h, int64_t N, const double *d_frac, double *d_E, doub
 		e3 = next_event(h);
 		if (!(e0 && e1 && e2 && e3))
 			return fail(CC_ERR_CUDA, "cudaEventCreate failed");
-		CC_CUDA(cudaEventRecord(e0, st));
+		CC_CUDA(record_timing(e0, st));
 	}
 	if (!want_rho_mode && h->use_fused && !h->d_skip && fused_eligible(h, N, mixed)) {
 		// one cooperative launch: the whole evaluation is reported as the force interval
 		if (e1)
-			CC_CUDA(cudaEventRecord(e1, st));
+			CC_CUDA(record_timing(e1, st));
 		if (e2)
-			CC_CUDA(cudaEventRecord(e2, st));
+			CC_CUDA(record_timing(e2, st));
 		int rc = run_fused(h, N, d_frac, d_E, d_F, d_gfrac, mixed, st);
 		if (e3)
-			CC_CUDA(cudaEventRecord(e3, st));
+			CC_CUDA(record_timing(e3, st));
 		return rc;
 	}
 	int rc = run_rho(h, h->main, N, d_frac, d_E, want_rho_mode, mixed, l, st, e1);
 	if (rc)
 		return rc;
 	if (e2)
-		CC_CUDA(cudaEventRecord(e2, st));
+		CC_CUDA(record_timing(e2, st));
 	if (d_F || d_gfrac)
 		rc = run_force(h, N, d_frac, d_F, d_gfrac, mixed, l, st);
 	if (e3)
-		CC_CUDA(cudaEventRecord(e3, st));
+		CC_CUDA(record_timing(e3, st));
 	return rc;
 }
 
@@ -888,6 +903,11 @@ int cc_destroy(cc_handle *h)
 	cudaFree(h->d_fcounters);
 	cudaFree(h->d_E);
 	cudaFreeHost(h->h_pin);
+	cudaFree(h->d_modes);
+	cudaFree(h->d_modeV);
+	cudaFree(h->d_rho_trial);
+	cudaFree(h->d_rho_cur);
+	cudaFree(h->d_mc_part);
 	cudaFree(h->d_tabP);
 	cudaFree(h->d_tabE);
 	cudaFree(h->d_bar);
@@ -953,6 +973,7 @@ int cc_set_positions(cc_handle *h, int64_t N, const double *frac)
 	}
 	h->N = N;
 	h->lastF_valid = false;
+	h->mc_valid = false;
 	return CC_OK;
 }
 
@@ -1132,6 +1153,67 @@ int cc_objective(cc_handle *h, int64_t N, const double *x, double rescale, doubl
 	return CC_OK;
 }
 
+int cc_mc_try_move(cc_handle *h, const double *s_prev, const double *s_after, double *dE)
+{
+	if (int rc = check_handle(h))
+		return rc;
+	if (!s_prev || !s_after || !dE)
+		return fail(CC_ERR_ARG, "null move arguments");
+	if (h->N < 0)
+		return fail(CC_ERR_STATE, "positions not set");
+	const int M = (int)h->V.size(), d = h->d;
+	for (int c = 0; c < d; c++)
+		if (!std::isfinite(s_prev[c]) || !std::isfinite(s_after[c]))
+			return fail(CC_ERR_ARG, "non-finite move");
+	h->mc_pending = false;
+	if (M == 0) {
+		*dE = 0.0;
+		return CC_OK;
+	}
+	const int nb = (M + cc::kMcThreads - 1) / cc::kMcThreads;
+	if (!h->d_modes) {
+		int rc;
+		if ((rc = upload(&h->d_modes, h->modes)) || (rc = upload(&h->d_modeV, h->V)) ||
+		    (rc = dev_alloc(&h->d_rho_trial, M)) || (rc = dev_alloc(&h->d_rho_cur, M)) ||
+		    (rc = dev_alloc(&h->d_mc_part, nb + 1)))
+			return rc;
+	}
+	if (!h->mc_valid) {
+		// rho of the bound positions in mode order (FP64), as the cached RhoReal / RhoImag of the reference
+		const Launch l = choose_launch(h->main.plan, h->N, false);
+		if (int rc = run_rho(h, h->main, h->N, h->d_frac, h->d_E, true, false, l, h->stream))
+			return rc;
+		CC_CUDA(cudaMemcpyAsync(h->d_rho_cur, h->main.rho_mode, sizeof(double2) * M, cudaMemcpyDeviceToDevice,
+		                        h->stream));
+		h->mc_valid = true;
+	}
+	double sp[3] = {0, 0, 0}, sa[3] = {0, 0, 0};
+	for (int c = 0; c < d; c++) {
+		sp[c] = s_prev[c];
+		sa[c] = s_after[c];
+	}
+	cc::cc_mc_kernel<<<nb, cc::kMcThreads, 0, h->stream>>>(h->d_modes, d, h->d_modeV, h->d_rho_cur, M, sp[0], sp[1],
+	                                                        sp[2], sa[0], sa[1], sa[2], h->d_rho_trial, h->d_mc_part);
+	cc::cc_mc_sum_kernel<<<1, 32, 0, h->stream>>>(h->d_mc_part, nb, 1.0 / h->volume, h->d_mc_part + nb);
+	CC_CUDA(cudaGetLastError());
+	CC_CUDA(cudaMemcpyAsync(h->h_pin, h->d_mc_part + nb, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+	CC_CUDA(cudaStreamSynchronize(h->stream));
+	*dE = h->h_pin[0];
+	h->mc_pending = true;
+	return CC_OK;
+}
+
+int cc_mc_accept_move(cc_handle *h)
+{
+	if (int rc = check_handle(h))
+		return rc;
+	if (!h->mc_pending)
+		return fail(CC_ERR_STATE, "no trial move to accept");
+	std::swap(h->d_rho_cur, h->d_rho_trial);
+	h->mc_pending = false;
+	return CC_OK;
+}
+
 int cc_set_path(cc_handle *h, int path)
 {
 	if (int rc = check_handle(h))
@@ -1155,7 +1237,8 @@ int cc_set_timing(cc_handle *h, int on)
 	if (int rc = check_handle(h))
 		return rc;
 	h->timing = on != 0;
-	h->ev_used = 0;
+	if (on)
+		h->ev_used = 0;   // switching on starts a new record; switching off keeps it for cc_get_timing
 	return CC_OK;
 }
 
@@ -1297,6 +1380,17 @@ int cc_minimize(cc_handle *h, int64_t N, double *frac, const cc_lbfgs_opts *opts
 		return fail(CC_ERR_ARG, "invalid minimisation arguments");
 	if ((int64_t)N * h->d > (1 << 30))
 		return fail(CC_ERR_ARG, "too many variables");
+	if (o.precision == CC_PREC_SCHEDULE && h->main.plan.nslot > 0) {
+		// the precision schedule is per instance: run it as a batch of one
+		cc_batch *bt = nullptr;
+		int rc2 = cc_batch_create(1, &h, &N, &bt);
+		if (rc2 == CC_OK)
+			rc2 = cc_batch_minimize(bt, &frac, &o, result);
+		cc_batch_destroy(bt);
+		if (rc2 == CC_OK)
+			rc2 = cc_set_positions(h, N, frac);
+		return rc2;
+	}
 	const int d = h->d, n = (int)(N * d), m = o.history;
 	const int nblk = std::max(1, std::min(148, n / 2048));
 	LbBuffers b;
@@ -1485,10 +1579,10 @@ int batch_launch(int D, bool mixed, cc::BatchArgs &a, cudaStream_t st)
 	}
 }
 
-// evaluate every group with the given descriptors (lb = the minimisation's)
+// evaluate every group with the given descriptors (lb = the minimisation's); precision CC_PREC_SCHEDULE launches
+// the mixed and the FP64 kernel, each evaluating the instances of its stage
 int batch_eval(cc_batch *b, bool lb, int precision, cudaStream_t st)
 {
-	const bool mixed = precision == CC_PREC_MIXED;
 	for (BatchGroup &g : b->groups) {
 		cc::BatchArgs a;
 		a.inst = lb ? g.d_inst_lb : g.d_inst;
@@ -1496,8 +1590,14 @@ int batch_eval(cc_batch *b, bool lb, int precision, cudaStream_t st)
 		for (int k = 0; k < 4; k++)
 			a.pre[k] = g.d_pre + k * (a.B + 1);
 		a.bar = b->d_bar;
-		if (int rc = batch_launch(g.D, mixed, a, st))
+		if (precision == CC_PREC_SCHEDULE) {
+			if (int rc = batch_launch(g.D, true, a, st))
+				return rc;
+			if (int rc = batch_launch(g.D, false, a, st))
+				return rc;
+		} else if (int rc = batch_launch(g.D, precision == CC_PREC_MIXED, a, st)) {
 			return rc;
+		}
 	}
 	return CC_OK;
 }
@@ -1776,6 +1876,9 @@ int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opt
 		CC_CUDA(cudaMemset(l.g, 0, 8 * n));
 		CC_CUDA(cudaMemset(l.d, 0, 8 * n));
 		s0.stopval = o.stopval == CC_STOPVAL_GROUND_STATE ? 1e-20 * (double)b->N[i] : o.stopval;
+		s0.sched = o.precision == CC_PREC_SCHEDULE;
+		s0.stage = o.precision == CC_PREC_FP64 ? 1 : 0;
+		s0.switch_E = o.switch_energy_per_particle * (double)b->N[i];
 		CC_CUDA(cudaMemcpy(l.st, &s0, sizeof(s0), cudaMemcpyHostToDevice));
 	}
 	if ((rc = upload_into(d_lb, lbi)))
@@ -1790,13 +1893,15 @@ int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opt
 			in.gfrac_out = lbi[i].gt;
 			in.F_out = nullptr;
 			in.status = &lbi[i].st->status;
+			in.stage = &lbi[i].st->stage;
 			gi.push_back(in);
 		}
 		CC_CUDA(cudaMemcpy(g.d_inst_lb, gi.data(), sizeof(cc::BInst) * gi.size(), cudaMemcpyHostToDevice));
 	}
 	cudaStream_t st = b->stream;
 	const bool sched = o.precision == CC_PREC_SCHEDULE;
-	const int prec0 = o.precision == CC_PREC_FP64 ? CC_PREC_FP64 : CC_PREC_MIXED;
+	// schedule: both kernels per iteration while some instance is in the mixed stage, then FP64 only
+	const int prec0 = o.precision;
 	auto iteration = [&](int prec) -> int {
 		if (int r2 = batch_eval(b, true, prec, st))
 			return r2;
@@ -1832,7 +1937,7 @@ int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opt
 	// warm-up: make sure the cooperative kernels' occupancy is queried before capture
 	int tmp = 0;
 	for (BatchGroup &g : b->groups)
-		if ((rc = (prec0 == CC_PREC_MIXED ? (g.D == 1 ? batch_grid<1, true>(&tmp) : g.D == 2 ? batch_grid<2, true>(&tmp)
+		if ((rc = (prec0 != CC_PREC_FP64 ? (g.D == 1 ? batch_grid<1, true>(&tmp) : g.D == 2 ? batch_grid<2, true>(&tmp)
 		                                                                                       : batch_grid<3, true>(&tmp))
 		                                  : (g.D == 1 ? batch_grid<1, false>(&tmp) : g.D == 2 ? batch_grid<2, false>(&tmp)
 		                                                                                       : batch_grid<3, false>(&tmp)))) ||
@@ -1858,20 +1963,18 @@ int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opt
 			destroy_graphs();
 			return cleanup(rc);
 		}
-		bool running = false, all_low = true;
+		bool running = false, any_mixed = false;
 		for (int i = 0; i < count; i++) {
 			CC_CUDA(cudaMemcpyAsync(&hs[i], lbi[i].st, offsetof(cc::LbState, w), cudaMemcpyDeviceToHost, st));
 		}
 		CC_CUDA(cudaStreamSynchronize(st));
 		for (int i = 0; i < count; i++) {
 			running |= hs[i].status == cc::kLbRunning;
-			if (hs[i].status == cc::kLbRunning && !(std::isfinite(hs[i].E) &&
-			                                         hs[i].E <= o.switch_energy_per_particle * (double)b->N[i]))
-				all_low = false;
+			any_mixed |= hs[i].status == cc::kLbRunning && hs[i].stage == 0;
 		}
 		if (!running)
 			break;
-		if (sched && stage == 0 && all_low)
+		if (sched && stage == 0 && !any_mixed)
 			stage = 1;
 	}
 	destroy_graphs();

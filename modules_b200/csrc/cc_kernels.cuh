@@ -640,4 +640,63 @@ __global__ void __launch_bounds__(kForceThreads, 2) cc_force_kernel(ForceArgs a)
 		a.counters[blockIdx.x] = 0u;
 }
 
+// ---------------------------------------------------------------------------------------------------------------
+// Monte Carlo trial move: one particle from s_prev to s_after (ShiftedCCPotential_ForMC::TryMove)
+// ---------------------------------------------------------------------------------------------------------------
+// rho'(k) = rho(k) - exp(i k.r_prev) + exp(i k.r_after); dE = sum_k V (|rho'|^2 - |rho|^2) / Volume, with the change
+// formed as 2 Re(conj(rho) delta) + |delta|^2 (no cancellation between two whole energies). Block partial sums in a
+// fixed order; cc_mc_sum_kernel adds the blocks in order.
+constexpr int kMcThreads = 256;
+
+static __global__ void __launch_bounds__(kMcThreads) cc_mc_kernel(const int32_t *__restrict__ modes, int D,
+                                                                  const double *__restrict__ V,
+                                                                  const double2 *__restrict__ rho, int M, double sp0,
+                                                                  double sp1, double sp2, double sa0, double sa1,
+                                                                  double sa2, double2 *__restrict__ rho_trial,
+                                                                  double *__restrict__ bpart)
+{
+	__shared__ double sh[kMcThreads / 32];
+	const int m = blockIdx.x * kMcThreads + threadIdx.x;
+	double e = 0.0;
+	if (m < M) {
+		const double sp[3] = {sp0, sp1, sp2}, sa[3] = {sa0, sa1, sa2};
+		double hp = 0, lp = 0, ha = 0, la = 0;
+		for (int c = 0; c < D; c++) {
+			const int n = modes[(size_t)m * D + c];
+			acc_phase(n, sp[c], hp, lp);
+			acc_phase(n, sa[c], ha, la);
+		}
+		double tp = __dadd_rn(hp, lp), ta = __dadd_rn(ha, la);
+		tp = __dsub_rn(tp, rint(tp));
+		ta = __dsub_rn(ta, rint(ta));
+		const double2 zp = expi2pi(tp), za = expi2pi(ta);
+		const double2 r = rho[m];
+		const double2 dl = make_double2(za.x - zp.x, za.y - zp.y);
+		rho_trial[m] = make_double2(r.x + dl.x, r.y + dl.y);
+		e = V[m] * (2.0 * (r.x * dl.x + r.y * dl.y) + dl.x * dl.x + dl.y * dl.y);
+	}
+	for (int o = 16; o > 0; o >>= 1)
+		e += __shfl_down_sync(0xffffffffu, e, o);
+	if ((threadIdx.x & 31) == 0)
+		sh[threadIdx.x >> 5] = e;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double t = 0.0;
+		for (int w = 0; w < kMcThreads / 32; w++)
+			t += sh[w];
+		bpart[blockIdx.x] = t;
+	}
+}
+
+static __global__ void cc_mc_sum_kernel(const double *__restrict__ bpart, int nb, double inv_vol, double *out)
+{
+	double t = 0.0;
+	for (int b = threadIdx.x; b < nb; b += 32)
+		t += bpart[b];
+	for (int o = 16; o > 0; o >>= 1)
+		t += __shfl_down_sync(0xffffffffu, t, o);
+	if (threadIdx.x == 0)
+		*out = t * inv_vol;
+}
+
 }  // namespace cc

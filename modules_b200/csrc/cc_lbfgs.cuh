@@ -40,6 +40,9 @@ struct LbState {
 	int m, count, head;     // history size, pairs stored, ring slot of the oldest pair
 	int status, accepted, rejects, small_steps;
 	int newslot;            // ring slot the update kernel fills with the accepted pair, or -1
+	int stage;              // precision stage of the evaluations: 0 mixed, 1 FP64
+	int sched;              // 1: mixed precision until switch_E (or a stall), then FP64
+	double switch_E;
 	double gmax;            // max |g| at x
 	double gg;              // g.g at x
 	double w[2 * kLbMaxHist];
@@ -185,6 +188,17 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 				st->status = kLbLineSearch;
 			else if (st->evals >= st->max_evals)
 				st->status = kLbMaxEval;
+			if (st->sched && st->stage == 0 && st->status == kLbLineSearch) {
+				// the mixed stage stalled at its noise floor: continue in FP64 from x with a fresh history
+				st->status = kLbRunning;
+				st->stage = 1;
+				st->count = 0;
+				st->head = 0;
+				st->E = INFINITY;
+				st->alpha = 0.0;
+				st->rejects = 0;
+				st->small_steps = 0;
+			}
 		} else {
 			st->accepted = 1;
 			st->rejects = 0;
@@ -206,7 +220,7 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 			st->E = Et;
 			st->gmax = gtmax;
 			st->gg = gtgt;
-			if (Et <= st->stopval)
+			if (Et <= st->stopval && !(st->sched && st->stage == 0))
 				st->status = kLbStopval;
 			else if (gtmax <= st->gtol)
 				st->status = kLbGtol;
@@ -214,6 +228,14 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 				st->status = kLbFtol;
 			else if (st->evals >= st->max_evals)
 				st->status = kLbMaxEval;
+			if (st->sched && st->stage == 0 &&
+			    (Et <= st->switch_E || st->status == kLbGtol || st->status == kLbFtol)) {
+				// switch to FP64: the accepted point is re-evaluated in FP64 as a fresh start (E = inf accepts it)
+				st->status = kLbRunning;
+				st->stage = 1;
+				st->small_steps = 0;
+				sh_accept = 2;
+			}
 		}
 	}
 	__syncthreads();
@@ -289,7 +311,16 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 			gdn += w1[a] * Sg[ia] - gam * t[a] * Yg[ia];
 		}
 		gdn = lb_warp_sum(gdn);
-		if (lane == 0) {
+		if (lane == 0 && sh_accept == 2) {
+			// stage switch: move to the accepted point (the update kernel does), drop the history, zero step
+			st->count = 0;
+			st->head = 0;
+			st->newslot = -1;
+			st->E = INFINITY;
+			st->gamma = 1.0;
+			st->gd = 0.0;
+			st->alpha = 0.0;
+		} else if (lane == 0) {
 			gdn = -(gam * gtgt + gdn);
 			int kk = k;
 			st->gamma = gam;

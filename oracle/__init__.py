@@ -60,6 +60,8 @@ def ref_lib():
         lib.ccref_structure_factor.argtypes = [_vp, _l, _vp, _vp]
         lib.ccref_minimize.restype = _d
         lib.ccref_minimize.argtypes = [_vp, _l, _vp, _d, _l, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_l)]
+        lib.ccref_mc_trymove.restype = _d
+        lib.ccref_mc_trymove.argtypes = [_vp, _vp, _vp, ctypes.c_int]
         lib.ccref_kset_cli.restype = _l
         lib.ccref_kset_cli.argtypes = [ctypes.c_int, _vp, _l, _d, ctypes.c_int, _l, _vp, _vp]
         _REF = lib
@@ -141,6 +143,11 @@ class Ref:
         S = np.zeros(max(len(kcart), 1))
         self.lib.ccref_structure_factor(self.h, len(kcart), _p(kcart), _p(S))
         return S[: len(kcart)]
+
+    def mc_try_move(self, s_prev, s_after, accept=False):
+        a = np.ascontiguousarray(s_prev, np.float64)
+        b = np.ascontiguousarray(s_after, np.float64)
+        return self.lib.ccref_mc_trymove(self.h, _p(a), _p(b), 1 if accept else 0)
 
     def minimize(self, frac, emin=-1.0, maxeval=5000, history=40, fast=0):
         x = np.ascontiguousarray(frac, np.float64).reshape(-1, self.d).copy()

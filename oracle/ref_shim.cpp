@@ -34,6 +34,7 @@ struct RefHandle {
 	std::vector<GeometryVector> basis;
 	std::unique_ptr<Configuration> config;
 	std::unique_ptr<ShiftedCCPotential> pot;
+	std::unique_ptr<ShiftedCCPotential_ForMC> mc;   // ccref_mc_trymove's MC object, created at its first call
 	int nthreads;
 };
 
@@ -224,6 +225,30 @@ void ccref_structure_factor(void *p, long K, const double *kcart, double *S)
 			rho += std::exp(std::complex<double>(0, k.Dot(h->config->GetCartesianCoordinates(i))));
 		S[q] = (rho.real() * rho.real() + rho.imag() * rho.imag()) / np;
 	}
+}
+
+// The reference's ShiftedCCPotential_ForMC::TryMove (:1931-1950) on the bound configuration, for a move of one
+// particle between two fractional positions (converted to Cartesian with the cell); accept = 1 also runs AcceptMove
+// and keeps the ForMC object for later calls (its rho then follows the accepted moves, as in an MC run).
+double ccref_mc_trymove(void *p, const double *s_prev, const double *s_after, int accept)
+{
+	RefHandle *h = static_cast<RefHandle *>(p);
+	std::unique_ptr<ShiftedCCPotential_ForMC> &mc = h->mc;
+	if (!mc) {
+		h->pot->SetConfiguration(*h->config);
+		mc.reset(new ShiftedCCPotential_ForMC(*h->pot));
+		mc->SetConfiguration(*h->config);
+		mc->GetRho();
+	}
+	GeometryVector a(h->d), b(h->d);
+	for (int i = 0; i < h->d; i++) {
+		a.AddFrom(s_prev[i] * h->basis[i]);
+		b.AddFrom(s_after[i] * h->basis[i]);
+	}
+	const double dE = mc->TryMove(a, b);
+	if (accept)
+		mc->AcceptMove();
+	return dE;
 }
 
 // Restated three-pass minimisation (RelaxStructure_NLOPT / _Emin, StructureOptimization.cpp:1046-1090) with the

@@ -61,3 +61,13 @@ def test_batch_minimize_same_alone_and_in_mix(gpu):
         alone = gpu.CCBatch([pots[k]], [N[k]])
         xa, Ea, ea, ia, sa = alone.minimize([fracs[k]])
         assert np.array_equal(xa[0], xs[k]) and Ea[0] == E[k] and ea[0] == evals[k]
+
+
+def test_batch_precision_schedule_reaches_ground_states(gpu):
+    """Mixed precision first, FP64 per instance once E/N <= 1e-10 or the mixed stage stalls: every instance ends
+    at Phi/N < 1e-20 (FP64 energy of the result)."""
+    pots, N, fracs = _instances(gpu, SPECS[:5], seed=8)
+    batch = gpu.CCBatch(pots, N)
+    xs, E, evals, iters, status = batch.minimize(fracs, precision=gpu.PREC_SCHEDULE, switch_energy_per_particle=1e-10)
+    print("schedule:", [f"{e / n:.1e}" for e, n in zip(E, N)], evals.tolist(), status.tolist())
+    assert np.all(E / np.array(N) < 1e-20)
