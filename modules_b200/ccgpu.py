@@ -214,7 +214,7 @@ class CCPotential:
 
     def energy_and_forces(self, precision=PREC_FP64, forces=True):
         E = _d()
-        F = np.zeros((max(self.N or 0, 1), self.d)) if forces else None
+        F = np.empty((max(self.N or 0, 1), self.d)) if forces else None
         _check(self._lib.cc_energy_grad(self._h, ctypes.byref(E), _ptr(F) if forces else None, precision))
         return (E.value, F[: self.N]) if forces else (E.value, None)
 

@@ -154,10 +154,14 @@ struct cc_handle {
 	size_t partialG_cap = 0;
 	unsigned *d_fcounters = nullptr;
 	double *d_E = nullptr;
-	double *h_pin = nullptr;        // pinned staging of N*d doubles (+1 for E)
+	double *h_pin = nullptr;        // pinned results: E at [0], N*d forces or gradients from [2]
 	size_t pin_cap = 0;
-	std::vector<double> lastF;      // forces of the last cc_energy_grad
-	bool lastF_valid = false;
+	double *h_in = nullptr;         // pinned staging of the wrapped positions (N*d)
+	size_t in_cap = 0;
+	cudaEvent_t ev_in = nullptr;    // recorded after the last copy out of h_in
+	bool in_pending = false;
+	bool lastF_valid = false;       // h_pin + 2 holds the forces of the bound positions
+	bool fused_ran = false;         // a fused launch ran since the barrier word was last read
 	// fused (cooperative) path
 	cc::TabSpec gspec;
 	void *d_tabP = nullptr, *d_tabE = nullptr;
@@ -383,12 +387,62 @@ int ensure_particles(cc_handle *h, int64_t N)
 		cudaFreeHost(h->h_pin);
 		h->h_pin = nullptr;
 		h->pin_cap = 0;
+		h->lastF_valid = false;
 		cudaError_t e = cudaMallocHost(reinterpret_cast<void **>(&h->h_pin), pin * sizeof(double));
 		if (e != cudaSuccess)
 			return fail(CC_ERR_OOM, std::string("cudaMallocHost: ") + cudaGetErrorString(e));
 		h->pin_cap = pin;
 	}
 	return CC_OK;
+}
+
+// Pinned input staging of n doubles, free for writing: the previous copy out of it has completed.
+int input_staging(cc_handle *h, size_t n)
+{
+	if (!h->ev_in)
+		CC_CUDA(cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming));
+	if (h->in_pending) {
+		CC_CUDA(cudaEventSynchronize(h->ev_in));
+		h->in_pending = false;
+	}
+	n = std::max<size_t>(n, 1);
+	if (n > h->in_cap) {
+		cudaFreeHost(h->h_in);
+		h->h_in = nullptr;
+		h->in_cap = 0;
+		cudaError_t e = cudaMallocHost(reinterpret_cast<void **>(&h->h_in), n * sizeof(double));
+		if (e != cudaSuccess)
+			return fail(CC_ERR_OOM, std::string("cudaMallocHost: ") + cudaGetErrorString(e));
+		h->in_cap = n;
+	}
+	return CC_OK;
+}
+
+// Copy n staged doubles to d_frac on the handle's stream; the staging is reusable once ev_in has passed.
+int upload_staged(cc_handle *h, size_t n)
+{
+	if (n == 0)
+		return CC_OK;
+	CC_CUDA(cudaMemcpyAsync(h->d_frac, h->h_in, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+	CC_CUDA(cudaEventRecord(h->ev_in, h->stream));
+	h->in_pending = true;
+	return CC_OK;
+}
+
+// Wrap into [0,1) as Configuration::Insert does (core/PeriodicCellList.h:517-538: floor twice). Values already in
+// [0,1) are returned unchanged, which is what the two floors give for them. Returns false on a non-finite value.
+inline bool wrap_unit(double x, double *out)
+{
+	if (x >= 0.0 && x < 1.0) {
+		*out = x;
+		return true;
+	}
+	if (!std::isfinite(x))
+		return false;
+	double s = x - std::floor(x);
+	s -= std::floor(s);
+	*out = s;
+	return true;
 }
 
 int ensure_partial(DevKSet &k, size_t elems)
@@ -681,8 +735,11 @@ int run_fused(cc_handle *h, int64_t N, const double *d_frac, double *d_E, double
 }
 
 // A grid barrier of an earlier fused launch that ran out of time leaves its error word set: report it and reset.
-int check_barrier(cc_handle *h)
+int check_barrier(cc_handle *h, bool always = false)
 {
+	if (!always && !h->fused_ran)
+		return CC_OK;
+	h->fused_ran = false;
 	unsigned w[3] = {0, 0, 0};
 	CC_CUDA(cudaMemcpy(w, h->d_bar, sizeof(w), cudaMemcpyDeviceToHost));
 	if (w[2] != 0u) {
@@ -794,6 +851,7 @@ int eval_device(cc_handle *h, int64_t N, const double *d_frac, double *d_E, doub
 		if (e2)
 			CC_CUDA(record_timing(e2, st));
 		int rc = run_fused(h, N, d_frac, d_E, d_F, d_gfrac, mixed, st);
+		h->fused_ran = true;
 		if (e3)
 			CC_CUDA(record_timing(e3, st));
 		return rc;
@@ -903,6 +961,9 @@ int cc_destroy(cc_handle *h)
 	cudaFree(h->d_fcounters);
 	cudaFree(h->d_E);
 	cudaFreeHost(h->h_pin);
+	cudaFreeHost(h->h_in);
+	if (h->ev_in)
+		cudaEventDestroy(h->ev_in);
 	cudaFree(h->d_modes);
 	cudaFree(h->d_modeV);
 	cudaFree(h->d_rho_trial);
@@ -958,19 +1019,14 @@ int cc_set_positions(cc_handle *h, int64_t N, const double *frac)
 	if (int rc = ensure_particles(h, N))
 		return rc;
 	const int d = h->d;
-	for (int64_t i = 0; i < N * d; i++) {
-		const double x = frac[i];
-		if (!std::isfinite(x))
+	if (int rc = input_staging(h, (size_t)N * d))
+		return rc;
+	double *in = h->h_in;
+	for (int64_t i = 0; i < N * d; i++)
+		if (!wrap_unit(frac[i], in + i))
 			return fail(CC_ERR_ARG, "non-finite fractional coordinate");
-		// wrap into [0,1) as Configuration::Insert does (floor twice)
-		double s = x - std::floor(x);
-		s -= std::floor(s);
-		h->h_pin[i] = s;
-	}
-	if (N > 0) {
-		CC_CUDA(cudaMemcpyAsync(h->d_frac, h->h_pin, sizeof(double) * N * d, cudaMemcpyHostToDevice, h->stream));
-		CC_CUDA(cudaStreamSynchronize(h->stream));
-	}
+	if (int rc = upload_staged(h, (size_t)N * d))
+		return rc;
 	h->N = N;
 	h->lastF_valid = false;
 	h->mc_valid = false;
@@ -993,13 +1049,13 @@ int cc_energy_grad(cc_handle *h, double *E, double *F, int precision)
 	CC_CUDA(cudaMemcpyAsync(h->h_pin, h->d_E, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
 	if (F && N > 0)
 		CC_CUDA(cudaMemcpyAsync(h->h_pin + 2, h->d_F, sizeof(double) * N * h->d, cudaMemcpyDeviceToHost, h->stream));
+	h->lastF_valid = false;
 	CC_CUDA(cudaStreamSynchronize(h->stream));
 	if (int rc = check_barrier(h))
 		return rc;
 	*E = h->h_pin[0];
 	if (F && N > 0) {
 		std::memcpy(F, h->h_pin + 2, sizeof(double) * N * h->d);
-		h->lastF.assign(F, F + N * h->d);
 		h->lastF_valid = true;
 	}
 	return CC_OK;
@@ -1063,7 +1119,7 @@ int cc_force_one(cc_handle *h, int64_t i, double *f)
 			return rc;
 	}
 	for (int e = 0; e < h->d; e++)
-		f[e] = h->lastF[(size_t)i * h->d + e];
+		f[e] = h->h_pin[2 + (size_t)i * h->d + e];
 	return CC_OK;
 }
 
@@ -1124,16 +1180,13 @@ int cc_objective(cc_handle *h, int64_t N, const double *x, double rescale, doubl
 	}
 	if (int rc = ensure_particles(h, N))
 		return rc;
-	for (int64_t i = 0; i < N * d; i++) {
-		if (!std::isfinite(x[i]))
+	if (int rc = input_staging(h, (size_t)N * d))
+		return rc;
+	for (int64_t i = 0; i < N * d; i++)
+		if (!std::isfinite(x[i]) || !wrap_unit(x[i] / rescale, h->h_in + i))
 			return fail(CC_ERR_ARG, "non-finite variable");
-		double s = x[i] / rescale;
-		s -= std::floor(s);
-		s -= std::floor(s);
-		h->h_pin[i] = s;
-	}
-	if (N > 0)
-		CC_CUDA(cudaMemcpyAsync(h->d_frac, h->h_pin, sizeof(double) * N * d, cudaMemcpyHostToDevice, h->stream));
+	if (int rc = upload_staged(h, (size_t)N * d))
+		return rc;
 	h->N = N;
 	h->lastF_valid = false;
 	if (int rc = eval_device(h, N, h->d_frac, h->d_E, nullptr, grad ? h->d_gfrac : nullptr, false, precision,
@@ -1229,7 +1282,7 @@ int cc_check_device_error(cc_handle *h)
 	if (int rc = check_handle(h))
 		return rc;
 	CC_CUDA(cudaDeviceSynchronize());
-	return check_barrier(h);
+	return check_barrier(h, true);
 }
 
 int cc_set_timing(cc_handle *h, int on)

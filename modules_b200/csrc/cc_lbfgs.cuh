@@ -154,7 +154,7 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 		return;
 	__shared__ double tot[5 * kLbMaxHist + 6];
 	__shared__ double Sg[kLbMaxHist], Yg[kLbMaxHist], t[kLbMaxHist], q[kLbMaxHist], w1[kLbMaxHist];
-	__shared__ int sh_accept, sh_newslot, sh_k;
+	__shared__ int sh_accept, sh_newslot;
 	const int m = st->m, nd = lb_ndots(m);
 	for (int k = threadIdx.x; k < nd; k += kLbSolveThreads) {
 		double v = in.part[k];
