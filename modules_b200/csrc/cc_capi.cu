@@ -18,6 +18,7 @@
 #include <cstddef>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -218,24 +219,75 @@ cudaError_t record_timing(cudaEvent_t e, cudaStream_t st)
 
 constexpr size_t kRhoTabBudget = 48 * 1024;   // shared memory for one chunk of rho tables
 
+template <typename C> size_t rho_smem(int row, int chunk, int L)
+{
+	return std::max((size_t)chunk * (row | 1) * sizeof(C), (size_t)cc::kRhoWarps * 32 * L * sizeof(double2));
+}
+template <typename C> size_t force_smem(int row, int d)
+{
+	return std::max((size_t)row * 32 * sizeof(C), (size_t)cc::kForceWarps * 32 * d * sizeof(double));
+}
+
+int rho_wave(int d, bool mixed, int csize, size_t smem);   // resident rho blocks (clusters of csize) on the device
+int force_wave(int d, bool mixed, size_t smem);            // resident force blocks on the device
+
+// Per-block fixed cost of each kernel (table build, barriers, split reduction) expressed in particle-k pairs of its
+// main loop, from block-level timelines of the 3D N=2000 and 2D N=20000 workloads on B200.
+constexpr double kRhoFixedPairs = 17000.0;
+constexpr double kForceFixedPairs = 4600.0;
+
+// Estimated time of `blocks` equal blocks sharing `pairs`, `wave` of them resident at once.
+double grid_cost(int64_t blocks, int wave, double pairs, double fixed_pairs)
+{
+	const int64_t waves = (blocks + wave - 1) / wave;
+	return (double)waves * (1.0 + pairs / (double)blocks / fixed_pairs);
+}
+
 Launch choose_launch(const cc::Plan &p, int64_t N, bool mixed)
 {
 	Launch l;
-	const int target = sm_count() * 4;   // resident 256-thread blocks
-	// rho: particle splits to fill the chip, at least 2 particles per block; clusters of up to 8 splits
-	const int ng = std::max(1, p.nbgroups());
-	int ns = std::max(1, (target + ng - 1) / ng);
-	ns = (int)std::min<int64_t>(ns, std::max<int64_t>(1, N / 2));
-	ns = std::min(ns, 4096);
-	l.csize = ns >= 8 ? 8 : ns >= 4 ? 4 : ns >= 2 ? 2 : 1;
-	ns = (ns + l.csize - 1) / l.csize * l.csize;
-	l.per_split = (int)std::max<int64_t>(1, (N + ns - 1) / ns);
-	l.nsplit = ns;
 	const size_t esz = mixed ? sizeof(float2) : sizeof(double2);
 	l.chunk = (int)std::max<size_t>(8, std::min<size_t>(64, kRhoTabBudget / (esz * std::max(1, p.block_max_row | 1))));
-	// force: split the segments when there are too few particle groups
+	const double pairs = (double)std::max<int64_t>(N, 1) * (double)std::max<int64_t>(p.real_segs, 1) * p.L;
+	// rho: particle splits (a multiple of the cluster size, at least 2 particles each) with the least estimated time
+	// over whole waves of resident blocks
+	const int ng = std::max(1, p.nbgroups());
+	const size_t rsm = mixed ? rho_smem<float2>(p.block_max_row, l.chunk, p.L)
+	                         : rho_smem<double2>(p.block_max_row, l.chunk, p.L);
+	const int maxns = (int)std::max<int64_t>(1, std::min<int64_t>(N / 2, 4096));
+	double best = 1e300;
+	l.csize = 1;
+	l.nsplit = 1;
+	for (int cs = 8; cs >= 1; cs >>= 1) {
+		const int wave = std::max(cs, rho_wave(p.d, mixed, cs, rsm));
+		for (int ns = cs; ns <= maxns; ns += cs) {
+			const double c = grid_cost((int64_t)ns * ng, wave, pairs, kRhoFixedPairs) * (cs == 8 ? 1.0 : 1.02);
+			if (c < best) {
+				best = c;
+				l.csize = cs;
+				l.nsplit = ns;
+			}
+			if ((int64_t)ns * ng > 4LL * wave)
+				break;
+		}
+	}
+	l.per_split = (int)std::max<int64_t>(1, (N + l.nsplit - 1) / l.nsplit);
+	// force: segment splits of every group of 32 particles, chosen the same way
 	const int64_t pg = std::max<int64_t>(1, (N + 31) / 32);
-	l.want_force = (int)std::max<int64_t>(1, std::min<int64_t>((target + pg - 1) / pg, 1024));
+	const size_t fsm = mixed ? force_smem<float2>(cc::kMaxRow, p.d) : force_smem<double2>(cc::kMaxRow, p.d);
+	const int fwave = std::max(1, force_wave(p.d, mixed, fsm));
+	const int maxnk = (int)std::max<int64_t>(1, std::min<int64_t>(p.real_segs, 1024));
+	best = 1e300;
+	l.want_force = 1;
+	for (int nk = 1; nk <= maxnk; nk++) {
+		const double c = grid_cost(pg * nk, fwave, pairs, kForceFixedPairs);
+		if (c < best) {
+			best = c;
+			l.want_force = nk;
+		}
+		if (pg * nk > 4LL * fwave)
+			break;
+	}
 	return l;
 }
 
@@ -259,26 +311,105 @@ cudaError_t launch_pdl(Kern kern, dim3 grid, dim3 block, size_t smem, cudaStream
 	cfg.numAttrs = 1;
 	return cudaLaunchKernelEx(&cfg, kern, a);
 }
-template <typename C> size_t rho_smem(int row, int chunk, int L)
+template <int D, int L, bool MIXED> cudaError_t rho_attr()
 {
-	return std::max((size_t)chunk * (row | 1) * sizeof(C), (size_t)cc::kRhoWarps * 32 * L * sizeof(double2));
+	typedef typename std::conditional<MIXED, float2, double2>::type C;
+	static cudaError_t e = cudaFuncSetAttribute(cc::cc_rho_kernel<D, L, MIXED>,
+	                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                                            (int)rho_smem<C>(cc::kMaxRow, 64, L));
+	return e;
 }
-template <typename C> size_t force_smem(int row, int d)
+template <int D, int L, bool MIXED> cudaError_t force_attr()
 {
-	return std::max((size_t)row * 32 * sizeof(C), (size_t)cc::kForceWarps * 32 * d * sizeof(double));
+	typedef typename std::conditional<MIXED, float2, double2>::type C;
+	static cudaError_t e = cudaFuncSetAttribute(cc::cc_force_kernel<D, L, MIXED>,
+	                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                                            (int)force_smem<C>(cc::kMaxRow, D));
+	return e;
 }
+
+// Resident blocks of one wave, from the occupancy calculator (cached per device, kernel, cluster size and smem).
+struct WaveKey {
+	int dev, kind, d, mixed, csize;
+	size_t smem;
+	bool operator==(const WaveKey &o) const
+	{
+		return dev == o.dev && kind == o.kind && d == o.d && mixed == o.mixed && csize == o.csize && smem == o.smem;
+	}
+};
+std::mutex g_wave_mu;
+std::vector<std::pair<WaveKey, int> > g_waves;
+
+template <int D, bool MIXED> int rho_wave_t(int csize, size_t smem)
+{
+	if (rho_attr<D, 8, MIXED>() != cudaSuccess)
+		return sm_count() * 3;
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = dim3(1, csize);
+	cfg.blockDim = dim3(cc::kRhoThreads);
+	cfg.dynamicSmemBytes = smem;
+	cudaLaunchAttribute at[1];
+	at[0].id = cudaLaunchAttributeClusterDimension;
+	at[0].val.clusterDim.x = 1;
+	at[0].val.clusterDim.y = csize;
+	at[0].val.clusterDim.z = 1;
+	cfg.attrs = at;
+	cfg.numAttrs = 1;
+	int n = 0;
+	if (cudaOccupancyMaxActiveClusters(&n, cc::cc_rho_kernel<D, 8, MIXED>, &cfg) != cudaSuccess || n <= 0) {
+		cudaGetLastError();
+		return sm_count() * 3;
+	}
+	return n * csize;
+}
+template <int D, bool MIXED> int force_wave_t(size_t smem)
+{
+	int n = 0;
+	if (force_attr<D, 8, MIXED>() != cudaSuccess ||
+	    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, cc::cc_force_kernel<D, 8, MIXED>, cc::kForceThreads, smem) !=
+	        cudaSuccess ||
+	    n <= 0) {
+		cudaGetLastError();
+		n = 2;
+	}
+	return n * sm_count();
+}
+
+int cached_wave(int kind, int d, bool mixed, int csize, size_t smem)
+{
+	int dev = 0;
+	cudaGetDevice(&dev);
+	const WaveKey k = {dev, kind, d, mixed ? 1 : 0, csize, smem};
+	{
+		std::lock_guard<std::mutex> g(g_wave_mu);
+		for (auto &e : g_waves)
+			if (e.first == k)
+				return e.second;
+	}
+	int w;
+	if (kind == 0)
+		w = d == 1 ? (mixed ? rho_wave_t<1, true>(csize, smem) : rho_wave_t<1, false>(csize, smem))
+		  : d == 2 ? (mixed ? rho_wave_t<2, true>(csize, smem) : rho_wave_t<2, false>(csize, smem))
+		           : (mixed ? rho_wave_t<3, true>(csize, smem) : rho_wave_t<3, false>(csize, smem));
+	else
+		w = d == 1 ? (mixed ? force_wave_t<1, true>(smem) : force_wave_t<1, false>(smem))
+		  : d == 2 ? (mixed ? force_wave_t<2, true>(smem) : force_wave_t<2, false>(smem))
+		           : (mixed ? force_wave_t<3, true>(smem) : force_wave_t<3, false>(smem));
+	std::lock_guard<std::mutex> g(g_wave_mu);
+	g_waves.push_back(std::make_pair(k, w));
+	return w;
+}
+
+int rho_wave(int d, bool mixed, int csize, size_t smem) { return cached_wave(0, d, mixed, csize, smem); }
+int force_wave(int d, bool mixed, size_t smem) { return cached_wave(1, d, mixed, 1, smem); }
 
 template <int D, int L, bool MIXED> int launch_rho_t(const cc::RhoArgs &a, int ngroups, int nsplit, int csize, int row,
                                                      cudaStream_t st)
 {
 	typedef typename std::conditional<MIXED, float2, double2>::type C;
 	auto kern = cc::cc_rho_kernel<D, L, MIXED>;
-	static bool attr = false;
-	if (!attr) {
-		CC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-		                             (int)rho_smem<C>(cc::kMaxRow, 64, L)));
-		attr = true;
-	}
+	if (cudaError_t e = rho_attr<D, L, MIXED>())
+		return fail(CC_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
 	cudaLaunchConfig_t cfg = {};
 	cfg.gridDim = dim3(ngroups, nsplit);
 	cfg.blockDim = dim3(cc::kRhoThreads);
@@ -301,12 +432,8 @@ template <int D, int L, bool MIXED> int launch_force_t(const cc::ForceArgs &a, i
 {
 	typedef typename std::conditional<MIXED, float2, double2>::type C;
 	auto kern = cc::cc_force_kernel<D, L, MIXED>;
-	static bool attr = false;
-	if (!attr) {
-		CC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-		                             (int)force_smem<C>(cc::kMaxRow, D)));
-		attr = true;
-	}
+	if (cudaError_t e = force_attr<D, L, MIXED>())
+		return fail(CC_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
 	CC_CUDA(launch_pdl(kern, dim3((unsigned)((N + 31) / 32), a.nksplit), dim3(cc::kForceThreads), force_smem<C>(row, D),
 	                   st, a));
 	return CC_OK;

@@ -87,6 +87,15 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 	return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
 
+// Three-term recurrence along a lattice line: z_{r+1} = c z_r - z_{r-1} with c = 2 cos(theta), for z_r = z_0 w^r and
+// w = exp(i theta) (z_{r+1} + z_{r-1} = (w + 1/w) z_r). Two FMAs per step instead of a complex product; the rounding
+// error of step r is amplified by at most |sin(r theta) / sin(theta)| <= r, so a line of L slots stays within
+// ~L^2/2 ulps.
+__device__ __forceinline__ double2 cheb_next(double c, double2 q, double2 p)
+{
+	return make_double2(fma(c, q.x, -p.x), fma(c, q.y, -p.y));
+}
+
 // exp(2 pi i t): (cos, sin)
 __device__ __forceinline__ double2 expi2pi(double t)
 {
@@ -301,17 +310,31 @@ __global__ void __launch_bounds__(kRhoThreads, 3) cc_rho_kernel(RhoArgs a)
 			const C *r0 = tab + i * row, *r1 = r0 + row;
 			C z0 = seed_from<D, C>(r0, 1, ix), z1 = seed_from<D, C>(r1, 1, ix);
 			const C w0 = r0[ix.w], w1 = r1[ix.w];
+			if constexpr (MIXED) {
 #pragma unroll
-			for (int r = 0; r < L; r++) {
-				if (MIXED) {
+				for (int r = 0; r < L; r++) {
 					accf[r].x += z0.x + z1.x;
 					accf[r].y += z0.y + z1.y;
-				} else {
-					acc[r].x += (double)z0.x + (double)z1.x;
-					acc[r].y += (double)z0.y + (double)z1.y;
+					z0 = cmul(z0, w0);
+					z1 = cmul(z1, w1);
 				}
-				z0 = cmul(z0, w0);
-				z1 = cmul(z1, w1);
+			} else {
+				const double c0 = 2.0 * w0.x, c1 = 2.0 * w1.x;
+				double2 p0 = z0, p1 = z1, q0 = cmul(z0, w0), q1 = cmul(z1, w1);
+				acc[0].x += p0.x + p1.x;
+				acc[0].y += p0.y + p1.y;
+				acc[1].x += q0.x + q1.x;
+				acc[1].y += q0.y + q1.y;
+#pragma unroll
+				for (int r = 2; r < L; r++) {
+					const double2 n0 = cheb_next(c0, q0, p0), n1 = cheb_next(c1, q1, p1);
+					acc[r].x += n0.x + n1.x;
+					acc[r].y += n0.y + n1.y;
+					p0 = q0;
+					q0 = n0;
+					p1 = q1;
+					q1 = n1;
+				}
 			}
 			if (MIXED && (since_flush += 2) >= SUB) {
 				since_flush = 0;
@@ -328,16 +351,28 @@ __global__ void __launch_bounds__(kRhoThreads, 3) cc_rho_kernel(RhoArgs a)
 			const C *r0 = tab + i * row;
 			C z0 = seed_from<D, C>(r0, 1, ix);
 			const C w0 = r0[ix.w];
+			if constexpr (MIXED) {
 #pragma unroll
-			for (int r = 0; r < L; r++) {
-				if (MIXED) {
+				for (int r = 0; r < L; r++) {
 					accf[r].x += z0.x;
 					accf[r].y += z0.y;
-				} else {
-					acc[r].x += (double)z0.x;
-					acc[r].y += (double)z0.y;
+					z0 = cmul(z0, w0);
 				}
-				z0 = cmul(z0, w0);
+			} else {
+				const double c0 = 2.0 * w0.x;
+				double2 p0 = z0, q0 = cmul(z0, w0);
+				acc[0].x += p0.x;
+				acc[0].y += p0.y;
+				acc[1].x += q0.x;
+				acc[1].y += q0.y;
+#pragma unroll
+				for (int r = 2; r < L; r++) {
+					const double2 n0 = cheb_next(c0, q0, p0);
+					acc[r].x += n0.x;
+					acc[r].y += n0.y;
+					p0 = q0;
+					q0 = n0;
+				}
 			}
 		}
 	}
@@ -536,11 +571,13 @@ __global__ void __launch_bounds__(kForceThreads, 2) cc_force_kernel(ForceArgs a)
 	const int q0 = a.kstart[ks], q1 = a.kstart[ks + 1];
 	if (threadIdx.x == 0)
 		sp = a.kspec[ks];
-	cudaGridDependencySynchronize();   // u of this step is complete
-	if (a.skip && *a.skip)
-		return;
 	__syncthreads();
+	// The tables need only the positions, which the rho pass of this evaluation has already read: they are built
+	// while the reduce kernel still runs (programmatic dependent launch), before waiting for u.
 	build_tables<D, C>(sp, a.frac, pbase, 32, nvalid, tab, 1, 32, threadIdx.x, kForceThreads);
+	cudaGridDependencySynchronize();   // u of this step is complete
+	if (a.skip && *a.skip)             // uniform over the grid
+		return;
 	__syncthreads();
 
 	double g[D];
@@ -576,12 +613,32 @@ __global__ void __launch_bounds__(kForceThreads, 2) cc_force_kernel(ForceArgs a)
 		C z = seed_from<D, C>(tab + lane, 32, ix);
 		const C w = tab[ix.w * 32 + lane];
 		R S0 = 0, S1 = 0;
+		if constexpr (MIXED) {
 #pragma unroll
-		for (int r = 0; r < L; r++) {
-			const R t = uu[r].x * z.y + uu[r].y * z.x;
-			S0 += t;
-			S1 = fma((R)r, t, S1);
-			z = cmul(z, w);
+			for (int r = 0; r < L; r++) {
+				const R t = uu[r].x * z.y + uu[r].y * z.x;
+				S0 += t;
+				S1 = fma((R)r, t, S1);
+				z = cmul(z, w);
+			}
+		} else {
+			const double c = 2.0 * w.x;
+			double2 p = z, q = cmul(z, w);
+			S0 = uu[0].x * p.y + uu[0].y * p.x;
+			{
+				const double t = uu[1].x * q.y + uu[1].y * q.x;
+				S0 += t;
+				S1 = t;
+			}
+#pragma unroll
+			for (int r = 2; r < L; r++) {
+				const double2 n = cheb_next(c, q, p);
+				const double t = uu[r].x * n.y + uu[r].y * n.x;
+				S0 += t;
+				S1 = fma((double)r, t, S1);
+				p = q;
+				q = n;
+			}
 		}
 		const double S0d = (double)S0;
 		if (D >= 2)
