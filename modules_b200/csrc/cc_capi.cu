@@ -223,10 +223,7 @@ template <typename C> size_t rho_smem(int row, int chunk, int L)
 {
 	return std::max((size_t)chunk * (row | 1) * sizeof(C), (size_t)cc::kRhoWarps * 32 * L * sizeof(double2));
 }
-template <typename C> size_t force_smem(int row, int d)
-{
-	return std::max((size_t)row * 32 * sizeof(C), (size_t)cc::kForceWarps * 32 * d * sizeof(double));
-}
+template <typename C> size_t force_smem(int row, int d) { return cc::force_smem_bytes<C>(row, d, 8); }
 
 int rho_wave(int d, bool mixed, int csize, size_t smem);   // resident rho blocks (clusters of csize) on the device
 int force_wave(int d, bool mixed, size_t smem);            // resident force blocks on the device
@@ -274,7 +271,8 @@ Launch choose_launch(const cc::Plan &p, int64_t N, bool mixed)
 	l.per_split = (int)std::max<int64_t>(1, (N + l.nsplit - 1) / l.nsplit);
 	// force: segment splits of every group of 32 particles, chosen the same way
 	const int64_t pg = std::max<int64_t>(1, (N + 31) / 32);
-	const size_t fsm = mixed ? force_smem<float2>(cc::kMaxRow, p.d) : force_smem<double2>(cc::kMaxRow, p.d);
+	// (the tables of a split usually stay within 64 entries per particle)
+	const size_t fsm = mixed ? force_smem<float2>(64, p.d) : force_smem<double2>(64, p.d);
 	const int fwave = std::max(1, force_wave(p.d, mixed, fsm));
 	const int maxnk = (int)std::max<int64_t>(1, std::min<int64_t>(p.real_segs, 1024));
 	best = 1e300;

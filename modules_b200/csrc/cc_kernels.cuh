@@ -550,17 +550,32 @@ __device__ __forceinline__ void write_force(const ForceArgs &a, int j, const dou
 	write_force_out<D>(a.F_out, a.gfrac_out, a.recip, a.fscale, j, g);
 }
 
+constexpr int kForceUChunk = 128;   // segments whose slot weights are staged in shared memory at once
+
+// Dynamic shared memory of the force kernel for tables of `row` entries: the staged weights, then the tables; the
+// per-warp sums reuse it after the loop.
+template <typename C> __host__ __device__ constexpr size_t force_smem_bytes(int row, int d, int L)
+{
+	return ((size_t)L * kForceUChunk + (size_t)row * 32) * sizeof(C) > (size_t)kForceWarps * 32 * d * sizeof(double)
+	           ? ((size_t)L * kForceUChunk + (size_t)row * 32) * sizeof(C)
+	           : (size_t)kForceWarps * 32 * d * sizeof(double);
+}
+
 // Grid (ceil(N/32), nksplit). Block = 32 particles (lanes) x 8 warps striding over the split's segments; the tables of
-// the block's particles for the split are built once (entry-major, so a warp reads 32 consecutive entries).
+// the block's particles for the split are built once (entry-major, so a warp reads 32 consecutive entries). The slot
+// weights u of up to kForceUChunk segments at a time are staged in shared memory in the compute type (slot-major, so a
+// warp's read of one weight is a broadcast).
 template <int D, int L, bool MIXED>
-__global__ void __launch_bounds__(kForceThreads, 2) cc_force_kernel(ForceArgs a)
+__global__ void __launch_bounds__(kForceThreads, 3) cc_force_kernel(ForceArgs a)
 {
 	typedef typename std::conditional<MIXED, float, double>::type R;
 	typedef typename std::conditional<MIXED, float2, double2>::type C;
 	extern __shared__ __align__(16) unsigned char smem[];
-	C *tab = reinterpret_cast<C *>(smem);            // row x 32, entry-major
+	C *sh_u = reinterpret_cast<C *>(smem);           // L x kForceUChunk, slot-major
+	C *tab = sh_u + L * kForceUChunk;                // row x 32, entry-major
 	double *sh_g = reinterpret_cast<double *>(smem); // reused after the loop: kForceWarps x 32 x D
 	__shared__ TabSpec sp;
+	__shared__ Seg sh_seg[kForceUChunk];
 	__shared__ int sh_last;
 
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -578,74 +593,67 @@ __global__ void __launch_bounds__(kForceThreads, 2) cc_force_kernel(ForceArgs a)
 	cudaGridDependencySynchronize();   // u of this step is complete
 	if (a.skip && *a.skip)             // uniform over the grid
 		return;
-	__syncthreads();
 
 	double g[D];
 #pragma unroll
 	for (int e = 0; e < D; e++)
 		g[e] = 0.0;
-	// software pipeline: the next segment's descriptor and weights are loaded while this one is computed
-	int q = q0 + warp;
-	Seg nsg = {0, 0, 0, 0};
-	double2 nu[L];
-	if (q < q1) {
-		nsg = a.segs[q];
-#pragma unroll
-		for (int r = 0; r < L; r++)
-			nu[r] = __ldg(a.u_slot + q + (size_t)r * a.nseg);
-	}
-	for (; q < q1; q += kForceWarps) {
-		const Seg sgm = nsg;
-		C uu[L];
-#pragma unroll
-		for (int r = 0; r < L; r++)
-			uu[r] = to_c<C>(nu[r]);
-		const int qn = q + kForceWarps;
-		if (qn < q1) {
-			nsg = a.segs[qn];
-#pragma unroll
-			for (int r = 0; r < L; r++)
-				nu[r] = __ldg(a.u_slot + qn + (size_t)r * a.nseg);
+	for (int c0 = q0; c0 < q1; c0 += kForceUChunk) {
+		const int nq = min(kForceUChunk, q1 - c0);
+		__syncthreads();   // tables complete (first chunk); the previous chunk's weights are no longer read
+		for (int e = threadIdx.x; e < nq * L; e += kForceThreads) {
+			const int r = e / nq, qq = e - r * nq;
+			sh_u[r * kForceUChunk + qq] = to_c<C>(a.u_slot[(size_t)r * a.nseg + c0 + qq]);
 		}
-		if (sgm.len == 0)   // padding segment of a rho group: weight 0, no table entries
-			continue;
-		const SeedIdx ix = seed_index<D>(sp, sgm);
-		C z = seed_from<D, C>(tab + lane, 32, ix);
-		const C w = tab[ix.w * 32 + lane];
-		R S0 = 0, S1 = 0;
-		if constexpr (MIXED) {
+		for (int e = threadIdx.x; e < nq; e += kForceThreads)
+			sh_seg[e] = a.segs[c0 + e];
+		__syncthreads();
+		for (int qq = warp; qq < nq; qq += kForceWarps) {
+			const Seg sgm = sh_seg[qq];
+			if (sgm.len == 0)   // padding segment of a rho group: weight 0, no table entries
+				continue;
+			const C *uu = sh_u + qq;
+			const SeedIdx ix = seed_index<D>(sp, sgm);
+			C z = seed_from<D, C>(tab + lane, 32, ix);
+			const C w = tab[ix.w * 32 + lane];
+			R S0 = 0, S1 = 0;
+			if constexpr (MIXED) {
 #pragma unroll
-			for (int r = 0; r < L; r++) {
-				const R t = uu[r].x * z.y + uu[r].y * z.x;
-				S0 += t;
-				S1 = fma((R)r, t, S1);
-				z = cmul(z, w);
-			}
-		} else {
-			const double c = 2.0 * w.x;
-			double2 p = z, q = cmul(z, w);
-			S0 = uu[0].x * p.y + uu[0].y * p.x;
-			{
-				const double t = uu[1].x * q.y + uu[1].y * q.x;
-				S0 += t;
-				S1 = t;
-			}
+				for (int r = 0; r < L; r++) {
+					const C u = uu[r * kForceUChunk];
+					const R t = u.x * z.y + u.y * z.x;
+					S0 += t;
+					S1 = fma((R)r, t, S1);
+					z = cmul(z, w);
+				}
+			} else {
+				const double c = 2.0 * w.x;
+				double2 p = z, q = cmul(z, w);
+				const double2 u0 = uu[0], u1 = uu[kForceUChunk];
+				S0 = u0.x * p.y + u0.y * p.x;
+				{
+					const double t = u1.x * q.y + u1.y * q.x;
+					S0 += t;
+					S1 = t;
+				}
 #pragma unroll
-			for (int r = 2; r < L; r++) {
-				const double2 n = cheb_next(c, q, p);
-				const double t = uu[r].x * n.y + uu[r].y * n.x;
-				S0 += t;
-				S1 = fma((double)r, t, S1);
-				p = q;
-				q = n;
+				for (int r = 2; r < L; r++) {
+					const double2 n = cheb_next(c, q, p);
+					const double2 u = uu[r * kForceUChunk];
+					const double t = u.x * n.y + u.y * n.x;
+					S0 += t;
+					S1 = fma((double)r, t, S1);
+					p = q;
+					q = n;
+				}
 			}
+			const double S0d = (double)S0;
+			if (D >= 2)
+				g[0] = fma(S0d, (double)sgm.p0, g[0]);
+			if (D >= 3)
+				g[1] = fma(S0d, (double)sgm.p1, g[1]);
+			g[D - 1] = fma(S0d, (double)sgm.start, g[D - 1] + (double)S1);
 		}
-		const double S0d = (double)S0;
-		if (D >= 2)
-			g[0] = fma(S0d, (double)sgm.p0, g[0]);
-		if (D >= 3)
-			g[1] = fma(S0d, (double)sgm.p1, g[1]);
-		g[D - 1] = fma(S0d, (double)sgm.start, g[D - 1] + (double)S1);
 	}
 
 	cudaTriggerProgrammaticLaunchCompletion();
