@@ -258,7 +258,8 @@ Launch choose_launch(const cc::Plan &p, int64_t N, bool mixed)
 	for (int cs = 8; cs >= 1; cs >>= 1) {
 		const int wave = std::max(cs, rho_wave(p.d, mixed, cs, rsm));
 		for (int ns = cs; ns <= maxns; ns += cs) {
-			const double c = grid_cost((int64_t)ns * ng, wave, pairs, kRhoFixedPairs) * (cs == 8 ? 1.0 : 1.02);
+			// smaller clusters leave more partial rows to the reduce kernel
+			const double c = grid_cost((int64_t)ns * ng, wave, pairs, kRhoFixedPairs) * (cs == 8 ? 1.0 : 1.15);
 			if (c < best) {
 				best = c;
 				l.csize = cs;
@@ -599,8 +600,9 @@ int ensure_partialG(cc_handle *h, size_t elems)
 }
 
 // rho pass of k-set `k` over N device positions: rho per slot, u, and the energy into d_E.
+// energy_in_force: a force pass follows and sums the energy partials (one reduce-block ticket less on the path).
 int run_rho(cc_handle *h, DevKSet &k, int64_t N, const double *d_frac, double *d_E, bool want_rho_mode, bool mixed,
-            const Launch &l, cudaStream_t st, cudaEvent_t after_rho = nullptr)
+            const Launch &l, cudaStream_t st, cudaEvent_t after_rho = nullptr, bool energy_in_force = false)
 {
 	const cc::Plan &p = k.plan;
 	if (p.nslot == 0) {
@@ -642,6 +644,7 @@ int run_rho(cc_handle *h, DevKSet &k, int64_t N, const double *d_frac, double *d
 	r.inv_vol = 1.0 / h->volume;
 	r.shift = h->shift;
 	r.E_out = d_E;
+	r.finalize = energy_in_force ? 0 : 1;
 	r.skip = h->d_skip;
 	CC_CUDA(launch_pdl(cc::cc_reduce_kernel, dim3((p.nslot + 31) / 32), dim3(cc::kRedThreads), 0, st, r));
 	if (want_rho_mode && !p.mode_slot.empty()) {
@@ -652,8 +655,9 @@ int run_rho(cc_handle *h, DevKSet &k, int64_t N, const double *d_frac, double *d
 	return CC_OK;
 }
 
+// d_E: when not null, the force kernel also writes the energy (run_rho was called with energy_in_force).
 int run_force(cc_handle *h, int64_t N, const double *d_frac, double *d_F, double *d_gfrac, bool mixed,
-              const Launch &l, cudaStream_t st)
+              const Launch &l, cudaStream_t st, double *d_E = nullptr)
 {
 	const cc::Plan &p = h->main.plan;
 	if (N == 0)
@@ -690,6 +694,11 @@ int run_force(cc_handle *h, int64_t N, const double *d_frac, double *d_F, double
 	a.fscale = 2.0 / h->volume;
 	a.F_out = d_F;
 	a.gfrac_out = d_gfrac;
+	a.eblock = h->main.eblock;
+	a.neblock = (p.nslot + 31) / 32;   // the reduce kernel's grid
+	a.inv_vol = 1.0 / h->volume;
+	a.shift = h->shift;
+	a.E_out = d_E;
 	a.skip = h->d_skip;
 	return launch_force(h->d, a, mixed, N, f->host.max_row, st);
 }
@@ -981,13 +990,15 @@ int eval_device(cc_handle *h, int64_t N, const double *d_frac, double *d_E, doub
 			CC_CUDA(record_timing(e3, st));
 		return rc;
 	}
-	int rc = run_rho(h, h->main, N, d_frac, d_E, want_rho_mode, mixed, l, st, e1);
+	// with forces (and a constraint set and particles), the force kernel finishes the energy
+	const bool e_in_force = (d_F || d_gfrac) && N > 0 && h->main.plan.nslot > 0;
+	int rc = run_rho(h, h->main, N, d_frac, d_E, want_rho_mode, mixed, l, st, e1, e_in_force);
 	if (rc)
 		return rc;
 	if (e2)
 		CC_CUDA(record_timing(e2, st));
 	if (d_F || d_gfrac)
-		rc = run_force(h, N, d_frac, d_F, d_gfrac, mixed, l, st);
+		rc = run_force(h, N, d_frac, d_F, d_gfrac, mixed, l, st, e_in_force ? d_E : nullptr);
 	if (e3)
 		CC_CUDA(record_timing(e3, st));
 	return rc;

@@ -425,6 +425,7 @@ struct ReduceArgs {
 	unsigned *ticket;         // 1, zero between launches
 	double inv_vol, shift;
 	double *E_out;
+	int finalize;             // 0: the force kernel that follows sums eblock into E_out
 	const int *skip;
 };
 
@@ -488,6 +489,8 @@ static __global__ void __launch_bounds__(kRedThreads) cc_reduce_kernel(ReduceArg
 		if (lane == 0)
 			a.eblock[blockIdx.x] = e;
 	}
+	if (!a.finalize)
+		return;
 	__threadfence();
 	__syncthreads();
 	if (threadIdx.x == 0)
@@ -538,6 +541,10 @@ struct ForceArgs {
 	double fscale;            // 2 / Volume
 	double *F_out;            // N x D Cartesian forces, or nullptr
 	double *gfrac_out;        // N x D dPhi/ds, or nullptr
+	const double *eblock;     // energy partials of the reduce blocks (neblock), summed into E_out by block (0, 0) when
+	int neblock;              // E_out is set (the reduce kernel then leaves E to this kernel)
+	double inv_vol, shift;
+	double *E_out;
 	const int *skip;
 };
 
@@ -593,6 +600,17 @@ __global__ void __launch_bounds__(kForceThreads, 3) cc_force_kernel(ForceArgs a)
 	cudaGridDependencySynchronize();   // u of this step is complete
 	if (a.skip && *a.skip)             // uniform over the grid
 		return;
+	if (a.E_out && blockIdx.x == 0 && blockIdx.y == 0 && warp == 0) {
+		// the energy, summed in the order of the reduce kernel's last block
+		double e = 0.0;
+		for (int b = lane; b < a.neblock; b += 32)
+			e += a.eblock[b];
+#pragma unroll
+		for (int o = 16; o > 0; o >>= 1)
+			e += __shfl_down_sync(0xffffffffu, e, o);
+		if (lane == 0)
+			*a.E_out = e * a.inv_vol + a.shift;
+	}
 
 	double g[D];
 #pragma unroll
