@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstdio>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -89,8 +90,13 @@ struct DevKSet {
 	}
 };
 
+// Bumped by every device or pinned allocation of the library and by changes of by-value kernel parameters: a
+// captured evaluation graph whose generation differs may hold stale pointers and is captured again.
+std::atomic<unsigned long long> g_alloc_gen{1};
+
 template <class T> int dev_alloc(T **p, size_t n)
 {
+	g_alloc_gen++;
 	*p = nullptr;
 	if (n == 0)
 		n = 1;
@@ -163,6 +169,19 @@ struct cc_handle {
 	bool in_pending = false;
 	bool lastF_valid = false;       // h_pin + 2 holds the forces of the bound positions
 	bool fused_ran = false;         // a fused launch ran since the barrier word was last read
+	bool upload_pending = false;    // h_in holds positions not yet copied to d_frac
+	double *d_pin = nullptr;        // device view of h_pin (mapped pinned memory): kernels write E and F there
+	// captured evaluations of cc_energy_grad (upload + kernels writing into h_pin), per (N, precision, forces)
+	struct EvalGraph {
+		int64_t N;
+		int precision, forces;
+		unsigned long long gen;
+		cudaGraphExec_t exec;
+	};
+	std::vector<EvalGraph> graphs;
+	int64_t last_N = -1;            // key and generation of the last direct cc_energy_grad (captured when repeated)
+	int last_precision = -1, last_forces = -1;
+	unsigned long long last_gen = 0;
 	// fused (cooperative) path
 	cc::TabSpec gspec;
 	void *d_tabP = nullptr, *d_tabE = nullptr;
@@ -514,9 +533,14 @@ int ensure_particles(cc_handle *h, int64_t N)
 		h->h_pin = nullptr;
 		h->pin_cap = 0;
 		h->lastF_valid = false;
-		cudaError_t e = cudaMallocHost(reinterpret_cast<void **>(&h->h_pin), pin * sizeof(double));
+		h->d_pin = nullptr;
+		g_alloc_gen++;
+		cudaError_t e = cudaHostAlloc(reinterpret_cast<void **>(&h->h_pin), pin * sizeof(double), cudaHostAllocMapped);
 		if (e != cudaSuccess)
-			return fail(CC_ERR_OOM, std::string("cudaMallocHost: ") + cudaGetErrorString(e));
+			return fail(CC_ERR_OOM, std::string("cudaHostAlloc: ") + cudaGetErrorString(e));
+		e = cudaHostGetDevicePointer(reinterpret_cast<void **>(&h->d_pin), h->h_pin, 0);
+		if (e != cudaSuccess)
+			return fail(CC_ERR_CUDA, std::string("cudaHostGetDevicePointer: ") + cudaGetErrorString(e));
 		h->pin_cap = pin;
 	}
 	return CC_OK;
@@ -533,6 +557,7 @@ int input_staging(cc_handle *h, size_t n)
 	}
 	n = std::max<size_t>(n, 1);
 	if (n > h->in_cap) {
+		g_alloc_gen++;
 		cudaFreeHost(h->h_in);
 		h->h_in = nullptr;
 		h->in_cap = 0;
@@ -547,12 +572,21 @@ int input_staging(cc_handle *h, size_t n)
 // Copy n staged doubles to d_frac on the handle's stream; the staging is reusable once ev_in has passed.
 int upload_staged(cc_handle *h, size_t n)
 {
+	h->upload_pending = false;
 	if (n == 0)
 		return CC_OK;
 	CC_CUDA(cudaMemcpyAsync(h->d_frac, h->h_in, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
 	CC_CUDA(cudaEventRecord(h->ev_in, h->stream));
 	h->in_pending = true;
 	return CC_OK;
+}
+
+// Positions staged by cc_set_positions are copied to the device by the first call that reads them.
+int flush_upload(cc_handle *h)
+{
+	if (!h->upload_pending || h->N <= 0)
+		return CC_OK;
+	return upload_staged(h, (size_t)h->N * h->d);
 }
 
 // Wrap into [0,1) as Configuration::Insert does (core/PeriodicCellList.h:517-538: floor twice). Values already in
@@ -1004,6 +1038,68 @@ int eval_device(cc_handle *h, int64_t N, const double *d_frac, double *d_E, doub
 	return rc;
 }
 
+// cc_energy_grad as one CUDA graph: copy of the staged positions, the rho / reduce / force kernels writing E and F into
+// mapped pinned memory. A key is captured on its second consecutive use with no allocation in between (the first,
+// direct evaluation makes every allocation the launch needs); *done tells whether the graph ran.
+int launch_eval_graph(cc_handle *h, int64_t N, int precision, int forces, bool *done)
+{
+	*done = false;
+	const unsigned long long gen = g_alloc_gen.load();
+	for (size_t i = 0; i < h->graphs.size(); i++) {
+		cc_handle::EvalGraph &g = h->graphs[i];
+		if (g.N != N || g.precision != precision || g.forces != forces)
+			continue;
+		if (g.gen != gen) {
+			cudaGraphExecDestroy(g.exec);
+			h->graphs.erase(h->graphs.begin() + i);
+			break;
+		}
+		CC_CUDA(cudaGraphLaunch(g.exec, h->stream));
+		CC_CUDA(cudaEventRecord(h->ev_in, h->stream));
+		h->in_pending = true;
+		h->upload_pending = false;
+		*done = true;
+		return CC_OK;
+	}
+	if (!(h->last_N == N && h->last_precision == precision && h->last_forces == forces && h->last_gen == gen))
+		return CC_OK;
+	if (h->in_pending) {   // the staging buffer is read by the graph's first node
+		CC_CUDA(cudaEventSynchronize(h->ev_in));
+		h->in_pending = false;
+	}
+	cudaGraph_t graph = nullptr;
+	CC_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+	cudaError_t ce = cudaMemcpyAsync(h->d_frac, h->h_in, sizeof(double) * N * h->d, cudaMemcpyHostToDevice, h->stream);
+	int rc = ce == cudaSuccess ? eval_device(h, N, h->d_frac, h->d_pin, forces ? h->d_pin + 2 : nullptr, nullptr,
+	                                         false, precision, h->stream)
+	                           : CC_ERR_CUDA;
+	const cudaError_t ee = cudaStreamEndCapture(h->stream, &graph);
+	if (rc != CC_OK || ce != cudaSuccess || ee != cudaSuccess || g_alloc_gen.load() != gen) {
+		if (graph)
+			cudaGraphDestroy(graph);
+		cudaGetLastError();
+		return CC_OK;   // not capturable now: the caller evaluates directly
+	}
+	cudaGraphExec_t exec = nullptr;
+	const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+	cudaGraphDestroy(graph);
+	if (ie != cudaSuccess) {
+		cudaGetLastError();
+		return CC_OK;
+	}
+	if (h->graphs.size() >= 4) {
+		cudaGraphExecDestroy(h->graphs.front().exec);
+		h->graphs.erase(h->graphs.begin());
+	}
+	h->graphs.push_back({N, precision, forces, gen, exec});
+	CC_CUDA(cudaGraphLaunch(exec, h->stream));
+	CC_CUDA(cudaEventRecord(h->ev_in, h->stream));
+	h->in_pending = true;
+	h->upload_pending = false;
+	*done = true;
+	return CC_OK;
+}
+
 template <typename T> __global__ void fma_probe_kernel(T *out, int iters, T a, T b)
 {
 	T x[8];
@@ -1114,6 +1210,8 @@ int cc_destroy(cc_handle *h)
 		cudaFree(kv.second);
 	for (cudaEvent_t e : h->ev)
 		cudaEventDestroy(e);
+	for (auto &g : h->graphs)
+		cudaGraphExecDestroy(g.exec);
 	if (h->stream)
 		cudaStreamDestroy(h->stream);
 	delete h;
@@ -1143,6 +1241,7 @@ int cc_set_rho_offset(cc_handle *h, double offset)
 		return fail(CC_ERR_ARG, "offset must be finite");
 	h->rho_offset = offset;
 	h->lastF_valid = false;
+	g_alloc_gen++;   // captured evaluations hold the old offset
 	return CC_OK;
 }
 
@@ -1159,10 +1258,12 @@ int cc_set_positions(cc_handle *h, int64_t N, const double *frac)
 		return rc;
 	double *in = h->h_in;
 	for (int64_t i = 0; i < N * d; i++)
-		if (!wrap_unit(frac[i], in + i))
+		if (!wrap_unit(frac[i], in + i)) {
+			h->upload_pending = false;
+			h->N = -1;
 			return fail(CC_ERR_ARG, "non-finite fractional coordinate");
-	if (int rc = upload_staged(h, (size_t)N * d))
-		return rc;
+		}
+	h->upload_pending = true;
 	h->N = N;
 	h->lastF_valid = false;
 	h->mc_valid = false;
@@ -1180,12 +1281,24 @@ int cc_energy_grad(cc_handle *h, double *E, double *F, int precision)
 	if (!E)
 		return fail(CC_ERR_ARG, "E is null");
 	const int64_t N = h->N;
-	if (int rc = eval_device(h, N, h->d_frac, h->d_E, F ? h->d_F : nullptr, nullptr, false, precision, h->stream))
-		return rc;
-	CC_CUDA(cudaMemcpyAsync(h->h_pin, h->d_E, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-	if (F && N > 0)
-		CC_CUDA(cudaMemcpyAsync(h->h_pin + 2, h->d_F, sizeof(double) * N * h->d, cudaMemcpyDeviceToHost, h->stream));
+	const int forces = (F && N > 0) ? 1 : 0;
 	h->lastF_valid = false;
+	// E and F are written by the kernels straight into the mapped pinned result buffer
+	bool done = false;
+	if (!h->timing && !h->use_fused && !h->d_skip && N > 0 && h->main.plan.nslot > 0)
+		if (int rc = launch_eval_graph(h, N, precision, forces, &done))
+			return rc;
+	if (!done) {
+		if (int rc = flush_upload(h))
+			return rc;
+		if (int rc = eval_device(h, N, h->d_frac, h->d_pin, forces ? h->d_pin + 2 : nullptr, nullptr, false,
+		                         precision, h->stream))
+			return rc;
+		h->last_N = N;
+		h->last_precision = precision;
+		h->last_forces = forces;
+		h->last_gen = g_alloc_gen.load();
+	}
 	CC_CUDA(cudaStreamSynchronize(h->stream));
 	if (int rc = check_barrier(h))
 		return rc;
@@ -1221,6 +1334,8 @@ int cc_rho(cc_handle *h, double *re, double *im, int precision)
 		return rc;
 	if (h->N < 0)
 		return fail(CC_ERR_STATE, "positions not set");
+	if (int rc = flush_upload(h))
+		return rc;
 	const int64_t N = h->N;
 	const size_t M = h->V.size();
 	const Launch l = choose_launch(h->main.plan, N, precision == CC_PREC_MIXED);
@@ -1285,6 +1400,8 @@ int cc_structure_factor(cc_handle *h, int64_t K, const int32_t *modes, double *S
 			return rc;
 		h->sk_modes = key;
 	}
+	if (int rc = flush_upload(h))
+		return rc;
 	const Launch l = choose_launch(h->sk.plan, N, precision == CC_PREC_MIXED);
 	const double save_off = h->rho_offset;
 	h->rho_offset = 0.0;   // S(k) of the particles themselves (StructureFactor has no fixed-particle offset)
@@ -1369,6 +1486,8 @@ int cc_mc_try_move(cc_handle *h, const double *s_prev, const double *s_after, do
 	}
 	if (!h->mc_valid) {
 		// rho of the bound positions in mode order (FP64), as the cached RhoReal / RhoImag of the reference
+		if (int rc = flush_upload(h))
+			return rc;
 		const Launch l = choose_launch(h->main.plan, h->N, false);
 		if (int rc = run_rho(h, h->main, h->N, h->d_frac, h->d_E, true, false, l, h->stream))
 			return rc;
