@@ -166,8 +166,112 @@ def batched_workload(cc, count, seed=2024):
     return pots, Ns, fracs, pairs
 
 
-def run_extras(args, cc, torch):
+def half_space_modes(d, nmax_f):
+    """Integer modes n with |n| <= nmax_f and first nonzero component > 0 (the half space of the k-set rule)."""
+    m = int(np.floor(nmax_f))
+    axes = [np.arange(-m, m + 1)] * d
+    n = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, d)
+    n = n[(n * n).sum(1) <= nmax_f * nmax_f + 1e-9]
+    first = np.array([row[np.nonzero(row)[0][0]] if row.any() else 0 for row in n])
+    return np.ascontiguousarray(n[first > 0], dtype=np.int32)
+
+
+def device_eval_ms(torch, pot, n, d, frac_dev, prec, reps=5):
+    """Median CUDA-event time of energy+forces on resident positions, L2 flushed (256 MB write) before each eval."""
+    E = torch.zeros(1, dtype=torch.float64, device="cuda")
+    F = torch.zeros((n, d), dtype=torch.float64, device="cuda")
+    flush = torch.empty(32 << 20, dtype=torch.float64, device="cuda")
+    st = torch.cuda.Stream()
+    evs = []
+    with torch.cuda.stream(st):
+        for i in range(2 + reps):
+            flush.fill_(float(i))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            pot.energy_grad_device(n, frac_dev.data_ptr(), E.data_ptr(), F.data_ptr(), precision=prec,
+                                   stream=st.cuda_stream)
+            b.record(st)
+            evs.append((a, b))
+    torch.cuda.synchronize()
+    ms = float(np.median([a.elapsed_time(b) for a, b in evs[2:]]))
+    return ms, float(E.item()), F.cpu().numpy()
+
+
+def run_single_legs(cc, torch):
+    """The other single-configuration workloads of the path: the 2D N=100 ground state, the 3D N=2000 full
+    minimisation with S(k) on |k| <= 1.5 K, and 2D N=1e5 in FP64 against mixed precision (errors reported)."""
     out = {}
+    # 2D N=100 chi=0.30 (M=60): FP64 device L-BFGS to Phi/N < 1e-20 from five seeded starts
+    d, n, chi = 2, 100, 0.30
+    basis = np.eye(d) * n ** (1.0 / d)
+    modes, V = cc.stealthy_kset(d, basis, n, chi)
+    pot = cc.CCPotential(d, basis, modes, V)
+    ts, evs, epp = [], [], []
+    for seed in range(5):
+        f0 = np.random.default_rng(100 + seed).random((n, d))
+        t0 = time.perf_counter()
+        _x, E, ev, _it, _st = pot.minimize(f0, stopval=1e-20 * n)
+        ts.append(time.perf_counter() - t0)
+        evs.append(ev)
+        epp.append(E / n)
+    out["ground_state_2d_n100"] = {"workload": "2D N=100 chi=0.30 M=60 v=1, FP64 L-BFGS (history 40) to Phi/N < 1e-20, "
+                                               "5 seeded starts", "median_s": float(np.median(ts)),
+                                   "median_evals": float(np.median(evs)), "max_E_per_particle": float(max(epp))}
+    # 3D N=2000 chi=0.45 (M=2724): full minimisation (FP64, and mixed then FP64), then S(k) on |k| <= 1.5 K
+    d, n, chi = 3, 2000, 0.45
+    side = n ** (1.0 / d)
+    basis = np.eye(d) * side
+    modes, V = cc.stealthy_kset(d, basis, n, chi)
+    pot = cc.CCPotential(d, basis, modes, V)
+    f0 = np.random.default_rng(7).random((n, d))
+    t0 = time.perf_counter()
+    x, E, ev, _it, _st = pot.minimize(f0, stopval=1e-20 * n)
+    t_fp64 = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    _x2, E2, ev2, _it2, _st2 = pot.minimize(f0, stopval=1e-20 * n, precision=cc.PREC_SCHEDULE,
+                                            switch_energy_per_particle=1e-10)
+    t_sched = time.perf_counter() - t0
+    nmax = float(np.sqrt((np.asarray(modes, np.float64) ** 2).sum(1).max()))
+    kq = half_space_modes(d, 1.5 * nmax)
+    inside = (kq.astype(np.float64) ** 2).sum(1) <= nmax * nmax + 1e-9
+    pot.set_configuration(x)
+    S = pot.structure_factor(kq)
+    reps = 20
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        S = pot.structure_factor(kq)
+    t_sk = (time.perf_counter() - t0) / reps
+    out["minimise_3d_n2000"] = {
+        "workload": "3D N=2000 chi=0.45 M=2724 v=1 from a seeded uniform start, to Phi/N < 1e-20",
+        "fp64_s": t_fp64, "fp64_evals": int(ev), "fp64_E_per_particle": E / n,
+        "schedule_s": t_sched, "schedule_evals": int(ev2), "schedule_E_per_particle": E2 / n,
+        "sk_modes": int(len(kq)), "sk_ms_per_call": t_sk * 1e3, "max_S_constrained": float(S[inside].max()),
+        "mean_S_beyond": float(S[~inside].mean())}
+    # 2D N=1e5 chi=0.20 (M=40002): FP64 and mixed precision on the same positions
+    d, n, chi = 2, 100000, 0.20
+    basis = np.eye(d) * n ** (1.0 / d)
+    modes, V = cc.stealthy_kset(d, basis, n, chi)
+    pot = cc.CCPotential(d, basis, modes, V)
+    frac = np.random.default_rng(11).random((n, d))
+    fdev = torch.tensor(frac, dtype=torch.float64, device="cuda")
+    ms64, E64, F64 = device_eval_ms(torch, pot, n, d, fdev, cc.PREC_FP64)
+    msmx, Emx, Fmx = device_eval_ms(torch, pot, n, d, fdev, cc.PREC_MIXED)
+    pot.set_configuration(frac)
+    re64, im64 = pot.rho(cc.PREC_FP64)
+    remx, immx = pot.rho(cc.PREC_MIXED)
+    pairs = n * len(V)
+    out["large_2d_n100000"] = {
+        "workload": "2D N=100000 chi=0.20 M=40002 v=1, energy + forces, L2 flushed before each evaluation",
+        "fp64_ms": ms64, "mixed_ms": msmx, "fp64_pairs_per_s": pairs / (ms64 / 1e3),
+        "mixed_pairs_per_s": pairs / (msmx / 1e3),
+        "mixed_rel_err_E": abs(Emx - E64) / abs(E64),
+        "mixed_max_err_F_over_max_F": float(np.abs(Fmx - F64).max() / np.abs(F64).max()),
+        "mixed_max_err_rho_over_sqrtN": float(max(np.abs(remx - re64).max(), np.abs(immx - im64).max()) / np.sqrt(n))}
+    return out
+
+
+def run_extras(args, cc, torch):
+    out = run_single_legs(cc, torch)
     # batched uneven instances: one batched energy+gradient step, CUDA-event timed, inputs resident
     pots, Ns, fracs, pairs = batched_workload(cc, args.batch)
     batch = cc.CCBatch(pots, Ns)

@@ -153,23 +153,59 @@ __global__ void __launch_bounds__(kFusedThreads, 2) cc_batch_kernel(BatchArgs a)
 				const C *r0 = tabP + (size_t)j * rowP, *r1 = r0 + (size_t)kFusedWarps * rowP;
 				C z0 = seed_from_l2<D, C>(r0, 1, ix), z1 = seed_from_l2<D, C>(r1, 1, ix);
 				const C w0 = __ldcg(r0 + ix.w), w1 = __ldcg(r1 + ix.w);
+				if constexpr (MIXED) {
 #pragma unroll
-				for (int r = 0; r < L; r++) {
-					acc[r].x += (double)z0.x + (double)z1.x;
-					acc[r].y += (double)z0.y + (double)z1.y;
-					z0 = cmul(z0, w0);
-					z1 = cmul(z1, w1);
+					for (int r = 0; r < L; r++) {
+						acc[r].x += (double)z0.x + (double)z1.x;
+						acc[r].y += (double)z0.y + (double)z1.y;
+						z0 = cmul(z0, w0);
+						z1 = cmul(z1, w1);
+					}
+				} else {
+					const double c0 = 2.0 * w0.x, c1 = 2.0 * w1.x;
+					double2 p0 = z0, p1 = z1, q0 = cmul(z0, w0), q1 = cmul(z1, w1);
+					acc[0].x += p0.x + p1.x;
+					acc[0].y += p0.y + p1.y;
+					acc[1].x += q0.x + q1.x;
+					acc[1].y += q0.y + q1.y;
+#pragma unroll
+					for (int r = 2; r < L; r++) {
+						const double2 n0 = cheb_next(c0, q0, p0), n1 = cheb_next(c1, q1, p1);
+						acc[r].x += n0.x + n1.x;
+						acc[r].y += n0.y + n1.y;
+						p0 = q0;
+						q0 = n0;
+						p1 = q1;
+						q1 = n1;
+					}
 				}
 			}
 			if (j < j1) {
 				const C *r0 = tabP + (size_t)j * rowP;
 				C z0 = seed_from_l2<D, C>(r0, 1, ix);
 				const C w0 = __ldcg(r0 + ix.w);
+				if constexpr (MIXED) {
 #pragma unroll
-				for (int r = 0; r < L; r++) {
-					acc[r].x += (double)z0.x;
-					acc[r].y += (double)z0.y;
-					z0 = cmul(z0, w0);
+					for (int r = 0; r < L; r++) {
+						acc[r].x += (double)z0.x;
+						acc[r].y += (double)z0.y;
+						z0 = cmul(z0, w0);
+					}
+				} else {
+					const double c0 = 2.0 * w0.x;
+					double2 p0 = z0, q0 = cmul(z0, w0);
+					acc[0].x += p0.x;
+					acc[0].y += p0.y;
+					acc[1].x += q0.x;
+					acc[1].y += q0.y;
+#pragma unroll
+					for (int r = 2; r < L; r++) {
+						const double2 n0 = cheb_next(c0, q0, p0);
+						acc[r].x += n0.x;
+						acc[r].y += n0.y;
+						p0 = q0;
+						q0 = n0;
+					}
 				}
 			}
 #pragma unroll
@@ -273,13 +309,37 @@ __global__ void __launch_bounds__(kFusedThreads, 2) cc_batch_kernel(BatchArgs a)
 				const C w = __ldcg(col + (size_t)ix.w * in.Npad);
 				const double2 *uq = in.u_slot + q;
 				R S0 = 0, S1 = 0;
+				if constexpr (MIXED) {
 #pragma unroll
-				for (int r = 0; r < L; r++) {
-					const C uu = to_c<C>(__ldcg(uq + (size_t)r * in.nseg));
-					const R t = uu.x * z.y + uu.y * z.x;
-					S0 += t;
-					S1 = fma((R)r, t, S1);
-					z = cmul(z, w);
+					for (int r = 0; r < L; r++) {
+						const C uu = to_c<C>(__ldcg(uq + (size_t)r * in.nseg));
+						const R t = uu.x * z.y + uu.y * z.x;
+						S0 += t;
+						S1 = fma((R)r, t, S1);
+						z = cmul(z, w);
+					}
+				} else {
+					double2 uu[L];
+#pragma unroll
+					for (int r = 0; r < L; r++)
+						uu[r] = __ldcg(uq + (size_t)r * in.nseg);
+					const double c = 2.0 * w.x;
+					double2 p = z, qz = cmul(z, w);
+					S0 = uu[0].x * p.y + uu[0].y * p.x;
+					{
+						const double t = uu[1].x * qz.y + uu[1].y * qz.x;
+						S0 += t;
+						S1 = t;
+					}
+#pragma unroll
+					for (int r = 2; r < L; r++) {
+						const double2 n = cheb_next(c, qz, p);
+						const double t = uu[r].x * n.y + uu[r].y * n.x;
+						S0 += t;
+						S1 = fma((double)r, t, S1);
+						p = qz;
+						qz = n;
+					}
 				}
 				const double S0d = (double)S0;
 				if (D >= 2)
