@@ -63,6 +63,22 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def max_over_ranks(x, device):
+    """The largest of every rank's x (a time): replicas are timed by the slowest one. Identity for one process."""
+    import torch
+
+    if not (torch.distributed.is_available() and torch.distributed.is_initialized()):
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(units_per_rank, seconds, world):
+    """Whole-job throughput of `world` replicas that each processed units_per_rank in at most `seconds`."""
+    return world * units_per_rank / seconds
+
+
 class Clocks:
     """nvidia-smi samples of SM clock and throttle reasons while running."""
 
@@ -424,11 +440,8 @@ def run_ours(args):
     torch.cuda.synchronize()
     ms = t_start.elapsed_time(t_end)
     clk = clocks.stop()
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * K / (ms / 1e3)
+    ms = max_over_ranks(ms, dev)
+    value = replica_rate(K, ms / 1e3, world)
 
     # per-kernel CUDA-event timing: events recorded around each kernel INSIDE a replayed CUDA graph of G steps (so no
     # host launch gap falls between an event and its kernel); the events are created before the capture
@@ -469,12 +482,8 @@ def run_ours(args):
     for i in range(KE):
         pot.set_configuration(host_pool[i % P])
         e_, _ = pot.energy_and_forces(precision=prec)
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = world * KE / e2e_s
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dev)
+    e2e = replica_rate(KE, e2e_s, world)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -200,9 +200,10 @@ int cc_kset_stealthy(int d, const double *basis, int64_t N, double chi, int type
                      double *V, int64_t *M);
 
 /* --- allocation-free evaluation (no counterpart in the reference) -----------------------------------------------
- * For callers that cannot allocate GPU memory: code running while a CUDA graph is captured (cudaMalloc is refused
- * under global-mode capture) and processes whose memory manager owns the device's memory. They cannot create a
- * cc_handle (cc_create allocates). cc_energy_noalloc allocates nothing, on the device or the host: the caller passes
+ * For callers that cannot allocate GPU memory: processes whose memory manager (a caching allocator, a serving
+ * engine with a fixed HBM budget) owns the device's memory and lets no library allocate beside it, and loops that
+ * must not pay for cudaMalloc, which can synchronise the device. They cannot create a cc_handle (cc_create
+ * allocates). cc_energy_noalloc allocates nothing, on the device or the host: the caller passes
  * every input and output in its own device memory, and the only scratch is a fixed array of
  * CC_NOALLOC_SCRATCH_BYTES inside the library, which every GPU that loads the library holds until the process exits.
  *   d, basis (host, d x d), M modes (device, M x d int32), V (device, M), shift, N fractional positions (device,

@@ -1,8 +1,8 @@
 // cc_noalloc.cu — cc_energy_noalloc: the rho + energy pass for callers that cannot allocate GPU memory.
 //
-// Who needs it: code that runs while a CUDA graph is being captured (cudaMalloc is not allowed under global-mode
-// stream capture), and host programs whose memory manager has already reserved the device's memory (a caching
-// allocator or a serving engine with a fixed HBM budget) and does not allow a library to allocate on the side.
+// Who needs it: host programs whose memory manager has already reserved the device's memory (a caching allocator or
+// a serving engine with a fixed HBM budget) and does not allow a library to allocate on the side, and loops that must
+// not pay for cudaMalloc, which can synchronise the whole device.
 // Such callers cannot create a cc_handle, because cc_create allocates the planned k-set and work buffers.
 //
 // This entry point takes every input and output in the caller's own device memory and computes

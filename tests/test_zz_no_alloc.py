@@ -1,7 +1,7 @@
 """cc_energy_noalloc, the allocation-free entry point, against the regular entry points.
 
-It exists for callers that cannot allocate GPU memory: code running inside CUDA graph capture, where cudaMalloc is
-refused, and processes whose memory manager owns all device memory. The test calls it through the C ABI with
+It exists for callers that cannot allocate GPU memory: processes whose memory manager owns all device memory, and
+loops that must not pay for cudaMalloc, which can synchronise the device. The test calls it through the C ABI with
 caller-owned device buffers (torch tensors) twice in a row (the second call must not see stale scratch contents)
 and compares E and rho with cc_energy_grad / cc_rho on the same inputs, at the FP64 path's tolerance: 1e-10 of the
 reference tests' scales. This file sorts last so a stop-at-first-failure run has run every other test first.
