@@ -199,6 +199,29 @@ int cc_energy_grad_device(cc_handle *h, int64_t N, const double *d_frac, double 
 int cc_kset_stealthy(int d, const double *basis, int64_t N, double chi, int type, int64_t cap, int32_t *modes,
                      double *V, int64_t *M);
 
+/* --- isotropic structure factor ---------------------------------------------------------------------------------
+ * cc_kset_isotropic: the wavevectors of GetKs (core/PeriodicCellList.cpp:509-735) for a cell (host only, no GPU
+ * needed), as K integer modes (K x d) with |k| (K): for d >= 2 the half-space lattice points with
+ * circular_kmin < |k| < circular_kmax ordered by (|k|^2, k_x), or, when linear_kmax differs from circular_kmax, the
+ * multiples i k (|i k| <= linear_kmax) of the first point of each lattice direction in that circle; for d = 1 the
+ * multiples of the reciprocal vector (see the reference for circular_kmin > 0). sample_probability < 1 keeps each
+ * multiple with that probability, drawn as the reference draws it (Mersenne Twister seeded with 98765).
+ * *K receives the count (CC_ERR_ARG if cap is too small, *K then holds the need).
+ *
+ * cc_isotropic_structure_factor: IsotropicStructureFactor (pairstat/StructureFactor.cpp:79-260) over nconfigs
+ * configurations (bases: nconfigs x d x d, row i = a_i; N[j] particles at frac[j], N[j] x d fractional): S(k) of every
+ * wavevector on the GPU (FP64), binned by floor(|k| / k_precision) (k_precision 0: the first reciprocal vector's
+ * length). option 0: bin means over wavevectors; 1: S(k) averaged over the k-space shell volume for |k| <=
+ * circular_kmax; 2: one row per wavevector (every cell must give the same count), sorted by |k|. Rows of 4 doubles
+ * (k, S, dk, dS) as the reference's GeometryVector(4) results; *count receives the number of rows (CC_ERR_ARG if cap
+ * is too small). Wavevectors are recomputed when a configuration's basis differs from the previous one. */
+int cc_kset_isotropic(int d, const double *basis, double circular_kmax, double linear_kmax, double sample_probability,
+                      double circular_kmin, int64_t cap, int32_t *modes, double *kamp, int64_t *K);
+int cc_isotropic_structure_factor(int d, int64_t nconfigs, const double *bases, const int64_t *N,
+                                  const double *const *frac, double circular_kmax, double linear_kmax,
+                                  double k_precision, double sample_probability, int option, double circular_kmin,
+                                  double *results, int64_t cap, int64_t *count);
+
 /* --- allocation-free evaluation (no counterpart in the reference) -----------------------------------------------
  * For callers that cannot allocate GPU memory: processes whose memory manager (a caching allocator, a serving
  * engine with a fixed HBM budget) owns the device's memory and lets no library allocate beside it, and loops that

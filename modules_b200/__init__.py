@@ -6,7 +6,9 @@ thin ctypes binding of that ABI for Python callers (tests, benchmarks); it mirro
 interface (Energy, AllForce, Force, GetRho, SetConfiguration) and has no CPU fallback.
 """
 from .ccgpu import (STOPVAL_GROUND_STATE, CCBatch, CCError, CCPotential, PREC_FP64, PREC_MIXED, PREC_SCHEDULE, device_available, library_path, load_library,
-                    probe_fma_peak, serve, stealthy_kset)
+                    probe_fma_peak, serve, stealthy_kset, isotropic_kset,
+                    isotropic_structure_factor)
 
 __all__ = ["STOPVAL_GROUND_STATE", "CCBatch", "CCError", "CCPotential", "PREC_FP64", "PREC_MIXED", "PREC_SCHEDULE", "device_available", "library_path",
-           "load_library", "probe_fma_peak", "serve", "stealthy_kset"]
+           "load_library", "probe_fma_peak", "serve", "stealthy_kset",
+           "isotropic_kset", "isotropic_structure_factor"]

@@ -80,6 +80,9 @@ _SIGS = {
     "cc_objective": (_i, [_vp, _i64, _vp, _d, ctypes.POINTER(_d), _vp, _i]),
     "cc_energy_grad_device": (_i, [_vp, _i64, _vp, _vp, _vp, _vp, _i, _vp]),
     "cc_kset_stealthy": (_i, [_i, _vp, _i64, _d, _i, _i64, _vp, _vp, ctypes.POINTER(_i64)]),
+    "cc_kset_isotropic": (_i, [_i, _vp, _d, _d, _d, _d, _i64, _vp, _vp, ctypes.POINTER(_i64)]),
+    "cc_isotropic_structure_factor": (_i, [_i, _i64, _vp, _vp, _vp, _d, _d, _d, _d, _i, _d, _vp, _i64,
+                                           ctypes.POINTER(_i64)]),
     "cc_set_timing": (_i, [_vp, _i]),
     "cc_get_timing": (_i, [_vp, ctypes.POINTER(_d), ctypes.POINTER(_d), ctypes.POINTER(_d), ctypes.POINTER(_i64)]),
     "cc_plan_info": (_i, [_vp, _i64, ctypes.POINTER(_i), ctypes.POINTER(_i64), ctypes.POINTER(_i),
@@ -148,6 +151,45 @@ def stealthy_kset(d, basis, N, chi, type_=0):
     V = np.zeros(max(M.value, 1))
     _check(lib.cc_kset_stealthy(d, _ptr(basis), N, chi, type_, M.value, _ptr(modes), _ptr(V), ctypes.byref(M)))
     return modes[:M.value], V[:M.value]
+
+
+def isotropic_kset(d, basis, circular_kmax, linear_kmax, sample_probability=1.0, circular_kmin=0.0):
+    """The wavevectors of the reference's GetKs for a cell: (modes int32 K x d, |k| float64 K). Host only."""
+    lib = load_library()
+    basis = np.ascontiguousarray(basis, dtype=np.float64).reshape(d, d)
+    K = _i64(0)
+    args = (d, _ptr(basis), circular_kmax, linear_kmax, sample_probability, circular_kmin)
+    rc = lib.cc_kset_isotropic(*args, 0, None, None, ctypes.byref(K))
+    if rc not in (0, -1) or (rc == -1 and K.value == 0):
+        _check(rc)
+    modes = np.zeros((max(K.value, 1), d), np.int32)
+    kamp = np.zeros(max(K.value, 1))
+    _check(lib.cc_kset_isotropic(*args, K.value, _ptr(modes), _ptr(kamp), ctypes.byref(K)))
+    return modes[:K.value], kamp[:K.value]
+
+
+def isotropic_structure_factor(d, bases, fracs, circular_kmax, linear_kmax, k_precision=0.01, sample_probability=1.0,
+                               option=0, circular_kmin=0.0):
+    """IsotropicStructureFactor over configurations (bases[j]: d x d rows a_i; fracs[j]: N_j x d fractional).
+    Returns an (R, 4) array of rows (k, S, dk, dS) as the reference's results."""
+    lib = load_library()
+    n = len(fracs)
+    B = np.ascontiguousarray(np.asarray(bases, dtype=np.float64).reshape(n, d, d))
+    arrs = [np.ascontiguousarray(f, dtype=np.float64).reshape(-1, d) for f in fracs]
+    N = np.array([len(a) for a in arrs], dtype=np.int64)
+    ptrs = (_vp * n)(*[a.ctypes.data_as(_vp) for a in arrs])
+    cnt = _i64(0)
+    args = (d, n, _ptr(B), _ptr(N), ptrs, circular_kmax, linear_kmax, k_precision, sample_probability, option,
+            circular_kmin)
+    # rows: at most one per bin (options 0, 1) or one per wavevector of the first cell (option 2)
+    if option == 2:
+        cap = len(isotropic_kset(d, B[0], circular_kmax, linear_kmax, sample_probability, circular_kmin)[1])
+    else:
+        kp = k_precision if k_precision > 0 else float(np.linalg.norm(2 * np.pi * np.linalg.inv(B[0]).T[0]))
+        cap = int(np.floor(linear_kmax / kp)) + 1 if linear_kmax > 0 else 0
+    out = np.zeros((max(cap, 1), 4))
+    _check(lib.cc_isotropic_structure_factor(*args, _ptr(out), cap, ctypes.byref(cnt)))
+    return out[:cnt.value]
 
 
 def probe_fma_peak(precision=PREC_FP64):

@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstdio>
+#include <array>
 #include <atomic>
 #include <cstring>
 #include <mutex>
@@ -2328,6 +2329,156 @@ int cc_kset_stealthy(int d, const double *basis, int64_t N, double chi, int type
 		return fail(CC_ERR_ARG, "cap too small for the k-set");
 	std::memcpy(modes, mv.data(), mv.size() * sizeof(int32_t));
 	std::memcpy(V, vv.data(), vv.size() * sizeof(double));
+	return CC_OK;
+}
+
+
+int cc_kset_isotropic(int d, const double *basis, double circular_kmax, double linear_kmax, double sample_probability,
+                      double circular_kmin, int64_t cap, int32_t *modes, double *kamp, int64_t *K)
+{
+	if (d < 1 || d > 3 || !basis || !K || cap < 0 || (cap > 0 && (!modes || !kamp)) || std::isnan(circular_kmax) ||
+	    std::isnan(linear_kmax) || std::isnan(sample_probability) || std::isnan(circular_kmin))
+		return fail(CC_ERR_ARG, "invalid wavevector-list arguments");
+	std::vector<int32_t> mv;
+	std::vector<double> kv;
+	if (!cc::isotropic_ks(d, basis, circular_kmax, linear_kmax, sample_probability, circular_kmin, mv, kv))
+		return fail(CC_ERR_ARG, "degenerate cell, non-positive 1D cell or too many wavevectors");
+	*K = (int64_t)kv.size();
+	if (*K > cap)
+		return fail(CC_ERR_ARG, "cap too small for the wavevector list");
+	std::memcpy(modes, mv.data(), mv.size() * sizeof(int32_t));
+	std::memcpy(kamp, kv.data(), kv.size() * sizeof(double));
+	return CC_OK;
+}
+
+int cc_isotropic_structure_factor(int d, int64_t nconfigs, const double *bases, const int64_t *N,
+                                  const double *const *frac, double circular_kmax, double linear_kmax,
+                                  double k_precision, double sample_probability, int option, double circular_kmin,
+                                  double *results, int64_t cap, int64_t *count)
+{
+	if (d < 1 || d > 3 || nconfigs < 1 || !bases || !N || !frac || !count || cap < 0 || (cap > 0 && !results))
+		return fail(CC_ERR_ARG, "invalid isotropic S(k) arguments");
+	if (option < 0 || option > 2)
+		return fail(CC_ERR_ARG, "option must be 0 (average over wavevectors), 1 (over k-space volume) or 2 (per wavevector)");
+	if (std::isnan(k_precision) || k_precision < 0.0 || std::isnan(sample_probability) || std::isnan(circular_kmin))
+		return fail(CC_ERR_ARG, "k_precision must be >= 0 (0: the first reciprocal vector's length)");
+	*count = 0;
+	// the reference returns no result for these
+	if (!(circular_kmax > 0.0) || !(linear_kmax > 0.0) || circular_kmin > circular_kmax)
+		return CC_OK;
+	const int dd = d * d;
+	double vol0 = 0.0, recip0[9];
+	if (!cc::cell_geometry(d, bases, &vol0, recip0))
+		return fail(CC_ERR_ARG, "degenerate cell basis");
+	if (k_precision == 0.0) {
+		cc::reciprocal_by_projection(d, bases, recip0);   // the reference's |b_0|
+		double b2 = 0.0;
+		for (int x = 0; x < d; x++)
+			b2 += recip0[x] * recip0[x];
+		k_precision = std::sqrt(b2);
+	}
+	struct Bin {
+		double n = 0, k1 = 0, k2 = 0, s1 = 0, s2 = 0;
+	};
+	const size_t nbin = (size_t)std::floor(linear_kmax / k_precision) + 1;
+	if (!(linear_kmax / k_precision < 1e9))
+		return fail(CC_ERR_ARG, "linear_kmax / k_precision is too large");
+	std::vector<Bin> bins(option == 2 ? 0 : nbin);
+	double ident[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+	double I[9];
+	for (int i = 0; i < d; i++)
+		for (int j = 0; j < d; j++)
+			I[i * d + j] = ident[i * 3 + j];
+	// S(k) depends only on the integer modes and the fractional positions: one handle serves every configuration
+	cc_handle *h = nullptr;
+	if (int rc = cc_create(d, I, 0, nullptr, nullptr, 0.0, &h))
+		return rc;
+	std::vector<int32_t> modes;
+	std::vector<double> kamp, S;
+	int rc = CC_OK;
+	for (int64_t j = 0; j < nconfigs && rc == CC_OK; j++) {
+		const double *bj = bases + (size_t)j * dd;
+		const bool same = j > 0 && std::equal(bj, bj + dd, bases + (size_t)(j - 1) * dd);
+		if (!same) {
+			if (!cc::isotropic_ks(d, bj, circular_kmax, linear_kmax, sample_probability, circular_kmin, modes, kamp)) {
+				rc = fail(CC_ERR_ARG, "degenerate cell, non-positive 1D cell or too many wavevectors");
+				break;
+			}
+			if (option == 2) {
+				if (j == 0)
+					bins.assign(kamp.size(), Bin());
+				else if (kamp.size() != bins.size()) {
+					rc = fail(CC_ERR_ARG, "per-wavevector S(k) needs the same number of wavevectors in every cell");
+					break;
+				}
+			}
+		}
+		const int64_t K = (int64_t)kamp.size();
+		if (K == 0)
+			continue;
+		if (N[j] < 0 || (N[j] > 0 && !frac[j])) {
+			rc = fail(CC_ERR_ARG, "invalid particle count or null positions");
+			break;
+		}
+		S.resize((size_t)K);
+		if ((rc = cc_set_positions(h, N[j], frac[j])) || (rc = cc_structure_factor(h, K, modes.data(), S.data(), CC_PREC_FP64)))
+			break;
+		for (int64_t i = 0; i < K; i++) {
+			size_t b = (size_t)i;
+			if (option != 2) {
+				b = (size_t)std::floor(kamp[i] / k_precision);
+				if (b >= bins.size())
+					continue;
+			}
+			Bin &q = bins[b];
+			q.n += 1.0;
+			q.k1 += kamp[i];
+			q.k2 += kamp[i] * kamp[i];
+			q.s1 += S[i];
+			q.s2 += S[i] * S[i];
+		}
+	}
+	cc_destroy(h);
+	if (rc)
+		return rc;
+	// rows (k, S, dk, dS) as IsotropicStructureFactor (pairstat/StructureFactor.cpp:199-256)
+	auto ball = [d](double r) {
+		const double c = d == 1 ? 2.0 : d == 2 ? M_PI : 4.1887902047863909846;
+		return c * std::pow(r, (double)d);
+	};
+	const double omega = std::pow(2.0 * M_PI, (double)d) / vol0 / (double)nconfigs;
+	std::vector<std::array<double, 4> > rows;
+	for (const Bin &q : bins) {
+		if (!(q.n > 0.0))
+			continue;
+		std::array<double, 4> r;
+		r[0] = q.k1 / q.n;
+		const double kv = (q.k2 / q.n - r[0] * r[0]) / q.n;
+		r[2] = kv > 0 ? std::sqrt(kv) : 0.0;
+		const double mean = q.s1 / q.n, sv = q.s2 / q.n - mean * mean;
+		if (option == 0 || r[0] > circular_kmax) {
+			r[1] = mean;
+			r[3] = std::sqrt((sv > 0 ? sv : 0.0) / q.n);
+		} else if (option == 1) {
+			const double vd = 0.5 * (ball(r[0] + 0.5 * k_precision) - ball(r[0] - 0.5 * k_precision));
+			r[1] = q.s1 * omega / vd;
+			r[2] = 0.5 * k_precision;
+			r[3] = (omega / vd) * std::sqrt((sv > 0 ? sv : 0.0) / q.n);
+		} else {
+			r[1] = mean;
+			r[3] = q.n;
+		}
+		rows.push_back(r);
+	}
+	if (option == 2)   // by |k|; equal |k| keep the order the reference's sort gives them on the same sequence
+		std::sort(rows.begin(), rows.end(),
+		          [](const std::array<double, 4> &a, const std::array<double, 4> &b) { return a[0] < b[0]; });
+	*count = (int64_t)rows.size();
+	if (*count > cap)
+		return fail(CC_ERR_ARG, "cap too small for the S(k) rows");
+	for (size_t i = 0; i < rows.size(); i++)
+		for (int c = 0; c < 4; c++)
+			results[i * 4 + c] = rows[i][c];
 	return CC_OK;
 }
 

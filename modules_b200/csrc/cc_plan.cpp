@@ -5,6 +5,8 @@
 #include <array>
 #include <cmath>
 #include <numeric>
+#include <random>
+#include <set>
 
 namespace cc {
 
@@ -394,6 +396,228 @@ bool stealthy_kset(int d, const double *basis, int64_t N, double chi, int type, 
 				w = std::pow(1.0 - x, 2.0);
 		}
 		V[m] = w;
+	}
+	return true;
+}
+
+namespace {
+
+int64_t gcd64(int64_t a, int64_t b)
+{
+	a = a < 0 ? -a : a;
+	b = b < 0 ? -b : b;
+	while (b) {
+		const int64_t t = a % b;
+		a = b;
+		b = t;
+	}
+	return a;
+}
+
+// Cartesian k = sum_e n_e b_e, accumulated axis by axis from zero (as GeometryVector sums), and k.k.
+void lattice_k(int d, const double *recip, const int64_t *n, double *k)
+{
+	for (int x = 0; x < d; x++)
+		k[x] = 0.0;
+	for (int e = 0; e < d; e++)
+		for (int x = 0; x < d; x++)
+			k[x] = k[x] + (double)n[e] * recip[e * d + x];
+}
+
+double mod2(int d, const double *k)
+{
+	double s = 0.0;
+	for (int x = 0; x < d; x++)
+		s += k[x] * k[x];
+	return s;
+}
+
+double dot(int d, const double *u, const double *v)
+{
+	double s = 0.0;
+	for (int x = 0; x < d; x++)
+		s += u[x] * v[x];
+	return s;
+}
+
+// Reciprocal basis formed as the reference's cell forms it (core/PeriodicCellList.h:999-1030): b_i = a_i minus its
+// projections on the Gram-Schmidt orthogonalised other basis vectors, scaled by 2 pi / (b_i . a_i). Same algebra as
+// cell_geometry's inverse, but the same rounding as the reference, so lattice vectors of equal length compare equal
+// (and order) exactly as there.
+void reciprocal_by_projection_impl(int d, const double *a, double *recip)
+{
+	for (int i = 0; i < d; i++) {
+		double r[3], ortho[2][3];
+		int no = 0;
+		for (int x = 0; x < d; x++)
+			r[x] = a[i * d + x];
+		for (int j = 0; j < d; j++) {
+			if (j == i)
+				continue;
+			double t[3];
+			for (int x = 0; x < d; x++)
+				t[x] = a[j * d + x];
+			for (int o = 0; o < no; o++) {
+				const double c = dot(d, t, ortho[o]) / mod2(d, ortho[o]);
+				for (int x = 0; x < d; x++)
+					t[x] -= ortho[o][x] * c;
+			}
+			for (int x = 0; x < d; x++)
+				ortho[no][x] = t[x];
+			no++;
+		}
+		for (int o = 0; o < no; o++) {
+			const double c = dot(d, ortho[o], r) / mod2(d, ortho[o]);
+			for (int x = 0; x < d; x++)
+				r[x] -= ortho[o][x] * c;
+		}
+		const double sc = 2.0 * M_PI / dot(d, r, a + i * d);
+		for (int x = 0; x < d; x++)
+			recip[i * d + x] = r[x] * sc;
+	}
+}
+
+}  // namespace
+
+void reciprocal_by_projection(int d, const double *basis, double *recip)
+{
+	reciprocal_by_projection_impl(d, basis, recip);
+}
+
+bool isotropic_ks(int d, const double *basis, double circ_kmax, double lin_kmax, double sample_prob, double circ_kmin,
+                  std::vector<int32_t> &modes, std::vector<double> &kamp, size_t max_ks)
+{
+	modes.clear();
+	kamp.clear();
+	double vol = 0.0, recip[9];
+	if (d < 1 || d > 3 || !cell_geometry(d, basis, &vol, recip))
+		return false;
+	if (!(circ_kmax > 0.0) || !(lin_kmax > 0.0))
+		return true;
+	reciprocal_by_projection_impl(d, basis, recip);
+	std::mt19937 rng(98765u);
+	auto keep = [&]() { return sample_prob >= 1.0 || (double)rng() / 4294967296.0 < sample_prob; };
+	auto push = [&](int64_t n0, int64_t n1, int64_t n2, double amp) {
+		const int64_t n[3] = {n0, n1, n2};
+		for (int e = 0; e < d; e++) {
+			if (n[e] > INT32_MAX || n[e] < INT32_MIN)
+				return false;
+			modes.push_back((int32_t)n[e]);
+		}
+		kamp.push_back(amp);
+		return kamp.size() <= max_ks;
+	};
+	if (d == 1) {
+		const double b = recip[0];
+		if (!(b > 0.0))
+			return false;
+		if (circ_kmin <= 0.0) {
+			for (int64_t i = 1;; i++) {
+				const double kx = (double)i * b;
+				if (kx > lin_kmax)
+					break;
+				if (keep() && !push(i, 0, 0, std::sqrt(kx * kx)))
+					return false;
+			}
+			return true;
+		}
+		std::vector<int64_t> seed;
+		std::vector<double> seedk;
+		for (int64_t i = 1;; i++) {
+			const double kx = (double)i * b;
+			if (kx > circ_kmax)
+				break;
+			if (kx > circ_kmin && keep()) {
+				if (!push(i, 0, 0, std::sqrt(kx * kx)))
+					return false;
+				seed.push_back(i);
+				seedk.push_back(kx);
+			}
+		}
+		if (seed.empty())
+			return true;
+		for (int64_t i = 2;; i++) {
+			for (size_t j = 0; j < seed.size(); j++) {
+				const double kx = (double)i * seedk[j];
+				if (kx > lin_kmax)
+					return true;
+				if (keep() && !push(i * seed[j], 0, 0, std::sqrt(kx * kx)))
+					return false;
+			}
+		}
+	}
+	// d >= 2: half-space points of the circle, by (|k|^2, k_x)
+	int64_t lim[3] = {0, 0, 0};
+	for (int e = 0; e < d; e++) {
+		double a2 = 0.0;
+		for (int x = 0; x < d; x++)
+			a2 += basis[e * d + x] * basis[e * d + x];
+		lim[e] = (int64_t)std::ceil(circ_kmax * std::sqrt(a2) / (2.0 * M_PI));
+		if (lim[e] > 100000)
+			return false;
+	}
+	struct P {
+		int64_t n[3];
+		double k2, kx;
+	};
+	std::vector<P> circle;
+	const double K2 = circ_kmax * circ_kmax, Kmin2 = circ_kmin * circ_kmin;
+	// the reference's odometer order (axis 0 fastest): std::sort below then orders ties as the reference's does
+	int64_t n[3] = {0, 0, 0};
+	for (n[2] = (d == 3 ? -lim[2] : 0); n[2] <= (d == 3 ? lim[2] : 0); n[2]++)
+		for (n[1] = -lim[1]; n[1] <= lim[1]; n[1]++)
+			for (n[0] = -lim[0]; n[0] <= lim[0]; n[0]++) {
+				int first = 0;
+				for (int e = 0; e < d && first == 0; e++)
+					first = n[e] > 0 ? 1 : n[e] < 0 ? -1 : 0;
+				if (first < 0)
+					continue;   // the inverted half (k = 0 fails the k^2 > kmin^2 test below)
+				double k[3];
+				lattice_k(d, recip, n, k);
+				const double k2 = mod2(d, k);
+				if (k2 < K2 && k2 > Kmin2) {
+					circle.push_back({{n[0], n[1], n[2]}, k2, k[0]});
+					if (circle.size() > max_ks)
+						return false;
+				}
+			}
+	std::sort(circle.begin(), circle.end(), [](const P &a, const P &b) {
+		if (a.k2 != b.k2)
+			return a.k2 < b.k2;
+		return a.kx < b.kx;
+	});
+	if (lin_kmax == circ_kmax) {
+		for (const P &q : circle)
+			if (!push(q.n[0], q.n[1], q.n[2], std::sqrt(q.k2)))
+				return false;
+		return true;
+	}
+	// the first point of each lattice direction (directions compared as primitive integer vectors)
+	std::set<std::array<int64_t, 3> > seen;
+	std::vector<P> first;
+	for (const P &q : circle) {
+		int64_t g = 0;
+		for (int e = 0; e < d; e++)
+			g = gcd64(g, q.n[e]);
+		std::array<int64_t, 3> key = {q.n[0] / g, q.n[1] / g, d == 3 ? q.n[2] / g : 0};
+		if (!seen.insert(key).second)
+			continue;
+		first.push_back(q);
+	}
+	const double L2 = lin_kmax * lin_kmax;
+	for (const P &q : first) {
+		double k[3];
+		lattice_k(d, recip, q.n, k);
+		for (int64_t i = 1;; i++) {
+			double t[3];
+			for (int x = 0; x < d; x++)
+				t[x] = (double)i * k[x];
+			const double t2 = mod2(d, t);
+			if (t2 > L2)
+				break;
+			if (keep() && !push(i * q.n[0], i * q.n[1], i * q.n[2], std::sqrt(t2)))
+				return false;
+		}
 	}
 	return true;
 }

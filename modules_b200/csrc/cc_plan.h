@@ -87,4 +87,21 @@ bool cartesian_to_modes(int d, const double *basis, int64_t M, const double *k, 
 bool stealthy_kset(int d, const double *basis, int64_t N, double chi, int type, std::vector<int32_t> &modes,
                    std::vector<double> &V);
 
+// The wavevectors of GetKs (core/PeriodicCellList.cpp:509-735) as integer modes, with |k| formed the way the
+// reference forms it (k = sum_e n_e b_e summed in axis order, |k| = sqrt(k.k)):
+//   d >= 2: the half-space lattice points with circ_kmin^2 < |k|^2 < circ_kmax^2, ordered by (|k|^2, k_x); when
+//           lin_kmax differs from circ_kmax, instead every multiple i k (i >= 1, |i k| <= lin_kmax) of the first of
+//           those points in each lattice direction;
+//   d == 1: the multiples i b (b the reciprocal vector) up to lin_kmax, or, with circ_kmin > 0, the seeds in
+//           (circ_kmin, circ_kmax] followed by their multiples, round by round, until one exceeds lin_kmax.
+// With sample_prob < 1 each candidate of the multiples is kept when a Mersenne Twister seeded with 98765 draws below
+// sample_prob (the reference's RandomGenerator: draw / 2^32). false for a degenerate cell, a 1D cell of non-positive
+// length, or more than max_ks wavevectors.
+// The reciprocal basis rows formed as the reference's cell forms them (core/PeriodicCellList.h:999-1030: projection
+// on the Gram-Schmidt orthogonalised other basis vectors, scaled by 2 pi / (b_i . a_i)); same rounding as there.
+void reciprocal_by_projection(int d, const double *basis, double *recip);
+
+bool isotropic_ks(int d, const double *basis, double circ_kmax, double lin_kmax, double sample_prob, double circ_kmin,
+                  std::vector<int32_t> &modes, std::vector<double> &kamp, size_t max_ks = 50000000);
+
 }  // namespace cc

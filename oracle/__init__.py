@@ -64,6 +64,11 @@ def ref_lib():
         lib.ccref_mc_trymove.argtypes = [_vp, _vp, _vp, ctypes.c_int]
         lib.ccref_kset_cli.restype = _l
         lib.ccref_kset_cli.argtypes = [ctypes.c_int, _vp, _l, _d, ctypes.c_int, _l, _vp, _vp]
+        lib.ccref_getks.restype = _l
+        lib.ccref_getks.argtypes = [ctypes.c_int, _vp, _d, _d, _d, _d, _l, _vp]
+        lib.ccref_isotropic_sk.restype = _l
+        lib.ccref_isotropic_sk.argtypes = [ctypes.c_int, _l, _vp, _vp, _vp, _d, _d, _d, _d, ctypes.c_int, _d, _l,
+                                           _vp]
         _REF = lib
     return _REF
 
@@ -190,3 +195,27 @@ def port_sk(d, basis, frac, kcart):
     S = np.zeros(max(len(kcart), 1))
     lib.cco_sk(d, _p(basis), len(frac), _p(frac), len(kcart), _p(kcart), _p(S))
     return S[: len(kcart)]
+
+
+def ref_getks(d, basis, circ, lin, p=1.0, kmin=0.0, cap=2000000):
+    """GetKs of the reference (restated in oracle/sk_oracle.cpp): Cartesian wavevectors (K x d)."""
+    basis = np.ascontiguousarray(basis, np.float64).reshape(d, d)
+    out = np.zeros((cap, d))
+    K = ref_lib().ccref_getks(d, _p(basis), circ, lin, p, kmin, cap, _p(out))
+    if K < 0:
+        raise ValueError("cap too small")
+    return out[:K]
+
+
+def ref_isotropic_sk(d, bases, fracs, circ, lin, kprec=0.01, p=1.0, option=0, kmin=0.0, cap=200000):
+    """The reference's own IsotropicStructureFactor (pairstat/StructureFactor.cpp): rows (k, S, dk, dS)."""
+    n = len(fracs)
+    B = np.ascontiguousarray(np.asarray(bases, np.float64).reshape(n, d, d))
+    arrs = [np.ascontiguousarray(f, np.float64).reshape(-1, d) for f in fracs]
+    N = np.array([len(a) for a in arrs], dtype=np.int64)
+    ptrs = (_vp * n)(*[a.ctypes.data_as(_vp) for a in arrs])
+    out = np.zeros((cap, 4))
+    R = ref_lib().ccref_isotropic_sk(d, n, _p(B), _p(N), ptrs, circ, lin, kprec, p, option, kmin, cap, _p(out))
+    if R < 0:
+        raise ValueError("cap too small")
+    return out[:R]

@@ -52,4 +52,4 @@ double Volume(const GeometryVector *vecs, DimensionType dimension)
 size_t Verbosity = 0;
 time_t ProgramStart = 0;
 time_t TimeLimit = 0;
-std::ostream logfile(std::cerr.rdbuf());
+std::ostream logfile(nullptr);   // progress bars of the reference code go nowhere
