@@ -222,6 +222,24 @@ int cc_isotropic_structure_factor(int d, int64_t nconfigs, const double *bases, 
                                   double k_precision, double sample_probability, int option, double circular_kmin,
                                   double *results, int64_t cap, int64_t *count);
 
+/* --- multi-species stealthy potential with soft-core contact -----------------------------------------------------
+ * MultiStealthyPotential (apps/CCOptimization/MultiStealthyPotential.h:115-481, .cpp:139-985):
+ *   E   = u0 sum_s (N_s/N) Phi_s + e0 sum_{i<j} sum_images [r < s_ij] (1 - r/s_ij)^2,   s_ij = R_i + R_j,
+ *   F_i = u0 (N_s/N) F_i^(CC,s) + e0 sum_{j != i} sum_images [r < s_ij] (2/s_ij)(1/r - 1/s_ij)(r_i - r_j),
+ * Phi_s the collective-coordinate energy of species s over its own particles (constraint set: M[s] integer modes
+ * modes[s] (M[s] x d) with weights V[s]); coincident particles (r < 1e-15) get the reference's unit push along the
+ * first axis. The contact term is off when |e0| <= 1e-10 (as the reference's WithRepulsion).
+ * cc_multi_set_configuration: N particles at fractional frac (N x d), species[i] in 0..nspecies-1, radii (N, each
+ * > 0) or NULL for the reference's default 0.5. cc_multi_energy_grad: E and, if F is not NULL, Cartesian forces
+ * (N x d). Calls on one object are not thread-safe. */
+typedef struct cc_multi cc_multi;
+int cc_multi_create(int d, const double *basis, int nspecies, const int64_t *M, const int32_t *const *modes,
+                    const double *const *V, double u0, double e0, cc_multi **out);
+int cc_multi_set_configuration(cc_multi *m, int64_t N, const double *frac, const int32_t *species,
+                               const double *radii);
+int cc_multi_energy_grad(cc_multi *m, double *E, double *F);
+int cc_multi_destroy(cc_multi *m);
+
 /* --- allocation-free evaluation (no counterpart in the reference) -----------------------------------------------
  * For callers that cannot allocate GPU memory: processes whose memory manager (a caching allocator, a serving
  * engine with a fixed HBM budget) owns the device's memory and lets no library allocate beside it, and loops that

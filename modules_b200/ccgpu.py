@@ -81,6 +81,10 @@ _SIGS = {
     "cc_energy_grad_device": (_i, [_vp, _i64, _vp, _vp, _vp, _vp, _i, _vp]),
     "cc_kset_stealthy": (_i, [_i, _vp, _i64, _d, _i, _i64, _vp, _vp, ctypes.POINTER(_i64)]),
     "cc_kset_isotropic": (_i, [_i, _vp, _d, _d, _d, _d, _i64, _vp, _vp, ctypes.POINTER(_i64)]),
+    "cc_multi_create": (_i, [_i, _vp, _i, _vp, _vp, _vp, _d, _d, ctypes.POINTER(_vp)]),
+    "cc_multi_set_configuration": (_i, [_vp, _i64, _vp, _vp, _vp]),
+    "cc_multi_energy_grad": (_i, [_vp, ctypes.POINTER(_d), _vp]),
+    "cc_multi_destroy": (_i, [_vp]),
     "cc_isotropic_structure_factor": (_i, [_i, _i64, _vp, _vp, _vp, _d, _d, _d, _d, _i, _d, _vp, _i64,
                                            ctypes.POINTER(_i64)]),
     "cc_set_timing": (_i, [_vp, _i]),
@@ -190,6 +194,45 @@ def isotropic_structure_factor(d, bases, fracs, circular_kmax, linear_kmax, k_pr
     out = np.zeros((max(cap, 1), 4))
     _check(lib.cc_isotropic_structure_factor(*args, _ptr(out), cap, ctypes.byref(cnt)))
     return out[:cnt.value]
+
+
+class CCMulti:
+    """MultiStealthyPotential: species with their own constraint sets (integer modes + weights) over subsets of the
+    particles, plus the soft-core contact repulsion of strength e0; u0 scales the collective-coordinate part."""
+
+    def __init__(self, d, basis, modes_per_species, V_per_species, u0=1.0, e0=1.0):
+        self._lib = load_library()
+        self.d = d
+        basis = np.ascontiguousarray(basis, dtype=np.float64).reshape(d, d)
+        self._modes = [np.ascontiguousarray(m, dtype=np.int32).reshape(-1, d) for m in modes_per_species]
+        self._V = [np.ascontiguousarray(v, dtype=np.float64) for v in V_per_species]
+        S = len(self._V)
+        M = np.array([len(v) for v in self._V], dtype=np.int64)
+        mp = (_vp * S)(*[m.ctypes.data_as(_vp) for m in self._modes])
+        vp = (_vp * S)(*[v.ctypes.data_as(_vp) for v in self._V])
+        h = _vp()
+        _check(self._lib.cc_multi_create(d, _ptr(basis), S, _ptr(M), mp, vp, u0, e0, ctypes.byref(h)))
+        self._h = h
+        self.N = None
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.cc_multi_destroy(self._h)
+            self._h = None
+
+    def set_configuration(self, frac, species, radii=None):
+        frac = np.ascontiguousarray(frac, dtype=np.float64).reshape(-1, self.d)
+        sp = np.ascontiguousarray(species, dtype=np.int32)
+        rad = None if radii is None else np.ascontiguousarray(radii, dtype=np.float64)
+        _check(self._lib.cc_multi_set_configuration(self._h, len(frac), _ptr(frac), _ptr(sp),
+                                                    None if rad is None else _ptr(rad)))
+        self.N = len(frac)
+
+    def energy_and_forces(self, forces=True):
+        E = _d()
+        F = np.empty((max(self.N or 0, 1), self.d)) if forces else None
+        _check(self._lib.cc_multi_energy_grad(self._h, ctypes.byref(E), _ptr(F) if forces else None))
+        return (E.value, F[: self.N]) if forces else (E.value, None)
 
 
 def probe_fma_peak(precision=PREC_FP64):

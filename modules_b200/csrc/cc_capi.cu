@@ -34,6 +34,19 @@ int fail(int code, const std::string &msg)
 	return code;
 }
 
+}  // namespace
+
+namespace cc {
+// Error reporting for the library's other translation units: sets the message cc_last_error() returns.
+int set_error(int code, const char *msg)
+{
+	g_err = msg;
+	return code;
+}
+}  // namespace cc
+
+namespace {
+
 #define CC_CUDA(call)                                                                                         \
 	do {                                                                                                      \
 		cudaError_t e_ = (call);                                                                              \

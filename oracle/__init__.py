@@ -66,6 +66,9 @@ def ref_lib():
         lib.ccref_kset_cli.argtypes = [ctypes.c_int, _vp, _l, _d, ctypes.c_int, _l, _vp, _vp]
         lib.ccref_getks.restype = _l
         lib.ccref_getks.argtypes = [ctypes.c_int, _vp, _d, _d, _d, _d, _l, _vp]
+        lib.ccref_multi_eval.restype = ctypes.c_int
+        lib.ccref_multi_eval.argtypes = [ctypes.c_int, _vp, ctypes.c_int, _vp, _vp, _vp, _d, _d, _l, _vp, _vp, _vp,
+                                         ctypes.POINTER(_d), _vp]
         lib.ccref_isotropic_sk.restype = _l
         lib.ccref_isotropic_sk.argtypes = [ctypes.c_int, _l, _vp, _vp, _vp, _d, _d, _d, _d, ctypes.c_int, _d, _l,
                                            _vp]
@@ -219,3 +222,24 @@ def ref_isotropic_sk(d, bases, fracs, circ, lin, kprec=0.01, p=1.0, option=0, km
     if R < 0:
         raise ValueError("cap too small")
     return out[:R]
+
+
+def ref_multi_eval(d, basis, kcarts, Vs, u0, e0, frac, species, radii=None):
+    """The reference's own MultiStealthyPotential: (E, F) with F Cartesian (N x d)."""
+    basis = np.ascontiguousarray(basis, np.float64).reshape(d, d)
+    S = len(Vs)
+    M = np.array([len(v) for v in Vs], dtype=np.int64)
+    ks = [np.ascontiguousarray(k, np.float64).reshape(-1, d) for k in kcarts]
+    vs = [np.ascontiguousarray(v, np.float64) for v in Vs]
+    kp = (_vp * S)(*[k.ctypes.data_as(_vp) for k in ks])
+    vp = (_vp * S)(*[v.ctypes.data_as(_vp) for v in vs])
+    frac = np.ascontiguousarray(frac, np.float64).reshape(-1, d)
+    sp = np.ascontiguousarray(species, np.int32)
+    rad = None if radii is None else np.ascontiguousarray(radii, np.float64)
+    E = _d()
+    F = np.zeros((max(len(frac), 1), d))
+    rc = ref_lib().ccref_multi_eval(d, _p(basis), S, _p(M), kp, vp, u0, e0, len(frac), _p(frac), _p(sp),
+                                    None if rad is None else _p(rad), ctypes.byref(E), _p(F))
+    if rc != 0:
+        raise ValueError("the reference's MultiStealthyPotential threw")
+    return E.value, F[:len(frac)]

@@ -53,3 +53,16 @@ size_t Verbosity = 0;
 time_t ProgramStart = 0;
 time_t TimeLimit = 0;
 std::ostream logfile(nullptr);   // progress bars of the reference code go nowhere
+
+// GeometryVector's binary I/O (core/GeometryVector.cpp) is named by the SpherePacking file readers that the
+// multi-species potential's translation unit pulls in; the oracle never reads or writes a packing file, so these
+// only write and read the d coordinates as raw doubles.
+void GeometryVector::WriteBinary(std::ostream &ofile, DimensionType dimension) const
+{
+	ofile.write(reinterpret_cast<const char *>(this->x), sizeof(double) * dimension);
+}
+
+void GeometryVector::ReadBinary(std::istream &ifile, DimensionType dimension)
+{
+	ifile.read(reinterpret_cast<char *>(this->x), sizeof(double) * dimension);
+}
