@@ -270,6 +270,9 @@ def run_single_legs(cc, torch):
     pot = cc.CCPotential(d, basis, modes, V)
     frac = np.random.default_rng(11).random((n, d))
     fdev = torch.tensor(frac, dtype=torch.float64, device="cuda")
+    pot.set_path(cc.PATH_NUFFT)
+    msnu, Enu, Fnu = device_eval_ms(torch, pot, n, d, fdev, cc.PREC_FP64)
+    pot.set_path(cc.PATH_SPLIT)   # the direct kernels, FP64 and mixed
     ms64, E64, F64 = device_eval_ms(torch, pot, n, d, fdev, cc.PREC_FP64)
     msmx, Emx, Fmx = device_eval_ms(torch, pot, n, d, fdev, cc.PREC_MIXED)
     pot.set_configuration(frac)
@@ -278,6 +281,9 @@ def run_single_legs(cc, torch):
     pairs = n * len(V)
     out["large_2d_n100000"] = {
         "workload": "2D N=100000 chi=0.20 M=40002 v=1, energy + forces, L2 flushed before each evaluation",
+        "nufft_ms": msnu, "nufft_pairs_per_s_equivalent": pairs / (msnu / 1e3),
+        "nufft_rel_err_E": abs(Enu - E64) / abs(E64),
+        "nufft_max_err_F_over_max_F": float(np.abs(Fnu - F64).max() / np.abs(F64).max()),
         "fp64_ms": ms64, "mixed_ms": msmx, "fp64_pairs_per_s": pairs / (ms64 / 1e3),
         "mixed_pairs_per_s": pairs / (msmx / 1e3),
         "mixed_rel_err_E": abs(Emx - E64) / abs(E64),

@@ -263,11 +263,17 @@ int cc_energy_noalloc(int d, const double *basis, int64_t M, const int32_t *d_mo
 const char *cc_noalloc_last_error(void);
 
 /* --- execution path (no counterpart in the reference) ---------------------------------------------------------
- * CC_PATH_SPLIT (default): three kernels per evaluation (rho, split reduction + energy, forces) chained by
+ * CC_PATH_SPLIT: three kernels per evaluation (rho, split reduction + energy, forces) chained by
  * programmatic dependent launch. CC_PATH_FUSED: problems whose per-particle phase tables fit 64 MiB per layout run
  * as ONE cooperative kernel per evaluation (phases separated by grid barriers whose waits are bounded; larger ones
- * still take the split path). Results agree to rounding; each path repeats bitwise. */
-enum { CC_PATH_SPLIT = 0, CC_PATH_FUSED = 1 };
+ * still take the split path). CC_PATH_NUFFT: energies and forces by non-uniform FFTs (the reference's FINUFFT
+ * backend, CollectiveCoordinatePotential.h:119-1250): a type-1 transform for rho, type-2 transforms for the forces,
+ * "exponential of semicircle" kernel of width 14 on a fine grid of twice the mode range, always in FP64, errors
+ * ~1e-13 of sum |c|; its cost grows with N w^d + grid log(grid) instead of N M, so it wins for many particles and
+ * many modes. CC_PATH_AUTO (the default, as the reference gates its FINUFFT backend): the NUFFT path for an
+ * evaluation whose estimated time is lower there (e.g. 2D N=1e5 with M=4e4 modes), the split path otherwise.
+ * Results agree to rounding; each path repeats bitwise. */
+enum { CC_PATH_SPLIT = 0, CC_PATH_FUSED = 1, CC_PATH_NUFFT = 2, CC_PATH_AUTO = 3 };
 int cc_set_path(cc_handle *h, int path);
 
 /* Synchronise the device and report CC_ERR_TIMEOUT if a bounded grid-barrier wait of an earlier device-path

@@ -62,6 +62,7 @@ class ServeOpts(ctypes.Structure):
 
 
 PREC_SCHEDULE = 2
+PATH_SPLIT, PATH_FUSED, PATH_NUFFT, PATH_AUTO = 0, 1, 2, 3
 STOPVAL_GROUND_STATE = -1.0
 
 _SIGS = {
@@ -376,7 +377,8 @@ class CCPotential:
     AcceptMove = accept_move
 
     def set_path(self, path):
-        """0 = the three-kernel split path (default), 1 = one fused cooperative kernel when the tables fit."""
+        """PATH_AUTO (default): PATH_NUFFT where it is estimated faster, else PATH_SPLIT; PATH_SPLIT: the three-kernel
+        direct path; PATH_FUSED: one cooperative kernel when the tables fit; PATH_NUFFT: non-uniform FFTs (FP64)."""
         _check(self._lib.cc_set_path(self._h, int(path)))
 
     def check_device_error(self):

@@ -11,6 +11,7 @@
 #include "cc_fused.cuh"
 #include "cc_kernels.cuh"
 #include "cc_lbfgs.cuh"
+#include "cc_nufft.cuh"
 #include "cc_plan.h"
 
 #include <algorithm>
@@ -207,6 +208,18 @@ struct cc_handle {
 	size_t partialF_cap = 0;
 	std::vector<std::pair<int, int *> > kstarts;   // even segment splits per count
 	bool use_fused = false;         // cc_set_path
+	bool use_nufft = false;         // cc_set_path(CC_PATH_NUFFT)
+	bool auto_path = true;          // CC_PATH_AUTO (default): the NUFFT path where its estimated time is lower
+	double nu_grid_est = -1.0;      // fine-grid points the NUFFT path would use (computed once)
+	// non-uniform FFT path (cc_nufft.cuh), set up at its first use
+	bool nu_ready = false;
+	cc::NufftDev nu = {};
+	int64_t nu_ngrid = 0;
+	int nu_rho_blocks = 0;
+	int *d_nu_mode_u = nullptr;
+	std::vector<void *> nu_bufs;    // device buffers owned by the NUFFT set-up
+	cufftHandle nu_p1 = 0, nu_p2 = 0;
+	bool nu_p1_ok = false, nu_p2_ok = false;
 	// Monte Carlo: rho in mode order of the bound positions, the trial rho and the device modes
 	int32_t *d_modes = nullptr;
 	double *d_modeV = nullptr;
@@ -916,6 +929,235 @@ int run_fused(cc_handle *h, int64_t N, const double *d_frac, double *d_E, double
 	return launch_fused(h->d, mixed, a, grid, st);
 }
 
+// ---------------------------------------------------------------------------------------------------------------
+// non-uniform FFT path
+// ---------------------------------------------------------------------------------------------------------------
+// Gauss-Legendre nodes and weights on [-1, 1]: Newton's method on the three-term Legendre recurrence from the
+// asymptotic first guesses cos(pi (i + 3/4) / (q + 1/2)).
+void gauss_legendre(int q, std::vector<double> &x, std::vector<double> &w)
+{
+	x.assign(q, 0.0);
+	w.assign(q, 0.0);
+	for (int i = 0; i < q; i++) {
+		double z = std::cos(M_PI * (i + 0.75) / (q + 0.5)), dp = 1.0;
+		for (int it = 0; it < 100; it++) {
+			double p0 = 1.0, p1 = z;
+			for (int k = 2; k <= q; k++) {
+				const double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+				p0 = p1;
+				p1 = p2;
+			}
+			dp = q * (z * p1 - p0) / (z * z - 1.0);
+			const double dz = p1 / dp;
+			z -= dz;
+			if (std::fabs(dz) < 1e-16)
+				break;
+		}
+		x[i] = z;
+		w[i] = 2.0 / ((1.0 - z * z) * dp * dp);
+	}
+}
+
+// Smallest n >= lo whose only prime factors are 2, 3, 5 and 7 (sizes cuFFT transforms fastest), even.
+int fft_size(int lo)
+{
+	for (int n = std::max(lo, 2);; n++) {
+		if (n & 1)
+			continue;
+		int r = n;
+		for (int p : {2, 3, 5, 7})
+			while (r % p == 0)
+				r /= p;
+		if (r == 1)
+			return n;
+	}
+}
+
+template <class T> int nu_alloc(cc_handle *h, T **p, size_t n)
+{
+	if (int rc = dev_alloc(p, n))
+		return rc;
+	h->nu_bufs.push_back(*p);
+	return CC_OK;
+}
+
+int nufft_setup(cc_handle *h)
+{
+	if (h->nu_ready)
+		return CC_OK;
+	const int d = h->d;
+	const int64_t M = (int64_t)h->V.size();
+	// unique modes (sorted) with summed weights, and each input mode's unique index
+	std::vector<int64_t> order((size_t)M);
+	for (int64_t m = 0; m < M; m++)
+		order[m] = m;
+	auto less = [&](int64_t a, int64_t b) {
+		for (int e = 0; e < d; e++)
+			if (h->modes[a * d + e] != h->modes[b * d + e])
+				return h->modes[a * d + e] < h->modes[b * d + e];
+		return a < b;
+	};
+	std::sort(order.begin(), order.end(), less);
+	std::vector<int32_t> um;
+	std::vector<double> uV;
+	std::vector<int> mode_u((size_t)std::max<int64_t>(M, 1), 0);
+	int K[3] = {0, 0, 0};
+	for (int64_t k = 0; k < M; k++) {
+		const int64_t m = order[k];
+		const bool same = k > 0 && std::equal(h->modes.begin() + m * d, h->modes.begin() + (m + 1) * d,
+		                                      h->modes.begin() + order[k - 1] * d);
+		if (!same) {
+			for (int e = 0; e < d; e++) {
+				um.push_back(h->modes[m * d + e]);
+				K[e] = std::max(K[e], std::abs(h->modes[m * d + e]));
+			}
+			uV.push_back(0.0);
+		}
+		uV.back() += h->V[m];
+		mode_u[m] = (int)uV.size() - 1;
+	}
+	const int U = (int)uV.size();
+	cc::NufftDev &a = h->nu;
+	a = cc::NufftDev();
+	a.beta = cc::kNufftBetaPerW * cc::kNufftW;
+	int64_t ngrid = 1;
+	for (int e = 0; e < 3; e++) {
+		a.nf[e] = 1;
+		a.K[e] = 0;
+	}
+	for (int e = 0; e < d; e++) {
+		a.K[e] = K[e];
+		a.nf[e] = fft_size(std::max(2 * (2 * K[e] + 1), 2 * cc::kNufftW));
+		ngrid *= a.nf[e];
+	}
+	if (ngrid > ((int64_t)1 << 28))
+		return fail(CC_ERR_ARG, "the k-set's fine grid is too large for the NUFFT path");
+	// phihat_e(n) = 2 int_0^{w/2} phi(t) cos(2 pi n t / nf_e) dt by Gauss-Legendre quadrature
+	std::vector<double> gx, gw;
+	gauss_legendre(4 * cc::kNufftW + 40, gx, gw);
+	for (int e = 0; e < d; e++) {
+		std::vector<double> ph((size_t)(2 * K[e] + 1));
+		for (int n = -K[e]; n <= K[e]; n++) {
+			double acc = 0.0;
+			for (size_t q = 0; q < gx.size(); q++) {
+				const double t = 0.25 * cc::kNufftW * (gx[q] + 1.0), wt = 0.25 * cc::kNufftW * gw[q];
+				const double z = 1.0 - (2.0 * t / cc::kNufftW) * (2.0 * t / cc::kNufftW);
+				const double phi = z > 0 ? std::exp(a.beta * (std::sqrt(z) - 1.0)) : 0.0;
+				acc += wt * phi * std::cos(2.0 * M_PI * n * t / a.nf[e]);
+			}
+			ph[n + K[e]] = 2.0 * acc;
+		}
+		double *dp = nullptr;
+		if (int rc = nu_alloc(h, &dp, ph.size()))
+			return rc;
+		CC_CUDA(cudaMemcpy(dp, ph.data(), ph.size() * sizeof(double), cudaMemcpyHostToDevice));
+		a.phihat[e] = dp;
+	}
+	int32_t *d_um = nullptr;
+	double *d_uV = nullptr;
+	unsigned long long *gi = nullptr;
+	double *gr = nullptr, *epart = nullptr;
+	double2 *spec = nullptr, *coef = nullptr, *rho_u = nullptr, *u_u = nullptr;
+	const int64_t nspec = ngrid / a.nf[d - 1] * (a.nf[d - 1] / 2 + 1);
+	const int nblk = std::max(1, (U + 255) / 256);
+	int rc;
+	if ((rc = nu_alloc(h, &d_um, (size_t)std::max(U, 1) * d)) || (rc = nu_alloc(h, &d_uV, (size_t)std::max(U, 1))) ||
+	    (rc = nu_alloc(h, &gi, (size_t)ngrid)) || (rc = nu_alloc(h, &gr, (size_t)ngrid)) ||
+	    (rc = nu_alloc(h, &spec, (size_t)nspec)) || (rc = nu_alloc(h, &coef, (size_t)ngrid * d)) ||
+	    (rc = nu_alloc(h, &rho_u, (size_t)std::max(U, 1))) || (rc = nu_alloc(h, &u_u, (size_t)std::max(U, 1))) ||
+	    (rc = nu_alloc(h, &epart, (size_t)nblk)) || (rc = nu_alloc(h, &h->d_nu_mode_u, mode_u.size())))
+		return rc;
+	if (U > 0) {
+		CC_CUDA(cudaMemcpy(d_um, um.data(), um.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+		CC_CUDA(cudaMemcpy(d_uV, uV.data(), uV.size() * sizeof(double), cudaMemcpyHostToDevice));
+	}
+	CC_CUDA(cudaMemcpy(h->d_nu_mode_u, mode_u.data(), mode_u.size() * sizeof(int), cudaMemcpyHostToDevice));
+	a.U = U;
+	a.umodes = d_um;
+	a.uV = d_uV;
+	a.gi = gi;
+	a.gr = gr;
+	a.spec = spec;
+	a.coef = coef;
+	a.rho_u = rho_u;
+	a.u_u = u_u;
+	a.epart = epart;
+	int dims[3] = {a.nf[0], a.nf[1], a.nf[2]};
+	if (cufftPlanMany(&h->nu_p1, d, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, 1) != CUFFT_SUCCESS)
+		return fail(CC_ERR_CUDA, "cufftPlanMany (D2Z) failed");
+	h->nu_p1_ok = true;
+	if (cufftPlanMany(&h->nu_p2, d, dims, nullptr, 1, (int)ngrid, nullptr, 1, (int)ngrid, CUFFT_Z2Z, d) !=
+	    CUFFT_SUCCESS)
+		return fail(CC_ERR_CUDA, "cufftPlanMany (Z2Z) failed");
+	h->nu_p2_ok = true;
+	h->nu_ngrid = ngrid;
+	h->nu_rho_blocks = nblk;
+	h->nu_ready = true;
+	return CC_OK;
+}
+
+template <int D>
+int run_nufft_t(cc_handle *h, int64_t N, const double *d_frac, double *d_E, double *d_F, double *d_gfrac,
+                bool want_rho_mode, cudaStream_t st)
+{
+	cc::NufftDev a = h->nu;
+	a.skip = h->d_skip;
+	const int64_t ngrid = h->nu_ngrid;
+	CC_CUDA(cudaMemsetAsync(a.gi, 0, sizeof(unsigned long long) * ngrid, st));
+	if (N > 0) {
+		const int64_t items = N * cc::kNufftW;
+		cc::nufft_spread_kernel<D><<<(unsigned)((items + cc::kNufftThreads - 1) / cc::kNufftThreads), cc::kNufftThreads,
+		                             0, st>>>(a, d_frac, (int)N);
+		CC_CUDA(cudaGetLastError());
+	}
+	cc::nufft_fix_to_double_kernel<<<(unsigned)((ngrid + 255) / 256), 256, 0, st>>>(a, ngrid);
+	CC_CUDA(cudaGetLastError());
+	if (cufftSetStream(h->nu_p1, st) != CUFFT_SUCCESS ||
+	    cufftExecD2Z(h->nu_p1, a.gr, reinterpret_cast<cufftDoubleComplex *>(const_cast<double2 *>(a.spec))) !=
+	        CUFFT_SUCCESS)
+		return fail(CC_ERR_CUDA, "cufftExecD2Z failed");
+	cc::nufft_rho_kernel<D><<<h->nu_rho_blocks, 256, 0, st>>>(a, h->rho_offset);
+	CC_CUDA(cudaGetLastError());
+	cc::nufft_energy_kernel<<<1, 32, 0, st>>>(a, h->nu_rho_blocks, 1.0 / h->volume, h->shift, d_E);
+	CC_CUDA(cudaGetLastError());
+	const int M = (int)h->V.size();
+	if (want_rho_mode && M > 0) {
+		cc::nufft_gather_rho_kernel<<<(M + 255) / 256, 256, 0, st>>>(a.rho_u, h->d_nu_mode_u, M, h->main.rho_mode);
+		CC_CUDA(cudaGetLastError());
+	}
+	if (!(d_F || d_gfrac) || N == 0)
+		return CC_OK;
+	CC_CUDA(cudaMemsetAsync(a.coef, 0, sizeof(double2) * ngrid * D, st));
+	cc::nufft_coef_kernel<D><<<h->nu_rho_blocks, 256, 0, st>>>(a, ngrid);
+	CC_CUDA(cudaGetLastError());
+	if (cufftSetStream(h->nu_p2, st) != CUFFT_SUCCESS ||
+	    cufftExecZ2Z(h->nu_p2, reinterpret_cast<cufftDoubleComplex *>(a.coef),
+	                 reinterpret_cast<cufftDoubleComplex *>(a.coef), CUFFT_INVERSE) != CUFFT_SUCCESS)
+		return fail(CC_ERR_CUDA, "cufftExecZ2Z failed");
+	cc::NufftOut o;
+	for (int i = 0; i < 9; i++)
+		o.recip[i] = h->recip[i];
+	o.fscale = 2.0 / h->volume;
+	o.F_out = d_F;
+	o.gfrac_out = d_gfrac;
+	cc::nufft_interp_kernel<D><<<(unsigned)((N + cc::kNufftThreads - 1) / cc::kNufftThreads), cc::kNufftThreads, 0,
+	                             st>>>(a, d_frac, (int)N, ngrid, o);
+	CC_CUDA(cudaGetLastError());
+	return CC_OK;
+}
+
+int run_nufft(cc_handle *h, int64_t N, const double *d_frac, double *d_E, double *d_F, double *d_gfrac,
+              bool want_rho_mode, cudaStream_t st)
+{
+	if (int rc = nufft_setup(h))
+		return rc;
+	switch (h->d) {
+	case 1: return run_nufft_t<1>(h, N, d_frac, d_E, d_F, d_gfrac, want_rho_mode, st);
+	case 2: return run_nufft_t<2>(h, N, d_frac, d_E, d_F, d_gfrac, want_rho_mode, st);
+	default: return run_nufft_t<3>(h, N, d_frac, d_E, d_F, d_gfrac, want_rho_mode, st);
+	}
+}
+
 // A grid barrier of an earlier fused launch that ran out of time leaves its error word set: report it and reset.
 int check_barrier(cc_handle *h, bool always = false)
 {
@@ -1011,6 +1253,36 @@ cudaEvent_t next_event(cc_handle *h)
 	return h->ev[h->ev_used++];
 }
 
+// CC_PATH_AUTO: the NUFFT path when its estimated time is below the direct path's. Direct: N x slots at 700 G
+// pairs/s; NUFFT: 2e-11 d s per particle and kernel point (spread + interpolation, W^d points), 2e-10 s per fine-grid
+// point and transform, 30 us of launches. The constants are conservative fits of B200 timings (2D N=1e5 M=40002:
+// 0.38 ms NUFFT against 5.1 ms direct; 3D N=2000 M=2724: 25 us direct).
+bool nufft_preferred(cc_handle *h, int64_t N)
+{
+	if (h->main.plan.nslot == 0 || N < 1024)
+		return false;
+	const int d = h->d;
+	if (h->nu_grid_est < 0) {
+		double grid = 1.0;
+		for (int e = 0; e < d; e++) {
+			int K = 0;
+			for (size_t m = e; m < h->modes.size(); m += d)
+				K = std::max(K, std::abs(h->modes[m]));
+			grid *= fft_size(std::max(2 * (2 * K + 1), 2 * cc::kNufftW));
+		}
+		h->nu_grid_est = grid;
+	}
+	const double grid = h->nu_grid_est;
+	double w = 1.0;
+	for (int e = 0; e < d; e++)
+		w *= cc::kNufftW;
+	if (grid > (double)((int64_t)1 << 28))
+		return false;
+	const double direct = (double)N * (double)h->main.plan.real_segs * h->main.plan.L / 7e11;
+	const double nufft = 2e-11 * d * (double)N * w + 2e-10 * grid * (1 + d) + 3e-5;
+	return nufft < direct;
+}
+
 int eval_device(cc_handle *h, int64_t N, const double *d_frac, double *d_E, double *d_F, double *d_gfrac,
                 bool want_rho_mode, int precision, cudaStream_t st)
 {
@@ -1025,6 +1297,17 @@ int eval_device(cc_handle *h, int64_t N, const double *d_frac, double *d_E, doub
 		if (!(e0 && e1 && e2 && e3))
 			return fail(CC_ERR_CUDA, "cudaEventCreate failed");
 		CC_CUDA(record_timing(e0, st));
+	}
+	if ((h->use_nufft || (h->auto_path && nufft_preferred(h, N))) && h->main.plan.nslot > 0) {
+		// non-uniform FFT path (FP64 whatever the precision): reported as the force interval
+		if (e1)
+			CC_CUDA(record_timing(e1, st));
+		if (e2)
+			CC_CUDA(record_timing(e2, st));
+		int rc = run_nufft(h, N, d_frac, d_E, d_F, d_gfrac, want_rho_mode, st);
+		if (e3)
+			CC_CUDA(record_timing(e3, st));
+		return rc;
 	}
 	if (!want_rho_mode && h->use_fused && !h->d_skip && fused_eligible(h, N, mixed)) {
 		// one cooperative launch: the whole evaluation is reported as the force interval
@@ -1226,6 +1509,12 @@ int cc_destroy(cc_handle *h)
 		cudaEventDestroy(e);
 	for (auto &g : h->graphs)
 		cudaGraphExecDestroy(g.exec);
+	if (h->nu_p1_ok)
+		cufftDestroy(h->nu_p1);
+	if (h->nu_p2_ok)
+		cufftDestroy(h->nu_p2);
+	for (void *b : h->nu_bufs)
+		cudaFree(b);
 	if (h->stream)
 		cudaStreamDestroy(h->stream);
 	delete h;
@@ -1352,9 +1641,14 @@ int cc_rho(cc_handle *h, double *re, double *im, int precision)
 		return rc;
 	const int64_t N = h->N;
 	const size_t M = h->V.size();
-	const Launch l = choose_launch(h->main.plan, N, precision == CC_PREC_MIXED);
-	if (int rc = run_rho(h, h->main, N, h->d_frac, h->d_E, true, precision == CC_PREC_MIXED, l, h->stream))
-		return rc;
+	if ((h->use_nufft || (h->auto_path && nufft_preferred(h, N))) && h->main.plan.nslot > 0) {
+		if (int rc = run_nufft(h, N, h->d_frac, h->d_E, nullptr, nullptr, true, h->stream))
+			return rc;
+	} else {
+		const Launch l = choose_launch(h->main.plan, N, precision == CC_PREC_MIXED);
+		if (int rc = run_rho(h, h->main, N, h->d_frac, h->d_E, true, precision == CC_PREC_MIXED, l, h->stream))
+			return rc;
+	}
 	if (M == 0)
 		return CC_OK;
 	std::vector<double2> tmp(M);
@@ -1540,9 +1834,12 @@ int cc_set_path(cc_handle *h, int path)
 {
 	if (int rc = check_handle(h))
 		return rc;
-	if (path != CC_PATH_SPLIT && path != CC_PATH_FUSED)
-		return fail(CC_ERR_ARG, "path must be CC_PATH_SPLIT or CC_PATH_FUSED");
+	if (path != CC_PATH_SPLIT && path != CC_PATH_FUSED && path != CC_PATH_NUFFT && path != CC_PATH_AUTO)
+		return fail(CC_ERR_ARG, "path must be CC_PATH_SPLIT, CC_PATH_FUSED, CC_PATH_NUFFT or CC_PATH_AUTO");
 	h->use_fused = path == CC_PATH_FUSED;
+	h->use_nufft = path == CC_PATH_NUFFT;
+	h->auto_path = path == CC_PATH_AUTO;
+	g_alloc_gen++;   // captured evaluations hold the old path
 	return CC_OK;
 }
 

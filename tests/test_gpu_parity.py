@@ -191,9 +191,11 @@ def test_mixed_precision_error(gpu):
     assert rel_E < 1e-5 and rel_F < 1e-4
 
 
-def test_large_size_properties(gpu):
+@pytest.mark.parametrize("path", ["split", "auto"])
+def test_large_size_properties(gpu, path):
     """2D N=1e5 chi=0.20 (M=40002, 4e9 pairs): properties that hold at any size: total force zero,
-    translation invariance of E and F, mixed path close to FP64."""
+    translation invariance of E and F, and (direct path) mixed precision close to FP64. The default path takes the
+    NUFFT route at this size."""
     N = 100000
     side = np.sqrt(N)
     modes, V = gpu.stealthy_kset(2, np.eye(2) * side, N, 0.20)
@@ -201,6 +203,7 @@ def test_large_size_properties(gpu):
     rng = np.random.default_rng(5)
     frac = rng.random((N, 2))
     p = gpu.CCPotential(2, np.eye(2) * side, modes, V)
+    p.set_path(gpu.PATH_SPLIT if path == "split" else gpu.PATH_AUTO)
     p.set_configuration(frac)
     E, F = p.energy_and_forces()
     assert np.abs(F.sum(0)).max() <= 1e-9 * np.abs(F).sum(0).max()
@@ -208,6 +211,8 @@ def test_large_size_properties(gpu):
     E2, F2 = p.energy_and_forces()
     assert abs(E2 - E) <= 1e-10 * E
     assert np.abs(F2 - F).max() <= 1e-9 * np.abs(F).max()
+    if path != "split":
+        return
     p.set_configuration(frac)
     E3, F3 = p.energy_and_forces(precision=gpu.PREC_MIXED)
     print(f"N=1e5 mixed vs fp64: rel dE={abs(E3 - E) / E:.2e} rel dF={np.abs(F3 - F).max() / np.abs(F).max():.2e}")
