@@ -339,6 +339,23 @@ Launch choose_launch(const cc::Plan &p, int64_t N, bool mixed)
 // ---------------------------------------------------------------------------------------------------------------
 // kernel dispatch
 // ---------------------------------------------------------------------------------------------------------------
+// The same for kernels of several arguments.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl_n(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args... args)
+{
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = grid;
+	cfg.blockDim = block;
+	cfg.dynamicSmemBytes = smem;
+	cfg.stream = st;
+	cudaLaunchAttribute attr[1];
+	attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+	attr[0].val.programmaticStreamSerializationAllowed = 1;
+	cfg.attrs = attr;
+	cfg.numAttrs = 1;
+	return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 // Launch with programmatic stream serialization: the kernel may be scheduled while the previous kernel on the stream
 // drains; it calls cudaGridDependencySynchronize() before it reads that kernel's results.
 template <typename Kern, typename Arg>
@@ -676,7 +693,7 @@ int run_rho(cc_handle *h, DevKSet &k, int64_t N, const double *d_frac, double *d
 	const int rows = nsplit / csize;
 	if (int rc = ensure_partial(k, (size_t)rows * p.nslot))
 		return rc;
-	cc::RhoArgs a;
+	cc::RhoArgs a = {};
 	a.frac = d_frac;
 	a.N = (int)N;
 	a.per_split = N > 0 ? l.per_split : 0;
@@ -692,7 +709,7 @@ int run_rho(cc_handle *h, DevKSet &k, int64_t N, const double *d_frac, double *d
 		return rc;
 	if (after_rho)
 		CC_CUDA(record_timing(after_rho, st));
-	cc::ReduceArgs r;
+	cc::ReduceArgs r = {};
 	r.partial = k.partial;
 	r.nsplit = rows;
 	r.nslot = p.nslot;
@@ -739,7 +756,7 @@ int run_force(cc_handle *h, int64_t N, const double *d_frac, double *d_F, double
 		if (rc)
 			return rc;
 	}
-	cc::ForceArgs a;
+	cc::ForceArgs a = {};
 	a.frac = d_frac;
 	a.N = (int)N;
 	a.segs = h->main.segs;
@@ -2141,96 +2158,109 @@ struct Arena {
 	template <class T> T *at(size_t off) { return reinterpret_cast<T *>(base + off); }
 };
 
+// One dimension's instances of a batch, evaluated by the multi-instance rho / reduce / force kernels: per instance
+// the arguments of each kernel (set 0: the batch positions and outputs; set 1: a minimisation's trial points), the
+// prefix sums of the blocks of each launch and the grid shapes.
 struct BatchGroup {
 	int D = 0;
 	std::vector<int> members;            // instance indices
-	cc::BInst *d_inst = nullptr;         // evaluation descriptors (batch positions)
-	cc::BInst *d_inst_lb = nullptr;      // minimisation descriptors (L-BFGS trial points)
-	int *d_pre = nullptr;                // 4 x (B + 1)
-	int total[4] = {0, 0, 0, 0};
+	cc::RhoArgs *d_rho[2] = {nullptr, nullptr};
+	cc::ReduceArgs *d_red[2] = {nullptr, nullptr};
+	cc::ForceArgs *d_force[2] = {nullptr, nullptr};
+	int *d_pre = nullptr;                // 3 x (B + 1): rho, reduce and force blocks
+	int *d_shape = nullptr;              // 3 x B: block groups, reduce chunks, particle groups
+	unsigned *d_queue = nullptr;         // 2 words per launch kind: work queues of the persistent launches
+	int total[3] = {0, 0, 0};
+	int rho_row = 1, force_row = 1;      // largest table rows (shared memory of the launches)
+	std::vector<cc::RhoArgs> rho;        // host copies of set 0
+	std::vector<cc::ReduceArgs> red;
+	std::vector<cc::ForceArgs> force;
 };
+
+constexpr int kBatchChunk = 16;          // particles whose rho tables are built at once in a batch
+constexpr int kBatchPerSplit = 64;       // particles per rho block of a batch instance
+constexpr int kBatchSegsPerSplit = 64;   // segments per force block of a batch instance
 
 }  // namespace
 
 struct cc_batch {
 	std::vector<cc_handle *> h;
 	std::vector<int64_t> N;
-	std::vector<cc::BInst> inst;         // host copies (evaluation descriptors)
 	std::vector<BatchGroup> groups;
 	Arena arena;
 	std::vector<size_t> off_frac, off_F, off_E;
 	cudaStream_t stream = nullptr;
-	unsigned *d_bar = nullptr;
 };
 
 namespace {
 
-template <int D, bool MIXED> int batch_grid(int *grid)
+template <int D, bool MIXED> cudaError_t multi_attrs()
 {
-	static int per_sm = -1;
-	if (per_sm < 0) {
-		CC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cc::cc_batch_kernel<D, 8, MIXED>,
-		                                                     cc::kFusedThreads, 0));
-		if (per_sm < 1)
-			return fail(CC_ERR_CUDA, "batch kernel cannot be resident");
-	}
-	*grid = per_sm * sm_count();
+	typedef typename std::conditional<MIXED, float2, double2>::type C;
+	static cudaError_t e = [] {
+		cudaError_t r = cudaFuncSetAttribute(cc::cc_mrho_kernel<D, 8, MIXED>,
+		                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                                     (int)rho_smem<C>(cc::kMaxRow, kBatchChunk, 8));
+		if (r == cudaSuccess)
+			r = cudaFuncSetAttribute(cc::cc_mforce_kernel<D, 8, MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			                         (int)force_smem<C>(cc::kMaxRow, D));
+		return r;
+	}();
+	return e;
+}
+
+// the three launches of one group: which = 0 (batch positions) or 1 (minimisation trial points)
+template <int D, bool MIXED> int multi_launch_t(BatchGroup &g, int which, cudaStream_t st)
+{
+	typedef typename std::conditional<MIXED, float2, double2>::type C;
+	if (cudaError_t e = multi_attrs<D, MIXED>())
+		return fail(CC_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+	const int B = (int)g.members.size(), want = MIXED ? 0 : 1;
+	const int *pre = g.d_pre, *shape = g.d_shape;
+	// persistent grids: at most the resident blocks (3 per SM for rho and force, 8 for the reduction)
+	const int res3 = 3 * sm_count(), res8 = 8 * sm_count();
+	if (g.total[0] > 0)
+		CC_CUDA(launch_pdl_n(cc::cc_mrho_kernel<D, 8, MIXED>, dim3(std::min(g.total[0], res3)), dim3(cc::kRhoThreads),
+		                   rho_smem<C>(g.rho_row, kBatchChunk, 8), st, (const cc::RhoArgs *)g.d_rho[which], pre,
+		                   shape, B, want, g.d_queue));
+	if (g.total[1] > 0)
+		CC_CUDA(launch_pdl_n(cc::cc_mreduce_kernel, dim3(std::min(g.total[1], res8)), dim3(cc::kRedThreads), 0, st,
+		                   (const cc::ReduceArgs *)g.d_red[which], pre + (B + 1), shape + B, B, want, g.d_queue + 2));
+	if (g.total[2] > 0)
+		CC_CUDA(launch_pdl_n(cc::cc_mforce_kernel<D, 8, MIXED>, dim3(std::min(g.total[2], res3)), dim3(cc::kForceThreads),
+		                   force_smem<C>(g.force_row, D), st, (const cc::ForceArgs *)g.d_force[which],
+		                   pre + 2 * (B + 1), shape + 2 * B, B, want, g.d_queue + 4));
 	return CC_OK;
 }
 
-template <int D, bool MIXED> int batch_launch_t(cc::BatchArgs &a, cudaStream_t st)
+int multi_launch(BatchGroup &g, bool mixed, int which, cudaStream_t st)
 {
-	int grid = 0;
-	if (int rc = batch_grid<D, MIXED>(&grid))
-		return rc;
-	void *args[] = {&a};
-	CC_CUDA(cudaLaunchCooperativeKernel((const void *)cc::cc_batch_kernel<D, 8, MIXED>, dim3(grid),
-	                                    dim3(cc::kFusedThreads), args, 0, st));
-	return CC_OK;
-}
-
-int batch_launch(int D, bool mixed, cc::BatchArgs &a, cudaStream_t st)
-{
-	switch (D) {
-	case 1: return mixed ? batch_launch_t<1, true>(a, st) : batch_launch_t<1, false>(a, st);
-	case 2: return mixed ? batch_launch_t<2, true>(a, st) : batch_launch_t<2, false>(a, st);
-	default: return mixed ? batch_launch_t<3, true>(a, st) : batch_launch_t<3, false>(a, st);
+	switch (g.D) {
+	case 1: return mixed ? multi_launch_t<1, true>(g, which, st) : multi_launch_t<1, false>(g, which, st);
+	case 2: return mixed ? multi_launch_t<2, true>(g, which, st) : multi_launch_t<2, false>(g, which, st);
+	default: return mixed ? multi_launch_t<3, true>(g, which, st) : multi_launch_t<3, false>(g, which, st);
 	}
 }
 
 // evaluate every group with the given descriptors (lb = the minimisation's); precision CC_PREC_SCHEDULE launches
-// the mixed and the FP64 kernel, each evaluating the instances of its stage
+// the mixed and the FP64 kernels, each evaluating the instances of its stage
 int batch_eval(cc_batch *b, bool lb, int precision, cudaStream_t st)
 {
 	for (BatchGroup &g : b->groups) {
-		cc::BatchArgs a;
-		a.inst = lb ? g.d_inst_lb : g.d_inst;
-		a.B = (int)g.members.size();
-		for (int k = 0; k < 4; k++)
-			a.pre[k] = g.d_pre + k * (a.B + 1);
-		a.bar = b->d_bar;
 		if (precision == CC_PREC_SCHEDULE) {
-			if (int rc = batch_launch(g.D, true, a, st))
+			if (int rc = multi_launch(g, true, lb ? 1 : 0, st))
 				return rc;
-			if (int rc = batch_launch(g.D, false, a, st))
+			if (int rc = multi_launch(g, false, lb ? 1 : 0, st))
 				return rc;
-		} else if (int rc = batch_launch(g.D, precision == CC_PREC_MIXED, a, st)) {
+		} else if (int rc = multi_launch(g, precision == CC_PREC_MIXED, lb ? 1 : 0, st)) {
 			return rc;
 		}
 	}
 	return CC_OK;
 }
 
-int batch_check_barrier(cc_batch *b)
-{
-	unsigned w[3] = {0, 0, 0};
-	CC_CUDA(cudaMemcpy(w, b->d_bar, sizeof(w), cudaMemcpyDeviceToHost));
-	if (w[2] != 0u) {
-		CC_CUDA(cudaMemset(b->d_bar, 0, 3 * sizeof(unsigned)));
-		return fail(CC_ERR_TIMEOUT, "a grid barrier wait ran out in the batch kernel");
-	}
-	return CC_OK;
-}
+// the multi-instance kernels wait on nothing: no device timeout can be pending
+int batch_check_barrier(cc_batch *) { return CC_OK; }
 
 }  // namespace
 
@@ -2247,9 +2277,13 @@ int cc_batch_create(int count, cc_handle *const *handles, const int64_t *N, cc_b
 	cc_batch *b = new cc_batch();
 	b->h.assign(handles, handles + count);
 	b->N.assign(N, N + count);
-	b->inst.resize(count);
-	// sizes
-	std::vector<size_t> o_tabP(count), o_tabE(count), o_part(count), o_u(count), o_ep(count), o_pg(count), o_fc(count);
+	// per instance: launch shapes, force splits (cached on the handle's k-set) and buffer offsets in one arena
+	struct Sizes {
+		int nsplit, nchunks, pgroups, nks, max_row;
+		const DevSplits *f;
+		size_t o_part, o_rho, o_u, o_eb, o_tk, o_pg, o_fc;
+	};
+	std::vector<Sizes> z(count);
 	b->off_frac.resize(count);
 	b->off_F.resize(count);
 	b->off_E.resize(count);
@@ -2257,66 +2291,38 @@ int cc_batch_create(int count, cc_handle *const *handles, const int64_t *N, cc_b
 		cc_handle *h = handles[i];
 		const cc::Plan &p = h->main.plan;
 		const int64_t n = N[i];
-		const int Npad = (int)((n + 31) / 32 * 32);
-		const int rowP = h->gspec.row | 1;
-		const int nsplit = (int)((n + cc::kBatchSplit - 1) / cc::kBatchSplit);
-		const int nks = std::max(1, (int)(p.segs.size() + cc::kBatchSegs - 1) / cc::kBatchSegs);
+		Sizes &q = z[i];
+		q.nsplit = (int)((n + kBatchPerSplit - 1) / kBatchPerSplit);
+		q.nchunks = (p.nslot + 31) / 32;
+		q.pgroups = (int)((n + 31) / 32);
+		const int want = (int)std::max<int64_t>(1, (p.real_segs + kBatchSegsPerSplit - 1) / kBatchSegsPerSplit);
+		if (int rc = get_splits(h->main, want, &q.f)) {
+			delete b;
+			return rc;
+		}
+		q.nks = q.f->host.count();
+		q.max_row = q.f->host.max_row;
 		b->off_frac[i] = b->arena.take(sizeof(double) * n * h->d);
 		b->off_F[i] = b->arena.take(sizeof(double) * n * h->d);
 		b->off_E[i] = b->arena.take(sizeof(double));
-		o_tabP[i] = b->arena.take(sizeof(double2) * (size_t)rowP * Npad);
-		o_tabE[i] = b->arena.take(sizeof(double2) * (size_t)h->gspec.row * Npad);
-		o_part[i] = b->arena.take(sizeof(double2) * (size_t)nsplit * p.nslot);
-		o_u[i] = b->arena.take(sizeof(double2) * p.nslot);
-		o_ep[i] = b->arena.take(sizeof(double) * ((p.nslot + 255) / 256));
-		o_pg[i] = b->arena.take(sizeof(double) * (size_t)nks * n * h->d);
-		o_fc[i] = b->arena.take(sizeof(unsigned) * ((n + 31) / 32));
+		q.o_part = b->arena.take(sizeof(double2) * (size_t)q.nsplit * p.nslot);
+		q.o_rho = b->arena.take(sizeof(double2) * p.nslot);
+		q.o_u = b->arena.take(sizeof(double2) * p.nslot);
+		q.o_eb = b->arena.take(sizeof(double) * q.nchunks);
+		q.o_tk = b->arena.take(sizeof(unsigned));
+		q.o_pg = b->arena.take(sizeof(double) * (size_t)q.nks * n * h->d);
+		q.o_fc = b->arena.take(sizeof(unsigned) * q.pgroups);
 	}
 	int rc;
-	if ((rc = dev_alloc(&b->arena.base, b->arena.used)) || (rc = dev_alloc(&b->d_bar, 4))) {
+	if ((rc = dev_alloc(&b->arena.base, b->arena.used))) {
 		cc_batch_destroy(b);
 		return rc;
 	}
 	b->arena.cap = b->arena.used;
-	if (cudaMemset(b->arena.base, 0, b->arena.used) != cudaSuccess || cudaMemset(b->d_bar, 0, 16) != cudaSuccess ||
+	if (cudaMemset(b->arena.base, 0, b->arena.used) != cudaSuccess ||
 	    cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
 		cc_batch_destroy(b);
 		return fail(CC_ERR_CUDA, "batch initialisation failed");
-	}
-	for (int i = 0; i < count; i++) {
-		cc_handle *h = handles[i];
-		const cc::Plan &p = h->main.plan;
-		cc::BInst &in = b->inst[i];
-		std::memset(&in, 0, sizeof(in));
-		in.frac = b->arena.at<double>(b->off_frac[i]);
-		in.E_out = b->arena.at<double>(b->off_E[i]);
-		in.F_out = b->arena.at<double>(b->off_F[i]);
-		in.gfrac_out = nullptr;
-		in.status = nullptr;
-		in.N = (int)N[i];
-		in.Npad = (int)((N[i] + 31) / 32 * 32);
-		in.segs = h->main.segs;
-		in.ngroups = p.ngroups();
-		in.nseg = (int)p.segs.size();
-		in.nslot = p.nslot;
-		in.slotV = h->main.slotV;
-		in.rho_offset = h->rho_offset;
-		in.inv_vol = 1.0 / h->volume;
-		in.shift = h->shift;
-		in.spec = h->gspec;
-		in.tabP = b->arena.at<void>(o_tabP[i]);
-		in.tabE = b->arena.at<void>(o_tabE[i]);
-		in.nsplit = (int)((N[i] + cc::kBatchSplit - 1) / cc::kBatchSplit);
-		in.partial = b->arena.at<double2>(o_part[i]);
-		in.u_slot = b->arena.at<double2>(o_u[i]);
-		in.epart = b->arena.at<double>(o_ep[i]);
-		in.nechunk = (p.nslot + 255) / 256;
-		in.nks = std::max(1, (int)(p.segs.size() + cc::kBatchSegs - 1) / cc::kBatchSegs);
-		in.partialG = b->arena.at<double>(o_pg[i]);
-		in.fcounters = b->arena.at<unsigned>(o_fc[i]);
-		for (int k = 0; k < 9; k++)
-			in.recip[k] = h->recip[k];
-		in.fscale = 2.0 / h->volume;
 	}
 	// one group per dimension
 	for (int D = 1; D <= 3; D++) {
@@ -2327,20 +2333,82 @@ int cc_batch_create(int count, cc_handle *const *handles, const int64_t *N, cc_b
 				g.members.push_back(i);
 		if (g.members.empty())
 			continue;
+		// largest instances first: the work queues then hand out the longest items first
+		std::stable_sort(g.members.begin(), g.members.end(), [&](int x, int y) {
+			return (double)N[x] * handles[x]->main.plan.real_segs > (double)N[y] * handles[y]->main.plan.real_segs;
+		});
 		const int B = (int)g.members.size();
-		std::vector<int> pre(4 * (B + 1), 0);
-		std::vector<cc::BInst> gi;
+		std::vector<int> pre(3 * (B + 1), 0), shape(3 * B, 0);
 		for (int k = 0; k < B; k++) {
-			const cc::BInst &in = b->inst[g.members[k]];
-			const int c[4] = {(in.N * in.spec.items + cc::kFusedThreads - 1) / cc::kFusedThreads, in.ngroups * in.nsplit,
-			                  in.nechunk, ((in.N + 31) / 32) * in.nks};
-			for (int ph = 0; ph < 4; ph++)
+			const int i = g.members[k];
+			cc_handle *h = handles[i];
+			const cc::Plan &p = h->main.plan;
+			const Sizes &q = z[i];
+			cc::RhoArgs ra = {};
+			ra.frac = b->arena.at<double>(b->off_frac[i]);
+			ra.N = (int)N[i];
+			ra.per_split = kBatchPerSplit;
+			ra.chunk = kBatchChunk;
+			ra.segs = h->main.segs;
+			ra.bstart = h->main.bstart;
+			ra.bspec = h->main.bspec;
+			ra.nseg = (int)p.segs.size();
+			ra.nslot = p.nslot;
+			ra.partial = b->arena.at<double2>(q.o_part);
+			cc::ReduceArgs rr = {};
+			rr.partial = ra.partial;
+			rr.nsplit = q.nsplit;
+			rr.nslot = p.nslot;
+			rr.slotV = h->main.slotV;
+			rr.rho_offset = h->rho_offset;
+			rr.rho_slot = b->arena.at<double2>(q.o_rho);
+			rr.u_slot = b->arena.at<double2>(q.o_u);
+			rr.eblock = b->arena.at<double>(q.o_eb);
+			rr.ticket = b->arena.at<unsigned>(q.o_tk);
+			rr.inv_vol = 1.0 / h->volume;
+			rr.shift = h->shift;
+			rr.E_out = b->arena.at<double>(b->off_E[i]);
+			rr.finalize = 0;   // the force kernel sums the energy terms
+			cc::ForceArgs fa = {};
+			fa.frac = ra.frac;
+			fa.N = ra.N;
+			fa.segs = h->main.segs;
+			fa.kstart = q.f->kstart;
+			fa.kspec = q.f->kspec;
+			fa.nksplit = q.nks;
+			fa.u_slot = rr.u_slot;
+			fa.nseg = ra.nseg;
+			fa.partialG = b->arena.at<double>(q.o_pg);
+			fa.counters = b->arena.at<unsigned>(q.o_fc);
+			for (int c = 0; c < 9; c++)
+				fa.recip[c] = h->recip[c];
+			fa.fscale = 2.0 / h->volume;
+			fa.F_out = b->arena.at<double>(b->off_F[i]);
+			fa.gfrac_out = nullptr;
+			fa.eblock = rr.eblock;
+			fa.neblock = q.nchunks;
+			fa.inv_vol = rr.inv_vol;
+			fa.shift = rr.shift;
+			fa.E_out = rr.E_out;
+			g.rho.push_back(ra);
+			g.red.push_back(rr);
+			g.force.push_back(fa);
+			const int c[3] = {p.nbgroups() * q.nsplit, q.nchunks, q.pgroups * q.nks};
+			const int sh[3] = {p.nbgroups(), q.nchunks, q.pgroups};
+			for (int ph = 0; ph < 3; ph++) {
 				pre[ph * (B + 1) + k + 1] = pre[ph * (B + 1) + k] + c[ph];
-			gi.push_back(in);
+				shape[ph * B + k] = sh[ph];
+			}
+			g.rho_row = std::max(g.rho_row, p.block_max_row);
+			g.force_row = std::max(g.force_row, q.max_row);
 		}
-		for (int ph = 0; ph < 4; ph++)
+		for (int ph = 0; ph < 3; ph++)
 			g.total[ph] = pre[ph * (B + 1) + B];
-		if ((rc = upload(&g.d_inst, gi)) || (rc = upload(&g.d_pre, pre)) || (rc = dev_alloc(&g.d_inst_lb, B))) {
+		if ((rc = upload(&g.d_rho[0], g.rho)) || (rc = upload(&g.d_red[0], g.red)) ||
+		    (rc = upload(&g.d_force[0], g.force)) || (rc = dev_alloc(&g.d_rho[1], B)) ||
+		    (rc = dev_alloc(&g.d_red[1], B)) || (rc = dev_alloc(&g.d_force[1], B)) || (rc = upload(&g.d_pre, pre)) ||
+		    (rc = upload(&g.d_shape, shape)) || (rc = dev_alloc(&g.d_queue, 6)) ||
+		    (rc = (cudaMemset(g.d_queue, 0, 6 * sizeof(unsigned)) == cudaSuccess ? CC_OK : CC_ERR_CUDA))) {
 			b->groups.push_back(g);
 			cc_batch_destroy(b);
 			return rc;
@@ -2358,12 +2426,16 @@ int cc_batch_destroy(cc_batch *b)
 	if (b->stream)
 		cudaStreamSynchronize(b->stream);
 	for (BatchGroup &g : b->groups) {
-		cudaFree(g.d_inst);
-		cudaFree(g.d_inst_lb);
+		for (int w = 0; w < 2; w++) {
+			cudaFree(g.d_rho[w]);
+			cudaFree(g.d_red[w]);
+			cudaFree(g.d_force[w]);
+		}
 		cudaFree(g.d_pre);
+		cudaFree(g.d_shape);
+		cudaFree(g.d_queue);
 	}
 	cudaFree(b->arena.base);
-	cudaFree(b->d_bar);
 	if (b->stream)
 		cudaStreamDestroy(b->stream);
 	delete b;
@@ -2504,18 +2576,28 @@ int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opt
 		return cleanup(rc);
 	// minimisation descriptors: evaluate at x_trial into the L-BFGS buffers, skip finished instances
 	for (BatchGroup &g : b->groups) {
-		std::vector<cc::BInst> gi;
-		for (int i : g.members) {
-			cc::BInst in = b->inst[i];
-			in.frac = lbi[i].xt;
-			in.E_out = &lbi[i].st->Et;
-			in.gfrac_out = lbi[i].gt;
-			in.F_out = nullptr;
-			in.status = &lbi[i].st->status;
-			in.stage = &lbi[i].st->stage;
-			gi.push_back(in);
+		std::vector<cc::RhoArgs> ra = g.rho;
+		std::vector<cc::ReduceArgs> rr = g.red;
+		std::vector<cc::ForceArgs> fa = g.force;
+		for (size_t k = 0; k < g.members.size(); k++) {
+			const int i = g.members[k];
+			const int *status = &lbi[i].st->status, *stage = &lbi[i].st->stage;
+			ra[k].frac = lbi[i].xt;
+			ra[k].skip = status;
+			ra[k].stage = stage;
+			rr[k].E_out = &lbi[i].st->Et;
+			rr[k].skip = status;
+			rr[k].stage = stage;
+			fa[k].frac = lbi[i].xt;
+			fa[k].E_out = &lbi[i].st->Et;
+			fa[k].gfrac_out = lbi[i].gt;
+			fa[k].F_out = nullptr;
+			fa[k].skip = status;
+			fa[k].stage = stage;
 		}
-		CC_CUDA(cudaMemcpy(g.d_inst_lb, gi.data(), sizeof(cc::BInst) * gi.size(), cudaMemcpyHostToDevice));
+		if ((rc = upload_into(g.d_rho[1], ra)) || (rc = upload_into(g.d_red[1], rr)) ||
+		    (rc = upload_into(g.d_force[1], fa)))
+			return cleanup(rc);
 	}
 	cudaStream_t st = b->stream;
 	const bool sched = o.precision == CC_PREC_SCHEDULE;
@@ -2553,16 +2635,15 @@ int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opt
 			if (ge)
 				cudaGraphExecDestroy(ge);
 	};
-	// warm-up: make sure the cooperative kernels' occupancy is queried before capture
-	int tmp = 0;
+	// kernel attributes are set before the capture
 	for (BatchGroup &g : b->groups)
-		if ((rc = (prec0 != CC_PREC_FP64 ? (g.D == 1 ? batch_grid<1, true>(&tmp) : g.D == 2 ? batch_grid<2, true>(&tmp)
-		                                                                                       : batch_grid<3, true>(&tmp))
-		                                  : (g.D == 1 ? batch_grid<1, false>(&tmp) : g.D == 2 ? batch_grid<2, false>(&tmp)
-		                                                                                       : batch_grid<3, false>(&tmp)))) ||
-		    (sched && (rc = (g.D == 1 ? batch_grid<1, false>(&tmp) : g.D == 2 ? batch_grid<2, false>(&tmp)
-		                                                                      : batch_grid<3, false>(&tmp)))))
-			return cleanup(rc);
+		for (int mx = 0; mx < 2; mx++) {
+			cudaError_t e = g.D == 1 ? (mx ? multi_attrs<1, true>() : multi_attrs<1, false>())
+			              : g.D == 2 ? (mx ? multi_attrs<2, true>() : multi_attrs<2, false>())
+			                         : (mx ? multi_attrs<3, true>() : multi_attrs<3, false>());
+			if (e != cudaSuccess)
+				return cleanup(fail(CC_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
+		}
 	if ((rc = make_graph(prec0, &gexec[0])) || (sched && (rc = make_graph(CC_PREC_FP64, &gexec[1])))) {
 		destroy_graphs();
 		return cleanup(rc);

@@ -228,6 +228,50 @@ __device__ __forceinline__ void write_force_out(double *F_out, double *gfrac_out
 	}
 }
 
+// An evaluation is skipped when its skip word is nonzero (a finished minimisation) or its stage word differs from the
+// launch's stage (the precision schedule of batched minimisations). Both pointers may be null.
+__device__ __forceinline__ bool eval_skipped(const int *skip, const int *stage, int want_stage)
+{
+	return (skip && *(volatile const int *)skip) || (stage && *(volatile const int *)stage != want_stage);
+}
+
+// Work queue of a persistent multi-instance launch: q[0] the next item, q[1] the blocks that found it empty. The last
+// block to leave resets both, so the next launch starts at item 0. Items are independent and write their own outputs,
+// so the order in which blocks take them does not change any result.
+__device__ __forceinline__ int queue_next(unsigned *q, int *sh_item)
+{
+	__syncthreads();   // the previous item's shared memory is no longer read
+	if (threadIdx.x == 0)
+		*sh_item = (int)atomicAdd(q, 1u);
+	__syncthreads();
+	return *sh_item;
+}
+
+__device__ __forceinline__ void queue_leave(unsigned *q)
+{
+	if (threadIdx.x == 0) {
+		__threadfence();
+		if (atomicAdd(q + 1, 1u) == gridDim.x - 1) {
+			q[0] = 0u;
+			q[1] = 0u;
+		}
+	}
+}
+
+// Instance of a multi-instance launch's block: pre[b] <= item < pre[b + 1] (binary search, B + 1 prefix sums).
+__device__ __forceinline__ int find_instance(const int *pre, int B, int item)
+{
+	int lo = 0, hi = B;
+	while (hi - lo > 1) {
+		const int mid = (lo + hi) >> 1;
+		if (__ldg(pre + mid) <= item)
+			lo = mid;
+		else
+			hi = mid;
+	}
+	return lo;
+}
+
 // ---------------------------------------------------------------------------------------------------------------
 // rho pass
 // ---------------------------------------------------------------------------------------------------------------
@@ -242,6 +286,8 @@ struct RhoArgs {
 	int nseg, nslot;          // nseg = ngroups * 32, nslot = nseg * L
 	double2 *partial;         // [nsplit / cluster][nslot]
 	const int *skip;          // if not null and nonzero, the launch does nothing (a finished minimisation)
+	const int *stage;         // if not null, the launch does nothing unless *stage == want_stage
+	int want_stage;
 };
 
 constexpr int kRhoWarps = 8;
@@ -251,8 +297,10 @@ constexpr int kRhoThreads = kRhoWarps * 32;
 // block owns the 32 segments of rho group bstart[g] + w (one per lane) and walks every particle of the block's split;
 // the tables of a chunk of particles are built once for the block group's spec and shared by all warps. The cluster's
 // blocks are added in rank order through distributed shared memory into one partial row.
-template <int D, int L, bool MIXED>
-__global__ void __launch_bounds__(kRhoThreads, 3) cc_rho_kernel(RhoArgs a)
+// Block (bg, split) of the rho pass. CLUSTER: the blocks of a thread-block cluster (consecutive splits) are added
+// through distributed shared memory into partial row split / cluster size; otherwise the block writes row `split`.
+template <int D, int L, bool MIXED, bool CLUSTER>
+__device__ __forceinline__ void rho_body(const RhoArgs &a, const int bg, const int split)
 {
 	typedef typename std::conditional<MIXED, float2, double2>::type C;
 	constexpr int SUB = 16;
@@ -261,9 +309,7 @@ __global__ void __launch_bounds__(kRhoThreads, 3) cc_rho_kernel(RhoArgs a)
 	double2 *red = reinterpret_cast<double2 *>(smem); // after the loop: kRhoWarps x L x 32
 	__shared__ TabSpec sp;
 
-	cg::cluster_group cluster = cg::this_cluster();
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	const int bg = blockIdx.x, split = blockIdx.y;
 	if (threadIdx.x == 0)
 		sp = a.bspec[bg];
 	const int g0 = a.bstart[bg], nwg = a.bstart[bg + 1] - g0;
@@ -273,7 +319,7 @@ __global__ void __launch_bounds__(kRhoThreads, 3) cc_rho_kernel(RhoArgs a)
 	const int j0 = min(a.N, split * a.per_split);
 	const int j1 = min(a.N, j0 + a.per_split);
 	cudaGridDependencySynchronize();   // inputs of this step are complete (programmatic dependent launch)
-	if (a.skip && *a.skip)             // uniform over the grid: no block reaches a cluster barrier
+	if (eval_skipped(a.skip, a.stage, a.want_stage))   // uniform over the instance: no block reaches a cluster barrier
 		return;
 	__syncthreads();
 	const int row = sp.row | 1;        // odd row stride: consecutive particles' rows start in different banks
@@ -385,7 +431,17 @@ __global__ void __launch_bounds__(kRhoThreads, 3) cc_rho_kernel(RhoArgs a)
 	}
 	cudaTriggerProgrammaticLaunchCompletion();   // the next kernel may be scheduled; it waits for this grid
 
+	if constexpr (!CLUSTER) {
+		// one partial row per block
+		if (active) {
+#pragma unroll
+			for (int r = 0; r < L; r++)
+				a.partial[(size_t)split * a.nslot + (size_t)r * a.nseg + (g0 + warp) * 32 + lane] = acc[r];
+		}
+		return;
+	}
 	// this block's sums, layout [warp][r][lane], then the cluster's blocks in rank order
+	cg::cluster_group cluster = cg::this_cluster();
 	__syncthreads();
 	if (active) {
 #pragma unroll
@@ -412,6 +468,37 @@ __global__ void __launch_bounds__(kRhoThreads, 3) cc_rho_kernel(RhoArgs a)
 	cluster.sync();
 }
 
+// Grid (nbgroups, nsplit), clusters of `csize` blocks along y (the particle splits of one block group). Warp w of a
+// block owns the 32 segments of rho group bstart[g] + w (one per lane) and walks every particle of the block's split;
+// the tables of a chunk of particles are built once for the block group's spec and shared by all warps. The cluster's
+// blocks are added in rank order through distributed shared memory into one partial row.
+template <int D, int L, bool MIXED>
+__global__ void __launch_bounds__(kRhoThreads, 3) cc_rho_kernel(RhoArgs a)
+{
+	rho_body<D, L, MIXED, true>(a, blockIdx.x, blockIdx.y);
+}
+
+// The rho pass of many instances in one persistent launch: blocks take items from a work queue; item i belongs to
+// instance b with pre[b] <= i < pre[b+1] and is block (local % nbgroups[b], local / nbgroups[b]) of that instance's
+// grid; no clusters (one row per block). Items of skipped instances cost a lookup and a flag read.
+template <int D, int L, bool MIXED>
+__global__ void __launch_bounds__(kRhoThreads, 3) cc_mrho_kernel(const RhoArgs *__restrict__ args,
+                                                                const int *__restrict__ pre,
+                                                                const int *__restrict__ nbgroups, int B,
+                                                                int want_stage, unsigned *queue)
+{
+	__shared__ int sh_item;
+	const int total = __ldg(pre + B);
+	for (int item; (item = queue_next(queue, &sh_item)) < total;) {
+		const int b = find_instance(pre, B, item);
+		RhoArgs a = args[b];
+		a.want_stage = want_stage;
+		const int local = item - __ldg(pre + b), ng = __ldg(nbgroups + b);
+		rho_body<D, L, MIXED, false>(a, local % ng, local / ng);
+	}
+	queue_leave(queue);
+}
+
 // ---------------------------------------------------------------------------------------------------------------
 // split reduction, u = V conj(rho), energy
 // ---------------------------------------------------------------------------------------------------------------
@@ -427,20 +514,23 @@ struct ReduceArgs {
 	double *E_out;
 	int finalize;             // 0: the force kernel that follows sums eblock into E_out
 	const int *skip;
+	const int *stage;
+	int want_stage;
 };
 
 constexpr int kRedThreads = 256;   // 32 slots x 8 split chunks
 
-static __global__ void __launch_bounds__(kRedThreads) cc_reduce_kernel(ReduceArgs a)
+// Block `chunk` (32 slots) of the split reduction of an instance with `nchunks` such blocks.
+__device__ __forceinline__ void reduce_body(const ReduceArgs &a, const int chunk, const int nchunks)
 {
 	__shared__ double2 sh[8][32];
 	__shared__ int sh_last;
 	const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
-	const int slot = blockIdx.x * 32 + lane;
+	const int slot = chunk * 32 + lane;
 	const int per = (a.nsplit + 7) >> 3;
 	cudaGridDependencySynchronize();
 	cudaTriggerProgrammaticLaunchCompletion();
-	if (a.skip && *a.skip)
+	if (eval_skipped(a.skip, a.stage, a.want_stage))
 		return;
 	const int s0 = min(a.nsplit, c * per), s1 = min(a.nsplit, s0 + per);
 	double2 t = make_double2(0.0, 0.0);
@@ -487,20 +577,20 @@ static __global__ void __launch_bounds__(kRedThreads) cc_reduce_kernel(ReduceArg
 		for (int o = 16; o > 0; o >>= 1)
 			e += __shfl_down_sync(0xffffffffu, e, o);
 		if (lane == 0)
-			a.eblock[blockIdx.x] = e;
+			a.eblock[chunk] = e;
 	}
 	if (!a.finalize)
 		return;
 	__threadfence();
 	__syncthreads();
 	if (threadIdx.x == 0)
-		sh_last = (atomicAdd(a.ticket, 1u) == gridDim.x - 1);
+		sh_last = (atomicAdd(a.ticket, 1u) == (unsigned)nchunks - 1);
 	__syncthreads();
 	if (!sh_last || c != 0)
 		return;
 	__threadfence();
 	double e = 0.0;
-	for (int b = lane; b < (int)gridDim.x; b += 32)
+	for (int b = lane; b < nchunks; b += 32)
 		e += __ldcg(&a.eblock[b]);
 #pragma unroll
 	for (int o = 16; o > 0; o >>= 1)
@@ -509,6 +599,28 @@ static __global__ void __launch_bounds__(kRedThreads) cc_reduce_kernel(ReduceArg
 		*a.E_out = e * a.inv_vol + a.shift;
 		*a.ticket = 0u;
 	}
+}
+
+static __global__ void __launch_bounds__(kRedThreads) cc_reduce_kernel(ReduceArgs a)
+{
+	reduce_body(a, blockIdx.x, gridDim.x);
+}
+
+// The split reduction of many instances in one persistent launch (item -> instance b, chunk item - pre[b]).
+static __global__ void __launch_bounds__(kRedThreads) cc_mreduce_kernel(const ReduceArgs *__restrict__ args,
+                                                                     const int *__restrict__ pre,
+                                                                     const int *__restrict__ nchunks, int B,
+                                                                     int want_stage, unsigned *queue)
+{
+	__shared__ int sh_item;
+	const int total = __ldg(pre + B);
+	for (int item; (item = queue_next(queue, &sh_item)) < total;) {
+		const int b = find_instance(pre, B, item);
+		ReduceArgs a = args[b];
+		a.want_stage = want_stage;
+		reduce_body(a, item - __ldg(pre + b), __ldg(nchunks + b));
+	}
+	queue_leave(queue);
 }
 
 // rho in input-mode order (repeated modes read their shared slot)
@@ -546,6 +658,8 @@ struct ForceArgs {
 	double inv_vol, shift;
 	double *E_out;
 	const int *skip;
+	const int *stage;
+	int want_stage;
 };
 
 constexpr int kForceWarps = 8;
@@ -573,7 +687,7 @@ template <typename C> __host__ __device__ constexpr size_t force_smem_bytes(int 
 // weights u of up to kForceUChunk segments at a time are staged in shared memory in the compute type (slot-major, so a
 // warp's read of one weight is a broadcast).
 template <int D, int L, bool MIXED>
-__global__ void __launch_bounds__(kForceThreads, 3) cc_force_kernel(ForceArgs a)
+__device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup, const int ks)
 {
 	typedef typename std::conditional<MIXED, float, double>::type R;
 	typedef typename std::conditional<MIXED, float2, double2>::type C;
@@ -586,11 +700,14 @@ __global__ void __launch_bounds__(kForceThreads, 3) cc_force_kernel(ForceArgs a)
 	__shared__ int sh_last;
 
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	const int pbase = blockIdx.x * 32;
+	const int pbase = pgroup * 32;
 	const int j = pbase + lane;
 	const int nvalid = min(32, a.N - pbase);
-	const int ks = blockIdx.y;
 	const int q0 = a.kstart[ks], q1 = a.kstart[ks + 1];
+	// The skip and stage words are written by kernels that completed before this evaluation's rho pass (whose
+	// completion this block's launch implies), like the positions: a finished instance builds no tables.
+	if (eval_skipped(a.skip, a.stage, a.want_stage))
+		return;
 	if (threadIdx.x == 0)
 		sp = a.kspec[ks];
 	__syncthreads();
@@ -598,9 +715,9 @@ __global__ void __launch_bounds__(kForceThreads, 3) cc_force_kernel(ForceArgs a)
 	// while the reduce kernel still runs (programmatic dependent launch), before waiting for u.
 	build_tables<D, C>(sp, a.frac, pbase, 32, nvalid, tab, 1, 32, threadIdx.x, kForceThreads);
 	cudaGridDependencySynchronize();   // u of this step is complete
-	if (a.skip && *a.skip)             // uniform over the grid
+	if (eval_skipped(a.skip, a.stage, a.want_stage))   // uniform over the instance
 		return;
-	if (a.E_out && blockIdx.x == 0 && blockIdx.y == 0 && warp == 0) {
+	if (a.E_out && pgroup == 0 && ks == 0 && warp == 0) {
 		// the energy, summed in the order of the reduce kernel's last block
 		double e = 0.0;
 		for (int b = lane; b < a.neblock; b += 32)
@@ -703,7 +820,7 @@ __global__ void __launch_bounds__(kForceThreads, 3) cc_force_kernel(ForceArgs a)
 	__threadfence();
 	__syncwarp();
 	if (lane == 0)
-		sh_last = (atomicAdd(&a.counters[blockIdx.x], 1u) == (unsigned)(a.nksplit - 1));
+		sh_last = (atomicAdd(&a.counters[pgroup], 1u) == (unsigned)(a.nksplit - 1));
 	__syncwarp();
 	if (!sh_last)
 		return;
@@ -720,7 +837,33 @@ __global__ void __launch_bounds__(kForceThreads, 3) cc_force_kernel(ForceArgs a)
 		write_force<D>(a, j, v);
 	}
 	if (lane == 0)
-		a.counters[blockIdx.x] = 0u;
+		a.counters[pgroup] = 0u;
+}
+
+template <int D, int L, bool MIXED>
+__global__ void __launch_bounds__(kForceThreads, 3) cc_force_kernel(ForceArgs a)
+{
+	force_body<D, L, MIXED>(a, blockIdx.x, blockIdx.y);
+}
+
+// The force pass of many instances in one persistent launch: item -> instance b, block (local % pgroups[b],
+// local / pgroups[b]) of its grid.
+template <int D, int L, bool MIXED>
+__global__ void __launch_bounds__(kForceThreads, 3) cc_mforce_kernel(const ForceArgs *__restrict__ args,
+                                                                    const int *__restrict__ pre,
+                                                                    const int *__restrict__ pgroups, int B,
+                                                                    int want_stage, unsigned *queue)
+{
+	__shared__ int sh_item;
+	const int total = __ldg(pre + B);
+	for (int item; (item = queue_next(queue, &sh_item)) < total;) {
+		const int b = find_instance(pre, B, item);
+		ForceArgs a = args[b];
+		a.want_stage = want_stage;
+		const int local = item - __ldg(pre + b), pg = __ldg(pgroups + b);
+		force_body<D, L, MIXED>(a, local % pg, local / pg);
+	}
+	queue_leave(queue);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
