@@ -1122,8 +1122,7 @@ int run_nufft_t(cc_handle *h, int64_t N, const double *d_frac, double *d_E, doub
 	const int64_t ngrid = h->nu_ngrid;
 	CC_CUDA(cudaMemsetAsync(a.gi, 0, sizeof(unsigned long long) * ngrid, st));
 	if (N > 0) {
-		const int64_t items = N * cc::kNufftW;
-		cc::nufft_spread_kernel<D><<<(unsigned)((items + cc::kNufftThreads - 1) / cc::kNufftThreads), cc::kNufftThreads,
+		cc::nufft_spread_kernel<D><<<(unsigned)((N + cc::kNufftPerBlock - 1) / cc::kNufftPerBlock), cc::kNufftThreads,
 		                             0, st>>>(a, d_frac, (int)N);
 		CC_CUDA(cudaGetLastError());
 	}
@@ -1157,7 +1156,7 @@ int run_nufft_t(cc_handle *h, int64_t N, const double *d_frac, double *d_E, doub
 	o.fscale = 2.0 / h->volume;
 	o.F_out = d_F;
 	o.gfrac_out = d_gfrac;
-	cc::nufft_interp_kernel<D><<<(unsigned)((N + cc::kNufftThreads - 1) / cc::kNufftThreads), cc::kNufftThreads, 0,
+	cc::nufft_interp_kernel<D><<<(unsigned)((N + cc::kNufftPerBlock - 1) / cc::kNufftPerBlock), cc::kNufftThreads, 0,
 	                             st>>>(a, d_frac, (int)N, ngrid, o);
 	CC_CUDA(cudaGetLastError());
 	return CC_OK;
@@ -1270,10 +1269,11 @@ cudaEvent_t next_event(cc_handle *h)
 	return h->ev[h->ev_used++];
 }
 
-// CC_PATH_AUTO: the NUFFT path when its estimated time is below the direct path's. Direct: N x slots at 700 G
-// pairs/s; NUFFT: 2e-11 d s per particle and kernel point (spread + interpolation, W^d points), 2e-10 s per fine-grid
-// point and transform, 30 us of launches. The constants are conservative fits of B200 timings (2D N=1e5 M=40002:
-// 0.38 ms NUFFT against 5.1 ms direct; 3D N=2000 M=2724: 25 us direct).
+// CC_PATH_AUTO: the NUFFT path when its estimated time, with a 20 % margin, is below the direct path's. Direct:
+// N x slots at 700 G pairs/s; NUFFT: 1.8e-11 s per particle and kernel point (spread + interpolation, W^d points),
+// 5e-11 s per fine-grid point and transform, 25 us of launches. Fits of B200 timings: 2D N=1e5 M=40002 0.29 ms NUFFT
+// against 5.1 ms direct; 2D N=2e4 M=8002 0.087 against 0.25; 3D N=2e4 M=27085 0.96 against 0.90; 3D N=1e5 M=135008
+// 4.9 against 20; 3D N=2000 M=2724 0.14 against 0.025.
 bool nufft_preferred(cc_handle *h, int64_t N)
 {
 	if (h->main.plan.nslot == 0 || N < 1024)
@@ -1296,8 +1296,8 @@ bool nufft_preferred(cc_handle *h, int64_t N)
 	if (grid > (double)((int64_t)1 << 28))
 		return false;
 	const double direct = (double)N * (double)h->main.plan.real_segs * h->main.plan.L / 7e11;
-	const double nufft = 2e-11 * d * (double)N * w + 2e-10 * grid * (1 + d) + 3e-5;
-	return nufft < direct;
+	const double nufft = 1.8e-11 * (double)N * w + 5e-11 * grid * (1 + d) + 2.5e-5;
+	return 1.2 * nufft < direct;
 }
 
 int eval_device(cc_handle *h, int64_t N, const double *d_frac, double *d_E, double *d_F, double *d_gfrac,
@@ -1577,12 +1577,20 @@ int cc_set_positions(cc_handle *h, int64_t N, const double *frac)
 	if (int rc = input_staging(h, (size_t)N * d))
 		return rc;
 	double *in = h->h_in;
+	// positions already in [0,1) (the usual case) are copied as they are; NaN fails both comparisons
+	bool unit = true;
 	for (int64_t i = 0; i < N * d; i++)
-		if (!wrap_unit(frac[i], in + i)) {
-			h->upload_pending = false;
-			h->N = -1;
-			return fail(CC_ERR_ARG, "non-finite fractional coordinate");
-		}
+		unit &= (frac[i] >= 0.0) & (frac[i] < 1.0);
+	if (unit) {
+		std::memcpy(in, frac, sizeof(double) * N * d);
+	} else {
+		for (int64_t i = 0; i < N * d; i++)
+			if (!wrap_unit(frac[i], in + i)) {
+				h->upload_pending = false;
+				h->N = -1;
+				return fail(CC_ERR_ARG, "non-finite fractional coordinate");
+			}
+	}
 	h->upload_pending = true;
 	h->N = N;
 	h->lastF_valid = false;

@@ -68,36 +68,58 @@ __device__ __forceinline__ int wrap_index(int g, int n)
 	return g < 0 ? g + n : g;
 }
 
-// Type-1 spread: one thread per (particle, first-axis point), fixed-point atomics into the grid.
+constexpr int kNufftLanes = 16;                    // lanes per particle (kNufftW of them active)
+constexpr int kNufftPerBlock = kNufftThreads / kNufftLanes;   // particles per block (two per warp)
+
+// The kernel weights of particle j along every axis into shared memory (lane t < W computes entry t of each axis);
+// returns false for a lane without a particle. The 16 lanes of a particle are in one warp.
+template <int D>
+__device__ __forceinline__ bool nufft_weights(const NufftDev &a, const double *frac, int N, int j, int t,
+                                              double (*sk)[kNufftW], int *sg0)
+{
+	const bool valid = j < N;
+	if (valid) {
+#pragma unroll
+		for (int e = 0; e < D; e++) {
+			const double x = frac[(size_t)j * D + e] * a.nf[e];
+			const int g0 = (int)ceil(x - 0.5 * kNufftW);
+			if (t < kNufftW)
+				sk[e][t] = es_kernel((double)(g0 + t) - x, a.beta);
+			if (t == 0)
+				sg0[e] = g0;
+		}
+	}
+	__syncwarp();
+	return valid;
+}
+
+// Type-1 spread: 16 lanes per particle; lane t0 adds the particle's weights of first-axis point g0 + t0 to the grid
+// in fixed point (integer atomics: the sum does not depend on their order).
 template <int D> __global__ void __launch_bounds__(kNufftThreads) nufft_spread_kernel(NufftDev a, const double *frac, int N)
 {
-	const int64_t t = (int64_t)blockIdx.x * kNufftThreads + threadIdx.x;
+	__shared__ double sk[kNufftPerBlock][3][kNufftW];
+	__shared__ int sg0[kNufftPerBlock][3];
 	if (a.skip && *a.skip)
 		return;
-	if (t >= (int64_t)N * kNufftW)
+	const int p = threadIdx.x / kNufftLanes, t0 = threadIdx.x % kNufftLanes;
+	const int j = blockIdx.x * kNufftPerBlock + p;
+	if (!nufft_weights<D>(a, frac, N, j, t0, sk[p], sg0[p]) || t0 >= kNufftW)
 		return;
-	const int j = (int)(t / kNufftW), t0 = (int)(t - (int64_t)j * kNufftW);
-	double k[3][kNufftW];
-	int g0[3] = {0, 0, 0};
-#pragma unroll
-	for (int e = 0; e < D; e++)
-		g0[e] = es_weights(frac[(size_t)j * D + e] * a.nf[e], a.beta, k[e]);
-	const int i0 = wrap_index(g0[0] + t0, a.nf[0]);
-	const double w0 = k[0][t0];
+	const int i0 = wrap_index(sg0[p][0] + t0, a.nf[0]);
+	const double w0 = sk[p][0][t0];
 	if constexpr (D == 1) {
 		atomicAdd(a.gi + i0, (unsigned long long)llrint(w0 * kNufftFix));
 	} else {
 		for (int t1 = 0; t1 < kNufftW; t1++) {
-			const int i1 = wrap_index(g0[1] + t1, a.nf[1]);
-			const double w01 = w0 * k[1][t1];
+			const int i1 = wrap_index(sg0[p][1] + t1, a.nf[1]);
+			const double w01 = w0 * sk[p][1][t1];
 			if constexpr (D == 2) {
 				atomicAdd(a.gi + (size_t)i0 * a.nf[1] + i1, (unsigned long long)llrint(w01 * kNufftFix));
 			} else {
 				const size_t base = ((size_t)i0 * a.nf[1] + i1) * a.nf[2];
-#pragma unroll 2
 				for (int t2 = 0; t2 < kNufftW; t2++) {
-					const int i2 = wrap_index(g0[2] + t2, a.nf[2]);
-					atomicAdd(a.gi + base + i2, (unsigned long long)llrint(w01 * k[2][t2] * kNufftFix));
+					const int i2 = wrap_index(sg0[p][2] + t2, a.nf[2]);
+					atomicAdd(a.gi + base + i2, (unsigned long long)llrint(w01 * sk[p][2][t2] * kNufftFix));
 				}
 			}
 		}
@@ -221,33 +243,32 @@ struct NufftOut {
 	double *gfrac_out;        // N x D dPhi/ds, or nullptr
 };
 
-// type-2 interpolation: one thread per particle; g_e = Im(sum_g phi G_e[g]); forces as the direct force kernel
+// type-2 interpolation: 16 lanes per particle; lane t0 sums the first-axis point g0 + t0, the lanes' sums are added
+// in a fixed butterfly; g_e = Im(sum_g phi G_e[g]) and the forces as the direct force kernel
 template <int D>
 __global__ void __launch_bounds__(kNufftThreads) nufft_interp_kernel(NufftDev a, const double *frac, int N,
                                                                      int64_t ngrid, NufftOut o)
 {
-	const int j = blockIdx.x * kNufftThreads + threadIdx.x;
+	__shared__ double sk[kNufftPerBlock][3][kNufftW];
+	__shared__ int sg0[kNufftPerBlock][3];
 	if (a.skip && *a.skip)
 		return;
-	if (j >= N)
-		return;
-	double k[3][kNufftW];
-	int g0[3] = {0, 0, 0};
-#pragma unroll
-	for (int e = 0; e < D; e++)
-		g0[e] = es_weights(frac[(size_t)j * D + e] * a.nf[e], a.beta, k[e]);
+	const int p = threadIdx.x / kNufftLanes, t0 = threadIdx.x % kNufftLanes;
+	const int j = blockIdx.x * kNufftPerBlock + p;
+	const bool valid = nufft_weights<D>(a, frac, N, j, t0, sk[p], sg0[p]);
 	double acc[D];
 #pragma unroll
 	for (int e = 0; e < D; e++)
 		acc[e] = 0.0;
-	for (int t0 = 0; t0 < kNufftW; t0++) {
-		const int i0 = wrap_index(g0[0] + t0, a.nf[0]);
+	if (valid && t0 < kNufftW) {
+		const int i0 = wrap_index(sg0[p][0] + t0, a.nf[0]);
+		const double w0 = sk[p][0][t0];
 		if constexpr (D == 1) {
-			acc[0] = fma(k[0][t0], a.coef[i0].y, acc[0]);
+			acc[0] = w0 * a.coef[i0].y;
 		} else {
 			for (int t1 = 0; t1 < kNufftW; t1++) {
-				const int i1 = wrap_index(g0[1] + t1, a.nf[1]);
-				const double w01 = k[0][t0] * k[1][t1];
+				const int i1 = wrap_index(sg0[p][1] + t1, a.nf[1]);
+				const double w01 = w0 * sk[p][1][t1];
 				if constexpr (D == 2) {
 					const size_t idx = (size_t)i0 * a.nf[1] + i1;
 #pragma unroll
@@ -256,8 +277,8 @@ __global__ void __launch_bounds__(kNufftThreads) nufft_interp_kernel(NufftDev a,
 				} else {
 					const size_t base = ((size_t)i0 * a.nf[1] + i1) * a.nf[2];
 					for (int t2 = 0; t2 < kNufftW; t2++) {
-						const size_t idx = base + wrap_index(g0[2] + t2, a.nf[2]);
-						const double w = w01 * k[2][t2];
+						const size_t idx = base + wrap_index(sg0[p][2] + t2, a.nf[2]);
+						const double w = w01 * sk[p][2][t2];
 #pragma unroll
 						for (int e = 0; e < D; e++)
 							acc[e] = fma(w, a.coef[(size_t)e * ngrid + idx].y, acc[e]);
@@ -266,7 +287,13 @@ __global__ void __launch_bounds__(kNufftThreads) nufft_interp_kernel(NufftDev a,
 			}
 		}
 	}
-	write_force_out<D>(o.F_out, o.gfrac_out, o.recip, o.fscale, j, acc);
+#pragma unroll
+	for (int off = kNufftLanes / 2; off > 0; off >>= 1)
+#pragma unroll
+		for (int e = 0; e < D; e++)
+			acc[e] += __shfl_xor_sync(0xffffffffu, acc[e], off, kNufftLanes);
+	if (valid && t0 == 0)
+		write_force_out<D>(o.F_out, o.gfrac_out, o.recip, o.fscale, j, acc);
 }
 
 }  // namespace cc

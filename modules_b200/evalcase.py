@@ -1,6 +1,6 @@
 """Evaluate one synthetic stealthy configuration a few times (for profiling a single kernel launch sequence).
 
-    python -m modules_b200.evalcase --d 2 --N 20000 --chi 0.2 --evals 3 [--mixed] [--fused]
+    python -m modules_b200.evalcase --d 2 --N 20000 --chi 0.2 --evals 3 [--mixed] [--path split|fused|nufft|auto]
 
 The configuration: N uniform random points (seed 1) in a periodic cube of unit density, the CLI's Type 0 k-set.
 """
@@ -18,12 +18,14 @@ def main():
     ap.add_argument("--chi", type=float, default=0.2)
     ap.add_argument("--evals", type=int, default=3)
     ap.add_argument("--mixed", action="store_true")
-    ap.add_argument("--fused", action="store_true")
+    ap.add_argument("--fused", action="store_true", help="same as --path fused")
+    ap.add_argument("--path", default="split", choices=["split", "fused", "nufft", "auto"])
     a = ap.parse_args()
     basis = np.eye(a.d) * a.N ** (1.0 / a.d)
     modes, V = cc.stealthy_kset(a.d, basis, a.N, a.chi)
     pot = cc.CCPotential(a.d, basis, modes, V)
-    pot.set_path(1 if a.fused else 0)
+    paths = {"split": cc.PATH_SPLIT, "fused": cc.PATH_FUSED, "nufft": cc.PATH_NUFFT, "auto": cc.PATH_AUTO}
+    pot.set_path(cc.PATH_FUSED if a.fused else paths[a.path])
     pot.set_configuration(np.random.default_rng(1).random((a.N, a.d)))
     E = None
     for _ in range(a.evals):

@@ -13,7 +13,8 @@ def build(reference=os.environ.get("CC_REFERENCE_TREE", "/root/reference")):
     os.makedirs(os.path.dirname(EXE), exist_ok=True)
     cmd = ["/usr/bin/g++", "-std=c++17", "-O2", "-fopenmp", "-w",
            "-I" + os.path.join(ROOT, "oracle", "standins"), "-I" + os.path.join(reference, "core"),
-           "-I" + os.path.join(reference, "potential"), "-I" + os.path.join(ROOT, "include"),
+           "-I" + os.path.join(reference, "potential"), "-I" + os.path.join(reference, "apps", "CCOptimization"),
+           "-I" + os.path.join(ROOT, "include"),
            os.path.join(ROOT, "tests", "adapter_check.cpp"), "-o", EXE,
            "-L" + os.path.join(ROOT, "oracle", "_ref"), "-lccref",
            "-L" + os.path.join(ROOT, "modules_b200"), "-l:libccgpu.so",

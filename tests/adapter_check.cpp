@@ -2,14 +2,19 @@
 // reference build (oracle/_ref/libccref.so: LuksanPLIS, Potential::~Potential, Volume) and libccgpu.so.
 //   1. GpuCCPotential (include/GpuCCPotential.h) against the reference's ShiftedCCPotential on the same
 //      Configuration and constraints: Energy, AllForce, Force(i), EnergyAndAllForce, GetRho (1e-10 of the scales).
+//   3. GpuMultiStealthyPotential (include/GpuMultiStealthyPotential.h) against the reference's MultiStealthyPotential
+//      (compiled into oracle/_ref/libccref.so) on a skew 2D cell with three species and unequal radii: Energy and
+//      AllForce (1e-10), and EnergyAndAllForce equal to Energy then AllForce bitwise.
 //   2. The structure optimiser's Switch-0 objective (restated from potential/StructureOptimization.cpp:447-536) finds
 //      CombinedEnergyForce by dynamic_cast and drives the reference's LuksanPLIS with the GPU adapter to the
 //      stealthy ground state of a 2D N=100 chi=0.30 configuration (E/N < 1e-20).
 // Prints one line per check and exits 0 only if all pass.
 #include "GpuCCPotential.h"
+#include "GpuMultiStealthyPotential.h"
 #include "LuksanPLIS.h"
 
 #include <cmath>
+#include <iostream>
 #include <cstdio>
 #include <random>
 #include <vector>
@@ -166,6 +171,64 @@ int main()
 		const int st = LuksanPLIS(n * d, objective, &aux, x.data(), &minf, 1e-20 * n, 5000, 40, &evals, 0);
 		std::printf("LuksanPLIS status %d after %d evaluations\n", st, evals);
 		check(minf / n < 1e-20, "ground state E/N via Objective + LuksanPLIS + GpuCCPotential", minf / n, 1e-20);
+	}
+	// ---- 3. the multi-species potential with contact against the reference class ---------------------------------
+	{
+		const int d = 2, n = 90, S = 3;
+		Configuration c = make_config(d, {10.0, 0.0, 3.0, 9.0}, n, rng);
+		std::uniform_real_distribution<double> ur(0.25, 0.45);
+		std::vector<double> radii(n);
+		for (auto &r : radii)
+			r = ur(rng);
+		std::streambuf *saved = std::cout.rdbuf(nullptr);   // the reference reports its set-up on stdout
+		MultiStealthyPotential ref(d, 1.0);
+		GpuMultiStealthyPotential gpu(d, 1.0);
+		ref.u0 = gpu.u0 = 1.5;
+		ref.SetNumSpecies(S);
+		gpu.SetNumSpecies(S);
+		for (int s = 0; s < S; s++) {
+			std::vector<int32_t> modes(2 * 512);
+			std::vector<double> V(512);
+			int64_t M = 0;
+			const double basis[4] = {10.0, 0.0, 3.0, 9.0};
+			if (cc_kset_stealthy(d, basis, n / S, 0.2 + 0.05 * s, 3, 512, modes.data(), V.data(), &M) != CC_OK)
+				return 2;
+			for (int64_t q = 0; q < M; q++) {
+				GeometryVector k(d);
+				k.AddFrom((double)modes[q * d] * c.GetReciprocalBasisVector(0));
+				k.AddFrom((double)modes[q * d + 1] * c.GetReciprocalBasisVector(1));
+				ref.AddConstraint(s, k, std::vector<double>{V[q]});
+				gpu.AddConstraint(s, k, std::vector<double>{V[q]});
+			}
+		}
+		ref.SetConfiguration(c);
+		gpu.SetConfiguration(c);
+		for (int i = 0; i < n; i++) {
+			ref.SetSpeciesOfParticle(i, i % S);
+			gpu.SetSpeciesOfParticle(i, i % S);
+		}
+		ref.SetSecureRadii(radii);
+		gpu.SetSecureRadii(radii);
+		std::cout.rdbuf(saved);
+		const double Er = ref.Energy(), Eg = gpu.Energy();
+		check(std::abs(Er - Eg) <= 1e-10 * std::abs(Er), "multi-species Energy", Eg, Er);
+		std::vector<GeometryVector> fr, fg, fc;
+		ref.AllForce(fr);
+		gpu.AllForce(fg);
+		double worst = 0, fmax = 1.0;
+		for (size_t i = 0; i < fr.size(); i++)
+			for (int j = 0; j < d; j++) {
+				worst = std::max(worst, std::abs(fr[i].x[j] - fg[i].x[j]));
+				fmax = std::max(fmax, std::abs(fr[i].x[j]));
+			}
+		check(fg.size() == fr.size() && worst <= 1e-10 * fmax, "multi-species AllForce max |dF| / max(1,|F|)",
+		      worst / fmax, 1e-10);
+		const double Ec = gpu.EnergyAndAllForce(fc);
+		bool same = Ec == Eg && fc.size() == fg.size();
+		for (size_t i = 0; same && i < fc.size(); i++)
+			for (int j = 0; j < d; j++)
+				same = same && fc[i].x[j] == fg[i].x[j];
+		check(same, "multi-species EnergyAndAllForce == Energy then AllForce (bitwise)", Ec, Eg);
 	}
 	std::printf(failures ? "ADAPTER FAIL\n" : "ADAPTER OK\n");
 	return failures ? 1 : 0;
