@@ -7,10 +7,10 @@
 //   cc_force_kernel -> Cartesian forces and/or the gradient in fractional coordinates.
 // There is no CPU path: without a CUDA device every call that computes returns CC_ERR_NOGPU.
 #include "../../include/cc_gpu.h"
-#include "cc_batch.cuh"
 #include "cc_fused.cuh"
 #include "cc_kernels.cuh"
 #include "cc_lbfgs.cuh"
+#include "cc_multi_launch.h"
 #include "cc_nufft.cuh"
 #include "cc_plan.h"
 
@@ -2185,9 +2185,9 @@ struct BatchGroup {
 	std::vector<cc::ForceArgs> force;
 };
 
-constexpr int kBatchChunk = 16;          // particles whose rho tables are built at once in a batch
-constexpr int kBatchPerSplit = 64;       // particles per rho block of a batch instance
-constexpr int kBatchSegsPerSplit = 64;   // segments per force block of a batch instance
+using cc::kBatchChunk;
+using cc::kBatchPerSplit;
+using cc::kBatchSegsPerSplit;
 
 }  // namespace
 
@@ -2217,29 +2217,56 @@ template <int D, bool MIXED> cudaError_t multi_attrs()
 	return e;
 }
 
-// the three launches of one group: which = 0 (batch positions) or 1 (minimisation trial points)
-template <int D, bool MIXED> int multi_launch_t(BatchGroup &g, int which, cudaStream_t st)
+template <int D, bool MIXED>
+int multi_launch_raw(const cc::RhoArgs *rho, const cc::ReduceArgs *red, const cc::ForceArgs *force, const int *pre,
+                     const int *shape, int B, const int total[3], int rho_row, int force_row, unsigned *queue,
+                     cudaStream_t st)
 {
 	typedef typename std::conditional<MIXED, float2, double2>::type C;
 	if (cudaError_t e = multi_attrs<D, MIXED>())
 		return fail(CC_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
-	const int B = (int)g.members.size(), want = MIXED ? 0 : 1;
-	const int *pre = g.d_pre, *shape = g.d_shape;
+	const int want = MIXED ? 0 : 1;
 	// persistent grids: at most the resident blocks (3 per SM for rho and force, 8 for the reduction)
 	const int res3 = 3 * sm_count(), res8 = 8 * sm_count();
-	if (g.total[0] > 0)
-		CC_CUDA(launch_pdl_n(cc::cc_mrho_kernel<D, 8, MIXED>, dim3(std::min(g.total[0], res3)), dim3(cc::kRhoThreads),
-		                   rho_smem<C>(g.rho_row, kBatchChunk, 8), st, (const cc::RhoArgs *)g.d_rho[which], pre,
-		                   shape, B, want, g.d_queue));
-	if (g.total[1] > 0)
-		CC_CUDA(launch_pdl_n(cc::cc_mreduce_kernel, dim3(std::min(g.total[1], res8)), dim3(cc::kRedThreads), 0, st,
-		                   (const cc::ReduceArgs *)g.d_red[which], pre + (B + 1), shape + B, B, want, g.d_queue + 2));
-	if (g.total[2] > 0)
-		CC_CUDA(launch_pdl_n(cc::cc_mforce_kernel<D, 8, MIXED>, dim3(std::min(g.total[2], res3)), dim3(cc::kForceThreads),
-		                   force_smem<C>(g.force_row, D), st, (const cc::ForceArgs *)g.d_force[which],
-		                   pre + 2 * (B + 1), shape + 2 * B, B, want, g.d_queue + 4));
+	if (total[0] > 0)
+		CC_CUDA(launch_pdl_n(cc::cc_mrho_kernel<D, 8, MIXED>, dim3(std::min(total[0], res3)), dim3(cc::kRhoThreads),
+		                   rho_smem<C>(rho_row, kBatchChunk, 8), st, rho, pre, shape, B, want, queue));
+	if (total[1] > 0)
+		CC_CUDA(launch_pdl_n(cc::cc_mreduce_kernel, dim3(std::min(total[1], res8)), dim3(cc::kRedThreads), 0, st, red,
+		                   pre + (B + 1), shape + B, B, want, queue + 2));
+	if (total[2] > 0)
+		CC_CUDA(launch_pdl_n(cc::cc_mforce_kernel<D, 8, MIXED>, dim3(std::min(total[2], res3)), dim3(cc::kForceThreads),
+		                   force_smem<C>(force_row, D), st, force, pre + 2 * (B + 1), shape + 2 * B, B, want,
+		                   queue + 4));
 	return CC_OK;
 }
+
+// the three launches of one group: which = 0 (batch positions) or 1 (minimisation trial points)
+template <int D, bool MIXED> int multi_launch_t(BatchGroup &g, int which, cudaStream_t st)
+{
+	return multi_launch_raw<D, MIXED>(g.d_rho[which], g.d_red[which], g.d_force[which], g.d_pre, g.d_shape,
+	                                  (int)g.members.size(), g.total, g.rho_row, g.force_row, g.d_queue, st);
+}
+
+}  // namespace
+
+int cc::launch_multi(int D, bool mixed, const RhoArgs *rho, const ReduceArgs *red, const ForceArgs *force,
+                     const int *pre, const int *shape, int B, const int total[3], int rho_row, int force_row,
+                     unsigned *queue, cudaStream_t st)
+{
+	if (B < 1)
+		return CC_OK;
+	switch (D) {
+	case 1: return mixed ? multi_launch_raw<1, true>(rho, red, force, pre, shape, B, total, rho_row, force_row, queue, st)
+	                     : multi_launch_raw<1, false>(rho, red, force, pre, shape, B, total, rho_row, force_row, queue, st);
+	case 2: return mixed ? multi_launch_raw<2, true>(rho, red, force, pre, shape, B, total, rho_row, force_row, queue, st)
+	                     : multi_launch_raw<2, false>(rho, red, force, pre, shape, B, total, rho_row, force_row, queue, st);
+	default: return mixed ? multi_launch_raw<3, true>(rho, red, force, pre, shape, B, total, rho_row, force_row, queue, st)
+	                      : multi_launch_raw<3, false>(rho, red, force, pre, shape, B, total, rho_row, force_row, queue, st);
+	}
+}
+
+namespace {
 
 int multi_launch(BatchGroup &g, bool mixed, int which, cudaStream_t st)
 {

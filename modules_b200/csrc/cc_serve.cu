@@ -5,14 +5,15 @@
 //   1. admit every request that has arrived, in arrival order, while a slot is free and the request's device memory
 //      fits the HBM budget (its k-set is planned on the host, its k-set arrays, phase tables, partial sums and L-BFGS
 //      state are allocated from a stream-ordered pool and stay resident until it finishes);
-//   2. run `iters_per_round` L-BFGS iterations for every admitted request at once: per iteration one cooperative batch
-//      evaluation per dimension (cc_batch.cuh) and one launch each of the batched L-BFGS kernels (cc_lbfgs.cuh);
+//   2. run `iters_per_round` L-BFGS iterations for every admitted request at once: per iteration one multi-instance
+//      evaluation per dimension (the persistent rho / reduce / force kernels, cc_multi_launch.h) and one launch each of
+//      the batched L-BFGS kernels (cc_lbfgs.cuh);
 //   3. retire finished requests (time-to-ground-state = completion - arrival) and free their memory.
 // Requests that arrive while others are on the GPU join at the next round, so their work overlaps; an instance's
 // iterates do not depend on the rest of the batch (every sum has a fixed per-instance order), so a request's result
 // is the same alone and in the mix.
 #include "../../include/cc_gpu.h"
-#include "cc_batch.cuh"
+#include "cc_multi_launch.h"
 #include "cc_lbfgs.cuh"
 #include "cc_plan.h"
 
@@ -58,36 +59,13 @@ struct Slot {
 	int64_t N = 0;
 	size_t bytes = 0;
 	unsigned char *mem = nullptr;
-	cc::BInst bi;
+	cc::RhoArgs ra;
+	cc::ReduceArgs rr;
+	cc::ForceArgs fa;
+	int blocks[3], shape[3];   // rho / reduce / force blocks and grid shapes of the multi-instance launches
+	int rho_row, force_row;
 	cc::LbInst li;
 };
-
-template <int D> int grid_for()
-{
-	static int per_sm = -1;
-	if (per_sm < 0) {
-		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cc::cc_batch_kernel<D, 8, false>, cc::kFusedThreads,
-		                                                  0) != cudaSuccess)
-			per_sm = 0;
-	}
-	int sms = 148, dev = 0;
-	cudaGetDevice(&dev);
-	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-	return per_sm * sms;
-}
-
-int launch_batch(int D, cc::BatchArgs &a, cudaStream_t st)
-{
-	void *args[] = {&a};
-	const void *k = D == 1 ? (const void *)cc::cc_batch_kernel<1, 8, false>
-	                       : D == 2 ? (const void *)cc::cc_batch_kernel<2, 8, false>
-	                                : (const void *)cc::cc_batch_kernel<3, 8, false>;
-	const int grid = D == 1 ? grid_for<1>() : D == 2 ? grid_for<2>() : grid_for<3>();
-	if (grid < 1)
-		return sfail(CC_ERR_CUDA, "batch kernel cannot be resident");
-	SV_CUDA(cudaLaunchCooperativeKernel(k, dim3(grid), dim3(cc::kFusedThreads), args, 0, st));
-	return CC_OK;
-}
 
 // Plan and allocate a request; returns CC_OK and fills the slot.
 int open_slot(const cc_request &r, int idx, int m, int nblk_cap, cudaStream_t st, Slot &s)
@@ -102,21 +80,23 @@ int open_slot(const cc_request &r, int idx, int m, int nblk_cap, cudaStream_t st
 	if (!cc::stealthy_kset(d, basis, r.N, r.chi, r.vtype, modes, V) || V.empty())
 		return sfail(CC_ERR_ARG, "request k-set is empty or invalid");
 	cc::Plan p = cc::build_plan(d, (int64_t)V.size(), modes.data(), V.data(), 8);
-	cc::TabSpec g = cc::global_spec(p);
+	const int want = (int)std::max<int64_t>(1, (p.real_segs + cc::kBatchSegsPerSplit - 1) / cc::kBatchSegsPerSplit);
+	cc::ForceSplits fs = cc::force_splits(p, want);
 	double vol = 0, recip[9] = {0};
 	cc::cell_geometry(d, basis, &vol, recip);
 	const int64_t N = r.N;
 	const int n = (int)(N * d);
-	const int Npad = (int)((N + 31) / 32 * 32);
-	const int nsplit = (int)((N + cc::kBatchSplit - 1) / cc::kBatchSplit);
-	const int nks = std::max(1, (int)(p.segs.size() + cc::kBatchSegs - 1) / cc::kBatchSegs);
+	const int nsplit = (int)((N + cc::kBatchPerSplit - 1) / cc::kBatchPerSplit);
+	const int nchunks = (p.nslot + 31) / 32, pgroups = (int)((N + 31) / 32);
+	const int nks = fs.count();
 	Carve c;
 	const size_t o_segs = c.take(sizeof(cc::Seg) * p.segs.size()), o_slotV = c.take(sizeof(double) * p.nslot),
-	             o_tabP = c.take(sizeof(double2) * (size_t)(g.row | 1) * Npad),
-	             o_tabE = c.take(sizeof(double2) * (size_t)g.row * Npad),
-	             o_part = c.take(sizeof(double2) * (size_t)nsplit * p.nslot), o_u = c.take(sizeof(double2) * p.nslot),
-	             o_ep = c.take(sizeof(double) * ((p.nslot + 255) / 256)),
-	             o_pg = c.take(sizeof(double) * (size_t)nks * n), o_fc = c.take(sizeof(unsigned) * ((N + 31) / 32)),
+	             o_bstart = c.take(sizeof(int) * p.bstart.size()), o_bspec = c.take(sizeof(cc::TabSpec) * p.bspec.size()),
+	             o_kstart = c.take(sizeof(int) * fs.start.size()), o_kspec = c.take(sizeof(cc::TabSpec) * fs.spec.size()),
+	             o_part = c.take(sizeof(double2) * (size_t)nsplit * p.nslot), o_rho = c.take(sizeof(double2) * p.nslot),
+	             o_u = c.take(sizeof(double2) * p.nslot), o_ep = c.take(sizeof(double) * nchunks),
+	             o_tk = c.take(sizeof(unsigned)), o_pg = c.take(sizeof(double) * (size_t)nks * n),
+	             o_fc = c.take(sizeof(unsigned) * pgroups),
 	             o_x = c.take(8 * n), o_g = c.take(8 * n), o_d = c.take(8 * n), o_xt = c.take(8 * n), o_gt = c.take(8 * n),
 	             o_S = c.take(8 * (size_t)n * m), o_Y = c.take(8 * (size_t)n * m),
 	             o_lp = c.take(8 * (size_t)nblk_cap * cc::lb_ndots(m)), o_st = c.take(sizeof(cc::LbState));
@@ -125,7 +105,14 @@ int open_slot(const cc_request &r, int idx, int m, int nblk_cap, cudaStream_t st
 	unsigned char *b = s.mem;
 	SV_CUDA(cudaMemcpyAsync(b + o_segs, p.segs.data(), sizeof(cc::Seg) * p.segs.size(), cudaMemcpyHostToDevice, st));
 	SV_CUDA(cudaMemcpyAsync(b + o_slotV, p.slotV.data(), sizeof(double) * p.nslot, cudaMemcpyHostToDevice, st));
-	SV_CUDA(cudaMemsetAsync(b + o_fc, 0, sizeof(unsigned) * ((N + 31) / 32), st));
+	SV_CUDA(cudaMemcpyAsync(b + o_bstart, p.bstart.data(), sizeof(int) * p.bstart.size(), cudaMemcpyHostToDevice, st));
+	SV_CUDA(cudaMemcpyAsync(b + o_bspec, p.bspec.data(), sizeof(cc::TabSpec) * p.bspec.size(), cudaMemcpyHostToDevice,
+	                        st));
+	SV_CUDA(cudaMemcpyAsync(b + o_kstart, fs.start.data(), sizeof(int) * fs.start.size(), cudaMemcpyHostToDevice, st));
+	SV_CUDA(cudaMemcpyAsync(b + o_kspec, fs.spec.data(), sizeof(cc::TabSpec) * fs.spec.size(), cudaMemcpyHostToDevice,
+	                        st));
+	SV_CUDA(cudaMemsetAsync(b + o_tk, 0, sizeof(unsigned), st));
+	SV_CUDA(cudaMemsetAsync(b + o_fc, 0, sizeof(unsigned) * pgroups, st));
 	std::vector<double> x0(n);
 	for (int k = 0; k < n; k++) {
 		double v = r.frac0[k] - std::floor(r.frac0[k]);
@@ -161,37 +148,67 @@ int open_slot(const cc_request &r, int idx, int m, int nblk_cap, cudaStream_t st
 	l.Y = reinterpret_cast<double *>(b + o_Y);
 	l.part = reinterpret_cast<double *>(b + o_lp);
 	l.st = reinterpret_cast<cc::LbState *>(b + o_st);
-	cc::BInst &in = s.bi;
-	std::memset(&in, 0, sizeof(in));
-	in.frac = l.xt;
-	in.E_out = &l.st->Et;
-	in.gfrac_out = l.gt;
-	in.F_out = nullptr;
-	in.status = &l.st->status;
-	in.N = (int)N;
-	in.Npad = Npad;
-	in.segs = reinterpret_cast<const cc::Seg *>(b + o_segs);
-	in.ngroups = p.ngroups();
-	in.nseg = (int)p.segs.size();
-	in.nslot = p.nslot;
-	in.slotV = reinterpret_cast<const double *>(b + o_slotV);
-	in.rho_offset = 0.0;
-	in.inv_vol = 1.0 / vol;
-	in.shift = 0.0;
-	in.spec = g;
-	in.tabP = b + o_tabP;
-	in.tabE = b + o_tabE;
-	in.nsplit = nsplit;
-	in.partial = reinterpret_cast<double2 *>(b + o_part);
-	in.u_slot = reinterpret_cast<double2 *>(b + o_u);
-	in.epart = reinterpret_cast<double *>(b + o_ep);
-	in.nechunk = (p.nslot + 255) / 256;
-	in.nks = nks;
-	in.partialG = reinterpret_cast<double *>(b + o_pg);
-	in.fcounters = reinterpret_cast<unsigned *>(b + o_fc);
+	const int *status = &l.st->status;
+	cc::RhoArgs &ra = s.ra;
+	ra = cc::RhoArgs();
+	ra.frac = l.xt;
+	ra.N = (int)N;
+	ra.per_split = cc::kBatchPerSplit;
+	ra.chunk = cc::kBatchChunk;
+	ra.segs = reinterpret_cast<const cc::Seg *>(b + o_segs);
+	ra.bstart = reinterpret_cast<const int *>(b + o_bstart);
+	ra.bspec = reinterpret_cast<const cc::TabSpec *>(b + o_bspec);
+	ra.nseg = (int)p.segs.size();
+	ra.nslot = p.nslot;
+	ra.partial = reinterpret_cast<double2 *>(b + o_part);
+	ra.skip = status;
+	cc::ReduceArgs &rr = s.rr;
+	rr = cc::ReduceArgs();
+	rr.partial = ra.partial;
+	rr.nsplit = nsplit;
+	rr.nslot = p.nslot;
+	rr.slotV = reinterpret_cast<const double *>(b + o_slotV);
+	rr.rho_offset = 0.0;
+	rr.rho_slot = reinterpret_cast<double2 *>(b + o_rho);
+	rr.u_slot = reinterpret_cast<double2 *>(b + o_u);
+	rr.eblock = reinterpret_cast<double *>(b + o_ep);
+	rr.ticket = reinterpret_cast<unsigned *>(b + o_tk);
+	rr.inv_vol = 1.0 / vol;
+	rr.shift = 0.0;
+	rr.E_out = &l.st->Et;
+	rr.finalize = 0;   // the force kernel sums the energy terms
+	rr.skip = status;
+	cc::ForceArgs &fa = s.fa;
+	fa = cc::ForceArgs();
+	fa.frac = l.xt;
+	fa.N = (int)N;
+	fa.segs = ra.segs;
+	fa.kstart = reinterpret_cast<const int *>(b + o_kstart);
+	fa.kspec = reinterpret_cast<const cc::TabSpec *>(b + o_kspec);
+	fa.nksplit = nks;
+	fa.u_slot = rr.u_slot;
+	fa.nseg = ra.nseg;
+	fa.partialG = reinterpret_cast<double *>(b + o_pg);
+	fa.counters = reinterpret_cast<unsigned *>(b + o_fc);
 	for (int k = 0; k < 9; k++)
-		in.recip[k] = recip[k];
-	in.fscale = 2.0 / vol;
+		fa.recip[k] = recip[k];
+	fa.fscale = 2.0 / vol;
+	fa.F_out = nullptr;
+	fa.gfrac_out = l.gt;
+	fa.eblock = rr.eblock;
+	fa.neblock = nchunks;
+	fa.inv_vol = rr.inv_vol;
+	fa.shift = 0.0;
+	fa.E_out = &l.st->Et;
+	fa.skip = status;
+	s.blocks[0] = p.nbgroups() * nsplit;
+	s.blocks[1] = nchunks;
+	s.blocks[2] = pgroups * nks;
+	s.shape[0] = p.nbgroups();
+	s.shape[1] = nchunks;
+	s.shape[2] = pgroups;
+	s.rho_row = std::max(1, p.block_max_row);
+	s.force_row = std::max(1, fs.max_row);
 	return CC_OK;
 }
 
@@ -200,11 +217,10 @@ size_t estimate_bytes(const cc_request &r, int m, int nblk_cap)
 {
 	const double M = std::ceil(r.chi * (double)r.N * r.d) * 1.1 + 64;
 	const double nseg = M / 4 + 64, nslot = nseg * 8;
-	const double n = (double)r.N * r.d, Npad = (double)((r.N + 31) / 32 * 32);
-	const double row = 128;
-	const double nsplit = std::ceil(r.N / (double)cc::kBatchSplit), nks = std::ceil(nseg / cc::kBatchSegs);
-	const double bytes = 16 * nseg + 8 * nslot + 2 * 16 * row * Npad + 16 * nsplit * nslot + 16 * nslot +
-	                     8 * nks * n + 8 * n * (5 + 2 * m) + 8.0 * nblk_cap * cc::lb_ndots(m) + 8192;
+	const double n = (double)r.N * r.d;
+	const double nsplit = std::ceil(r.N / (double)cc::kBatchPerSplit), nks = std::ceil(nseg / cc::kBatchSegsPerSplit) + 2;
+	const double bytes = 16 * nseg + 8 * nslot + 2 * 768 * (nseg / 256 + nks + 2) + 16 * nsplit * nslot + 32 * nslot +
+	                     8 * nks * n + 8 * n * (5 + 2 * m) + 8.0 * nblk_cap * cc::lb_ndots(m) + 16384;
 	return (size_t)bytes;
 }
 
@@ -237,16 +253,21 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 	const int nblk_cap = 32;
 	cudaStream_t st;
 	SV_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-	// device descriptor arrays sized for max_slots
-	cc::BInst *d_bi = nullptr;
+	// device descriptor arrays sized for max_slots; one work queue (6 words) per dimension
+	cc::RhoArgs *d_ra = nullptr;
+	cc::ReduceArgs *d_rr = nullptr;
+	cc::ForceArgs *d_fa = nullptr;
 	cc::LbInst *d_li = nullptr;
-	int *d_pre = nullptr;
-	unsigned *d_bar = nullptr;
-	SV_CUDA(cudaMalloc(&d_bi, sizeof(cc::BInst) * o.max_slots));
+	int *d_pre = nullptr, *d_shape = nullptr;
+	unsigned *d_queue = nullptr;
+	SV_CUDA(cudaMalloc(&d_ra, sizeof(cc::RhoArgs) * o.max_slots));
+	SV_CUDA(cudaMalloc(&d_rr, sizeof(cc::ReduceArgs) * o.max_slots));
+	SV_CUDA(cudaMalloc(&d_fa, sizeof(cc::ForceArgs) * o.max_slots));
 	SV_CUDA(cudaMalloc(&d_li, sizeof(cc::LbInst) * o.max_slots));
-	SV_CUDA(cudaMalloc(&d_pre, sizeof(int) * 4 * (o.max_slots + 1) * 3));
-	SV_CUDA(cudaMalloc(&d_bar, 16));
-	SV_CUDA(cudaMemset(d_bar, 0, 16));
+	SV_CUDA(cudaMalloc(&d_pre, sizeof(int) * 3 * (o.max_slots + 3)));
+	SV_CUDA(cudaMalloc(&d_shape, sizeof(int) * 3 * o.max_slots));
+	SV_CUDA(cudaMalloc(&d_queue, sizeof(unsigned) * 18));
+	SV_CUDA(cudaMemset(d_queue, 0, sizeof(unsigned) * 18));
 	std::vector<int> order(count);
 	for (int i = 0; i < count; i++)
 		order[i] = i;
@@ -293,47 +314,58 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 			li[a] = active[a].li;
 			maxn = std::max(maxn, li[a].n);
 		}
-		std::vector<cc::BInst> bi;
-		std::vector<int> pre;
+		std::vector<cc::RhoArgs> ra;
+		std::vector<cc::ReduceArgs> rr;
+		std::vector<cc::ForceArgs> fa;
+		std::vector<int> pre, shape;
 		struct G {
-			int D, off, B, pre_off;
+			int D, off, B, pre_off, shape_off, total[3], rho_row, force_row;
 		};
 		std::vector<G> groups;
 		for (int D = 1; D <= 3; D++) {
-			G g = {D, (int)bi.size(), 0, (int)pre.size()};
+			G g = {D, (int)ra.size(), 0, (int)pre.size(), (int)shape.size(), {0, 0, 0}, 1, 1};
+			std::vector<int> members;
 			for (int a = 0; a < A; a++)
-				if (active[a].d == D) {
-					bi.push_back(active[a].bi);
-					g.B++;
-				}
-			if (!g.B)
+				if (active[a].d == D)
+					members.push_back(a);
+			if (members.empty())
 				continue;
-			std::vector<int> p4(4 * (g.B + 1), 0);
+			g.B = (int)members.size();
+			std::vector<int> p3(3 * (g.B + 1), 0), s3(3 * g.B, 0);
 			for (int k = 0; k < g.B; k++) {
-				const cc::BInst &in = bi[g.off + k];
-				const int c[4] = {(in.N * in.spec.items + cc::kFusedThreads - 1) / cc::kFusedThreads,
-				                  in.ngroups * in.nsplit, in.nechunk, ((in.N + 31) / 32) * in.nks};
-				for (int ph = 0; ph < 4; ph++)
-					p4[ph * (g.B + 1) + k + 1] = p4[ph * (g.B + 1) + k] + c[ph];
+				const Slot &sl = active[members[k]];
+				ra.push_back(sl.ra);
+				rr.push_back(sl.rr);
+				fa.push_back(sl.fa);
+				for (int ph = 0; ph < 3; ph++) {
+					p3[ph * (g.B + 1) + k + 1] = p3[ph * (g.B + 1) + k] + sl.blocks[ph];
+					s3[ph * g.B + k] = sl.shape[ph];
+				}
+				g.rho_row = std::max(g.rho_row, sl.rho_row);
+				g.force_row = std::max(g.force_row, sl.force_row);
 			}
-			pre.insert(pre.end(), p4.begin(), p4.end());
+			for (int ph = 0; ph < 3; ph++)
+				g.total[ph] = p3[ph * (g.B + 1) + g.B];
+			pre.insert(pre.end(), p3.begin(), p3.end());
+			shape.insert(shape.end(), s3.begin(), s3.end());
 			groups.push_back(g);
 		}
-		SV_CUDA(cudaMemcpyAsync(d_bi, bi.data(), sizeof(cc::BInst) * bi.size(), cudaMemcpyHostToDevice, st));
+		SV_CUDA(cudaMemcpyAsync(d_ra, ra.data(), sizeof(cc::RhoArgs) * ra.size(), cudaMemcpyHostToDevice, st));
+		SV_CUDA(cudaMemcpyAsync(d_rr, rr.data(), sizeof(cc::ReduceArgs) * rr.size(), cudaMemcpyHostToDevice, st));
+		SV_CUDA(cudaMemcpyAsync(d_fa, fa.data(), sizeof(cc::ForceArgs) * fa.size(), cudaMemcpyHostToDevice, st));
 		SV_CUDA(cudaMemcpyAsync(d_li, li.data(), sizeof(cc::LbInst) * A, cudaMemcpyHostToDevice, st));
 		SV_CUDA(cudaMemcpyAsync(d_pre, pre.data(), sizeof(int) * pre.size(), cudaMemcpyHostToDevice, st));
+		SV_CUDA(cudaMemcpyAsync(d_shape, shape.data(), sizeof(int) * shape.size(), cudaMemcpyHostToDevice, st));
+		// the descriptor vectors are pageable: the copies complete before the iterations read them
 		const int nblk = std::max(1, std::min(nblk_cap, maxn / 2048));
 		for (int it = 0; it < o.iters_per_round && rc == CC_OK; it++) {
-			for (const G &g : groups) {
-				cc::BatchArgs ba;
-				ba.inst = d_bi + g.off;
-				ba.B = g.B;
-				for (int k = 0; k < 4; k++)
-					ba.pre[k] = d_pre + g.pre_off + k * (g.B + 1);
-				ba.bar = d_bar;
-				if ((rc = launch_batch(g.D, ba, st)))
+			for (const G &g : groups)
+				if ((rc = cc::launch_multi(g.D, false, d_ra + g.off, d_rr + g.off, d_fa + g.off, d_pre + g.pre_off,
+				                           d_shape + g.shape_off, g.B, g.total, g.rho_row, g.force_row,
+				                           d_queue + 6 * (g.D - 1), st))) {
+					s_err = std::string("serve: ") + cc_last_error();
 					break;
-			}
+				}
 			if (rc)
 				break;
 			cc::lb_dots_kernel<<<dim3(nblk, A), cc::kLbThreads, 0, st>>>(d_li, nblk);
@@ -349,12 +381,6 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 		for (int a = 0; a < A; a++)
 			SV_CUDA(cudaMemcpyAsync(&hs[a], active[a].li.st, offsetof(cc::LbState, w), cudaMemcpyDeviceToHost, st));
 		SV_CUDA(cudaStreamSynchronize(st));
-		unsigned bar[3];
-		SV_CUDA(cudaMemcpy(bar, d_bar, sizeof(bar), cudaMemcpyDeviceToHost));
-		if (bar[2]) {
-			rc = sfail(CC_ERR_TIMEOUT, "serve: a grid barrier wait ran out");
-			break;
-		}
 		const double tdone = now();
 		std::vector<Slot> keep;
 		for (int a = 0; a < A; a++) {
@@ -378,10 +404,13 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 	cudaStreamSynchronize(st);
 	if (wall_s)
 		*wall_s = now();
-	cudaFree(d_bi);
+	cudaFree(d_ra);
+	cudaFree(d_rr);
+	cudaFree(d_fa);
 	cudaFree(d_li);
 	cudaFree(d_pre);
-	cudaFree(d_bar);
+	cudaFree(d_shape);
+	cudaFree(d_queue);
 	cudaStreamDestroy(st);
 	return rc;
 }
