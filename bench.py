@@ -298,6 +298,7 @@ def run_extras(args, cc, torch):
     pots, Ns, fracs, pairs = batched_workload(cc, args.batch)
     batch = cc.CCBatch(pots, Ns)
     batch.set_positions(fracs)
+    tile = batch.autotune(reps=2)   # tile shapes chosen by timing the candidates on this batch
     st = torch.cuda.Stream()
     with torch.cuda.stream(st):
         for _ in range(3):
@@ -314,7 +315,8 @@ def run_extras(args, cc, torch):
     ms = a.elapsed_time(b) / reps
     out["batched"] = {"workload": f"{args.batch} instances, d in {{2,3}}, N log-uniform [200,5000], chi U[0.10,0.49], "
                                   "v=(1-|k|/K)^2, FP64", "ms_per_step": ms, "instance_evals_per_s": args.batch / (ms / 1e3),
-                      "pairs_per_s": pairs / (ms / 1e3), "launches_per_step": 2}
+                      "pairs_per_s": pairs / (ms / 1e3), "launches_per_step": 3 * len({p.d for p in pots}),
+                      "autotuned_tile": {"particles_per_rho_block": tile[0], "segments_per_force_block": tile[1]}}
     del batch
     # ground states per second: the plain single-configuration FP64 path, one instance after another, against the
     # batched minimisation of the same instances (mixed precision until E/N <= 1e-10, then FP64)
@@ -336,6 +338,8 @@ def run_extras(args, cc, torch):
         plain_E.append(E / n)
     t_plain = time.perf_counter() - t0
     gb = cc.CCBatch(gpots, gN)
+    gb.set_positions(gfr)
+    gb.autotune(reps=2)
     t0 = time.perf_counter()
     xs, E, ev, it, stt = gb.minimize(gfr, precision=cc.PREC_SCHEDULE, switch_energy_per_particle=1e-10)
     t_batch = time.perf_counter() - t0

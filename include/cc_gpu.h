@@ -146,6 +146,12 @@ int cc_batch_energy_grad(cc_batch *b, double *E, double *const *F, int precision
 int cc_batch_eval_device(cc_batch *b, int precision, void *stream);
 /* Minimise every instance from its bound positions; frac[i] (host) receives the results, results[i] the outcomes. */
 int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opts, cc_lbfgs_result *results);
+/* Autotuner of the batch's tile shapes: times `reps` FP64 evaluations of the bound positions for every candidate
+ * (particles per rho block 32 / 64 / 128 / 256 / 512 x segments per force block 32 / 64 / 128 / 256) with CUDA events and keeps
+ * the fastest for the batch's later evaluations and minimisations (default before tuning: 64 x 64). The chosen shape
+ * is returned in *per_split and *segs_per_split (either may be NULL). Results of different shapes agree to rounding;
+ * with one shape every instance's result is independent of the rest of the batch. */
+int cc_batch_autotune(cc_batch *b, int reps, int *per_split, int *segs_per_split);
 
 /* --- Monte Carlo moves ----------------------------------------------------------------------------------------------
  * Replace ShiftedCCPotential_ForMC::TryMove / AcceptMove (potential/CollectiveCoordinatePotential.h:1906-1957): the

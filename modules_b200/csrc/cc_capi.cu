@@ -2189,6 +2189,15 @@ using cc::kBatchChunk;
 using cc::kBatchPerSplit;
 using cc::kBatchSegsPerSplit;
 
+// an instance's evaluation buffers in the batch arena
+struct BatchBufs {
+	size_t o_part, o_rho, o_u, o_eb, o_tk, o_pg, o_fc;
+};
+
+// tile shapes the autotuner times: particles per rho block, segments per force block
+constexpr int kTuneSplits[] = {32, 64, 128, 256, 512};
+constexpr int kTuneSegs[] = {32, 64, 128, 256};
+
 }  // namespace
 
 struct cc_batch {
@@ -2197,6 +2206,8 @@ struct cc_batch {
 	std::vector<BatchGroup> groups;
 	Arena arena;
 	std::vector<size_t> off_frac, off_F, off_E;
+	std::vector<BatchBufs> bufs;
+	int per_split = 0, segs_per_split = 0;   // the tile shape in use
 	cudaStream_t stream = nullptr;
 };
 
@@ -2277,6 +2288,100 @@ int multi_launch(BatchGroup &g, bool mixed, int which, cudaStream_t st)
 	}
 }
 
+// (Re)build every group's evaluation descriptors (set 0) for a tile shape: per_split particles per rho block and
+// force splits of about segs_per_split segments; the arena holds the buffers of every candidate shape.
+int batch_build(cc_batch *b, int per_split, int segs_per_split)
+{
+	for (BatchGroup &g : b->groups) {
+		const int B = (int)g.members.size();
+		std::vector<int> pre(3 * (B + 1), 0), shape(3 * B, 0);
+		g.rho.clear();
+		g.red.clear();
+		g.force.clear();
+		g.rho_row = g.force_row = 1;
+		for (int k = 0; k < B; k++) {
+			const int i = g.members[k];
+			cc_handle *h = b->h[i];
+			const cc::Plan &p = h->main.plan;
+			const BatchBufs &q = b->bufs[i];
+			const int64_t n = b->N[i];
+			const int nsplit = (int)((n + per_split - 1) / per_split);
+			const int nchunks = (p.nslot + 31) / 32, pgroups = (int)((n + 31) / 32);
+			const DevSplits *f = nullptr;
+			const int want = (int)std::max<int64_t>(1, (p.real_segs + segs_per_split - 1) / segs_per_split);
+			if (int rc = get_splits(h->main, want, &f))
+				return rc;
+			cc::RhoArgs ra = {};
+			ra.frac = b->arena.at<double>(b->off_frac[i]);
+			ra.N = (int)n;
+			ra.per_split = per_split;
+			ra.chunk = kBatchChunk;
+			ra.segs = h->main.segs;
+			ra.bstart = h->main.bstart;
+			ra.bspec = h->main.bspec;
+			ra.nseg = (int)p.segs.size();
+			ra.nslot = p.nslot;
+			ra.partial = b->arena.at<double2>(q.o_part);
+			cc::ReduceArgs rr = {};
+			rr.partial = ra.partial;
+			rr.nsplit = nsplit;
+			rr.nslot = p.nslot;
+			rr.slotV = h->main.slotV;
+			rr.rho_offset = h->rho_offset;
+			rr.rho_slot = b->arena.at<double2>(q.o_rho);
+			rr.u_slot = b->arena.at<double2>(q.o_u);
+			rr.eblock = b->arena.at<double>(q.o_eb);
+			rr.ticket = b->arena.at<unsigned>(q.o_tk);
+			rr.inv_vol = 1.0 / h->volume;
+			rr.shift = h->shift;
+			rr.E_out = b->arena.at<double>(b->off_E[i]);
+			rr.finalize = 0;   // the force kernel sums the energy terms
+			cc::ForceArgs fa = {};
+			fa.frac = ra.frac;
+			fa.N = ra.N;
+			fa.segs = h->main.segs;
+			fa.kstart = f->kstart;
+			fa.kspec = f->kspec;
+			fa.nksplit = f->host.count();
+			fa.u_slot = rr.u_slot;
+			fa.nseg = ra.nseg;
+			fa.partialG = b->arena.at<double>(q.o_pg);
+			fa.counters = b->arena.at<unsigned>(q.o_fc);
+			for (int c = 0; c < 9; c++)
+				fa.recip[c] = h->recip[c];
+			fa.fscale = 2.0 / h->volume;
+			fa.F_out = b->arena.at<double>(b->off_F[i]);
+			fa.gfrac_out = nullptr;
+			fa.eblock = rr.eblock;
+			fa.neblock = nchunks;
+			fa.inv_vol = rr.inv_vol;
+			fa.shift = rr.shift;
+			fa.E_out = rr.E_out;
+			g.rho.push_back(ra);
+			g.red.push_back(rr);
+			g.force.push_back(fa);
+			const int c[3] = {p.nbgroups() * nsplit, nchunks, pgroups * fa.nksplit};
+			const int sh[3] = {p.nbgroups(), nchunks, pgroups};
+			for (int ph = 0; ph < 3; ph++) {
+				pre[ph * (B + 1) + k + 1] = pre[ph * (B + 1) + k] + c[ph];
+				shape[ph * B + k] = sh[ph];
+			}
+			g.rho_row = std::max(g.rho_row, p.block_max_row);
+			g.force_row = std::max(g.force_row, f->host.max_row);
+		}
+		for (int ph = 0; ph < 3; ph++)
+			g.total[ph] = pre[ph * (B + 1) + B];
+		int rc;
+		if ((rc = upload_into(g.d_rho[0], g.rho)) || (rc = upload_into(g.d_red[0], g.red)) ||
+		    (rc = upload_into(g.d_force[0], g.force)) || (rc = upload_into(g.d_pre, pre)) ||
+		    (rc = upload_into(g.d_shape, shape)))
+			return rc;
+	}
+	b->per_split = per_split;
+	b->segs_per_split = segs_per_split;
+	return CC_OK;
+}
+
 // evaluate every group with the given descriptors (lb = the minimisation's); precision CC_PREC_SCHEDULE launches
 // the mixed and the FP64 kernels, each evaluating the instances of its stage
 int batch_eval(cc_batch *b, bool lb, int precision, cudaStream_t st)
@@ -2312,41 +2417,39 @@ int cc_batch_create(int count, cc_handle *const *handles, const int64_t *N, cc_b
 	cc_batch *b = new cc_batch();
 	b->h.assign(handles, handles + count);
 	b->N.assign(N, N + count);
-	// per instance: launch shapes, force splits (cached on the handle's k-set) and buffer offsets in one arena
-	struct Sizes {
-		int nsplit, nchunks, pgroups, nks, max_row;
-		const DevSplits *f;
-		size_t o_part, o_rho, o_u, o_eb, o_tk, o_pg, o_fc;
-	};
-	std::vector<Sizes> z(count);
+	// per instance: buffers sized for every tile shape the autotuner may choose (the most particle splits and force
+	// splits among the candidates), carved out of one arena
 	b->off_frac.resize(count);
 	b->off_F.resize(count);
 	b->off_E.resize(count);
+	b->bufs.resize(count);
 	for (int i = 0; i < count; i++) {
 		cc_handle *h = handles[i];
 		const cc::Plan &p = h->main.plan;
 		const int64_t n = N[i];
-		Sizes &q = z[i];
-		q.nsplit = (int)((n + kBatchPerSplit - 1) / kBatchPerSplit);
-		q.nchunks = (p.nslot + 31) / 32;
-		q.pgroups = (int)((n + 31) / 32);
-		const int want = (int)std::max<int64_t>(1, (p.real_segs + kBatchSegsPerSplit - 1) / kBatchSegsPerSplit);
-		if (int rc = get_splits(h->main, want, &q.f)) {
-			delete b;
-			return rc;
+		BatchBufs &q = b->bufs[i];
+		int max_nks = 1;
+		for (int segs : kTuneSegs) {
+			const DevSplits *f = nullptr;
+			const int want = (int)std::max<int64_t>(1, (p.real_segs + segs - 1) / segs);
+			if (int rc = get_splits(h->main, want, &f)) {
+				delete b;
+				return rc;
+			}
+			max_nks = std::max(max_nks, f->host.count());
 		}
-		q.nks = q.f->host.count();
-		q.max_row = q.f->host.max_row;
+		const int max_nsplit = (int)((n + kTuneSplits[0] - 1) / kTuneSplits[0]);
+		const int nchunks = (p.nslot + 31) / 32, pgroups = (int)((n + 31) / 32);
 		b->off_frac[i] = b->arena.take(sizeof(double) * n * h->d);
 		b->off_F[i] = b->arena.take(sizeof(double) * n * h->d);
 		b->off_E[i] = b->arena.take(sizeof(double));
-		q.o_part = b->arena.take(sizeof(double2) * (size_t)q.nsplit * p.nslot);
+		q.o_part = b->arena.take(sizeof(double2) * (size_t)max_nsplit * p.nslot);
 		q.o_rho = b->arena.take(sizeof(double2) * p.nslot);
 		q.o_u = b->arena.take(sizeof(double2) * p.nslot);
-		q.o_eb = b->arena.take(sizeof(double) * q.nchunks);
+		q.o_eb = b->arena.take(sizeof(double) * nchunks);
 		q.o_tk = b->arena.take(sizeof(unsigned));
-		q.o_pg = b->arena.take(sizeof(double) * (size_t)q.nks * n * h->d);
-		q.o_fc = b->arena.take(sizeof(unsigned) * q.pgroups);
+		q.o_pg = b->arena.take(sizeof(double) * (size_t)max_nks * n * h->d);
+		q.o_fc = b->arena.take(sizeof(unsigned) * pgroups);
 	}
 	int rc;
 	if ((rc = dev_alloc(&b->arena.base, b->arena.used))) {
@@ -2359,7 +2462,7 @@ int cc_batch_create(int count, cc_handle *const *handles, const int64_t *N, cc_b
 		cc_batch_destroy(b);
 		return fail(CC_ERR_CUDA, "batch initialisation failed");
 	}
-	// one group per dimension
+	// one group per dimension, instances by decreasing work (the work queues then hand out the longest items first)
 	for (int D = 1; D <= 3; D++) {
 		BatchGroup g;
 		g.D = D;
@@ -2368,89 +2471,73 @@ int cc_batch_create(int count, cc_handle *const *handles, const int64_t *N, cc_b
 				g.members.push_back(i);
 		if (g.members.empty())
 			continue;
-		// largest instances first: the work queues then hand out the longest items first
 		std::stable_sort(g.members.begin(), g.members.end(), [&](int x, int y) {
 			return (double)N[x] * handles[x]->main.plan.real_segs > (double)N[y] * handles[y]->main.plan.real_segs;
 		});
 		const int B = (int)g.members.size();
-		std::vector<int> pre(3 * (B + 1), 0), shape(3 * B, 0);
-		for (int k = 0; k < B; k++) {
-			const int i = g.members[k];
-			cc_handle *h = handles[i];
-			const cc::Plan &p = h->main.plan;
-			const Sizes &q = z[i];
-			cc::RhoArgs ra = {};
-			ra.frac = b->arena.at<double>(b->off_frac[i]);
-			ra.N = (int)N[i];
-			ra.per_split = kBatchPerSplit;
-			ra.chunk = kBatchChunk;
-			ra.segs = h->main.segs;
-			ra.bstart = h->main.bstart;
-			ra.bspec = h->main.bspec;
-			ra.nseg = (int)p.segs.size();
-			ra.nslot = p.nslot;
-			ra.partial = b->arena.at<double2>(q.o_part);
-			cc::ReduceArgs rr = {};
-			rr.partial = ra.partial;
-			rr.nsplit = q.nsplit;
-			rr.nslot = p.nslot;
-			rr.slotV = h->main.slotV;
-			rr.rho_offset = h->rho_offset;
-			rr.rho_slot = b->arena.at<double2>(q.o_rho);
-			rr.u_slot = b->arena.at<double2>(q.o_u);
-			rr.eblock = b->arena.at<double>(q.o_eb);
-			rr.ticket = b->arena.at<unsigned>(q.o_tk);
-			rr.inv_vol = 1.0 / h->volume;
-			rr.shift = h->shift;
-			rr.E_out = b->arena.at<double>(b->off_E[i]);
-			rr.finalize = 0;   // the force kernel sums the energy terms
-			cc::ForceArgs fa = {};
-			fa.frac = ra.frac;
-			fa.N = ra.N;
-			fa.segs = h->main.segs;
-			fa.kstart = q.f->kstart;
-			fa.kspec = q.f->kspec;
-			fa.nksplit = q.nks;
-			fa.u_slot = rr.u_slot;
-			fa.nseg = ra.nseg;
-			fa.partialG = b->arena.at<double>(q.o_pg);
-			fa.counters = b->arena.at<unsigned>(q.o_fc);
-			for (int c = 0; c < 9; c++)
-				fa.recip[c] = h->recip[c];
-			fa.fscale = 2.0 / h->volume;
-			fa.F_out = b->arena.at<double>(b->off_F[i]);
-			fa.gfrac_out = nullptr;
-			fa.eblock = rr.eblock;
-			fa.neblock = q.nchunks;
-			fa.inv_vol = rr.inv_vol;
-			fa.shift = rr.shift;
-			fa.E_out = rr.E_out;
-			g.rho.push_back(ra);
-			g.red.push_back(rr);
-			g.force.push_back(fa);
-			const int c[3] = {p.nbgroups() * q.nsplit, q.nchunks, q.pgroups * q.nks};
-			const int sh[3] = {p.nbgroups(), q.nchunks, q.pgroups};
-			for (int ph = 0; ph < 3; ph++) {
-				pre[ph * (B + 1) + k + 1] = pre[ph * (B + 1) + k] + c[ph];
-				shape[ph * B + k] = sh[ph];
-			}
-			g.rho_row = std::max(g.rho_row, p.block_max_row);
-			g.force_row = std::max(g.force_row, q.max_row);
-		}
-		for (int ph = 0; ph < 3; ph++)
-			g.total[ph] = pre[ph * (B + 1) + B];
-		if ((rc = upload(&g.d_rho[0], g.rho)) || (rc = upload(&g.d_red[0], g.red)) ||
-		    (rc = upload(&g.d_force[0], g.force)) || (rc = dev_alloc(&g.d_rho[1], B)) ||
-		    (rc = dev_alloc(&g.d_red[1], B)) || (rc = dev_alloc(&g.d_force[1], B)) || (rc = upload(&g.d_pre, pre)) ||
-		    (rc = upload(&g.d_shape, shape)) || (rc = dev_alloc(&g.d_queue, 6)) ||
-		    (rc = (cudaMemset(g.d_queue, 0, 6 * sizeof(unsigned)) == cudaSuccess ? CC_OK : CC_ERR_CUDA))) {
-			b->groups.push_back(g);
+		b->groups.push_back(g);
+		BatchGroup &gg = b->groups.back();
+		if ((rc = dev_alloc(&gg.d_rho[0], B)) || (rc = dev_alloc(&gg.d_red[0], B)) ||
+		    (rc = dev_alloc(&gg.d_force[0], B)) || (rc = dev_alloc(&gg.d_rho[1], B)) ||
+		    (rc = dev_alloc(&gg.d_red[1], B)) || (rc = dev_alloc(&gg.d_force[1], B)) ||
+		    (rc = dev_alloc(&gg.d_pre, 3 * (B + 1))) || (rc = dev_alloc(&gg.d_shape, 3 * B)) ||
+		    (rc = dev_alloc(&gg.d_queue, 6)) ||
+		    (rc = (cudaMemset(gg.d_queue, 0, 6 * sizeof(unsigned)) == cudaSuccess ? CC_OK : CC_ERR_CUDA))) {
 			cc_batch_destroy(b);
 			return rc;
 		}
-		b->groups.push_back(g);
+	}
+	if ((rc = batch_build(b, kBatchPerSplit, kBatchSegsPerSplit))) {
+		cc_batch_destroy(b);
+		return rc;
 	}
 	*out = b;
+	return CC_OK;
+}
+
+int cc_batch_autotune(cc_batch *b, int reps, int *per_split, int *segs_per_split)
+{
+	if (!b || reps < 1)
+		return fail(CC_ERR_ARG, "invalid autotune arguments");
+	cudaEvent_t e0, e1;
+	CC_CUDA(cudaEventCreate(&e0));
+	CC_CUDA(cudaEventCreate(&e1));
+	float best = 1e30f;
+	int bp = b->per_split, bs = b->segs_per_split, rc = CC_OK;
+	for (int ps : kTuneSplits)
+		for (int sg : kTuneSegs) {
+			if ((rc = batch_build(b, ps, sg)) || (rc = batch_eval(b, false, CC_PREC_FP64, b->stream)))
+				break;
+			if (cudaEventRecord(e0, b->stream) != cudaSuccess) {
+				rc = fail(CC_ERR_CUDA, "cudaEventRecord failed");
+				break;
+			}
+			for (int r = 0; r < reps && rc == CC_OK; r++)
+				rc = batch_eval(b, false, CC_PREC_FP64, b->stream);
+			if (rc)
+				break;
+			float ms = 0.0f;
+			if (cudaEventRecord(e1, b->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+			    cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+				rc = fail(CC_ERR_CUDA, "autotune timing failed");
+				break;
+			}
+			if (ms < best) {
+				best = ms;
+				bp = ps;
+				bs = sg;
+			}
+		}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	if (rc)
+		return rc;
+	if ((rc = batch_build(b, bp, bs)))
+		return rc;
+	if (per_split)
+		*per_split = bp;
+	if (segs_per_split)
+		*segs_per_split = bs;
 	return CC_OK;
 }
 

@@ -71,3 +71,18 @@ def test_batch_precision_schedule_reaches_ground_states(gpu):
     xs, E, evals, iters, status = batch.minimize(fracs, precision=gpu.PREC_SCHEDULE, switch_energy_per_particle=1e-10)
     print("schedule:", [f"{e / n:.1e}" for e, n in zip(E, N)], evals.tolist(), status.tolist())
     assert np.all(E / np.array(N) < 1e-20)
+
+
+def test_batch_autotune_keeps_results(gpu):
+    """The autotuner picks one of the candidate tile shapes; results before and after agree to rounding, and a tuned
+    batch still evaluates every instance as before within 1e-12 relative."""
+    pots, N, fracs = _instances(gpu, SPECS, seed=11)
+    batch = gpu.CCBatch(pots, N)
+    batch.set_positions(fracs)
+    E0, F0 = batch.energy_and_forces()
+    ps, sg = batch.autotune(reps=1)
+    assert ps in (32, 64, 128, 256, 512) and sg in (32, 64, 128, 256)
+    E1, F1 = batch.energy_and_forces()
+    for e0, e1, f0, f1 in zip(E0, E1, F0, F1):
+        assert abs(e1 - e0) <= 1e-12 * abs(e0)
+        assert np.abs(f1 - f0).max() <= 1e-12 * max(np.abs(f0).max(), 1.0)
