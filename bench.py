@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--batch", type=int, default=512, help="instances of the batched uneven workload")
     ap.add_argument("--gs-instances", type=int, default=48, help="instances of the ground-states/s comparison")
     ap.add_argument("--served", type=int, default=300, help="requests of the served sample")
+    ap.add_argument("--served-rate", type=float, default=60.0, help="Poisson arrival rate of the served stream (1/s)")
+    ap.add_argument("--served-full", action="store_true",
+                    help="the served stream's full distribution: N clipped to [100, 20000], chi U[0.05, 0.49]")
     return ap.parse_args()
 
 
@@ -354,18 +357,19 @@ def run_extras(args, cc, torch):
     # served stream (a bounded sample of the 10000-request workload)
     rng = np.random.default_rng(99)
     reqs, t = [], 0.0
-    rate = 60.0
+    rate = args.served_rate
+    nmax, chimax = (20000, 0.49) if args.served_full else (4000, 0.40)
     for _ in range(args.served):
         t += rng.exponential(1.0 / rate)
         d = int(rng.choice([2, 3]))
-        n = int(np.clip(np.exp(rng.normal(np.log(1000), 0.6)), 100, 4000))
-        chi = float(rng.uniform(0.05, 0.40))
+        n = int(np.clip(np.exp(rng.normal(np.log(1000), 0.6)), 100, nmax))
+        chi = float(rng.uniform(0.05, chimax))
         reqs.append(dict(d=d, N=n, chi=chi, vtype=int(rng.choice([0, 3])), frac0=rng.random((n, d)), arrival_s=t))
     res, wall = cc.serve(reqs, iters_per_round=16)
     lat = np.array([r["t_done"] - q["arrival_s"] for r, q in zip(res, reqs)])
     ok = np.array([r["E"] / q["N"] < 1e-20 for r, q in zip(res, reqs)])
-    out["served"] = {"workload": f"{args.served} requests, Poisson arrivals at {rate:.0f}/s, d in {{2,3}}, N log-normal "
-                                 "(median 1000, clipped to [100,4000]), chi U[0.05,0.40], v in {1,(1-|k|/K)^2}",
+    out["served"] = {"workload": f"{args.served} requests, Poisson arrivals at {rate:g}/s, d in {{2,3}}, N log-normal "
+                                 f"(median 1000, clipped to [100,{nmax}]), chi U[0.05,{chimax:g}], v in {{1,(1-|k|/K)^2}}",
                      "ground_states_per_s": len(reqs) / wall, "p50_ms": float(np.percentile(lat, 50) * 1e3),
                      "p99_ms": float(np.percentile(lat, 99) * 1e3), "reached": int(ok.sum()), "wall_s": wall}
     return out
