@@ -2252,6 +2252,42 @@ int multi_launch_raw(const cc::RhoArgs *rho, const cc::ReduceArgs *red, const cc
 	return CC_OK;
 }
 
+template <int D> cudaError_t multi_sched_attrs()
+{
+	static cudaError_t e = [] {
+		cudaError_t r = cudaFuncSetAttribute(cc::cc_mrho_sched_kernel<D, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                                     (int)rho_smem<double2>(cc::kMaxRow, kBatchChunk, 8));
+		if (r == cudaSuccess)
+			r = cudaFuncSetAttribute(cc::cc_mforce_sched_kernel<D, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			                         (int)force_smem<double2>(cc::kMaxRow, D));
+		return r;
+	}();
+	return e;
+}
+
+// one launch of each kernel for a group whose instances take their precision from their stage words
+template <int D> int multi_launch_sched_t(BatchGroup &g, int which, cudaStream_t st)
+{
+	if (cudaError_t attr = multi_sched_attrs<D>())
+		return fail(CC_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(attr));
+	const int B = (int)g.members.size();
+	const int res3 = 3 * sm_count(), res8 = 8 * sm_count();
+	if (g.total[0] > 0)
+		CC_CUDA(launch_pdl_n(cc::cc_mrho_sched_kernel<D, 8>, dim3(std::min(g.total[0], res3)), dim3(cc::kRhoThreads),
+		                   rho_smem<double2>(g.rho_row, kBatchChunk, 8), st, (const cc::RhoArgs *)g.d_rho[which],
+		                   (const int *)g.d_pre, (const int *)g.d_shape, B, g.d_queue));
+	if (g.total[1] > 0)
+		CC_CUDA(launch_pdl_n(cc::cc_mreduce_kernel, dim3(std::min(g.total[1], res8)), dim3(cc::kRedThreads), 0, st,
+		                   (const cc::ReduceArgs *)g.d_red[which], (const int *)g.d_pre + (B + 1),
+		                   (const int *)g.d_shape + B, B, -1, g.d_queue + 2));
+	if (g.total[2] > 0)
+		CC_CUDA(launch_pdl_n(cc::cc_mforce_sched_kernel<D, 8>, dim3(std::min(g.total[2], res3)),
+		                   dim3(cc::kForceThreads), force_smem<double2>(g.force_row, D), st,
+		                   (const cc::ForceArgs *)g.d_force[which], (const int *)g.d_pre + 2 * (B + 1),
+		                   (const int *)g.d_shape + 2 * B, B, g.d_queue + 4));
+	return CC_OK;
+}
+
 // the three launches of one group: which = 0 (batch positions) or 1 (minimisation trial points)
 template <int D, bool MIXED> int multi_launch_t(BatchGroup &g, int which, cudaStream_t st)
 {
@@ -2383,14 +2419,15 @@ int batch_build(cc_batch *b, int per_split, int segs_per_split)
 }
 
 // evaluate every group with the given descriptors (lb = the minimisation's); precision CC_PREC_SCHEDULE launches
-// the mixed and the FP64 kernels, each evaluating the instances of its stage
+// kernels that evaluate each instance at the precision of its stage word (FP64 where it has none)
 int batch_eval(cc_batch *b, bool lb, int precision, cudaStream_t st)
 {
 	for (BatchGroup &g : b->groups) {
 		if (precision == CC_PREC_SCHEDULE) {
-			if (int rc = multi_launch(g, true, lb ? 1 : 0, st))
-				return rc;
-			if (int rc = multi_launch(g, false, lb ? 1 : 0, st))
+			const int rc = g.D == 1 ? multi_launch_sched_t<1>(g, lb ? 1 : 0, st)
+			             : g.D == 2 ? multi_launch_sched_t<2>(g, lb ? 1 : 0, st)
+			                        : multi_launch_sched_t<3>(g, lb ? 1 : 0, st);
+			if (rc)
 				return rc;
 		} else if (int rc = multi_launch(g, precision == CC_PREC_MIXED, lb ? 1 : 0, st)) {
 			return rc;
@@ -2723,7 +2760,8 @@ int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opt
 	}
 	cudaStream_t st = b->stream;
 	const bool sched = o.precision == CC_PREC_SCHEDULE;
-	// schedule: both kernels per iteration while some instance is in the mixed stage, then FP64 only
+	// schedule: one launch per kernel, each instance at its stage's precision, while some instance is in the mixed
+	// stage; then the FP64 kernels only
 	const int prec0 = o.precision;
 	auto iteration = [&](int prec) -> int {
 		if (int r2 = batch_eval(b, true, prec, st))
@@ -2759,8 +2797,10 @@ int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opt
 	};
 	// kernel attributes are set before the capture
 	for (BatchGroup &g : b->groups)
-		for (int mx = 0; mx < 2; mx++) {
-			cudaError_t e = g.D == 1 ? (mx ? multi_attrs<1, true>() : multi_attrs<1, false>())
+		for (int mx = 0; mx < 3; mx++) {
+			cudaError_t e = mx == 2 ? (g.D == 1 ? multi_sched_attrs<1>() : g.D == 2 ? multi_sched_attrs<2>()
+			                                                                         : multi_sched_attrs<3>())
+			              : g.D == 1 ? (mx ? multi_attrs<1, true>() : multi_attrs<1, false>())
 			              : g.D == 2 ? (mx ? multi_attrs<2, true>() : multi_attrs<2, false>())
 			                         : (mx ? multi_attrs<3, true>() : multi_attrs<3, false>());
 			if (e != cudaSuccess)

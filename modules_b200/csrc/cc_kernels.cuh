@@ -499,6 +499,30 @@ __global__ void __launch_bounds__(kRhoThreads, 3) cc_mrho_kernel(const RhoArgs *
 	queue_leave(queue);
 }
 
+// The same with each instance's precision taken from its stage word (0: mixed, else FP64): one launch serves a
+// batched minimisation whose instances are in different stages of the precision schedule.
+template <int D, int L>
+__global__ void __launch_bounds__(kRhoThreads, 3) cc_mrho_sched_kernel(const RhoArgs *__restrict__ args,
+                                                                      const int *__restrict__ pre,
+                                                                      const int *__restrict__ nbgroups, int B,
+                                                                      unsigned *queue)
+{
+	__shared__ int sh_item;
+	const int total = __ldg(pre + B);
+	for (int item; (item = queue_next(queue, &sh_item)) < total;) {
+		const int b = find_instance(pre, B, item);
+		RhoArgs a = args[b];
+		const bool mixed = a.stage && *(volatile const int *)a.stage == 0;
+		a.stage = nullptr;   // the stage picks the precision; only the skip word can skip
+		const int local = item - __ldg(pre + b), ng = __ldg(nbgroups + b);
+		if (mixed)
+			rho_body<D, L, true, false>(a, local % ng, local / ng);
+		else
+			rho_body<D, L, false, false>(a, local % ng, local / ng);
+	}
+	queue_leave(queue);
+}
+
 // ---------------------------------------------------------------------------------------------------------------
 // split reduction, u = V conj(rho), energy
 // ---------------------------------------------------------------------------------------------------------------
@@ -618,6 +642,8 @@ static __global__ void __launch_bounds__(kRedThreads) cc_mreduce_kernel(const Re
 		const int b = find_instance(pre, B, item);
 		ReduceArgs a = args[b];
 		a.want_stage = want_stage;
+		if (want_stage < 0)   // a launch for every stage (the sched kernels)
+			a.stage = nullptr;
 		reduce_body(a, item - __ldg(pre + b), __ldg(nchunks + b));
 	}
 	queue_leave(queue);
@@ -862,6 +888,29 @@ __global__ void __launch_bounds__(kForceThreads, 3) cc_mforce_kernel(const Force
 		a.want_stage = want_stage;
 		const int local = item - __ldg(pre + b), pg = __ldg(pgroups + b);
 		force_body<D, L, MIXED>(a, local % pg, local / pg);
+	}
+	queue_leave(queue);
+}
+
+// The force pass with each instance's precision taken from its stage word (see cc_mrho_sched_kernel).
+template <int D, int L>
+__global__ void __launch_bounds__(kForceThreads, 3) cc_mforce_sched_kernel(const ForceArgs *__restrict__ args,
+                                                                          const int *__restrict__ pre,
+                                                                          const int *__restrict__ pgroups, int B,
+                                                                          unsigned *queue)
+{
+	__shared__ int sh_item;
+	const int total = __ldg(pre + B);
+	for (int item; (item = queue_next(queue, &sh_item)) < total;) {
+		const int b = find_instance(pre, B, item);
+		ForceArgs a = args[b];
+		const bool mixed = a.stage && *(volatile const int *)a.stage == 0;
+		a.stage = nullptr;
+		const int local = item - __ldg(pre + b), pg = __ldg(pgroups + b);
+		if (mixed)
+			force_body<D, L, true>(a, local % pg, local / pg);
+		else
+			force_body<D, L, false>(a, local % pg, local / pg);
 	}
 	queue_leave(queue);
 }
