@@ -214,7 +214,7 @@ struct cc_handle {
 	// non-uniform FFT path (cc_nufft.cuh), set up at its first use
 	bool nu_ready = false;
 	cc::NufftDev nu = {};
-	int64_t nu_ngrid = 0;
+	int64_t nu_ngrid = 0, nu_nspec = 0;
 	int nu_rho_blocks = 0;
 	int *d_nu_mode_u = nullptr;
 	std::vector<void *> nu_bufs;    // device buffers owned by the NUFFT set-up
@@ -1073,14 +1073,15 @@ int nufft_setup(cc_handle *h)
 	int32_t *d_um = nullptr;
 	double *d_uV = nullptr;
 	unsigned long long *gi = nullptr;
-	double *gr = nullptr, *epart = nullptr;
+	double *gr = nullptr, *epart = nullptr, *gim = nullptr;
 	double2 *spec = nullptr, *coef = nullptr, *rho_u = nullptr, *u_u = nullptr;
 	const int64_t nspec = ngrid / a.nf[d - 1] * (a.nf[d - 1] / 2 + 1);
 	const int nblk = std::max(1, (U + 255) / 256);
 	int rc;
 	if ((rc = nu_alloc(h, &d_um, (size_t)std::max(U, 1) * d)) || (rc = nu_alloc(h, &d_uV, (size_t)std::max(U, 1))) ||
 	    (rc = nu_alloc(h, &gi, (size_t)ngrid)) || (rc = nu_alloc(h, &gr, (size_t)ngrid)) ||
-	    (rc = nu_alloc(h, &spec, (size_t)nspec)) || (rc = nu_alloc(h, &coef, (size_t)ngrid * d)) ||
+	    (rc = nu_alloc(h, &spec, (size_t)nspec)) || (rc = nu_alloc(h, &coef, (size_t)nspec * d)) ||
+	    (rc = nu_alloc(h, &gim, (size_t)ngrid * d)) ||
 	    (rc = nu_alloc(h, &rho_u, (size_t)std::max(U, 1))) || (rc = nu_alloc(h, &u_u, (size_t)std::max(U, 1))) ||
 	    (rc = nu_alloc(h, &epart, (size_t)nblk)) || (rc = nu_alloc(h, &h->d_nu_mode_u, mode_u.size())))
 		return rc;
@@ -1096,6 +1097,7 @@ int nufft_setup(cc_handle *h)
 	a.gr = gr;
 	a.spec = spec;
 	a.coef = coef;
+	a.gim = gim;
 	a.rho_u = rho_u;
 	a.u_u = u_u;
 	a.epart = epart;
@@ -1103,11 +1105,12 @@ int nufft_setup(cc_handle *h)
 	if (cufftPlanMany(&h->nu_p1, d, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, 1) != CUFFT_SUCCESS)
 		return fail(CC_ERR_CUDA, "cufftPlanMany (D2Z) failed");
 	h->nu_p1_ok = true;
-	if (cufftPlanMany(&h->nu_p2, d, dims, nullptr, 1, (int)ngrid, nullptr, 1, (int)ngrid, CUFFT_Z2Z, d) !=
+	if (cufftPlanMany(&h->nu_p2, d, dims, nullptr, 1, (int)nspec, nullptr, 1, (int)ngrid, CUFFT_Z2D, d) !=
 	    CUFFT_SUCCESS)
-		return fail(CC_ERR_CUDA, "cufftPlanMany (Z2Z) failed");
+		return fail(CC_ERR_CUDA, "cufftPlanMany (Z2D) failed");
 	h->nu_p2_ok = true;
 	h->nu_ngrid = ngrid;
+	h->nu_nspec = nspec;
 	h->nu_rho_blocks = nblk;
 	h->nu_ready = true;
 	return CC_OK;
@@ -1143,13 +1146,13 @@ int run_nufft_t(cc_handle *h, int64_t N, const double *d_frac, double *d_E, doub
 	}
 	if (!(d_F || d_gfrac) || N == 0)
 		return CC_OK;
-	CC_CUDA(cudaMemsetAsync(a.coef, 0, sizeof(double2) * ngrid * D, st));
-	cc::nufft_coef_kernel<D><<<h->nu_rho_blocks, 256, 0, st>>>(a, ngrid);
+	CC_CUDA(cudaMemsetAsync(a.coef, 0, sizeof(double2) * h->nu_nspec * D, st));
+	cc::nufft_coef_kernel<D><<<h->nu_rho_blocks, 256, 0, st>>>(a, h->nu_nspec);
 	CC_CUDA(cudaGetLastError());
+	// complex-to-real (the input spectra are overwritten; they are rebuilt every evaluation)
 	if (cufftSetStream(h->nu_p2, st) != CUFFT_SUCCESS ||
-	    cufftExecZ2Z(h->nu_p2, reinterpret_cast<cufftDoubleComplex *>(a.coef),
-	                 reinterpret_cast<cufftDoubleComplex *>(a.coef), CUFFT_INVERSE) != CUFFT_SUCCESS)
-		return fail(CC_ERR_CUDA, "cufftExecZ2Z failed");
+	    cufftExecZ2D(h->nu_p2, reinterpret_cast<cufftDoubleComplex *>(a.coef), a.gim) != CUFFT_SUCCESS)
+		return fail(CC_ERR_CUDA, "cufftExecZ2D failed");
 	cc::NufftOut o;
 	for (int i = 0; i < 9; i++)
 		o.recip[i] = h->recip[i];
@@ -1270,10 +1273,11 @@ cudaEvent_t next_event(cc_handle *h)
 }
 
 // CC_PATH_AUTO: the NUFFT path when its estimated time, with a 20 % margin, is below the direct path's. Direct:
-// N x slots at 700 G pairs/s; NUFFT: 1.8e-11 s per particle and kernel point (spread + interpolation, W^d points),
-// 5e-11 s per fine-grid point and transform, 25 us of launches. Fits of B200 timings: 2D N=1e5 M=40002 0.29 ms NUFFT
-// against 5.1 ms direct; 2D N=2e4 M=8002 0.087 against 0.25; 3D N=2e4 M=27085 0.96 against 0.90; 3D N=1e5 M=135008
-// 4.9 against 20; 3D N=2000 M=2724 0.14 against 0.025.
+// N x slots at 700 G pairs/s; NUFFT: 3.9e-12 s per particle and kernel point (spread + interpolation, W^d points),
+// 7.2e-12 s per fine-grid point and transform, 80 us of launches and transforms at small sizes. Fitted to B200
+// timings of single evaluations (L2 flushed, FP64 energy + forces): 2D N=1e5 M=40002 0.165 ms NUFFT against 5.1 ms
+// direct; 2D N=2e4 M=8002 0.083 against 0.26; 3D N=2e4 M=12055 0.31 against 0.44; 3D N=1e5 M=60020 1.21 against
+// 9.3; 3D N=2000 M=2724 0.13 against 0.034.
 bool nufft_preferred(cc_handle *h, int64_t N)
 {
 	if (h->main.plan.nslot == 0 || N < 1024)
@@ -1296,7 +1300,7 @@ bool nufft_preferred(cc_handle *h, int64_t N)
 	if (grid > (double)((int64_t)1 << 28))
 		return false;
 	const double direct = (double)N * (double)h->main.plan.real_segs * h->main.plan.L / 7e11;
-	const double nufft = 1.8e-11 * (double)N * w + 5e-11 * grid * (1 + d) + 2.5e-5;
+	const double nufft = 3.9e-12 * (double)N * w + 7.2e-12 * grid * (1 + d) + 8e-5;
 	return 1.2 * nufft < direct;
 }
 

@@ -8,10 +8,12 @@
 // coordinates (phase exp(2 pi i n.s)) and x = n_f s:
 //   type 1:  f[g] = sum_j prod_e phi(g_e - x_je)   (spread),   F(n) = sum_g f[g] e^{2 pi i n.g / n_f}   (cuFFT),
 //            rho(n) = F(n) / prod_e phihat_e(n_e),   phihat(n) = int phi(t) cos(2 pi n t / n_f) dt;
-//   type 2:  C[n] = c_n / prod_e phihat_e(n_e),  G[g] = sum_n C[n] e^{2 pi i n.g / n_f}  (cuFFT),
+//   type 2:  C[n] = c_n / prod_e phihat_e(n_e),  G[g] = Im sum_n C[n] e^{2 pi i n.g / n_f}  (cuFFT),
 //            v(s_j) = sum_g prod_e phi(g_e - x_je) G[g]  (interpolation),
-// with c_n = u_n n_e for the force axis e (u = V conj(rho)) and g_e(j) = Im v(s_j), the integer-index gradient of the
-// direct force kernel. Errors are ~1e-13 of sum|c| (measured against direct sums of the same modes).
+// with c_n = u_n n_e for the force axis e (u = V conj(rho)) and g_e(j) = v(s_j), the integer-index gradient of the
+// direct force kernel. Im sum_n C[n] e^{i theta_n} = sum_n H[n] e^{i theta_n} with the Hermitian
+// H[n] = (A[n] + conj(A[-n])) / 2, A = -i C, so G is one complex-to-real transform of H's half spectrum.
+// Errors are ~1e-13 of sum|c| (measured against direct sums of the same modes).
 //
 // Determinism: the spread grid accumulates in 64-bit fixed point (scale 2^40) with integer atomics, whose sum does not
 // depend on their order; every other sum has a fixed order. Results repeat bitwise.
@@ -40,7 +42,8 @@ struct NufftDev {
 	unsigned long long *gi;   // spread grid (fixed point), nf0 * nf1 * nf2
 	double *gr;               // the same as doubles
 	const double2 *spec;      // D2Z output: nf0 x nf1 x (nf2/2 + 1) along the last used axis
-	double2 *coef;            // D type-2 grids, nf0 * nf1 * nf2 each
+	double2 *coef;            // D type-2 half spectra H (Z2D input), the D2Z layout each
+	double *gim;              // D type-2 real grids G (Z2D output), nf0 * nf1 * nf2 each
 	double2 *rho_u, *u_u;     // per unique mode
 	double *epart;            // per block of the rho kernel
 	const int *skip;
@@ -68,7 +71,11 @@ __device__ __forceinline__ int wrap_index(int g, int n)
 	return g < 0 ? g + n : g;
 }
 
-constexpr int kNufftLanes = 16;                    // lanes per particle (kNufftW of them active)
+// the next grid index along an axis of n points, wrapping at n (i in [0, n))
+__device__ __forceinline__ int wrap_next(int i, int n) { return i + 1 == n ? 0 : i + 1; }
+
+constexpr int kNufftLanes = 16;                    // lanes per particle (kNufftW of them active): lane t takes the
+                                                   // grid points of offset t along the last (contiguous) axis
 constexpr int kNufftPerBlock = kNufftThreads / kNufftLanes;   // particles per block (two per warp)
 
 // The kernel weights of particle j along every axis into shared memory (lane t < W computes entry t of each axis);
@@ -93,33 +100,38 @@ __device__ __forceinline__ bool nufft_weights(const NufftDev &a, const double *f
 	return valid;
 }
 
-// Type-1 spread: 16 lanes per particle; lane t0 adds the particle's weights of first-axis point g0 + t0 to the grid
-// in fixed point (integer atomics: the sum does not depend on their order).
+// Type-1 spread: 16 lanes per particle; lane t adds the particle's weights of last-axis point g_last + t, row by row
+// of the other axes (a particle's 14 lanes hit 14 consecutive grid words), in fixed point (integer atomics: the sum
+// does not depend on their order).
 template <int D> __global__ void __launch_bounds__(kNufftThreads) nufft_spread_kernel(NufftDev a, const double *frac, int N)
 {
 	__shared__ double sk[kNufftPerBlock][3][kNufftW];
 	__shared__ int sg0[kNufftPerBlock][3];
 	if (a.skip && *a.skip)
 		return;
-	const int p = threadIdx.x / kNufftLanes, t0 = threadIdx.x % kNufftLanes;
+	const int p = threadIdx.x / kNufftLanes, t = threadIdx.x % kNufftLanes;
 	const int j = blockIdx.x * kNufftPerBlock + p;
-	if (!nufft_weights<D>(a, frac, N, j, t0, sk[p], sg0[p]) || t0 >= kNufftW)
+	if (!nufft_weights<D>(a, frac, N, j, t, sk[p], sg0[p]) || t >= kNufftW)
 		return;
-	const int i0 = wrap_index(sg0[p][0] + t0, a.nf[0]);
-	const double w0 = sk[p][0][t0];
+	constexpr int L = D - 1;
+	const int il = wrap_index(sg0[p][L] + t, a.nf[L]);
+	const double wl = sk[p][L][t];
 	if constexpr (D == 1) {
-		atomicAdd(a.gi + i0, (unsigned long long)llrint(w0 * kNufftFix));
+		atomicAdd(a.gi + il, (unsigned long long)llrint(wl * kNufftFix));
 	} else {
-		for (int t1 = 0; t1 < kNufftW; t1++) {
-			const int i1 = wrap_index(sg0[p][1] + t1, a.nf[1]);
-			const double w01 = w0 * sk[p][1][t1];
+		int i0 = wrap_index(sg0[p][0], a.nf[0]);
+#pragma unroll 2
+		for (int t0 = 0; t0 < kNufftW; t0++, i0 = wrap_next(i0, a.nf[0])) {
+			const double w0 = sk[p][0][t0];
 			if constexpr (D == 2) {
-				atomicAdd(a.gi + (size_t)i0 * a.nf[1] + i1, (unsigned long long)llrint(w01 * kNufftFix));
+				atomicAdd(a.gi + (size_t)i0 * a.nf[1] + il, (unsigned long long)llrint(w0 * wl * kNufftFix));
 			} else {
-				const size_t base = ((size_t)i0 * a.nf[1] + i1) * a.nf[2];
-				for (int t2 = 0; t2 < kNufftW; t2++) {
-					const int i2 = wrap_index(sg0[p][2] + t2, a.nf[2]);
-					atomicAdd(a.gi + base + i2, (unsigned long long)llrint(w01 * sk[p][2][t2] * kNufftFix));
+				int i1 = wrap_index(sg0[p][1], a.nf[1]);
+#pragma unroll 7
+				for (int t1 = 0; t1 < kNufftW; t1++, i1 = wrap_next(i1, a.nf[1])) {
+					const double w01 = w0 * sk[p][1][t1];
+					atomicAdd(a.gi + ((size_t)i0 * a.nf[1] + i1) * a.nf[2] + il,
+					          (unsigned long long)llrint(w01 * wl * kNufftFix));
 				}
 			}
 		}
@@ -211,28 +223,49 @@ static __global__ void nufft_gather_rho_kernel(const double2 *rho_u, const int *
 		rho_mode[m] = rho_u[mode_u[m]];
 }
 
-// type-2 coefficients: C_e[n] = u_n n_e / phihat(n) on each axis' grid (the grids were zeroed)
-template <int D> __global__ void __launch_bounds__(256) nufft_coef_kernel(NufftDev a, int64_t ngrid)
+// type-2 coefficients: with C_e[n] = u_n n_e / phihat(n) and A = -i C_e, the half spectrum of each axis' Hermitian
+// H[m] = (A[m] + conj(A[-m])) / 2 (the spectra were zeroed). Mode n adds A/2 at +n and conj(A)/2 at -n where these lie
+// in the stored half (last index 0 .. nf/2). An entry m receives at most two terms (from the modes m and -m, the
+// modes being unique), and a sum of two terms onto zero does not depend on their order: the result repeats bitwise.
+template <int D> __global__ void __launch_bounds__(256) nufft_coef_kernel(NufftDev a, int64_t nspec)
 {
 	const int u = blockIdx.x * 256 + threadIdx.x;
 	if (a.skip && *a.skip)
 		return;
 	if (u >= a.U)
 		return;
+	constexpr int L = D - 1;
+	const int half = a.nf[L] / 2 + 1;
 	int n[3] = {0, 0, 0};
 	double ph = 1.0;
-	size_t idx = 0;
+	size_t ip = 0, im = 0;
+	bool hp = true, hm = true;
 #pragma unroll
 	for (int c = 0; c < D; c++) {
 		n[c] = a.umodes[(size_t)u * D + c];
 		ph *= phihat_of(a, c, n[c]);
-		idx = idx * a.nf[c] + wrap_index(n[c], a.nf[c]);
+		const int mp = wrap_index(n[c], a.nf[c]), mm = wrap_index(-n[c], a.nf[c]);
+		if (c == L) {
+			hp = mp < half;
+			hm = mm < half;
+		}
+		ip = ip * (c == L ? half : a.nf[c]) + mp;
+		im = im * (c == L ? half : a.nf[c]) + mm;
 	}
 	const double2 uu = a.u_u[u];
 #pragma unroll
 	for (int c = 0; c < D; c++) {
 		const double s = (double)n[c] / ph;
-		a.coef[(size_t)c * ngrid + idx] = make_double2(uu.x * s, uu.y * s);
+		const double cx = uu.x * s, cy = uu.y * s;   // C = cx + i cy, A = cy - i cx
+		double2 *H = a.coef + (size_t)c * nspec;
+		if (hp) {
+			atomicAdd(&H[ip].x, 0.5 * cy);
+			atomicAdd(&H[ip].y, -0.5 * cx);
+		}
+		if (hm) {
+			atomicAdd(&H[im].x, 0.5 * cy);
+			atomicAdd(&H[im].y, 0.5 * cx);
+		}
 	}
 }
 
@@ -243,8 +276,9 @@ struct NufftOut {
 	double *gfrac_out;        // N x D dPhi/ds, or nullptr
 };
 
-// type-2 interpolation: 16 lanes per particle; lane t0 sums the first-axis point g0 + t0, the lanes' sums are added
-// in a fixed butterfly; g_e = Im(sum_g phi G_e[g]) and the forces as the direct force kernel
+// type-2 interpolation: 16 lanes per particle; lane t sums the last-axis point g_last + t over the rows of the other
+// axes (a particle's 14 lanes read 14 consecutive grid words), the lanes' sums are added in a fixed butterfly;
+// g_e = sum_g phi G_e[g] and the forces as the direct force kernel
 template <int D>
 __global__ void __launch_bounds__(kNufftThreads) nufft_interp_kernel(NufftDev a, const double *frac, int N,
                                                                      int64_t ngrid, NufftOut o)
@@ -253,36 +287,57 @@ __global__ void __launch_bounds__(kNufftThreads) nufft_interp_kernel(NufftDev a,
 	__shared__ int sg0[kNufftPerBlock][3];
 	if (a.skip && *a.skip)
 		return;
-	const int p = threadIdx.x / kNufftLanes, t0 = threadIdx.x % kNufftLanes;
+	const int p = threadIdx.x / kNufftLanes, t = threadIdx.x % kNufftLanes;
 	const int j = blockIdx.x * kNufftPerBlock + p;
-	const bool valid = nufft_weights<D>(a, frac, N, j, t0, sk[p], sg0[p]);
+	const bool valid = nufft_weights<D>(a, frac, N, j, t, sk[p], sg0[p]);
 	double acc[D];
 #pragma unroll
 	for (int e = 0; e < D; e++)
 		acc[e] = 0.0;
-	if (valid && t0 < kNufftW) {
-		const int i0 = wrap_index(sg0[p][0] + t0, a.nf[0]);
-		const double w0 = sk[p][0][t0];
+	if (valid && t < kNufftW) {
+		constexpr int L = D - 1;
+		const int il = wrap_index(sg0[p][L] + t, a.nf[L]);
+		const double wl = sk[p][L][t];
 		if constexpr (D == 1) {
-			acc[0] = w0 * a.coef[i0].y;
+			acc[0] = wl * a.gim[il];
+		} else if constexpr (D == 2) {
+			// all rows' loads issued before the sums (the row indices wrap incrementally)
+			int i0 = wrap_index(sg0[p][0], a.nf[0]);
+			double v[kNufftW][D];
+#pragma unroll
+			for (int t0 = 0; t0 < kNufftW; t0++, i0 = wrap_next(i0, a.nf[0])) {
+				const size_t idx = (size_t)i0 * a.nf[1] + il;
+#pragma unroll
+				for (int e = 0; e < D; e++)
+					v[t0][e] = __ldg(a.gim + (size_t)e * ngrid + idx);
+			}
+#pragma unroll
+			for (int t0 = 0; t0 < kNufftW; t0++) {
+				const double w = sk[p][0][t0] * wl;
+#pragma unroll
+				for (int e = 0; e < D; e++)
+					acc[e] = fma(w, v[t0][e], acc[e]);
+			}
 		} else {
-			for (int t1 = 0; t1 < kNufftW; t1++) {
-				const int i1 = wrap_index(sg0[p][1] + t1, a.nf[1]);
-				const double w01 = w0 * sk[p][1][t1];
-				if constexpr (D == 2) {
-					const size_t idx = (size_t)i0 * a.nf[1] + i1;
+			int i0 = wrap_index(sg0[p][0], a.nf[0]);
+			const int i1s = wrap_index(sg0[p][1], a.nf[1]);
+			for (int t0 = 0; t0 < kNufftW; t0++, i0 = wrap_next(i0, a.nf[0])) {
+				const double w0 = sk[p][0][t0];
+				int i1 = i1s;
+				double v[kNufftW][D];
+#pragma unroll
+				for (int t1 = 0; t1 < kNufftW; t1++, i1 = wrap_next(i1, a.nf[1])) {
+					const size_t idx = ((size_t)i0 * a.nf[1] + i1) * a.nf[2] + il;
 #pragma unroll
 					for (int e = 0; e < D; e++)
-						acc[e] = fma(w01, a.coef[(size_t)e * ngrid + idx].y, acc[e]);
-				} else {
-					const size_t base = ((size_t)i0 * a.nf[1] + i1) * a.nf[2];
-					for (int t2 = 0; t2 < kNufftW; t2++) {
-						const size_t idx = base + wrap_index(sg0[p][2] + t2, a.nf[2]);
-						const double w = w01 * sk[p][2][t2];
+						v[t1][e] = __ldg(a.gim + (size_t)e * ngrid + idx);
+				}
 #pragma unroll
-						for (int e = 0; e < D; e++)
-							acc[e] = fma(w, a.coef[(size_t)e * ngrid + idx].y, acc[e]);
-					}
+				for (int t1 = 0; t1 < kNufftW; t1++) {
+					const double w = w0 * sk[p][1][t1] * wl;
+#pragma unroll
+					for (int e = 0; e < D; e++)
+						acc[e] = fma(w, v[t1][e], acc[e]);
 				}
 			}
 		}
@@ -292,7 +347,7 @@ __global__ void __launch_bounds__(kNufftThreads) nufft_interp_kernel(NufftDev a,
 #pragma unroll
 		for (int e = 0; e < D; e++)
 			acc[e] += __shfl_xor_sync(0xffffffffu, acc[e], off, kNufftLanes);
-	if (valid && t0 == 0)
+	if (valid && t == 0)
 		write_force_out<D>(o.F_out, o.gfrac_out, o.recip, o.fscale, j, acc);
 }
 
