@@ -167,24 +167,6 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def batched_workload(cc, count, seed=2024):
-    """512 independent stealthy configurations: d in {2,3}, N log-uniform in [200, 5000], chi U[0.10, 0.49],
-    v(k) = (1 - |k|/K)^2 (GeneratePotential Type 3), unit density, uniform random positions."""
-    rng = np.random.default_rng(seed)
-    pots, Ns, fracs, pairs = [], [], [], 0
-    for _ in range(count):
-        d = int(rng.choice([2, 3]))
-        n = int(round(np.exp(rng.uniform(np.log(200), np.log(5000)))))
-        chi = float(rng.uniform(0.10, 0.49))
-        basis = np.eye(d) * n ** (1.0 / d)
-        modes, V = cc.stealthy_kset(d, basis, n, chi, 3)
-        pots.append(cc.CCPotential(d, basis, modes, V))
-        Ns.append(n)
-        fracs.append(rng.random((n, d)))
-        pairs += n * len(V)
-    return pots, Ns, fracs, pairs
-
-
 def half_space_modes(d, nmax_f):
     """Integer modes n with |n| <= nmax_f and first nonzero component > 0 (the half space of the k-set rule)."""
     m = int(np.floor(nmax_f))
@@ -298,6 +280,7 @@ def run_single_legs(cc, torch):
 def run_extras(args, cc, torch):
     out = run_single_legs(cc, torch)
     # batched uneven instances: one batched energy+gradient step, CUDA-event timed, inputs resident
+    from modules_b200.workloads import batched_workload
     pots, Ns, fracs, pairs = batched_workload(cc, args.batch)
     batch = cc.CCBatch(pots, Ns)
     batch.set_positions(fracs)

@@ -1,8 +1,11 @@
 """Evaluate one synthetic stealthy configuration a few times (for profiling a single kernel launch sequence).
 
     python -m modules_b200.evalcase --d 2 --N 20000 --chi 0.2 --evals 3 [--mixed] [--path split|fused|nufft|auto]
+    python -m modules_b200.evalcase --batch 512 --evals 3 [--mixed]
 
 The configuration: N uniform random points (seed 1) in a periodic cube of unit density, the CLI's Type 0 k-set.
+With --batch: the seeded batch of uneven instances of the benchmark (modules_b200.workloads.batched_workload),
+evaluated as one batch (the multi-instance kernels) with the default tile shape.
 """
 import argparse
 
@@ -20,7 +23,17 @@ def main():
     ap.add_argument("--mixed", action="store_true")
     ap.add_argument("--fused", action="store_true", help="same as --path fused")
     ap.add_argument("--path", default="split", choices=["split", "fused", "nufft", "auto"])
+    ap.add_argument("--batch", type=int, default=0, help="evaluate the seeded batch of this many instances")
     a = ap.parse_args()
+    if a.batch > 0:
+        from .workloads import batched_workload
+        pots, Ns, fracs, pairs = batched_workload(cc, a.batch)
+        batch = cc.CCBatch(pots, Ns)
+        batch.set_positions(fracs)
+        for _ in range(a.evals):
+            E, _F = batch.energy_and_forces(precision=cc.PREC_MIXED if a.mixed else cc.PREC_FP64)
+        print(f"batch of {a.batch}: {pairs} particle-k pairs, sum E={float(np.sum(E)):.12e}")
+        return
     basis = np.eye(a.d) * a.N ** (1.0 / a.d)
     modes, V = cc.stealthy_kset(a.d, basis, a.N, a.chi)
     pot = cc.CCPotential(a.d, basis, modes, V)
