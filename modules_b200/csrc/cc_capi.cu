@@ -2213,6 +2213,12 @@ struct cc_batch {
 	std::vector<BatchBufs> bufs;
 	int per_split = 0, segs_per_split = 0;   // the tile shape in use
 	cudaStream_t stream = nullptr;
+	// L-BFGS state of cc_batch_minimize, kept between calls (grow-only): a minimisation makes no allocation call
+	// into the driver once the batch has run one
+	unsigned char *lb_base = nullptr;
+	size_t lb_cap = 0;
+	cc::LbInst *d_lb = nullptr;
+	int d_lb_cap = 0;
 };
 
 namespace {
@@ -2599,6 +2605,8 @@ int cc_batch_destroy(cc_batch *b)
 		cudaFree(g.d_queue);
 	}
 	cudaFree(b->arena.base);
+	cudaFree(b->lb_base);
+	cudaFree(b->d_lb);
 	if (b->stream)
 		cudaStreamDestroy(b->stream);
 	delete b;
@@ -2684,17 +2692,26 @@ int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opt
 		op[i] = ar.take(8 * (size_t)nblk * cc::lb_ndots(m));
 		ost[i] = ar.take(sizeof(cc::LbState));
 	}
-	cc::LbInst *d_lb = nullptr;
 	int rc;
-	if ((rc = dev_alloc(&ar.base, ar.used)) || (rc = dev_alloc(&d_lb, count))) {
-		cudaFree(ar.base);
-		return rc;
+	if (b->lb_cap < ar.used) {
+		cudaFree(b->lb_base);
+		b->lb_base = nullptr;
+		b->lb_cap = 0;
+		if ((rc = dev_alloc(&b->lb_base, ar.used)))
+			return rc;
+		b->lb_cap = ar.used;
 	}
-	auto cleanup = [&](int code) {
-		cudaFree(ar.base);
-		cudaFree(d_lb);
-		return code;
-	};
+	if (b->d_lb_cap < count) {
+		cudaFree(b->d_lb);
+		b->d_lb = nullptr;
+		b->d_lb_cap = 0;
+		if ((rc = dev_alloc(&b->d_lb, count)))
+			return rc;
+		b->d_lb_cap = count;
+	}
+	ar.base = b->lb_base;
+	cc::LbInst *d_lb = b->d_lb;
+	auto cleanup = [&](int code) { return code; };
 	std::vector<cc::LbInst> lbi(count);
 	cc::LbState s0;
 	std::memset(&s0, 0, sizeof(s0));

@@ -68,7 +68,7 @@ struct Slot {
 };
 
 // Plan and allocate a request; returns CC_OK and fills the slot.
-int open_slot(const cc_request &r, int idx, int m, int nblk_cap, cudaStream_t st, Slot &s)
+int open_slot(const cc_request &r, int idx, int m, int nblk_cap, cudaMemPool_t pool, cudaStream_t st, Slot &s)
 {
 	const int d = r.d;
 	const double side = std::pow((double)r.N, 1.0 / d);   // unit density
@@ -101,7 +101,7 @@ int open_slot(const cc_request &r, int idx, int m, int nblk_cap, cudaStream_t st
 	             o_S = c.take(8 * (size_t)n * m), o_Y = c.take(8 * (size_t)n * m),
 	             o_lp = c.take(8 * (size_t)nblk_cap * cc::lb_ndots(m)), o_st = c.take(sizeof(cc::LbState));
 	s.bytes = c.used;
-	SV_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&s.mem), c.used, st));
+	SV_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void **>(&s.mem), c.used, pool, st));
 	unsigned char *b = s.mem;
 	SV_CUDA(cudaMemcpyAsync(b + o_segs, p.segs.data(), sizeof(cc::Seg) * p.segs.size(), cudaMemcpyHostToDevice, st));
 	SV_CUDA(cudaMemcpyAsync(b + o_slotV, p.slotV.data(), sizeof(double) * p.nslot, cudaMemcpyHostToDevice, st));
@@ -253,6 +253,33 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 	const int nblk_cap = 32;
 	cudaStream_t st;
 	SV_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+	// The requests' memory comes from a pool of the server's own that keeps what it holds (release threshold: all)
+	// and holds the HBM budget from the start (as far as the device has it free): admitting and retiring requests then
+	// makes no allocation call into the driver, whose calls took up to ~1 s under contention on shared hosts.
+	int dev = 0;
+	SV_CUDA(cudaGetDevice(&dev));
+	cudaMemPoolProps pprops = {};
+	pprops.allocType = cudaMemAllocationTypePinned;
+	pprops.location.type = cudaMemLocationTypeDevice;
+	pprops.location.id = dev;
+	cudaMemPool_t pool = nullptr;
+	SV_CUDA(cudaMemPoolCreate(&pool, &pprops));
+	{
+		uint64_t keep = UINT64_MAX;
+		SV_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+		size_t free_b = 0, total_b = 0;
+		SV_CUDA(cudaMemGetInfo(&free_b, &total_b));
+		const size_t margin = (size_t)1 << 30;
+		const size_t reserve = std::min(o.hbm_budget, free_b > margin ? free_b - margin : 0);
+		if (reserve > 0) {
+			void *p = nullptr;
+			if (cudaMallocFromPoolAsync(&p, reserve, pool, st) == cudaSuccess)
+				cudaFreeAsync(p, st);
+			else
+				cudaGetLastError();   // no reservation: the pool grows on demand
+			SV_CUDA(cudaStreamSynchronize(st));
+		}
+	}
 	// device descriptor arrays sized for max_slots; one work queue (6 words) per dimension
 	cc::RhoArgs *d_ra = nullptr;
 	cc::ReduceArgs *d_rr = nullptr;
@@ -289,7 +316,7 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 			if (!active.empty() && used + need > o.hbm_budget)
 				break;
 			Slot s;
-			if ((rc = open_slot(r, order[next], m, nblk_cap, st, s)))
+			if ((rc = open_slot(r, order[next], m, nblk_cap, pool, st, s)))
 				break;
 			used += s.bytes;
 			out[order[next]].t_admit = now();
@@ -411,6 +438,7 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 	cudaFree(d_pre);
 	cudaFree(d_shape);
 	cudaFree(d_queue);
+	cudaMemPoolDestroy(pool);
 	cudaStreamDestroy(st);
 	return rc;
 }
