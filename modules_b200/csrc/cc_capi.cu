@@ -2040,7 +2040,7 @@ int cc_minimize(cc_handle *h, int64_t N, double *frac, const cc_lbfgs_opts *opts
 		return rc2;
 	}
 	const int d = h->d, n = (int)(N * d), m = o.history;
-	const int nblk = std::max(1, std::min(148, n / 2048));
+	const int nblk = cc::lb_blocks(n, 148);
 	LbBuffers b;
 	int rc;
 	if ((rc = dev_alloc(&b.x, n)) || (rc = dev_alloc(&b.g, n)) || (rc = dev_alloc(&b.d, n)) || (rc = dev_alloc(&b.xt, n)) ||
@@ -2675,7 +2675,7 @@ int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opt
 	int maxn = 0;
 	for (int i = 0; i < count; i++)
 		maxn = std::max(maxn, (int)(b->N[i] * b->h[i]->d));
-	const int nblk = std::max(1, std::min(32, maxn / 2048));
+	const int nblk = cc::lb_blocks(maxn, cc::kLbMaxBlocks);
 	// L-BFGS buffers of every instance in one allocation
 	Arena ar;
 	std::vector<size_t> ox(count), og(count), od(count), oxt(count), ogt(count), oS(count), oY(count), op(count),

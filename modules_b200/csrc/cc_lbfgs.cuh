@@ -64,11 +64,20 @@ struct LbInst {
 // products, so s'.y' and the history cross terms carry no cancellation.
 __host__ __device__ constexpr int lb_ndots(int m) { return 5 * m + 6; }
 
-static __global__ void __launch_bounds__(kLbThreads) lb_dots_kernel(const LbInst *insts, int nblk)
+// Blocks of the dot-product kernel for an instance of n variables: one variable per thread (kLbThreads per block),
+// at most `cap` blocks. A function of n and the cap only, so an instance's sums do not depend on the rest of a batch.
+__host__ __device__ constexpr int lb_blocks(int n, int cap)
+{
+	return n <= 0 ? 1 : ((n + kLbThreads - 1) / kLbThreads < cap ? (n + kLbThreads - 1) / kLbThreads : cap);
+}
+constexpr int kLbMaxBlocks = 64;   // cap of the batched minimisation and the server
+
+static __global__ void __launch_bounds__(kLbThreads) lb_dots_kernel(const LbInst *insts, int cap)
 {
 	const LbInst in = insts[blockIdx.y];
 	const LbState *st = in.st;
-	if (st->status != kLbRunning)
+	const int nblk = lb_blocks(in.n, cap);
+	if (st->status != kLbRunning || (int)blockIdx.x >= nblk)
 		return;
 	const int m = st->m, nd = lb_ndots(m);
 	const int per = (in.n + nblk - 1) / nblk;
@@ -146,12 +155,13 @@ constexpr int kLbSolveThreads = 256;
 // One block per instance: block totals of the dot products (parallel over the products, blocks summed in order),
 // accept / reject and the step length (thread 0), history matrices (parallel over slots), the triangular solves of
 // the compact form (warp 0, lanes split every inner sum), g.d of the new direction and the stop tests.
-static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const LbInst *insts, int nblk)
+static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const LbInst *insts, int cap)
 {
 	const LbInst in = insts[blockIdx.x];
 	LbState *st = in.st;
 	if (st->status != kLbRunning)
 		return;
+	const int nblk = lb_blocks(in.n, cap);
 	__shared__ double tot[5 * kLbMaxHist + 6];
 	__shared__ double Sg[kLbMaxHist], Yg[kLbMaxHist], t[kLbMaxHist], q[kLbMaxHist], w1[kLbMaxHist];
 	__shared__ int sh_accept, sh_newslot;

@@ -67,6 +67,23 @@ struct Slot {
 	cc::LbInst li;
 };
 
+// Particles per rho block of a served request: the largest power of two in [kServeMinPerSplit, kBatchPerSplit] whose
+// blocks hold at most kServeRhoPairs particle-slot pairs (particles x the widest block group's slots). Serving runs
+// light loads, where an iteration lasts about one block's time: smaller rho tiles cut it for the large requests.
+constexpr int kServeMinPerSplit = 16;
+constexpr int64_t kServeRhoPairs = 1 << 15;
+int serve_per_split(const cc::Plan &p)
+{
+	int max_wg = 1;
+	for (int g = 0; g < p.nbgroups(); g++)
+		max_wg = std::max(max_wg, p.bstart[g + 1] - p.bstart[g]);
+	const int64_t bslots = (int64_t)max_wg * 32 * p.L;
+	int per = cc::kBatchPerSplit;
+	while (per > kServeMinPerSplit && (int64_t)per * bslots > kServeRhoPairs)
+		per /= 2;
+	return per;
+}
+
 // Plan and allocate a request; returns CC_OK and fills the slot.
 int open_slot(const cc_request &r, int idx, int m, int nblk_cap, cudaMemPool_t pool, cudaStream_t st, Slot &s)
 {
@@ -86,7 +103,8 @@ int open_slot(const cc_request &r, int idx, int m, int nblk_cap, cudaMemPool_t p
 	cc::cell_geometry(d, basis, &vol, recip);
 	const int64_t N = r.N;
 	const int n = (int)(N * d);
-	const int nsplit = (int)((N + cc::kBatchPerSplit - 1) / cc::kBatchPerSplit);
+	const int per_split = serve_per_split(p);
+	const int nsplit = (int)((N + per_split - 1) / per_split);
 	const int nchunks = (p.nslot + 31) / 32, pgroups = (int)((N + 31) / 32);
 	const int nks = fs.count();
 	Carve c;
@@ -153,7 +171,7 @@ int open_slot(const cc_request &r, int idx, int m, int nblk_cap, cudaMemPool_t p
 	ra = cc::RhoArgs();
 	ra.frac = l.xt;
 	ra.N = (int)N;
-	ra.per_split = cc::kBatchPerSplit;
+	ra.per_split = per_split;
 	ra.chunk = cc::kBatchChunk;
 	ra.segs = reinterpret_cast<const cc::Seg *>(b + o_segs);
 	ra.bstart = reinterpret_cast<const int *>(b + o_bstart);
@@ -218,7 +236,7 @@ size_t estimate_bytes(const cc_request &r, int m, int nblk_cap)
 	const double M = std::ceil(r.chi * (double)r.N * r.d) * 1.1 + 64;
 	const double nseg = M / 4 + 64, nslot = nseg * 8;
 	const double n = (double)r.N * r.d;
-	const double nsplit = std::ceil(r.N / (double)cc::kBatchPerSplit), nks = std::ceil(nseg / cc::kBatchSegsPerSplit) + 2;
+	const double nsplit = std::ceil(r.N / (double)kServeMinPerSplit), nks = std::ceil(nseg / cc::kBatchSegsPerSplit) + 2;
 	const double bytes = 16 * nseg + 8 * nslot + 2 * 768 * (nseg / 256 + nks + 2) + 16 * nsplit * nslot + 32 * nslot +
 	                     8 * nks * n + 8 * n * (5 + 2 * m) + 8.0 * nblk_cap * cc::lb_ndots(m) + 16384;
 	return (size_t)bytes;
@@ -250,7 +268,7 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
 		return sfail(CC_ERR_NOGPU, "no CUDA device is visible");
 	const int m = o.history;
-	const int nblk_cap = 32;
+	const int nblk_cap = cc::kLbMaxBlocks;
 	cudaStream_t st;
 	SV_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
 	// The requests' memory comes from a pool of the server's own that keeps what it holds (release threshold: all)
@@ -384,7 +402,7 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 		SV_CUDA(cudaMemcpyAsync(d_pre, pre.data(), sizeof(int) * pre.size(), cudaMemcpyHostToDevice, st));
 		SV_CUDA(cudaMemcpyAsync(d_shape, shape.data(), sizeof(int) * shape.size(), cudaMemcpyHostToDevice, st));
 		// the descriptor vectors are pageable: the copies complete before the iterations read them
-		const int nblk = std::max(1, std::min(nblk_cap, maxn / 2048));
+		const int nblk = cc::lb_blocks(maxn, nblk_cap);
 		for (int it = 0; it < o.iters_per_round && rc == CC_OK; it++) {
 			for (const G &g : groups)
 				if ((rc = cc::launch_multi(g.D, false, d_ra + g.off, d_rr + g.off, d_fa + g.off, d_pre + g.pre_off,
