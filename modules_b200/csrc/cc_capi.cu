@@ -155,6 +155,28 @@ int upload_kset(DevKSet &k, const cc::Plan &plan)
 	return CC_OK;
 }
 
+// Device state of cc_minimize (L-BFGS of one configuration), kept by the handle between calls (grow-only).
+struct LbBuffers {
+	double *x = nullptr, *g = nullptr, *d = nullptr, *xt = nullptr, *gt = nullptr, *S = nullptr, *Y = nullptr;
+	double *part = nullptr;
+	cc::LbState *st = nullptr;
+	cc::LbInst *inst = nullptr;
+	void release()
+	{
+		cudaFree(x);
+		cudaFree(g);
+		cudaFree(d);
+		cudaFree(xt);
+		cudaFree(gt);
+		cudaFree(S);
+		cudaFree(Y);
+		cudaFree(part);
+		cudaFree(st);
+		cudaFree(inst);
+		*this = LbBuffers();
+	}
+};
+
 }  // namespace
 
 struct cc_handle {
@@ -228,6 +250,13 @@ struct cc_handle {
 	bool mc_valid = false, mc_pending = false;
 	const int *d_skip = nullptr;    // evaluations do nothing while *d_skip != 0 (set by cc_minimize)
 	bool timing = false;            // cc_set_timing
+	// cc_minimize's state, kept between calls so that a minimisation makes no allocation call into the driver once
+	// the handle has run one of its size: FP64 / mixed buffers (capacities n variables, m pairs, nblk dot blocks) and
+	// the batch of one that runs the precision schedule (for sched_N particles)
+	LbBuffers lb;
+	int lb_n = 0, lb_m = 0, lb_nblk = 0;
+	cc_batch *sched_batch = nullptr;
+	int64_t sched_N = -1;
 	std::vector<cudaEvent_t> ev;    // 3 events per timed evaluation
 	size_t ev_used = 0;
 };
@@ -1502,6 +1531,9 @@ int cc_destroy(cc_handle *h)
 		return CC_OK;
 	if (h->stream)
 		cudaStreamSynchronize(h->stream);
+	if (h->sched_batch)
+		cc_batch_destroy(h->sched_batch);
+	h->lb.release();
 	h->main.release();
 	h->sk.release();
 	cudaFree(h->d_frac);
@@ -1961,27 +1993,6 @@ int cc_lbfgs_defaults(cc_lbfgs_opts *o)
 
 namespace {
 
-struct LbBuffers {
-	double *x = nullptr, *g = nullptr, *d = nullptr, *xt = nullptr, *gt = nullptr, *S = nullptr, *Y = nullptr;
-	double *part = nullptr;
-	cc::LbState *st = nullptr;
-	cc::LbInst *inst = nullptr;
-	void release()
-	{
-		cudaFree(x);
-		cudaFree(g);
-		cudaFree(d);
-		cudaFree(xt);
-		cudaFree(gt);
-		cudaFree(S);
-		cudaFree(Y);
-		cudaFree(part);
-		cudaFree(st);
-		cudaFree(inst);
-		*this = LbBuffers();
-	}
-};
-
 // one iteration: evaluation at x_trial, dot products, solve, update
 int lb_iteration(cc_handle *h, int64_t N, LbBuffers &b, int n, int nblk, int prec, cudaStream_t st)
 {
@@ -2029,30 +2040,45 @@ int cc_minimize(cc_handle *h, int64_t N, double *frac, const cc_lbfgs_opts *opts
 	if ((int64_t)N * h->d > (1 << 30))
 		return fail(CC_ERR_ARG, "too many variables");
 	if (o.precision == CC_PREC_SCHEDULE && h->main.plan.nslot > 0) {
-		// the precision schedule is per instance: run it as a batch of one
-		cc_batch *bt = nullptr;
-		int rc2 = cc_batch_create(1, &h, &N, &bt);
-		if (rc2 == CC_OK)
-			rc2 = cc_batch_minimize(bt, &frac, &o, result);
-		cc_batch_destroy(bt);
+		// the precision schedule is per instance: run it as a batch of one (kept by the handle for this N)
+		int rc2 = CC_OK;
+		if (!h->sched_batch || h->sched_N != N) {
+			if (h->sched_batch)
+				cc_batch_destroy(h->sched_batch);
+			h->sched_batch = nullptr;
+			h->sched_N = -1;
+			if ((rc2 = cc_batch_create(1, &h, &N, &h->sched_batch)) != CC_OK)
+				return rc2;
+			h->sched_N = N;
+		}
+		rc2 = cc_batch_minimize(h->sched_batch, &frac, &o, result);
 		if (rc2 == CC_OK)
 			rc2 = cc_set_positions(h, N, frac);
 		return rc2;
 	}
 	const int d = h->d, n = (int)(N * d), m = o.history;
 	const int nblk = cc::lb_blocks(n, 148);
-	LbBuffers b;
+	LbBuffers &b = h->lb;
 	int rc;
-	if ((rc = dev_alloc(&b.x, n)) || (rc = dev_alloc(&b.g, n)) || (rc = dev_alloc(&b.d, n)) || (rc = dev_alloc(&b.xt, n)) ||
-	    (rc = dev_alloc(&b.gt, n)) || (rc = dev_alloc(&b.S, (size_t)m * n)) || (rc = dev_alloc(&b.Y, (size_t)m * n)) ||
-	    (rc = dev_alloc(&b.part, (size_t)nblk * cc::lb_ndots(m))) || (rc = dev_alloc(&b.st, 1)) ||
-	    (rc = dev_alloc(&b.inst, 1)) || (rc = ensure_particles(h, N))) {
+	if (h->lb_n < n || h->lb_m < m || h->lb_nblk < nblk) {
+		const int cn = std::max(n, h->lb_n), cm = std::max(m, h->lb_m), cb = std::max(nblk, h->lb_nblk);
 		b.release();
-		return rc;
+		h->lb_n = h->lb_m = h->lb_nblk = 0;
+		if ((rc = dev_alloc(&b.x, cn)) || (rc = dev_alloc(&b.g, cn)) || (rc = dev_alloc(&b.d, cn)) ||
+		    (rc = dev_alloc(&b.xt, cn)) || (rc = dev_alloc(&b.gt, cn)) || (rc = dev_alloc(&b.S, (size_t)cm * cn)) ||
+		    (rc = dev_alloc(&b.Y, (size_t)cm * cn)) || (rc = dev_alloc(&b.part, (size_t)cb * cc::lb_ndots(cm))) ||
+		    (rc = dev_alloc(&b.st, 1)) || (rc = dev_alloc(&b.inst, 1))) {
+			b.release();
+			return rc;
+		}
+		h->lb_n = cn;
+		h->lb_m = cm;
+		h->lb_nblk = cb;
 	}
+	if ((rc = ensure_particles(h, N)))
+		return rc;
 	auto cleanup = [&](int code) {
 		h->d_skip = nullptr;
-		b.release();
 		return code;
 	};
 	std::vector<double> x0((size_t)n);
@@ -2135,7 +2161,6 @@ int cc_minimize(cc_handle *h, int64_t N, double *frac, const cc_lbfgs_opts *opts
 		double v = x0[i] - std::floor(x0[i]);
 		frac[i] = v - std::floor(v);
 	}
-	b.release();
 	if ((rc = cc_set_positions(h, N, frac)))
 		return rc;
 	double E = 0.0;
