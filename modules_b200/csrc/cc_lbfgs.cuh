@@ -72,6 +72,11 @@ __host__ __device__ constexpr int lb_blocks(int n, int cap)
 }
 constexpr int kLbMaxBlocks = 64;   // cap of the batched minimisation and the server
 
+// Block partials of the dot products. The block's variables are taken in chunks of kLbThreads: the chunk's g_t,
+// y = g_t - g and s = x_t - x go to shared memory once; warp w then forms the five products of history pairs w, w + 8,
+// w + 16, ... over the chunk (every lane up to 8 variables, loads issued together), so the pairs' loads run in
+// parallel across warps instead of one pair after another. Sums have a fixed order (lanes by a fixed tree, chunks in
+// order, warps in order for the non-pair products), so a run repeats bitwise.
 static __global__ void __launch_bounds__(kLbThreads) lb_dots_kernel(const LbInst *insts, int cap)
 {
 	const LbInst in = insts[blockIdx.y];
@@ -79,21 +84,64 @@ static __global__ void __launch_bounds__(kLbThreads) lb_dots_kernel(const LbInst
 	const int nblk = lb_blocks(in.n, cap);
 	if (st->status != kLbRunning || (int)blockIdx.x >= nblk)
 		return;
+	constexpr int kWarps = kLbThreads / 32;
 	const int m = st->m, nd = lb_ndots(m);
 	const int per = (in.n + nblk - 1) / nblk;
 	const int j0 = blockIdx.x * per, j1 = min(in.n, j0 + per);
-	__shared__ double red[kLbThreads / 32][5 * kLbMaxHist + 6];
+	__shared__ double sgt[kLbThreads], syn[kLbThreads], ssn[kLbThreads];
+	__shared__ double pr[5 * kLbMaxHist];
+	__shared__ double red[kWarps][6];
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	const int count = st->count;
 	double a[6] = {0, 0, 0, 0, 0, 0};
-	for (int j = j0 + threadIdx.x; j < j1; j += kLbThreads) {
-		const double gt = in.gt[j], yj = gt - in.g[j], sj = in.xt[j] - in.x[j];
-		a[0] += gt * in.d[j];
-		a[1] += gt * gt;
-		a[2] += sj * yj;
-		a[3] += yj * yj;
-		a[4] += yj * gt;
-		a[5] = fmax(a[5], fabs(gt));
+	for (int k = threadIdx.x; k < 5 * count; k += kLbThreads)
+		pr[k] = 0.0;
+	for (int c0 = j0; c0 < j1; c0 += kLbThreads) {
+		const int cn = min(kLbThreads, j1 - c0);
+		__syncthreads();   // the previous chunk is no longer read
+		if (threadIdx.x < cn) {
+			const int j = c0 + threadIdx.x;
+			const double gt = in.gt[j], yj = gt - in.g[j], sj = in.xt[j] - in.x[j];
+			a[0] += gt * in.d[j];
+			a[1] += gt * gt;
+			a[2] += sj * yj;
+			a[3] += yj * yj;
+			a[4] += yj * gt;
+			a[5] = fmax(a[5], fabs(gt));
+			sgt[threadIdx.x] = gt;
+			syn[threadIdx.x] = yj;
+			ssn[threadIdx.x] = sj;
+		}
+		__syncthreads();
+		for (int i = warp; i < count; i += kWarps) {
+			const double *s = in.S + (size_t)i * in.n + c0, *y = in.Y + (size_t)i * in.n + c0;
+			double si[kLbThreads / 32], yi[kLbThreads / 32];
+#pragma unroll
+			for (int e = 0; e < kLbThreads / 32; e++) {
+				const int k = lane + 32 * e;
+				si[e] = k < cn ? s[k] : 0.0;
+				yi[e] = k < cn ? y[k] : 0.0;
+			}
+			double b[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+			for (int e = 0; e < kLbThreads / 32; e++) {
+				const int k = lane + 32 * e;
+				if (k < cn) {
+					b[0] += si[e] * sgt[k];
+					b[1] += yi[e] * sgt[k];
+					b[2] += si[e] * syn[k];
+					b[3] += yi[e] * syn[k];
+					b[4] += yi[e] * ssn[k];
+				}
+			}
+#pragma unroll
+			for (int k = 0; k < 5; k++)
+				for (int o = 16; o > 0; o >>= 1)
+					b[k] += __shfl_down_sync(0xffffffffu, b[k], o);
+			if (lane == 0)
+				for (int k = 0; k < 5; k++)
+					pr[5 * i + k] += b[k];
+		}
 	}
 #pragma unroll
 	for (int k = 0; k < 5; k++)
@@ -103,38 +151,18 @@ static __global__ void __launch_bounds__(kLbThreads) lb_dots_kernel(const LbInst
 		a[5] = fmax(a[5], __shfl_down_sync(0xffffffffu, a[5], o));
 	if (lane == 0)
 		for (int k = 0; k < 6; k++)
-			red[warp][5 * kLbMaxHist + k] = a[k];
-	for (int i = 0; i < count; i++) {
-		const double *s = in.S + (size_t)i * in.n, *y = in.Y + (size_t)i * in.n;
-		double b[5] = {0, 0, 0, 0, 0};
-		for (int j = j0 + threadIdx.x; j < j1; j += kLbThreads) {
-			const double gt = in.gt[j], yn = gt - in.g[j], sn = in.xt[j] - in.x[j];
-			const double si = s[j], yi = y[j];
-			b[0] += si * gt;
-			b[1] += yi * gt;
-			b[2] += si * yn;
-			b[3] += yi * yn;
-			b[4] += yi * sn;
-		}
-#pragma unroll
-		for (int k = 0; k < 5; k++)
-			for (int o = 16; o > 0; o >>= 1)
-				b[k] += __shfl_down_sync(0xffffffffu, b[k], o);
-		if (lane == 0)
-			for (int k = 0; k < 5; k++)
-				red[warp][5 * i + k] = b[k];
-	}
+			red[warp][k] = a[k];
 	__syncthreads();
 	double *out = in.part + (size_t)blockIdx.x * nd;
 	for (int k = threadIdx.x; k < nd; k += kLbThreads) {
-		const int src = k < 5 * m ? k : 5 * kLbMaxHist + (k - 5 * m);
-		if (k < 5 * m && k / 5 >= count) {
-			out[k] = 0.0;
+		if (k < 5 * m) {
+			out[k] = k / 5 < count ? pr[k] : 0.0;
 			continue;
 		}
-		double t = red[0][src];
-		for (int w = 1; w < kLbThreads / 32; w++)
-			t = (k == nd - 1) ? fmax(t, red[w][src]) : t + red[w][src];
+		const int q = k - 5 * m;
+		double t = red[0][q];
+		for (int w = 1; w < kWarps; w++)
+			t = (q == 5) ? fmax(t, red[w][q]) : t + red[w][q];
 		out[k] = t;
 	}
 }
