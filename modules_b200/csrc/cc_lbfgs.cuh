@@ -192,6 +192,7 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 	const int nblk = lb_blocks(in.n, cap);
 	__shared__ double tot[5 * kLbMaxHist + 6];
 	__shared__ double Sg[kLbMaxHist], Yg[kLbMaxHist], t[kLbMaxHist], q[kLbMaxHist], w1[kLbMaxHist];
+	__shared__ double sR[kLbMaxHist * kLbMaxHist];
 	__shared__ int sh_accept, sh_newslot;
 	const int m = st->m, nd = lb_ndots(m);
 	for (int k = threadIdx.x; k < nd; k += kLbSolveThreads) {
@@ -306,40 +307,55 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 		st->Sg[i] = Sg[i];
 		st->Yg[i] = Yg[i];
 	}
-	// compact-form solves on warp 0 (chronological index a <-> ring slot (head + a) % m)
-	if (threadIdx.x < 32) {
-		const int lane = threadIdx.x;
-		// t = R^-1 S^T g, R[a][b] = s_a . y_b (a <= b): backward substitution
-		for (int a = k - 1; a >= 0; a--) {
-			const int ia = (head + a) % m;
-			double v = 0.0;
-			for (int b = a + 1 + lane; b < k; b += 32)
-				v += st->SY[ia * m + (head + b) % m] * t[b];
-			v = lb_warp_sum(v);
+	// compact-form solves (chronological index a <-> ring slot (head + a) % m). R[a][b] = s_a . y_b (a <= b) goes to
+	// shared memory; the triangular solves run column by column on warp 0 (lane l owns rows l and l + 32: one
+	// broadcast and two multiply-adds per column), the product with Y^T Y on all warps.
+	for (int e = threadIdx.x; e < k * k; e += kLbSolveThreads) {
+		const int a = e / k, b = e - a * k;
+		sR[e] = st->SY[((head + a) % m) * m + (head + b) % m];
+	}
+	__syncthreads();
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	if (warp == 0) {
+		// t = R^-1 S^T g: backward substitution
+		double r0 = lane < k ? Sg[(head + lane) % m] : 0.0, r1 = lane + 32 < k ? Sg[(head + lane + 32) % m] : 0.0;
+		for (int b = k - 1; b >= 0; b--) {
+			const double own = (b < 32 ? r0 : r1) / sR[b * k + b];
+			const double tb = __shfl_sync(0xffffffffu, own, b & 31);
 			if (lane == 0)
-				t[a] = (Sg[ia] - v) / st->SY[ia * m + ia];
-			__syncwarp();
+				t[b] = tb;
+			if (lane < b)
+				r0 -= sR[lane * k + b] * tb;
+			if (lane + 32 < b)
+				r1 -= sR[(lane + 32) * k + b] * tb;
 		}
-		// q = D t + gamma Y^T Y t - gamma Y^T g
-		for (int a = lane; a < k; a += 32) {
-			const int ia = (head + a) % m;
-			double v = 0.0;
-			for (int b = 0; b < k; b++)
-				v += st->YY[ia * m + (head + b) % m] * t[b];
-			q[a] = st->SY[ia * m + ia] * t[a] + gam * v - gam * Yg[ia];
+	}
+	__syncthreads();
+	// q = D t + gamma Y^T Y t - gamma Y^T g: row a on warp a mod 8, lanes over b, sums by a fixed tree
+	for (int a = warp; a < k; a += kLbSolveThreads / 32) {
+		const int ia = (head + a) % m;
+		double v = 0.0;
+		for (int b = lane; b < k; b += 32)
+			v += st->YY[ia * m + (head + b) % m] * t[b];
+		v = lb_warp_sum(v);
+		if (lane == 0)
+			q[a] = sR[a * k + a] * t[a] + gam * v - gam * Yg[ia];
+	}
+	__syncthreads();
+	if (warp == 0) {
+		// w1 = R^-T q: forward substitution
+		double r0 = lane < k ? q[lane] : 0.0, r1 = lane + 32 < k ? q[lane + 32] : 0.0;
+		for (int b = 0; b < k; b++) {
+			const double own = (b < 32 ? r0 : r1) / sR[b * k + b];
+			const double wb = __shfl_sync(0xffffffffu, own, b & 31);
+			if (lane == 0)
+				w1[b] = wb;
+			if (lane > b && lane < k)
+				r0 -= sR[b * k + lane] * wb;
+			if (lane + 32 > b && lane + 32 < k)
+				r1 -= sR[b * k + lane + 32] * wb;
 		}
 		__syncwarp();
-		// w1 = R^-T q: forward substitution
-		for (int a = 0; a < k; a++) {
-			const int ia = (head + a) % m;
-			double v = 0.0;
-			for (int b = lane; b < a; b += 32)
-				v += st->SY[((head + b) % m) * m + ia] * w1[b];
-			v = lb_warp_sum(v);
-			if (lane == 0)
-				w1[a] = (q[a] - v) / st->SY[ia * m + ia];
-			__syncwarp();
-		}
 		// store per ring slot: w[slot] = w1, w[kLbMaxHist + slot] = -gamma t; g.d of d = -(gamma g + S w1 + gamma Y w2)
 		double gdn = 0.0;
 		for (int a = lane; a < k; a += 32) {
