@@ -167,8 +167,6 @@ static __global__ void __launch_bounds__(kLbThreads) lb_dots_kernel(const LbInst
 	}
 }
 
-// ring slot of the c-th oldest pair
-__device__ __forceinline__ int lb_slot(const LbState *st, int c) { return (st->head + c) % st->m; }
 
 // warp-wide sum with a fixed tree (every lane gets the total)
 __device__ __forceinline__ double lb_warp_sum(double v)
@@ -419,14 +417,31 @@ static __global__ void __launch_bounds__(kLbThreads) lb_update_kernel(const LbIn
 		in.g[j] = gt;
 		if (st->status != kLbRunning)
 			return;
+		// the pairs' loads are issued four at a time; the sum runs over the pairs in order
+		const int count = st->count, head = st->head;
+		const double *__restrict__ S = in.S + j, *__restrict__ Y = in.Y + j, *__restrict__ w = st->w;
+		const size_t n = (size_t)in.n;
 		double v = st->gamma * gt;
-		for (int c = 0; c < st->count; c++) {
-			const int i = lb_slot(st, c);
-			v += st->w[i] * in.S[(size_t)i * in.n + j] + st->w[kLbMaxHist + i] * in.Y[(size_t)i * in.n + j];
+		int c = 0;
+		for (; c + 4 <= count; c += 4) {
+			int i[4];
+			double sv[4], yv[4];
+#pragma unroll
+			for (int u = 0; u < 4; u++) {
+				i[u] = (head + c + u) % m;
+				sv[u] = S[i[u] * n];
+				yv[u] = Y[i[u] * n];
+			}
+#pragma unroll
+			for (int u = 0; u < 4; u++)
+				v += w[i[u]] * sv[u] + w[kLbMaxHist + i[u]] * yv[u];
+		}
+		for (; c < count; c++) {
+			const int i = (head + c) % m;
+			v += w[i] * S[i * n] + w[kLbMaxHist + i] * Y[i * n];
 		}
 		in.d[j] = -v;
 	}
-	(void)m;
 	in.xt[j] = in.x[j] + st->alpha * in.d[j];
 }
 
