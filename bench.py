@@ -338,16 +338,10 @@ def run_extras(args, cc, torch):
         "max_E_per_particle_batched": float(epp.max()), "max_E_per_particle_plain": float(max(plain_E))}
     del gb
     # served stream (a bounded sample of the 10000-request workload)
-    rng = np.random.default_rng(99)
-    reqs, t = [], 0.0
+    from modules_b200.workloads import served_stream
     rate = args.served_rate
     nmax, chimax = (20000, 0.49) if args.served_full else (4000, 0.40)
-    for _ in range(args.served):
-        t += rng.exponential(1.0 / rate)
-        d = int(rng.choice([2, 3]))
-        n = int(np.clip(np.exp(rng.normal(np.log(1000), 0.6)), 100, nmax))
-        chi = float(rng.uniform(0.05, chimax))
-        reqs.append(dict(d=d, N=n, chi=chi, vtype=int(rng.choice([0, 3])), frac0=rng.random((n, d)), arrival_s=t))
+    reqs = served_stream(args.served, rate, nmax, chimax)
     res, wall = cc.serve(reqs, iters_per_round=16)
     lat = np.array([r["t_done"] - q["arrival_s"] for r, q in zip(res, reqs)])
     ok = np.array([r["E"] / q["N"] < 1e-20 for r, q in zip(res, reqs)])

@@ -2,10 +2,13 @@
 
     python -m modules_b200.evalcase --d 2 --N 20000 --chi 0.2 --evals 3 [--mixed] [--path split|fused|nufft|auto]
     python -m modules_b200.evalcase --batch 512 --evals 3 [--mixed]
+    python -m modules_b200.evalcase --serve 120
 
 The configuration: N uniform random points (seed 1) in a periodic cube of unit density, the CLI's Type 0 k-set.
 With --batch: the seeded batch of uneven instances of the benchmark (modules_b200.workloads.batched_workload),
 evaluated as one batch (the multi-instance kernels) with the default tile shape.
+With --serve: the seeded served stream of the benchmark (modules_b200.workloads.served_stream: arrivals at 60/s,
+N <= 4000, chi <= 0.40) through modules_b200.serve with 16 iterations per round.
 """
 import argparse
 
@@ -24,7 +27,15 @@ def main():
     ap.add_argument("--fused", action="store_true", help="same as --path fused")
     ap.add_argument("--path", default="split", choices=["split", "fused", "nufft", "auto"])
     ap.add_argument("--batch", type=int, default=0, help="evaluate the seeded batch of this many instances")
+    ap.add_argument("--serve", type=int, default=0, help="serve the seeded stream of this many requests")
     a = ap.parse_args()
+    if a.serve > 0:
+        from .workloads import served_stream
+        reqs = served_stream(a.serve)
+        res, wall = cc.serve(reqs, iters_per_round=16)
+        reached = sum(r["E"] / q["N"] < 1e-20 for r, q in zip(res, reqs))
+        print(f"served {a.serve} requests in {wall:.2f} s, {reached} reached E/N < 1e-20")
+        return
     if a.batch > 0:
         from .workloads import batched_workload
         pots, Ns, fracs, pairs = batched_workload(cc, a.batch)

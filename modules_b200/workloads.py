@@ -19,3 +19,18 @@ def batched_workload(cc, count, seed=2024):
         fracs.append(rng.random((n, d)))
         pairs += n * len(V)
     return pots, Ns, fracs, pairs
+
+
+def served_stream(count, rate=60.0, nmax=4000, chimax=0.40, seed=99):
+    """`count` ground-state requests with Poisson arrivals at `rate` per second: d in {2,3}, N log-normal (median
+    1000, sigma 0.6) clipped to [100, nmax], chi U[0.05, chimax], v(k) = 1 or (1 - |k|/K)^2, uniform random start.
+    Returns a list of request dicts for modules_b200.serve."""
+    rng = np.random.default_rng(seed)
+    reqs, t = [], 0.0
+    for _ in range(count):
+        t += rng.exponential(1.0 / rate)
+        d = int(rng.choice([2, 3]))
+        n = int(np.clip(np.exp(rng.normal(np.log(1000), 0.6)), 100, nmax))
+        chi = float(rng.uniform(0.05, chimax))
+        reqs.append(dict(d=d, N=n, chi=chi, vtype=int(rng.choice([0, 3])), frac0=rng.random((n, d)), arrival_s=t))
+    return reqs
