@@ -71,7 +71,7 @@ struct Slot {
 // blocks hold at most kServeRhoPairs particle-slot pairs (particles x the widest block group's slots). Serving runs
 // light loads, where an iteration lasts about one block's time: smaller rho tiles cut it for the large requests.
 constexpr int kServeMinPerSplit = 16;
-constexpr int64_t kServeRhoPairs = 1 << 15;
+constexpr int64_t kServeRhoPairs = 1 << 14;
 int serve_per_split(const cc::Plan &p)
 {
 	int max_wg = 1;
