@@ -698,6 +698,7 @@ __device__ __forceinline__ void write_force(const ForceArgs &a, int j, const dou
 }
 
 constexpr int kForceUChunk = 128;   // segments whose slot weights are staged in shared memory at once
+constexpr int kForceRun = 4;        // FP64 force pass: segments of a lattice line on one recurrence before a new seed
 
 // Dynamic shared memory of the force kernel for tables of `row` entries: the staged weights, then the tables; the
 // per-warp sums reuse it after the loop.
@@ -769,6 +770,65 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 		for (int e = threadIdx.x; e < nq; e += kForceThreads)
 			sh_seg[e] = a.segs[c0 + e];
 		__syncthreads();
+		if constexpr (!MIXED) {
+			// FP64: warp w takes a contiguous run of the chunk's segments; a segment that continues the previous one
+			// on its lattice line (same line, start + L, previous one full) continues the three-term recurrence
+			// instead of being seeded from the tables, for up to kForceRun segments in a row
+			const int per = (nq + kForceWarps - 1) / kForceWarps;
+			const int qa = min(nq, warp * per), qb = min(nq, qa + per);
+			double2 p = make_double2(0.0, 0.0), q = make_double2(0.0, 0.0);
+			double c = 0.0;
+			int run = 0;
+			Seg prev = {0, 0, 0, 0};
+			for (int qq = qa; qq < qb; qq++) {
+				const Seg sgm = sh_seg[qq];
+				if (sgm.len == 0) {   // padding segment of a rho group: weight 0, no table entries
+					run = 0;
+					continue;
+				}
+				const double2 *uu = sh_u + qq;
+				double2 z0, z1;
+				if (run > 0 && run < kForceRun && prev.len == L && sgm.p0 == prev.p0 && sgm.p1 == prev.p1 &&
+				    sgm.start == prev.start + L) {
+					z0 = cheb_next(c, q, p);
+					z1 = cheb_next(c, z0, q);
+					run++;
+				} else {
+					const SeedIdx ix = seed_index<D>(sp, sgm);
+					z0 = seed_from<D, double2>(tab + lane, 32, ix);
+					const double2 w = tab[ix.w * 32 + lane];
+					c = 2.0 * w.x;
+					z1 = cmul(z0, w);
+					run = 1;
+				}
+				const double2 u0 = uu[0], u1 = uu[kForceUChunk];
+				double S0 = u0.x * z0.y + u0.y * z0.x, S1;
+				{
+					const double t = u1.x * z1.y + u1.y * z1.x;
+					S0 += t;
+					S1 = t;
+				}
+				p = z0;
+				q = z1;
+#pragma unroll
+				for (int r = 2; r < L; r++) {
+					const double2 n = cheb_next(c, q, p);
+					const double2 u = uu[r * kForceUChunk];
+					const double t = u.x * n.y + u.y * n.x;
+					S0 += t;
+					S1 = fma((double)r, t, S1);
+					p = q;
+					q = n;
+				}
+				if (D >= 2)
+					g[0] = fma(S0, (double)sgm.p0, g[0]);
+				if (D >= 3)
+					g[1] = fma(S0, (double)sgm.p1, g[1]);
+				g[D - 1] = fma(S0, (double)sgm.start, g[D - 1] + S1);
+				prev = sgm;
+			}
+			continue;
+		}
 		for (int qq = warp; qq < nq; qq += kForceWarps) {
 			const Seg sgm = sh_seg[qq];
 			if (sgm.len == 0)   // padding segment of a rho group: weight 0, no table entries
