@@ -225,6 +225,10 @@ def run_single_legs(cc, torch):
     modes, V = cc.stealthy_kset(d, basis, n, chi)
     pot = cc.CCPotential(d, basis, modes, V)
     f0 = np.random.default_rng(7).random((n, d))
+    # one untimed minimisation per precision from another start: the handle's first call allocates its L-BFGS state
+    fw = np.random.default_rng(8).random((n, d))
+    pot.minimize(fw, stopval=1e-20 * n, max_evals=50)
+    pot.minimize(fw, stopval=1e-20 * n, max_evals=50, precision=cc.PREC_SCHEDULE, switch_energy_per_particle=1e-10)
     t0 = time.perf_counter()
     x, E, ev, _it, _st = pot.minimize(f0, stopval=1e-20 * n)
     t_fp64 = time.perf_counter() - t0
@@ -243,7 +247,8 @@ def run_single_legs(cc, torch):
         S = pot.structure_factor(kq)
     t_sk = (time.perf_counter() - t0) / reps
     out["minimise_3d_n2000"] = {
-        "workload": "3D N=2000 chi=0.45 M=2724 v=1 from a seeded uniform start, to Phi/N < 1e-20",
+        "workload": "3D N=2000 chi=0.45 M=2724 v=1 from a seeded uniform start, to Phi/N < 1e-20 (after an untimed "
+                    "50-evaluation minimisation on the same handle)",
         "fp64_s": t_fp64, "fp64_evals": int(ev), "fp64_E_per_particle": E / n,
         "schedule_s": t_sched, "schedule_evals": int(ev2), "schedule_E_per_particle": E2 / n,
         "sk_modes": int(len(kq)), "sk_ms_per_call": t_sk * 1e3, "max_S_constrained": float(S[inside].max()),
