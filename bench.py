@@ -37,7 +37,7 @@ METRIC = "CC energy+grad evals/s"
 UNIT = "evals/s"
 # DRAM bytes (read + write) per launch of the kernels on this workload, from one ncu capture
 # (profiles/cc_kernels_3d_n2000_ncu.md: dram__bytes_read.sum + dram__bytes_write.sum)
-NCU_TRAFFIC_BYTES = {"cc_force_kernel": 0.143e6, "cc_rho_kernel": 0.078e6, "cc_reduce_kernel": 1.418e6}
+NCU_TRAFFIC_BYTES = {"cc_force_kernel": 0.144e6, "cc_rho_kernel": 0.078e6, "cc_reduce_kernel": 1.418e6}
 WORKLOAD = "3D stealthy CC ground-state evaluation: N=2000 uniform in a periodic cube (unit density), chi=0.45, " \
            "M=2724 half-space k (v=1), FP64 energy + Cartesian forces"
 
