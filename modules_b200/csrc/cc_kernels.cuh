@@ -827,53 +827,53 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 				g[D - 1] = fma(S0, (double)sgm.start, g[D - 1] + S1);
 				prev = sgm;
 			}
-			continue;
-		}
-		for (int qq = warp; qq < nq; qq += kForceWarps) {
-			const Seg sgm = sh_seg[qq];
-			if (sgm.len == 0)   // padding segment of a rho group: weight 0, no table entries
-				continue;
-			const C *uu = sh_u + qq;
-			const SeedIdx ix = seed_index<D>(sp, sgm);
-			C z = seed_from<D, C>(tab + lane, 32, ix);
-			const C w = tab[ix.w * 32 + lane];
-			R S0 = 0, S1 = 0;
-			if constexpr (MIXED) {
-#pragma unroll
-				for (int r = 0; r < L; r++) {
-					const C u = uu[r * kForceUChunk];
-					const R t = u.x * z.y + u.y * z.x;
-					S0 += t;
-					S1 = fma((R)r, t, S1);
-					z = cmul(z, w);
+		} else {
+			for (int qq = warp; qq < nq; qq += kForceWarps) {
+				const Seg sgm = sh_seg[qq];
+				if (sgm.len == 0)   // padding segment of a rho group: weight 0, no table entries
+					continue;
+				const C *uu = sh_u + qq;
+				const SeedIdx ix = seed_index<D>(sp, sgm);
+				C z = seed_from<D, C>(tab + lane, 32, ix);
+				const C w = tab[ix.w * 32 + lane];
+				R S0 = 0, S1 = 0;
+				if constexpr (MIXED) {
+	#pragma unroll
+					for (int r = 0; r < L; r++) {
+						const C u = uu[r * kForceUChunk];
+						const R t = u.x * z.y + u.y * z.x;
+						S0 += t;
+						S1 = fma((R)r, t, S1);
+						z = cmul(z, w);
+					}
+				} else {
+					const double c = 2.0 * w.x;
+					double2 p = z, q = cmul(z, w);
+					const double2 u0 = uu[0], u1 = uu[kForceUChunk];
+					S0 = u0.x * p.y + u0.y * p.x;
+					{
+						const double t = u1.x * q.y + u1.y * q.x;
+						S0 += t;
+						S1 = t;
+					}
+	#pragma unroll
+					for (int r = 2; r < L; r++) {
+						const double2 n = cheb_next(c, q, p);
+						const double2 u = uu[r * kForceUChunk];
+						const double t = u.x * n.y + u.y * n.x;
+						S0 += t;
+						S1 = fma((double)r, t, S1);
+						p = q;
+						q = n;
+					}
 				}
-			} else {
-				const double c = 2.0 * w.x;
-				double2 p = z, q = cmul(z, w);
-				const double2 u0 = uu[0], u1 = uu[kForceUChunk];
-				S0 = u0.x * p.y + u0.y * p.x;
-				{
-					const double t = u1.x * q.y + u1.y * q.x;
-					S0 += t;
-					S1 = t;
-				}
-#pragma unroll
-				for (int r = 2; r < L; r++) {
-					const double2 n = cheb_next(c, q, p);
-					const double2 u = uu[r * kForceUChunk];
-					const double t = u.x * n.y + u.y * n.x;
-					S0 += t;
-					S1 = fma((double)r, t, S1);
-					p = q;
-					q = n;
-				}
+				const double S0d = (double)S0;
+				if (D >= 2)
+					g[0] = fma(S0d, (double)sgm.p0, g[0]);
+				if (D >= 3)
+					g[1] = fma(S0d, (double)sgm.p1, g[1]);
+				g[D - 1] = fma(S0d, (double)sgm.start, g[D - 1] + (double)S1);
 			}
-			const double S0d = (double)S0;
-			if (D >= 2)
-				g[0] = fma(S0d, (double)sgm.p0, g[0]);
-			if (D >= 3)
-				g[1] = fma(S0d, (double)sgm.p1, g[1]);
-			g[D - 1] = fma(S0d, (double)sgm.start, g[D - 1] + (double)S1);
 		}
 	}
 
