@@ -2224,8 +2224,8 @@ struct BatchBufs {
 };
 
 // tile shapes the autotuner times: particles per rho block, segments per force block
-constexpr int kTuneSplits[] = {32, 64, 128, 256, 512};
-constexpr int kTuneSegs[] = {32, 64, 128, 256};
+constexpr int kTuneSplits[] = {32, 64, 128, 256, 512, 1024};
+constexpr int kTuneSegs[] = {32, 64, 128, 256, 512, 1024};
 
 }  // namespace
 
