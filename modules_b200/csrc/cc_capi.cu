@@ -1613,13 +1613,15 @@ int cc_set_positions(cc_handle *h, int64_t N, const double *frac)
 	if (int rc = input_staging(h, (size_t)N * d))
 		return rc;
 	double *in = h->h_in;
-	// positions already in [0,1) (the usual case) are copied as they are; NaN fails both comparisons
+	// positions already in [0,1) (the usual case) are copied as they are, in the same pass that checks them; NaN
+	// fails both comparisons
 	bool unit = true;
-	for (int64_t i = 0; i < N * d; i++)
-		unit &= (frac[i] >= 0.0) & (frac[i] < 1.0);
-	if (unit) {
-		std::memcpy(in, frac, sizeof(double) * N * d);
-	} else {
+	for (int64_t i = 0; i < N * d; i++) {
+		const double x = frac[i];
+		in[i] = x;
+		unit &= (x >= 0.0) & (x < 1.0);
+	}
+	if (!unit) {
 		for (int64_t i = 0; i < N * d; i++)
 			if (!wrap_unit(frac[i], in + i)) {
 				h->upload_pending = false;
