@@ -1666,6 +1666,7 @@ int cc_energy_grad(cc_handle *h, double *E, double *F, int precision)
 		h->last_gen = g_alloc_gen.load();
 	}
 	CC_CUDA(cudaStreamSynchronize(h->stream));
+	h->in_pending = false;   // ev_in was recorded on this stream: the staging buffer is free again
 	if (int rc = check_barrier(h))
 		return rc;
 	*E = h->h_pin[0];
