@@ -2246,6 +2246,7 @@ struct cc_batch {
 	unsigned char *lb_base = nullptr;
 	size_t lb_cap = 0;
 	cc::LbInst *d_lb = nullptr;
+	cc::LbBrief *d_brief = nullptr;
 	int d_lb_cap = 0;
 };
 
@@ -2635,6 +2636,7 @@ int cc_batch_destroy(cc_batch *b)
 	cudaFree(b->arena.base);
 	cudaFree(b->lb_base);
 	cudaFree(b->d_lb);
+	cudaFree(b->d_brief);
 	if (b->stream)
 		cudaStreamDestroy(b->stream);
 	delete b;
@@ -2731,9 +2733,11 @@ int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opt
 	}
 	if (b->d_lb_cap < count) {
 		cudaFree(b->d_lb);
+		cudaFree(b->d_brief);
 		b->d_lb = nullptr;
+		b->d_brief = nullptr;
 		b->d_lb_cap = 0;
-		if ((rc = dev_alloc(&b->d_lb, count)))
+		if ((rc = dev_alloc(&b->d_lb, count)) || (rc = dev_alloc(&b->d_brief, count)))
 			return rc;
 		b->d_lb_cap = count;
 	}
@@ -2859,7 +2863,7 @@ int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opt
 		destroy_graphs();
 		return cleanup(rc);
 	}
-	std::vector<cc::LbState> hs(count);
+	std::vector<cc::LbBrief> hs(count);
 	int stage = 0;
 	const int64_t max_rounds = o.max_evals / o.iters_per_check + 2;
 	for (int64_t round = 0; round < max_rounds; round++) {
@@ -2875,10 +2879,16 @@ int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opt
 			return cleanup(rc);
 		}
 		bool running = false, any_mixed = false;
-		for (int i = 0; i < count; i++) {
-			CC_CUDA(cudaMemcpyAsync(&hs[i], lbi[i].st, offsetof(cc::LbState, w), cudaMemcpyDeviceToHost, st));
+		cc::lb_brief_kernel<<<(count + 127) / 128, 128, 0, st>>>(d_lb, count, b->d_brief);
+		e = cudaGetLastError();
+		if (e == cudaSuccess)
+			e = cudaMemcpyAsync(hs.data(), b->d_brief, sizeof(cc::LbBrief) * count, cudaMemcpyDeviceToHost, st);
+		if (e == cudaSuccess)
+			e = cudaStreamSynchronize(st);
+		if (e != cudaSuccess) {
+			destroy_graphs();
+			return cleanup(fail(CC_ERR_CUDA, std::string("batch minimisation status: ") + cudaGetErrorString(e)));
 		}
-		CC_CUDA(cudaStreamSynchronize(st));
 		for (int i = 0; i < count; i++) {
 			running |= hs[i].status == cc::kLbRunning;
 			any_mixed |= hs[i].status == cc::kLbRunning && hs[i].stage == 0;

@@ -51,6 +51,13 @@ struct LbState {
 	double Sg[kLbMaxHist], Yg[kLbMaxHist];// S^T g, Y^T g at x (ring slots)
 };
 
+// What the host reads of each instance between blocks of iterations (gathered into one array: one copy per check)
+struct LbBrief {
+	int64_t evals, iters;
+	double E;
+	int status, stage;
+};
+
 struct LbInst {
 	int n;                  // variables
 	double *x, *g, *d, *xt, *gt;
@@ -443,6 +450,15 @@ static __global__ void __launch_bounds__(kLbThreads) lb_update_kernel(const LbIn
 		in.d[j] = -v;
 	}
 	in.xt[j] = in.x[j] + st->alpha * in.d[j];
+}
+
+static __global__ void lb_brief_kernel(const LbInst *insts, int count, LbBrief *out)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < count) {
+		const LbState *st = insts[i].st;
+		out[i] = LbBrief{st->evals, st->iters, st->E, st->status, st->stage};
+	}
 }
 
 }  // namespace cc

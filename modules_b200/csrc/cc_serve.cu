@@ -305,6 +305,7 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 	cc::LbInst *d_li = nullptr;
 	int *d_pre = nullptr, *d_shape = nullptr;
 	unsigned *d_queue = nullptr;
+	cc::LbBrief *d_brief = nullptr;
 	SV_CUDA(cudaMalloc(&d_ra, sizeof(cc::RhoArgs) * o.max_slots));
 	SV_CUDA(cudaMalloc(&d_rr, sizeof(cc::ReduceArgs) * o.max_slots));
 	SV_CUDA(cudaMalloc(&d_fa, sizeof(cc::ForceArgs) * o.max_slots));
@@ -312,6 +313,7 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 	SV_CUDA(cudaMalloc(&d_pre, sizeof(int) * 3 * (o.max_slots + 3)));
 	SV_CUDA(cudaMalloc(&d_shape, sizeof(int) * 3 * o.max_slots));
 	SV_CUDA(cudaMalloc(&d_queue, sizeof(unsigned) * 18));
+	SV_CUDA(cudaMalloc(&d_brief, sizeof(cc::LbBrief) * o.max_slots));
 	SV_CUDA(cudaMemset(d_queue, 0, sizeof(unsigned) * 18));
 	std::vector<int> order(count);
 	for (int i = 0; i < count; i++)
@@ -322,7 +324,7 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 	size_t used = 0;
 	int next = 0, done = 0;
 	int rc = CC_OK;
-	std::vector<cc::LbState> hs(o.max_slots);
+	std::vector<cc::LbBrief> hs(o.max_slots);
 	const auto t0 = std::chrono::steady_clock::now();
 	auto now = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
 	while (done < count && rc == CC_OK) {
@@ -423,8 +425,10 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 		if (rc)
 			break;
 		// 3. retire finished requests
-		for (int a = 0; a < A; a++)
-			SV_CUDA(cudaMemcpyAsync(&hs[a], active[a].li.st, offsetof(cc::LbState, w), cudaMemcpyDeviceToHost, st));
+		// every slot's status, energy and evaluation count: one gather kernel, one copy (d_li holds this round's slots)
+		cc::lb_brief_kernel<<<(A + 127) / 128, 128, 0, st>>>(d_li, A, d_brief);
+		SV_CUDA(cudaGetLastError());
+		SV_CUDA(cudaMemcpyAsync(hs.data(), d_brief, sizeof(cc::LbBrief) * A, cudaMemcpyDeviceToHost, st));
 		SV_CUDA(cudaStreamSynchronize(st));
 		const double tdone = now();
 		std::vector<Slot> keep;
@@ -456,6 +460,7 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 	cudaFree(d_pre);
 	cudaFree(d_shape);
 	cudaFree(d_queue);
+	cudaFree(d_brief);
 	cudaMemPoolDestroy(pool);
 	cudaStreamDestroy(st);
 	return rc;
