@@ -2241,6 +2241,9 @@ struct cc_batch {
 	std::vector<BatchBufs> bufs;
 	int per_split = 0, segs_per_split = 0;   // the tile shape in use
 	cudaStream_t stream = nullptr;
+	// the groups after the first run on side streams, forked from and joined back into the launching stream
+	cudaStream_t side[2] = {nullptr, nullptr};
+	cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
 	// L-BFGS state of cc_batch_minimize, kept between calls (grow-only): a minimisation makes no allocation call
 	// into the driver once the batch has run one
 	unsigned char *lb_base = nullptr;
@@ -2459,17 +2462,30 @@ int batch_build(cc_batch *b, int per_split, int segs_per_split)
 
 // evaluate every group with the given descriptors (lb = the minimisation's); precision CC_PREC_SCHEDULE launches
 // kernels that evaluate each instance at the precision of its stage word (FP64 where it has none)
+// The groups (one per dimension) are independent: the first runs on `st`, the others on side streams forked from
+// and joined back into `st` (parallel branches when captured in a graph), so their launches overlap on the device.
 int batch_eval(cc_batch *b, bool lb, int precision, cudaStream_t st)
 {
-	for (BatchGroup &g : b->groups) {
+	const int ng = (int)b->groups.size();
+	if (ng > 1)
+		CC_CUDA(cudaEventRecord(b->ev_fork, st));
+	for (int k = 0; k < ng; k++) {
+		BatchGroup &g = b->groups[k];
+		cudaStream_t gs = k == 0 ? st : b->side[k - 1];
+		if (k > 0)
+			CC_CUDA(cudaStreamWaitEvent(gs, b->ev_fork, 0));
 		if (precision == CC_PREC_SCHEDULE) {
-			const int rc = g.D == 1 ? multi_launch_sched_t<1>(g, lb ? 1 : 0, st)
-			             : g.D == 2 ? multi_launch_sched_t<2>(g, lb ? 1 : 0, st)
-			                        : multi_launch_sched_t<3>(g, lb ? 1 : 0, st);
+			const int rc = g.D == 1 ? multi_launch_sched_t<1>(g, lb ? 1 : 0, gs)
+			             : g.D == 2 ? multi_launch_sched_t<2>(g, lb ? 1 : 0, gs)
+			                        : multi_launch_sched_t<3>(g, lb ? 1 : 0, gs);
 			if (rc)
 				return rc;
-		} else if (int rc = multi_launch(g, precision == CC_PREC_MIXED, lb ? 1 : 0, st)) {
+		} else if (int rc = multi_launch(g, precision == CC_PREC_MIXED, lb ? 1 : 0, gs)) {
 			return rc;
+		}
+		if (k > 0) {
+			CC_CUDA(cudaEventRecord(b->ev_join[k - 1], gs));
+			CC_CUDA(cudaStreamWaitEvent(st, b->ev_join[k - 1], 0));
 		}
 	}
 	return CC_OK;
@@ -2534,7 +2550,12 @@ int cc_batch_create(int count, cc_handle *const *handles, const int64_t *N, cc_b
 	}
 	b->arena.cap = b->arena.used;
 	if (cudaMemset(b->arena.base, 0, b->arena.used) != cudaSuccess ||
-	    cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+	    cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+	    cudaStreamCreateWithFlags(&b->side[0], cudaStreamNonBlocking) != cudaSuccess ||
+	    cudaStreamCreateWithFlags(&b->side[1], cudaStreamNonBlocking) != cudaSuccess ||
+	    cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+	    cudaEventCreateWithFlags(&b->ev_join[0], cudaEventDisableTiming) != cudaSuccess ||
+	    cudaEventCreateWithFlags(&b->ev_join[1], cudaEventDisableTiming) != cudaSuccess) {
 		cc_batch_destroy(b);
 		return fail(CC_ERR_CUDA, "batch initialisation failed");
 	}
@@ -2637,6 +2658,16 @@ int cc_batch_destroy(cc_batch *b)
 	cudaFree(b->lb_base);
 	cudaFree(b->d_lb);
 	cudaFree(b->d_brief);
+	for (int k = 0; k < 2; k++) {
+		if (b->side[k]) {
+			cudaStreamSynchronize(b->side[k]);
+			cudaStreamDestroy(b->side[k]);
+		}
+		if (b->ev_join[k])
+			cudaEventDestroy(b->ev_join[k]);
+	}
+	if (b->ev_fork)
+		cudaEventDestroy(b->ev_fork);
 	if (b->stream)
 		cudaStreamDestroy(b->stream);
 	delete b;
