@@ -271,6 +271,14 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 	const int nblk_cap = cc::kLbMaxBlocks;
 	cudaStream_t st;
 	SV_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+	// the dimension groups after the first run on side streams forked from and joined back into st
+	cudaStream_t side[2];
+	cudaEvent_t ev_fork, ev_join[2];
+	SV_CUDA(cudaStreamCreateWithFlags(&side[0], cudaStreamNonBlocking));
+	SV_CUDA(cudaStreamCreateWithFlags(&side[1], cudaStreamNonBlocking));
+	SV_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+	SV_CUDA(cudaEventCreateWithFlags(&ev_join[0], cudaEventDisableTiming));
+	SV_CUDA(cudaEventCreateWithFlags(&ev_join[1], cudaEventDisableTiming));
 	// The requests' memory comes from a pool of the server's own that keeps what it holds (release threshold: all)
 	// and holds the HBM budget from the start (as far as the device has it free): admitting and retiring requests then
 	// makes no allocation call into the driver, whose calls took up to ~1 s under contention on shared hosts.
@@ -406,13 +414,28 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 		// the descriptor vectors are pageable: the copies complete before the iterations read them
 		const int nblk = cc::lb_blocks(maxn, nblk_cap);
 		for (int it = 0; it < o.iters_per_round && rc == CC_OK; it++) {
-			for (const G &g : groups)
+			const int ng = (int)groups.size();
+			if (ng > 1 && cudaEventRecord(ev_fork, st) != cudaSuccess) {
+				rc = sfail(CC_ERR_CUDA, "serve: event record failed");
+				break;
+			}
+			for (int k = 0; k < ng && rc == CC_OK; k++) {
+				const G &g = groups[k];
+				cudaStream_t gs = k == 0 ? st : side[k - 1];
+				if (k > 0 && cudaStreamWaitEvent(gs, ev_fork, 0) != cudaSuccess) {
+					rc = sfail(CC_ERR_CUDA, "serve: stream wait failed");
+					break;
+				}
 				if ((rc = cc::launch_multi(g.D, false, d_ra + g.off, d_rr + g.off, d_fa + g.off, d_pre + g.pre_off,
 				                           d_shape + g.shape_off, g.B, g.total, g.rho_row, g.force_row,
-				                           d_queue + 6 * (g.D - 1), st))) {
+				                           d_queue + 6 * (g.D - 1), gs))) {
 					s_err = std::string("serve: ") + cc_last_error();
 					break;
 				}
+				if (k > 0 && (cudaEventRecord(ev_join[k - 1], gs) != cudaSuccess ||
+				              cudaStreamWaitEvent(st, ev_join[k - 1], 0) != cudaSuccess))
+					rc = sfail(CC_ERR_CUDA, "serve: stream join failed");
+			}
 			if (rc)
 				break;
 			cc::lb_dots_kernel<<<dim3(nblk, A), cc::kLbThreads, 0, st>>>(d_li, nblk);
@@ -448,6 +471,8 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 		}
 		active.swap(keep);
 	}
+	cudaStreamSynchronize(side[0]);   // on an error path a side stream may not have been joined yet
+	cudaStreamSynchronize(side[1]);
 	for (Slot &s : active)
 		cudaFreeAsync(s.mem, st);
 	cudaStreamSynchronize(st);
@@ -462,6 +487,12 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 	cudaFree(d_queue);
 	cudaFree(d_brief);
 	cudaMemPoolDestroy(pool);
+	for (int k = 0; k < 2; k++) {
+		cudaStreamSynchronize(side[k]);
+		cudaStreamDestroy(side[k]);
+		cudaEventDestroy(ev_join[k]);
+	}
+	cudaEventDestroy(ev_fork);
 	cudaStreamDestroy(st);
 	return rc;
 }
