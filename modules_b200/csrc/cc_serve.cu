@@ -361,7 +361,9 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 			}
 			continue;
 		}
-		// 2. descriptors of the active set, grouped by dimension
+		// 2. descriptors of the active set, grouped by dimension (the slots ordered by dimension, so that each group's
+		// L-BFGS instances are a contiguous range)
+		std::stable_sort(active.begin(), active.end(), [](const Slot &x, const Slot &y) { return x.d < y.d; });
 		const int A = (int)active.size();
 		std::vector<cc::LbInst> li(A);
 		int maxn = 0;
@@ -374,11 +376,11 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 		std::vector<cc::ForceArgs> fa;
 		std::vector<int> pre, shape;
 		struct G {
-			int D, off, B, pre_off, shape_off, total[3], rho_row, force_row;
+			int D, off, B, pre_off, shape_off, total[3], rho_row, force_row, maxn;
 		};
 		std::vector<G> groups;
 		for (int D = 1; D <= 3; D++) {
-			G g = {D, (int)ra.size(), 0, (int)pre.size(), (int)shape.size(), {0, 0, 0}, 1, 1};
+			G g = {D, (int)ra.size(), 0, (int)pre.size(), (int)shape.size(), {0, 0, 0}, 1, 1, 0};
 			std::vector<int> members;
 			for (int a = 0; a < A; a++)
 				if (active[a].d == D)
@@ -398,6 +400,7 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 				}
 				g.rho_row = std::max(g.rho_row, sl.rho_row);
 				g.force_row = std::max(g.force_row, sl.force_row);
+				g.maxn = std::max(g.maxn, sl.li.n);
 			}
 			for (int ph = 0; ph < 3; ph++)
 				g.total[ph] = p3[ph * (g.B + 1) + g.B];
@@ -412,39 +415,40 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 		SV_CUDA(cudaMemcpyAsync(d_pre, pre.data(), sizeof(int) * pre.size(), cudaMemcpyHostToDevice, st));
 		SV_CUDA(cudaMemcpyAsync(d_shape, shape.data(), sizeof(int) * shape.size(), cudaMemcpyHostToDevice, st));
 		// the descriptor vectors are pageable: the copies complete before the iterations read them
-		const int nblk = cc::lb_blocks(maxn, nblk_cap);
+		// Each group runs its iterations (energy and gradient, then its instances' L-BFGS step) on its own stream,
+		// forked from st at the start of the round and joined back at its end; the launches are issued iteration by
+		// iteration across the groups, so every stream has work queued from the start.
+		(void)maxn;
+		const int ng = (int)groups.size();
+		if (ng > 1 && cudaEventRecord(ev_fork, st) != cudaSuccess)
+			rc = sfail(CC_ERR_CUDA, "serve: event record failed");
+		for (int k = 1; k < ng && rc == CC_OK; k++)
+			if (cudaStreamWaitEvent(side[k - 1], ev_fork, 0) != cudaSuccess)
+				rc = sfail(CC_ERR_CUDA, "serve: stream wait failed");
 		for (int it = 0; it < o.iters_per_round && rc == CC_OK; it++) {
-			const int ng = (int)groups.size();
-			if (ng > 1 && cudaEventRecord(ev_fork, st) != cudaSuccess) {
-				rc = sfail(CC_ERR_CUDA, "serve: event record failed");
-				break;
-			}
 			for (int k = 0; k < ng && rc == CC_OK; k++) {
 				const G &g = groups[k];
 				cudaStream_t gs = k == 0 ? st : side[k - 1];
-				if (k > 0 && cudaStreamWaitEvent(gs, ev_fork, 0) != cudaSuccess) {
-					rc = sfail(CC_ERR_CUDA, "serve: stream wait failed");
-					break;
-				}
+				const cc::LbInst *gli = d_li + g.off;
+				const int gnblk = cc::lb_blocks(g.maxn, nblk_cap);
 				if ((rc = cc::launch_multi(g.D, false, d_ra + g.off, d_rr + g.off, d_fa + g.off, d_pre + g.pre_off,
 				                           d_shape + g.shape_off, g.B, g.total, g.rho_row, g.force_row,
 				                           d_queue + 6 * (g.D - 1), gs))) {
 					s_err = std::string("serve: ") + cc_last_error();
 					break;
 				}
-				if (k > 0 && (cudaEventRecord(ev_join[k - 1], gs) != cudaSuccess ||
-				              cudaStreamWaitEvent(st, ev_join[k - 1], 0) != cudaSuccess))
-					rc = sfail(CC_ERR_CUDA, "serve: stream join failed");
+				cc::lb_dots_kernel<<<dim3(gnblk, g.B), cc::kLbThreads, 0, gs>>>(gli, gnblk);
+				cc::lb_solve_kernel<<<g.B, cc::kLbSolveThreads, 0, gs>>>(gli, gnblk);
+				cc::lb_update_kernel<<<dim3((g.maxn + cc::kLbThreads - 1) / cc::kLbThreads, g.B), cc::kLbThreads, 0,
+				                       gs>>>(gli);
+				if (cudaGetLastError() != cudaSuccess)
+					rc = sfail(CC_ERR_CUDA, "serve: kernel launch failed");
 			}
-			if (rc)
-				break;
-			cc::lb_dots_kernel<<<dim3(nblk, A), cc::kLbThreads, 0, st>>>(d_li, nblk);
-			cc::lb_solve_kernel<<<A, cc::kLbSolveThreads, 0, st>>>(d_li, nblk);
-			cc::lb_update_kernel<<<dim3((maxn + cc::kLbThreads - 1) / cc::kLbThreads, A), cc::kLbThreads, 0, st>>>(
-			    d_li);
-			if (cudaGetLastError() != cudaSuccess)
-				rc = sfail(CC_ERR_CUDA, "serve: kernel launch failed");
 		}
+		for (int k = 1; k < ng && rc == CC_OK; k++)
+			if (cudaEventRecord(ev_join[k - 1], side[k - 1]) != cudaSuccess ||
+			    cudaStreamWaitEvent(st, ev_join[k - 1], 0) != cudaSuccess)
+				rc = sfail(CC_ERR_CUDA, "serve: stream join failed");
 		if (rc)
 			break;
 		// 3. retire finished requests
