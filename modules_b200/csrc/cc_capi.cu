@@ -2248,7 +2248,7 @@ struct cc_batch {
 	// into the driver once the batch has run one
 	unsigned char *lb_base = nullptr;
 	size_t lb_cap = 0;
-	cc::LbInst *d_lb = nullptr;
+	cc::LbInst *d_lb = nullptr;   // 2 x d_lb_cap: the instances in order, then grouped by dimension
 	cc::LbBrief *d_brief = nullptr;
 	int d_lb_cap = 0;
 };
@@ -2462,6 +2462,16 @@ int batch_build(cc_batch *b, int per_split, int segs_per_split)
 
 // evaluate every group with the given descriptors (lb = the minimisation's); precision CC_PREC_SCHEDULE launches
 // kernels that evaluate each instance at the precision of its stage word (FP64 where it has none)
+// one group's evaluation (the descriptors of set lb ? 1 : 0) on stream gs
+int group_eval(BatchGroup &g, bool lb, int precision, cudaStream_t gs)
+{
+	if (precision == CC_PREC_SCHEDULE)
+		return g.D == 1 ? multi_launch_sched_t<1>(g, lb ? 1 : 0, gs)
+		     : g.D == 2 ? multi_launch_sched_t<2>(g, lb ? 1 : 0, gs)
+		                : multi_launch_sched_t<3>(g, lb ? 1 : 0, gs);
+	return multi_launch(g, precision == CC_PREC_MIXED, lb ? 1 : 0, gs);
+}
+
 // The groups (one per dimension) are independent: the first runs on `st`, the others on side streams forked from
 // and joined back into `st` (parallel branches when captured in a graph), so their launches overlap on the device.
 int batch_eval(cc_batch *b, bool lb, int precision, cudaStream_t st)
@@ -2474,15 +2484,8 @@ int batch_eval(cc_batch *b, bool lb, int precision, cudaStream_t st)
 		cudaStream_t gs = k == 0 ? st : b->side[k - 1];
 		if (k > 0)
 			CC_CUDA(cudaStreamWaitEvent(gs, b->ev_fork, 0));
-		if (precision == CC_PREC_SCHEDULE) {
-			const int rc = g.D == 1 ? multi_launch_sched_t<1>(g, lb ? 1 : 0, gs)
-			             : g.D == 2 ? multi_launch_sched_t<2>(g, lb ? 1 : 0, gs)
-			                        : multi_launch_sched_t<3>(g, lb ? 1 : 0, gs);
-			if (rc)
-				return rc;
-		} else if (int rc = multi_launch(g, precision == CC_PREC_MIXED, lb ? 1 : 0, gs)) {
+		if (int rc = group_eval(g, lb, precision, gs))
 			return rc;
-		}
 		if (k > 0) {
 			CC_CUDA(cudaEventRecord(b->ev_join[k - 1], gs));
 			CC_CUDA(cudaStreamWaitEvent(st, b->ev_join[k - 1], 0));
@@ -2768,7 +2771,7 @@ int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opt
 		b->d_lb = nullptr;
 		b->d_brief = nullptr;
 		b->d_lb_cap = 0;
-		if ((rc = dev_alloc(&b->d_lb, count)) || (rc = dev_alloc(&b->d_brief, count)))
+		if ((rc = dev_alloc(&b->d_lb, 2 * (size_t)count)) || (rc = dev_alloc(&b->d_brief, count)))
 			return rc;
 		b->d_lb_cap = count;
 	}
@@ -2817,6 +2820,19 @@ int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opt
 	}
 	if ((rc = upload_into(d_lb, lbi)))
 		return cleanup(rc);
+	// the same instances grouped by dimension (each group's L-BFGS kernels run on its own stream)
+	std::vector<cc::LbInst> lbg;
+	std::vector<int> g_off, g_maxn;
+	for (BatchGroup &g : b->groups) {
+		g_off.push_back((int)lbg.size());
+		int mx = 0;
+		for (int i : g.members) {
+			lbg.push_back(lbi[i]);
+			mx = std::max(mx, lbi[i].n);
+		}
+		g_maxn.push_back(mx);
+	}
+	CC_CUDA(cudaMemcpy(d_lb + count, lbg.data(), sizeof(cc::LbInst) * lbg.size(), cudaMemcpyHostToDevice));
 	// minimisation descriptors: evaluate at x_trial into the L-BFGS buffers, skip finished instances
 	for (BatchGroup &g : b->groups) {
 		std::vector<cc::RhoArgs> ra = g.rho;
@@ -2847,21 +2863,41 @@ int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opt
 	// schedule: one launch per kernel, each instance at its stage's precision, while some instance is in the mixed
 	// stage; then the FP64 kernels only
 	const int prec0 = o.precision;
-	auto iteration = [&](int prec) -> int {
-		if (int r2 = batch_eval(b, true, prec, st))
-			return r2;
-		cc::lb_dots_kernel<<<dim3(nblk, count), cc::kLbThreads, 0, st>>>(d_lb, nblk);
-		cc::lb_solve_kernel<<<count, cc::kLbSolveThreads, 0, st>>>(d_lb, nblk);
-		cc::lb_update_kernel<<<dim3((maxn + cc::kLbThreads - 1) / cc::kLbThreads, count), cc::kLbThreads, 0, st>>>(d_lb);
-		CC_CUDA(cudaGetLastError());
+	// Each dimension group runs its iterations (evaluation, then its instances' L-BFGS step) on its own stream,
+	// forked from st at the start of the graph and joined back at its end; launches interleaved by iteration.
+	(void)nblk;
+	(void)maxn;
+	const int ngr = (int)b->groups.size();
+	auto iterations = [&](int prec) -> int {
+		if (ngr > 1) {
+			CC_CUDA(cudaEventRecord(b->ev_fork, st));
+			for (int k = 1; k < ngr; k++)
+				CC_CUDA(cudaStreamWaitEvent(b->side[k - 1], b->ev_fork, 0));
+		}
+		for (int it = 0; it < o.iters_per_check; it++)
+			for (int k = 0; k < ngr; k++) {
+				BatchGroup &g = b->groups[k];
+				cudaStream_t gs = k == 0 ? st : b->side[k - 1];
+				if (int r2 = group_eval(g, true, prec, gs))
+					return r2;
+				const cc::LbInst *gl = d_lb + count + g_off[k];
+				const int gb = (int)g.members.size(), gn = cc::lb_blocks(g_maxn[k], cc::kLbMaxBlocks);
+				cc::lb_dots_kernel<<<dim3(gn, gb), cc::kLbThreads, 0, gs>>>(gl, gn);
+				cc::lb_solve_kernel<<<gb, cc::kLbSolveThreads, 0, gs>>>(gl, gn);
+				cc::lb_update_kernel<<<dim3((g_maxn[k] + cc::kLbThreads - 1) / cc::kLbThreads, gb), cc::kLbThreads, 0,
+				                       gs>>>(gl);
+				CC_CUDA(cudaGetLastError());
+			}
+		for (int k = 1; k < ngr; k++) {
+			CC_CUDA(cudaEventRecord(b->ev_join[k - 1], b->side[k - 1]));
+			CC_CUDA(cudaStreamWaitEvent(st, b->ev_join[k - 1], 0));
+		}
 		return CC_OK;
 	};
 	auto make_graph = [&](int prec, cudaGraphExec_t *out) -> int {
 		cudaGraph_t g = nullptr;
 		CC_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-		int r2 = CC_OK;
-		for (int k = 0; k < o.iters_per_check && r2 == CC_OK; k++)
-			r2 = iteration(prec);
+		const int r2 = iterations(prec);
 		cudaError_t e = cudaStreamEndCapture(st, &g);
 		if (r2)
 			return r2;
