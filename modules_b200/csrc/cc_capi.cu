@@ -2001,9 +2001,7 @@ int lb_iteration(cc_handle *h, int64_t N, LbBuffers &b, int n, int nblk, int pre
 {
 	if (int rc = eval_device(h, N, b.xt, &b.st->Et, nullptr, b.gt, false, prec, st))
 		return rc;
-	cc::lb_dots_kernel<<<dim3(nblk, 1), cc::kLbThreads, 0, st>>>(b.inst, nblk);
-	cc::lb_solve_kernel<<<1, cc::kLbSolveThreads, 0, st>>>(b.inst, nblk);
-	cc::lb_update_kernel<<<dim3((n + cc::kLbThreads - 1) / cc::kLbThreads, 1), cc::kLbThreads, 0, st>>>(b.inst);
+	CC_CUDA(cc::lb_step(b.inst, 1, nblk, n, st));
 	CC_CUDA(cudaGetLastError());
 	return CC_OK;
 }
@@ -2882,10 +2880,7 @@ int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opt
 					return r2;
 				const cc::LbInst *gl = d_lb + count + g_off[k];
 				const int gb = (int)g.members.size(), gn = cc::lb_blocks(g_maxn[k], cc::kLbMaxBlocks);
-				cc::lb_dots_kernel<<<dim3(gn, gb), cc::kLbThreads, 0, gs>>>(gl, gn);
-				cc::lb_solve_kernel<<<gb, cc::kLbSolveThreads, 0, gs>>>(gl, gn);
-				cc::lb_update_kernel<<<dim3((g_maxn[k] + cc::kLbThreads - 1) / cc::kLbThreads, gb), cc::kLbThreads, 0,
-				                       gs>>>(gl);
+				CC_CUDA(cc::lb_step(gl, gb, gn, g_maxn[k], gs));
 				CC_CUDA(cudaGetLastError());
 			}
 		for (int k = 1; k < ngr; k++) {

@@ -86,6 +86,7 @@ constexpr int kLbMaxBlocks = 64;   // cap of the batched minimisation and the se
 // order, warps in order for the non-pair products), so a run repeats bitwise.
 static __global__ void __launch_bounds__(kLbThreads) lb_dots_kernel(const LbInst *insts, int cap)
 {
+	cudaGridDependencySynchronize();   // launched early (programmatic dependent launch): the evaluation is complete
 	const LbInst in = insts[blockIdx.y];
 	const LbState *st = in.st;
 	const int nblk = lb_blocks(in.n, cap);
@@ -190,6 +191,7 @@ constexpr int kLbSolveThreads = 256;
 // the compact form (warp 0, lanes split every inner sum), g.d of the new direction and the stop tests.
 static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const LbInst *insts, int cap)
 {
+	cudaGridDependencySynchronize();
 	const LbInst in = insts[blockIdx.x];
 	LbState *st = in.st;
 	if (st->status != kLbRunning)
@@ -403,6 +405,7 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 // reject: x_trial = x + alpha d.
 static __global__ void __launch_bounds__(kLbThreads) lb_update_kernel(const LbInst *insts)
 {
+	cudaGridDependencySynchronize();
 	const LbInst in = insts[blockIdx.y];
 	const LbState *st = in.st;
 	if (st->status != kLbRunning && !(st->accepted && st->status != kLbLineSearch))
@@ -459,6 +462,32 @@ static __global__ void lb_brief_kernel(const LbInst *insts, int count, LbBrief *
 		const LbState *st = insts[i].st;
 		out[i] = LbBrief{st->evals, st->iters, st->E, st->status, st->stage};
 	}
+}
+
+// The three kernels of one L-BFGS step on stream st for `count` instances (insts), at most `cap` dot-product blocks
+// per instance and `maxn` variables in the largest one. Each is launched with programmatic stream serialisation:
+// it is scheduled while the previous kernel drains and waits for it (cudaGridDependencySynchronize) before it reads.
+inline cudaError_t lb_step(const LbInst *insts, int count, int cap, int maxn, cudaStream_t st)
+{
+	cudaLaunchAttribute attr[1];
+	attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+	attr[0].val.programmaticStreamSerializationAllowed = 1;
+	cudaLaunchConfig_t cfg = {};
+	cfg.stream = st;
+	cfg.attrs = attr;
+	cfg.numAttrs = 1;
+	cfg.gridDim = dim3(cap, count);
+	cfg.blockDim = dim3(kLbThreads);
+	cudaError_t e = cudaLaunchKernelEx(&cfg, lb_dots_kernel, insts, cap);
+	if (e != cudaSuccess)
+		return e;
+	cfg.gridDim = dim3(count);
+	cfg.blockDim = dim3(kLbSolveThreads);
+	if ((e = cudaLaunchKernelEx(&cfg, lb_solve_kernel, insts, cap)) != cudaSuccess)
+		return e;
+	cfg.gridDim = dim3((maxn + kLbThreads - 1) / kLbThreads, count);
+	cfg.blockDim = dim3(kLbThreads);
+	return cudaLaunchKernelEx(&cfg, lb_update_kernel, insts);
 }
 
 }  // namespace cc

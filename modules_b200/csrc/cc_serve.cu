@@ -437,11 +437,7 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 					s_err = std::string("serve: ") + cc_last_error();
 					break;
 				}
-				cc::lb_dots_kernel<<<dim3(gnblk, g.B), cc::kLbThreads, 0, gs>>>(gli, gnblk);
-				cc::lb_solve_kernel<<<g.B, cc::kLbSolveThreads, 0, gs>>>(gli, gnblk);
-				cc::lb_update_kernel<<<dim3((g.maxn + cc::kLbThreads - 1) / cc::kLbThreads, g.B), cc::kLbThreads, 0,
-				                       gs>>>(gli);
-				if (cudaGetLastError() != cudaSuccess)
+				if (cc::lb_step(gli, g.B, gnblk, g.maxn, gs) != cudaSuccess)
 					rc = sfail(CC_ERR_CUDA, "serve: kernel launch failed");
 			}
 		}
