@@ -200,6 +200,7 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 	__shared__ double tot[5 * kLbMaxHist + 6];
 	__shared__ double Sg[kLbMaxHist], Yg[kLbMaxHist], t[kLbMaxHist], q[kLbMaxHist], w1[kLbMaxHist];
 	__shared__ double sR[kLbMaxHist * kLbMaxHist];
+	__shared__ double rdiag[kLbMaxHist];
 	__shared__ int sh_accept, sh_newslot;
 	const int m = st->m, nd = lb_ndots(m);
 	for (int k = threadIdx.x; k < nd; k += kLbSolveThreads) {
@@ -321,13 +322,16 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 		const int a = e / k, b = e - a * k;
 		sR[e] = st->SY[((head + a) % m) * m + (head + b) % m];
 	}
+	// reciprocals of the diagonal s_a . y_a, formed in parallel (the solves then multiply)
+	for (int a = threadIdx.x; a < k; a += kLbSolveThreads)
+		rdiag[a] = 1.0 / st->SY[((head + a) % m) * m + (head + a) % m];
 	__syncthreads();
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	if (warp == 0) {
 		// t = R^-1 S^T g: backward substitution
 		double r0 = lane < k ? Sg[(head + lane) % m] : 0.0, r1 = lane + 32 < k ? Sg[(head + lane + 32) % m] : 0.0;
 		for (int b = k - 1; b >= 0; b--) {
-			const double own = (b < 32 ? r0 : r1) / sR[b * k + b];
+			const double own = (b < 32 ? r0 : r1) * rdiag[b];
 			const double tb = __shfl_sync(0xffffffffu, own, b & 31);
 			if (lane == 0)
 				t[b] = tb;
@@ -353,7 +357,7 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 		// w1 = R^-T q: forward substitution
 		double r0 = lane < k ? q[lane] : 0.0, r1 = lane + 32 < k ? q[lane + 32] : 0.0;
 		for (int b = 0; b < k; b++) {
-			const double own = (b < 32 ? r0 : r1) / sR[b * k + b];
+			const double own = (b < 32 ? r0 : r1) * rdiag[b];
 			const double wb = __shfl_sync(0xffffffffu, own, b & 31);
 			if (lane == 0)
 				w1[b] = wb;
