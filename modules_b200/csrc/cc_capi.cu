@@ -250,9 +250,9 @@ struct cc_handle {
 	bool mc_valid = false, mc_pending = false;
 	const int *d_skip = nullptr;    // evaluations do nothing while *d_skip != 0 (set by cc_minimize)
 	bool timing = false;            // cc_set_timing
-	// cc_minimize's state, kept between calls so that a minimisation makes no allocation call into the driver once
-	// the handle has run one of its size: FP64 / mixed buffers (capacities n variables, m pairs, nblk dot blocks) and
-	// the batch of one that runs the precision schedule (for sched_N particles)
+	// cc_minimize's state, kept between calls so that a minimisation makes no allocation call into the CUDA driver
+	// once the handle has run one of its size: FP64 / mixed buffers (capacities n variables, m pairs, nblk dot
+	// blocks) and the batch of one that runs the precision schedule (for sched_N particles)
 	LbBuffers lb;
 	int lb_n = 0, lb_m = 0, lb_nblk = 0;
 	cc_batch *sched_batch = nullptr;
@@ -2243,7 +2243,7 @@ struct cc_batch {
 	cudaStream_t side[2] = {nullptr, nullptr};
 	cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
 	// L-BFGS state of cc_batch_minimize, kept between calls (grow-only): a minimisation makes no allocation call
-	// into the driver once the batch has run one
+	// into the CUDA driver once the batch has run one
 	unsigned char *lb_base = nullptr;
 	size_t lb_cap = 0;
 	cc::LbInst *d_lb = nullptr;   // 2 x d_lb_cap: the instances in order, then grouped by dimension

@@ -281,7 +281,7 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 	SV_CUDA(cudaEventCreateWithFlags(&ev_join[1], cudaEventDisableTiming));
 	// The requests' memory comes from a pool of the server's own that keeps what it holds (release threshold: all)
 	// and holds the HBM budget from the start (as far as the device has it free): admitting and retiring requests then
-	// makes no allocation call into the driver, whose calls took up to ~1 s under contention on shared hosts.
+	// makes no allocation call into the CUDA driver, whose calls took up to ~1 s under contention on shared hosts.
 	int dev = 0;
 	SV_CUDA(cudaGetDevice(&dev));
 	cudaMemPoolProps pprops = {};

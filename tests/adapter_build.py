@@ -1,5 +1,5 @@
 """Build tests/_build/adapter_check: the GPU adapter compiled against the reference's own headers (needs the reference
-tree; the binary then runs on a GPU box without it)."""
+tree; the binary then runs on a machine without it)."""
 import os
 import subprocess
 
