@@ -200,7 +200,8 @@ struct cc_handle {
 	double *d_E = nullptr;
 	double *h_pin = nullptr;        // pinned results: E at [0], N*d forces or gradients from [2]
 	size_t pin_cap = 0;
-	double *h_in = nullptr;         // pinned staging of the wrapped positions (N*d)
+	double *h_in = nullptr;         // pinned staging of the wrapped positions (N*d), mapped
+	double *d_in = nullptr;         // device view of h_in (read by the upload kernel of the host-path graph)
 	size_t in_cap = 0;
 	cudaEvent_t ev_in = nullptr;    // recorded after the last copy out of h_in
 	bool in_pending = false;
@@ -633,10 +634,18 @@ int input_staging(cc_handle *h, size_t n)
 		g_alloc_gen++;
 		cudaFreeHost(h->h_in);
 		h->h_in = nullptr;
+		h->d_in = nullptr;
 		h->in_cap = 0;
-		cudaError_t e = cudaMallocHost(reinterpret_cast<void **>(&h->h_in), n * sizeof(double));
+		cudaError_t e = cudaHostAlloc(reinterpret_cast<void **>(&h->h_in), n * sizeof(double), cudaHostAllocMapped);
 		if (e != cudaSuccess)
-			return fail(CC_ERR_OOM, std::string("cudaMallocHost: ") + cudaGetErrorString(e));
+			return fail(CC_ERR_OOM, std::string("cudaHostAlloc: ") + cudaGetErrorString(e));
+		e = cudaHostGetDevicePointer(reinterpret_cast<void **>(&h->d_in), h->h_in, 0);
+		if (e != cudaSuccess) {
+			cudaFreeHost(h->h_in);
+			h->h_in = nullptr;
+			h->d_in = nullptr;
+			return fail(CC_ERR_CUDA, std::string("cudaHostGetDevicePointer: ") + cudaGetErrorString(e));
+		}
 		h->in_cap = n;
 	}
 	return CC_OK;
@@ -1416,7 +1425,11 @@ int launch_eval_graph(cc_handle *h, int64_t N, int precision, int forces, bool *
 	}
 	cudaGraph_t graph = nullptr;
 	CC_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-	cudaError_t ce = cudaMemcpyAsync(h->d_frac, h->h_in, sizeof(double) * N * h->d, cudaMemcpyHostToDevice, h->stream);
+	// the positions come in through a kernel reading the mapped staging buffer (the rho kernel after it is then
+	// launched while it drains, programmatic dependent launch, which a copy node would not allow)
+	const int64_t nv = N * h->d;
+	cc::cc_upload_kernel<<<(unsigned)((nv + 255) / 256), 256, 0, h->stream>>>(h->d_in, h->d_frac, nv);
+	cudaError_t ce = cudaGetLastError();
 	int rc = ce == cudaSuccess ? eval_device(h, N, h->d_frac, h->d_pin, forces ? h->d_pin + 2 : nullptr, nullptr,
 	                                         false, precision, h->stream)
 	                           : CC_ERR_CUDA;

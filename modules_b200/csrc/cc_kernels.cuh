@@ -661,6 +661,14 @@ static __global__ void cc_gather_rho_kernel(const double2 *__restrict__ rho_slot
 // E = shift when there is no constraint
 static __global__ void cc_set_scalar_kernel(double *p, double v) { *p = v; }
 
+// n doubles from src (mapped pinned host memory) to dst (device memory)
+static __global__ void cc_upload_kernel(const double *__restrict__ src, double *__restrict__ dst, int64_t n)
+{
+	const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n)
+		dst[i] = src[i];
+}
+
 // ---------------------------------------------------------------------------------------------------------------
 // force pass
 // ---------------------------------------------------------------------------------------------------------------
