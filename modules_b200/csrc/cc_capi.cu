@@ -201,7 +201,9 @@ struct cc_handle {
 	double *h_pin = nullptr;        // pinned results: E at [0], N*d forces or gradients from [2]
 	size_t pin_cap = 0;
 	double *h_in = nullptr;         // pinned staging of the wrapped positions (N*d), mapped
-	double *d_in = nullptr;         // device view of h_in (read by the upload kernel of the host-path graph)
+	double *d_in = nullptr;         // device view of h_in (read by the first kernel of the host-path graph)
+	double *rho_copy = nullptr;     // while the host-path graph is captured on the three-kernel path: the rho kernel
+	                                // reads the positions from d_in and stores them here (d_frac) for the force kernel
 	size_t in_cap = 0;
 	cudaEvent_t ev_in = nullptr;    // recorded after the last copy out of h_in
 	bool in_pending = false;
@@ -743,6 +745,7 @@ int run_rho(cc_handle *h, DevKSet &k, int64_t N, const double *d_frac, double *d
 	a.nslot = p.nslot;
 	a.partial = k.partial;
 	a.skip = h->d_skip;
+	a.frac_copy = (&k == &h->main) ? h->rho_copy : nullptr;
 	if (int rc = launch_rho(h->d, a, mixed, p.nbgroups(), nsplit, csize, p.block_max_row, st))
 		return rc;
 	if (after_rho)
@@ -1383,6 +1386,8 @@ int eval_device(cc_handle *h, int64_t N, const double *d_frac, double *d_E, doub
 	// with forces (and a constraint set and particles), the force kernel finishes the energy
 	const bool e_in_force = (d_F || d_gfrac) && N > 0 && h->main.plan.nslot > 0;
 	int rc = run_rho(h, h->main, N, d_frac, d_E, want_rho_mode, mixed, l, st, e1, e_in_force);
+	if (h->rho_copy)   // the rho kernel has stored the positions in device memory for the force kernel
+		d_frac = h->rho_copy;
 	if (rc)
 		return rc;
 	if (e2)
@@ -1425,14 +1430,25 @@ int launch_eval_graph(cc_handle *h, int64_t N, int precision, int forces, bool *
 	}
 	cudaGraph_t graph = nullptr;
 	CC_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-	// the positions come in through a kernel reading the mapped staging buffer (the rho kernel after it is then
-	// launched while it drains, programmatic dependent launch, which a copy node would not allow)
-	const int64_t nv = N * h->d;
-	cc::cc_upload_kernel<<<(unsigned)((nv + 255) / 256), 256, 0, h->stream>>>(h->d_in, h->d_frac, nv);
-	cudaError_t ce = cudaGetLastError();
-	int rc = ce == cudaSuccess ? eval_device(h, N, h->d_frac, h->d_pin, forces ? h->d_pin + 2 : nullptr, nullptr,
-	                                         false, precision, h->stream)
-	                           : CC_ERR_CUDA;
+	// Positions from the mapped staging buffer: on the three-kernel path the rho kernel reads them there and stores
+	// them into d_frac for the force kernel; on the NUFFT path a kernel copies them first. Either way the first
+	// kernel of the evaluation reads host memory, and no copy node sits in front of the programmatic dependent launches.
+	const bool nufft = h->use_nufft || (h->auto_path && nufft_preferred(h, N));
+	cudaError_t ce = cudaSuccess;
+	int rc;
+	if (nufft) {
+		const int64_t nv = N * h->d;
+		cc::cc_upload_kernel<<<(unsigned)((nv + 255) / 256), 256, 0, h->stream>>>(h->d_in, h->d_frac, nv);
+		ce = cudaGetLastError();
+		rc = ce == cudaSuccess ? eval_device(h, N, h->d_frac, h->d_pin, forces ? h->d_pin + 2 : nullptr, nullptr, false,
+		                                     precision, h->stream)
+		                       : CC_ERR_CUDA;
+	} else {
+		h->rho_copy = h->d_frac;
+		rc = eval_device(h, N, h->d_in, h->d_pin, forces ? h->d_pin + 2 : nullptr, nullptr, false, precision,
+		                 h->stream);
+		h->rho_copy = nullptr;
+	}
 	const cudaError_t ee = cudaStreamEndCapture(h->stream, &graph);
 	if (rc != CC_OK || ce != cudaSuccess || ee != cudaSuccess || g_alloc_gen.load() != gen) {
 		if (graph)

@@ -288,6 +288,8 @@ struct RhoArgs {
 	const int *skip;          // if not null and nonzero, the launch does nothing (a finished minimisation)
 	const int *stage;         // if not null, the launch does nothing unless *stage == want_stage
 	int want_stage;
+	double *frac_copy;        // if not null, the blocks of block group 0 also store their particles' coordinates
+	                          // there (frac is then host memory the kernels that follow do not read)
 };
 
 constexpr int kRhoWarps = 8;
@@ -321,6 +323,9 @@ __device__ __forceinline__ void rho_body(const RhoArgs &a, const int bg, const i
 	cudaGridDependencySynchronize();   // inputs of this step are complete (programmatic dependent launch)
 	if (eval_skipped(a.skip, a.stage, a.want_stage))   // uniform over the instance: no block reaches a cluster barrier
 		return;
+	if (a.frac_copy && bg == 0)
+		for (int t = threadIdx.x; t < (j1 - j0) * D; t += kRhoThreads)
+			a.frac_copy[(size_t)j0 * D + t] = a.frac[(size_t)j0 * D + t];
 	__syncthreads();
 	const int row = sp.row | 1;        // odd row stride: consecutive particles' rows start in different banks
 	SeedIdx ix = seed_index<D>(sp, sg);
