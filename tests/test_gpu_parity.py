@@ -80,6 +80,29 @@ def test_force_one_and_repeatability(gpu):
         assert np.array_equal(p.force(i), F1[i])
 
 
+def test_graph_path_tracks_positions(gpu):
+    """From its second identical call on, cc_energy_grad replays a captured graph that reads the staged positions
+    itself; every visit of each of several configurations must give the first visit's energy, forces and rho
+    (bitwise), rho being computed afterwards from the device copy of the positions that the graph leaves."""
+    r = load_golden("lattice_3d_skew")
+    p = make_pot(gpu, r)
+    rng = np.random.default_rng(4)
+    confs = [r["frac"]] + [rng.random(r["frac"].shape) for _ in range(3)]
+    first = []
+    for c in confs:
+        p.set_configuration(c)
+        E, F = p.energy_and_forces()
+        first.append((E, F.copy(), p.rho()))
+    for _ in range(3):
+        for c, (E0, F0, (re0, im0)) in zip(confs, first):
+            for _k in range(2):   # consecutive identical calls: the second at the latest runs the graph
+                p.set_configuration(c)
+                E, F = p.energy_and_forces()
+                assert E == E0 and np.array_equal(F, F0)
+            re, im = p.rho()
+            assert np.array_equal(re, re0) and np.array_equal(im, im0)
+
+
 def test_finite_difference(gpu):
     """TestFiniteDifference: central differences of the energy (h = 5e-5, rtol 1e-5, atol 1e-8)."""
     r = load_golden("fd_2d_skew")
