@@ -1642,15 +1642,16 @@ int cc_set_positions(cc_handle *h, int64_t N, const double *frac)
 	if (int rc = input_staging(h, (size_t)N * d))
 		return rc;
 	double *in = h->h_in;
-	// positions already in [0,1) (the usual case) are copied as they are, in the same pass that checks them; NaN
-	// fails both comparisons
-	bool unit = true;
-	for (int64_t i = 0; i < N * d; i++) {
+	// positions already in [0,1) (the usual case) are copied as they are, in the same pass that checks them (an
+	// integer flag the compiler vectorises); NaN fails both comparisons
+	long bad = 0;
+	const int64_t nv = N * d;
+	for (int64_t i = 0; i < nv; i++) {
 		const double x = frac[i];
 		in[i] = x;
-		unit &= (x >= 0.0) & (x < 1.0);
+		bad |= (long)!(x >= 0.0) | (long)!(x < 1.0);
 	}
-	if (!unit) {
+	if (bad) {
 		for (int64_t i = 0; i < N * d; i++)
 			if (!wrap_unit(frac[i], in + i)) {
 				h->upload_pending = false;
