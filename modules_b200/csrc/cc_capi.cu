@@ -2893,8 +2893,6 @@ int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opt
 	const int prec0 = o.precision;
 	// Each dimension group runs its iterations (evaluation, then its instances' L-BFGS step) on its own stream,
 	// forked from st at the start of the graph and joined back at its end; launches interleaved by iteration.
-	(void)nblk;
-	(void)maxn;
 	const int ngr = (int)b->groups.size();
 	auto iterations = [&](int prec) -> int {
 		if (ngr > 1) {

@@ -366,11 +366,8 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 		std::stable_sort(active.begin(), active.end(), [](const Slot &x, const Slot &y) { return x.d < y.d; });
 		const int A = (int)active.size();
 		std::vector<cc::LbInst> li(A);
-		int maxn = 0;
-		for (int a = 0; a < A; a++) {
+		for (int a = 0; a < A; a++)
 			li[a] = active[a].li;
-			maxn = std::max(maxn, li[a].n);
-		}
 		std::vector<cc::RhoArgs> ra;
 		std::vector<cc::ReduceArgs> rr;
 		std::vector<cc::ForceArgs> fa;
@@ -418,7 +415,6 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 		// Each group runs its iterations (energy and gradient, then its instances' L-BFGS step) on its own stream,
 		// forked from st at the start of the round and joined back at its end; the launches are issued iteration by
 		// iteration across the groups, so every stream has work queued from the start.
-		(void)maxn;
 		const int ng = (int)groups.size();
 		if (ng > 1 && cudaEventRecord(ev_fork, st) != cudaSuccess)
 			rc = sfail(CC_ERR_CUDA, "serve: event record failed");
