@@ -14,23 +14,29 @@
 // part removed by rint, so the phase carries ~1e-16 of a turn of error for any |n| (the reference forms k.r in
 // Cartesian coordinates, whose rounding grows with |k.r|).
 //
-// Per evaluation (FP64 or mixed):
-//   cc_rho_kernel    grid (rho groups x particle splits), 512 threads = one segment per thread; all warps of a block
-//                    walk the block's particles (tables staged per chunk of 32 particles, read as broadcasts).
-//                    Writes per-split partial sums of every slot.
-//   cc_reduce_kernel sums the splits of every slot in split order (8 chunks in parallel, combined in chunk order),
-//                    forms rho, u = V conj(rho) and the energy (block partials summed in block order by the last
-//                    block, which takes an atomic ticket and never waits).
-//   cc_force_kernel  grid (particle groups of 32 x segment splits), 512 threads = 32 particles (lanes) x 16 warps
-//                    striding over the split's segments unit by unit (a unit = up to 64 segments with its own tables).
-//                    Per segment: S0 = sum_r t_r, S1 = sum_r r t_r with t_r = Im(u_r z_r); the integer-index gradient
-//                    is g += S0 (prefix, start) + (0, S1). Splits are summed in split order by the last block of each
-//                    particle group. Cartesian F = (2/V) sum_e g_e b_e; dPhi/ds_e = -(2/V) 2 pi g_e.
+// Per evaluation (FP64 or mixed), every kernel 256 threads:
+//   cc_rho_kernel    grid (block groups x particle splits), thread-block clusters of up to 8 splits. Warp w owns the
+//                    32 segments of one rho group (a lane per segment); all warps walk the block's particles, whose
+//                    tables are built per chunk in shared memory. The cluster's blocks add their sums through
+//                    distributed shared memory into one partial row of every slot.
+//   cc_reduce_kernel sums the partial rows of every slot in row order (8 chunks in parallel, combined in chunk order),
+//                    forms rho, u = V conj(rho) and one energy term per block (summed in block order by the force
+//                    kernel, or by the reduce kernel's last block, which takes an atomic ticket and never waits).
+//   cc_force_kernel  grid (particle groups of 32 x segment splits): 32 particles (lanes) x 8 warps sharing the split's
+//                    segments, whose weights u are staged 128 segments at a time. Per segment: S0 = sum_r t_r,
+//                    S1 = sum_r r t_r with t_r = Im(u_r z_r); the integer-index gradient is g += S0 (prefix, start)
+//                    + (0, S1). In FP64 a warp takes a contiguous run of segments and continues the recurrence along a
+//                    lattice line for up to kForceRun segments. Splits are summed in split order by the last block of
+//                    each particle group. Cartesian F = (2/V) sum_e g_e b_e; dPhi/ds_e = -(2/V) 2 pi g_e.
+//   The kernels are chained by programmatic dependent launch: each is scheduled while its predecessor drains and
+//   waits for it (cudaGridDependencySynchronize) before reading its results.
+//   cc_mrho / cc_mreduce / cc_mforce: the same block bodies for many instances in one persistent launch each, items
+//   (instance, block) taken from a work queue.
 // Every sum has a fixed order, so results repeat bitwise.
 //
-// Mixed precision: tables are built in FP64 and rounded to FP32; seeds, recurrences and per-segment sums run in
-// FP32; per-thread rho sums are flushed to FP64 every 16 particles, per-segment force sums are added to FP64; all
-// cross-thread sums are FP64.
+// Mixed precision: tables are built in FP64 and rounded to FP32; seeds and the rotations along a segment (complex
+// products) run in FP32; per-thread rho sums are flushed to FP64 every 16 particles, per-segment force sums are added
+// to FP64; all cross-thread sums are FP64.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
