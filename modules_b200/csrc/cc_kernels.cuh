@@ -4,7 +4,8 @@
 // L = 8 modes that share every index but the last and whose last index runs start, start+1, ... (a piece of a lattice
 // line). For a particle with fractional coordinates s the phases of a segment are
 //     z_r = exp(2 pi i n_r.s) = z_0 w^r,   w = exp(2 pi i s_last),
-// so after one seed z_0 every further phase is one complex multiplication (FMA work). Seeds come from per-particle
+// so after one seed z_0 every further phase is one step of a recurrence (FMA work: the three-term recurrence in FP64,
+// a complex product in the mixed path). Seeds come from per-particle
 // PHASE TABLES built in shared memory for the block's particles: T_e(m) = exp(2 pi i m s_e) over the index range the
 // block's segments use, either in full or as coarse (stride 8) x fine (0..7) factors; each 8-entry block of a table
 // starts from an exactly reduced FP64 sincospi and continues by at most 7 FP64 complex multiplications, so table
