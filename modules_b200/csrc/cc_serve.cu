@@ -3,12 +3,14 @@
 // Requests (a stealthy CC configuration each: d, N, chi, weight type, start positions, arrival time) are minimised
 // to their ground state on one GPU. The server works in rounds:
 //   1. admit every request that has arrived, in arrival order, while a slot is free and the request's device memory
-//      fits the HBM budget (its k-set is planned on the host, its k-set arrays, phase tables, partial sums and L-BFGS
-//      state are allocated from a stream-ordered pool and stay resident until it finishes);
-//   2. run `iters_per_round` L-BFGS iterations for every admitted request at once: per iteration one multi-instance
-//      evaluation per dimension (the persistent rho / reduce / force kernels, cc_multi_launch.h) and one launch each of
-//      the batched L-BFGS kernels (cc_lbfgs.cuh);
-//   3. retire finished requests (time-to-ground-state = completion - arrival) and free their memory.
+//      fits the HBM budget (its k-set is planned on the host, its k-set arrays, partial sums and L-BFGS state are
+//      allocated from the server's own stream-ordered pool, which holds the budget, and stay resident until it
+//      finishes);
+//   2. run `iters_per_round` L-BFGS iterations for every admitted request at once: each dimension group on its own
+//      stream, per iteration one multi-instance evaluation (the persistent rho / reduce / force kernels,
+//      cc_multi_launch.h) and one launch each of the batched L-BFGS kernels (cc_lbfgs.cuh) for its requests;
+//   3. read every request's status (one gather kernel, one copy), retire finished requests (time-to-ground-state =
+//      completion - arrival) and free their memory.
 // Requests that arrive while others are on the GPU join at the next round, so their work overlaps; an instance's
 // iterates do not depend on the rest of the batch (every sum has a fixed per-instance order), so a request's result
 // is the same alone and in the mix.
