@@ -132,9 +132,10 @@ int cc_minimize(cc_handle *h, int64_t N, double *frac, const cc_lbfgs_opts *opts
 
 /* --- batches of independent configurations (no counterpart in the reference, which evaluates one at a time) ---
  * A batch holds `count` instances, each an existing handle (its cell, constraint set, Shift) with a fixed particle
- * count N[i]. One evaluation of the batch is one cooperative kernel launch per dimension present (work items of all
- * instances share the persistent grid); a batched minimisation runs every instance's L-BFGS at once, and instances
- * that have finished are skipped item by item. The handles must outlive the batch. */
+ * count N[i]. One evaluation of the batch is, per dimension present, one persistent launch of each of the rho, reduce
+ * and force kernels (work items of all instances share the grid), the dimensions on parallel streams; a batched
+ * minimisation runs every instance's L-BFGS at once, and instances that have finished are skipped item by item. The
+ * handles must outlive the batch. */
 typedef struct cc_batch cc_batch;
 int cc_batch_create(int count, cc_handle *const *handles, const int64_t *N, cc_batch **out);
 int cc_batch_destroy(cc_batch *b);
@@ -147,8 +148,9 @@ int cc_batch_eval_device(cc_batch *b, int precision, void *stream);
 /* Minimise every instance from its bound positions; frac[i] (host) receives the results, results[i] the outcomes. */
 int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opts, cc_lbfgs_result *results);
 /* Autotuner of the batch's tile shapes: times `reps` FP64 evaluations of the bound positions for every candidate
- * (particles per rho block 32 / 64 / 128 / 256 / 512 x segments per force block 32 / 64 / 128 / 256) with CUDA events and keeps
- * the fastest for the batch's later evaluations and minimisations (default before tuning: 64 x 64). The chosen shape
+ * (particles per rho block 32 / 64 / 128 / 256 / 512 / 1024 x segments per force block 32 / 64 / 128 / 256 / 512 /
+ * 1024) with CUDA events and keeps the fastest for the batch's later evaluations and minimisations (default before
+ * tuning: 64 x 64). The chosen shape
  * is returned in *per_split and *segs_per_split (either may be NULL). Results of different shapes agree to rounding;
  * with one shape every instance's result is independent of the rest of the batch. */
 int cc_batch_autotune(cc_batch *b, int reps, int *per_split, int *segs_per_split);

@@ -409,7 +409,8 @@ class CCPotential:
 
 
 class CCBatch:
-    """Many independent configurations evaluated (and minimised) together: one cooperative launch per dimension."""
+    """Many independent configurations evaluated (and minimised) together: per dimension, one persistent launch of
+    each multi-instance kernel (rho, reduce, force), the dimensions on parallel streams."""
 
     def __init__(self, pots, N):
         self._lib = load_library()
