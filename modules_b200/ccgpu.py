@@ -217,6 +217,8 @@ class CCMulti:
         _check(self._lib.cc_multi_create(d, _ptr(basis), S, _ptr(M), mp, vp, u0, e0, ctypes.byref(h)))
         self._h = h
         self.N = None
+        self.basis = basis
+        self.nspecies = S
 
     def __del__(self):
         if getattr(self, "_h", None):
@@ -230,6 +232,15 @@ class CCMulti:
         _check(self._lib.cc_multi_set_configuration(self._h, len(frac), _ptr(frac), _ptr(sp),
                                                     None if rad is None else _ptr(rad)))
         self.N = len(frac)
+
+    def set_snapshot(self, snapshot):
+        """Bind an MSPB snapshot (modules_b200.mspb): its relative coordinates, species labels and radii. The
+        snapshot's cell must be the potential's (bitwise) and its labels must name the potential's species."""
+        if snapshot.d != self.d or not np.array_equal(snapshot.basis, self.basis):
+            raise ValueError("the snapshot's cell is not the potential's")
+        if snapshot.N and int(snapshot.species.max()) >= self.nspecies:
+            raise ValueError("the snapshot has species labels beyond the potential's species")
+        self.set_configuration(snapshot.rel, snapshot.species.astype(np.int32), snapshot.radii)
 
     def energy_and_forces(self, forces=True):
         E = _d()

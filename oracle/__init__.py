@@ -243,3 +243,71 @@ def ref_multi_eval(d, basis, kcarts, Vs, u0, e0, frac, species, radii=None):
     if rc != 0:
         raise ValueError("the reference's MultiStealthyPotential threw")
     return E.value, F[:len(frac)]
+
+
+def _mspb_lib():
+    lib = ref_lib()
+    if not getattr(lib, "_mspb_set", False):
+        c = ctypes.c_char_p
+        lib.ccref_mspb_write.argtypes = [c, ctypes.c_int, _l, ctypes.c_ulonglong, _vp, _vp, _vp, _vp, _vp, _vp,
+                                         ctypes.c_int]
+        lib.ccref_mspb_read.argtypes = [c, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(_l),
+                                        ctypes.POINTER(ctypes.c_ulonglong), _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int]
+        lib.ccref_mspbpack_import.argtypes = [c, c, _vp, ctypes.c_int]
+        lib.ccref_mspbpack_count.argtypes = [c, ctypes.POINTER(_l), _vp, ctypes.c_int]
+        lib.ccref_mspbpack_export.argtypes = [c, _l, c, _vp, ctypes.c_int]
+        lib._mspb_set = True
+    return lib
+
+
+class RefMSPBError(ValueError):
+    """The reference's MSPB code threw (its message)."""
+
+
+def _mspb_call(fn, *args):
+    err = ctypes.create_string_buffer(512)
+    if fn(*args, err, 512) != 0:
+        raise RefMSPBError(err.value.decode())
+
+
+def ref_mspb_write(path, basis, ids, species, rel, radii, species_count):
+    """The reference's MSPBSnapshot::Write of one snapshot to `path`."""
+    basis = np.ascontiguousarray(basis, np.float64)
+    d = basis.shape[0]
+    rel = np.ascontiguousarray(rel, np.float64).reshape(-1, d)
+    ids = np.ascontiguousarray(ids, np.uint64)
+    species = np.ascontiguousarray(species, np.uint32)
+    radii = np.ascontiguousarray(radii, np.float64)
+    _mspb_call(_mspb_lib().ccref_mspb_write, str(path).encode(), d, len(rel), int(species_count), _p(basis),
+               _p(ids), _p(species), _p(rel), _p(radii))
+
+
+def ref_mspb_read(path):
+    """The reference's MSPBSnapshot::Read of one file: dict(basis, ids, species, rel, radii, species_count)."""
+    lib = _mspb_lib()
+    d, n, ns = ctypes.c_int(), _l(), ctypes.c_ulonglong()
+    _mspb_call(lib.ccref_mspb_read, str(path).encode(), ctypes.byref(d), ctypes.byref(n), ctypes.byref(ns),
+               None, None, None, None, None)
+    D, N = d.value, n.value
+    basis, ids = np.zeros((D, D)), np.zeros(N, np.uint64)
+    species, rel, radii = np.zeros(N, np.uint32), np.zeros((N, D)), np.zeros(N)
+    _mspb_call(lib.ccref_mspb_read, str(path).encode(), ctypes.byref(d), ctypes.byref(n), ctypes.byref(ns),
+               _p(basis), _p(ids), _p(species), _p(rel), _p(radii))
+    return dict(basis=basis, ids=ids, species=species, rel=rel, radii=radii, species_count=ns.value)
+
+
+def ref_mspbpack_import(prefix, path):
+    """MSPB_Pack(prefix).ImportFile(path) of the reference."""
+    _mspb_call(_mspb_lib().ccref_mspbpack_import, str(prefix).encode(), str(path).encode())
+
+
+def ref_mspbpack_count(prefix):
+    """MSPB_Pack(prefix).NumConfig() of the reference."""
+    n = _l()
+    _mspb_call(_mspb_lib().ccref_mspbpack_count, str(prefix).encode(), ctypes.byref(n))
+    return n.value
+
+
+def ref_mspbpack_export(prefix, index, path):
+    """MSPB_Pack(prefix).ExportFile(index, path) of the reference."""
+    _mspb_call(_mspb_lib().ccref_mspbpack_export, str(prefix).encode(), int(index), str(path).encode())

@@ -50,3 +50,26 @@ def test_multi_arguments(gpu):
     pot.set_configuration(frac, np.zeros(10, np.int32))
     E, F = pot.energy_and_forces()
     assert np.isfinite(E) and F.shape == (10, 2)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", NAMES[:3])
+def test_multi_from_mspb_snapshot(gpu, name, tmp_path):
+    """A configuration stored as an MSPB snapshot (the reference optimiser's export format), read back and bound with
+    CCMulti.set_snapshot, evaluates like the configuration bound directly and within 1e-10 of the reference."""
+    from modules_b200 import mspb
+    direct = _build(gpu, name)
+    E0, F0 = direct.energy_and_forces()
+    d = int(G[name + "__d"])
+    n = len(G[name + "__frac"])
+    radii = G[name + "__radii"] if len(G[name + "__radii"]) else np.full(n, 0.5)
+    snap = mspb.Snapshot.create(G[name + "__basis"].reshape(d, d), G[name + "__frac"], species=G[name + "__species"],
+                                radii=radii, ids=np.arange(n)[::-1] + 100, species_count=len(G[name + "__M"]))
+    path = tmp_path / "conf.mspb"
+    mspb.write(path, snap)
+    direct.set_snapshot(mspb.read(path))
+    E, F = direct.energy_and_forces()
+    assert E == E0 and np.array_equal(F, F0)
+    Er, Fr = float(G[name + "__E"]), G[name + "__F"]
+    assert abs(E - Er) <= 1e-10 * abs(Er)
+    assert np.abs(F - Fr).max() <= 1e-10 * max(1.0, np.abs(Fr).max())
