@@ -70,6 +70,14 @@ int cc_create(int d, const double *basis, int64_t M, const int32_t *modes, const
 int cc_create_cartesian(int d, const double *basis, int64_t M, const double *k, const double *V, double shift,
                         cc_handle **out);
 
+/* The S2 form, the reference's ShiftedCCPotential_S2 (potential/CollectiveCoordinatePotential.h:1642-1749, constraints
+ * added by its AddConstraint(k, {V, S0})): E = sum_m V_m (|rho(k_m)|^2 / N - S0_m)^2 + shift, with no volume factor,
+ * F_i = (4 / N) sum_m V_m (|rho|^2 / N - S0_m) Im(conj(rho) e^{i k.r_i}) k_m. Arguments as cc_create plus S0 (M
+ * targets); modes must be distinct (CC_ERR_ARG otherwise). Evaluated in FP64 on the split rho / reduce / force path
+ * whatever the precision asked; cc_set_path(CC_PATH_NUFFT), single-particle moves and batches refuse it (CC_ERR_ARG). */
+int cc_create_s2(int d, const double *basis, int64_t M, const int32_t *modes, const double *V, const double *S0,
+                 double shift, cc_handle **out);
+
 int cc_destroy(cc_handle *h);
 
 /* Number of constraints, dimension, volume and the integer modes (M x d) of a handle. */

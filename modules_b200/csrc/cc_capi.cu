@@ -233,6 +233,8 @@ struct cc_handle {
 	size_t partialF_cap = 0;
 	std::vector<std::pair<int, int *> > kstarts;   // even segment splits per count
 	bool use_fused = false;         // cc_set_path
+	// S2 form (cc_create_s2): per-slot targets S0, E = sum V (|rho|^2 / N - S0)^2 + shift; split path only
+	double *d_slotS0 = nullptr;
 	bool use_nufft = false;         // cc_set_path(CC_PATH_NUFFT)
 	bool auto_path = true;          // CC_PATH_AUTO (default): the NUFFT path where its estimated time is lower
 	double nu_grid_est = -1.0;      // fine-grid points the NUFFT path would use (computed once)
@@ -765,6 +767,11 @@ int run_rho(cc_handle *h, DevKSet &k, int64_t N, const double *d_frac, double *d
 	r.E_out = d_E;
 	r.finalize = energy_in_force ? 0 : 1;
 	r.skip = h->d_skip;
+	if (h->d_slotS0 && &k == &h->main) {
+		r.slotS0 = h->d_slotS0;
+		r.npart = (double)N;
+		r.inv_vol = 1.0;
+	}
 	CC_CUDA(launch_pdl(cc::cc_reduce_kernel, dim3((p.nslot + 31) / 32), dim3(cc::kRedThreads), 0, st, r));
 	if (want_rho_mode && !p.mode_slot.empty()) {
 		const int M = (int)p.mode_slot.size();
@@ -819,6 +826,10 @@ int run_force(cc_handle *h, int64_t N, const double *d_frac, double *d_F, double
 	a.shift = h->shift;
 	a.E_out = d_E;
 	a.skip = h->d_skip;
+	if (h->d_slotS0) {   // F = (4 / N) sum_k Im(u z) k with u = V dS conj(rho)
+		a.fscale = 4.0 / (double)N;
+		a.inv_vol = 1.0;
+	}
 	return launch_force(h->d, a, mixed, N, f->host.max_row, st);
 }
 
@@ -829,7 +840,7 @@ constexpr size_t kFusedTabCap = 64u << 20;   // bytes per table layout: beyond t
 
 bool fused_eligible(const cc_handle *h, int64_t N, bool mixed)
 {
-	if (N <= 0 || h->main.plan.nslot == 0)
+	if (N <= 0 || h->main.plan.nslot == 0 || h->d_slotS0)
 		return false;
 	const size_t esz = mixed ? sizeof(float2) : sizeof(double2);
 	const size_t Npad = (size_t)(N + 31) / 32 * 32;
@@ -1321,7 +1332,7 @@ cudaEvent_t next_event(cc_handle *h)
 // 9.3; 3D N=2000 M=2724 0.13 against 0.034.
 bool nufft_preferred(cc_handle *h, int64_t N)
 {
-	if (h->main.plan.nslot == 0 || N < 1024)
+	if (h->main.plan.nslot == 0 || N < 1024 || h->d_slotS0)
 		return false;
 	const int d = h->d;
 	if (h->nu_grid_est < 0) {
@@ -1348,7 +1359,7 @@ bool nufft_preferred(cc_handle *h, int64_t N)
 int eval_device(cc_handle *h, int64_t N, const double *d_frac, double *d_E, double *d_F, double *d_gfrac,
                 bool want_rho_mode, int precision, cudaStream_t st)
 {
-	const bool mixed = precision == CC_PREC_MIXED;
+	const bool mixed = precision == CC_PREC_MIXED && !h->d_slotS0;   // the S2 form evaluates in FP64
 	const Launch l = choose_launch(h->main.plan, N, mixed);
 	cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
 	if (h->timing && h->ev_used + 4 <= 4 * 100000) {
@@ -1554,6 +1565,36 @@ int cc_create_cartesian(int d, const double *basis, int64_t M, const double *k, 
 	return create_common(d, basis, M, modes.data(), V, shift, out);
 }
 
+int cc_create_s2(int d, const double *basis, int64_t M, const int32_t *modes, const double *V, const double *S0,
+                 double shift, cc_handle **out)
+{
+	if (!out)
+		return fail(CC_ERR_ARG, "out is null");
+	*out = nullptr;
+	if (M > 0 && !S0)
+		return fail(CC_ERR_ARG, "null S0");
+	for (int64_t m = 0; m < M; m++)
+		if (!std::isfinite(S0[m]))
+			return fail(CC_ERR_ARG, "non-finite target S0");
+	cc_handle *h = nullptr;
+	if (int rc = create_common(d, basis, M, modes, V, shift, &h))
+		return rc;
+	const cc::Plan &p = h->main.plan;
+	if (p.unique_modes != M) {
+		cc_destroy(h);
+		return fail(CC_ERR_ARG, "S2 constraints need distinct modes");
+	}
+	std::vector<double> slotS0((size_t)p.nslot, 0.0);
+	for (int64_t m = 0; m < M; m++)
+		slotS0[(size_t)p.mode_slot[(size_t)m]] = S0[m];
+	if (int rc = upload(&h->d_slotS0, slotS0)) {
+		cc_destroy(h);
+		return rc;
+	}
+	*out = h;
+	return CC_OK;
+}
+
 int cc_destroy(cc_handle *h)
 {
 	if (!h)
@@ -1571,6 +1612,7 @@ int cc_destroy(cc_handle *h)
 	cudaFree(h->d_partialG);
 	cudaFree(h->d_fcounters);
 	cudaFree(h->d_E);
+	cudaFree(h->d_slotS0);
 	cudaFreeHost(h->h_pin);
 	cudaFreeHost(h->h_in);
 	if (h->ev_in)
@@ -1867,6 +1909,8 @@ int cc_mc_try_move(cc_handle *h, const double *s_prev, const double *s_after, do
 		return rc;
 	if (!s_prev || !s_after || !dE)
 		return fail(CC_ERR_ARG, "null move arguments");
+	if (h->d_slotS0)
+		return fail(CC_ERR_ARG, "single-particle moves evaluate the plain collective-coordinate form only");
 	if (h->N < 0)
 		return fail(CC_ERR_STATE, "positions not set");
 	const int M = (int)h->V.size(), d = h->d;
@@ -1930,6 +1974,8 @@ int cc_set_path(cc_handle *h, int path)
 		return rc;
 	if (path != CC_PATH_SPLIT && path != CC_PATH_FUSED && path != CC_PATH_NUFFT && path != CC_PATH_AUTO)
 		return fail(CC_ERR_ARG, "path must be CC_PATH_SPLIT, CC_PATH_FUSED, CC_PATH_NUFFT or CC_PATH_AUTO");
+	if (h->d_slotS0 && path == CC_PATH_NUFFT)
+		return fail(CC_ERR_ARG, "the NUFFT path evaluates the plain collective-coordinate form only");
 	h->use_fused = path == CC_PATH_FUSED;
 	h->use_nufft = path == CC_PATH_NUFFT;
 	h->auto_path = path == CC_PATH_AUTO;
@@ -2070,6 +2116,8 @@ int cc_minimize(cc_handle *h, int64_t N, double *frac, const cc_lbfgs_opts *opts
 		return fail(CC_ERR_ARG, "invalid minimisation arguments");
 	if ((int64_t)N * h->d > (1 << 30))
 		return fail(CC_ERR_ARG, "too many variables");
+	if (h->d_slotS0)   // the S2 form evaluates in FP64 only
+		o.precision = CC_PREC_FP64;
 	if (o.precision == CC_PREC_SCHEDULE && h->main.plan.nslot > 0) {
 		// the precision schedule is per instance: run it as a batch of one (kept by the handle for this N)
 		int rc2 = CC_OK;
@@ -2534,9 +2582,12 @@ int cc_batch_create(int count, cc_handle *const *handles, const int64_t *N, cc_b
 	if (!out || count < 1 || !handles || !N)
 		return fail(CC_ERR_ARG, "invalid batch arguments");
 	*out = nullptr;
-	for (int i = 0; i < count; i++)
+	for (int i = 0; i < count; i++) {
 		if (!handles[i] || N[i] < 1 || N[i] > (1 << 26) || handles[i]->main.plan.nslot == 0)
 			return fail(CC_ERR_ARG, "every instance needs a handle with constraints and 1 <= N <= 2^26");
+		if (handles[i]->d_slotS0)
+			return fail(CC_ERR_ARG, "batches hold the plain collective-coordinate form only");
+	}
 	cc_batch *b = new cc_batch();
 	b->h.assign(handles, handles + count);
 	b->N.assign(N, N + count);

@@ -552,6 +552,10 @@ struct ReduceArgs {
 	const int *skip;
 	const int *stage;
 	int want_stage;
+	// S2 form (the reference's ShiftedCCPotential_S2) when not null: targets S0 per slot, e = V (|rho|^2 / N - S0)^2,
+	// u = V (|rho|^2 / N - S0) conj(rho); npart = N
+	const double *slotS0;
+	double npart;
 };
 
 constexpr int kRedThreads = 256;   // 32 slots x 8 split chunks
@@ -605,9 +609,16 @@ __device__ __forceinline__ void reduce_body(const ReduceArgs &a, const int chunk
 		if (slot < a.nslot) {
 			rho.x += a.rho_offset;
 			a.rho_slot[slot] = rho;
-			const double v = a.slotV[slot];
+			double v = a.slotV[slot];
+			const double r2 = rho.x * rho.x + rho.y * rho.y;
+			if (a.slotS0) {
+				const double ds = r2 / a.npart - a.slotS0[slot];
+				v *= ds;
+				e = v * ds;
+			} else {
+				e = v * r2;
+			}
 			a.u_slot[slot] = make_double2(v * rho.x, -v * rho.y);
-			e = v * (rho.x * rho.x + rho.y * rho.y);
 		}
 #pragma unroll
 		for (int o = 16; o > 0; o >>= 1)

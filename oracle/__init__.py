@@ -48,6 +48,8 @@ def ref_lib():
         lib = ctypes.CDLL(REF_LIB)
         lib.ccref_create.restype = _vp
         lib.ccref_create.argtypes = [ctypes.c_int, _vp, _l, _vp, _vp, _vp, _d, ctypes.c_int]
+        lib.ccref_create_s2.restype = _vp
+        lib.ccref_create_s2.argtypes = [ctypes.c_int, _vp, _l, _vp, _vp, _vp, _d, ctypes.c_int]
         lib.ccref_destroy.argtypes = [_vp]
         lib.ccref_kcart.argtypes = [_vp, _vp]
         lib.ccref_volume.restype = _d
@@ -99,9 +101,10 @@ def lattice_k(basis, modes):
 
 
 class Ref:
-    """The reference's ShiftedCCPotential (Direct backend) over a cell; modes or Cartesian k."""
+    """The reference's ShiftedCCPotential (Direct backend) over a cell; modes or Cartesian k. With S0 (integer modes)
+    the reference's ShiftedCCPotential_S2 instead (potential/CollectiveCoordinatePotential.h:1642-1749)."""
 
-    def __init__(self, d, basis, V, modes=None, kcart=None, shift=0.0, nthreads=None):
+    def __init__(self, d, basis, V, modes=None, kcart=None, shift=0.0, nthreads=None, S0=None):
         self.lib = ref_lib()
         self.d = d
         self.basis = np.ascontiguousarray(basis, np.float64).reshape(d, d)
@@ -110,7 +113,11 @@ class Ref:
         m = np.ascontiguousarray(modes, np.int32) if modes is not None else None
         k = np.ascontiguousarray(kcart, np.float64) if kcart is not None else None
         nt = nthreads or os.cpu_count() or 1
-        self.h = self.lib.ccref_create(d, _p(self.basis), self.M, _p(m), _p(k), _p(V), shift, nt)
+        if S0 is not None:
+            S0 = np.ascontiguousarray(S0, np.float64)
+            self.h = self.lib.ccref_create_s2(d, _p(self.basis), self.M, _p(m), _p(V), _p(S0), shift, nt)
+        else:
+            self.h = self.lib.ccref_create(d, _p(self.basis), self.M, _p(m), _p(k), _p(V), shift, nt)
         if not self.h:
             raise ValueError("ccref_create failed")
         self.N = 0

@@ -140,6 +140,32 @@ void *ccref_create(int d, const double *basis, long M, const int32_t *modes, con
 	return h;
 }
 
+// The reference's ShiftedCCPotential_S2 (potential/CollectiveCoordinatePotential.h:1642-1749): E = sum_k V (|rho|^2 / N - S0)^2
+// + Shift, constraints added through its AddConstraint(k, {V, S0}); evaluated with ccref_set_positions / ccref_eval.
+void *ccref_create_s2(int d, const double *basis, long M, const int32_t *modes, const double *V, const double *S0,
+                      double shift, int nthreads)
+{
+	if (d < 1 || d > 4 || M < 0)
+		return nullptr;
+	RefHandle *h = new RefHandle();
+	h->d = d;
+	for (int i = 0; i < d; i++)
+		h->basis.push_back(MakeVec(d, basis + d * i));
+	h->config = EmptyConfig(h);
+	ShiftedCCPotential_S2 *s2 = new ShiftedCCPotential_S2(d);
+	h->pot.reset(s2);
+	h->nthreads = nthreads < 1 ? 1 : nthreads;
+	h->pot->ParallelNumThread = h->nthreads;
+	h->pot->Shift = shift;
+	for (long m = 0; m < M; m++) {
+		GeometryVector k(d);
+		for (int e = 0; e < d; e++)
+			k.AddFrom(static_cast<double>(modes[m * d + e]) * h->config->GetReciprocalBasisVector(e));
+		s2->AddConstraint(k, std::vector<double>{V[m], S0[m]});
+	}
+	return h;
+}
+
 void ccref_destroy(void *p) { delete static_cast<RefHandle *>(p); }
 
 // Cartesian k of every constraint (M x d).

@@ -1,0 +1,143 @@
+"""The S2 form (cc_create_s2 / CCPotential(S0=...)) against the reference's ShiftedCCPotential_S2
+(potential/CollectiveCoordinatePotential.h:1642-1749): E = sum_k V (|rho|^2 / N - S0)^2 + Shift and
+F_i = -(4 / N) sum_k V dS (Im rho cos k.r - Re rho sin k.r) k.
+
+The CPU tests pin a numpy restatement of those formulas to the compiled reference; the GPU tests compare the sm_100a
+path with the reference at 1e-10 of the rounding scales below (rho ~ N; an error of eps in rho moves S by about
+2 |rho| eps / N, so the energy scale is sum |V| (|dS| + 1)^2 and the force scale (4 / N) sum |V| (|dS| + 1)(|rho| + 1)|k|).
+"""
+import numpy as np
+import pytest
+
+import oracle
+
+needs_ref = pytest.mark.skipif(not oracle.ref_available(), reason="reference oracle not built")
+RTOL = 1e-10
+
+
+def skew_basis(d):
+    b = np.eye(d) * 7.0
+    if d >= 2:
+        b[1, 0] = 1.75
+    if d == 3:
+        b[2, 1] = -0.9
+        b[2, 0] = 0.4
+    return b
+
+
+def case(d, N, kmax, seed):
+    """A near-lattice configuration (so that some S(k) are small and the targets matter), distinct modes with both
+    k and -k present for some of them, random weights and targets."""
+    rng = np.random.default_rng(seed)
+    side = int(np.ceil(N ** (1.0 / d)))
+    grid = np.stack(np.meshgrid(*[np.arange(side)] * d, indexing="ij"), -1).reshape(-1, d)[:N] / side
+    frac = (grid + rng.normal(0, 0.08 / side, grid.shape)) % 1.0
+    r = np.arange(-kmax, kmax + 1)
+    modes = np.stack(np.meshgrid(*[r] * d, indexing="ij"), -1).reshape(-1, d)
+    modes = modes[np.any(modes != 0, axis=1)]
+    modes = modes[rng.random(len(modes)) < 0.6]
+    rng.shuffle(modes)
+    V = rng.uniform(0.2, 2.0, len(modes))
+    S0 = rng.uniform(0.0, 1.5, len(modes))
+    return skew_basis(d), np.ascontiguousarray(frac), modes.astype(np.int32), V, S0
+
+
+def restatement(basis, frac, modes, V, S0, shift):
+    """The reference's S2 Energy and Force(i) in numpy."""
+    N = len(frac)
+    k = oracle.lattice_k(basis, modes)
+    r = frac @ basis
+    ph = r @ k.T
+    c, s = np.cos(ph), np.sin(ph)
+    re, im = c.sum(0), s.sum(0)
+    dS = (re * re + im * im) / N - S0
+    E = float((V * dS * dS).sum()) + shift
+    coef = (4.0 / N) * V * dS
+    F = -((im * c - re * s) * coef) @ k
+    return E, F, re, im, dS, k
+
+
+def tol_scales(V, dS, re, im, k, N):
+    kn = np.sqrt((k * k).sum(1))
+    rho = np.sqrt(re * re + im * im)
+    return (float((np.abs(V) * (np.abs(dS) + 1) ** 2).sum()),
+            float((4.0 / N) * (np.abs(V) * (np.abs(dS) + 1) * (rho + 1) * kn).sum()))
+
+
+@needs_ref
+@pytest.mark.parametrize("d,N,kmax", [(1, 40, 25), (2, 300, 6), (3, 200, 3)])
+def test_restatement_matches_reference(d, N, kmax):
+    basis, frac, modes, V, S0 = case(d, N, kmax, 11 + d)
+    ref = oracle.Ref(d, basis, V, modes=modes, shift=0.3, S0=S0)
+    ref.set_positions(frac)
+    E, F, re, im = ref.eval()
+    E2, F2, re2, im2, dS, k = restatement(basis, frac, modes, V, S0, 0.3)
+    sE, sF = tol_scales(V, dS, re2, im2, k, N)
+    assert abs(E - E2) <= 1e-12 * sE
+    assert np.abs(F - F2).max() <= 1e-12 * sF
+    assert np.abs(re - re2).max() <= 1e-12 * N and np.abs(im - im2).max() <= 1e-12 * N
+    for i in (0, N // 2, N - 1):
+        assert np.abs(ref.force_one(i) - F2[i]).max() <= 1e-12 * sF
+
+
+@pytest.mark.gpu
+@needs_ref
+@pytest.mark.parametrize("d,N,kmax", [(1, 64, 40), (2, 1000, 9), (3, 2000, 5), (2, 20000, 12)])
+def test_gpu_matches_reference(gpu, d, N, kmax):
+    basis, frac, modes, V, S0 = case(d, N, kmax, 100 + d + N)
+    ref = oracle.Ref(d, basis, V, modes=modes, shift=-0.25, S0=S0)
+    ref.set_positions(frac)
+    Eref, Fref, re, im = ref.eval()
+    k = oracle.lattice_k(basis, modes)
+    dS = (re * re + im * im) / N - S0
+    sE, sF = tol_scales(V, dS, re, im, k, N)
+    p = gpu.CCPotential(d, basis, modes, V, -0.25, S0=S0)
+    p.set_configuration(frac)
+    for _ in range(3):   # direct, then captured evaluations of the same key
+        E, F = p.energy_and_forces()
+        assert abs(E - Eref) <= RTOL * sE, (E, Eref)
+        assert np.abs(F - Fref).max() <= RTOL * sF
+    assert p.energy() == E
+    gre, gim = p.rho()
+    assert np.abs(gre - re).max() <= RTOL * N and np.abs(gim - im).max() <= RTOL * N
+    assert np.array_equal(p.force(N // 3), F[N // 3])
+
+
+@pytest.mark.gpu
+def test_gpu_fp64_only_and_refusals(gpu):
+    basis, frac, modes, V, S0 = case(2, 3000, 8, 5)
+    p = gpu.CCPotential(2, basis, modes, V, 0.0, S0=S0)
+    p.set_configuration(frac)
+    E, F = p.energy_and_forces()
+    Em, Fm = p.energy_and_forces(precision=gpu.PREC_MIXED)   # evaluated in FP64 whatever the precision
+    assert Em == E and np.array_equal(Fm, F)
+    p.set_path(gpu.PATH_FUSED)                                  # the fused kernel holds the plain form: split path
+    Ef, Ff = p.energy_and_forces()
+    assert Ef == E and np.array_equal(Ff, F)
+    with pytest.raises(gpu.CCError):
+        p.set_path(gpu.PATH_NUFFT)
+    with pytest.raises(gpu.CCError):
+        p.try_move(frac[0], (frac[0] + 0.01) % 1.0)
+    with pytest.raises(gpu.CCError):
+        gpu.CCBatch([p], [len(frac)])
+    with pytest.raises(gpu.CCError):
+        gpu.CCPotential(2, basis, np.vstack([modes, modes[:1]]), np.append(V, 1.0), 0.0, S0=np.append(S0, 0.5))
+    with pytest.raises(ValueError):
+        gpu.CCPotential(2, basis, modes, V, 0.0, S0=S0[:-1])
+
+
+@pytest.mark.gpu
+def test_gpu_minimize_s2(gpu):
+    """Stealthy targets (S0 = 0) at a small constrained fraction: the device L-BFGS drives E to its ground state 0,
+    and the reported energy is the potential's at the returned positions."""
+    basis, frac, modes, V, _ = case(2, 400, 3, 9)
+    rng = np.random.default_rng(3)
+    start = rng.random((400, 2))
+    p = gpu.CCPotential(2, basis, modes, V, 0.0, S0=np.zeros(len(V)))
+    p.set_configuration(start)
+    E0 = p.energy()
+    x, E, evals, iters, status = p.minimize(start, stopval=1e-20, max_evals=20000,
+                                            precision=gpu.PREC_SCHEDULE)
+    assert evals > 0 and E < 1e-6 * E0
+    p.set_configuration(x)
+    assert abs(p.energy() - E) <= 1e-12 * E0
