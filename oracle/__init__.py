@@ -50,6 +50,11 @@ def ref_lib():
         lib.ccref_create.argtypes = [ctypes.c_int, _vp, _l, _vp, _vp, _vp, _d, ctypes.c_int]
         lib.ccref_create_s2.restype = _vp
         lib.ccref_create_s2.argtypes = [ctypes.c_int, _vp, _l, _vp, _vp, _vp, _d, ctypes.c_int]
+        lib.ccref_create_varbox.restype = _vp
+        lib.ccref_create_varbox.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _d, _d, ctypes.c_int]
+        lib.ccref_varbox_state.argtypes = [_vp, _vp, _vp, _vp]
+        lib.ccref_constraints.argtypes = [_vp, _vp, _vp]
+        lib.ccref_varbox_weights.argtypes = [_vp, _l, _vp, _vp, _vp]
         lib.ccref_destroy.argtypes = [_vp]
         lib.ccref_kcart.argtypes = [_vp, _vp]
         lib.ccref_volume.restype = _d
@@ -169,6 +174,53 @@ class Ref:
         ev = _l()
         E = self.lib.ccref_minimize(self.h, len(x), _p(x), emin, maxeval, history, fast, ctypes.byref(ev))
         return E, x, ev.value
+
+
+VARBOX_KINDS = ["K2Potential", "KM3Potential", "K2K2Potential", "K2K2Potential_noV0", "KM3K2Potential_noV0",
+                "KM2K2Potential", "KM3K2Potential", "KM4K2Potential", "KM3KM2Potential", "KM3KMLogPotential",
+                "KM2KnPotential", "KM3KnPotential", "KM4KnPotential", "KM2KlcPotential", "KM3KlcPotential",
+                "KM4KlcPotential"]
+
+
+class RefVarBox(Ref):
+    """One of the reference's named variable-cell potentials (potential/CCPotential_Kernels.h) at a fixed cell; its
+    constraints and shift are generated by its own SetConfiguration when positions are set. eval() is for the plain
+    kinds only: the S2 kinds leave S0 empty (state() reports its length), so their Energy would read past it."""
+
+    def __init__(self, name, d, basis, rK=1.0, n=0.0, nthreads=None):
+        self.lib = ref_lib()
+        self.d = d
+        self.basis = np.ascontiguousarray(basis, np.float64).reshape(d, d)
+        nt = nthreads or os.cpu_count() or 1
+        self.h = self.lib.ccref_create_varbox(VARBOX_KINDS.index(name), d, _p(self.basis), rK, n, nt)
+        if not self.h:
+            raise ValueError("ccref_create_varbox failed")
+        self.M = 0
+        self.N = 0
+
+    def set_positions(self, frac):
+        super().set_positions(frac)
+        self.M = self.state()[0]
+
+    def state(self):
+        M, shift, nS0 = _l(), _d(), _l()
+        self.lib.ccref_varbox_state(self.h, ctypes.byref(M), ctypes.byref(shift), ctypes.byref(nS0))
+        return M.value, shift.value, nS0.value
+
+    def constraints(self):
+        M = self.state()[0]
+        k = np.zeros((max(M, 1), self.d))
+        V = np.zeros(max(M, 1))
+        self.lib.ccref_constraints(self.h, _p(k), _p(V))
+        return k[:M], V[:M]
+
+    def weights(self, kcart):
+        """The class's own tildeV(k) and S0(k) (NaN for the plain kinds) at Cartesian wavevectors."""
+        kcart = np.ascontiguousarray(kcart, np.float64).reshape(-1, self.d)
+        V = np.zeros(max(len(kcart), 1))
+        S0 = np.zeros(max(len(kcart), 1))
+        self.lib.ccref_varbox_weights(self.h, len(kcart), _p(kcart), _p(V), _p(S0))
+        return V[:len(kcart)], S0[:len(kcart)]
 
 
 def ref_kset(d, basis, N, chi, type_=0, cap=400000):

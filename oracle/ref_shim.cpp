@@ -17,12 +17,14 @@
 //   - the Type 0-3 k-set of GeneratePotential (apps/CollectiveCoordinateCLI/CollectiveCoordinateCLI.cpp:180-265);
 //   - StructureFactor(config, k) (pairstat/StructureFactor.cpp:56-65).
 #include "CollectiveCoordinatePotential.h"
+#include "CCPotential_Kernels.h"
 #include "LuksanPLIS.h"
 
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <functional>
 #include <limits>
 #include <memory>
 #include <vector>
@@ -36,6 +38,27 @@ struct RefHandle {
 	std::unique_ptr<ShiftedCCPotential> pot;
 	std::unique_ptr<ShiftedCCPotential_ForMC> mc;   // ccref_mc_trymove's MC object, created at its first call
 	int nthreads;
+	// varBox potentials: the reference's own tildeV(k) and S0(k) at a wavevector (S0 NaN for the plain kinds)
+	std::function<void(const GeometryVector &, double *, double *)> weights;
+	ShiftedCCPotential_S2 *s2 = nullptr;
+};
+
+// Access to the protected weight and target functions of a varBox potential class.
+template <class P> struct ProbeV : P {
+	template <class... A> ProbeV(A... a) : P(a...) {}
+	void eval(const GeometryVector &k, double *v, double *s0)
+	{
+		*v = this->tildeVk(k);
+		*s0 = std::numeric_limits<double>::quiet_NaN();
+	}
+};
+template <class P> struct ProbeVS : P {
+	template <class... A> ProbeVS(A... a) : P(a...) {}
+	void eval(const GeometryVector &k, double *v, double *s0)
+	{
+		*v = this->tildeVk(k);
+		*s0 = this->S0k(k);
+	}
 };
 
 GeometryVector MakeVec(int d, const double *x)
@@ -164,6 +187,80 @@ void *ccref_create_s2(int d, const double *basis, long M, const int32_t *modes, 
 		s2->AddConstraint(k, std::vector<double>{V[m], S0[m]});
 	}
 	return h;
+}
+
+// The named variable-cell potentials of potential/CCPotential_Kernels.h:190-191, 339-358 at the cell `basis`:
+//   0 K2Potential, 1 KM3Potential (ShiftedCCPotential_varBox), 2 K2K2Potential, 3 K2K2Potential_noV0,
+//   4 KM3K2Potential_noV0, 5 KM2K2Potential, 6 KM3K2Potential, 7 KM4K2Potential, 8 KM3KM2Potential,
+//   9 KM3KMLogPotential, 10-12 KM2/KM3/KM4KnPotential(n), 13-15 KM2/KM3/KM4KlcPotential(n).
+// Their constraints (k within rK, weights tildeV(k)) and shifts are generated by their own SetConfiguration, i.e. by
+// ccref_set_positions.
+void *ccref_create_varbox(int kind, int d, const double *basis, double rK, double n, int nthreads)
+{
+	if (d < 1 || d > 4 || kind < 0 || kind > 15)
+		return nullptr;
+	RefHandle *h = new RefHandle();
+	h->d = d;
+	for (int i = 0; i < d; i++)
+		h->basis.push_back(MakeVec(d, basis + d * i));
+	h->config = EmptyConfig(h);
+	auto plain = [&](auto *q) {
+		h->weights = [q](const GeometryVector &k, double *v, double *s0) { q->eval(k, v, s0); };
+		h->pot.reset(q);
+	};
+	auto s2 = [&](auto *q) {
+		plain(q);
+		h->s2 = q;
+	};
+	switch (kind) {
+	case 0: plain(new ProbeV<K2Potential>(d, rK)); break;
+	case 1: plain(new ProbeV<KM3Potential>(d, rK)); break;
+	case 2: s2(new ProbeVS<K2K2Potential>(d, rK)); break;
+	case 3: s2(new ProbeVS<K2K2Potential_noV0>(d, rK)); break;
+	case 4: s2(new ProbeVS<KM3K2Potential_noV0>(d, rK)); break;
+	case 5: s2(new ProbeVS<KM2K2Potential>(d, rK)); break;
+	case 6: s2(new ProbeVS<KM3K2Potential>(d, rK)); break;
+	case 7: s2(new ProbeVS<KM4K2Potential>(d, rK)); break;
+	case 8: s2(new ProbeVS<KM3KM2Potential>(d, rK)); break;
+	case 9: s2(new ProbeVS<KM3KMLogPotential>(d, rK)); break;
+	case 10: s2(new ProbeVS<KM2KnPotential>(d, n, rK)); break;
+	case 11: s2(new ProbeVS<KM3KnPotential>(d, n, rK)); break;
+	case 12: s2(new ProbeVS<KM4KnPotential>(d, n, rK)); break;
+	case 13: s2(new ProbeVS<KM2KlcPotential>(d, n, rK)); break;
+	case 14: s2(new ProbeVS<KM3KlcPotential>(d, n, rK)); break;
+	default: s2(new ProbeVS<KM4KlcPotential>(d, n, rK)); break;
+	}
+	h->nthreads = nthreads < 1 ? 1 : nthreads;
+	h->pot->ParallelNumThread = h->nthreads;
+	return h;
+}
+
+// Constraint count, Shift and, for the S2 kinds, the length of the S0 list (-1 for the plain kinds).
+void ccref_varbox_state(void *p, long *M, double *shift, long *nS0)
+{
+	RefHandle *h = static_cast<RefHandle *>(p);
+	*M = (long)h->pot->constraints.size();
+	*shift = h->pot->Shift;
+	*nS0 = h->s2 ? (long)h->s2->S0.size() : -1;
+}
+
+// The constraints' Cartesian k (M x d) and weights V (M).
+void ccref_constraints(void *p, double *k, double *V)
+{
+	RefHandle *h = static_cast<RefHandle *>(p);
+	for (size_t m = 0; m < h->pot->constraints.size(); m++) {
+		for (int e = 0; e < h->d; e++)
+			k[m * h->d + e] = h->pot->constraints[m].k.x[e];
+		V[m] = h->pot->constraints[m].V;
+	}
+}
+
+// tildeV(k) and S0(k) of a varBox handle's class at M Cartesian wavevectors.
+void ccref_varbox_weights(void *p, long M, const double *k, double *V, double *S0)
+{
+	RefHandle *h = static_cast<RefHandle *>(p);
+	for (long m = 0; m < M; m++)
+		h->weights(MakeVec(h->d, k + m * h->d), V + m, S0 + m);
 }
 
 void ccref_destroy(void *p) { delete static_cast<RefHandle *>(p); }

@@ -66,3 +66,30 @@ void GeometryVector::ReadBinary(std::istream &ifile, DimensionType dimension)
 {
 	ifile.read(reinterpret_cast<char *>(this->x), sizeof(double) * dimension);
 }
+
+// GSL stand-ins for potential/CCPotential_varBox.h (declared in standins/gsl/gsl_linalg.h). Only that header's cell
+// derivatives call them, and the oracle never does: each throws, so a call by mistake fails loudly.
+#include <gsl/gsl_linalg.h>
+
+#include <stdexcept>
+
+[[noreturn]] static void gsl_standin()
+{
+	throw std::logic_error("GSL stand-in reached: cell derivatives are not part of the oracle");
+}
+
+gsl_matrix *gsl_matrix_alloc(size_t, size_t) { gsl_standin(); }
+void gsl_matrix_free(gsl_matrix *) { gsl_standin(); }
+double gsl_matrix_get(const gsl_matrix *, size_t, size_t) { gsl_standin(); }
+void gsl_matrix_set(gsl_matrix *, size_t, size_t, double) { gsl_standin(); }
+gsl_vector *gsl_vector_alloc(size_t) { gsl_standin(); }
+void gsl_vector_free(gsl_vector *) { gsl_standin(); }
+double gsl_vector_get(const gsl_vector *, size_t) { gsl_standin(); }
+void gsl_vector_set(gsl_vector *, size_t, double) { gsl_standin(); }
+void gsl_vector_set_zero(gsl_vector *) { gsl_standin(); }
+gsl_permutation *gsl_permutation_alloc(size_t) { gsl_standin(); }
+gsl_permutation *gsl_permutation_calloc(size_t) { gsl_standin(); }
+void gsl_permutation_free(gsl_permutation *) { gsl_standin(); }
+int gsl_linalg_LU_decomp(gsl_matrix *, gsl_permutation *, int *) { gsl_standin(); }
+int gsl_linalg_LU_solve(const gsl_matrix *, const gsl_permutation *, const gsl_vector *, gsl_vector *) { gsl_standin(); }
+int gsl_linalg_LU_invert(const gsl_matrix *, const gsl_permutation *, gsl_matrix *) { gsl_standin(); }
