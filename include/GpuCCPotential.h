@@ -1,13 +1,17 @@
-/* GpuCCPotential.h — drop-in GPU replacement for the reference's ShiftedCCPotential (header-only C++ adapter).
+/* GpuCCPotential.h — drop-in GPU replacements for the reference's ShiftedCCPotential and ShiftedCCPotential_S2
+ * (header-only C++ adapter).
  *
  * Include it in code built against the reference (it needs potential/CollectiveCoordinatePotential.h and
- * potential/CombinedEnergyForce.h on the include path) and link libccgpu.so. The class derives from ShiftedCCPotential
- * (potential/CollectiveCoordinatePotential.h:53-1497) and CombinedEnergyForce (potential/CombinedEnergyForce.h), so the
- * structure optimiser's Objective (potential/StructureOptimization.cpp:447-536) finds EnergyAndAllForce by
- * dynamic_cast and makes one GPU evaluation per step; MD/MC drivers call Energy / AllForce / Force as before.
+ * potential/CombinedEnergyForce.h on the include path) and link libccgpu.so. GpuCCPotential derives from
+ * ShiftedCCPotential (potential/CollectiveCoordinatePotential.h:53-1497), GpuCCPotential_S2 from ShiftedCCPotential_S2
+ * (:1642-1749; its AddConstraint(k, {V, S0}) and public S0 list are the reference's), both also from
+ * CombinedEnergyForce (potential/CombinedEnergyForce.h), so the structure optimiser's Objective
+ * (potential/StructureOptimization.cpp:447-536) finds EnergyAndAllForce by dynamic_cast and makes one GPU evaluation
+ * per step; MD/MC drivers call Energy / AllForce / Force as before.
  *
  * Contract kept from the reference:
- *   - constraints / Shift are the public members of ShiftedCCPotential; a change is seen at the next evaluation;
+ *   - constraints / Shift (and S0 for the S2 form) are the public members of the reference class; a change is seen at
+ *     the next evaluation; the S2 form needs one S0 per constraint and distinct wavevectors;
  *     every k must lie on the reciprocal lattice of the bound cell (std::invalid_argument otherwise);
  *   - SetConfiguration binds a Configuration the caller keeps alive (non-owning), invalidating cached results;
  *   - EnergyAndAllForce equals Energy() followed by AllForce() bitwise (both read one cached GPU evaluation);
@@ -28,10 +32,10 @@
 #include <string>
 #include <vector>
 
-class GpuCCPotential : public ShiftedCCPotential, public CombinedEnergyForce
+template <class Base> class GpuCCAdapter : public Base, public CombinedEnergyForce
 {
 	cc_handle *handle_ = nullptr;
-	std::vector<double> kcopy_, vcopy_, basis_;   // the constraint set and cell the handle was built from
+	std::vector<double> kcopy_, vcopy_, s0copy_, basis_;   // the constraint set and cell the handle was built from
 	double shift_copy_ = 0.0;
 	std::vector<double> frac_, forces_;
 	double energy_ = 0.0;
@@ -52,6 +56,10 @@ class GpuCCPotential : public ShiftedCCPotential, public CombinedEnergyForce
 
 	const Configuration &Bound() const { return *this->pConfig; }
 
+	// the targets of the S2 form; none for the plain form
+	static const std::vector<double> *Targets(const ShiftedCCPotential &) { return nullptr; }
+	static const std::vector<double> *Targets(const ShiftedCCPotential_S2 &p) { return &p.S0; }
+
 	// (Re)create the handle when the constraints, Shift or the cell changed; upload positions when dirty.
 	void Sync()
 	{
@@ -69,10 +77,21 @@ class GpuCCPotential : public ShiftedCCPotential, public CombinedEnergyForce
 				k.push_back(q.k.x[j]);
 			V.push_back(q.V);
 		}
-		if (!handle_ || k != kcopy_ || V != vcopy_ || basis != basis_ || this->Shift != shift_copy_) {
+		const std::vector<double> *S0 = Targets(*this);
+		if (S0 && S0->size() != V.size())
+			throw std::invalid_argument("GpuCCPotential: the S2 form needs one S0 per constraint");
+		if (!handle_ || k != kcopy_ || V != vcopy_ || basis != basis_ || this->Shift != shift_copy_ ||
+		    (S0 && *S0 != s0copy_)) {
 			cc_destroy(handle_);
 			handle_ = nullptr;
-			Check(cc_create_cartesian(d, basis.data(), (int64_t)V.size(), k.data(), V.data(), this->Shift, &handle_));
+			if (S0)
+				Check(cc_create_s2_cartesian(d, basis.data(), (int64_t)V.size(), k.data(), V.data(), S0->data(),
+				                             this->Shift, &handle_));
+			else
+				Check(cc_create_cartesian(d, basis.data(), (int64_t)V.size(), k.data(), V.data(), this->Shift,
+				                          &handle_));
+			if (S0)
+				s0copy_ = *S0;
 			kcopy_.swap(k);
 			vcopy_.swap(V);
 			basis_.swap(basis);
@@ -102,13 +121,14 @@ class GpuCCPotential : public ShiftedCCPotential, public CombinedEnergyForce
 	}
 
 public:
-	explicit GpuCCPotential(DimensionType dimension) : ShiftedCCPotential(dimension) {}
-	explicit GpuCCPotential(const ShiftedCCPotential &src) : ShiftedCCPotential(src) {}
-	GpuCCPotential(const GpuCCPotential &) = delete;
-	GpuCCPotential &operator=(const GpuCCPotential &) = delete;
-	virtual ~GpuCCPotential() { cc_destroy(handle_); }
+	explicit GpuCCAdapter(DimensionType dimension) : Base(dimension) {}
+	explicit GpuCCAdapter(const Base &src) : Base(src) {}
+	GpuCCAdapter(const GpuCCAdapter &) = delete;
+	GpuCCAdapter &operator=(const GpuCCAdapter &) = delete;
+	virtual ~GpuCCAdapter() { cc_destroy(handle_); }
 
-	/* CC_PREC_FP64 (default, the reference's arithmetic to rounding) or CC_PREC_MIXED. */
+	/* CC_PREC_FP64 (default, the reference's arithmetic to rounding) or CC_PREC_MIXED (the S2 form evaluates in FP64
+	 * either way). */
 	void SetPrecision(int precision)
 	{
 		precision_ = precision;
@@ -117,7 +137,7 @@ public:
 
 	virtual void SetConfiguration(const Configuration &Position)
 	{
-		ShiftedCCPotential::SetConfiguration(Position);
+		Base::SetConfiguration(Position);
 		positions_dirty_ = true;
 		result_valid_ = false;
 	}
@@ -154,7 +174,7 @@ public:
 		Evaluate();
 		const int d = this->Dimension;
 		if (i >= frac_.size() / d)
-			throw std::out_of_range("GpuCCPotential::Force: particle index out of range");
+			throw std::out_of_range("GpuCCPotential: Force: particle index out of range");
 		result = GeometryVector(d);
 		for (int j = 0; j < d; j++)
 			result.x[j] = forces_[i * d + j];
@@ -165,6 +185,20 @@ public:
 		AllForce(forces);
 		return energy_;
 	}
+};
+
+class GpuCCPotential : public GpuCCAdapter<ShiftedCCPotential>
+{
+public:
+	explicit GpuCCPotential(DimensionType dimension) : GpuCCAdapter<ShiftedCCPotential>(dimension) {}
+	explicit GpuCCPotential(const ShiftedCCPotential &src) : GpuCCAdapter<ShiftedCCPotential>(src) {}
+};
+
+class GpuCCPotential_S2 : public GpuCCAdapter<ShiftedCCPotential_S2>
+{
+public:
+	explicit GpuCCPotential_S2(DimensionType dimension) : GpuCCAdapter<ShiftedCCPotential_S2>(dimension) {}
+	explicit GpuCCPotential_S2(const ShiftedCCPotential_S2 &src) : GpuCCAdapter<ShiftedCCPotential_S2>(src) {}
 };
 
 #endif

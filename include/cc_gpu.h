@@ -78,6 +78,10 @@ int cc_create_cartesian(int d, const double *basis, int64_t M, const double *k, 
 int cc_create_s2(int d, const double *basis, int64_t M, const int32_t *modes, const double *V, const double *S0,
                  double shift, cc_handle **out);
 
+/* As cc_create_s2 with Cartesian k (M x d), mapped to modes as in cc_create_cartesian. */
+int cc_create_s2_cartesian(int d, const double *basis, int64_t M, const double *k, const double *V, const double *S0,
+                           double shift, cc_handle **out);
+
 int cc_destroy(cc_handle *h);
 
 /* Number of constraints, dimension, volume and the integer modes (M x d) of a handle. */

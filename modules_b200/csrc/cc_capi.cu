@@ -1595,6 +1595,17 @@ int cc_create_s2(int d, const double *basis, int64_t M, const int32_t *modes, co
 	return CC_OK;
 }
 
+int cc_create_s2_cartesian(int d, const double *basis, int64_t M, const double *k, const double *V, const double *S0,
+                           double shift, cc_handle **out)
+{
+	if (d < 1 || d > 3 || !basis || M < 0 || (M > 0 && !k))
+		return fail(CC_ERR_ARG, "invalid arguments");
+	std::vector<int32_t> modes((size_t)M * d);
+	if (!cc::cartesian_to_modes(d, basis, M, k, modes.data()))
+		return fail(CC_ERR_NONLATTICE, "a Cartesian k is not on the reciprocal lattice of the cell");
+	return cc_create_s2(d, basis, M, modes.data(), V, S0, shift, out);
+}
+
 int cc_destroy(cc_handle *h)
 {
 	if (!h)

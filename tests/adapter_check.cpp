@@ -8,6 +8,9 @@
 //   2. The structure optimiser's Switch-0 objective (restated from potential/StructureOptimization.cpp:447-536) finds
 //      CombinedEnergyForce by dynamic_cast and drives the reference's LuksanPLIS with the GPU adapter to the
 //      stealthy ground state of a 2D N=100 chi=0.30 configuration (E/N < 1e-20).
+//   4. GpuCCPotential_S2 against the reference's ShiftedCCPotential_S2 (constraints through AddConstraint(k, {V, S0}))
+//      on a skew 2D cell: Energy and AllForce within 1e-10 of the S2 rounding scales, Force(i), EnergyAndAllForce
+//      bitwise, and a changed S0 seen at the next evaluation.
 // Prints one line per check and exits 0 only if all pass.
 #include "GpuCCPotential.h"
 #include "GpuMultiStealthyPotential.h"
@@ -229,6 +232,61 @@ int main()
 			for (int j = 0; j < d; j++)
 				same = same && fc[i].x[j] == fg[i].x[j];
 		check(same, "multi-species EnergyAndAllForce == Energy then AllForce (bitwise)", Ec, Eg);
+	}
+	// ---- 4. the S2 form against the reference's ShiftedCCPotential_S2 --------------------------------------------
+	{
+		const int d = 2, n = 80;
+		Configuration c = make_config(d, {9.0, 0.0, 2.0, 8.5}, n, rng);
+		ShiftedCCPotential_S2 ref(d);
+		GpuCCPotential_S2 gpu(d);
+		std::uniform_real_distribution<double> uv(0.2, 2.0), us(0.0, 1.5);
+		for (int a = -4; a <= 4; a++)
+			for (int b = -4; b <= 4; b++) {
+				if (a < 0 || (a == 0 && b <= 0))
+					continue;
+				GeometryVector k(d);
+				k.AddFrom((double)a * c.GetReciprocalBasisVector(0));
+				k.AddFrom((double)b * c.GetReciprocalBasisVector(1));
+				const std::vector<double> vals{uv(rng), us(rng)};
+				ref.AddConstraint(k, vals);
+				gpu.AddConstraint(k, vals);
+			}
+		ref.Shift = gpu.Shift = -0.5;
+		ref.SetConfiguration(c);
+		gpu.SetConfiguration(c);
+		ref.GetRho();
+		double sE = 0, sF = 0;
+		for (size_t q = 0; q < ref.constraints.size(); q++) {
+			const double r2 = ref.RhoReal[q] * ref.RhoReal[q] + ref.RhoImag[q] * ref.RhoImag[q];
+			const double dS = std::abs(r2 / n - ref.S0[q]) + 1;
+			sE += std::abs(ref.constraints[q].V) * dS * dS;
+			sF += 4.0 / n * std::abs(ref.constraints[q].V) * dS * (std::sqrt(r2) + 1) *
+			      std::sqrt(ref.constraints[q].k.Modulus2());
+		}
+		const double Er = ref.Energy(), Eg = gpu.Energy();
+		check(std::abs(Er - Eg) <= 1e-10 * sE, "S2 Energy", Eg, Er);
+		std::vector<GeometryVector> fr, fg, fc;
+		ref.AllForce(fr);
+		gpu.AllForce(fg);
+		double worst = 0;
+		for (size_t i = 0; i < fr.size(); i++)
+			for (int j = 0; j < d; j++)
+				worst = std::max(worst, std::abs(fr[i].x[j] - fg[i].x[j]));
+		check(fg.size() == fr.size() && worst <= 1e-10 * sF, "S2 AllForce max |dF| / scale", worst / sF, 1e-10);
+		GeometryVector f1;
+		gpu.Force(f1, 41);
+		check(f1.x[0] == fg[41].x[0] && f1.x[1] == fg[41].x[1], "S2 Force(i) == AllForce[i]", f1.x[0], fg[41].x[0]);
+		const double Ec = gpu.EnergyAndAllForce(fc);
+		bool same = Ec == Eg && fc.size() == fg.size();
+		for (size_t i = 0; same && i < fc.size(); i++)
+			for (int j = 0; j < d; j++)
+				same = same && fc[i].x[j] == fg[i].x[j];
+		check(same, "S2 EnergyAndAllForce == Energy then AllForce (bitwise)", Ec, Eg);
+		ref.S0[3] += 0.75;
+		gpu.S0[3] += 0.75;
+		ref.RhoValid = false;
+		const double Er2 = ref.Energy(), Eg2 = gpu.Energy();
+		check(Er2 != Er && std::abs(Er2 - Eg2) <= 1e-10 * sE, "S2 target change seen", Eg2, Er2);
 	}
 	std::printf(failures ? "ADAPTER FAIL\n" : "ADAPTER OK\n");
 	return failures ? 1 : 0;
