@@ -78,6 +78,15 @@ int cc_create_cartesian(int d, const double *basis, int64_t M, const double *k, 
 int cc_create_s2(int d, const double *basis, int64_t M, const int32_t *modes, const double *V, const double *S0,
                  double shift, cc_handle **out);
 
+/* The S2 form over nsub sub-configurations, the reference's ShiftedCCPotential_S2_MultiConfig
+ * (potential/CollectiveCoordinatePotential.h:1756-1870): particles [c Np, (c + 1) Np), Np = N / nsub, form
+ * sub-configuration c; E = sum_m V_m (<S(k_m)> - S0_m)^2 + shift with <S> = sum_c |rho_c|^2 / (Np nsub), and the
+ * force on a particle of sub-configuration c is (4 / (Np nsub)) sum_m V_m dS_m Im(conj(rho_c) e^{i k.r}) k_m. N must
+ * be a multiple of nsub (CC_ERR_ARG otherwise); cc_rho refuses the handle (rho is per sub-configuration). Otherwise as
+ * cc_create_s2; nsub = 1 is the S2 form. */
+int cc_create_s2_multiconfig(int d, const double *basis, int64_t M, const int32_t *modes, const double *V,
+                             const double *S0, double shift, int nsub, cc_handle **out);
+
 /* As cc_create_s2 with Cartesian k (M x d), mapped to modes as in cc_create_cartesian. */
 int cc_create_s2_cartesian(int d, const double *basis, int64_t M, const double *k, const double *V, const double *S0,
                            double shift, cc_handle **out);

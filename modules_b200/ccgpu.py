@@ -71,6 +71,7 @@ _SIGS = {
     "cc_create": (_i, [_i, _vp, _i64, _vp, _vp, _d, ctypes.POINTER(_vp)]),
     "cc_create_cartesian": (_i, [_i, _vp, _i64, _vp, _vp, _d, ctypes.POINTER(_vp)]),
     "cc_create_s2": (_i, [_i, _vp, _i64, _vp, _vp, _vp, _d, ctypes.POINTER(_vp)]),
+    "cc_create_s2_multiconfig": (_i, [_i, _vp, _i64, _vp, _vp, _vp, _d, _i, ctypes.POINTER(_vp)]),
     "cc_destroy": (_i, [_vp]),
     "cc_info": (_i, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i), ctypes.POINTER(_d), _vp]),
     "cc_set_rho_offset": (_i, [_vp, _d]),
@@ -261,15 +262,19 @@ class CCPotential:
     """GPU ShiftedCCPotential over a cell ``basis`` (rows a_i) with integer ``modes`` (k = sum_e n_e b_e).
 
     With ``S0`` (one target per mode, integer modes, distinct) it is the S2 form, the reference's ShiftedCCPotential_S2
-    (potential/CollectiveCoordinatePotential.h:1642-1749): E = sum_k V(k) (|rho(k)|^2 / N - S0(k))^2 + shift."""
+    (potential/CollectiveCoordinatePotential.h:1642-1749): E = sum_k V(k) (|rho(k)|^2 / N - S0(k))^2 + shift. With
+    ``nsub`` > 1 as well, ShiftedCCPotential_S2_MultiConfig (:1756-1870): the N particles are nsub consecutive
+    sub-configurations and S(k) is their mean."""
 
-    def __init__(self, d, basis, modes=None, V=None, shift=0.0, kcart=None, S0=None):
+    def __init__(self, d, basis, modes=None, V=None, shift=0.0, kcart=None, S0=None, nsub=1):
         self._lib = load_library()
         self.d = int(d)
         self.basis = np.ascontiguousarray(basis, dtype=np.float64).reshape(self.d, self.d)
         h = _vp()
         if kcart is not None and S0 is not None:
             raise ValueError("the S2 form takes integer modes")
+        if nsub != 1 and S0 is None:
+            raise ValueError("sub-configurations belong to the S2 form")
         if kcart is not None:
             kc = np.ascontiguousarray(kcart, dtype=np.float64).reshape(-1, self.d)
             V = np.ascontiguousarray(V, dtype=np.float64).reshape(-1)
@@ -284,8 +289,8 @@ class CCPotential:
                 S0 = np.ascontiguousarray(S0, dtype=np.float64).reshape(-1)
                 if len(S0) != len(V):
                     raise ValueError("modes and S0 differ in length")
-                _check(self._lib.cc_create_s2(self.d, _ptr(self.basis), len(V), _ptr(modes), _ptr(V), _ptr(S0),
-                                              shift, ctypes.byref(h)))
+                _check(self._lib.cc_create_s2_multiconfig(self.d, _ptr(self.basis), len(V), _ptr(modes), _ptr(V),
+                                                          _ptr(S0), shift, int(nsub), ctypes.byref(h)))
             else:
                 _check(self._lib.cc_create(self.d, _ptr(self.basis), len(V), _ptr(modes), _ptr(V), shift,
                                            ctypes.byref(h)))

@@ -235,6 +235,11 @@ struct cc_handle {
 	bool use_fused = false;         // cc_set_path
 	// S2 form (cc_create_s2): per-slot targets S0, E = sum V (|rho|^2 / N - S0)^2 + shift; split path only
 	double *d_slotS0 = nullptr;
+	// S2 over nsub sub-configurations (cc_create_s2_multiconfig): rho and u per sub-configuration, block partials
+	int nsub = 1;
+	double2 *d_msub = nullptr;      // [2][nsub][nslot]: rho, then u
+	double *d_mpart = nullptr;      // energy partials of the combination, then one scratch word
+	size_t msub_cap = 0, mpart_cap = 0;
 	bool use_nufft = false;         // cc_set_path(CC_PATH_NUFFT)
 	bool auto_path = true;          // CC_PATH_AUTO (default): the NUFFT path where its estimated time is lower
 	double nu_grid_est = -1.0;      // fine-grid points the NUFFT path would use (computed once)
@@ -721,8 +726,11 @@ int ensure_partialG(cc_handle *h, size_t elems)
 
 // rho pass of k-set `k` over N device positions: rho per slot, u, and the energy into d_E.
 // energy_in_force: a force pass follows and sums the energy partials (one reduce-block ticket less on the path).
+// rho_out / u_out: where the reduce writes rho and u per slot (the k-set's own buffers when null; the S2 form's
+// per-slot targets then apply).
 int run_rho(cc_handle *h, DevKSet &k, int64_t N, const double *d_frac, double *d_E, bool want_rho_mode, bool mixed,
-            const Launch &l, cudaStream_t st, cudaEvent_t after_rho = nullptr, bool energy_in_force = false)
+            const Launch &l, cudaStream_t st, cudaEvent_t after_rho = nullptr, bool energy_in_force = false,
+            double2 *rho_out = nullptr, double2 *u_out = nullptr)
 {
 	const cc::Plan &p = k.plan;
 	if (p.nslot == 0) {
@@ -767,7 +775,10 @@ int run_rho(cc_handle *h, DevKSet &k, int64_t N, const double *d_frac, double *d
 	r.E_out = d_E;
 	r.finalize = energy_in_force ? 0 : 1;
 	r.skip = h->d_skip;
-	if (h->d_slotS0 && &k == &h->main) {
+	if (rho_out) {
+		r.rho_slot = rho_out;
+		r.u_slot = u_out;
+	} else if (h->d_slotS0 && &k == &h->main) {
 		r.slotS0 = h->d_slotS0;
 		r.npart = (double)N;
 		r.inv_vol = 1.0;
@@ -782,8 +793,11 @@ int run_rho(cc_handle *h, DevKSet &k, int64_t N, const double *d_frac, double *d
 }
 
 // d_E: when not null, the force kernel also writes the energy (run_rho was called with energy_in_force).
+// u_in / fscale_in: the slot coefficients and force scale to use instead of the handle's (one sub-configuration of
+// the multi-configuration S2 form).
 int run_force(cc_handle *h, int64_t N, const double *d_frac, double *d_F, double *d_gfrac, bool mixed,
-              const Launch &l, cudaStream_t st, double *d_E = nullptr)
+              const Launch &l, cudaStream_t st, double *d_E = nullptr, const double2 *u_in = nullptr,
+              double fscale_in = 0.0)
 {
 	const cc::Plan &p = h->main.plan;
 	if (N == 0)
@@ -829,6 +843,10 @@ int run_force(cc_handle *h, int64_t N, const double *d_frac, double *d_F, double
 	if (h->d_slotS0) {   // F = (4 / N) sum_k Im(u z) k with u = V dS conj(rho)
 		a.fscale = 4.0 / (double)N;
 		a.inv_vol = 1.0;
+	}
+	if (u_in) {
+		a.u_slot = u_in;
+		a.fscale = fscale_in;
 	}
 	return launch_force(h->d, a, mixed, N, f->host.max_row, st);
 }
@@ -1356,9 +1374,73 @@ bool nufft_preferred(cc_handle *h, int64_t N)
 	return 1.2 * nufft < direct;
 }
 
+// ShiftedCCPotential_S2_MultiConfig (potential/CollectiveCoordinatePotential.h:1756-1870): particles
+// [c Np, (c + 1) Np) form sub-configuration c; per c a rho pass into its own rho / u slab, one combination over the
+// sub-configurations (the mean S(k), the energy and u_c), then per c a force pass with scale 4 / Np / nsub. FP64.
+int eval_multiconfig(cc_handle *h, int64_t N, const double *d_frac, double *d_E, double *d_F, double *d_gfrac,
+                     cudaStream_t st)
+{
+	const int nsub = h->nsub, d = h->d;
+	const int64_t Np = N / nsub;
+	DevKSet &k = h->main;
+	const cc::Plan &p = k.plan;
+	if (p.nslot == 0) {
+		cc::cc_set_scalar_kernel<<<1, 1, 0, st>>>(d_E, h->shift);
+		CC_CUDA(cudaGetLastError());
+		if (N > 0 && d_F)
+			CC_CUDA(cudaMemsetAsync(d_F, 0, sizeof(double) * N * d, st));
+		if (N > 0 && d_gfrac)
+			CC_CUDA(cudaMemsetAsync(d_gfrac, 0, sizeof(double) * N * d, st));
+		return CC_OK;
+	}
+	const size_t slab = (size_t)nsub * p.nslot;
+	const int nb = (p.nslot + cc::kS2mThreads - 1) / cc::kS2mThreads;
+	if (int rc = grow(&h->d_msub, h->msub_cap, 2 * slab))
+		return rc;
+	if (int rc = grow(&h->d_mpart, h->mpart_cap, (size_t)nb + 1))
+		return rc;
+	double2 *rho = h->d_msub, *u = h->d_msub + slab;
+	const Launch l = choose_launch(p, Np, false);
+	double *copy = h->rho_copy;   // graph path: the rho passes store the positions for the force passes
+	for (int c = 0; c < nsub; c++) {
+		h->rho_copy = copy ? copy + (size_t)c * Np * d : nullptr;
+		const int rc = run_rho(h, k, Np, d_frac + (size_t)c * Np * d, h->d_mpart + nb, false, false, l, st, nullptr,
+		                       false, rho + (size_t)c * p.nslot, u + (size_t)c * p.nslot);
+		if (rc) {
+			h->rho_copy = copy;
+			return rc;
+		}
+	}
+	h->rho_copy = copy;
+	if (copy)
+		d_frac = copy;
+	cc::cc_s2multi_kernel<<<nb, cc::kS2mThreads, 0, st>>>(rho, u, p.nslot, nsub, k.slotV, h->d_slotS0,
+	                                                       (double)Np * (double)nsub, h->d_mpart);
+	CC_CUDA(cudaGetLastError());
+	cc::cc_mc_sum_kernel<<<1, 32, 0, st>>>(h->d_mpart, nb, 1.0, d_E, h->shift);
+	CC_CUDA(cudaGetLastError());
+	if (!(d_F || d_gfrac) || Np == 0)
+		return CC_OK;
+	const double fscale = 4.0 / (double)Np / (double)nsub;
+	for (int c = 0; c < nsub; c++) {
+		const size_t off = (size_t)c * Np * d;
+		if (int rc = run_force(h, Np, d_frac + off, d_F ? d_F + off : nullptr, d_gfrac ? d_gfrac + off : nullptr,
+		                       false, l, st, nullptr, u + (size_t)c * p.nslot, fscale))
+			return rc;
+	}
+	return CC_OK;
+}
+
 int eval_device(cc_handle *h, int64_t N, const double *d_frac, double *d_E, double *d_F, double *d_gfrac,
                 bool want_rho_mode, int precision, cudaStream_t st)
 {
+	if (h->nsub > 1) {
+		if (N % h->nsub)
+			return fail(CC_ERR_ARG, "the particle count is not a multiple of the number of sub-configurations");
+		if (want_rho_mode)
+			return fail(CC_ERR_ARG, "rho per constraint is per sub-configuration in the multi-configuration form");
+		return eval_multiconfig(h, N, d_frac, d_E, d_F, d_gfrac, st);
+	}
 	const bool mixed = precision == CC_PREC_MIXED && !h->d_slotS0;   // the S2 form evaluates in FP64
 	const Launch l = choose_launch(h->main.plan, N, mixed);
 	cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
@@ -1595,6 +1677,17 @@ int cc_create_s2(int d, const double *basis, int64_t M, const int32_t *modes, co
 	return CC_OK;
 }
 
+int cc_create_s2_multiconfig(int d, const double *basis, int64_t M, const int32_t *modes, const double *V,
+                             const double *S0, double shift, int nsub, cc_handle **out)
+{
+	if (nsub < 1)
+		return fail(CC_ERR_ARG, "the number of sub-configurations must be positive");
+	if (int rc = cc_create_s2(d, basis, M, modes, V, S0, shift, out))
+		return rc;
+	(*out)->nsub = nsub;
+	return CC_OK;
+}
+
 int cc_create_s2_cartesian(int d, const double *basis, int64_t M, const double *k, const double *V, const double *S0,
                            double shift, cc_handle **out)
 {
@@ -1624,6 +1717,8 @@ int cc_destroy(cc_handle *h)
 	cudaFree(h->d_fcounters);
 	cudaFree(h->d_E);
 	cudaFree(h->d_slotS0);
+	cudaFree(h->d_msub);
+	cudaFree(h->d_mpart);
 	cudaFreeHost(h->h_pin);
 	cudaFreeHost(h->h_in);
 	if (h->ev_in)
@@ -1689,6 +1784,8 @@ int cc_set_positions(cc_handle *h, int64_t N, const double *frac)
 		return rc;
 	if (N < 0 || (N > 0 && !frac) || N > ((int64_t)1 << 31) - 64)
 		return fail(CC_ERR_ARG, "invalid particle count or null positions");
+	if (N % h->nsub)
+		return fail(CC_ERR_ARG, "the particle count is not a multiple of the number of sub-configurations");
 	if (int rc = ensure_particles(h, N))
 		return rc;
 	const int d = h->d;
@@ -1784,6 +1881,8 @@ int cc_rho(cc_handle *h, double *re, double *im, int precision)
 		return rc;
 	if (h->N < 0)
 		return fail(CC_ERR_STATE, "positions not set");
+	if (h->nsub > 1)
+		return fail(CC_ERR_ARG, "rho per constraint is per sub-configuration in the multi-configuration form");
 	if (int rc = flush_upload(h))
 		return rc;
 	const int64_t N = h->N;

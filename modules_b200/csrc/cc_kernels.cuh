@@ -1054,7 +1054,8 @@ static __global__ void __launch_bounds__(kMcThreads) cc_mc_kernel(const int32_t 
 	}
 }
 
-static __global__ void cc_mc_sum_kernel(const double *__restrict__ bpart, int nb, double inv_vol, double *out)
+static __global__ void cc_mc_sum_kernel(const double *__restrict__ bpart, int nb, double inv_vol, double *out,
+                                        double shift = 0.0)
 {
 	double t = 0.0;
 	for (int b = threadIdx.x; b < nb; b += 32)
@@ -1062,7 +1063,47 @@ static __global__ void cc_mc_sum_kernel(const double *__restrict__ bpart, int nb
 	for (int o = 16; o > 0; o >>= 1)
 		t += __shfl_down_sync(0xffffffffu, t, o);
 	if (threadIdx.x == 0)
-		*out = t * inv_vol;
+		*out = t * inv_vol + shift;
+}
+
+// ShiftedCCPotential_S2_MultiConfig (potential/CollectiveCoordinatePotential.h:1777-1870) over nsub sub-configurations
+// whose rho per slot are rho[c * nslot + slot]: Snow = sum_c |rho_c|^2 / count (count = Np nsub), dS = Snow - S0,
+// u_c = V dS conj(rho_c) for every c (the force pass of sub-configuration c reads u_c), and per-block partials of
+// V dS^2 in bpart[blockIdx.x].
+constexpr int kS2mThreads = 256;
+static __global__ void __launch_bounds__(kS2mThreads)
+cc_s2multi_kernel(const double2 *__restrict__ rho, double2 *__restrict__ u, int nslot, int nsub,
+                  const double *__restrict__ slotV, const double *__restrict__ slotS0, double count,
+                  double *__restrict__ bpart)
+{
+	__shared__ double sh[kS2mThreads / 32];
+	const int slot = blockIdx.x * kS2mThreads + threadIdx.x;
+	double e = 0.0;
+	if (slot < nslot) {
+		double snow = 0.0;
+		for (int c = 0; c < nsub; c++) {
+			const double2 r = rho[(size_t)c * nslot + slot];
+			snow += r.x * r.x + r.y * r.y;
+		}
+		const double ds = snow / count - slotS0[slot];
+		const double w = slotV[slot] * ds;
+		e = w * ds;
+		for (int c = 0; c < nsub; c++) {
+			const double2 r = rho[(size_t)c * nslot + slot];
+			u[(size_t)c * nslot + slot] = make_double2(w * r.x, -w * r.y);
+		}
+	}
+	for (int o = 16; o > 0; o >>= 1)
+		e += __shfl_down_sync(0xffffffffu, e, o);
+	if ((threadIdx.x & 31) == 0)
+		sh[threadIdx.x >> 5] = e;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double t = 0.0;
+		for (int w = 0; w < kS2mThreads / 32; w++)
+			t += sh[w];
+		bpart[blockIdx.x] = t;
+	}
 }
 
 }  // namespace cc

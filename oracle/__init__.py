@@ -50,6 +50,9 @@ def ref_lib():
         lib.ccref_create.argtypes = [ctypes.c_int, _vp, _l, _vp, _vp, _vp, _d, ctypes.c_int]
         lib.ccref_create_s2.restype = _vp
         lib.ccref_create_s2.argtypes = [ctypes.c_int, _vp, _l, _vp, _vp, _vp, _d, ctypes.c_int]
+        lib.ccref_create_s2_multiconfig.restype = _vp
+        lib.ccref_create_s2_multiconfig.argtypes = [ctypes.c_int, _vp, _l, _vp, _vp, _vp, _d, ctypes.c_int,
+                                                    ctypes.c_int]
         lib.ccref_create_varbox.restype = _vp
         lib.ccref_create_varbox.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _d, _d, ctypes.c_int]
         lib.ccref_varbox_state.argtypes = [_vp, _vp, _vp, _vp]
@@ -107,9 +110,10 @@ def lattice_k(basis, modes):
 
 class Ref:
     """The reference's ShiftedCCPotential (Direct backend) over a cell; modes or Cartesian k. With S0 (integer modes)
-    the reference's ShiftedCCPotential_S2 instead (potential/CollectiveCoordinatePotential.h:1642-1749)."""
+    the reference's ShiftedCCPotential_S2 instead (potential/CollectiveCoordinatePotential.h:1642-1749), and with nsub
+    its ShiftedCCPotential_S2_MultiConfig (:1756-1870)."""
 
-    def __init__(self, d, basis, V, modes=None, kcart=None, shift=0.0, nthreads=None, S0=None):
+    def __init__(self, d, basis, V, modes=None, kcart=None, shift=0.0, nthreads=None, S0=None, nsub=None):
         self.lib = ref_lib()
         self.d = d
         self.basis = np.ascontiguousarray(basis, np.float64).reshape(d, d)
@@ -118,7 +122,11 @@ class Ref:
         m = np.ascontiguousarray(modes, np.int32) if modes is not None else None
         k = np.ascontiguousarray(kcart, np.float64) if kcart is not None else None
         nt = nthreads or os.cpu_count() or 1
-        if S0 is not None:
+        if nsub is not None:   # ShiftedCCPotential_S2_MultiConfig
+            S0 = np.ascontiguousarray(S0, np.float64)
+            self.h = self.lib.ccref_create_s2_multiconfig(d, _p(self.basis), self.M, _p(m), _p(V), _p(S0), shift,
+                                                          int(nsub), nt)
+        elif S0 is not None:
             S0 = np.ascontiguousarray(S0, np.float64)
             self.h = self.lib.ccref_create_s2(d, _p(self.basis), self.M, _p(m), _p(V), _p(S0), shift, nt)
         else:

@@ -189,6 +189,34 @@ void *ccref_create_s2(int d, const double *basis, long M, const int32_t *modes, 
 	return h;
 }
 
+// The reference's ShiftedCCPotential_S2_MultiConfig (potential/CollectiveCoordinatePotential.h:1756-1870) over nsub
+// sub-configurations, constraints and targets appended to its public lists as the CLI's Type 15 does
+// (apps/CollectiveCoordinateCLI/CollectiveCoordinateCLI.cpp:524-540). N must be a multiple of nsub when positions are set.
+void *ccref_create_s2_multiconfig(int d, const double *basis, long M, const int32_t *modes, const double *V,
+                                  const double *S0, double shift, int nsub, int nthreads)
+{
+	if (d < 1 || d > 4 || M < 0 || nsub < 1)
+		return nullptr;
+	RefHandle *h = new RefHandle();
+	h->d = d;
+	for (int i = 0; i < d; i++)
+		h->basis.push_back(MakeVec(d, basis + d * i));
+	h->config = EmptyConfig(h);
+	ShiftedCCPotential_S2_MultiConfig *mc = new ShiftedCCPotential_S2_MultiConfig(d, (size_t)nsub);
+	h->pot.reset(mc);
+	h->nthreads = nthreads < 1 ? 1 : nthreads;
+	h->pot->ParallelNumThread = h->nthreads;
+	h->pot->Shift = shift;
+	for (long m = 0; m < M; m++) {
+		GeometryVector k(d);
+		for (int e = 0; e < d; e++)
+			k.AddFrom(static_cast<double>(modes[m * d + e]) * h->config->GetReciprocalBasisVector(e));
+		mc->constraints.emplace_back(k, V[m]);
+		mc->S0.push_back(S0[m]);
+	}
+	return h;
+}
+
 // The named variable-cell potentials of potential/CCPotential_Kernels.h:190-191, 339-358 at the cell `basis`:
 //   0 K2Potential, 1 KM3Potential (ShiftedCCPotential_varBox), 2 K2K2Potential, 3 K2K2Potential_noV0,
 //   4 KM3K2Potential_noV0, 5 KM2K2Potential, 6 KM3K2Potential, 7 KM4K2Potential, 8 KM3KM2Potential,
@@ -307,10 +335,12 @@ void ccref_eval(void *p, double *E, double *F, double *rhoRe, double *rhoIm)
 			for (int e = 0; e < h->d; e++)
 				F[i * h->d + e] = forces[i].x[e];
 	}
+	// M values (a multi-configuration potential holds M per sub-configuration: the first sub-configuration's)
+	const size_t M = std::min(h->pot->constraints.size(), h->pot->RhoReal.size());
 	if (rhoRe)
-		std::memcpy(rhoRe, h->pot->RhoReal.data(), sizeof(double) * h->pot->RhoReal.size());
+		std::memcpy(rhoRe, h->pot->RhoReal.data(), sizeof(double) * M);
 	if (rhoIm)
-		std::memcpy(rhoIm, h->pot->RhoImag.data(), sizeof(double) * h->pot->RhoImag.size());
+		std::memcpy(rhoIm, h->pot->RhoImag.data(), sizeof(double) * M);
 }
 
 // The reference's single-particle Force(i).

@@ -141,3 +141,79 @@ def test_gpu_minimize_s2(gpu):
     assert evals > 0 and E < 1e-6 * E0
     p.set_configuration(x)
     assert abs(p.energy() - E) <= 1e-12 * E0
+
+
+def multiconfig_restatement(basis, frac, modes, V, S0, shift, nsub):
+    """The reference's ShiftedCCPotential_S2_MultiConfig Energy and Force(i) in numpy
+    (potential/CollectiveCoordinatePotential.h:1777-1870)."""
+    N = len(frac)
+    Np = N // nsub
+    k = oracle.lattice_k(basis, modes)
+    ph = (frac @ basis) @ k.T
+    c, s = np.cos(ph), np.sin(ph)
+    re = c.reshape(nsub, Np, -1).sum(1)
+    im = s.reshape(nsub, Np, -1).sum(1)
+    snow = (re * re + im * im).sum(0) / (Np * nsub)
+    dS = snow - S0
+    E = float((V * dS * dS).sum()) + shift
+    coef = (4.0 / Np) * V * dS / nsub
+    sub = np.repeat(np.arange(nsub), Np)
+    F = -((im[sub] * c - re[sub] * s) * coef) @ k
+    return E, F, re, im, dS, k
+
+
+@needs_ref
+@pytest.mark.parametrize("d,N,kmax,nsub", [(2, 300, 6, 3), (3, 200, 3, 4), (1, 60, 20, 5)])
+def test_multiconfig_restatement_matches_reference(d, N, kmax, nsub):
+    basis, frac, modes, V, S0 = case(d, N, kmax, 21 + d)
+    ref = oracle.Ref(d, basis, V, modes=modes, shift=0.4, S0=S0, nsub=nsub)
+    ref.set_positions(frac)
+    E, F, _, _ = ref.eval()
+    E2, F2, re, im, dS, k = multiconfig_restatement(basis, frac, modes, V, S0, 0.4, nsub)
+    sE, sF = tol_scales(V, dS, np.sqrt((re * re + im * im).sum(0)), 0 * dS, k, N // nsub)
+    assert abs(E - E2) <= 1e-12 * sE
+    assert np.abs(F - F2).max() <= 1e-12 * sF
+
+
+@pytest.mark.gpu
+@needs_ref
+@pytest.mark.parametrize("d,N,kmax,nsub", [(2, 1200, 9, 3), (3, 2000, 5, 4), (2, 6000, 10, 2), (1, 100, 30, 5)])
+def test_gpu_multiconfig_matches_reference(gpu, d, N, kmax, nsub):
+    basis, frac, modes, V, S0 = case(d, N, kmax, 300 + d + nsub)
+    ref = oracle.Ref(d, basis, V, modes=modes, shift=0.125, S0=S0, nsub=nsub)
+    ref.set_positions(frac)
+    Eref, Fref, _, _ = ref.eval()
+    _, _, re, im, dS, k = multiconfig_restatement(basis, frac, modes, V, S0, 0.125, nsub)
+    sE, sF = tol_scales(V, dS, np.sqrt((re * re + im * im).sum(0)), 0 * dS, k, N // nsub)
+    p = gpu.CCPotential(d, basis, modes, V, 0.125, S0=S0, nsub=nsub)
+    p.set_configuration(frac)
+    for _ in range(3):   # direct, then captured evaluations of the same key
+        E, F = p.energy_and_forces()
+        assert abs(E - Eref) <= RTOL * sE, (E, Eref)
+        assert np.abs(F - Fref).max() <= RTOL * sF
+    assert p.energy() == E
+
+
+@pytest.mark.gpu
+def test_gpu_multiconfig_rules(gpu):
+    basis, frac, modes, V, S0 = case(2, 600, 6, 41)
+    one = gpu.CCPotential(2, basis, modes, V, 0.0, S0=S0, nsub=1)
+    s2 = gpu.CCPotential(2, basis, modes, V, 0.0, S0=S0)
+    one.set_configuration(frac)
+    s2.set_configuration(frac)
+    E1, F1 = one.energy_and_forces()
+    E2, F2 = s2.energy_and_forces()
+    assert E1 == E2 and np.array_equal(F1, F2)          # one sub-configuration is the S2 form
+    p = gpu.CCPotential(2, basis, modes, V, 0.0, S0=S0, nsub=4)
+    with pytest.raises(gpu.CCError):
+        p.set_configuration(frac[:598])                  # not a multiple of the sub-configuration count
+    p.set_configuration(frac)
+    with pytest.raises(gpu.CCError):
+        p.rho()                                          # rho is per sub-configuration
+    E, F = p.energy_and_forces()
+    x, Em, evals, iters, status = p.minimize(frac, max_evals=300)
+    assert Em < E
+    p.set_configuration(x)
+    assert abs(p.energy() - Em) <= 1e-12 * E
+    with pytest.raises(ValueError):
+        gpu.CCPotential(2, basis, modes, V, 0.0, nsub=2)
