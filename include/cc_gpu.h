@@ -264,6 +264,11 @@ int cc_isotropic_structure_factor(int d, int64_t nconfigs, const double *bases, 
 typedef struct cc_multi cc_multi;
 int cc_multi_create(int d, const double *basis, int nspecies, const int64_t *M, const int32_t *const *modes,
                     const double *const *V, double u0, double e0, cc_multi **out);
+/* As cc_multi_create with S0[s] (M[s] targets, distinct modes) making species s's Phi_s the S2 form (cc_create_s2);
+ * a NULL S0[s] keeps that species plain. With one species, u0 = 1 and radii sigma / 2 this is the reference's
+ * RepulsiveCCPotential (apps/CCOptimization/RepulsiveCCPotential.h:21-159) with an S2 kernel (S0 != 0). */
+int cc_multi_create_s2(int d, const double *basis, int nspecies, const int64_t *M, const int32_t *const *modes,
+                       const double *const *V, const double *const *S0, double u0, double e0, cc_multi **out);
 int cc_multi_set_configuration(cc_multi *m, int64_t N, const double *frac, const int32_t *species,
                                const double *radii);
 int cc_multi_energy_grad(cc_multi *m, double *E, double *F);

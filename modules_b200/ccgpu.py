@@ -85,6 +85,7 @@ _SIGS = {
     "cc_kset_stealthy": (_i, [_i, _vp, _i64, _d, _i, _i64, _vp, _vp, ctypes.POINTER(_i64)]),
     "cc_kset_isotropic": (_i, [_i, _vp, _d, _d, _d, _d, _i64, _vp, _vp, ctypes.POINTER(_i64)]),
     "cc_multi_create": (_i, [_i, _vp, _i, _vp, _vp, _vp, _d, _d, ctypes.POINTER(_vp)]),
+    "cc_multi_create_s2": (_i, [_i, _vp, _i, _vp, _vp, _vp, _vp, _d, _d, ctypes.POINTER(_vp)]),
     "cc_multi_set_configuration": (_i, [_vp, _i64, _vp, _vp, _vp]),
     "cc_multi_energy_grad": (_i, [_vp, ctypes.POINTER(_d), _vp]),
     "cc_multi_destroy": (_i, [_vp]),
@@ -203,9 +204,11 @@ def isotropic_structure_factor(d, bases, fracs, circular_kmax, linear_kmax, k_pr
 
 class CCMulti:
     """MultiStealthyPotential: species with their own constraint sets (integer modes + weights) over subsets of the
-    particles, plus the soft-core contact repulsion of strength e0; u0 scales the collective-coordinate part."""
+    particles, plus the soft-core contact repulsion of strength e0; u0 scales the collective-coordinate part. With
+    ``S0_per_species`` (an array of targets, or None, per species) a species' collective-coordinate part is the S2
+    form."""
 
-    def __init__(self, d, basis, modes_per_species, V_per_species, u0=1.0, e0=1.0):
+    def __init__(self, d, basis, modes_per_species, V_per_species, u0=1.0, e0=1.0, S0_per_species=None):
         self._lib = load_library()
         self.d = d
         basis = np.ascontiguousarray(basis, dtype=np.float64).reshape(d, d)
@@ -216,7 +219,14 @@ class CCMulti:
         mp = (_vp * S)(*[m.ctypes.data_as(_vp) for m in self._modes])
         vp = (_vp * S)(*[v.ctypes.data_as(_vp) for v in self._V])
         h = _vp()
-        _check(self._lib.cc_multi_create(d, _ptr(basis), S, _ptr(M), mp, vp, u0, e0, ctypes.byref(h)))
+        if S0_per_species is None:
+            _check(self._lib.cc_multi_create(d, _ptr(basis), S, _ptr(M), mp, vp, u0, e0, ctypes.byref(h)))
+        else:
+            self._S0 = [None if t is None else np.ascontiguousarray(t, dtype=np.float64) for t in S0_per_species]
+            if len(self._S0) != S or any(t is not None and len(t) != len(v) for t, v in zip(self._S0, self._V)):
+                raise ValueError("one S0 list (or None) per species, one target per mode")
+            sp = (_vp * S)(*[None if t is None else t.ctypes.data_as(_vp) for t in self._S0])
+            _check(self._lib.cc_multi_create_s2(d, _ptr(basis), S, _ptr(M), mp, vp, sp, u0, e0, ctypes.byref(h)))
         self._h = h
         self.N = None
         self.basis = basis

@@ -158,10 +158,11 @@ struct cc_multi {
 	std::vector<double> h_E, h_F, h_fs;
 };
 
-extern "C" {
+namespace {
 
-int cc_multi_create(int d, const double *basis, int nspecies, const int64_t *M, const int32_t *const *modes,
-                    const double *const *V, double u0, double e0, cc_multi **out)
+// S0: per species the S2 targets (ShiftedCCPotential_S2 for that species' collective-coordinate part), or null
+int multi_create(int d, const double *basis, int nspecies, const int64_t *M, const int32_t *const *modes,
+                 const double *const *V, const double *const *S0, double u0, double e0, cc_multi **out)
 {
 	if (!out)
 		return cc::set_error(CC_ERR_ARG, "out is null");
@@ -180,7 +181,10 @@ int cc_multi_create(int d, const double *basis, int nspecies, const int64_t *M, 
 	m->repulsion = std::abs(e0) > 1e-10;   // as the reference's WithRepulsion
 	for (int s = 0; s < nspecies; s++) {
 		cc_handle *h = nullptr;
-		const int rc = cc_create(d, basis, M[s], M[s] > 0 ? modes[s] : nullptr, M[s] > 0 ? V[s] : nullptr, 0.0, &h);
+		const int32_t *ms = M[s] > 0 ? modes[s] : nullptr;
+		const double *vs = M[s] > 0 ? V[s] : nullptr;
+		const int rc = (S0 && S0[s]) ? cc_create_s2(d, basis, M[s], ms, vs, S0[s], 0.0, &h)
+		                             : cc_create(d, basis, M[s], ms, vs, 0.0, &h);
 		if (rc != CC_OK) {
 			cc_multi_destroy(m);
 			return rc;
@@ -194,6 +198,22 @@ int cc_multi_create(int d, const double *basis, int nspecies, const int64_t *M, 
 	m->members.resize(nspecies);
 	*out = m;
 	return CC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cc_multi_create(int d, const double *basis, int nspecies, const int64_t *M, const int32_t *const *modes,
+                    const double *const *V, double u0, double e0, cc_multi **out)
+{
+	return multi_create(d, basis, nspecies, M, modes, V, nullptr, u0, e0, out);
+}
+
+int cc_multi_create_s2(int d, const double *basis, int nspecies, const int64_t *M, const int32_t *const *modes,
+                       const double *const *V, const double *const *S0, double u0, double e0, cc_multi **out)
+{
+	return multi_create(d, basis, nspecies, M, modes, V, S0, u0, e0, out);
 }
 
 int cc_multi_destroy(cc_multi *m)

@@ -312,6 +312,25 @@ def ref_multi_eval(d, basis, kcarts, Vs, u0, e0, frac, species, radii=None):
     return E.value, F[:len(frac)]
 
 
+def ref_repulsive_eval(d, basis, kcart, V, e0, sigma, frac, S0=None, nthreads=None):
+    """The reference's own RepulsiveCCPotential (plain, or S2 with targets S0): (E, F) with F Cartesian (N x d)."""
+    lib = ref_lib()
+    lib.ccref_repulsive_eval.argtypes = [ctypes.c_int, _vp, _l, _vp, _vp, _vp, _d, _d, _l, _vp, ctypes.c_int, _vp,
+                                         _vp]
+    basis = np.ascontiguousarray(basis, np.float64).reshape(d, d)
+    kcart = np.ascontiguousarray(kcart, np.float64).reshape(-1, d)
+    V = np.ascontiguousarray(V, np.float64)
+    S0 = None if S0 is None else np.ascontiguousarray(S0, np.float64)
+    frac = np.ascontiguousarray(frac, np.float64).reshape(-1, d)
+    E = _d()
+    F = np.zeros((max(len(frac), 1), d))
+    rc = lib.ccref_repulsive_eval(d, _p(basis), len(V), _p(kcart), _p(V), _p(S0), e0, sigma, len(frac), _p(frac),
+                                  nthreads or os.cpu_count() or 1, ctypes.byref(E), _p(F))
+    if rc != 0:
+        raise ValueError("the reference's RepulsiveCCPotential threw")
+    return E.value, F[:len(frac)]
+
+
 def _mspb_lib():
     lib = ref_lib()
     if not getattr(lib, "_mspb_set", False):
