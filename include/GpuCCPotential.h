@@ -11,7 +11,7 @@
  *
  * Contract kept from the reference:
  *   - constraints / Shift (and S0 for the S2 form) are the public members of the reference class; a change is seen at
- *     the next evaluation; the S2 form needs one S0 per constraint and distinct wavevectors;
+ *     the next evaluation; the S2 form needs one S0 per constraint;
  *     every k must lie on the reciprocal lattice of the bound cell (std::invalid_argument otherwise);
  *   - SetConfiguration binds a Configuration the caller keeps alive (non-owning), invalidating cached results;
  *   - EnergyAndAllForce equals Energy() followed by AllForce() bitwise (both read one cached GPU evaluation);

@@ -73,7 +73,8 @@ int cc_create_cartesian(int d, const double *basis, int64_t M, const double *k, 
 /* The S2 form, the reference's ShiftedCCPotential_S2 (potential/CollectiveCoordinatePotential.h:1642-1749, constraints
  * added by its AddConstraint(k, {V, S0})): E = sum_m V_m (|rho(k_m)|^2 / N - S0_m)^2 + shift, with no volume factor,
  * F_i = (4 / N) sum_m V_m (|rho|^2 / N - S0_m) Im(conj(rho) e^{i k.r_i}) k_m. Arguments as cc_create plus S0 (M
- * targets); modes must be distinct (CC_ERR_ARG otherwise). Evaluated in FP64 on the split rho / reduce / force path
+ * targets); a repeated mode is one slot with the weights summed, the weighted mean target and the rest of the sum
+ * in the shift (CC_ERR_ARG when its weights sum to zero but are not all zero). Evaluated in FP64 on the split rho / reduce / force path
  * whatever the precision asked; cc_set_path(CC_PATH_NUFFT), single-particle moves and batches refuse it (CC_ERR_ARG). */
 int cc_create_s2(int d, const double *basis, int64_t M, const int32_t *modes, const double *V, const double *S0,
                  double shift, cc_handle **out);
@@ -264,7 +265,7 @@ int cc_isotropic_structure_factor(int d, int64_t nconfigs, const double *bases, 
 typedef struct cc_multi cc_multi;
 int cc_multi_create(int d, const double *basis, int nspecies, const int64_t *M, const int32_t *const *modes,
                     const double *const *V, double u0, double e0, cc_multi **out);
-/* As cc_multi_create with S0[s] (M[s] targets, distinct modes) making species s's Phi_s the S2 form (cc_create_s2);
+/* As cc_multi_create with S0[s] (M[s] targets) making species s's Phi_s the S2 form (cc_create_s2);
  * a NULL S0[s] keeps that species plain. With one species, u0 = 1 and radii sigma / 2 this is the reference's
  * RepulsiveCCPotential (apps/CCOptimization/RepulsiveCCPotential.h:21-159) with an S2 kernel (S0 != 0). */
 int cc_multi_create_s2(int d, const double *basis, int nspecies, const int64_t *M, const int32_t *const *modes,

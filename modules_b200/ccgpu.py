@@ -271,7 +271,7 @@ def probe_fma_peak(precision=PREC_FP64):
 class CCPotential:
     """GPU ShiftedCCPotential over a cell ``basis`` (rows a_i) with integer ``modes`` (k = sum_e n_e b_e).
 
-    With ``S0`` (one target per mode, integer modes, distinct) it is the S2 form, the reference's ShiftedCCPotential_S2
+    With ``S0`` (one target per mode, integer modes) it is the S2 form, the reference's ShiftedCCPotential_S2
     (potential/CollectiveCoordinatePotential.h:1642-1749): E = sum_k V(k) (|rho(k)|^2 / N - S0(k))^2 + shift. With
     ``nsub`` > 1 as well, ShiftedCCPotential_S2_MultiConfig (:1756-1870): the N particles are nsub consecutive
     sub-configurations and S(k) is their mean."""

@@ -1662,13 +1662,37 @@ int cc_create_s2(int d, const double *basis, int64_t M, const int32_t *modes, co
 	if (int rc = create_common(d, basis, M, modes, V, shift, &h))
 		return rc;
 	const cc::Plan &p = h->main.plan;
-	if (p.unique_modes != M) {
-		cc_destroy(h);
-		return fail(CC_ERR_ARG, "S2 constraints need distinct modes");
+	// A repeated mode shares one slot: over its copies sum_m V_m (S - S0_m)^2 = W (S - T)^2 + C with W = sum V_m (the
+	// slot's weight), T = sum V_m S0_m / W and C = sum V_m S0_m^2 - W T^2, which joins the shift. Copies whose weights
+	// sum to zero (but are not all zero) have no such form.
+	std::vector<double> slotS0((size_t)p.nslot, 0.0), vs0((size_t)p.nslot, 0.0), vs02((size_t)p.nslot, 0.0);
+	std::vector<int> copies((size_t)p.nslot, 0);
+	std::vector<char> nonzero((size_t)p.nslot, 0);
+	for (int64_t m = 0; m < M; m++) {
+		const size_t q = (size_t)p.mode_slot[(size_t)m];
+		slotS0[q] = S0[m];
+		vs0[q] += V[m] * S0[m];
+		vs02[q] += V[m] * S0[m] * S0[m];
+		copies[q]++;
+		nonzero[q] |= V[m] != 0.0;
 	}
-	std::vector<double> slotS0((size_t)p.nslot, 0.0);
-	for (int64_t m = 0; m < M; m++)
-		slotS0[(size_t)p.mode_slot[(size_t)m]] = S0[m];
+	double extra = 0.0;
+	for (size_t q = 0; q < (size_t)p.nslot; q++) {
+		if (copies[q] < 2)
+			continue;
+		const double W = p.slotV[q];
+		if (W == 0.0) {
+			if (nonzero[q]) {
+				cc_destroy(h);
+				return fail(CC_ERR_ARG, "repeated S2 modes whose weights sum to zero");
+			}
+			slotS0[q] = 0.0;
+			continue;
+		}
+		slotS0[q] = vs0[q] / W;
+		extra += vs02[q] - W * slotS0[q] * slotS0[q];
+	}
+	h->shift += extra;
 	if (int rc = upload(&h->d_slotS0, slotS0)) {
 		cc_destroy(h);
 		return rc;

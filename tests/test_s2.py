@@ -104,6 +104,30 @@ def test_gpu_matches_reference(gpu, d, N, kmax):
 
 
 @pytest.mark.gpu
+@needs_ref
+def test_gpu_repeated_modes_match_reference(gpu):
+    """The reference keeps repeated wavevectors as separate constraints; here they share a slot with the summed
+    weight, the weighted mean target and the remainder in the shift."""
+    basis, frac, modes, V, S0 = case(2, 800, 7, 77)
+    rng = np.random.default_rng(5)
+    pick = rng.choice(len(modes), 12, replace=False)
+    modes2 = np.vstack([modes, modes[pick], modes[pick[:4]]])
+    V2 = np.concatenate([V, rng.uniform(0.1, 1.0, 12), rng.uniform(-0.05, 0.5, 4)])
+    S02 = np.concatenate([S0, rng.uniform(0.0, 2.0, 16)])
+    ref = oracle.Ref(2, basis, V2, modes=modes2, shift=0.2, S0=S02)
+    ref.set_positions(frac)
+    Eref, Fref, re, im = ref.eval()
+    k = oracle.lattice_k(basis, modes2)
+    dS = (re * re + im * im) / len(frac) - S02
+    sE, sF = tol_scales(V2, dS, re, im, k, len(frac))
+    p = gpu.CCPotential(2, basis, modes2, V2, 0.2, S0=S02)
+    p.set_configuration(frac)
+    E, F = p.energy_and_forces()
+    assert abs(E - Eref) <= RTOL * sE, (E, Eref)
+    assert np.abs(F - Fref).max() <= RTOL * sF
+
+
+@pytest.mark.gpu
 def test_gpu_fp64_only_and_refusals(gpu):
     basis, frac, modes, V, S0 = case(2, 3000, 8, 5)
     p = gpu.CCPotential(2, basis, modes, V, 0.0, S0=S0)
@@ -120,8 +144,8 @@ def test_gpu_fp64_only_and_refusals(gpu):
         p.try_move(frac[0], (frac[0] + 0.01) % 1.0)
     with pytest.raises(gpu.CCError):
         gpu.CCBatch([p], [len(frac)])
-    with pytest.raises(gpu.CCError):
-        gpu.CCPotential(2, basis, np.vstack([modes, modes[:1]]), np.append(V, 1.0), 0.0, S0=np.append(S0, 0.5))
+    with pytest.raises(gpu.CCError):   # copies of a mode whose weights cancel have no S2 form
+        gpu.CCPotential(2, basis, np.vstack([modes, modes[:1]]), np.append(V, -V[0]), 0.0, S0=np.append(S0, 0.5))
     with pytest.raises(ValueError):
         gpu.CCPotential(2, basis, modes, V, 0.0, S0=S0[:-1])
 
