@@ -2,7 +2,8 @@
 
 Two CPU checkers of the collective-coordinate path:
   * ``Ref``  — the reference's own ShiftedCCPotential / LuksanPLIS compiled from its sources (oracle/_ref/libccref.so,
-    built by oracle/Makefile where the reference tree is present);
+    built by oracle/Makefile where the reference tree is present), with its S2, multi-configuration, varBox
+    (``RefVarBox``), multi-species, RepulsiveCCPotential, IsotropicStructureFactor and MSPB code;
   * ``port`` — the plain-C restatement oracle/cc_oracle.c (oracle/_build/libccoracle.so), pinned to the reference by
     tests/test_oracle.py and the golden vectors in tests/golden/.
 Nothing on the product path imports this package.

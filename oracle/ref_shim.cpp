@@ -10,7 +10,10 @@
 //   - Configuration (PeriodicCellList<AtomName>): Insert with the double floor wrap and the Cartesian
 //       coordinates sum_i s_i a_i (core/PeriodicCellList.h:517-538, :88-98), the reciprocal basis (:999-)
 //       and the reciprocal-lattice cell list used for the k-set enumeration;
-//   - LuksanPLIS (potential/LuksanPLIS.cpp), the L-BFGS the structure optimiser calls.
+//   - LuksanPLIS (potential/LuksanPLIS.cpp), the L-BFGS the structure optimiser calls;
+//   - ShiftedCCPotential_S2 and ShiftedCCPotential_S2_MultiConfig (potential/CollectiveCoordinatePotential.h:1642-1870)
+//     and the named variable-cell classes of potential/CCPotential_Kernels.h with their constraint generation
+//     (potential/CCPotential_varBox.h:129-202; its GSL-based cell derivatives link against throwing stand-ins).
 // What is restated here, because its translation unit needs GSL/NLopt/Boost that this machine lacks:
 //   - the Switch-0 objective (potential/StructureOptimization.cpp:339-350 FillParticles, :447-536 Objective)
 //     and the three-pass driver (:1046-1090, RelaxStructure_NLOPT and RelaxStructure_NLOPT_Emin);
