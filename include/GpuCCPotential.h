@@ -1,10 +1,11 @@
-/* GpuCCPotential.h — drop-in GPU replacements for the reference's ShiftedCCPotential and ShiftedCCPotential_S2
- * (header-only C++ adapter).
+/* GpuCCPotential.h — drop-in GPU replacements for the reference's ShiftedCCPotential, ShiftedCCPotential_S2 and
+ * ShiftedCCPotential_S2_MultiConfig (header-only C++ adapter).
  *
  * Include it in code built against the reference (it needs potential/CollectiveCoordinatePotential.h and
  * potential/CombinedEnergyForce.h on the include path) and link libccgpu.so. GpuCCPotential derives from
  * ShiftedCCPotential (potential/CollectiveCoordinatePotential.h:53-1497), GpuCCPotential_S2 from ShiftedCCPotential_S2
- * (:1642-1749; its AddConstraint(k, {V, S0}) and public S0 list are the reference's), both also from
+ * (:1642-1749; its AddConstraint(k, {V, S0}) and public S0 list are the reference's), GpuCCPotential_S2_MultiConfig
+ * from ShiftedCCPotential_S2_MultiConfig (:1756-1870; constraints and S0 pushed onto its public lists), all also from
  * CombinedEnergyForce (potential/CombinedEnergyForce.h), so the structure optimiser's Objective
  * (potential/StructureOptimization.cpp:447-536) finds EnergyAndAllForce by dynamic_cast and makes one GPU evaluation
  * per step; MD/MC drivers call Energy / AllForce / Force as before.
@@ -15,7 +16,8 @@
  *     every k must lie on the reciprocal lattice of the bound cell (std::invalid_argument otherwise);
  *   - SetConfiguration binds a Configuration the caller keeps alive (non-owning), invalidating cached results;
  *   - EnergyAndAllForce equals Energy() followed by AllForce() bitwise (both read one cached GPU evaluation);
- *   - GetRho fills RhoReal / RhoImag and sets RhoValid;
+ *   - GetRho fills RhoReal / RhoImag and sets RhoValid (not for the multi-configuration form, whose rho is per
+ *     sub-configuration: std::invalid_argument);
  *   - one object is not evaluated from several threads at once.
  * Errors of the C ABI become std::invalid_argument (CC_ERR_ARG, CC_ERR_NONLATTICE), std::logic_error (CC_ERR_STATE)
  * or std::runtime_error (the rest).
@@ -59,6 +61,9 @@ template <class Base> class GpuCCAdapter : public Base, public CombinedEnergyFor
 	// the targets of the S2 form; none for the plain form
 	static const std::vector<double> *Targets(const ShiftedCCPotential &) { return nullptr; }
 	static const std::vector<double> *Targets(const ShiftedCCPotential_S2 &p) { return &p.S0; }
+	static const std::vector<double> *Targets(const ShiftedCCPotential_S2_MultiConfig &p) { return &p.S0; }
+	static int SubConfigs(const ShiftedCCPotential &) { return 1; }
+	static int SubConfigs(const ShiftedCCPotential_S2_MultiConfig &p) { return (int)p.NSubConfig; }
 
 	// (Re)create the handle when the constraints, Shift or the cell changed; upload positions when dirty.
 	void Sync()
@@ -90,6 +95,8 @@ template <class Base> class GpuCCAdapter : public Base, public CombinedEnergyFor
 			else
 				Check(cc_create_cartesian(d, basis.data(), (int64_t)V.size(), k.data(), V.data(), this->Shift,
 				                          &handle_));
+			if (SubConfigs(*this) > 1)
+				Check(cc_set_subconfigurations(handle_, SubConfigs(*this)));
 			if (S0)
 				s0copy_ = *S0;
 			kcopy_.swap(k);
@@ -123,6 +130,7 @@ template <class Base> class GpuCCAdapter : public Base, public CombinedEnergyFor
 public:
 	explicit GpuCCAdapter(DimensionType dimension) : Base(dimension) {}
 	explicit GpuCCAdapter(const Base &src) : Base(src) {}
+	GpuCCAdapter(DimensionType dimension, size_t nsub) : Base(dimension, nsub) {}   // the multi-configuration form
 	GpuCCAdapter(const GpuCCAdapter &) = delete;
 	GpuCCAdapter &operator=(const GpuCCAdapter &) = delete;
 	virtual ~GpuCCAdapter() { cc_destroy(handle_); }
@@ -199,6 +207,19 @@ class GpuCCPotential_S2 : public GpuCCAdapter<ShiftedCCPotential_S2>
 public:
 	explicit GpuCCPotential_S2(DimensionType dimension) : GpuCCAdapter<ShiftedCCPotential_S2>(dimension) {}
 	explicit GpuCCPotential_S2(const ShiftedCCPotential_S2 &src) : GpuCCAdapter<ShiftedCCPotential_S2>(src) {}
+};
+
+class GpuCCPotential_S2_MultiConfig : public GpuCCAdapter<ShiftedCCPotential_S2_MultiConfig>
+{
+public:
+	GpuCCPotential_S2_MultiConfig(DimensionType dimension, size_t nsub)
+	    : GpuCCAdapter<ShiftedCCPotential_S2_MultiConfig>(dimension, nsub)
+	{
+	}
+	explicit GpuCCPotential_S2_MultiConfig(const ShiftedCCPotential_S2_MultiConfig &src)
+	    : GpuCCAdapter<ShiftedCCPotential_S2_MultiConfig>(src)
+	{
+	}
 };
 
 #endif

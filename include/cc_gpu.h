@@ -88,6 +88,11 @@ int cc_create_s2(int d, const double *basis, int64_t M, const int32_t *modes, co
 int cc_create_s2_multiconfig(int d, const double *basis, int64_t M, const int32_t *modes, const double *V,
                              const double *S0, double shift, int nsub, cc_handle **out);
 
+/* The sub-configuration count of an S2 handle (cc_create_s2 / cc_create_s2_cartesian): nsub > 1 makes it the
+ * multi-configuration form of cc_create_s2_multiconfig, 1 the S2 form. CC_ERR_ARG for a plain handle with
+ * constraints, nsub < 1, or bound positions whose count is not a multiple of nsub. */
+int cc_set_subconfigurations(cc_handle *h, int nsub);
+
 /* As cc_create_s2 with Cartesian k (M x d), mapped to modes as in cc_create_cartesian. */
 int cc_create_s2_cartesian(int d, const double *basis, int64_t M, const double *k, const double *V, const double *S0,
                            double shift, cc_handle **out);

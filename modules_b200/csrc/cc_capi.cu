@@ -1712,6 +1712,19 @@ int cc_create_s2_multiconfig(int d, const double *basis, int64_t M, const int32_
 	return CC_OK;
 }
 
+int cc_set_subconfigurations(cc_handle *h, int nsub)
+{
+	if (int rc = check_handle(h))
+		return rc;
+	if (nsub < 1 || (nsub > 1 && !h->d_slotS0 && !h->V.empty()))
+		return fail(CC_ERR_ARG, "sub-configurations belong to an S2 handle; their count must be positive");
+	if (h->N > 0 && h->N % nsub)
+		return fail(CC_ERR_ARG, "the particle count is not a multiple of the number of sub-configurations");
+	h->nsub = nsub;
+	g_alloc_gen++;   // captured evaluations hold the old form
+	return CC_OK;
+}
+
 int cc_create_s2_cartesian(int d, const double *basis, int64_t M, const double *k, const double *V, const double *S0,
                            double shift, cc_handle **out)
 {

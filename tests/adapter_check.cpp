@@ -11,6 +11,8 @@
 //   4. GpuCCPotential_S2 against the reference's ShiftedCCPotential_S2 (constraints through AddConstraint(k, {V, S0}))
 //      on a skew 2D cell: Energy and AllForce within 1e-10 of the S2 rounding scales, Force(i), EnergyAndAllForce
 //      bitwise, and a changed S0 seen at the next evaluation.
+//   5. GpuCCPotential_S2_MultiConfig against the reference's ShiftedCCPotential_S2_MultiConfig (3 sub-configurations,
+//      skew 3D cell): Energy and AllForce within 1e-10 of the S2 rounding scales.
 // Prints one line per check and exits 0 only if all pass.
 #include "GpuCCPotential.h"
 #include "GpuMultiStealthyPotential.h"
@@ -287,6 +289,55 @@ int main()
 		ref.RhoValid = false;
 		const double Er2 = ref.Energy(), Eg2 = gpu.Energy();
 		check(Er2 != Er && std::abs(Er2 - Eg2) <= 1e-10 * sE, "S2 target change seen", Eg2, Er2);
+	}
+	// ---- 5. the multi-configuration S2 form against the reference's class ------------------------------------------
+	{
+		const int d = 3, nsub = 3, n = 3 * 40;
+		Configuration c = make_config(d, {6.0, 0.0, 0.0, 1.0, 5.5, 0.0, -0.5, 0.75, 6.5}, n, rng);
+		ShiftedCCPotential_S2_MultiConfig ref(d, nsub);
+		GpuCCPotential_S2_MultiConfig gpu(d, nsub);
+		std::uniform_real_distribution<double> uv(0.2, 2.0), us(0.0, 1.5);
+		for (int a = -2; a <= 2; a++)
+			for (int b = -2; b <= 2; b++)
+				for (int e = -2; e <= 2; e++) {
+					if (a < 0 || (a == 0 && (b < 0 || (b == 0 && e <= 0))))
+						continue;
+					GeometryVector k(d);
+					k.AddFrom((double)a * c.GetReciprocalBasisVector(0));
+					k.AddFrom((double)b * c.GetReciprocalBasisVector(1));
+					k.AddFrom((double)e * c.GetReciprocalBasisVector(2));
+					const double V = uv(rng), S0 = us(rng);
+					ref.constraints.emplace_back(k, V);
+					ref.S0.push_back(S0);
+					gpu.constraints.emplace_back(k, V);
+					gpu.S0.push_back(S0);
+				}
+		ref.SetConfiguration(c);
+		gpu.SetConfiguration(c);
+		const double Er = ref.Energy(), Eg = gpu.Energy();
+		const int np = n / nsub;
+		double sE = 0, sF = 0;
+		for (size_t q = 0; q < ref.constraints.size(); q++) {
+			double r2 = 0;
+			for (int s = 0; s < nsub; s++) {
+				const size_t at = (size_t)s * ref.constraints.size() + q;
+				r2 += ref.RhoReal[at] * ref.RhoReal[at] + ref.RhoImag[at] * ref.RhoImag[at];
+			}
+			const double dS = std::abs(ref.Snow[q] - ref.S0[q]) + 1;
+			sE += std::abs(ref.constraints[q].V) * dS * dS;
+			sF += 4.0 / np * std::abs(ref.constraints[q].V) * dS * (std::sqrt(r2) + 1) *
+			      std::sqrt(ref.constraints[q].k.Modulus2());
+		}
+		check(std::abs(Er - Eg) <= 1e-10 * sE, "S2 multi-configuration Energy", Eg, Er);
+		std::vector<GeometryVector> fr, fg;
+		ref.AllForce(fr);
+		gpu.AllForce(fg);
+		double worst = 0;
+		for (size_t i = 0; i < fr.size(); i++)
+			for (int j = 0; j < d; j++)
+				worst = std::max(worst, std::abs(fr[i].x[j] - fg[i].x[j]));
+		check(fg.size() == fr.size() && worst <= 1e-10 * sF, "S2 multi-configuration AllForce max |dF| / scale",
+		      worst / sF, 1e-10);
 	}
 	std::printf(failures ? "ADAPTER FAIL\n" : "ADAPTER OK\n");
 	return failures ? 1 : 0;
