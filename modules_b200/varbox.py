@@ -159,3 +159,9 @@ class VarBoxPotential:
     def minimize(self, frac, **kw):
         """Device L-BFGS over the positions at the bound cell (see CCPotential.minimize)."""
         return self.pot.minimize(frac, **kw)
+
+    def close(self):
+        if self.pot is not None:
+            self.pot.close()
+            self.pot = None
+            self._key = None

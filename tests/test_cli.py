@@ -86,6 +86,14 @@ def test_selection_and_weights(type_, d):
     assert np.allclose(S0, want, rtol=1e-12, atol=1e-15)
 
 
+def test_type_arguments_are_checked():
+    from modules_b200 import cli
+    basis = cell(2, 300)
+    for kw in (dict(type_=15, S0=0.5), dict(type_=101), dict(type_=18), dict(type_=14), dict(type_=17, S0=0.5)):
+        with pytest.raises(ValueError):
+            cli.generate_potential(d=2, basis=basis, N=300, **kw)
+
+
 def test_repeated_points_merge():
     """A cell whose first points lie beyond |k| = 1.1: the growing collection appends them again at every step; they
     become one constraint each with the weight times the count."""
