@@ -13,9 +13,12 @@
 //      bitwise, and a changed S0 seen at the next evaluation.
 //   5. GpuCCPotential_S2_MultiConfig against the reference's ShiftedCCPotential_S2_MultiConfig (3 sub-configurations,
 //      skew 3D cell): Energy and AllForce within 1e-10 of the S2 rounding scales.
+//   6. GpuRepulsiveCCPotential against the reference's RepulsiveCCPotential (GetCCO's potential) with the plain and
+//      the S2 kernel on a skew 2D cell with contacts: Energy and AllForce within 1e-10 of max(1, |E|) and max(1, |F|).
 // Prints one line per check and exits 0 only if all pass.
 #include "GpuCCPotential.h"
 #include "GpuMultiStealthyPotential.h"
+#include "GpuRepulsiveCCPotential.h"
 #include "LuksanPLIS.h"
 
 #include <cmath>
@@ -338,6 +341,45 @@ int main()
 				worst = std::max(worst, std::abs(fr[i].x[j] - fg[i].x[j]));
 		check(fg.size() == fr.size() && worst <= 1e-10 * sF, "S2 multi-configuration AllForce max |dF| / scale",
 		      worst / sF, 1e-10);
+	}
+	// ---- 6. RepulsiveCCPotential, plain and S2 kernels -----------------------------------------------------------
+	for (int withS0 = 0; withS0 < 2; withS0++) {
+		const int d = 2, n = 90;
+		Configuration c = make_config(d, {10.0, 0.0, 2.5, 9.0}, n, rng);
+		std::streambuf *saved = std::cout.rdbuf(nullptr);   // the reference reports its set-up on stdout
+		RepulsiveCCPotential ref(d, 1.25, 0.9, withS0 ? 1.0 : 0.0);
+		GpuRepulsiveCCPotential gpu(d, 1.25, 0.9, withS0 ? 1.0 : 0.0);
+		std::cout.rdbuf(saved);
+		for (int a = 0; a <= 4; a++)
+			for (int b = -4; b <= 4; b++) {
+				if (a == 0 && b <= 0)
+					continue;
+				GeometryVector k(d);
+				k.AddFrom((double)a * c.GetReciprocalBasisVector(0));
+				k.AddFrom((double)b * c.GetReciprocalBasisVector(1));
+				std::vector<double> vals{1.0 / (1.0 + a + std::abs(b))};
+				if (withS0)
+					vals.push_back(0.7);
+				ref.CCPotential->AddConstraint(k, vals);
+				gpu.CCPotential->AddConstraint(k, vals);
+			}
+		ref.SetConfiguration(c);
+		gpu.SetConfiguration(c);
+		const double Er = ref.Energy(), Eg = gpu.Energy();
+		check(std::abs(Er - Eg) <= 1e-10 * std::max(1.0, std::abs(Er)),
+		      withS0 ? "Repulsive (S2 kernel) Energy" : "Repulsive Energy", Eg, Er);
+		std::vector<GeometryVector> fr, fg;
+		ref.AllForce(fr);
+		gpu.AllForce(fg);
+		double worst = 0, fmax = 1.0;
+		for (size_t i = 0; i < fr.size(); i++)
+			for (int j = 0; j < d; j++) {
+				worst = std::max(worst, std::abs(fr[i].x[j] - fg[i].x[j]));
+				fmax = std::max(fmax, std::abs(fr[i].x[j]));
+			}
+		check(fg.size() == fr.size() && worst <= 1e-10 * fmax,
+		      withS0 ? "Repulsive (S2 kernel) AllForce max |dF| / max(1,|F|)" : "Repulsive AllForce max |dF| / max(1,|F|)",
+		      worst / fmax, 1e-10);
 	}
 	std::printf(failures ? "ADAPTER FAIL\n" : "ADAPTER OK\n");
 	return failures ? 1 : 0;
