@@ -40,16 +40,22 @@ UNIT = "evals/s"
 NCU_TRAFFIC_BYTES = {"cc_force_kernel": 0.144e6, "cc_rho_kernel": 0.078e6, "cc_reduce_kernel": 1.418e6}
 WORKLOAD = "3D stealthy CC ground-state evaluation: N=2000 uniform in a periodic cube (unit density), chi=0.45, " \
            "M=2724 half-space k (v=1), FP64 energy + Cartesian forces"
+DATA = "synthetic (seeded uniform positions; k-set of the reference CLI's Type 0 rule)"
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20000)
-    ap.add_argument("--warmup", type=int, default=500)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--pool", type=int, default=3072, help="distinct configurations cycled through (> L2)")
+    ap.add_argument("--path", default="auto", choices=["auto", "split", "fused"],
+                    help="evaluation path of the headline (auto: the library's own choice for this size)")
+    ap.add_argument("--pool", type=int, default=4096,
+                    help="configurations per step: each step evaluates every one once (their positions exceed L2)")
+    ap.add_argument("--ref-seconds", type=float, default=120.0,
+                    help="reference arm: about this many seconds of evaluations over warm-up and timed steps")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched / ground-state / served measurements")
@@ -92,7 +98,7 @@ class Clocks:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                       "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                       "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
 
@@ -126,43 +132,89 @@ class Clocks:
                 "samples": len(rows), "reasons": sorted(reasons)}
 
 
-def cpu_reference_rate(seconds, steps=None, warmup=1):
-    """The reference's Direct path (oracle/_ref): evaluations/s on all host cores for this workload."""
+POOL_SEED = 1234
+
+
+def pool_positions(P, rank=0):
+    """The P distinct configurations of one step (seeded uniform fractional positions, P x N x D)."""
+    return np.random.default_rng(POOL_SEED + rank).random((P, N, D))
+
+
+def workload_config(M, P):
+    """The workload as both arms print it (same keys, same values)."""
+    return {"workload": WORKLOAD, "N": N, "d": D, "chi": CHI, "M": M, "pairs_per_eval": N * M,
+            "configs_per_step": P, "positions_seed": POOL_SEED,
+            "l2": f"inputs larger than L2: each step evaluates {P} distinct configurations "
+                  f"({P * N * D * 8 / 1e6:.0f} MB of positions)"}
+
+
+def reference_potential(cores):
+    """The reference's own ShiftedCCPotential (Direct path, oracle/_ref) on this workload's k-set, built by the
+    reference's own CLI rule (GeneratePotential Type 0)."""
     import oracle
     if not oracle.ref_available():
         raise RuntimeError("oracle/_ref/libccref.so is not built")
-    import modules_b200 as cc
-    modes, V = cc.stealthy_kset(D, np.eye(D) * SIDE, N, CHI)
+    basis = np.eye(D) * SIDE
+    modes, V = oracle.ref_kset(D, basis, N, CHI, 0)
+    return oracle.Ref(D, basis, V, modes=modes, nthreads=cores), len(V)
+
+
+def cpu_reference_rate(seconds, pool):
+    """The reference's Direct path on all host cores: SetConfiguration + Energy + AllForce per configuration of the
+    pool, in order, for about `seconds`. Returns (evals/s, cores, evals, seconds)."""
     cores = os.cpu_count() or 1
-    ref = oracle.Ref(D, np.eye(D) * SIDE, V, modes=modes, nthreads=cores)
-    rng = np.random.default_rng(99)
-    pool = [rng.random((N, D)) for _ in range(4)]
-    for i in range(warmup):
-        ref.set_positions(pool[i % 4])
-        ref.eval()
+    ref, _M = reference_potential(cores)
+    ref.set_positions(pool[0])
+    ref.eval()
     n = 0
     t0 = time.perf_counter()
     while True:
-        ref.set_positions(pool[n % 4])
+        ref.set_positions(pool[n % len(pool)])
         ref.eval()
         n += 1
         el = time.perf_counter() - t0
-        if (steps is not None and n >= steps) or (steps is None and el >= seconds and n >= 3):
+        if el >= seconds and n >= 3:
             break
     return n / el, cores, n, el
 
 
 def run_reference(args):
+    """The reference arm: the reference's own CPU path on this workload. A step of the workload is one evaluation of
+    each of the step's P configurations; the reference evaluates a bounded sample of each step (the first S of its
+    configurations, S fixed so that warm-up and timed steps take about --ref-seconds in all)."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    rate, cores, n, el = cpu_reference_rate(None, steps=args.steps, warmup=args.warmup)
+    cores = os.cpu_count() or 1
+    ref, M = reference_potential(cores)
+    P = args.pool
+    pool = pool_positions(P)
+    t0 = time.perf_counter()
+    for i in range(2):
+        ref.set_positions(pool[i])
+        ref.eval()
+    t_eval = (time.perf_counter() - t0) / 2
+    steps, warm = args.steps, args.warmup
+    S = int(max(1, min(P, args.ref_seconds / max(1, steps + warm) / t_eval)))
+
+    def one_step():
+        for i in range(S):
+            ref.set_positions(pool[i])
+            ref.eval()
+
+    for _ in range(warm):
+        one_step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one_step()
+    el = time.perf_counter() - t0
+    rate = steps * S / el
+    sample = (f"each step: the first {S} of its {P} configurations (SetConfiguration+Energy+AllForce, reference "
+              f"Direct path, OpenMP over {cores} threads); {steps} steps, {steps * S} evaluations in {el:.1f} s")
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / n, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded uniform positions)",
-            "config": {"workload": WORKLOAD, "N": N, "d": D, "chi": CHI, "M": 2724},
-            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
-                             "sample": f"{n} evaluations (SetConfiguration+Energy+AllForce), {el:.1f} s"},
+            "steps": steps, "warmup": warm, "ms_per_step": 1e3 * el / steps * (P / S), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA, "config": workload_config(M, P),
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
             "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -374,27 +426,27 @@ def run_ours(args):
     modes, V = cc.stealthy_kset(D, basis, N, CHI)
     M = len(V)
     pot = cc.CCPotential(D, basis, modes, V)
+    path = {"auto": cc.PATH_AUTO, "split": cc.PATH_SPLIT, "fused": cc.PATH_FUSED}[args.path]
+    pot.set_path(path)
     P = args.pool
-    rng = np.random.default_rng(1234 + rank)
-    host_pool = rng.random((P, N, D))
+    host_pool = pool_positions(P, rank)
     dev = torch.device("cuda", local)
     pool = torch.tensor(host_pool, dtype=torch.float64, device=dev)
     E = torch.zeros(P, dtype=torch.float64, device=dev)
     F = torch.zeros_like(pool)
     side = torch.cuda.Stream(device=dev)
 
-    def step(i, stream):
-        j = i % P
-        pot.energy_grad_device(N, pool[j].data_ptr(), E[j:j + 1].data_ptr(), F[j].data_ptr(), precision=prec,
+    def evaluate(i, stream):
+        pot.energy_grad_device(N, pool[i].data_ptr(), E[i:i + 1].data_ptr(), F[i].data_ptr(), precision=prec,
                                stream=stream)
 
-    # warm-up (also allocates the library's work buffers before any capture)
+    # first evaluations allocate the library's work buffers (before any capture)
     with torch.cuda.stream(side):
-        for i in range(max(args.warmup, 3)):
-            step(i, side.cuda_stream)
+        for i in range(3):
+            evaluate(i, side.cuda_stream)
     torch.cuda.synchronize()
 
-    # CUDA graphs of G consecutive steps covering the pool
+    # one step = one evaluation of each of the P configurations: CUDA graphs of G consecutive evaluations
     G = 128
     graphs = []
     for g0 in range(0, P, G):
@@ -402,28 +454,22 @@ def run_ours(args):
         with torch.cuda.graph(g, stream=side):
             cs = torch.cuda.current_stream().cuda_stream
             for i in range(g0, min(P, g0 + G)):
-                step(i, cs)
+                evaluate(i, cs)
         graphs.append(g)
     torch.cuda.synchronize()
 
-    def run_steps(K, stream):
-        done = 0
-        gi = 0
-        while done + G <= K:
-            graphs[gi % len(graphs)].replay()
-            gi += 1
-            done += G
-        with torch.cuda.stream(stream):
-            while done < K:
-                step(done, stream.cuda_stream)
-                done += 1
+    def run_step():
+        for g in graphs:
+            g.replay()
 
     with torch.cuda.stream(side):
-        run_steps(min(args.warmup, 4 * G) + G, side)
+        for _ in range(max(args.warmup, 3)):
+            run_step()
     torch.cuda.synchronize()
 
     K = args.steps
     clocks = Clocks(local)
+    time.sleep(0.3)   # the sampler is running before the timed region starts
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -431,68 +477,80 @@ def run_ours(args):
     t_end = torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(side):
         t_start.record(side)
-        run_steps(K, side)
+        for _ in range(K):
+            run_step()
         t_end.record(side)
     torch.cuda.synchronize()
     ms = t_start.elapsed_time(t_end)
     clk = clocks.stop()
     ms = max_over_ranks(ms, dev)
-    value = replica_rate(K, ms / 1e3, world)
+    value = replica_rate(K * P, ms / 1e3, world)
+    pot.check_device_error()
 
-    # per-kernel CUDA-event timing: events recorded around each kernel INSIDE a replayed CUDA graph of G steps (so no
-    # host launch gap falls between an event and its kernel); the events are created before the capture
+    # per-kernel CUDA-event timing: events recorded around each kernel INSIDE a replayed CUDA graph of G evaluations
+    # (no host launch gap falls between an event and its kernel); the events are created before the capture
     pot.set_timing(True)
     with torch.cuda.stream(side):
         for i in range(G):
-            step(i, side.cuda_stream)
+            evaluate(i, side.cuda_stream)
     pot.get_timing()
     pot.set_timing(True)
     tg = torch.cuda.CUDAGraph()
     with torch.cuda.graph(tg, stream=side):
         cs = torch.cuda.current_stream().cuda_stream
         for i in range(G):
-            step(i, cs)
+            evaluate(i, cs)
     pot.set_timing(False)
     torch.cuda.synchronize()
     with torch.cuda.stream(side):
         tg.replay()
+    torch.cuda.synchronize()
     rho_ms, red_ms, force_ms, nt = pot.get_timing()
     del tg
+    info = pot.plan_info(N)
+    info["path"] = pot.eval_path(N, prec)
     pairs = N * M
-    rho_flops, force_flops = 8.0 * pairs, (9.0 + 2 * D) * pairs
     t_rho, t_red, t_force = rho_ms / nt, red_ms / nt, force_ms / nt
     peak = cc.probe_fma_peak(cc.PREC_FP64 if prec == cc.PREC_FP64 else cc.PREC_MIXED)
-    if t_force >= t_rho:
-        dom, fl, tk = "cc_force_kernel", force_flops, t_force
+    one_kernel = info["path"] == "fused"
+    if one_kernel:
+        dom, fl, tk = "cc_fused_kernel", (17.0 + 2 * D) * pairs, t_force
+        kernel_ms = {"cc_fused_kernel": t_force}
+        launches_per_eval = 1
     else:
-        dom, fl, tk = "cc_rho_kernel", rho_flops, t_rho
+        rho_flops, force_flops = 8.0 * pairs, (9.0 + 2 * D) * pairs
+        if t_force >= t_rho:
+            dom, fl, tk = "cc_force_kernel", force_flops, t_force
+        else:
+            dom, fl, tk = "cc_rho_kernel", rho_flops, t_rho
+        kernel_ms = {"cc_rho_kernel": t_rho, "cc_reduce_kernel": t_red, "cc_force_kernel": t_force}
+        launches_per_eval = 3
     achieved = fl / (tk * 1e-3) / 1e12
 
-    # end to end through the C ABI with host buffers
-    KE = K
-    host_F = np.zeros((N, D))
+    # end to end through the C ABI with host buffers: per evaluation the positions go in (cc_set_positions) and E
+    # and F come out (cc_energy_grad); the same K steps of P configurations
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
     t0 = time.perf_counter()
-    for i in range(KE):
-        pot.set_configuration(host_pool[i % P])
-        e_, _ = pot.energy_and_forces(precision=prec)
+    for _ in range(K):
+        for i in range(P):
+            pot.set_configuration(host_pool[i])
+            pot.energy_and_forces(precision=prec)
     e2e_s = max_over_ranks(time.perf_counter() - t0, dev)
-    e2e = replica_rate(KE, e2e_s, world)
+    e2e = replica_rate(K * P, e2e_s, world)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            rate, cores, n, el = cpu_reference_rate(args.cpu_seconds)
+            rate, cores, n, el = cpu_reference_rate(args.cpu_seconds, host_pool)
             cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
-                   "sample": f"{n} evaluations of the same workload (SetConfiguration+Energy+AllForce, "
-                             f"reference Direct path, OpenMP over {cores} threads), {el:.1f} s"}
+                   "sample": f"{n} evaluations of the step's configurations in order (SetConfiguration+Energy+"
+                             f"AllForce, reference Direct path, OpenMP over {cores} threads), {el:.1f} s"}
         except Exception as exc:  # the baseline is a report, never a reason to drop the GPU line
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"unavailable: {exc}"}
 
-    info = pot.plan_info(N)
     extras = {}
     if rank == 0 and world == 1 and not args.no_extras:
         try:
@@ -503,24 +561,26 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
                 "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if prec == cc.PREC_FP64 else "f32-recurrence/f64-accumulate",
-                "data": "synthetic (seeded uniform positions, random k-set of the CLI rule)",
-                "config": {"workload": WORKLOAD, "N": N, "d": D, "chi": CHI, "M": M, "pairs_per_eval": pairs,
-                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                           "l2": f"inputs larger than L2: {P} distinct configurations "
-                                 f"({P * N * D * 8 / 1e6:.0f} MB) cycled round-robin",
-                           "graphs": f"CUDA graphs of {G} steps", "segment_len": info["L"],
-                           "segments": info["nseg"], "rho_splits": info["nsplit"], "force_splits": info["nksplit"]},
+                "data": DATA, "config": workload_config(M, P),
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                "method": {"path": info["path"], "graphs": f"CUDA graphs of {G} evaluations, {len(graphs)} per step",
+                           "segment_len": info["L"], "segments": info["nseg"], "rho_splits": info["nsplit"],
+                           "force_splits": info["nksplit"]},
                 "pairs_per_s": value * pairs,
-                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": N * D * 8,
-                        "d2h_bytes_per_step": N * D * 8 + 8},
-                "gpu_launches": 3 * K,
+                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": P * N * D * 8,
+                        "d2h_bytes_per_step": P * (N * D * 8 + 8)},
+                "gpu_launches": launches_per_eval * K * P,
                 "roofline": {"bound": "fp64_fma" if prec == cc.PREC_FP64 else "fp32_fma", "kernel": dom,
                              "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                             "peak_source": "measured in this run: FMA-chain probe kernel (cc_probe_fma_peak)",
+                             "peak_source": "measured in this run: FMA-chain probe kernel (cc_probe_fma_peak); "
+                                            "MEASURED_PEAKS.json has no FP64 figure",
                              "flops_per_launch": fl, "launch_ms": tk, "traffic": NCU_TRAFFIC_BYTES.get(dom),
-                             "traffic_unit": "bytes per launch (ncu capture)",
-                             "kernel_ms": {"cc_rho_kernel": t_rho, "cc_reduce_kernel": t_red,
-                                           "cc_force_kernel": t_force}},
+                             "traffic_unit": "bytes per launch (ncu capture)", "kernel_ms": kernel_ms,
+                             "timing": "CUDA events around each kernel inside a replayed graph; under programmatic "
+                                       "dependent launch consecutive kernels overlap, so the intervals overlap and "
+                                       "sum to more than the evaluation"
+                                       if not one_kernel else "CUDA events around the kernel inside a replayed graph",
+                             "eval_us": 1e3 * ms / (K * P)},
                 "clocks": clk, "cpu_baseline": cpu}
         line.update(extras)
         print(json.dumps(line), flush=True)

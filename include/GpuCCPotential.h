@@ -39,6 +39,7 @@ template <class Base> class GpuCCAdapter : public Base, public CombinedEnergyFor
 	cc_handle *handle_ = nullptr;
 	std::vector<double> kcopy_, vcopy_, s0copy_, basis_;   // the constraint set and cell the handle was built from
 	double shift_copy_ = 0.0;
+	int nsub_copy_ = 1;   // sub-configurations applied to the handle (NSubConfig of the multi-configuration form)
 	std::vector<double> frac_, forces_;
 	double energy_ = 0.0;
 	bool positions_dirty_ = true, result_valid_ = false;
@@ -95,8 +96,7 @@ template <class Base> class GpuCCAdapter : public Base, public CombinedEnergyFor
 			else
 				Check(cc_create_cartesian(d, basis.data(), (int64_t)V.size(), k.data(), V.data(), this->Shift,
 				                          &handle_));
-			if (SubConfigs(*this) > 1)
-				Check(cc_set_subconfigurations(handle_, SubConfigs(*this)));
+			nsub_copy_ = 1;   // a new handle starts with one configuration; NSubConfig is applied below
 			if (S0)
 				s0copy_ = *S0;
 			kcopy_.swap(k);
@@ -104,6 +104,12 @@ template <class Base> class GpuCCAdapter : public Base, public CombinedEnergyFor
 			basis_.swap(basis);
 			shift_copy_ = this->Shift;
 			positions_dirty_ = true;
+		}
+		// NSubConfig is a public member of the reference class: a change takes effect at the next evaluation
+		if (SubConfigs(*this) != nsub_copy_) {
+			Check(cc_set_subconfigurations(handle_, SubConfigs(*this)));
+			nsub_copy_ = SubConfigs(*this);
+			result_valid_ = false;
 		}
 		if (positions_dirty_) {
 			const size_t n = c.NumParticle();

@@ -28,6 +28,7 @@
 #include <cmath>
 #include <stdexcept>
 #include <string>
+#include <typeinfo>
 #include <vector>
 
 class GpuRepulsiveCCPotential : public RepulsiveCCPotential, public CombinedEnergyForce
@@ -71,24 +72,32 @@ class GpuRepulsiveCCPotential : public RepulsiveCCPotential, public CombinedEner
 			}
 			V.push_back(q.V);
 		}
+		// the two kernels the reference's constructor makes; another subclass put in CCPotential would have a form
+		// of its own, which this adapter does not evaluate
+		const ShiftedCCPotential &cc = *this->CCPotential;
+		if (typeid(cc) != typeid(ShiftedCCPotential) && typeid(cc) != typeid(ShiftedCCPotential_S2))
+			throw std::invalid_argument("GpuRepulsiveCCPotential: CCPotential must be a ShiftedCCPotential or a "
+			                            "ShiftedCCPotential_S2");
 		const ShiftedCCPotential_S2 *s2 = dynamic_cast<const ShiftedCCPotential_S2 *>(this->CCPotential.get());
+		// the repulsion is on or off as the reference's constructor decided (WithRepulsion), not by the current e0
+		const double e0 = this->WithRepulsion ? this->e0 : 0.0;
 		const std::vector<double> S0 = s2 ? s2->S0 : std::vector<double>();
 		if (s2 && S0.size() != V.size())
 			throw std::invalid_argument("GpuRepulsiveCCPotential: the S2 kernel needs one S0 per constraint");
 		if (!handle_ || basis != basis_ || modes != modes_ || V != V_ || S0 != S0_ || (s2 != nullptr) != s2_ ||
-		    this->e0 != e0_ || this->sigma != sigma_) {
+		    e0 != e0_ || this->sigma != sigma_) {
 			cc_multi_destroy(handle_);
 			handle_ = nullptr;
 			const int64_t M = (int64_t)V.size();
 			const int32_t *mp = modes.data();
 			const double *vp = V.data(), *sp = s2 ? S0.data() : nullptr;
-			Check(cc_multi_create_s2(d, basis.data(), 1, &M, &mp, &vp, &sp, 1.0, this->e0, &handle_));
+			Check(cc_multi_create_s2(d, basis.data(), 1, &M, &mp, &vp, &sp, 1.0, e0, &handle_));
 			basis_.swap(basis);
 			modes_.swap(modes);
 			V_.swap(V);
 			S0_ = S0;
 			s2_ = s2 != nullptr;
-			e0_ = this->e0;
+			e0_ = e0;
 			sigma_ = this->sigma;
 			positions_dirty_ = true;
 		}
@@ -125,10 +134,12 @@ public:
 		valid_ = false;
 	}
 
+	// The collective-coordinate part's Shift is added as the reference's CCPotential->Energy() adds it
+	// (potential/CollectiveCoordinatePotential.h:1371, :1705).
 	double Energy() override
 	{
 		Evaluate();
-		return energy_;
+		return energy_ + this->CCPotential->Shift;
 	}
 
 	void AllForce(std::vector<GeometryVector> &results) override
@@ -156,7 +167,7 @@ public:
 	double EnergyAndAllForce(std::vector<GeometryVector> &results) override
 	{
 		AllForce(results);
-		return energy_;
+		return energy_ + this->CCPotential->Shift;
 	}
 };
 

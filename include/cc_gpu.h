@@ -43,7 +43,8 @@ enum {
 	CC_ERR_TIMEOUT = -4,      /* a bounded device wait ran out */
 	CC_ERR_NONLATTICE = -5,   /* a Cartesian k is not on the reciprocal lattice of the cell */
 	CC_ERR_STATE = -6,        /* call order: e.g. energy requested before positions were set */
-	CC_ERR_NOGPU = -7         /* no CUDA device is visible: the library has no CPU path */
+	CC_ERR_NOGPU = -7,        /* no CUDA device is visible: the library has no CPU path */
+	CC_ERR_NAN = -8           /* cc_objective: the first variable is NaN (the reference's NotANumberFound) */
 };
 
 enum {
@@ -121,7 +122,10 @@ int cc_force_one(cc_handle *h, int64_t i, double *f);
 int cc_structure_factor(cc_handle *h, int64_t K, const int32_t *modes, double *S, int precision);
 
 /* The structure optimiser's Switch-0 objective: x = rescale * fractional coordinates (N*d), returns the energy in
- * *f and, if grad is not NULL, grad[i*d+j] = -F_i . a_j / rescale. */
+ * *f and, if grad is not NULL, grad[i*d+j] = -F_i . a_j / rescale. A NaN first variable returns CC_ERR_NAN and
+ * leaves *f and grad untouched, where the reference's Objective throws NotANumberFound
+ * (potential/StructureOptimization.cpp:460-461; its catch at :571 takes InvalidStructure only); any other non-finite
+ * variable returns CC_ERR_ARG. */
 int cc_objective(cc_handle *h, int64_t N, const double *x, double rescale, double *f, double *grad, int precision);
 
 /* --- structure optimisation (L-BFGS on the device) --------------------------------------------------------------
@@ -294,7 +298,9 @@ int cc_multi_destroy(cc_multi *m);
  * The first call on each device looks up the scratch array's device address (and may load the kernel), so make it
  * before any stream capture, with that device current. All calls share the one scratch array and each call leaves
  * its contents behind (the call clears what must start at zero): calls whose work overlaps on the GPU, e.g. on
- * two streams at once, race and must be serialised by the caller. */
+ * two streams at once, race and must be serialised by the caller. The looked-up address is kept per device for the
+ * life of the process: after a cudaDeviceReset the next call would pass a stale address, so do not reset a device
+ * between calls. */
 #define CC_NOALLOC_SCRATCH_BYTES (16u << 20)
 #define CC_NOALLOC_MAX_MODES 262144
 #define CC_NOALLOC_MAX_PARTICLES (1 << 30)
@@ -315,6 +321,9 @@ const char *cc_noalloc_last_error(void);
  * Results agree to rounding; each path repeats bitwise. */
 enum { CC_PATH_SPLIT = 0, CC_PATH_FUSED = 1, CC_PATH_NUFFT = 2, CC_PATH_AUTO = 3 };
 int cc_set_path(cc_handle *h, int path);
+/* The path (CC_PATH_SPLIT, CC_PATH_FUSED or CC_PATH_NUFFT) an evaluation of N particles at `precision` takes on this
+ * handle under its current cc_set_path choice. */
+int cc_eval_path(cc_handle *h, int64_t N, int precision, int *path);
 
 /* Synchronise the device and report CC_ERR_TIMEOUT if a bounded grid-barrier wait of an earlier device-path
  * evaluation ran out (the error is then cleared). Host-path calls check this themselves. */

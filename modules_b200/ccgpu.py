@@ -17,13 +17,17 @@ PREC_FP64 = 0
 PREC_MIXED = 1
 
 _STATUS = {0: "CC_OK", -1: "CC_ERR_ARG", -2: "CC_ERR_OOM", -3: "CC_ERR_CUDA", -4: "CC_ERR_TIMEOUT",
-           -5: "CC_ERR_NONLATTICE", -6: "CC_ERR_STATE", -7: "CC_ERR_NOGPU"}
+           -5: "CC_ERR_NONLATTICE", -6: "CC_ERR_STATE", -7: "CC_ERR_NOGPU", -8: "CC_ERR_NAN"}
 
 
 class CCError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"{_STATUS.get(code, code)}: {msg}")
         self.code = code
+
+
+class NotANumberFound(CCError):
+    """The objective's first variable is NaN (the reference's NotANumberFound, StructureOptimization.h:47)."""
 
 
 def library_path():
@@ -111,6 +115,7 @@ _SIGS = {
     "cc_mc_try_move": (_i, [_vp, _vp, _vp, ctypes.POINTER(_d)]),
     "cc_mc_accept_move": (_i, [_vp]),
     "cc_set_path": (_i, [_vp, _i]),
+    "cc_eval_path": (_i, [_vp, _i64, _i, ctypes.POINTER(_i)]),
     "cc_check_device_error": (_i, [_vp]),
     "cc_energy_noalloc": (_i, [_i, _vp, _i64, _vp, _vp, _d, _i64, _vp, _vp, _vp, _vp]),
     "cc_noalloc_last_error": (ctypes.c_char_p, []),
@@ -137,7 +142,7 @@ def load_library():
 
 def _check(rc):
     if rc != 0:
-        raise CCError(rc, load_library().cc_last_error().decode())
+        raise (NotANumberFound if rc == -8 else CCError)(rc, load_library().cc_last_error().decode())
 
 
 def _ptr(a):
@@ -421,6 +426,12 @@ class CCPotential:
         """PATH_AUTO (default): PATH_NUFFT where it is estimated faster, else PATH_SPLIT; PATH_SPLIT: the three-kernel
         direct path; PATH_FUSED: one cooperative kernel when the tables fit; PATH_NUFFT: non-uniform FFTs (FP64)."""
         _check(self._lib.cc_set_path(self._h, int(path)))
+
+    def eval_path(self, N, precision=PREC_FP64):
+        """The path an evaluation of N particles takes: "split", "fused" or "nufft"."""
+        p = _i()
+        _check(self._lib.cc_eval_path(self._h, int(N), precision, ctypes.byref(p)))
+        return {PATH_SPLIT: "split", PATH_FUSED: "fused", PATH_NUFFT: "nufft"}[p.value]
 
     def check_device_error(self):
         _check(self._lib.cc_check_device_error(self._h))

@@ -2015,13 +2015,10 @@ int cc_objective(cc_handle *h, int64_t N, const double *x, double rescale, doubl
 	if (!x || !f || N < 0 || !(rescale != 0.0))
 		return fail(CC_ERR_ARG, "invalid objective arguments");
 	const int d = h->d;
-	// A NaN first variable makes the reference's objective return MaxEnergy with a zero gradient.
-	if (N > 0 && x[0] != x[0]) {
-		*f = 1e10;
-		if (grad)
-			std::fill(grad, grad + N * d, 0.0);
-		return CC_OK;
-	}
+	// A NaN first variable is the reference's NotANumberFound (StructureOptimization.cpp:460-461), which its Objective
+	// does not catch: a status of its own, so a caller can stop its optimiser as the reference's does.
+	if (N > 0 && x[0] != x[0])
+		return fail(CC_ERR_NAN, "NotANumberFound: the first variable is NaN");
 	if (int rc = ensure_particles(h, N))
 		return rc;
 	if (int rc = input_staging(h, (size_t)N * d))
@@ -2188,6 +2185,24 @@ int cc_plan_info(const cc_handle *h, int64_t N, int *L, int64_t *nseg, int *nspl
 		*nsplit = l.nsplit;
 	if (nksplit)
 		*nksplit = (int)cc::force_splits(h->main.plan, l.want_force).count();
+	return CC_OK;
+}
+
+int cc_eval_path(cc_handle *h, int64_t N, int precision, int *path)
+{
+	if (int rc = check_handle(h))
+		return rc;
+	if (int rc = check_prec(precision))
+		return rc;
+	if (!path || N < 0)
+		return fail(CC_ERR_ARG, "invalid cc_eval_path arguments");
+	const bool mixed = precision == CC_PREC_MIXED && !h->d_slotS0;
+	if (h->nsub <= 1 && (h->use_nufft || (h->auto_path && nufft_preferred(h, N))) && h->main.plan.nslot > 0)
+		*path = CC_PATH_NUFFT;
+	else if (h->nsub <= 1 && h->use_fused && fused_eligible(h, N, mixed))
+		*path = CC_PATH_FUSED;
+	else
+		*path = CC_PATH_SPLIT;
 	return CC_OK;
 }
 

@@ -16,6 +16,8 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 namespace {
 
 constexpr size_t kScratchBytes = CC_NOALLOC_SCRATCH_BYTES;
@@ -27,7 +29,9 @@ constexpr int kChunkNA = 64;
 // gets the address with cudaGetSymbolAddress (once per device, see scratch_on_device).
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-void *g_scratch_ptr[kMaxDevices] = {nullptr};
+// Cached device addresses, one per device. Concurrent first calls from several host threads may each look the
+// address up and store the same value; the atomics make that well defined.
+std::atomic<void *> g_scratch_ptr[kMaxDevices];
 
 thread_local const char *g_na_err = "";
 
@@ -36,13 +40,13 @@ int scratch_on_device(int dev, void **out)
 {
 	if (dev < 0 || dev >= kMaxDevices)
 		return CC_ERR_ARG;
-	if (!g_scratch_ptr[dev]) {
-		void *p = nullptr;
+	void *p = g_scratch_ptr[dev].load(std::memory_order_relaxed);
+	if (!p) {
 		if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p)
 			return CC_ERR_CUDA;
-		g_scratch_ptr[dev] = p;
+		g_scratch_ptr[dev].store(p, std::memory_order_relaxed);
 	}
-	*out = g_scratch_ptr[dev];
+	*out = p;
 	return CC_OK;
 }
 

@@ -150,15 +150,20 @@ class VarBoxPotential:
             self._key = key
         self.pot.set_configuration(frac)
 
+    def _bound(self):
+        if self.pot is None:
+            raise RuntimeError("VarBoxPotential has no bound cell (closed, or set_configuration not called)")
+        return self.pot
+
     def energy_and_forces(self, forces=True):
-        return self.pot.energy_and_forces(forces=forces)
+        return self._bound().energy_and_forces(forces=forces)
 
     def energy(self):
-        return self.pot.energy()
+        return self._bound().energy()
 
     def minimize(self, frac, **kw):
         """Device L-BFGS over the positions at the bound cell (see CCPotential.minimize)."""
-        return self.pot.minimize(frac, **kw)
+        return self._bound().minimize(frac, **kw)
 
     def close(self):
         if self.pot is not None:

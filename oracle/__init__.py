@@ -17,18 +17,22 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libccref.so")
 PORT_LIB = os.path.join(HERE, "_build", "libccoracle.so")
-REFERENCE_TREE = os.environ.get("CC_REFERENCE_TREE", "/root/reference")
+# The reference's source tree, needed only to BUILD oracle/_ref (the built library then runs without it): the
+# CC_REFERENCE_TREE environment variable, or the ref_tree argument of build().
+REFERENCE_TREE = os.environ.get("CC_REFERENCE_TREE")
 
 _vp = ctypes.c_void_p
 _l = ctypes.c_long
 _d = ctypes.c_double
 
 
-def build(ref=True):
-    """Build the port (always) and the reference oracle (when the reference tree is present)."""
+def build(ref=True, ref_tree=None):
+    """Build the port (always) and the reference oracle (when a reference tree is given, by ref_tree or
+    CC_REFERENCE_TREE, and present)."""
     subprocess.run(["make", "-s", "-C", HERE, "port"], check=True)
-    if ref and os.path.isdir(REFERENCE_TREE):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REFERENCE_TREE}"], check=True)
+    tree = ref_tree or REFERENCE_TREE
+    if ref and tree and os.path.isdir(tree):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={tree}"], check=True)
 
 
 def _p(a):

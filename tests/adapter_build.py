@@ -7,8 +7,11 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 EXE = os.path.join(ROOT, "tests", "_build", "adapter_check")
 
 
-def build(reference=os.environ.get("CC_REFERENCE_TREE", "/root/reference")):
-    if not os.path.isdir(reference):
+def build(reference=None):
+    """Compile the check program; `reference` is the reference's source tree (default: CC_REFERENCE_TREE). Returns
+    None without a tree."""
+    reference = reference or os.environ.get("CC_REFERENCE_TREE")
+    if not reference or not os.path.isdir(reference):
         return None
     os.makedirs(os.path.dirname(EXE), exist_ok=True)
     cmd = ["/usr/bin/g++", "-std=c++17", "-O2", "-fopenmp", "-w",

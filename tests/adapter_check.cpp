@@ -341,6 +341,13 @@ int main()
 				worst = std::max(worst, std::abs(fr[i].x[j] - fg[i].x[j]));
 		check(fg.size() == fr.size() && worst <= 1e-10 * sF, "S2 multi-configuration AllForce max |dF| / scale",
 		      worst / sF, 1e-10);
+		// NSubConfig is public: a new value applies from the next SetConfiguration on (the reference recomputes Np)
+		ref.NSubConfig = gpu.NSubConfig = 2;
+		ref.SetConfiguration(c);
+		gpu.SetConfiguration(c);
+		const double Er2 = ref.Energy(), Eg2 = gpu.Energy();
+		check(Er2 != Er && std::abs(Er2 - Eg2) <= 1e-10 * sE, "S2 multi-configuration NSubConfig change seen", Eg2,
+		      Er2);
 	}
 	// ---- 6. RepulsiveCCPotential, plain and S2 kernels -----------------------------------------------------------
 	for (int withS0 = 0; withS0 < 2; withS0++) {
@@ -368,6 +375,14 @@ int main()
 		const double Er = ref.Energy(), Eg = gpu.Energy();
 		check(std::abs(Er - Eg) <= 1e-10 * std::max(1.0, std::abs(Er)),
 		      withS0 ? "Repulsive (S2 kernel) Energy" : "Repulsive Energy", Eg, Er);
+		// a nonzero Shift of the collective-coordinate part is in both energies
+		ref.CCPotential->Shift = gpu.CCPotential->Shift = 0.375;
+		const double Ers = ref.Energy(), Egs = gpu.Energy();
+		check(std::abs(Ers - Egs) <= 1e-10 * std::max(1.0, std::abs(Ers)) && std::abs(Ers - Er - 0.375) <= 1e-12,
+		      withS0 ? "Repulsive (S2 kernel) Energy with Shift" : "Repulsive Energy with Shift", Egs, Ers);
+		std::vector<GeometryVector> fs;
+		check(gpu.EnergyAndAllForce(fs) == Egs, "Repulsive EnergyAndAllForce equals Energy with Shift", Egs, Egs);
+		ref.CCPotential->Shift = gpu.CCPotential->Shift = 0.0;
 		std::vector<GeometryVector> fr, fg;
 		ref.AllForce(fr);
 		gpu.AllForce(fg);

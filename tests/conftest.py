@@ -21,7 +21,7 @@ def load_golden(name):
 
 
 def golden_eval_cases():
-    skip = {"ksets", "min_2d_n100", "sk_3d_n2000", "isotropic_sk", "multi_stealthy"}
+    skip = {"ksets", "min_2d_n100", "sk_3d_n2000", "isotropic_sk", "multi_stealthy", "large_2d_n100000"}
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
                   if os.path.basename(p)[:-4] not in skip)
 

@@ -8,7 +8,8 @@ import oracle
 from adapter_build import EXE, build
 
 
-@pytest.mark.skipif(not os.path.isdir(oracle.REFERENCE_TREE), reason="needs the reference tree to compile")
+@pytest.mark.skipif(not (oracle.REFERENCE_TREE and os.path.isdir(oracle.REFERENCE_TREE)),
+                    reason="needs the reference tree (CC_REFERENCE_TREE) to compile")
 def test_adapter_compiles_against_reference_headers(ccgpu):
     if not oracle.ref_available():
         oracle.build(ref=True)

@@ -30,11 +30,18 @@ def _worker(rank, world, port, out):
     try:
         t = bench.max_over_ranks(1.0 + rank, "cpu")   # rank 1 is the slower one
         rate = bench.replica_rate(100, t, world)
-        # the reference arm: rank 0 alone runs and prints (stubbed timing: no reference library is needed)
-        bench.cpu_reference_rate = lambda *a, **k: (50.0, 1, 10, 0.2)
+        # the reference arm: rank 0 alone runs and prints (a stand-in potential: no reference library is needed)
+        class FakeRef:
+            def set_positions(self, frac):
+                pass
+
+            def eval(self):
+                return None
+
+        bench.reference_potential = lambda cores: (FakeRef(), 2724)
 
         class A:
-            steps, warmup, gpus = 10, 3, world
+            steps, warmup, gpus, pool, ref_seconds = 10, 3, world, 8, 0.05
 
         buf = io.StringIO()
         with contextlib.redirect_stdout(buf):
@@ -55,6 +62,15 @@ def test_two_gloo_ranks():
     assert res[0][0] == pytest.approx(2.0) and res[1][0] == pytest.approx(2.0)
     assert res[0][1] == pytest.approx(100.0) and res[1][1] == pytest.approx(100.0)
     assert '"impl": "reference"' in res[0][2] and res[1][2] == ""
+    import json
+    line = json.loads(res[0][2])
+    assert line["config"] == bench_config(2724, 8) and line["steps"] == 10 and line["e2e"]["value"] == line["value"]
+
+
+def bench_config(M, P):
+    sys.path.insert(0, ROOT)
+    import bench
+    return bench.workload_config(M, P)
 
 
 def test_single_process_identity():

@@ -105,6 +105,18 @@ def test_forms_are_checked():
         varbox.constraints(3, CELLS[3], 10, "Lemniscate", None, "plain")
 
 
+def test_unbound_potential_raises():
+    """Energy, forces and minimisation before a cell is bound, or after close(), raise a clear error (no GPU call)."""
+    from modules_b200 import varbox
+    v = varbox.VarBoxPotential("K2Potential", d=2)
+    for call in (v.energy, v.energy_and_forces, lambda: v.minimize(np.zeros((4, 2)))):
+        with pytest.raises(RuntimeError, match="no bound cell"):
+            call()
+    v.close()
+    with pytest.raises(RuntimeError, match="no bound cell"):
+        v.energy()
+
+
 def near_lattice(d, N, seed):
     rng = np.random.default_rng(seed)
     side = int(np.ceil(N ** (1.0 / d)))
