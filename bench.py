@@ -61,10 +61,9 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip the batched / ground-state / served measurements")
     ap.add_argument("--batch", type=int, default=512, help="instances of the batched uneven workload")
     ap.add_argument("--gs-instances", type=int, default=48, help="instances of the ground-states/s comparison")
-    ap.add_argument("--served", type=int, default=300, help="requests of the served sample")
-    ap.add_argument("--served-rate", type=float, default=60.0, help="Poisson arrival rate of the served stream (1/s)")
-    ap.add_argument("--served-full", action="store_true",
-                    help="the served stream's full distribution: N clipped to [100, 20000], chi U[0.05, 0.49]")
+    ap.add_argument("--served", type=int, default=600, help="requests of the served sample (Poisson arrivals)")
+    ap.add_argument("--served-rate", type=float, default=20.0, help="Poisson arrival rate of the served stream (1/s)")
+    ap.add_argument("--served-capacity", type=int, default=300, help="requests of the capacity run (all at t = 0)")
     return ap.parse_args()
 
 
@@ -394,19 +393,44 @@ def run_extras(args, cc, torch):
         "speedup": t_plain / t_batch, "reached": int((epp < 1e-20).sum()),
         "max_E_per_particle_batched": float(epp.max()), "max_E_per_particle_plain": float(max(plain_E))}
     del gb
-    # served stream (a bounded sample of the 10000-request workload)
+    # served stream: config 5's distribution (N log-normal, median 1000, clipped to [100, 20000]; chi U[0.05, 0.49])
+    # on a bounded sample of its 10000 requests, first with Poisson arrivals, then with every request at t = 0
+    # (the server's capacity)
     from modules_b200.workloads import served_stream
-    rate = args.served_rate
-    nmax, chimax = (20000, 0.49) if args.served_full else (4000, 0.40)
-    reqs = served_stream(args.served, rate, nmax, chimax)
-    res, wall = cc.serve(reqs, iters_per_round=16)
-    lat = np.array([r["t_done"] - q["arrival_s"] for r, q in zip(res, reqs)])
-    ok = np.array([r["E"] / q["N"] < 1e-20 for r, q in zip(res, reqs)])
-    out["served"] = {"workload": f"{args.served} requests, Poisson arrivals at {rate:g}/s, d in {{2,3}}, N log-normal "
-                                 f"(median 1000, clipped to [100,{nmax}]), chi U[0.05,{chimax:g}], v in {{1,(1-|k|/K)^2}}",
-                     "ground_states_per_s": len(reqs) / wall, "p50_ms": float(np.percentile(lat, 50) * 1e3),
-                     "p99_ms": float(np.percentile(lat, 99) * 1e3), "reached": int(ok.sum()), "wall_s": wall}
+    out["served"] = served_leg(cc, served_stream(args.served, args.served_rate, 20000, 0.49),
+                               f"{args.served} requests, Poisson arrivals at {args.served_rate:g}/s")
+    cap = served_stream(args.served_capacity, args.served_rate, 20000, 0.49, seed=100)
+    for q in cap:
+        q["arrival_s"] = 0.0
+    out["served_capacity"] = served_leg(cc, cap, f"{args.served_capacity} requests, all arriving at t = 0")
     return out
+
+
+def served_leg(cc, reqs, what):
+    """Serve `reqs` and report throughput, time-to-ground-state percentiles and their split into admission wait
+    (arrival to admission) and run time (admission to completion)."""
+    res, wall = cc.serve(reqs, iters_per_round=16)
+    arr = np.array([q["arrival_s"] for q in reqs])
+    adm = np.array([r["t_admit"] for r in res])
+    fin = np.array([r["t_done"] for r in res])
+    lat, wait, run = fin - arr, adm - arr, fin - adm
+    ok = np.array([r["status"] >= 0 and r["E"] / q["N"] < 1e-20 for r, q in zip(res, reqs)])
+    slow = np.argsort(lat)[-max(1, len(lat) // 100):]   # the slowest 1 %
+    pct = lambda x, p: float(np.percentile(x, p) * 1e3)   # noqa: E731
+    return {"workload": what + ", d in {2,3}, N log-normal (median 1000, clipped to [100,20000]), chi U[0.05,0.49], "
+                               "v in {1,(1-|k|/K)^2}, each to Phi/N < 1e-20",
+            "requests": len(reqs), "ground_states_per_s": float(ok.sum()) / wall, "wall_s": wall,
+            "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99),
+            "admission_wait_p50_ms": pct(wait, 50), "admission_wait_p99_ms": pct(wait, 99),
+            "run_p50_ms": pct(run, 50), "run_p99_ms": pct(run, 99),
+            "slowest_1pct": {"admission_wait_ms": float(wait[slow].mean() * 1e3),
+                             "run_ms": float(run[slow].mean() * 1e3),
+                             "N_mean": float(np.mean([reqs[i]["N"] for i in slow])),
+                             "evals_mean": float(np.mean([res[i]["evals"] for i in slow]))},
+            "reached": int(ok.sum()), "not_reached": [
+                {"N": int(reqs[i]["N"]), "d": int(reqs[i]["d"]), "chi": float(reqs[i]["chi"]),
+                 "status": int(res[i]["status"]), "E_per_N": float(res[i]["E"] / reqs[i]["N"]),
+                 "evals": int(res[i]["evals"])} for i in np.nonzero(~ok)[0][:20]]}
 
 
 def run_ours(args):

@@ -200,7 +200,14 @@ int cc_mc_accept_move(cc_handle *h);
  * (d, N, chi) with weights vtype (0: v = 1, 3: v = (1 - |k|/K)^2, as cc_kset_stealthy), a start frac0 (N x d) and an
  * arrival time in seconds after the call starts. The server minimises every request to Phi/N < 1e-20 (FP64), admitting
  * arrived requests while a slot is free and their device memory fits hbm_budget, and running all admitted requests
- * together, iters_per_round L-BFGS iterations per round; finished requests leave between rounds. */
+ * together, iters_per_round L-BFGS iterations per round; finished requests leave between rounds.
+ * Admission scans the arrived requests in arrival order and admits each one that fits, so a large request waiting for
+ * memory does not hold back smaller ones behind it, until it has waited max_bypass_s (then nothing behind it is
+ * admitted before it). A request that cannot be served is rejected on its own and the others carry on: its result
+ * has status CC_ERR_ARG (invalid request, e.g. d outside 1..3, N < 1, chi <= 0, an empty k-set), CC_ERR_OOM (its
+ * estimated memory exceeds hbm_budget, or the pool could not allocate it) or CC_ERR_CUDA (its set-up copies failed),
+ * E = NaN, evals = 0 and t_admit = t_done = the time of the rejection. cc_serve itself returns an error only when
+ * the server cannot run at all (no device, invalid options, a failed launch). */
 typedef struct {
 	int d;
 	int64_t N;
@@ -209,11 +216,12 @@ typedef struct {
 	const double *frac0;
 	double arrival_s;
 	int64_t max_evals;          /* 0: 100000 */
+	double *frac_out;           /* if not NULL: receives the final positions (N x d fractional) when the request ends */
 } cc_request;
 typedef struct {
 	double E;                   /* energy at the end (FP64) */
 	int64_t evals;
-	int status;                 /* as cc_lbfgs_result.status */
+	int status;                 /* as cc_lbfgs_result.status (1..5), or a negative CC_ERR_* for a rejected request */
 	double t_admit, t_done;     /* seconds after the call started */
 } cc_request_result;
 typedef struct {
@@ -221,6 +229,7 @@ typedef struct {
 	int max_slots;              /* admitted requests at most, default 256 */
 	int iters_per_round;        /* default 16 */
 	int history;                /* L-BFGS pairs, default 40 */
+	double max_bypass_s;        /* admission may pass a waiting request for this long, default 1 s; 0: strict order */
 } cc_serve_opts;
 int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *opts, cc_request_result *results, double *wall_s);
 const char *cc_serve_last_error(void);

@@ -52,7 +52,8 @@ class LbfgsResult(ctypes.Structure):
 
 class ServeRequest(ctypes.Structure):
     _fields_ = [("d", ctypes.c_int), ("N", ctypes.c_int64), ("chi", ctypes.c_double), ("vtype", ctypes.c_int),
-                ("frac0", ctypes.c_void_p), ("arrival_s", ctypes.c_double), ("max_evals", ctypes.c_int64)]
+                ("frac0", ctypes.c_void_p), ("arrival_s", ctypes.c_double), ("max_evals", ctypes.c_int64),
+                ("frac_out", ctypes.c_void_p)]
 
 
 class ServeResult(ctypes.Structure):
@@ -62,7 +63,7 @@ class ServeResult(ctypes.Structure):
 
 class ServeOpts(ctypes.Structure):
     _fields_ = [("hbm_budget", ctypes.c_size_t), ("max_slots", ctypes.c_int), ("iters_per_round", ctypes.c_int),
-                ("history", ctypes.c_int)]
+                ("history", ctypes.c_int), ("max_bypass_s", ctypes.c_double)]
 
 
 PREC_SCHEDULE = 2
@@ -528,22 +529,31 @@ class CCBatch:
                 np.array([r.iters for r in res]), np.array([r.status for r in res]))
 
 
-def serve(requests, hbm_budget=16 << 30, max_slots=256, iters_per_round=16, history=40):
+def serve(requests, hbm_budget=16 << 30, max_slots=256, iters_per_round=16, history=40, max_bypass_s=1.0,
+          positions=False):
     """Run the continuous-batching ground-state server on `requests`, a list of dicts with keys d, N, chi, vtype,
-    frac0 (N x d array), arrival_s. Returns (list of result dicts, wall seconds)."""
+    frac0 (N x d array), arrival_s. Returns (list of result dicts, wall seconds); with positions=True each result
+    also holds "frac", the final positions. A request the server cannot serve comes back with a negative status (the
+    CC_ERR_* code: -1 invalid, -2 larger than the budget or out of memory) and E = NaN; the others are served."""
     lib = load_library()
-    keep = []
+    keep, finals = [], []
     reqs = (ServeRequest * len(requests))()
     for i, r in enumerate(requests):
         f = np.ascontiguousarray(r["frac0"], dtype=np.float64).reshape(int(r["N"]), int(r["d"]))
         keep.append(f)
+        fo = np.full_like(f, np.nan) if positions else None
+        finals.append(fo)
         reqs[i] = ServeRequest(int(r["d"]), int(r["N"]), float(r["chi"]), int(r.get("vtype", 0)),
-                               f.ctypes.data_as(_vp), float(r.get("arrival_s", 0.0)), int(r.get("max_evals", 0)))
-    opts = ServeOpts(hbm_budget, max_slots, iters_per_round, history)
+                               f.ctypes.data_as(_vp), float(r.get("arrival_s", 0.0)), int(r.get("max_evals", 0)),
+                               fo.ctypes.data_as(_vp) if positions else None)
+    opts = ServeOpts(hbm_budget, max_slots, iters_per_round, history, max_bypass_s)
     res = (ServeResult * len(requests))()
     wall = _d()
     rc = lib.cc_serve(reqs, len(requests), ctypes.byref(opts), res, ctypes.byref(wall))
     if rc != 0:
         raise CCError(rc, lib.cc_serve_last_error().decode())
     out = [dict(E=x.E, evals=x.evals, status=x.status, t_admit=x.t_admit, t_done=x.t_done) for x in res]
+    if positions:
+        for o, fo in zip(out, finals):
+            o["frac"] = fo
     return out, wall.value

@@ -86,6 +86,15 @@ int serve_per_split(const cc::Plan &p)
 	return per;
 }
 
+// Offsets of a request's arrays in its one allocation (see open_slot).
+struct SlotOffsets {
+	size_t segs, slotV, bstart, bspec, kstart, kspec, part, rho, u, ep, tk, pg, fc, x, g, d, xt, gt, S, Y, lp, st;
+};
+
+int fill_slot(const cc_request &r, int idx, int m, const cc::Plan &p, const cc::ForceSplits &fs, double vol,
+              const double *recip, int per_split, int nsplit, int nchunks, int pgroups, int nks, cudaStream_t st,
+              const SlotOffsets &off, Slot &s);
+
 // Plan and allocate a request; returns CC_OK and fills the slot.
 int open_slot(const cc_request &r, int idx, int m, int nblk_cap, cudaMemPool_t pool, cudaStream_t st, Slot &s)
 {
@@ -121,7 +130,38 @@ int open_slot(const cc_request &r, int idx, int m, int nblk_cap, cudaMemPool_t p
 	             o_S = c.take(8 * (size_t)n * m), o_Y = c.take(8 * (size_t)n * m),
 	             o_lp = c.take(8 * (size_t)nblk_cap * cc::lb_ndots(m)), o_st = c.take(sizeof(cc::LbState));
 	s.bytes = c.used;
-	SV_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void **>(&s.mem), c.used, pool, st));
+	{
+		const cudaError_t ae = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&s.mem), c.used, pool, st);
+		if (ae != cudaSuccess) {
+			cudaGetLastError();   // an allocation failure is not sticky: clear it and reject this request alone
+			s.mem = nullptr;
+			return sfail(ae == cudaErrorMemoryAllocation ? CC_ERR_OOM : CC_ERR_CUDA,
+			             std::string("request memory: ") + cudaGetErrorString(ae));
+		}
+	}
+	if (int rc = fill_slot(r, idx, m, p, fs, vol, recip, per_split, nsplit, nchunks, pgroups, nks, st,
+	                       {o_segs, o_slotV, o_bstart, o_bspec, o_kstart, o_kspec, o_part, o_rho, o_u, o_ep, o_tk,
+	                        o_pg, o_fc, o_x, o_g, o_d, o_xt, o_gt, o_S, o_Y, o_lp, o_st},
+	                       s)) {
+		cudaFreeAsync(s.mem, st);
+		s.mem = nullptr;
+		return rc;
+	}
+	return CC_OK;
+}
+
+// Upload a request's plan and start and fill its kernel arguments (its memory is allocated).
+int fill_slot(const cc_request &r, int idx, int m, const cc::Plan &p, const cc::ForceSplits &fs, double vol,
+              const double *recip, int per_split, int nsplit, int nchunks, int pgroups, int nks, cudaStream_t st,
+              const SlotOffsets &off, Slot &s)
+{
+	const size_t o_segs = off.segs, o_slotV = off.slotV, o_bstart = off.bstart, o_bspec = off.bspec,
+	             o_kstart = off.kstart, o_kspec = off.kspec, o_part = off.part, o_rho = off.rho, o_u = off.u,
+	             o_ep = off.ep, o_tk = off.tk, o_pg = off.pg, o_fc = off.fc, o_x = off.x, o_g = off.g, o_d = off.d,
+	             o_xt = off.xt, o_gt = off.gt, o_S = off.S, o_Y = off.Y, o_lp = off.lp, o_st = off.st;
+	const int d = r.d;
+	const int64_t N = r.N;
+	const int n = (int)(N * d);
 	unsigned char *b = s.mem;
 	SV_CUDA(cudaMemcpyAsync(b + o_segs, p.segs.data(), sizeof(cc::Seg) * p.segs.size(), cudaMemcpyHostToDevice, st));
 	SV_CUDA(cudaMemcpyAsync(b + o_slotV, p.slotV.data(), sizeof(double) * p.nslot, cudaMemcpyHostToDevice, st));
@@ -258,14 +298,12 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 	o.max_slots = 256;
 	o.iters_per_round = 16;
 	o.history = 40;
+	o.max_bypass_s = 1.0;
 	if (opts)
 		o = *opts;
-	if (o.max_slots < 1 || o.iters_per_round < 1 || o.history < 1 || o.history > cc::kLbMaxHist)
+	if (o.max_slots < 1 || o.iters_per_round < 1 || o.history < 1 || o.history > cc::kLbMaxHist ||
+	    !(o.max_bypass_s >= 0.0))
 		return sfail(CC_ERR_ARG, "invalid serve options");
-	for (int i = 0; i < count; i++)
-		if (reqs[i].d < 1 || reqs[i].d > 3 || reqs[i].N < 1 || reqs[i].N > (1 << 24) || !reqs[i].frac0 ||
-		    !(reqs[i].chi > 0) || (reqs[i].vtype < 0 || reqs[i].vtype > 3))
-			return sfail(CC_ERR_ARG, "invalid request");
 	int ndev = 0;
 	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
 		return sfail(CC_ERR_NOGPU, "no CUDA device is visible");
@@ -325,38 +363,81 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 	SV_CUDA(cudaMalloc(&d_queue, sizeof(unsigned) * 18));
 	SV_CUDA(cudaMalloc(&d_brief, sizeof(cc::LbBrief) * o.max_slots));
 	SV_CUDA(cudaMemset(d_queue, 0, sizeof(unsigned) * 18));
-	std::vector<int> order(count);
-	for (int i = 0; i < count; i++)
-		order[i] = i;
+	const auto t0 = std::chrono::steady_clock::now();
+	auto now = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
+	int done = 0;
+	// a request the server cannot serve gets a status of its own; the others carry on
+	auto reject = [&](int idx, int code) {
+		cc_request_result &res = out[idx];
+		res.E = NAN;
+		res.evals = 0;
+		res.status = code;
+		res.t_admit = res.t_done = now();
+		done++;
+	};
+	std::vector<int> order;
+	order.reserve(count);
+	for (int i = 0; i < count; i++) {
+		const cc_request &r = reqs[i];
+		bool ok = r.d >= 1 && r.d <= 3 && r.N >= 1 && r.N <= (1 << 24) && r.frac0 && r.chi > 0 && r.vtype >= 0 &&
+		          r.vtype <= 3 && std::isfinite(r.arrival_s) && r.max_evals >= 0;
+		for (int64_t k = 0; ok && k < r.N * r.d; k++)
+			ok = std::isfinite(r.frac0[k]);
+		if (ok)
+			order.push_back(i);
+		else
+			reject(i, CC_ERR_ARG);
+	}
 	std::stable_sort(order.begin(), order.end(),
 	                 [&](int a, int b) { return reqs[a].arrival_s < reqs[b].arrival_s; });
 	std::vector<Slot> active;
+	std::vector<int> pending;   // arrived and not yet admitted, in arrival order
 	size_t used = 0;
-	int next = 0, done = 0;
+	size_t next = 0;
 	int rc = CC_OK;
 	std::vector<cc::LbBrief> hs(o.max_slots);
-	const auto t0 = std::chrono::steady_clock::now();
-	auto now = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
 	while (done < count && rc == CC_OK) {
-		// 1. admission
+		// 1. admission: every arrived request that fits, in arrival order; one that does not fit yet may be passed
+		// by later ones until it has waited max_bypass_s
 		const double t = now();
-		while (next < count && reqs[order[next]].arrival_s <= t && (int)active.size() < o.max_slots) {
-			const cc_request &r = reqs[order[next]];
+		while (next < order.size() && reqs[order[next]].arrival_s <= t)
+			pending.push_back(order[next++]);
+		std::vector<int> waiting;
+		bool hold = false;
+		for (int idx : pending) {
+			if (hold || (int)active.size() >= o.max_slots) {
+				waiting.push_back(idx);
+				continue;
+			}
+			const cc_request &r = reqs[idx];
 			const size_t need = estimate_bytes(r, m, nblk_cap);
-			if (!active.empty() && used + need > o.hbm_budget)
-				break;
+			if (need > o.hbm_budget) {
+				reject(idx, CC_ERR_OOM);
+				continue;
+			}
+			if (used + need > o.hbm_budget) {
+				waiting.push_back(idx);
+				hold = now() - r.arrival_s > o.max_bypass_s;
+				continue;
+			}
 			Slot s;
-			if ((rc = open_slot(r, order[next], m, nblk_cap, pool, st, s)))
-				break;
+			const int orc = open_slot(r, idx, m, nblk_cap, pool, st, s);
+			if (orc != CC_OK) {
+				reject(idx, orc);
+				continue;
+			}
 			used += s.bytes;
-			out[order[next]].t_admit = now();
+			out[idx].t_admit = now();
 			active.push_back(s);
-			next++;
 		}
-		if (rc)
-			break;
+		pending.swap(waiting);
 		if (active.empty()) {
-			if (next < count) {
+			if (!pending.empty()) {   // nothing runs and a request still waits: it cannot be placed at all
+				reject(pending.front(), CC_ERR_OOM);
+				pending.erase(pending.begin());
+				continue;
+			}
+			if (next < order.size()) {
 				const double wait = reqs[order[next]].arrival_s - now();
 				if (wait > 0)
 					std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 0.01)));
@@ -459,6 +540,9 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 				continue;
 			}
 			cc_request_result &res = out[active[a].req];
+			if (double *fo = reqs[active[a].req].frac_out)
+				SV_CUDA(cudaMemcpyAsync(fo, active[a].li.x, sizeof(double) * active[a].li.n, cudaMemcpyDeviceToHost,
+				                        st));
 			res.E = hs[a].E;
 			res.evals = hs[a].evals;
 			res.status = hs[a].status;

@@ -24,7 +24,7 @@ def batched_workload(cc, count, seed=2024):
 def served_stream(count, rate=60.0, nmax=4000, chimax=0.40, seed=99):
     """`count` ground-state requests with Poisson arrivals at `rate` per second: d in {2,3}, N log-normal (median
     1000, sigma 0.6) clipped to [100, nmax], chi U[0.05, chimax], v(k) = 1 or (1 - |k|/K)^2, uniform random start.
-    Returns a list of request dicts for modules_b200.serve."""
+    Returns a list of request dicts for modules_b200.serve (seeded: the same arguments give the same stream)."""
     rng = np.random.default_rng(seed)
     reqs, t = [], 0.0
     for _ in range(count):

@@ -81,8 +81,33 @@ def test_batch_autotune_keeps_results(gpu):
     batch.set_positions(fracs)
     E0, F0 = batch.energy_and_forces()
     ps, sg = batch.autotune(reps=1)
-    assert ps in (32, 64, 128, 256, 512) and sg in (32, 64, 128, 256)
+    cands = (32, 64, 128, 256, 512, 1024)   # include/cc_gpu.h cc_batch_autotune: 6 x 6 candidate shapes
+    assert ps in cands and sg in cands
     E1, F1 = batch.energy_and_forces()
     for e0, e1, f0, f1 in zip(E0, E1, F0, F1):
         assert abs(e1 - e0) <= 1e-12 * abs(e0)
         assert np.abs(f1 - f0).max() <= 1e-12 * max(np.abs(f0).max(), 1.0)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "schedule"])
+def test_batch_ground_states_against_reference(gpu, precision):
+    """The north star's bar on batched ground states: the reference's own FP64 energy of each final configuration
+    (oracle/_ref, potential/CollectiveCoordinatePotential.h:1351-1372) is below 1e-20 per particle and within 1e-12
+    per particle of the GPU's energy."""
+    import oracle
+    if not oracle.ref_available():
+        pytest.skip("reference oracle not built")
+    pots, N, fracs = _instances(gpu, SPECS[:5], seed=21)
+    batch = gpu.CCBatch(pots, N)
+    prec = gpu.PREC_FP64 if precision == "fp64" else gpu.PREC_SCHEDULE
+    xs, E, evals, iters, status = batch.minimize(fracs, precision=prec, switch_energy_per_particle=1e-10)
+    for (d, n, chi, typ), x, e in zip(SPECS[:5], xs, E):
+        basis = np.eye(d) * n ** (1.0 / d)
+        modes, V = gpu.stealthy_kset(d, basis, n, chi, typ)
+        ref = oracle.Ref(d, basis, V, modes=modes)
+        ref.set_positions(x)
+        Er = ref.eval(forces=False)[0]
+        print(f"d={d} N={n}: GPU E/N={e / n:.3e} reference E/N={Er / n:.3e}")
+        # the stop rule is the GPU's E <= 1e-20 N; the reference's sum of the same configuration differs by rounding
+        # (|rho| ~ 1e-10 near the ground state, its rounding ~1e-15: ~1e-5 relative in E)
+        assert Er / n < 1.001e-20 and abs(e - Er) / n <= 1e-12

@@ -33,3 +33,64 @@ def test_serve_same_alone_and_in_mix(gpu):
         one = dict(reqs[k], arrival_s=0.0)
         alone, _ = gpu.serve([one], iters_per_round=8)
         assert alone[0]["E"] == mix[k]["E"] and alone[0]["evals"] == mix[k]["evals"]
+
+
+def test_serve_rejects_requests_it_cannot_serve(gpu):
+    """An invalid request and one larger than the whole budget are rejected with their own status (CC_ERR_ARG,
+    CC_ERR_OOM; E = NaN) while the other requests are served to their ground states."""
+    reqs = _requests()[:3]
+    rng = np.random.default_rng(9)
+    reqs.append(dict(d=2, N=100, chi=0.0, vtype=0, frac0=rng.random((100, 2)), arrival_s=0.001))   # chi <= 0
+    reqs.append(dict(d=3, N=20000, chi=0.40, vtype=0, frac0=rng.random((20000, 3)), arrival_s=0.002))
+    res, _ = gpu.serve(reqs, hbm_budget=100 << 20, iters_per_round=8)
+    for r, q in zip(res[:3], reqs[:3]):
+        assert r["status"] == 1 and r["E"] / q["N"] < 1e-20
+    assert res[3]["status"] == -1 and np.isnan(res[3]["E"]) and res[3]["evals"] == 0
+    assert res[4]["status"] == -2 and np.isnan(res[4]["E"]) and res[4]["evals"] == 0
+
+
+def _bypass_stream(seed=11):
+    """Two large 3D requests of which the budget holds one, then small 2D requests arriving behind the second."""
+    rng = np.random.default_rng(seed)
+    reqs = [dict(d=3, N=3000, chi=0.30, vtype=0, frac0=rng.random((3000, 3)), arrival_s=0.0),
+            dict(d=3, N=3000, chi=0.30, vtype=0, frac0=rng.random((3000, 3)), arrival_s=0.0005)]
+    for k in range(4):
+        reqs.append(dict(d=2, N=150, chi=0.25, vtype=0, frac0=rng.random((150, 2)), arrival_s=0.001 + 0.0005 * k))
+    return reqs
+
+
+def test_serve_small_requests_pass_a_waiting_large_one(gpu):
+    """With a budget that holds one large request, the second large request waits for memory; the small requests
+    behind it are admitted before it (max_bypass_s = 1 s), and not before it when bypassing is off (0 s). Every
+    request reaches its ground state either way, with the same result."""
+    reqs = _bypass_stream()
+    budget = 40 << 20
+    res, _ = gpu.serve(reqs, hbm_budget=budget, iters_per_round=8, max_bypass_s=1.0)
+    strict, _ = gpu.serve(reqs, hbm_budget=budget, iters_per_round=8, max_bypass_s=0.0)
+    for rr in (res, strict):
+        for r, q in zip(rr, reqs):
+            assert r["status"] == 1 and r["E"] / q["N"] < 1e-20
+    assert res[1]["t_admit"] >= res[0]["t_done"]          # the second large request waited for the first
+    assert max(r["t_admit"] for r in res[2:]) < res[1]["t_admit"]
+    assert min(r["t_admit"] for r in strict[2:]) >= strict[1]["t_admit"]
+    for a, b in zip(res, strict):
+        assert a["E"] == b["E"] and a["evals"] == b["evals"]
+
+
+def test_served_ground_states_against_reference(gpu):
+    """Each served request's final configuration, re-evaluated by the reference's own FP64 energy (oracle/_ref,
+    potential/CollectiveCoordinatePotential.h:1351-1372), is at its ground state: below 1e-20 per particle (to the
+    rounding of that sum) and within 1e-12 per particle of the server's energy."""
+    import oracle
+    if not oracle.ref_available():
+        pytest.skip("reference oracle not built")
+    reqs = _requests(seed=17)
+    res, _ = gpu.serve(reqs, iters_per_round=8, positions=True)
+    for r, q in zip(res, reqs):
+        d, n = q["d"], q["N"]
+        basis = np.eye(d) * n ** (1.0 / d)
+        modes, V = gpu.stealthy_kset(d, basis, n, q["chi"], q["vtype"])
+        ref = oracle.Ref(d, basis, V, modes=modes)
+        ref.set_positions(r["frac"])
+        Er = ref.eval(forces=False)[0]
+        assert r["status"] == 1 and Er / n < 1.001e-20 and abs(r["E"] - Er) / n <= 1e-12
