@@ -5,12 +5,14 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libccgpu.so")
-SOURCES = ["csrc/cc_capi.cu", "csrc/cc_plan.cpp", "csrc/cc_noalloc.cu", "csrc/cc_serve.cu", "csrc/cc_multi.cu"]
-HEADERS = ["csrc/cc_kernels.cuh", "csrc/cc_fused.cuh", "csrc/cc_lbfgs.cuh", "csrc/cc_plan.h", "csrc/cc_error.h", "csrc/cc_nufft.cuh", "csrc/cc_multi_launch.h", "../include/cc_gpu.h"]
+SOURCES = ["csrc/cc_capi.cu", "csrc/cc_batch.cu", "csrc/cc_plan.cpp", "csrc/cc_noalloc.cu", "csrc/cc_serve.cu",
+           "csrc/cc_multi.cu"]
+HEADERS = ["csrc/cc_internal.h", "csrc/cc_kernels.cuh", "csrc/cc_fused.cuh", "csrc/cc_lbfgs.cuh", "csrc/cc_plan.h", "csrc/cc_error.h", "csrc/cc_nufft.cuh", "csrc/cc_multi_launch.h", "../include/cc_gpu.h"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-    "-Xcompiler", "-fPIC,-O3", "-shared", "--expt-relaxed-constexpr", "-lcufft",
+    "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
 ]
+OBJDIR = os.path.join(HERE, "_build")
 
 
 def _stale():
@@ -21,14 +23,24 @@ def _stale():
 
 
 def build(force=False, verbose=False):
+    """Compile every source to an object (in parallel, for sm_100a) and link libccgpu.so."""
     if not force and not _stale():
         return LIB
     nvcc = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-    cmd = [nvcc] + NVCC_FLAGS + ["-o", LIB + ".tmp"] + [os.path.join(HERE, s) for s in SOURCES]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True, cwd=HERE)
+    os.makedirs(OBJDIR, exist_ok=True)
+    objs, procs = [], []
+    for src in SOURCES:
+        obj = os.path.join(OBJDIR, os.path.basename(src) + ".o")
+        cmd = [nvcc] + NVCC_FLAGS + (["-Xptxas=-v"] if verbose else []) + ["-c", os.path.join(HERE, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        objs.append(obj)
+        procs.append((cmd, subprocess.Popen(cmd, cwd=HERE)))
+    failed = [cmd for cmd, p in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
+    link = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB + ".tmp"] + objs + ["-lcufft"]
+    subprocess.run(link, check=True, cwd=HERE)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

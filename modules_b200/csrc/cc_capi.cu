@@ -8,6 +8,7 @@
 // There is no CPU path: without a CUDA device every call that computes returns CC_ERR_NOGPU.
 #include "../../include/cc_gpu.h"
 #include "cc_fused.cuh"
+#include "cc_internal.h"
 #include "cc_kernels.cuh"
 #include "cc_lbfgs.cuh"
 #include "cc_multi_launch.h"
@@ -26,8 +27,10 @@
 #include <vector>
 
 namespace {
-
 thread_local std::string g_err = "";
+}  // namespace
+
+namespace cci {
 
 int fail(int code, const std::string &msg)
 {
@@ -35,7 +38,9 @@ int fail(int code, const std::string &msg)
 	return code;
 }
 
-}  // namespace
+std::atomic<unsigned long long> g_alloc_gen{1};
+
+}  // namespace cci
 
 namespace cc {
 // Error reporting for the library's other translation units: sets the message cc_last_error() returns.
@@ -46,99 +51,47 @@ int set_error(int code, const char *msg)
 }
 }  // namespace cc
 
-namespace {
+using namespace cci;
 
-#define CC_CUDA(call)                                                                                         \
-	do {                                                                                                      \
-		cudaError_t e_ = (call);                                                                              \
-		if (e_ != cudaSuccess)                                                                                \
-			return fail(CC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));                    \
-	} while (0)
+int cci::check_prec(int precision)
+{
+	if (precision != CC_PREC_FP64 && precision != CC_PREC_MIXED)
+		return fail(CC_ERR_ARG, "precision must be CC_PREC_FP64 or CC_PREC_MIXED");
+	return CC_OK;
+}
 
-
-// ---------------------------------------------------------------------------------------------------------------
-// device-side k-set: a Plan uploaded
-// ---------------------------------------------------------------------------------------------------------------
-struct DevSplits {
-	int want = 0;
-	cc::ForceSplits host;
-	int *kstart = nullptr;
-	cc::TabSpec *kspec = nullptr;
-};
-
-struct DevKSet {
-	cc::Plan plan;
-	cc::Seg *segs = nullptr;
-	cc::TabSpec *rspec = nullptr;
-	int *bstart = nullptr;
-	cc::TabSpec *bspec = nullptr;
-	double *slotV = nullptr;
-	int *mode_slot = nullptr;
-	double2 *rho_slot = nullptr;
-	double2 *u_slot = nullptr;
-	double2 *rho_mode = nullptr;
-	double *eblock = nullptr;       // one per reduce block
-	unsigned *ticket = nullptr;
-	double2 *partial = nullptr;     // partial rows * nslot
-	size_t partial_cap = 0;         // in double2 elements
-	std::vector<DevSplits> splits;  // force splits per requested count
-
-	void release()
-	{
-		cudaFree(segs);
-		cudaFree(rspec);
-		cudaFree(bstart);
-		cudaFree(bspec);
-		cudaFree(slotV);
-		cudaFree(mode_slot);
-		cudaFree(rho_slot);
-		cudaFree(u_slot);
-		cudaFree(rho_mode);
-		cudaFree(eblock);
-		cudaFree(ticket);
-		cudaFree(partial);
-		for (DevSplits &f : splits) {
-			cudaFree(f.kstart);
-			cudaFree(f.kspec);
-		}
-		*this = DevKSet();
+int cci::sm_count()
+{
+	static int n = 0;
+	if (n == 0) {
+		int dev = 0;
+		cudaGetDevice(&dev);
+		if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+			n = 148;
 	}
-};
-
-// Bumped by every device or pinned allocation of the library and by changes of by-value kernel parameters: a
-// captured evaluation graph whose generation differs may hold stale pointers and is captured again.
-std::atomic<unsigned long long> g_alloc_gen{1};
-
-template <class T> int dev_alloc(T **p, size_t n)
-{
-	g_alloc_gen++;
-	*p = nullptr;
-	if (n == 0)
-		n = 1;
-	cudaError_t e = cudaMalloc(reinterpret_cast<void **>(p), n * sizeof(T));
-	if (e != cudaSuccess)
-		return fail(e == cudaErrorMemoryAllocation ? CC_ERR_OOM : CC_ERR_CUDA,
-		            std::string("cudaMalloc: ") + cudaGetErrorString(e));
-	return CC_OK;
+	return n;
 }
 
-template <class T> int upload(T **p, const std::vector<T> &v)
+int cci::get_splits(DevKSet &k, int want, const DevSplits **out)
 {
-	if (int rc = dev_alloc(p, v.size()))
+	for (const DevSplits &f : k.splits)
+		if (f.want == want) {
+			*out = &f;
+			return CC_OK;
+		}
+	DevSplits f;
+	f.want = want;
+	f.host = cc::force_splits(k.plan, want);
+	int rc;
+	if ((rc = upload(&f.kstart, f.host.start)) || (rc = upload(&f.kspec, f.host.spec)))
 		return rc;
-	if (!v.empty())
-		CC_CUDA(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+	k.splits.push_back(f);
+	*out = &k.splits.back();
 	return CC_OK;
 }
 
-template <class T> int upload_into(T *p, const std::vector<T> &v)
-{
-	if (!v.empty())
-		CC_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
-	return CC_OK;
-}
 
-int upload_kset(DevKSet &k, const cc::Plan &plan)
+int cci::upload_kset(DevKSet &k, const cc::Plan &plan)
 {
 	k.release();
 	k.plan = plan;
@@ -155,122 +108,6 @@ int upload_kset(DevKSet &k, const cc::Plan &plan)
 	return CC_OK;
 }
 
-// Device state of cc_minimize (L-BFGS of one configuration), kept by the handle between calls (grow-only).
-struct LbBuffers {
-	double *x = nullptr, *g = nullptr, *d = nullptr, *xt = nullptr, *gt = nullptr, *S = nullptr, *Y = nullptr;
-	double *part = nullptr;
-	cc::LbState *st = nullptr;
-	cc::LbInst *inst = nullptr;
-	void release()
-	{
-		cudaFree(x);
-		cudaFree(g);
-		cudaFree(d);
-		cudaFree(xt);
-		cudaFree(gt);
-		cudaFree(S);
-		cudaFree(Y);
-		cudaFree(part);
-		cudaFree(st);
-		cudaFree(inst);
-		*this = LbBuffers();
-	}
-};
-
-}  // namespace
-
-struct cc_handle {
-	int d = 0;
-	double basis[9] = {0};
-	double recip[9] = {0};
-	double volume = 0;
-	double shift = 0;
-	double rho_offset = 0;
-	std::vector<int32_t> modes;
-	std::vector<double> V;
-	DevKSet main;
-	DevKSet sk;                     // k-set of the last cc_structure_factor call
-	std::vector<int32_t> sk_modes;
-	cudaStream_t stream = nullptr;
-	int64_t N = -1;                 // bound particle count, -1 before cc_set_positions
-	size_t ncap = 0;                // capacity of the per-particle buffers
-	double *d_frac = nullptr, *d_F = nullptr, *d_gfrac = nullptr, *d_partialG = nullptr;
-	size_t partialG_cap = 0;
-	unsigned *d_fcounters = nullptr;
-	double *d_E = nullptr;
-	double *h_pin = nullptr;        // pinned results: E at [0], N*d forces or gradients from [2]
-	size_t pin_cap = 0;
-	double *h_in = nullptr;         // pinned staging of the wrapped positions (N*d), mapped
-	double *d_in = nullptr;         // device view of h_in (read by the first kernel of the host-path graph)
-	double *rho_copy = nullptr;     // while the host-path graph is captured on the three-kernel path: the rho kernel
-	                                // reads the positions from d_in and stores them here (d_frac) for the force kernel
-	size_t in_cap = 0;
-	cudaEvent_t ev_in = nullptr;    // recorded after the last copy out of h_in
-	bool in_pending = false;
-	bool lastF_valid = false;       // h_pin + 2 holds the forces of the bound positions
-	bool fused_ran = false;         // a fused launch ran since the barrier word was last read
-	bool upload_pending = false;    // h_in holds positions not yet copied to d_frac
-	double *d_pin = nullptr;        // device view of h_pin (mapped pinned memory): kernels write E and F there
-	// captured evaluations of cc_energy_grad (upload + kernels writing into h_pin), per (N, precision, forces)
-	struct EvalGraph {
-		int64_t N;
-		int precision, forces;
-		unsigned long long gen;
-		cudaGraphExec_t exec;
-	};
-	std::vector<EvalGraph> graphs;
-	int64_t last_N = -1;            // key and generation of the last direct cc_energy_grad (captured when repeated)
-	int last_precision = -1, last_forces = -1;
-	unsigned long long last_gen = 0;
-	// fused (cooperative) path
-	cc::TabSpec gspec;
-	void *d_tabP = nullptr, *d_tabE = nullptr;
-	size_t tab_cap = 0;             // bytes of each table buffer
-	unsigned *d_bar = nullptr;      // grid barrier words (arrivals, generation, error)
-	double *d_eblockF = nullptr;
-	int eblockF_cap = 0;
-	double2 *d_partialF = nullptr;
-	size_t partialF_cap = 0;
-	std::vector<std::pair<int, int *> > kstarts;   // even segment splits per count
-	bool use_fused = false;         // cc_set_path
-	// S2 form (cc_create_s2): per-slot targets S0, E = sum V (|rho|^2 / N - S0)^2 + shift; split path only
-	double *d_slotS0 = nullptr;
-	// S2 over nsub sub-configurations (cc_create_s2_multiconfig): rho and u per sub-configuration, block partials
-	int nsub = 1;
-	double2 *d_msub = nullptr;      // [2][nsub][nslot]: rho, then u
-	double *d_mpart = nullptr;      // energy partials of the combination, then one scratch word
-	size_t msub_cap = 0, mpart_cap = 0;
-	bool use_nufft = false;         // cc_set_path(CC_PATH_NUFFT)
-	bool auto_path = true;          // CC_PATH_AUTO (default): the NUFFT path where its estimated time is lower
-	double nu_grid_est = -1.0;      // fine-grid points the NUFFT path would use (computed once)
-	// non-uniform FFT path (cc_nufft.cuh), set up at its first use
-	bool nu_ready = false;
-	cc::NufftDev nu = {};
-	int64_t nu_ngrid = 0, nu_nspec = 0;
-	int nu_rho_blocks = 0;
-	int *d_nu_mode_u = nullptr;
-	std::vector<void *> nu_bufs;    // device buffers owned by the NUFFT set-up
-	cufftHandle nu_p1 = 0, nu_p2 = 0;
-	bool nu_p1_ok = false, nu_p2_ok = false;
-	// Monte Carlo: rho in mode order of the bound positions, the trial rho and the device modes
-	int32_t *d_modes = nullptr;
-	double *d_modeV = nullptr;
-	double2 *d_rho_trial = nullptr, *d_rho_cur = nullptr;
-	double *d_mc_part = nullptr;
-	bool mc_valid = false, mc_pending = false;
-	const int *d_skip = nullptr;    // evaluations do nothing while *d_skip != 0 (set by cc_minimize)
-	bool timing = false;            // cc_set_timing
-	// cc_minimize's state, kept between calls so that a minimisation makes no allocation call into the CUDA driver
-	// once the handle has run one of its size: FP64 / mixed buffers (capacities n variables, m pairs, nblk dot
-	// blocks) and the batch of one that runs the precision schedule (for sched_N particles)
-	LbBuffers lb;
-	int lb_n = 0, lb_m = 0, lb_nblk = 0;
-	cc_batch *sched_batch = nullptr;
-	int64_t sched_N = -1;
-	std::vector<cudaEvent_t> ev;    // 3 events per timed evaluation
-	size_t ev_used = 0;
-};
-
 namespace {
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -281,17 +118,6 @@ struct Launch {
 	int want_force;                       // force: requested number of segment splits
 };
 
-int sm_count()
-{
-	static int n = 0;
-	if (n == 0) {
-		int dev = 0;
-		cudaGetDevice(&dev);
-		if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
-			n = 148;
-	}
-	return n;
-}
 
 // Record a timing event; inside a stream capture it must be an external record node to carry a timestamp.
 cudaError_t record_timing(cudaEvent_t e, cudaStream_t st)
@@ -302,13 +128,6 @@ cudaError_t record_timing(cudaEvent_t e, cudaStream_t st)
 	return cudaEventRecord(e, st);
 }
 
-constexpr size_t kRhoTabBudget = 48 * 1024;   // shared memory for one chunk of rho tables
-
-template <typename C> size_t rho_smem(int row, int chunk, int L)
-{
-	return std::max((size_t)chunk * (row | 1) * sizeof(C), (size_t)cc::kRhoWarps * 32 * L * sizeof(double2));
-}
-template <typename C> size_t force_smem(int row, int d) { return cc::force_smem_bytes<C>(row, d, 8); }
 
 int rho_wave(int d, bool mixed, int csize, size_t smem);   // resident rho blocks (clusters of csize) on the device
 int force_wave(int d, bool mixed, size_t smem);            // resident force blocks on the device
@@ -378,22 +197,6 @@ Launch choose_launch(const cc::Plan &p, int64_t N, bool mixed)
 // ---------------------------------------------------------------------------------------------------------------
 // kernel dispatch
 // ---------------------------------------------------------------------------------------------------------------
-// The same for kernels of several arguments.
-template <typename... KArgs, typename... Args>
-cudaError_t launch_pdl_n(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args... args)
-{
-	cudaLaunchConfig_t cfg = {};
-	cfg.gridDim = grid;
-	cfg.blockDim = block;
-	cfg.dynamicSmemBytes = smem;
-	cfg.stream = st;
-	cudaLaunchAttribute attr[1];
-	attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-	attr[0].val.programmaticStreamSerializationAllowed = 1;
-	cfg.attrs = attr;
-	cfg.numAttrs = 1;
-	return cudaLaunchKernelEx(&cfg, kern, args...);
-}
 
 // Launch with programmatic stream serialization: the kernel may be scheduled while the previous kernel on the stream
 // drains; it calls cudaGridDependencySynchronize() before it reads that kernel's results.
@@ -569,23 +372,6 @@ int launch_force(int d, const cc::ForceArgs &a, bool mixed, int64_t N, int row, 
 }
 
 // force splits for `want`, uploaded once and cached on the k-set
-int get_splits(DevKSet &k, int want, const DevSplits **out)
-{
-	for (const DevSplits &f : k.splits)
-		if (f.want == want) {
-			*out = &f;
-			return CC_OK;
-		}
-	DevSplits f;
-	f.want = want;
-	f.host = cc::force_splits(k.plan, want);
-	int rc;
-	if ((rc = upload(&f.kstart, f.host.start)) || (rc = upload(&f.kspec, f.host.spec)))
-		return rc;
-	k.splits.push_back(f);
-	*out = &k.splits.back();
-	return CC_OK;
-}
 
 // ---------------------------------------------------------------------------------------------------------------
 // buffers
@@ -1266,13 +1052,6 @@ int check_handle(const cc_handle *h)
 {
 	if (!h)
 		return fail(CC_ERR_ARG, "null handle");
-	return CC_OK;
-}
-
-int check_prec(int precision)
-{
-	if (precision != CC_PREC_FP64 && precision != CC_PREC_MIXED)
-		return fail(CC_ERR_ARG, "precision must be CC_PREC_FP64 or CC_PREC_MIXED");
 	return CC_OK;
 }
 
@@ -2418,816 +2197,7 @@ int cc_minimize(cc_handle *h, int64_t N, double *frac, const cc_lbfgs_opts *opts
 
 }  // extern "C"
 
-// ===============================================================================================================
-// batches
-// ===============================================================================================================
-namespace {
-
-// carve 256-byte aligned pieces out of one device allocation
-struct Arena {
-	unsigned char *base = nullptr;
-	size_t used = 0, cap = 0;
-	size_t take(size_t bytes)
-	{
-		const size_t off = used;
-		used += (bytes + 255) / 256 * 256;
-		return off;
-	}
-	template <class T> T *at(size_t off) { return reinterpret_cast<T *>(base + off); }
-};
-
-// One dimension's instances of a batch, evaluated by the multi-instance rho / reduce / force kernels: per instance
-// the arguments of each kernel (set 0: the batch positions and outputs; set 1: a minimisation's trial points), the
-// prefix sums of the blocks of each launch and the grid shapes.
-struct BatchGroup {
-	int D = 0;
-	std::vector<int> members;            // instance indices
-	cc::RhoArgs *d_rho[2] = {nullptr, nullptr};
-	cc::ReduceArgs *d_red[2] = {nullptr, nullptr};
-	cc::ForceArgs *d_force[2] = {nullptr, nullptr};
-	int *d_pre = nullptr;                // 3 x (B + 1): rho, reduce and force blocks
-	int *d_shape = nullptr;              // 3 x B: block groups, reduce chunks, particle groups
-	unsigned *d_queue = nullptr;         // 2 words per launch kind: work queues of the persistent launches
-	int total[3] = {0, 0, 0};
-	int rho_row = 1, force_row = 1;      // largest table rows (shared memory of the launches)
-	std::vector<cc::RhoArgs> rho;        // host copies of set 0
-	std::vector<cc::ReduceArgs> red;
-	std::vector<cc::ForceArgs> force;
-};
-
-using cc::kBatchChunk;
-using cc::kBatchPerSplit;
-using cc::kBatchSegsPerSplit;
-
-// an instance's evaluation buffers in the batch arena
-struct BatchBufs {
-	size_t o_part, o_rho, o_u, o_eb, o_tk, o_pg, o_fc;
-};
-
-// tile shapes the autotuner times: particles per rho block, segments per force block
-constexpr int kTuneSplits[] = {32, 64, 128, 256, 512, 1024};
-constexpr int kTuneSegs[] = {32, 64, 128, 256, 512, 1024};
-
-}  // namespace
-
-struct cc_batch {
-	std::vector<cc_handle *> h;
-	std::vector<int64_t> N;
-	std::vector<BatchGroup> groups;
-	Arena arena;
-	std::vector<size_t> off_frac, off_F, off_E;
-	std::vector<BatchBufs> bufs;
-	int per_split = 0, segs_per_split = 0;   // the tile shape in use
-	cudaStream_t stream = nullptr;
-	// the groups after the first run on side streams, forked from and joined back into the launching stream
-	cudaStream_t side[2] = {nullptr, nullptr};
-	cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
-	// L-BFGS state of cc_batch_minimize, kept between calls (grow-only): a minimisation makes no allocation call
-	// into the CUDA driver once the batch has run one
-	unsigned char *lb_base = nullptr;
-	size_t lb_cap = 0;
-	cc::LbInst *d_lb = nullptr;   // 2 x d_lb_cap: the instances in order, then grouped by dimension
-	cc::LbBrief *d_brief = nullptr;
-	int d_lb_cap = 0;
-};
-
-namespace {
-
-template <int D, bool MIXED> cudaError_t multi_attrs()
-{
-	typedef typename std::conditional<MIXED, float2, double2>::type C;
-	static cudaError_t e = [] {
-		cudaError_t r = cudaFuncSetAttribute(cc::cc_mrho_kernel<D, 8, MIXED>,
-		                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-		                                     (int)rho_smem<C>(cc::kMaxRow, kBatchChunk, 8));
-		if (r == cudaSuccess)
-			r = cudaFuncSetAttribute(cc::cc_mforce_kernel<D, 8, MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			                         (int)force_smem<C>(cc::kMaxRow, D));
-		return r;
-	}();
-	return e;
-}
-
-template <int D, bool MIXED>
-int multi_launch_raw(const cc::RhoArgs *rho, const cc::ReduceArgs *red, const cc::ForceArgs *force, const int *pre,
-                     const int *shape, int B, const int total[3], int rho_row, int force_row, unsigned *queue,
-                     cudaStream_t st)
-{
-	typedef typename std::conditional<MIXED, float2, double2>::type C;
-	if (cudaError_t e = multi_attrs<D, MIXED>())
-		return fail(CC_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
-	const int want = MIXED ? 0 : 1;
-	// persistent grids: at most the resident blocks (3 per SM for rho and force, 8 for the reduction)
-	const int res3 = 3 * sm_count(), res8 = 8 * sm_count();
-	if (total[0] > 0)
-		CC_CUDA(launch_pdl_n(cc::cc_mrho_kernel<D, 8, MIXED>, dim3(std::min(total[0], res3)), dim3(cc::kRhoThreads),
-		                   rho_smem<C>(rho_row, kBatchChunk, 8), st, rho, pre, shape, B, want, queue));
-	if (total[1] > 0)
-		CC_CUDA(launch_pdl_n(cc::cc_mreduce_kernel, dim3(std::min(total[1], res8)), dim3(cc::kRedThreads), 0, st, red,
-		                   pre + (B + 1), shape + B, B, want, queue + 2));
-	if (total[2] > 0)
-		CC_CUDA(launch_pdl_n(cc::cc_mforce_kernel<D, 8, MIXED>, dim3(std::min(total[2], res3)), dim3(cc::kForceThreads),
-		                   force_smem<C>(force_row, D), st, force, pre + 2 * (B + 1), shape + 2 * B, B, want,
-		                   queue + 4));
-	return CC_OK;
-}
-
-template <int D> cudaError_t multi_sched_attrs()
-{
-	static cudaError_t e = [] {
-		cudaError_t r = cudaFuncSetAttribute(cc::cc_mrho_sched_kernel<D, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-		                                     (int)rho_smem<double2>(cc::kMaxRow, kBatchChunk, 8));
-		if (r == cudaSuccess)
-			r = cudaFuncSetAttribute(cc::cc_mforce_sched_kernel<D, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			                         (int)force_smem<double2>(cc::kMaxRow, D));
-		return r;
-	}();
-	return e;
-}
-
-// one launch of each kernel for a group whose instances take their precision from their stage words
-template <int D> int multi_launch_sched_t(BatchGroup &g, int which, cudaStream_t st)
-{
-	if (cudaError_t attr = multi_sched_attrs<D>())
-		return fail(CC_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(attr));
-	const int B = (int)g.members.size();
-	const int res3 = 3 * sm_count(), res8 = 8 * sm_count();
-	if (g.total[0] > 0)
-		CC_CUDA(launch_pdl_n(cc::cc_mrho_sched_kernel<D, 8>, dim3(std::min(g.total[0], res3)), dim3(cc::kRhoThreads),
-		                   rho_smem<double2>(g.rho_row, kBatchChunk, 8), st, (const cc::RhoArgs *)g.d_rho[which],
-		                   (const int *)g.d_pre, (const int *)g.d_shape, B, g.d_queue));
-	if (g.total[1] > 0)
-		CC_CUDA(launch_pdl_n(cc::cc_mreduce_kernel, dim3(std::min(g.total[1], res8)), dim3(cc::kRedThreads), 0, st,
-		                   (const cc::ReduceArgs *)g.d_red[which], (const int *)g.d_pre + (B + 1),
-		                   (const int *)g.d_shape + B, B, -1, g.d_queue + 2));
-	if (g.total[2] > 0)
-		CC_CUDA(launch_pdl_n(cc::cc_mforce_sched_kernel<D, 8>, dim3(std::min(g.total[2], res3)),
-		                   dim3(cc::kForceThreads), force_smem<double2>(g.force_row, D), st,
-		                   (const cc::ForceArgs *)g.d_force[which], (const int *)g.d_pre + 2 * (B + 1),
-		                   (const int *)g.d_shape + 2 * B, B, g.d_queue + 4));
-	return CC_OK;
-}
-
-// the three launches of one group: which = 0 (batch positions) or 1 (minimisation trial points)
-template <int D, bool MIXED> int multi_launch_t(BatchGroup &g, int which, cudaStream_t st)
-{
-	return multi_launch_raw<D, MIXED>(g.d_rho[which], g.d_red[which], g.d_force[which], g.d_pre, g.d_shape,
-	                                  (int)g.members.size(), g.total, g.rho_row, g.force_row, g.d_queue, st);
-}
-
-}  // namespace
-
-int cc::launch_multi(int D, bool mixed, const RhoArgs *rho, const ReduceArgs *red, const ForceArgs *force,
-                     const int *pre, const int *shape, int B, const int total[3], int rho_row, int force_row,
-                     unsigned *queue, cudaStream_t st)
-{
-	if (B < 1)
-		return CC_OK;
-	switch (D) {
-	case 1: return mixed ? multi_launch_raw<1, true>(rho, red, force, pre, shape, B, total, rho_row, force_row, queue, st)
-	                     : multi_launch_raw<1, false>(rho, red, force, pre, shape, B, total, rho_row, force_row, queue, st);
-	case 2: return mixed ? multi_launch_raw<2, true>(rho, red, force, pre, shape, B, total, rho_row, force_row, queue, st)
-	                     : multi_launch_raw<2, false>(rho, red, force, pre, shape, B, total, rho_row, force_row, queue, st);
-	default: return mixed ? multi_launch_raw<3, true>(rho, red, force, pre, shape, B, total, rho_row, force_row, queue, st)
-	                      : multi_launch_raw<3, false>(rho, red, force, pre, shape, B, total, rho_row, force_row, queue, st);
-	}
-}
-
-namespace {
-
-int multi_launch(BatchGroup &g, bool mixed, int which, cudaStream_t st)
-{
-	switch (g.D) {
-	case 1: return mixed ? multi_launch_t<1, true>(g, which, st) : multi_launch_t<1, false>(g, which, st);
-	case 2: return mixed ? multi_launch_t<2, true>(g, which, st) : multi_launch_t<2, false>(g, which, st);
-	default: return mixed ? multi_launch_t<3, true>(g, which, st) : multi_launch_t<3, false>(g, which, st);
-	}
-}
-
-// (Re)build every group's evaluation descriptors (set 0) for a tile shape: per_split particles per rho block and
-// force splits of about segs_per_split segments; the arena holds the buffers of every candidate shape.
-int batch_build(cc_batch *b, int per_split, int segs_per_split)
-{
-	for (BatchGroup &g : b->groups) {
-		const int B = (int)g.members.size();
-		std::vector<int> pre(3 * (B + 1), 0), shape(3 * B, 0);
-		g.rho.clear();
-		g.red.clear();
-		g.force.clear();
-		g.rho_row = g.force_row = 1;
-		for (int k = 0; k < B; k++) {
-			const int i = g.members[k];
-			cc_handle *h = b->h[i];
-			const cc::Plan &p = h->main.plan;
-			const BatchBufs &q = b->bufs[i];
-			const int64_t n = b->N[i];
-			const int nsplit = (int)((n + per_split - 1) / per_split);
-			const int nchunks = (p.nslot + 31) / 32, pgroups = (int)((n + 31) / 32);
-			const DevSplits *f = nullptr;
-			const int want = (int)std::max<int64_t>(1, (p.real_segs + segs_per_split - 1) / segs_per_split);
-			if (int rc = get_splits(h->main, want, &f))
-				return rc;
-			cc::RhoArgs ra = {};
-			ra.frac = b->arena.at<double>(b->off_frac[i]);
-			ra.N = (int)n;
-			ra.per_split = per_split;
-			ra.chunk = kBatchChunk;
-			ra.segs = h->main.segs;
-			ra.bstart = h->main.bstart;
-			ra.bspec = h->main.bspec;
-			ra.nseg = (int)p.segs.size();
-			ra.nslot = p.nslot;
-			ra.partial = b->arena.at<double2>(q.o_part);
-			cc::ReduceArgs rr = {};
-			rr.partial = ra.partial;
-			rr.nsplit = nsplit;
-			rr.nslot = p.nslot;
-			rr.slotV = h->main.slotV;
-			rr.rho_offset = h->rho_offset;
-			rr.rho_slot = b->arena.at<double2>(q.o_rho);
-			rr.u_slot = b->arena.at<double2>(q.o_u);
-			rr.eblock = b->arena.at<double>(q.o_eb);
-			rr.ticket = b->arena.at<unsigned>(q.o_tk);
-			rr.inv_vol = 1.0 / h->volume;
-			rr.shift = h->shift;
-			rr.E_out = b->arena.at<double>(b->off_E[i]);
-			rr.finalize = 0;   // the force kernel sums the energy terms
-			cc::ForceArgs fa = {};
-			fa.frac = ra.frac;
-			fa.N = ra.N;
-			fa.segs = h->main.segs;
-			fa.kstart = f->kstart;
-			fa.kspec = f->kspec;
-			fa.nksplit = f->host.count();
-			fa.u_slot = rr.u_slot;
-			fa.nseg = ra.nseg;
-			fa.partialG = b->arena.at<double>(q.o_pg);
-			fa.counters = b->arena.at<unsigned>(q.o_fc);
-			for (int c = 0; c < 9; c++)
-				fa.recip[c] = h->recip[c];
-			fa.fscale = 2.0 / h->volume;
-			fa.F_out = b->arena.at<double>(b->off_F[i]);
-			fa.gfrac_out = nullptr;
-			fa.eblock = rr.eblock;
-			fa.neblock = nchunks;
-			fa.inv_vol = rr.inv_vol;
-			fa.shift = rr.shift;
-			fa.E_out = rr.E_out;
-			g.rho.push_back(ra);
-			g.red.push_back(rr);
-			g.force.push_back(fa);
-			const int c[3] = {p.nbgroups() * nsplit, nchunks, pgroups * fa.nksplit};
-			const int sh[3] = {p.nbgroups(), nchunks, pgroups};
-			for (int ph = 0; ph < 3; ph++) {
-				pre[ph * (B + 1) + k + 1] = pre[ph * (B + 1) + k] + c[ph];
-				shape[ph * B + k] = sh[ph];
-			}
-			g.rho_row = std::max(g.rho_row, p.block_max_row);
-			g.force_row = std::max(g.force_row, f->host.max_row);
-		}
-		for (int ph = 0; ph < 3; ph++)
-			g.total[ph] = pre[ph * (B + 1) + B];
-		int rc;
-		if ((rc = upload_into(g.d_rho[0], g.rho)) || (rc = upload_into(g.d_red[0], g.red)) ||
-		    (rc = upload_into(g.d_force[0], g.force)) || (rc = upload_into(g.d_pre, pre)) ||
-		    (rc = upload_into(g.d_shape, shape)))
-			return rc;
-	}
-	b->per_split = per_split;
-	b->segs_per_split = segs_per_split;
-	return CC_OK;
-}
-
-// evaluate every group with the given descriptors (lb = the minimisation's); precision CC_PREC_SCHEDULE launches
-// kernels that evaluate each instance at the precision of its stage word (FP64 where it has none)
-// one group's evaluation (the descriptors of set lb ? 1 : 0) on stream gs
-int group_eval(BatchGroup &g, bool lb, int precision, cudaStream_t gs)
-{
-	if (precision == CC_PREC_SCHEDULE)
-		return g.D == 1 ? multi_launch_sched_t<1>(g, lb ? 1 : 0, gs)
-		     : g.D == 2 ? multi_launch_sched_t<2>(g, lb ? 1 : 0, gs)
-		                : multi_launch_sched_t<3>(g, lb ? 1 : 0, gs);
-	return multi_launch(g, precision == CC_PREC_MIXED, lb ? 1 : 0, gs);
-}
-
-// The groups (one per dimension) are independent: the first runs on `st`, the others on side streams forked from
-// and joined back into `st` (parallel branches when captured in a graph), so their launches overlap on the device.
-int batch_eval(cc_batch *b, bool lb, int precision, cudaStream_t st)
-{
-	const int ng = (int)b->groups.size();
-	if (ng > 1)
-		CC_CUDA(cudaEventRecord(b->ev_fork, st));
-	for (int k = 0; k < ng; k++) {
-		BatchGroup &g = b->groups[k];
-		cudaStream_t gs = k == 0 ? st : b->side[k - 1];
-		if (k > 0)
-			CC_CUDA(cudaStreamWaitEvent(gs, b->ev_fork, 0));
-		if (int rc = group_eval(g, lb, precision, gs))
-			return rc;
-		if (k > 0) {
-			CC_CUDA(cudaEventRecord(b->ev_join[k - 1], gs));
-			CC_CUDA(cudaStreamWaitEvent(st, b->ev_join[k - 1], 0));
-		}
-	}
-	return CC_OK;
-}
-
-// the multi-instance kernels wait on nothing: no device timeout can be pending
-int batch_check_barrier(cc_batch *) { return CC_OK; }
-
-}  // namespace
-
 extern "C" {
-
-int cc_batch_create(int count, cc_handle *const *handles, const int64_t *N, cc_batch **out)
-{
-	if (!out || count < 1 || !handles || !N)
-		return fail(CC_ERR_ARG, "invalid batch arguments");
-	*out = nullptr;
-	for (int i = 0; i < count; i++) {
-		if (!handles[i] || N[i] < 1 || N[i] > (1 << 26) || handles[i]->main.plan.nslot == 0)
-			return fail(CC_ERR_ARG, "every instance needs a handle with constraints and 1 <= N <= 2^26");
-		if (handles[i]->d_slotS0)
-			return fail(CC_ERR_ARG, "batches hold the plain collective-coordinate form only");
-	}
-	cc_batch *b = new cc_batch();
-	b->h.assign(handles, handles + count);
-	b->N.assign(N, N + count);
-	// per instance: buffers sized for every tile shape the autotuner may choose (the most particle splits and force
-	// splits among the candidates), carved out of one arena
-	b->off_frac.resize(count);
-	b->off_F.resize(count);
-	b->off_E.resize(count);
-	b->bufs.resize(count);
-	for (int i = 0; i < count; i++) {
-		cc_handle *h = handles[i];
-		const cc::Plan &p = h->main.plan;
-		const int64_t n = N[i];
-		BatchBufs &q = b->bufs[i];
-		int max_nks = 1;
-		for (int segs : kTuneSegs) {
-			const DevSplits *f = nullptr;
-			const int want = (int)std::max<int64_t>(1, (p.real_segs + segs - 1) / segs);
-			if (int rc = get_splits(h->main, want, &f)) {
-				delete b;
-				return rc;
-			}
-			max_nks = std::max(max_nks, f->host.count());
-		}
-		const int max_nsplit = (int)((n + kTuneSplits[0] - 1) / kTuneSplits[0]);
-		const int nchunks = (p.nslot + 31) / 32, pgroups = (int)((n + 31) / 32);
-		b->off_frac[i] = b->arena.take(sizeof(double) * n * h->d);
-		b->off_F[i] = b->arena.take(sizeof(double) * n * h->d);
-		b->off_E[i] = b->arena.take(sizeof(double));
-		q.o_part = b->arena.take(sizeof(double2) * (size_t)max_nsplit * p.nslot);
-		q.o_rho = b->arena.take(sizeof(double2) * p.nslot);
-		q.o_u = b->arena.take(sizeof(double2) * p.nslot);
-		q.o_eb = b->arena.take(sizeof(double) * nchunks);
-		q.o_tk = b->arena.take(sizeof(unsigned));
-		q.o_pg = b->arena.take(sizeof(double) * (size_t)max_nks * n * h->d);
-		q.o_fc = b->arena.take(sizeof(unsigned) * pgroups);
-	}
-	int rc;
-	if ((rc = dev_alloc(&b->arena.base, b->arena.used))) {
-		cc_batch_destroy(b);
-		return rc;
-	}
-	b->arena.cap = b->arena.used;
-	if (cudaMemset(b->arena.base, 0, b->arena.used) != cudaSuccess ||
-	    cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
-	    cudaStreamCreateWithFlags(&b->side[0], cudaStreamNonBlocking) != cudaSuccess ||
-	    cudaStreamCreateWithFlags(&b->side[1], cudaStreamNonBlocking) != cudaSuccess ||
-	    cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-	    cudaEventCreateWithFlags(&b->ev_join[0], cudaEventDisableTiming) != cudaSuccess ||
-	    cudaEventCreateWithFlags(&b->ev_join[1], cudaEventDisableTiming) != cudaSuccess) {
-		cc_batch_destroy(b);
-		return fail(CC_ERR_CUDA, "batch initialisation failed");
-	}
-	// one group per dimension, instances by decreasing work (the work queues then hand out the longest items first)
-	for (int D = 1; D <= 3; D++) {
-		BatchGroup g;
-		g.D = D;
-		for (int i = 0; i < count; i++)
-			if (handles[i]->d == D)
-				g.members.push_back(i);
-		if (g.members.empty())
-			continue;
-		std::stable_sort(g.members.begin(), g.members.end(), [&](int x, int y) {
-			return (double)N[x] * handles[x]->main.plan.real_segs > (double)N[y] * handles[y]->main.plan.real_segs;
-		});
-		const int B = (int)g.members.size();
-		b->groups.push_back(g);
-		BatchGroup &gg = b->groups.back();
-		if ((rc = dev_alloc(&gg.d_rho[0], B)) || (rc = dev_alloc(&gg.d_red[0], B)) ||
-		    (rc = dev_alloc(&gg.d_force[0], B)) || (rc = dev_alloc(&gg.d_rho[1], B)) ||
-		    (rc = dev_alloc(&gg.d_red[1], B)) || (rc = dev_alloc(&gg.d_force[1], B)) ||
-		    (rc = dev_alloc(&gg.d_pre, 3 * (B + 1))) || (rc = dev_alloc(&gg.d_shape, 3 * B)) ||
-		    (rc = dev_alloc(&gg.d_queue, 6)) ||
-		    (rc = (cudaMemset(gg.d_queue, 0, 6 * sizeof(unsigned)) == cudaSuccess ? CC_OK : CC_ERR_CUDA))) {
-			cc_batch_destroy(b);
-			return rc;
-		}
-	}
-	if ((rc = batch_build(b, kBatchPerSplit, kBatchSegsPerSplit))) {
-		cc_batch_destroy(b);
-		return rc;
-	}
-	*out = b;
-	return CC_OK;
-}
-
-int cc_batch_autotune(cc_batch *b, int reps, int *per_split, int *segs_per_split)
-{
-	if (!b || reps < 1)
-		return fail(CC_ERR_ARG, "invalid autotune arguments");
-	cudaEvent_t e0, e1;
-	CC_CUDA(cudaEventCreate(&e0));
-	CC_CUDA(cudaEventCreate(&e1));
-	float best = 1e30f;
-	int bp = b->per_split, bs = b->segs_per_split, rc = CC_OK;
-	for (int ps : kTuneSplits)
-		for (int sg : kTuneSegs) {
-			if ((rc = batch_build(b, ps, sg)) || (rc = batch_eval(b, false, CC_PREC_FP64, b->stream)))
-				break;
-			if (cudaEventRecord(e0, b->stream) != cudaSuccess) {
-				rc = fail(CC_ERR_CUDA, "cudaEventRecord failed");
-				break;
-			}
-			for (int r = 0; r < reps && rc == CC_OK; r++)
-				rc = batch_eval(b, false, CC_PREC_FP64, b->stream);
-			if (rc)
-				break;
-			float ms = 0.0f;
-			if (cudaEventRecord(e1, b->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
-			    cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
-				rc = fail(CC_ERR_CUDA, "autotune timing failed");
-				break;
-			}
-			if (ms < best) {
-				best = ms;
-				bp = ps;
-				bs = sg;
-			}
-		}
-	cudaEventDestroy(e0);
-	cudaEventDestroy(e1);
-	if (rc)
-		return rc;
-	if ((rc = batch_build(b, bp, bs)))
-		return rc;
-	if (per_split)
-		*per_split = bp;
-	if (segs_per_split)
-		*segs_per_split = bs;
-	return CC_OK;
-}
-
-int cc_batch_destroy(cc_batch *b)
-{
-	if (!b)
-		return CC_OK;
-	if (b->stream)
-		cudaStreamSynchronize(b->stream);
-	for (BatchGroup &g : b->groups) {
-		for (int w = 0; w < 2; w++) {
-			cudaFree(g.d_rho[w]);
-			cudaFree(g.d_red[w]);
-			cudaFree(g.d_force[w]);
-		}
-		cudaFree(g.d_pre);
-		cudaFree(g.d_shape);
-		cudaFree(g.d_queue);
-	}
-	cudaFree(b->arena.base);
-	cudaFree(b->lb_base);
-	cudaFree(b->d_lb);
-	cudaFree(b->d_brief);
-	for (int k = 0; k < 2; k++) {
-		if (b->side[k]) {
-			cudaStreamSynchronize(b->side[k]);
-			cudaStreamDestroy(b->side[k]);
-		}
-		if (b->ev_join[k])
-			cudaEventDestroy(b->ev_join[k]);
-	}
-	if (b->ev_fork)
-		cudaEventDestroy(b->ev_fork);
-	if (b->stream)
-		cudaStreamDestroy(b->stream);
-	delete b;
-	return CC_OK;
-}
-
-int cc_batch_set_positions(cc_batch *b, const double *const *frac)
-{
-	if (!b || !frac)
-		return fail(CC_ERR_ARG, "invalid batch arguments");
-	for (size_t i = 0; i < b->h.size(); i++) {
-		const size_t n = (size_t)b->N[i] * b->h[i]->d;
-		std::vector<double> w(n);
-		for (size_t k = 0; k < n; k++) {
-			if (!std::isfinite(frac[i][k]))
-				return fail(CC_ERR_ARG, "non-finite fractional coordinate");
-			double v = frac[i][k] - std::floor(frac[i][k]);
-			w[k] = v - std::floor(v);
-		}
-		CC_CUDA(cudaMemcpyAsync(b->arena.at<double>(b->off_frac[i]), w.data(), sizeof(double) * n,
-		                        cudaMemcpyHostToDevice, b->stream));
-		CC_CUDA(cudaStreamSynchronize(b->stream));
-	}
-	return CC_OK;
-}
-
-int cc_batch_eval_device(cc_batch *b, int precision, void *stream)
-{
-	if (!b)
-		return fail(CC_ERR_ARG, "null batch");
-	if (int rc = check_prec(precision))
-		return rc;
-	return batch_eval(b, false, precision, stream ? static_cast<cudaStream_t>(stream) : b->stream);
-}
-
-int cc_batch_energy_grad(cc_batch *b, double *E, double *const *F, int precision)
-{
-	if (!b || !E)
-		return fail(CC_ERR_ARG, "invalid batch arguments");
-	if (int rc = cc_batch_eval_device(b, precision, b->stream))
-		return rc;
-	CC_CUDA(cudaStreamSynchronize(b->stream));
-	if (int rc = batch_check_barrier(b))
-		return rc;
-	for (size_t i = 0; i < b->h.size(); i++) {
-		CC_CUDA(cudaMemcpy(&E[i], b->arena.at<double>(b->off_E[i]), sizeof(double), cudaMemcpyDeviceToHost));
-		if (F && F[i])
-			CC_CUDA(cudaMemcpy(F[i], b->arena.at<double>(b->off_F[i]), sizeof(double) * b->N[i] * b->h[i]->d,
-			                   cudaMemcpyDeviceToHost));
-	}
-	return CC_OK;
-}
-
-int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opts, cc_lbfgs_result *results)
-{
-	if (!b || !frac)
-		return fail(CC_ERR_ARG, "invalid batch arguments");
-	cc_lbfgs_opts o;
-	cc_lbfgs_defaults(&o);
-	if (opts)
-		o = *opts;
-	if (o.history < 1 || o.history > cc::kLbMaxHist || o.iters_per_check < 1 ||
-	    (o.precision != CC_PREC_FP64 && o.precision != CC_PREC_MIXED && o.precision != CC_PREC_SCHEDULE))
-		return fail(CC_ERR_ARG, "invalid minimisation options");
-	const int count = (int)b->h.size(), m = o.history;
-	int maxn = 0;
-	for (int i = 0; i < count; i++)
-		maxn = std::max(maxn, (int)(b->N[i] * b->h[i]->d));
-	const int nblk = cc::lb_blocks(maxn, cc::kLbMaxBlocks);
-	// L-BFGS buffers of every instance in one allocation
-	Arena ar;
-	std::vector<size_t> ox(count), og(count), od(count), oxt(count), ogt(count), oS(count), oY(count), op(count),
-	    ost(count);
-	for (int i = 0; i < count; i++) {
-		const size_t n = (size_t)b->N[i] * b->h[i]->d;
-		ox[i] = ar.take(8 * n);
-		og[i] = ar.take(8 * n);
-		od[i] = ar.take(8 * n);
-		oxt[i] = ar.take(8 * n);
-		ogt[i] = ar.take(8 * n);
-		oS[i] = ar.take(8 * n * m);
-		oY[i] = ar.take(8 * n * m);
-		op[i] = ar.take(8 * (size_t)nblk * cc::lb_ndots(m));
-		ost[i] = ar.take(sizeof(cc::LbState));
-	}
-	int rc;
-	if (b->lb_cap < ar.used) {
-		cudaFree(b->lb_base);
-		b->lb_base = nullptr;
-		b->lb_cap = 0;
-		if ((rc = dev_alloc(&b->lb_base, ar.used)))
-			return rc;
-		b->lb_cap = ar.used;
-	}
-	if (b->d_lb_cap < count) {
-		cudaFree(b->d_lb);
-		cudaFree(b->d_brief);
-		b->d_lb = nullptr;
-		b->d_brief = nullptr;
-		b->d_lb_cap = 0;
-		if ((rc = dev_alloc(&b->d_lb, 2 * (size_t)count)) || (rc = dev_alloc(&b->d_brief, count)))
-			return rc;
-		b->d_lb_cap = count;
-	}
-	ar.base = b->lb_base;
-	cc::LbInst *d_lb = b->d_lb;
-	auto cleanup = [&](int code) { return code; };
-	std::vector<cc::LbInst> lbi(count);
-	cc::LbState s0;
-	std::memset(&s0, 0, sizeof(s0));
-	s0.E = INFINITY;
-	s0.gamma = 1.0;
-	s0.gtol = o.gtol;
-	s0.ftol = o.ftol;
-	s0.max_evals = o.max_evals;
-	s0.m = m;
-	s0.newslot = -1;
-	for (int i = 0; i < count; i++) {
-		const size_t n = (size_t)b->N[i] * b->h[i]->d;
-		cc::LbInst &l = lbi[i];
-		l.n = (int)n;
-		l.x = ar.at<double>(ox[i]);
-		l.g = ar.at<double>(og[i]);
-		l.d = ar.at<double>(od[i]);
-		l.xt = ar.at<double>(oxt[i]);
-		l.gt = ar.at<double>(ogt[i]);
-		l.S = ar.at<double>(oS[i]);
-		l.Y = ar.at<double>(oY[i]);
-		l.part = ar.at<double>(op[i]);
-		l.st = ar.at<cc::LbState>(ost[i]);
-		std::vector<double> x0(n);
-		for (size_t k = 0; k < n; k++) {
-			if (!std::isfinite(frac[i][k]))
-				return cleanup(fail(CC_ERR_ARG, "non-finite start"));
-			double v = frac[i][k] - std::floor(frac[i][k]);
-			x0[k] = v - std::floor(v);
-		}
-		CC_CUDA(cudaMemcpy(l.x, x0.data(), 8 * n, cudaMemcpyHostToDevice));
-		CC_CUDA(cudaMemcpy(l.xt, x0.data(), 8 * n, cudaMemcpyHostToDevice));
-		CC_CUDA(cudaMemset(l.g, 0, 8 * n));
-		CC_CUDA(cudaMemset(l.d, 0, 8 * n));
-		s0.stopval = o.stopval == CC_STOPVAL_GROUND_STATE ? 1e-20 * (double)b->N[i] : o.stopval;
-		s0.sched = o.precision == CC_PREC_SCHEDULE;
-		s0.stage = o.precision == CC_PREC_FP64 ? 1 : 0;
-		s0.switch_E = o.switch_energy_per_particle * (double)b->N[i];
-		CC_CUDA(cudaMemcpy(l.st, &s0, sizeof(s0), cudaMemcpyHostToDevice));
-	}
-	if ((rc = upload_into(d_lb, lbi)))
-		return cleanup(rc);
-	// the same instances grouped by dimension (each group's L-BFGS kernels run on its own stream)
-	std::vector<cc::LbInst> lbg;
-	std::vector<int> g_off, g_maxn;
-	for (BatchGroup &g : b->groups) {
-		g_off.push_back((int)lbg.size());
-		int mx = 0;
-		for (int i : g.members) {
-			lbg.push_back(lbi[i]);
-			mx = std::max(mx, lbi[i].n);
-		}
-		g_maxn.push_back(mx);
-	}
-	CC_CUDA(cudaMemcpy(d_lb + count, lbg.data(), sizeof(cc::LbInst) * lbg.size(), cudaMemcpyHostToDevice));
-	// minimisation descriptors: evaluate at x_trial into the L-BFGS buffers, skip finished instances
-	for (BatchGroup &g : b->groups) {
-		std::vector<cc::RhoArgs> ra = g.rho;
-		std::vector<cc::ReduceArgs> rr = g.red;
-		std::vector<cc::ForceArgs> fa = g.force;
-		for (size_t k = 0; k < g.members.size(); k++) {
-			const int i = g.members[k];
-			const int *status = &lbi[i].st->status, *stage = &lbi[i].st->stage;
-			ra[k].frac = lbi[i].xt;
-			ra[k].skip = status;
-			ra[k].stage = stage;
-			rr[k].E_out = &lbi[i].st->Et;
-			rr[k].skip = status;
-			rr[k].stage = stage;
-			fa[k].frac = lbi[i].xt;
-			fa[k].E_out = &lbi[i].st->Et;
-			fa[k].gfrac_out = lbi[i].gt;
-			fa[k].F_out = nullptr;
-			fa[k].skip = status;
-			fa[k].stage = stage;
-		}
-		if ((rc = upload_into(g.d_rho[1], ra)) || (rc = upload_into(g.d_red[1], rr)) ||
-		    (rc = upload_into(g.d_force[1], fa)))
-			return cleanup(rc);
-	}
-	cudaStream_t st = b->stream;
-	const bool sched = o.precision == CC_PREC_SCHEDULE;
-	// schedule: one launch per kernel, each instance at its stage's precision, while some instance is in the mixed
-	// stage; then the FP64 kernels only
-	const int prec0 = o.precision;
-	// Each dimension group runs its iterations (evaluation, then its instances' L-BFGS step) on its own stream,
-	// forked from st at the start of the graph and joined back at its end; launches interleaved by iteration.
-	const int ngr = (int)b->groups.size();
-	auto iterations = [&](int prec) -> int {
-		if (ngr > 1) {
-			CC_CUDA(cudaEventRecord(b->ev_fork, st));
-			for (int k = 1; k < ngr; k++)
-				CC_CUDA(cudaStreamWaitEvent(b->side[k - 1], b->ev_fork, 0));
-		}
-		for (int it = 0; it < o.iters_per_check; it++)
-			for (int k = 0; k < ngr; k++) {
-				BatchGroup &g = b->groups[k];
-				cudaStream_t gs = k == 0 ? st : b->side[k - 1];
-				if (int r2 = group_eval(g, true, prec, gs))
-					return r2;
-				const cc::LbInst *gl = d_lb + count + g_off[k];
-				const int gb = (int)g.members.size(), gn = cc::lb_blocks(g_maxn[k], cc::kLbMaxBlocks);
-				CC_CUDA(cc::lb_step(gl, gb, gn, g_maxn[k], gs));
-				CC_CUDA(cudaGetLastError());
-			}
-		for (int k = 1; k < ngr; k++) {
-			CC_CUDA(cudaEventRecord(b->ev_join[k - 1], b->side[k - 1]));
-			CC_CUDA(cudaStreamWaitEvent(st, b->ev_join[k - 1], 0));
-		}
-		return CC_OK;
-	};
-	auto make_graph = [&](int prec, cudaGraphExec_t *out) -> int {
-		cudaGraph_t g = nullptr;
-		CC_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-		const int r2 = iterations(prec);
-		cudaError_t e = cudaStreamEndCapture(st, &g);
-		if (r2)
-			return r2;
-		if (e != cudaSuccess)
-			return fail(CC_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
-		e = cudaGraphInstantiate(out, g, 0);
-		cudaGraphDestroy(g);
-		if (e != cudaSuccess)
-			return fail(CC_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
-		return CC_OK;
-	};
-	cudaGraphExec_t gexec[2] = {nullptr, nullptr};
-	auto destroy_graphs = [&]() {
-		for (auto &ge : gexec)
-			if (ge)
-				cudaGraphExecDestroy(ge);
-	};
-	// kernel attributes are set before the capture
-	for (BatchGroup &g : b->groups)
-		for (int mx = 0; mx < 3; mx++) {
-			cudaError_t e = mx == 2 ? (g.D == 1 ? multi_sched_attrs<1>() : g.D == 2 ? multi_sched_attrs<2>()
-			                                                                         : multi_sched_attrs<3>())
-			              : g.D == 1 ? (mx ? multi_attrs<1, true>() : multi_attrs<1, false>())
-			              : g.D == 2 ? (mx ? multi_attrs<2, true>() : multi_attrs<2, false>())
-			                         : (mx ? multi_attrs<3, true>() : multi_attrs<3, false>());
-			if (e != cudaSuccess)
-				return cleanup(fail(CC_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e)));
-		}
-	if ((rc = make_graph(prec0, &gexec[0])) || (sched && (rc = make_graph(CC_PREC_FP64, &gexec[1])))) {
-		destroy_graphs();
-		return cleanup(rc);
-	}
-	std::vector<cc::LbBrief> hs(count);
-	int stage = 0;
-	const int64_t max_rounds = o.max_evals / o.iters_per_check + 2;
-	for (int64_t round = 0; round < max_rounds; round++) {
-		cudaError_t e = cudaGraphLaunch(gexec[stage], st);
-		if (e == cudaSuccess)
-			e = cudaStreamSynchronize(st);
-		if (e != cudaSuccess) {
-			destroy_graphs();
-			return cleanup(fail(CC_ERR_CUDA, std::string("batch minimisation: ") + cudaGetErrorString(e)));
-		}
-		if ((rc = batch_check_barrier(b))) {
-			destroy_graphs();
-			return cleanup(rc);
-		}
-		bool running = false, any_mixed = false;
-		cc::lb_brief_kernel<<<(count + 127) / 128, 128, 0, st>>>(d_lb, count, b->d_brief);
-		e = cudaGetLastError();
-		if (e == cudaSuccess)
-			e = cudaMemcpyAsync(hs.data(), b->d_brief, sizeof(cc::LbBrief) * count, cudaMemcpyDeviceToHost, st);
-		if (e == cudaSuccess)
-			e = cudaStreamSynchronize(st);
-		if (e != cudaSuccess) {
-			destroy_graphs();
-			return cleanup(fail(CC_ERR_CUDA, std::string("batch minimisation status: ") + cudaGetErrorString(e)));
-		}
-		for (int i = 0; i < count; i++) {
-			running |= hs[i].status == cc::kLbRunning;
-			any_mixed |= hs[i].status == cc::kLbRunning && hs[i].stage == 0;
-		}
-		if (!running)
-			break;
-		if (sched && stage == 0 && !any_mixed)
-			stage = 1;
-	}
-	destroy_graphs();
-	// results: positions wrapped into [0,1), FP64 energies of the results (one batched evaluation)
-	std::vector<const double *> fr(count);
-	for (int i = 0; i < count; i++) {
-		const size_t n = (size_t)b->N[i] * b->h[i]->d;
-		CC_CUDA(cudaMemcpy(frac[i], lbi[i].x, 8 * n, cudaMemcpyDeviceToHost));
-		for (size_t k = 0; k < n; k++) {
-			double v = frac[i][k] - std::floor(frac[i][k]);
-			frac[i][k] = v - std::floor(v);
-		}
-		fr[i] = frac[i];
-	}
-	cleanup(CC_OK);
-	if ((rc = cc_batch_set_positions(b, fr.data())))
-		return rc;
-	std::vector<double> E(count);
-	if ((rc = cc_batch_energy_grad(b, E.data(), nullptr, CC_PREC_FP64)))
-		return rc;
-	if (results)
-		for (int i = 0; i < count; i++) {
-			results[i].E = E[i];
-			results[i].evals = hs[i].evals;
-			results[i].iters = hs[i].iters;
-			results[i].status = hs[i].status == cc::kLbRunning ? cc::kLbMaxEval : hs[i].status;
-		}
-	return CC_OK;
-}
 
 int cc_kset_stealthy(int d, const double *basis, int64_t N, double chi, int type, int64_t cap, int32_t *modes,
                      double *V, int64_t *M)

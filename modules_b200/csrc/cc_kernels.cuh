@@ -31,13 +31,13 @@
 //                    each particle group. Cartesian F = (2/V) sum_e g_e b_e; dPhi/ds_e = -(2/V) 2 pi g_e.
 //   The kernels are chained by programmatic dependent launch: each is scheduled while its predecessor drains and
 //   waits for it (cudaGridDependencySynchronize) before reading its results.
-//   cc_mrho / cc_mreduce / cc_mforce: the same block bodies for many instances in one persistent launch each, items
-//   (instance, block) taken from a work queue.
+//   cc_mbatch_kernel: the same block bodies for many instances (any dimensions) in ONE persistent launch, items
+//   (instance, phase, block) taken from one work queue, the phases of an instance ordered by completion counts.
 // Every sum has a fixed order, so results repeat bitwise.
 //
-// Mixed precision: tables are built in FP64 and rounded to FP32; seeds and the rotations along a segment (complex
-// products) run in FP32; per-thread rho sums are flushed to FP64 every 16 particles, per-segment force sums are added
-// to FP64; all cross-thread sums are FP64.
+// Mixed precision: table entries are FP32 sincospi of the exactly reduced FP64 arguments, continued by FP32 products
+// within each 8-entry block; seeds and the three-term recurrence along a segment run in FP32; per-thread rho sums are
+// flushed to FP64 every 16 particles, per-segment force sums are added to FP64; all cross-thread sums are FP64.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -102,6 +102,11 @@ __device__ __forceinline__ double2 cheb_next(double c, double2 q, double2 p)
 {
 	return make_double2(fma(c, q.x, -p.x), fma(c, q.y, -p.y));
 }
+// The same in FP32 (the mixed path): a segment of L = 8 slots stays within ~L^2/2 = 32 FP32 ulps of its seed's phase.
+__device__ __forceinline__ float2 cheb_next(float c, float2 q, float2 p)
+{
+	return make_float2(fmaf(c, q.x, -p.x), fmaf(c, q.y, -p.y));
+}
 
 // exp(2 pi i t): (cos, sin)
 __device__ __forceinline__ double2 expi2pi(double t)
@@ -109,6 +114,13 @@ __device__ __forceinline__ double2 expi2pi(double t)
 	double s, c;
 	sincospi(2.0 * t, &s, &c);
 	return make_double2(c, s);
+}
+// exp(2 pi i t) in FP32 for an exactly reduced argument t in [-1/2, 1/2] (rounded once to FP32, ~3e-8 of a turn)
+__device__ __forceinline__ float2 expi2pi_f(double t)
+{
+	float s, c;
+	sincospif(2.0f * (float)t, &s, &c);
+	return make_float2(c, s);
 }
 
 template <typename C> __device__ __forceinline__ C to_c(double2 z);
@@ -140,13 +152,23 @@ __device__ __forceinline__ void build_tables(const TabSpec &sp, const double *__
 		const TabRun &run = sp.run[r];
 		const double s = (i < nvalid) ? frac[(first + i) * D + run.axis] : 0.0;
 		const int k0 = k * 8;
-		double2 z = expi2pi(phase1(run.m0 + run.stride * k0, s));
-		const double2 step = expi2pi(phase1(run.stride, s));
 		const int k1 = min(run.count, k0 + 8);
 		C *dst = tab + (size_t)i * pstride;
-		for (int kk = k0; kk < k1; kk++) {
-			dst[(run.off + kk) * estride] = to_c<C>(z);
-			z = cmul(z, step);
+		if constexpr (std::is_same<C, float2>::value) {
+			// mixed precision: FP32 sincospi of the exactly reduced FP64 argument, FP32 products along the block
+			float2 z = expi2pi_f(phase1(run.m0 + run.stride * k0, s));
+			const float2 step = expi2pi_f(phase1(run.stride, s));
+			for (int kk = k0; kk < k1; kk++) {
+				dst[(run.off + kk) * estride] = z;
+				z = cmul(z, step);
+			}
+		} else {
+			double2 z = expi2pi(phase1(run.m0 + run.stride * k0, s));
+			const double2 step = expi2pi(phase1(run.stride, s));
+			for (int kk = k0; kk < k1; kk++) {
+				dst[(run.off + kk) * estride] = to_c<C>(z);
+				z = cmul(z, step);
+			}
 		}
 	}
 }
@@ -279,6 +301,43 @@ __device__ __forceinline__ int find_instance(const int *pre, int B, int item)
 	return lo;
 }
 
+constexpr int kForceUChunk = 128;   // segments whose slot weights are staged in shared memory at once
+
+// Block-shared scalars and small arrays of the rho / reduce / force bodies. They live in ONE shared variable of a
+// non-template function, so a kernel that inlines several bodies (every dimension and precision of the fused batch
+// kernel) holds one set per block instead of one per body instantiation.
+struct BodyShared {
+	TabSpec sp;
+	Seg seg[kForceUChunk];
+	double2 red[8][32];
+	int last;
+};
+__device__ __forceinline__ BodyShared &body_shared()
+{
+	__shared__ BodyShared s;
+	return s;
+}
+
+// Bounded wait of a whole block until *ready >= need (a count other blocks of the same launch raise after their
+// items' results are visible). Thread 0 polls; after kReadySpins polls it sets *err and gives up, so a fault ends the
+// launch with an error status instead of a hang.
+constexpr unsigned kReadySpins = 1u << 22;
+__device__ __forceinline__ void wait_ready(const unsigned *ready, unsigned need, unsigned *err)
+{
+	if (threadIdx.x == 0) {
+		unsigned it = 0;
+		while (*(volatile const unsigned *)ready < need) {
+			if (++it > kReadySpins) {
+				atomicExch(err, 1u);
+				break;
+			}
+			__nanosleep(32);
+		}
+		__threadfence();
+	}
+	__syncthreads();
+}
+
 // ---------------------------------------------------------------------------------------------------------------
 // rho pass
 // ---------------------------------------------------------------------------------------------------------------
@@ -316,7 +375,7 @@ __device__ __forceinline__ void rho_body(const RhoArgs &a, const int bg, const i
 	extern __shared__ __align__(16) unsigned char smem[];
 	C *tab = reinterpret_cast<C *>(smem);             // chunk x row (particle-major)
 	double2 *red = reinterpret_cast<double2 *>(smem); // after the loop: kRhoWarps x L x 32
-	__shared__ TabSpec sp;
+	TabSpec &sp = body_shared().sp;
 
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	if (threadIdx.x == 0)
@@ -345,13 +404,15 @@ __device__ __forceinline__ void rho_body(const RhoArgs &a, const int bg, const i
 		}
 	}
 
+	// per-slot sums in the compute type (FP32 in the mixed path, flushed into the FP64 acc every SUB particles)
+	typedef typename std::conditional<MIXED, float, double>::type R;
 	double2 acc[L];
-	C accf[L];
+	C accC[L];
 #pragma unroll
 	for (int r = 0; r < L; r++) {
 		acc[r] = make_double2(0.0, 0.0);
-		accf[r].x = 0;
-		accf[r].y = 0;
+		accC[r].x = 0;
+		accC[r].y = 0;
 	}
 	int since_flush = 0;
 
@@ -368,26 +429,19 @@ __device__ __forceinline__ void rho_body(const RhoArgs &a, const int bg, const i
 			const C *r0 = tab + i * row, *r1 = r0 + row;
 			C z0 = seed_from<D, C>(r0, 1, ix), z1 = seed_from<D, C>(r1, 1, ix);
 			const C w0 = r0[ix.w], w1 = r1[ix.w];
-			if constexpr (MIXED) {
-#pragma unroll
-				for (int r = 0; r < L; r++) {
-					accf[r].x += z0.x + z1.x;
-					accf[r].y += z0.y + z1.y;
-					z0 = cmul(z0, w0);
-					z1 = cmul(z1, w1);
-				}
-			} else {
-				const double c0 = 2.0 * w0.x, c1 = 2.0 * w1.x;
-				double2 p0 = z0, p1 = z1, q0 = cmul(z0, w0), q1 = cmul(z1, w1);
-				acc[0].x += p0.x + p1.x;
-				acc[0].y += p0.y + p1.y;
-				acc[1].x += q0.x + q1.x;
-				acc[1].y += q0.y + q1.y;
+			{
+				// three-term recurrence along the segment
+				const R c0 = (R)2 * w0.x, c1 = (R)2 * w1.x;
+				C p0 = z0, p1 = z1, q0 = cmul(z0, w0), q1 = cmul(z1, w1);
+				accC[0].x += p0.x + p1.x;
+				accC[0].y += p0.y + p1.y;
+				accC[1].x += q0.x + q1.x;
+				accC[1].y += q0.y + q1.y;
 #pragma unroll
 				for (int r = 2; r < L; r++) {
-					const double2 n0 = cheb_next(c0, q0, p0), n1 = cheb_next(c1, q1, p1);
-					acc[r].x += n0.x + n1.x;
-					acc[r].y += n0.y + n1.y;
+					const C n0 = cheb_next(c0, q0, p0), n1 = cheb_next(c1, q1, p1);
+					accC[r].x += n0.x + n1.x;
+					accC[r].y += n0.y + n1.y;
 					p0 = q0;
 					q0 = n0;
 					p1 = q1;
@@ -398,10 +452,10 @@ __device__ __forceinline__ void rho_body(const RhoArgs &a, const int bg, const i
 				since_flush = 0;
 #pragma unroll
 				for (int r = 0; r < L; r++) {
-					acc[r].x += (double)accf[r].x;
-					acc[r].y += (double)accf[r].y;
-					accf[r].x = 0;
-					accf[r].y = 0;
+					acc[r].x += (double)accC[r].x;
+					acc[r].y += (double)accC[r].y;
+					accC[r].x = 0;
+					accC[r].y = 0;
 				}
 			}
 		}
@@ -409,36 +463,32 @@ __device__ __forceinline__ void rho_body(const RhoArgs &a, const int bg, const i
 			const C *r0 = tab + i * row;
 			C z0 = seed_from<D, C>(r0, 1, ix);
 			const C w0 = r0[ix.w];
-			if constexpr (MIXED) {
-#pragma unroll
-				for (int r = 0; r < L; r++) {
-					accf[r].x += z0.x;
-					accf[r].y += z0.y;
-					z0 = cmul(z0, w0);
-				}
-			} else {
-				const double c0 = 2.0 * w0.x;
-				double2 p0 = z0, q0 = cmul(z0, w0);
-				acc[0].x += p0.x;
-				acc[0].y += p0.y;
-				acc[1].x += q0.x;
-				acc[1].y += q0.y;
+			{
+				const R c0 = (R)2 * w0.x;
+				C p0 = z0, q0 = cmul(z0, w0);
+				accC[0].x += p0.x;
+				accC[0].y += p0.y;
+				accC[1].x += q0.x;
+				accC[1].y += q0.y;
 #pragma unroll
 				for (int r = 2; r < L; r++) {
-					const double2 n0 = cheb_next(c0, q0, p0);
-					acc[r].x += n0.x;
-					acc[r].y += n0.y;
+					const C n0 = cheb_next(c0, q0, p0);
+					accC[r].x += n0.x;
+					accC[r].y += n0.y;
 					p0 = q0;
 					q0 = n0;
 				}
 			}
 		}
 	}
-	if (MIXED) {
 #pragma unroll
-		for (int r = 0; r < L; r++) {
-			acc[r].x += (double)accf[r].x;
-			acc[r].y += (double)accf[r].y;
+	for (int r = 0; r < L; r++) {
+		if (MIXED) {
+			acc[r].x += (double)accC[r].x;
+			acc[r].y += (double)accC[r].y;
+		} else {
+			acc[r].x = (double)accC[r].x;
+			acc[r].y = (double)accC[r].y;
 		}
 	}
 	cudaTriggerProgrammaticLaunchCompletion();   // the next kernel may be scheduled; it waits for this grid
@@ -490,51 +540,6 @@ __global__ void __launch_bounds__(kRhoThreads, 3) cc_rho_kernel(RhoArgs a)
 	rho_body<D, L, MIXED, true>(a, blockIdx.x, blockIdx.y);
 }
 
-// The rho pass of many instances in one persistent launch: blocks take items from a work queue; item i belongs to
-// instance b with pre[b] <= i < pre[b+1] and is block (local % nbgroups[b], local / nbgroups[b]) of that instance's
-// grid; no clusters (one row per block). Items of skipped instances cost a lookup and a flag read.
-template <int D, int L, bool MIXED>
-__global__ void __launch_bounds__(kRhoThreads, 3) cc_mrho_kernel(const RhoArgs *__restrict__ args,
-                                                                const int *__restrict__ pre,
-                                                                const int *__restrict__ nbgroups, int B,
-                                                                int want_stage, unsigned *queue)
-{
-	__shared__ int sh_item;
-	const int total = __ldg(pre + B);
-	for (int item; (item = queue_next(queue, &sh_item)) < total;) {
-		const int b = find_instance(pre, B, item);
-		RhoArgs a = args[b];
-		a.want_stage = want_stage;
-		const int local = item - __ldg(pre + b), ng = __ldg(nbgroups + b);
-		rho_body<D, L, MIXED, false>(a, local % ng, local / ng);
-	}
-	queue_leave(queue);
-}
-
-// The same with each instance's precision taken from its stage word (0: mixed, else FP64): one launch serves a
-// batched minimisation whose instances are in different stages of the precision schedule.
-template <int D, int L>
-__global__ void __launch_bounds__(kRhoThreads, 3) cc_mrho_sched_kernel(const RhoArgs *__restrict__ args,
-                                                                      const int *__restrict__ pre,
-                                                                      const int *__restrict__ nbgroups, int B,
-                                                                      unsigned *queue)
-{
-	__shared__ int sh_item;
-	const int total = __ldg(pre + B);
-	for (int item; (item = queue_next(queue, &sh_item)) < total;) {
-		const int b = find_instance(pre, B, item);
-		RhoArgs a = args[b];
-		const bool mixed = a.stage && *(volatile const int *)a.stage == 0;
-		a.stage = nullptr;   // the stage picks the precision; only the skip word can skip
-		const int local = item - __ldg(pre + b), ng = __ldg(nbgroups + b);
-		if (mixed)
-			rho_body<D, L, true, false>(a, local % ng, local / ng);
-		else
-			rho_body<D, L, false, false>(a, local % ng, local / ng);
-	}
-	queue_leave(queue);
-}
-
 // ---------------------------------------------------------------------------------------------------------------
 // split reduction, u = V conj(rho), energy
 // ---------------------------------------------------------------------------------------------------------------
@@ -556,6 +561,11 @@ struct ReduceArgs {
 	// u = V (|rho|^2 / N - S0) conj(rho); npart = N
 	const double *slotS0;
 	double npart;
+	// fused batch launch: wait until *ready >= ready_need (the instance's rho items done) before reading partials;
+	// err is raised when that bounded wait runs out. Null outside that launch.
+	const unsigned *ready;
+	unsigned ready_need;
+	unsigned *err;
 };
 
 constexpr int kRedThreads = 256;   // 32 slots x 8 split chunks
@@ -563,8 +573,8 @@ constexpr int kRedThreads = 256;   // 32 slots x 8 split chunks
 // Block `chunk` (32 slots) of the split reduction of an instance with `nchunks` such blocks.
 __device__ __forceinline__ void reduce_body(const ReduceArgs &a, const int chunk, const int nchunks)
 {
-	__shared__ double2 sh[8][32];
-	__shared__ int sh_last;
+	double2 (&sh)[8][32] = body_shared().red;
+	int &sh_last = body_shared().last;
 	const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
 	const int slot = chunk * 32 + lane;
 	const int per = (a.nsplit + 7) >> 3;
@@ -572,6 +582,8 @@ __device__ __forceinline__ void reduce_body(const ReduceArgs &a, const int chunk
 	cudaTriggerProgrammaticLaunchCompletion();
 	if (eval_skipped(a.skip, a.stage, a.want_stage))
 		return;
+	if (a.ready)
+		wait_ready(a.ready, a.ready_need, a.err);
 	const int s0 = min(a.nsplit, c * per), s1 = min(a.nsplit, s0 + per);
 	double2 t = make_double2(0.0, 0.0);
 	if (slot < a.nslot) {
@@ -653,25 +665,6 @@ static __global__ void __launch_bounds__(kRedThreads) cc_reduce_kernel(ReduceArg
 	reduce_body(a, blockIdx.x, gridDim.x);
 }
 
-// The split reduction of many instances in one persistent launch (item -> instance b, chunk item - pre[b]).
-static __global__ void __launch_bounds__(kRedThreads) cc_mreduce_kernel(const ReduceArgs *__restrict__ args,
-                                                                     const int *__restrict__ pre,
-                                                                     const int *__restrict__ nchunks, int B,
-                                                                     int want_stage, unsigned *queue)
-{
-	__shared__ int sh_item;
-	const int total = __ldg(pre + B);
-	for (int item; (item = queue_next(queue, &sh_item)) < total;) {
-		const int b = find_instance(pre, B, item);
-		ReduceArgs a = args[b];
-		a.want_stage = want_stage;
-		if (want_stage < 0)   // a launch for every stage (the sched kernels)
-			a.stage = nullptr;
-		reduce_body(a, item - __ldg(pre + b), __ldg(nchunks + b));
-	}
-	queue_leave(queue);
-}
-
 // rho in input-mode order (repeated modes read their shared slot)
 static __global__ void cc_gather_rho_kernel(const double2 *__restrict__ rho_slot, const int *__restrict__ mode_slot, int M,
                                      double2 *__restrict__ rho_mode)
@@ -717,6 +710,11 @@ struct ForceArgs {
 	const int *skip;
 	const int *stage;
 	int want_stage;
+	// fused batch launch: wait until *ready >= ready_need (the instance's reduce items done) before reading u; err is
+	// raised when that bounded wait runs out. Null outside that launch.
+	const unsigned *ready;
+	unsigned ready_need;
+	unsigned *err;
 };
 
 constexpr int kForceWarps = 8;
@@ -728,7 +726,6 @@ __device__ __forceinline__ void write_force(const ForceArgs &a, int j, const dou
 	write_force_out<D>(a.F_out, a.gfrac_out, a.recip, a.fscale, j, g);
 }
 
-constexpr int kForceUChunk = 128;   // segments whose slot weights are staged in shared memory at once
 constexpr int kForceRun = 4;        // FP64 force pass: segments of a lattice line on one recurrence before a new seed
 
 // Dynamic shared memory of the force kernel for tables of `row` entries: the staged weights, then the tables; the
@@ -753,9 +750,9 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 	C *sh_u = reinterpret_cast<C *>(smem);           // L x kForceUChunk, slot-major
 	C *tab = sh_u + L * kForceUChunk;                // row x 32, entry-major
 	double *sh_g = reinterpret_cast<double *>(smem); // reused after the loop: kForceWarps x 32 x D
-	__shared__ TabSpec sp;
-	__shared__ Seg sh_seg[kForceUChunk];
-	__shared__ int sh_last;
+	TabSpec &sp = body_shared().sp;
+	Seg *sh_seg = body_shared().seg;
+	int &sh_last = body_shared().last;
 
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	const int pbase = pgroup * 32;
@@ -775,11 +772,13 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 	cudaGridDependencySynchronize();   // u of this step is complete
 	if (eval_skipped(a.skip, a.stage, a.want_stage))   // uniform over the instance
 		return;
+	if (a.ready)
+		wait_ready(a.ready, a.ready_need, a.err);
 	if (a.E_out && pgroup == 0 && ks == 0 && warp == 0) {
 		// the energy, summed in the order of the reduce kernel's last block
 		double e = 0.0;
 		for (int b = lane; b < a.neblock; b += 32)
-			e += a.eblock[b];
+			e += __ldcg(a.eblock + b);
 #pragma unroll
 		for (int o = 16; o > 0; o >>= 1)
 			e += __shfl_down_sync(0xffffffffu, e, o);
@@ -796,7 +795,7 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 		__syncthreads();   // tables complete (first chunk); the previous chunk's weights are no longer read
 		for (int e = threadIdx.x; e < nq * L; e += kForceThreads) {
 			const int r = e / nq, qq = e - r * nq;
-			sh_u[r * kForceUChunk + qq] = to_c<C>(a.u_slot[(size_t)r * a.nseg + c0 + qq]);
+			sh_u[r * kForceUChunk + qq] = to_c<C>(__ldcg(a.u_slot + (size_t)r * a.nseg + c0 + qq));
 		}
 		for (int e = threadIdx.x; e < nq; e += kForceThreads)
 			sh_seg[e] = a.segs[c0 + e];
@@ -865,38 +864,28 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 					continue;
 				const C *uu = sh_u + qq;
 				const SeedIdx ix = seed_index<D>(sp, sgm);
-				C z = seed_from<D, C>(tab + lane, 32, ix);
+				const C z = seed_from<D, C>(tab + lane, 32, ix);
 				const C w = tab[ix.w * 32 + lane];
-				R S0 = 0, S1 = 0;
-				if constexpr (MIXED) {
-	#pragma unroll
-					for (int r = 0; r < L; r++) {
-						const C u = uu[r * kForceUChunk];
-						const R t = u.x * z.y + u.y * z.x;
-						S0 += t;
-						S1 = fma((R)r, t, S1);
-						z = cmul(z, w);
-					}
-				} else {
-					const double c = 2.0 * w.x;
-					double2 p = z, q = cmul(z, w);
-					const double2 u0 = uu[0], u1 = uu[kForceUChunk];
-					S0 = u0.x * p.y + u0.y * p.x;
-					{
-						const double t = u1.x * q.y + u1.y * q.x;
-						S0 += t;
-						S1 = t;
-					}
-	#pragma unroll
-					for (int r = 2; r < L; r++) {
-						const double2 n = cheb_next(c, q, p);
-						const double2 u = uu[r * kForceUChunk];
-						const double t = u.x * n.y + u.y * n.x;
-						S0 += t;
-						S1 = fma((double)r, t, S1);
-						p = q;
-						q = n;
-					}
+				// three-term recurrence along the segment (re-seeded per segment: in FP32 a longer run would carry its
+				// error along)
+				const R c = (R)2 * w.x;
+				C p = z, q = cmul(z, w);
+				const C u0 = uu[0], u1 = uu[kForceUChunk];
+				R S0 = u0.x * p.y + u0.y * p.x, S1;
+				{
+					const R t = u1.x * q.y + u1.y * q.x;
+					S0 += t;
+					S1 = t;
+				}
+#pragma unroll
+				for (int r = 2; r < L; r++) {
+					const C n = cheb_next(c, q, p);
+					const C u = uu[r * kForceUChunk];
+					const R t = u.x * n.y + u.y * n.x;
+					S0 += t;
+					S1 = fma((R)r, t, S1);
+					p = q;
+					q = n;
 				}
 				const double S0d = (double)S0;
 				if (D >= 2)
@@ -963,47 +952,126 @@ __global__ void __launch_bounds__(kForceThreads, 3) cc_force_kernel(ForceArgs a)
 	force_body<D, L, MIXED>(a, blockIdx.x, blockIdx.y);
 }
 
-// The force pass of many instances in one persistent launch: item -> instance b, block (local % pgroups[b],
-// local / pgroups[b]) of its grid.
-template <int D, int L, bool MIXED>
-__global__ void __launch_bounds__(kForceThreads, 3) cc_mforce_kernel(const ForceArgs *__restrict__ args,
-                                                                    const int *__restrict__ pre,
-                                                                    const int *__restrict__ pgroups, int B,
-                                                                    int want_stage, unsigned *queue)
+// ---------------------------------------------------------------------------------------------------------------
+// fused batch evaluation: ONE persistent launch per batched energy + gradient step
+// ---------------------------------------------------------------------------------------------------------------
+// The rho, split-reduction and force items of every instance of a batch (every dimension) come from one work queue,
+// in that order: items [0, total[0]) are rho blocks, the next total[1] reduce chunks, the last total[2] force blocks,
+// each phase ordered by instance (instances by decreasing work). An item raises its instance's count of that phase
+// when its results are visible; a reduce item waits (bounded) for its instance's rho count, a force item for its
+// reduce count, after building its tables. An item only waits for items taken from the queue before it, by blocks that
+// are running and never wait for later items, so the launch cannot deadlock whatever number of blocks is resident. The
+// last force item of an instance resets its counts for the next launch. Each instance keeps its own plan, tiles and
+// fixed-order sums, so its results are those of the three-kernel batch evaluation, bitwise.
+struct MBatchArgs {
+	const RhoArgs *rho;
+	const ReduceArgs *red;
+	const ForceArgs *force;
+	const int *dim;       // B: dimension of each instance (1..3)
+	const int *pre;       // 3 x (B + 1): prefix sums of each instance's rho, reduce and force items
+	const int *shape;     // 3 x B: rho block groups, reduce chunks, force particle groups
+	int B;
+	int total[3];
+	int want_stage;       // MODE 0 / 1: instances whose stage word differs are skipped (as the three-kernel launches)
+	unsigned *queue;      // 2 words, zero between launches
+	unsigned *count;      // 3 x B completed items per instance and phase (zero between launches), then 1 error word
+};
+
+constexpr int kMBatchThreads = 256;
+
+template <int D, int MODE>
+__device__ __forceinline__ void mbatch_item(const MBatchArgs &A, int phase, int b, int local)
 {
-	__shared__ int sh_item;
-	const int total = __ldg(pre + B);
-	for (int item; (item = queue_next(queue, &sh_item)) < total;) {
-		const int b = find_instance(pre, B, item);
-		ForceArgs a = args[b];
-		a.want_stage = want_stage;
-		const int local = item - __ldg(pre + b), pg = __ldg(pgroups + b);
-		force_body<D, L, MIXED>(a, local % pg, local / pg);
+	// MODE 0: FP64, 1: mixed, 2: each instance at the precision of its stage word (mixed while it is 0)
+	unsigned *err = A.count + 3 * A.B;
+	if (phase == 0) {
+		RhoArgs r = A.rho[b];
+		bool mixed = MODE == 1;
+		if (MODE == 2) {
+			mixed = r.stage && *(volatile const int *)r.stage == 0;
+			r.stage = nullptr;
+		} else {
+			r.want_stage = A.want_stage;
+		}
+		const int ng = __ldg(A.shape + b);
+		if constexpr (MODE != 0) {
+			if (mixed) {
+				rho_body<D, 8, true, false>(r, local % ng, local / ng);
+				return;
+			}
+		}
+		if constexpr (MODE != 1)
+			rho_body<D, 8, false, false>(r, local % ng, local / ng);
+	} else if (phase == 1) {
+		ReduceArgs r = A.red[b];
+		if (MODE == 2)
+			r.stage = nullptr;
+		else
+			r.want_stage = A.want_stage;
+		r.ready = A.count + b;
+		r.ready_need = (unsigned)(__ldg(A.pre + b + 1) - __ldg(A.pre + b));
+		r.err = err;
+		reduce_body(r, local, __ldg(A.shape + A.B + b));
+	} else {
+		ForceArgs f = A.force[b];
+		bool mixed = MODE == 1;
+		if (MODE == 2) {
+			mixed = f.stage && *(volatile const int *)f.stage == 0;
+			f.stage = nullptr;
+		} else {
+			f.want_stage = A.want_stage;
+		}
+		f.ready = A.count + A.B + b;
+		f.ready_need = (unsigned)(__ldg(A.pre + (A.B + 1) + b + 1) - __ldg(A.pre + (A.B + 1) + b));
+		f.err = err;
+		const int pg = __ldg(A.shape + 2 * A.B + b);
+		if constexpr (MODE != 0) {
+			if (mixed) {
+				force_body<D, 8, true>(f, local % pg, local / pg);
+				return;
+			}
+		}
+		if constexpr (MODE != 1)
+			force_body<D, 8, false>(f, local % pg, local / pg);
 	}
-	queue_leave(queue);
 }
 
-// The force pass with each instance's precision taken from its stage word (see cc_mrho_sched_kernel).
-template <int D, int L>
-__global__ void __launch_bounds__(kForceThreads, 3) cc_mforce_sched_kernel(const ForceArgs *__restrict__ args,
-                                                                          const int *__restrict__ pre,
-                                                                          const int *__restrict__ pgroups, int B,
-                                                                          unsigned *queue)
+template <int MODE>
+__global__ void __launch_bounds__(kMBatchThreads, 3) cc_mbatch_kernel(MBatchArgs A)
 {
 	__shared__ int sh_item;
-	const int total = __ldg(pre + B);
-	for (int item; (item = queue_next(queue, &sh_item)) < total;) {
-		const int b = find_instance(pre, B, item);
-		ForceArgs a = args[b];
-		const bool mixed = a.stage && *(volatile const int *)a.stage == 0;
-		a.stage = nullptr;
-		const int local = item - __ldg(pre + b), pg = __ldg(pgroups + b);
-		if (mixed)
-			force_body<D, L, true>(a, local % pg, local / pg);
+	const int T0 = A.total[0], T1 = T0 + A.total[1], T = T1 + A.total[2];
+	// Under programmatic dependent launch this grid may be scheduled while the previous one still takes items from
+	// the same queue (its blocks trigger after their first item): wait for it to complete before taking any.
+	cudaGridDependencySynchronize();
+	for (int item; (item = queue_next(A.queue, &sh_item)) < T;) {
+		const int phase = item < T0 ? 0 : item < T1 ? 1 : 2;
+		const int *pre = A.pre + phase * (A.B + 1);
+		const int li = item - (phase == 0 ? 0 : phase == 1 ? T0 : T1);
+		const int b = find_instance(pre, A.B, li);
+		const int local = li - __ldg(pre + b);
+		const int d = __ldg(A.dim + b);
+		if (d == 3)
+			mbatch_item<3, MODE>(A, phase, b, local);
+		else if (d == 2)
+			mbatch_item<2, MODE>(A, phase, b, local);
 		else
-			force_body<D, L, false>(a, local % pg, local / pg);
+			mbatch_item<1, MODE>(A, phase, b, local);
+		// the item's results are visible before its count rises
+		__threadfence();
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			unsigned *cnt = A.count + phase * A.B + b;
+			const unsigned done = atomicAdd(cnt, 1u) + 1u;
+			if (phase == 2 && done == (unsigned)(__ldg(pre + b + 1) - __ldg(pre + b))) {
+				// the instance's last item: its counts start from zero in the next launch
+				A.count[b] = 0u;
+				A.count[A.B + b] = 0u;
+				*cnt = 0u;
+			}
+		}
 	}
-	queue_leave(queue);
+	queue_leave(A.queue);
 }
 
 // ---------------------------------------------------------------------------------------------------------------

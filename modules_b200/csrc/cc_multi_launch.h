@@ -1,4 +1,4 @@
-// cc_multi_launch.h — the multi-instance evaluation launch shared by the batch API and the server.
+// cc_multi_launch.h — the fused multi-instance evaluation launch shared by the batch API and the server.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -10,13 +10,10 @@ constexpr int kBatchChunk = 16;          // particles whose rho tables are built
 constexpr int kBatchPerSplit = 64;       // particles per rho block of an instance
 constexpr int kBatchSegsPerSplit = 64;   // segments per force block of an instance
 
-// One evaluation of B instances of dimension D: the persistent rho, reduce and force kernels (programmatic
-// dependent launch) over per-instance arguments on the device. pre: 3 x (B + 1) prefix sums of the instances' blocks
-// (rho, reduce, force), shape: 3 x B (block groups, reduce chunks, particle groups), total: the three sums;
-// rho_row / force_row: the largest table rows; queue: 6 zeroed words (reset by the kernels). MIXED for the mixed
-// precision kernels; instances whose stage word differs from 0 (mixed) or 1 (FP64) are skipped.
-int launch_multi(int D, bool mixed, const RhoArgs *rho, const ReduceArgs *red, const ForceArgs *force, const int *pre,
-                 const int *shape, int B, const int total[3], int rho_row, int force_row, unsigned *queue,
-                 cudaStream_t st);
+// One evaluation of B instances (any dimensions) in ONE launch of the fused batch kernel (cc_mbatch_kernel):
+// mode 0 FP64, 1 mixed, 2 each instance at the precision of its stage word. rho_row / force_row: the largest table
+// rows of the instances, maxd their largest dimension (they size the shared memory); the grid is the kernel's resident
+// blocks (or fewer when there are fewer items).
+int launch_mbatch(int mode, const MBatchArgs &a, int rho_row, int force_row, int maxd, cudaStream_t st);
 
 }  // namespace cc

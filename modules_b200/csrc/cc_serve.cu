@@ -2,13 +2,14 @@
 //
 // Requests (a stealthy CC configuration each: d, N, chi, weight type, start positions, arrival time) are minimised
 // to their ground state on one GPU. The server works in rounds:
-//   1. admit every request that has arrived, in arrival order, while a slot is free and the request's device memory
-//      fits the HBM budget (its k-set is planned on the host, its k-set arrays, partial sums and L-BFGS state are
-//      allocated from the server's own stream-ordered pool, which holds the budget, and stay resident until it
-//      finishes);
-//   2. run `iters_per_round` L-BFGS iterations for every admitted request at once: each dimension group on its own
-//      stream, per iteration one multi-instance evaluation (the persistent rho / reduce / force kernels,
-//      cc_multi_launch.h) and one launch each of the batched L-BFGS kernels (cc_lbfgs.cuh) for its requests;
+//   1. admit arrived requests, in arrival order, while a slot is free and the request's device memory fits the HBM
+//      budget (a request waiting for memory may be passed by later ones until it has waited max_bypass_s; one that can
+//      never be served is rejected with a status of its own). Its k-set is planned on the host; its k-set arrays,
+//      partial sums and L-BFGS state are allocated from the server's own stream-ordered pool, which holds the
+//      budget, and stay resident until it finishes;
+//   2. run `iters_per_round` L-BFGS iterations for every admitted request at once: per iteration ONE launch of the
+//      fused batch kernel evaluating every request (cc_multi_launch.h; requests of any dimension in one work queue)
+//      and one launch each of the batched L-BFGS kernels (cc_lbfgs.cuh);
 //   3. read every request's status (one gather kernel, one copy), retire finished requests (time-to-ground-state =
 //      completion - arrival) and free their memory.
 // Requests that arrive while others are on the GPU join at the next round, so their work overlaps; an instance's
@@ -311,14 +312,6 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 	const int nblk_cap = cc::kLbMaxBlocks;
 	cudaStream_t st;
 	SV_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-	// the dimension groups after the first run on side streams forked from and joined back into st
-	cudaStream_t side[2];
-	cudaEvent_t ev_fork, ev_join[2];
-	SV_CUDA(cudaStreamCreateWithFlags(&side[0], cudaStreamNonBlocking));
-	SV_CUDA(cudaStreamCreateWithFlags(&side[1], cudaStreamNonBlocking));
-	SV_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
-	SV_CUDA(cudaEventCreateWithFlags(&ev_join[0], cudaEventDisableTiming));
-	SV_CUDA(cudaEventCreateWithFlags(&ev_join[1], cudaEventDisableTiming));
 	// The requests' memory comes from a pool of the server's own that keeps what it holds (release threshold: all)
 	// and holds the HBM budget from the start (as far as the device has it free): admitting and retiring requests then
 	// makes no allocation call into the CUDA driver, whose calls took up to ~1 s under contention on shared hosts.
@@ -351,18 +344,23 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 	cc::ReduceArgs *d_rr = nullptr;
 	cc::ForceArgs *d_fa = nullptr;
 	cc::LbInst *d_li = nullptr;
-	int *d_pre = nullptr, *d_shape = nullptr;
-	unsigned *d_queue = nullptr;
+	int *d_pre = nullptr, *d_shape = nullptr, *d_dim = nullptr;
+	unsigned *d_queue = nullptr, *d_count = nullptr;
 	cc::LbBrief *d_brief = nullptr;
 	SV_CUDA(cudaMalloc(&d_ra, sizeof(cc::RhoArgs) * o.max_slots));
 	SV_CUDA(cudaMalloc(&d_rr, sizeof(cc::ReduceArgs) * o.max_slots));
 	SV_CUDA(cudaMalloc(&d_fa, sizeof(cc::ForceArgs) * o.max_slots));
 	SV_CUDA(cudaMalloc(&d_li, sizeof(cc::LbInst) * o.max_slots));
-	SV_CUDA(cudaMalloc(&d_pre, sizeof(int) * 3 * (o.max_slots + 3)));
+	SV_CUDA(cudaMalloc(&d_pre, sizeof(int) * 3 * (o.max_slots + 1)));
 	SV_CUDA(cudaMalloc(&d_shape, sizeof(int) * 3 * o.max_slots));
-	SV_CUDA(cudaMalloc(&d_queue, sizeof(unsigned) * 18));
+	SV_CUDA(cudaMalloc(&d_dim, sizeof(int) * o.max_slots));
+	SV_CUDA(cudaMalloc(&d_queue, sizeof(unsigned) * 2));
+	SV_CUDA(cudaMalloc(&d_count, sizeof(unsigned) * (3 * o.max_slots + 1)));
 	SV_CUDA(cudaMalloc(&d_brief, sizeof(cc::LbBrief) * o.max_slots));
-	SV_CUDA(cudaMemset(d_queue, 0, sizeof(unsigned) * 18));
+	SV_CUDA(cudaMemset(d_queue, 0, sizeof(unsigned) * 2));
+	// the fused launch's completion counts are zero between launches (its items reset them); the error word after
+	// the counts of the current round's requests must start at zero too
+	SV_CUDA(cudaMemset(d_count, 0, sizeof(unsigned) * (3 * o.max_slots + 1)));
 	const auto t0 = std::chrono::steady_clock::now();
 	auto now = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
 	int done = 0;
@@ -444,86 +442,65 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 			}
 			continue;
 		}
-		// 2. descriptors of the active set, grouped by dimension (the slots ordered by dimension, so that each group's
-		// L-BFGS instances are a contiguous range)
-		std::stable_sort(active.begin(), active.end(), [](const Slot &x, const Slot &y) { return x.d < y.d; });
+		// 2. descriptors of the active set, requests by decreasing work (the fused launch's work queue then hands out
+		// the longest items first)
+		std::stable_sort(active.begin(), active.end(), [](const Slot &x, const Slot &y) {
+			return (double)x.N * x.rr.nslot > (double)y.N * y.rr.nslot;
+		});
 		const int A = (int)active.size();
 		std::vector<cc::LbInst> li(A);
-		for (int a = 0; a < A; a++)
-			li[a] = active[a].li;
-		std::vector<cc::RhoArgs> ra;
-		std::vector<cc::ReduceArgs> rr;
-		std::vector<cc::ForceArgs> fa;
-		std::vector<int> pre, shape;
-		struct G {
-			int D, off, B, pre_off, shape_off, total[3], rho_row, force_row, maxn;
-		};
-		std::vector<G> groups;
-		for (int D = 1; D <= 3; D++) {
-			G g = {D, (int)ra.size(), 0, (int)pre.size(), (int)shape.size(), {0, 0, 0}, 1, 1, 0};
-			std::vector<int> members;
-			for (int a = 0; a < A; a++)
-				if (active[a].d == D)
-					members.push_back(a);
-			if (members.empty())
-				continue;
-			g.B = (int)members.size();
-			std::vector<int> p3(3 * (g.B + 1), 0), s3(3 * g.B, 0);
-			for (int k = 0; k < g.B; k++) {
-				const Slot &sl = active[members[k]];
-				ra.push_back(sl.ra);
-				rr.push_back(sl.rr);
-				fa.push_back(sl.fa);
-				for (int ph = 0; ph < 3; ph++) {
-					p3[ph * (g.B + 1) + k + 1] = p3[ph * (g.B + 1) + k] + sl.blocks[ph];
-					s3[ph * g.B + k] = sl.shape[ph];
-				}
-				g.rho_row = std::max(g.rho_row, sl.rho_row);
-				g.force_row = std::max(g.force_row, sl.force_row);
-				g.maxn = std::max(g.maxn, sl.li.n);
+		std::vector<cc::RhoArgs> ra(A);
+		std::vector<cc::ReduceArgs> rr(A);
+		std::vector<cc::ForceArgs> fa(A);
+		std::vector<int> pre(3 * (A + 1), 0), shape(3 * A, 0), dim(A, 0);
+		int rho_row = 1, force_row = 1, maxd = 1, maxn = 0;
+		for (int k = 0; k < A; k++) {
+			const Slot &sl = active[k];
+			li[k] = sl.li;
+			ra[k] = sl.ra;
+			rr[k] = sl.rr;
+			fa[k] = sl.fa;
+			for (int ph = 0; ph < 3; ph++) {
+				pre[ph * (A + 1) + k + 1] = pre[ph * (A + 1) + k] + sl.blocks[ph];
+				shape[ph * A + k] = sl.shape[ph];
 			}
-			for (int ph = 0; ph < 3; ph++)
-				g.total[ph] = p3[ph * (g.B + 1) + g.B];
-			pre.insert(pre.end(), p3.begin(), p3.end());
-			shape.insert(shape.end(), s3.begin(), s3.end());
-			groups.push_back(g);
+			dim[k] = sl.d;
+			rho_row = std::max(rho_row, sl.rho_row);
+			force_row = std::max(force_row, sl.force_row);
+			maxd = std::max(maxd, sl.d);
+			maxn = std::max(maxn, sl.li.n);
 		}
-		SV_CUDA(cudaMemcpyAsync(d_ra, ra.data(), sizeof(cc::RhoArgs) * ra.size(), cudaMemcpyHostToDevice, st));
-		SV_CUDA(cudaMemcpyAsync(d_rr, rr.data(), sizeof(cc::ReduceArgs) * rr.size(), cudaMemcpyHostToDevice, st));
-		SV_CUDA(cudaMemcpyAsync(d_fa, fa.data(), sizeof(cc::ForceArgs) * fa.size(), cudaMemcpyHostToDevice, st));
+		SV_CUDA(cudaMemcpyAsync(d_ra, ra.data(), sizeof(cc::RhoArgs) * A, cudaMemcpyHostToDevice, st));
+		SV_CUDA(cudaMemcpyAsync(d_rr, rr.data(), sizeof(cc::ReduceArgs) * A, cudaMemcpyHostToDevice, st));
+		SV_CUDA(cudaMemcpyAsync(d_fa, fa.data(), sizeof(cc::ForceArgs) * A, cudaMemcpyHostToDevice, st));
 		SV_CUDA(cudaMemcpyAsync(d_li, li.data(), sizeof(cc::LbInst) * A, cudaMemcpyHostToDevice, st));
 		SV_CUDA(cudaMemcpyAsync(d_pre, pre.data(), sizeof(int) * pre.size(), cudaMemcpyHostToDevice, st));
 		SV_CUDA(cudaMemcpyAsync(d_shape, shape.data(), sizeof(int) * shape.size(), cudaMemcpyHostToDevice, st));
+		SV_CUDA(cudaMemcpyAsync(d_dim, dim.data(), sizeof(int) * A, cudaMemcpyHostToDevice, st));
 		// the descriptor vectors are pageable: the copies complete before the iterations read them
-		// Each group runs its iterations (energy and gradient, then its instances' L-BFGS step) on its own stream,
-		// forked from st at the start of the round and joined back at its end; the launches are issued iteration by
-		// iteration across the groups, so every stream has work queued from the start.
-		const int ng = (int)groups.size();
-		if (ng > 1 && cudaEventRecord(ev_fork, st) != cudaSuccess)
-			rc = sfail(CC_ERR_CUDA, "serve: event record failed");
-		for (int k = 1; k < ng && rc == CC_OK; k++)
-			if (cudaStreamWaitEvent(side[k - 1], ev_fork, 0) != cudaSuccess)
-				rc = sfail(CC_ERR_CUDA, "serve: stream wait failed");
+		cc::MBatchArgs ma;
+		ma.rho = d_ra;
+		ma.red = d_rr;
+		ma.force = d_fa;
+		ma.dim = d_dim;
+		ma.pre = d_pre;
+		ma.shape = d_shape;
+		ma.B = A;
+		for (int ph = 0; ph < 3; ph++)
+			ma.total[ph] = pre[ph * (A + 1) + A];
+		ma.want_stage = 1;
+		ma.queue = d_queue;
+		ma.count = d_count;
+		const int nblk = cc::lb_blocks(maxn, nblk_cap);
+		// every iteration: one fused evaluation of all admitted requests, then their L-BFGS step
 		for (int it = 0; it < o.iters_per_round && rc == CC_OK; it++) {
-			for (int k = 0; k < ng && rc == CC_OK; k++) {
-				const G &g = groups[k];
-				cudaStream_t gs = k == 0 ? st : side[k - 1];
-				const cc::LbInst *gli = d_li + g.off;
-				const int gnblk = cc::lb_blocks(g.maxn, nblk_cap);
-				if ((rc = cc::launch_multi(g.D, false, d_ra + g.off, d_rr + g.off, d_fa + g.off, d_pre + g.pre_off,
-				                           d_shape + g.shape_off, g.B, g.total, g.rho_row, g.force_row,
-				                           d_queue + 6 * (g.D - 1), gs))) {
-					s_err = std::string("serve: ") + cc_last_error();
-					break;
-				}
-				if (cc::lb_step(gli, g.B, gnblk, g.maxn, gs) != cudaSuccess)
-					rc = sfail(CC_ERR_CUDA, "serve: kernel launch failed");
+			if ((rc = cc::launch_mbatch(0, ma, rho_row, force_row, maxd, st))) {
+				s_err = std::string("serve: ") + cc_last_error();
+				break;
 			}
+			if (cc::lb_step(d_li, A, nblk, maxn, st) != cudaSuccess)
+				rc = sfail(CC_ERR_CUDA, "serve: kernel launch failed");
 		}
-		for (int k = 1; k < ng && rc == CC_OK; k++)
-			if (cudaEventRecord(ev_join[k - 1], side[k - 1]) != cudaSuccess ||
-			    cudaStreamWaitEvent(st, ev_join[k - 1], 0) != cudaSuccess)
-				rc = sfail(CC_ERR_CUDA, "serve: stream join failed");
 		if (rc)
 			break;
 		// 3. retire finished requests
@@ -531,7 +508,13 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 		cc::lb_brief_kernel<<<(A + 127) / 128, 128, 0, st>>>(d_li, A, d_brief);
 		SV_CUDA(cudaGetLastError());
 		SV_CUDA(cudaMemcpyAsync(hs.data(), d_brief, sizeof(cc::LbBrief) * A, cudaMemcpyDeviceToHost, st));
+		unsigned wait_err = 0;
+		SV_CUDA(cudaMemcpyAsync(&wait_err, d_count + 3 * A, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
 		SV_CUDA(cudaStreamSynchronize(st));
+		if (wait_err) {
+			rc = sfail(CC_ERR_TIMEOUT, "serve: a bounded wait of the fused evaluation kernel ran out");
+			break;
+		}
 		const double tdone = now();
 		std::vector<Slot> keep;
 		for (int a = 0; a < A; a++) {
@@ -553,8 +536,6 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 		}
 		active.swap(keep);
 	}
-	cudaStreamSynchronize(side[0]);   // on an error path a side stream may not have been joined yet
-	cudaStreamSynchronize(side[1]);
 	for (Slot &s : active)
 		cudaFreeAsync(s.mem, st);
 	cudaStreamSynchronize(st);
@@ -566,15 +547,11 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 	cudaFree(d_li);
 	cudaFree(d_pre);
 	cudaFree(d_shape);
+	cudaFree(d_dim);
 	cudaFree(d_queue);
+	cudaFree(d_count);
 	cudaFree(d_brief);
 	cudaMemPoolDestroy(pool);
-	for (int k = 0; k < 2; k++) {
-		cudaStreamSynchronize(side[k]);
-		cudaStreamDestroy(side[k]);
-		cudaEventDestroy(ev_join[k]);
-	}
-	cudaEventDestroy(ev_fork);
 	cudaStreamDestroy(st);
 	return rc;
 }
