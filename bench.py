@@ -357,7 +357,7 @@ def run_extras(args, cc, torch):
     ms = a.elapsed_time(b) / reps
     out["batched"] = {"workload": f"{args.batch} instances, d in {{2,3}}, N log-uniform [200,5000], chi U[0.10,0.49], "
                                   "v=(1-|k|/K)^2, FP64", "ms_per_step": ms, "instance_evals_per_s": args.batch / (ms / 1e3),
-                      "pairs_per_s": pairs / (ms / 1e3), "launches_per_step": 3 * len({p.d for p in pots}),
+                      "pairs_per_s": pairs / (ms / 1e3), "launches_per_step": 1,
                       "autotuned_tile": {"particles_per_rho_block": tile[0], "segments_per_force_block": tile[1]}}
     del batch
     # ground states per second: the plain single-configuration FP64 path, one instance after another, against the

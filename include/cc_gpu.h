@@ -163,10 +163,11 @@ int cc_minimize(cc_handle *h, int64_t N, double *frac, const cc_lbfgs_opts *opts
 
 /* --- batches of independent configurations (no counterpart in the reference, which evaluates one at a time) ---
  * A batch holds `count` instances, each an existing handle (its cell, constraint set, Shift) with a fixed particle
- * count N[i]. One evaluation of the batch is, per dimension present, one persistent launch of each of the rho, reduce
- * and force kernels (work items of all instances share the grid), the dimensions on parallel streams; a batched
- * minimisation runs every instance's L-BFGS at once, and instances that have finished are skipped item by item. The
- * handles must outlive the batch. */
+ * count N[i]. One evaluation of the batch is ONE persistent launch of the fused batch kernel: the rho, split-reduction
+ * and force work items of every instance, of every dimension, share one work queue, an instance's phases ordered by
+ * completion counts (bounded waits: CC_ERR_TIMEOUT if one runs out); a batched minimisation runs every instance's
+ * L-BFGS at once, and instances that have finished are skipped item by item. An instance's results do not depend on
+ * the rest of the batch. The handles must outlive the batch. */
 typedef struct cc_batch cc_batch;
 int cc_batch_create(int count, cc_handle *const *handles, const int64_t *N, cc_batch **out);
 int cc_batch_destroy(cc_batch *b);
@@ -185,6 +186,11 @@ int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opt
  * is returned in *per_split and *segs_per_split (either may be NULL). Results of different shapes agree to rounding;
  * with one shape every instance's result is independent of the rest of the batch. */
 int cc_batch_autotune(cc_batch *b, int reps, int *per_split, int *segs_per_split);
+/* Test hook of the fused batch kernel's bounded waits: every wait gives up after `polls` polls (0: the default, about
+ * half a second) and, with phantom > 0, the reduction items of the first instance in the launch order wait for
+ * `phantom` rho items more than it has, so their waits run out: the evaluation then returns CC_ERR_TIMEOUT (its
+ * results are not to be used) and clears the error, and the next evaluation with phantom = 0 is a normal one. */
+int cc_batch_set_wait_test(cc_batch *b, unsigned polls, int phantom);
 
 /* --- Monte Carlo moves ----------------------------------------------------------------------------------------------
  * Replace ShiftedCCPotential_ForMC::TryMove / AcceptMove (potential/CollectiveCoordinatePotential.h:1906-1957): the

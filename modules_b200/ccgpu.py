@@ -109,6 +109,7 @@ _SIGS = {
     "cc_batch_energy_grad": (_i, [_vp, _vp, ctypes.POINTER(_vp), _i]),
     "cc_batch_eval_device": (_i, [_vp, _i, _vp]),
     "cc_batch_autotune": (_i, [_vp, _i, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
+    "cc_batch_set_wait_test": (_i, [_vp, ctypes.c_uint, _i]),
     "cc_batch_minimize": (_i, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(LbfgsOpts), ctypes.POINTER(LbfgsResult)]),
     "cc_serve": (_i, [ctypes.POINTER(ServeRequest), _i, ctypes.POINTER(ServeOpts), ctypes.POINTER(ServeResult),
                       ctypes.POINTER(_d)]),
@@ -512,6 +513,10 @@ class CCBatch:
         ps, sg = _i(), _i()
         _check(self._lib.cc_batch_autotune(self._b, reps, ctypes.byref(ps), ctypes.byref(sg)))
         return ps.value, sg.value
+
+    def set_wait_test(self, polls=0, phantom=0):
+        """Test hook of the fused batch kernel's bounded waits (include/cc_gpu.h cc_batch_set_wait_test)."""
+        _check(self._lib.cc_batch_set_wait_test(self._b, int(polls), int(phantom)))
 
     def minimize(self, fracs, stopval=STOPVAL_GROUND_STATE, history=40, max_evals=100000, precision=PREC_FP64,
                  gtol=0.0, ftol=1e-15, switch_energy_per_particle=1e-12, iters_per_check=32):

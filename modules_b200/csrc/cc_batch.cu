@@ -116,6 +116,7 @@ struct cc_batch {
 	unsigned *d_count = nullptr;             // 3 x B completion counts + 1 error word
 	int total[3] = {0, 0, 0};
 	int rho_row = 1, force_row = 1, maxd = 1;
+	unsigned wait_spins = 0, wait_phantom = 0;   // cc_batch_set_wait_test
 	std::vector<cc::RhoArgs> rho;            // host copies of set 0 (in `order`)
 	std::vector<cc::ReduceArgs> red;
 	std::vector<cc::ForceArgs> force;
@@ -145,6 +146,8 @@ cc::MBatchArgs batch_args(const cc_batch *b, int set, int want_stage)
 	a.want_stage = want_stage;
 	a.queue = b->d_queue;
 	a.count = b->d_count;
+	a.spins = b->wait_spins;
+	a.phantom = b->wait_phantom;
 	return a;
 }
 
@@ -447,6 +450,15 @@ int cc_batch_set_positions(cc_batch *b, const double *const *frac)
 		                        cudaMemcpyHostToDevice, b->stream));
 		CC_CUDA(cudaStreamSynchronize(b->stream));
 	}
+	return CC_OK;
+}
+
+int cc_batch_set_wait_test(cc_batch *b, unsigned polls, int phantom)
+{
+	if (!b || phantom < 0)
+		return fail(CC_ERR_ARG, "invalid wait test arguments");
+	b->wait_spins = polls;
+	b->wait_phantom = (unsigned)phantom;
 	return CC_OK;
 }
 

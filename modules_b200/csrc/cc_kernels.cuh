@@ -322,12 +322,13 @@ __device__ __forceinline__ BodyShared &body_shared()
 // items' results are visible). Thread 0 polls; after kReadySpins polls it sets *err and gives up, so a fault ends the
 // launch with an error status instead of a hang.
 constexpr unsigned kReadySpins = 1u << 22;
-__device__ __forceinline__ void wait_ready(const unsigned *ready, unsigned need, unsigned *err)
+__device__ __forceinline__ void wait_ready(const unsigned *ready, unsigned need, unsigned *err, unsigned spins)
 {
 	if (threadIdx.x == 0) {
+		const unsigned limit = spins ? spins : kReadySpins;
 		unsigned it = 0;
 		while (*(volatile const unsigned *)ready < need) {
-			if (++it > kReadySpins) {
+			if (++it > limit) {
 				atomicExch(err, 1u);
 				break;
 			}
@@ -562,9 +563,9 @@ struct ReduceArgs {
 	const double *slotS0;
 	double npart;
 	// fused batch launch: wait until *ready >= ready_need (the instance's rho items done) before reading partials;
-	// err is raised when that bounded wait runs out. Null outside that launch.
+	// err is raised when that bounded wait runs out (after ready_spins polls, 0: kReadySpins). Null outside it.
 	const unsigned *ready;
-	unsigned ready_need;
+	unsigned ready_need, ready_spins;
 	unsigned *err;
 };
 
@@ -583,7 +584,7 @@ __device__ __forceinline__ void reduce_body(const ReduceArgs &a, const int chunk
 	if (eval_skipped(a.skip, a.stage, a.want_stage))
 		return;
 	if (a.ready)
-		wait_ready(a.ready, a.ready_need, a.err);
+		wait_ready(a.ready, a.ready_need, a.err, a.ready_spins);
 	const int s0 = min(a.nsplit, c * per), s1 = min(a.nsplit, s0 + per);
 	double2 t = make_double2(0.0, 0.0);
 	if (slot < a.nslot) {
@@ -711,9 +712,9 @@ struct ForceArgs {
 	const int *stage;
 	int want_stage;
 	// fused batch launch: wait until *ready >= ready_need (the instance's reduce items done) before reading u; err is
-	// raised when that bounded wait runs out. Null outside that launch.
+	// raised when that bounded wait runs out (after ready_spins polls, 0: kReadySpins). Null outside that launch.
 	const unsigned *ready;
-	unsigned ready_need;
+	unsigned ready_need, ready_spins;
 	unsigned *err;
 };
 
@@ -773,7 +774,7 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 	if (eval_skipped(a.skip, a.stage, a.want_stage))   // uniform over the instance
 		return;
 	if (a.ready)
-		wait_ready(a.ready, a.ready_need, a.err);
+		wait_ready(a.ready, a.ready_need, a.err, a.ready_spins);
 	if (a.E_out && pgroup == 0 && ks == 0 && warp == 0) {
 		// the energy, summed in the order of the reduce kernel's last block
 		double e = 0.0;
@@ -975,6 +976,8 @@ struct MBatchArgs {
 	int want_stage;       // MODE 0 / 1: instances whose stage word differs are skipped (as the three-kernel launches)
 	unsigned *queue;      // 2 words, zero between launches
 	unsigned *count;      // 3 x B completed items per instance and phase (zero between launches), then 1 error word
+	unsigned spins;       // polls of each bounded wait before it gives up (0: kReadySpins)
+	unsigned phantom;     // test hook: instance 0's reduce items wait for this many rho items more than it has
 };
 
 constexpr int kMBatchThreads = 256;
@@ -1009,7 +1012,8 @@ __device__ __forceinline__ void mbatch_item(const MBatchArgs &A, int phase, int 
 		else
 			r.want_stage = A.want_stage;
 		r.ready = A.count + b;
-		r.ready_need = (unsigned)(__ldg(A.pre + b + 1) - __ldg(A.pre + b));
+		r.ready_need = (unsigned)(__ldg(A.pre + b + 1) - __ldg(A.pre + b)) + (b == 0 ? A.phantom : 0u);
+		r.ready_spins = A.spins;
 		r.err = err;
 		reduce_body(r, local, __ldg(A.shape + A.B + b));
 	} else {
@@ -1023,6 +1027,7 @@ __device__ __forceinline__ void mbatch_item(const MBatchArgs &A, int phase, int 
 		}
 		f.ready = A.count + A.B + b;
 		f.ready_need = (unsigned)(__ldg(A.pre + (A.B + 1) + b + 1) - __ldg(A.pre + (A.B + 1) + b));
+		f.ready_spins = A.spins;
 		f.err = err;
 		const int pg = __ldg(A.shape + 2 * A.B + b);
 		if constexpr (MODE != 0) {

@@ -491,6 +491,8 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 		ma.want_stage = 1;
 		ma.queue = d_queue;
 		ma.count = d_count;
+		ma.spins = 0;
+		ma.phantom = 0;
 		const int nblk = cc::lb_blocks(maxn, nblk_cap);
 		// every iteration: one fused evaluation of all admitted requests, then their L-BFGS step
 		for (int it = 0; it < o.iters_per_round && rc == CC_OK; it++) {

@@ -70,3 +70,28 @@ def test_objective_nan_first_variable(gpu):
     f1, g1 = p.objective(x, 10.0)
     assert f1 == f0 and np.array_equal(g1, g0)
     assert abs(f0 - float(r["E"])) <= 1e-10 * abs(float(r["E"]))
+
+
+@pytest.mark.gpu
+def test_batch_bounded_wait_runs_out_and_recovers(gpu):
+    """The fused batch kernel's bounded wait, made to run out from the host (the first instance's reduce items wait
+    for one rho item that does not exist, 2000 polls): the evaluation reports CC_ERR_TIMEOUT (-4), and the next
+    evaluation of the same batch, with the hook off, is bitwise the one before."""
+    rng = np.random.default_rng(3)
+    pots, N, fracs = [], [], []
+    for d, n, chi in [(2, 300, 0.3), (3, 400, 0.25), (2, 150, 0.4)]:
+        basis = np.eye(d) * n ** (1.0 / d)
+        modes, V = gpu.stealthy_kset(d, basis, n, chi)
+        pots.append(gpu.CCPotential(d, basis, modes, V))
+        N.append(n)
+        fracs.append(rng.random((n, d)))
+    batch = gpu.CCBatch(pots, N)
+    batch.set_positions(fracs)
+    E0, F0 = batch.energy_and_forces()
+    batch.set_wait_test(polls=2000, phantom=1)
+    with pytest.raises(gpu.CCError) as e:
+        batch.energy_and_forces()
+    assert e.value.code == -4
+    batch.set_wait_test(0, 0)
+    E1, F1 = batch.energy_and_forces()
+    assert np.array_equal(E0, E1) and all(np.array_equal(a, b) for a, b in zip(F0, F1))
