@@ -21,6 +21,11 @@
 namespace cc {
 
 constexpr int kLbMaxHist = 64;
+// Restarts of a stalled FP64 minimisation (line search without decrease, or relative change below ftol) while the
+// energy is above the stop value: the history is dropped and the run continues from the last accepted point, up to
+// this many times, as the reference's driver restarts its optimiser in each of its three passes
+// (potential/StructureOptimization.cpp:1046-1072).
+constexpr int kLbRestarts = 2;
 constexpr int kLbThreads = 256;
 
 enum LbStatus {
@@ -39,6 +44,7 @@ struct LbState {
 	int64_t max_evals, evals, iters;
 	int m, count, head;     // history size, pairs stored, ring slot of the oldest pair
 	int status, accepted, rejects, small_steps;
+	int restarts;           // fresh-history restarts after a stall short of the stop value (at most kLbRestarts)
 	int newslot;            // ring slot the update kernel fills with the accepted pair, or -1
 	int stage;              // precision stage of the evaluations: 0 mixed, 1 FP64
 	int sched;              // 1: mixed precision until switch_E (or a stall), then FP64
@@ -235,10 +241,15 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 				st->status = kLbLineSearch;
 			else if (st->evals >= st->max_evals)
 				st->status = kLbMaxEval;
-			if (st->sched && st->stage == 0 && st->status == kLbLineSearch) {
-				// the mixed stage stalled at its noise floor: continue in FP64 from x with a fresh history
+			const bool mixed_stage = st->sched && st->stage == 0;
+			if (st->status == kLbLineSearch && (mixed_stage || (E > st->stopval && st->restarts < kLbRestarts))) {
+				// the mixed stage stalled at its noise floor: continue in FP64 from x with a fresh history; an FP64
+				// run that stalled short of the stop value: restart from x with a fresh history
+				if (mixed_stage)
+					st->stage = 1;
+				else
+					st->restarts++;
 				st->status = kLbRunning;
-				st->stage = 1;
 				st->count = 0;
 				st->head = 0;
 				st->E = INFINITY;
@@ -280,6 +291,12 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 				// switch to FP64: the accepted point is re-evaluated in FP64 as a fresh start (E = inf accepts it)
 				st->status = kLbRunning;
 				st->stage = 1;
+				st->small_steps = 0;
+				sh_accept = 2;
+			} else if (st->status == kLbFtol && Et > st->stopval && st->restarts < kLbRestarts) {
+				// stalled short of the stop value: restart from the accepted point with a fresh history
+				st->status = kLbRunning;
+				st->restarts++;
 				st->small_steps = 0;
 				sh_accept = 2;
 			}
@@ -377,7 +394,8 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 		}
 		gdn = lb_warp_sum(gdn);
 		if (lane == 0 && sh_accept == 2) {
-			// stage switch: move to the accepted point (the update kernel does), drop the history, zero step
+			// fresh start (stage switch, or a restart after a stall): move to the accepted point (the update kernel
+			// does), drop the history, zero step
 			st->count = 0;
 			st->head = 0;
 			st->newslot = -1;
