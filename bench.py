@@ -304,32 +304,41 @@ def run_single_legs(cc, torch):
         "schedule_s": t_sched, "schedule_evals": int(ev2), "schedule_E_per_particle": E2 / n,
         "sk_modes": int(len(kq)), "sk_ms_per_call": t_sk * 1e3, "max_S_constrained": float(S[inside].max()),
         "mean_S_beyond": float(S[~inside].mean())}
-    # 2D N=1e5 chi=0.20 (M=40002): FP64 and mixed precision on the same positions
-    d, n, chi = 2, 100000, 0.20
-    basis = np.eye(d) * n ** (1.0 / d)
-    modes, V = cc.stealthy_kset(d, basis, n, chi)
-    pot = cc.CCPotential(d, basis, modes, V)
-    frac = np.random.default_rng(11).random((n, d))
+    # 2D N=1e5 chi=0.20 (M=40002): the configuration of tests/golden/large_2d_n100000.npz, whose E, F and rho are the
+    # reference's own FP64 results (made by tests/golden/make_golden_large.py); every path's error is against them
+    with np.load(os.path.join(ROOT, "tests", "golden", "large_2d_n100000.npz")) as z:
+        g = {k: z[k] for k in z.files}
+    d, n = 2, len(g["frac"])
+    modes, V, frac = g["modes"], g["V"], g["frac"]
+    pot = cc.CCPotential(d, g["basis"], modes, V)
     fdev = torch.tensor(frac, dtype=torch.float64, device="cuda")
+    kmax = 2 * np.pi * float(np.sqrt((modes.astype(np.float64) ** 2).sum(1).max())) / float(g["basis"][0, 0])
+    sF = 4 * float(np.abs(V).sum()) * n * kmax / float(g["volume"])   # the reference tests' force scale
+
+    def errs(E, F, prec):
+        pot.set_configuration(frac)
+        re, im = pot.rho(prec)
+        return {"rel_err_E": abs(E - float(g["E"])) / abs(float(g["E"])),
+                "max_err_F_over_max_F": float(np.abs(F - g["F"]).max() / np.abs(g["F"]).max()),
+                "max_err_F_over_scale": float(np.abs(F - g["F"]).max() / sF),
+                "max_err_rho_over_N": float(max(np.abs(re - g["rho_re"]).max(), np.abs(im - g["rho_im"]).max()) / n)}
+
     pot.set_path(cc.PATH_NUFFT)
     msnu, Enu, Fnu = device_eval_ms(torch, pot, n, d, fdev, cc.PREC_FP64)
+    e_nu = errs(Enu, Fnu, cc.PREC_FP64)
     pot.set_path(cc.PATH_SPLIT)   # the direct kernels, FP64 and mixed
     ms64, E64, F64 = device_eval_ms(torch, pot, n, d, fdev, cc.PREC_FP64)
+    e_64 = errs(E64, F64, cc.PREC_FP64)
     msmx, Emx, Fmx = device_eval_ms(torch, pot, n, d, fdev, cc.PREC_MIXED)
-    pot.set_configuration(frac)
-    re64, im64 = pot.rho(cc.PREC_FP64)
-    remx, immx = pot.rho(cc.PREC_MIXED)
+    e_mx = errs(Emx, Fmx, cc.PREC_MIXED)
     pairs = n * len(V)
     out["large_2d_n100000"] = {
-        "workload": "2D N=100000 chi=0.20 M=40002 v=1, energy + forces, L2 flushed before each evaluation",
+        "workload": "2D N=100000 chi=0.20 M=40002 v=1, energy + forces, L2 flushed before each evaluation; errors "
+                    "against the reference's own FP64 results on the same positions (tests/golden/large_2d_n100000)",
         "nufft_ms": msnu, "nufft_pairs_per_s_equivalent": pairs / (msnu / 1e3),
-        "nufft_rel_err_E": abs(Enu - E64) / abs(E64),
-        "nufft_max_err_F_over_max_F": float(np.abs(Fnu - F64).max() / np.abs(F64).max()),
-        "fp64_ms": ms64, "mixed_ms": msmx, "fp64_pairs_per_s": pairs / (ms64 / 1e3),
-        "mixed_pairs_per_s": pairs / (msmx / 1e3),
-        "mixed_rel_err_E": abs(Emx - E64) / abs(E64),
-        "mixed_max_err_F_over_max_F": float(np.abs(Fmx - F64).max() / np.abs(F64).max()),
-        "mixed_max_err_rho_over_sqrtN": float(max(np.abs(remx - re64).max(), np.abs(immx - im64).max()) / np.sqrt(n))}
+        "fp64_ms": ms64, "mixed_ms": msmx, "mixed_speedup": ms64 / msmx,
+        "fp64_pairs_per_s": pairs / (ms64 / 1e3), "mixed_pairs_per_s": pairs / (msmx / 1e3),
+        "nufft_vs_reference": e_nu, "fp64_vs_reference": e_64, "mixed_vs_reference": e_mx}
     return out
 
 
