@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--path", default="auto", choices=["auto", "split", "fused"],
+    ap.add_argument("--path", default="auto", choices=["auto", "split"],
                     help="evaluation path of the headline (auto: the library's own choice for this size)")
     ap.add_argument("--pool", type=int, default=4096,
                     help="configurations per step: each step evaluates every one once (their positions exceed L2)")
@@ -459,7 +459,7 @@ def run_ours(args):
     modes, V = cc.stealthy_kset(D, basis, N, CHI)
     M = len(V)
     pot = cc.CCPotential(D, basis, modes, V)
-    path = {"auto": cc.PATH_AUTO, "split": cc.PATH_SPLIT, "fused": cc.PATH_FUSED}[args.path]
+    path = {"auto": cc.PATH_AUTO, "split": cc.PATH_SPLIT}[args.path]
     pot.set_path(path)
     P = args.pool
     host_pool = pool_positions(P, rank)
@@ -545,19 +545,13 @@ def run_ours(args):
     pairs = N * M
     t_rho, t_red, t_force = rho_ms / nt, red_ms / nt, force_ms / nt
     peak = cc.probe_fma_peak(cc.PREC_FP64 if prec == cc.PREC_FP64 else cc.PREC_MIXED)
-    one_kernel = info["path"] == "fused"
-    if one_kernel:
-        dom, fl, tk = "cc_fused_kernel", (17.0 + 2 * D) * pairs, t_force
-        kernel_ms = {"cc_fused_kernel": t_force}
-        launches_per_eval = 1
+    rho_flops, force_flops = 8.0 * pairs, (9.0 + 2 * D) * pairs
+    if t_force >= t_rho:
+        dom, fl, tk = "cc_force_kernel", force_flops, t_force
     else:
-        rho_flops, force_flops = 8.0 * pairs, (9.0 + 2 * D) * pairs
-        if t_force >= t_rho:
-            dom, fl, tk = "cc_force_kernel", force_flops, t_force
-        else:
-            dom, fl, tk = "cc_rho_kernel", rho_flops, t_rho
-        kernel_ms = {"cc_rho_kernel": t_rho, "cc_reduce_kernel": t_red, "cc_force_kernel": t_force}
-        launches_per_eval = 3
+        dom, fl, tk = "cc_rho_kernel", rho_flops, t_rho
+    kernel_ms = {"cc_rho_kernel": t_rho, "cc_reduce_kernel": t_red, "cc_force_kernel": t_force}
+    launches_per_eval = 3
     achieved = fl / (tk * 1e-3) / 1e12
 
     # end to end through the C ABI with host buffers: per evaluation the positions go in (cc_set_positions) and E
@@ -611,8 +605,7 @@ def run_ours(args):
                              "traffic_unit": "bytes per launch (ncu capture)", "kernel_ms": kernel_ms,
                              "timing": "CUDA events around each kernel inside a replayed graph; under programmatic "
                                        "dependent launch consecutive kernels overlap, so the intervals overlap and "
-                                       "sum to more than the evaluation"
-                                       if not one_kernel else "CUDA events around the kernel inside a replayed graph",
+                                       "sum to more than the evaluation",
                              "eval_us": 1e3 * ms / (K * P)},
                 "clocks": clk, "cpu_baseline": cpu}
         line.update(extras)

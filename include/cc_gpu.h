@@ -325,23 +325,22 @@ const char *cc_noalloc_last_error(void);
 
 /* --- execution path (no counterpart in the reference) ---------------------------------------------------------
  * CC_PATH_SPLIT: three kernels per evaluation (rho, split reduction + energy, forces) chained by
- * programmatic dependent launch. CC_PATH_FUSED: problems whose per-particle phase tables fit 64 MiB per layout run
- * as ONE cooperative kernel per evaluation (phases separated by grid barriers whose waits are bounded; larger ones
- * still take the split path). CC_PATH_NUFFT: energies and forces by non-uniform FFTs (the reference's FINUFFT
+ * programmatic dependent launch (value 1 is not a path: a cooperative one-kernel evaluation measured slower than the
+ * split path at every size, 41.6 against 25.6 us at 3D N=2000, and was removed). CC_PATH_NUFFT: energies and forces by non-uniform FFTs (the reference's FINUFFT
  * backend, CollectiveCoordinatePotential.h:119-1250): a type-1 transform for rho, type-2 transforms for the forces,
  * "exponential of semicircle" kernel of width 14 on a fine grid of twice the mode range, always in FP64, errors
  * ~1e-13 of sum |c|; its cost grows with N w^d + grid log(grid) instead of N M, so it wins for many particles and
  * many modes. CC_PATH_AUTO (the default, as the reference gates its FINUFFT backend): the NUFFT path for an
  * evaluation whose estimated time is lower there (e.g. 2D N=1e5 with M=4e4 modes), the split path otherwise.
  * Results agree to rounding; each path repeats bitwise. */
-enum { CC_PATH_SPLIT = 0, CC_PATH_FUSED = 1, CC_PATH_NUFFT = 2, CC_PATH_AUTO = 3 };
+enum { CC_PATH_SPLIT = 0, CC_PATH_NUFFT = 2, CC_PATH_AUTO = 3 };
 int cc_set_path(cc_handle *h, int path);
-/* The path (CC_PATH_SPLIT, CC_PATH_FUSED or CC_PATH_NUFFT) an evaluation of N particles at `precision` takes on this
+/* The path (CC_PATH_SPLIT or CC_PATH_NUFFT) an evaluation of N particles at `precision` takes on this
  * handle under its current cc_set_path choice. */
 int cc_eval_path(cc_handle *h, int64_t N, int precision, int *path);
 
-/* Synchronise the device and report CC_ERR_TIMEOUT if a bounded grid-barrier wait of an earlier device-path
- * evaluation ran out (the error is then cleared). Host-path calls check this themselves. */
+/* Synchronise the device and report a CUDA error of an earlier device-path evaluation (no kernel of a handle waits
+ * on another block, so there is no timeout to report here). */
 int cc_check_device_error(cc_handle *h);
 
 /* --- measurement support (no counterpart in the reference) --------------------------------------------------- */

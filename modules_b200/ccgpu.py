@@ -67,7 +67,7 @@ class ServeOpts(ctypes.Structure):
 
 
 PREC_SCHEDULE = 2
-PATH_SPLIT, PATH_FUSED, PATH_NUFFT, PATH_AUTO = 0, 1, 2, 3
+PATH_SPLIT, PATH_NUFFT, PATH_AUTO = 0, 2, 3
 STOPVAL_GROUND_STATE = -1.0
 
 _SIGS = {
@@ -426,14 +426,14 @@ class CCPotential:
 
     def set_path(self, path):
         """PATH_AUTO (default): PATH_NUFFT where it is estimated faster, else PATH_SPLIT; PATH_SPLIT: the three-kernel
-        direct path; PATH_FUSED: one cooperative kernel when the tables fit; PATH_NUFFT: non-uniform FFTs (FP64)."""
+        direct path; PATH_NUFFT: non-uniform FFTs (FP64)."""
         _check(self._lib.cc_set_path(self._h, int(path)))
 
     def eval_path(self, N, precision=PREC_FP64):
-        """The path an evaluation of N particles takes: "split", "fused" or "nufft"."""
+        """The path an evaluation of N particles takes: "split" or "nufft"."""
         p = _i()
         _check(self._lib.cc_eval_path(self._h, int(N), precision, ctypes.byref(p)))
-        return {PATH_SPLIT: "split", PATH_FUSED: "fused", PATH_NUFFT: "nufft"}[p.value]
+        return {PATH_SPLIT: "split", PATH_NUFFT: "nufft"}[p.value]
 
     def check_device_error(self):
         _check(self._lib.cc_check_device_error(self._h))

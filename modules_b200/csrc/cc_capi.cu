@@ -7,7 +7,6 @@
 //   cc_force_kernel -> Cartesian forces and/or the gradient in fractional coordinates.
 // There is no CPU path: without a CUDA device every call that computes returns CC_ERR_NOGPU.
 #include "../../include/cc_gpu.h"
-#include "cc_fused.cuh"
 #include "cc_internal.h"
 #include "cc_kernels.cuh"
 #include "cc_lbfgs.cuh"
@@ -637,78 +636,7 @@ int run_force(cc_handle *h, int64_t N, const double *d_frac, double *d_F, double
 	return launch_force(h->d, a, mixed, N, f->host.max_row, st);
 }
 
-// ---------------------------------------------------------------------------------------------------------------
-// fused path: one cooperative launch per evaluation (tables in global memory, grid barriers)
-// ---------------------------------------------------------------------------------------------------------------
-constexpr size_t kFusedTabCap = 64u << 20;   // bytes per table layout: beyond this the three-kernel path runs
-
-bool fused_eligible(const cc_handle *h, int64_t N, bool mixed)
-{
-	if (N <= 0 || h->main.plan.nslot == 0 || h->d_slotS0)
-		return false;
-	const size_t esz = mixed ? sizeof(float2) : sizeof(double2);
-	const size_t Npad = (size_t)(N + 31) / 32 * 32;
-	return (size_t)((h->gspec.row | 1)) * Npad * esz <= kFusedTabCap;
-}
-
-template <int D, int L, bool MIXED> int fused_grid(int *grid)
-{
-	static int per_sm = -1;
-	if (per_sm < 0) {
-		CC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cc::cc_fused_kernel<D, L, MIXED>,
-		                                                     cc::kFusedThreads, 0));
-		if (per_sm < 1)
-			return fail(CC_ERR_CUDA, "fused kernel cannot be resident");
-	}
-	*grid = per_sm * sm_count();
-	return CC_OK;
-}
-
-template <int D, int L, bool MIXED> int launch_fused_t(cc::FusedArgs &a, int grid, cudaStream_t st)
-{
-	void *args[] = {&a};
-	CC_CUDA(cudaLaunchCooperativeKernel((const void *)cc::cc_fused_kernel<D, L, MIXED>, dim3(grid),
-	                                    dim3(cc::kFusedThreads), args, 0, st));
-	return CC_OK;
-}
-
-int fused_grid_d(int d, bool mixed, int *grid)
-{
-	switch (d) {
-	case 1: return mixed ? fused_grid<1, 8, true>(grid) : fused_grid<1, 8, false>(grid);
-	case 2: return mixed ? fused_grid<2, 8, true>(grid) : fused_grid<2, 8, false>(grid);
-	default: return mixed ? fused_grid<3, 8, true>(grid) : fused_grid<3, 8, false>(grid);
-	}
-}
-
-int launch_fused(int d, bool mixed, cc::FusedArgs &a, int grid, cudaStream_t st)
-{
-	switch (d) {
-	case 1: return mixed ? launch_fused_t<1, 8, true>(a, grid, st) : launch_fused_t<1, 8, false>(a, grid, st);
-	case 2: return mixed ? launch_fused_t<2, 8, true>(a, grid, st) : launch_fused_t<2, 8, false>(a, grid, st);
-	default: return mixed ? launch_fused_t<3, 8, true>(a, grid, st) : launch_fused_t<3, 8, false>(a, grid, st);
-	}
-}
-
-int get_kstart(cc_handle *h, int nks, int **out)
-{
-	for (auto &kv : h->kstarts)
-		if (kv.first == nks) {
-			*out = kv.second;
-			return CC_OK;
-		}
-	const int nseg = (int)h->main.plan.segs.size();
-	std::vector<int> ks(nks + 1);
-	for (int k = 0; k <= nks; k++)
-		ks[k] = (int)((int64_t)nseg * k / nks);
-	int *d = nullptr;
-	if (int rc = upload(&d, ks))
-		return rc;
-	h->kstarts.push_back(std::make_pair(nks, d));
-	*out = d;
-	return CC_OK;
-}
-
+// Grow a device buffer to n elements (contents not kept).
 template <class T> int grow(T **p, size_t &cap, size_t n)
 {
 	if (n <= cap)
@@ -720,86 +648,6 @@ template <class T> int grow(T **p, size_t &cap, size_t n)
 		return rc;
 	cap = n;
 	return CC_OK;
-}
-
-int run_fused(cc_handle *h, int64_t N, const double *d_frac, double *d_E, double *d_F, double *d_gfrac, bool mixed,
-              cudaStream_t st)
-{
-	const cc::Plan &p = h->main.plan;
-	int grid = 0;
-	if (int rc = fused_grid_d(h->d, mixed, &grid))
-		return rc;
-	const size_t esz = mixed ? sizeof(float2) : sizeof(double2);
-	const int Npad = (int)((N + 31) / 32 * 32);
-	const int rowP = h->gspec.row | 1;
-	const size_t tab_bytes = std::max((size_t)rowP * Npad, (size_t)h->gspec.row * Npad) * esz;
-	if (tab_bytes > h->tab_cap) {
-		cudaFree(h->d_tabP);
-		cudaFree(h->d_tabE);
-		h->d_tabP = h->d_tabE = nullptr;
-		h->tab_cap = 0;
-		unsigned char *a = nullptr, *b = nullptr;
-		int rc;
-		if ((rc = dev_alloc(&a, tab_bytes)) || (rc = dev_alloc(&b, tab_bytes)))
-			return rc;
-		h->d_tabP = a;
-		h->d_tabE = b;
-		h->tab_cap = tab_bytes;
-	}
-	const int ng = p.ngroups();
-	int nsplit = std::max(1, (2 * grid + ng - 1) / ng);
-	nsplit = (int)std::min<int64_t>(nsplit, std::max<int64_t>(1, N / 16));
-	const int per_split = (int)((N + nsplit - 1) / nsplit);
-	nsplit = (int)((N + per_split - 1) / per_split);
-	const int pg = (int)((N + 31) / 32);
-	const int nseg = (int)p.segs.size();
-	int nks = std::max(1, (2 * grid + pg - 1) / pg);
-	nks = std::min(nks, std::max(1, nseg / 64));
-	int *kstart = nullptr;
-	size_t eb_cap = (size_t)h->eblockF_cap;
-	if (int rc = get_kstart(h, nks, &kstart))
-		return rc;
-	if (int rc = grow(&h->d_eblockF, eb_cap, (size_t)grid))
-		return rc;
-	h->eblockF_cap = (int)eb_cap;
-	if (int rc = grow(&h->d_partialF, h->partialF_cap, (size_t)nsplit * p.nslot))
-		return rc;
-	if (nks > 1)
-		if (int rc = ensure_partialG(h, (size_t)nks * N * h->d))
-			return rc;
-	cc::FusedArgs a;
-	a.frac = d_frac;
-	a.N = (int)N;
-	a.segs = h->main.segs;
-	a.ngroups = ng;
-	a.nseg = nseg;
-	a.nslot = p.nslot;
-	a.slotV = h->main.slotV;
-	a.rho_offset = h->rho_offset;
-	a.inv_vol = 1.0 / h->volume;
-	a.shift = h->shift;
-	a.spec = h->gspec;
-	a.tabP = h->d_tabP;
-	a.tabE = h->d_tabE;
-	a.Npad = Npad;
-	a.nsplit = nsplit;
-	a.per_split = per_split;
-	a.partial = h->d_partialF;
-	a.rho_slot = h->main.rho_slot;
-	a.u_slot = h->main.u_slot;
-	a.eblock = h->d_eblockF;
-	a.kstart = kstart;
-	a.nksplit = nks;
-	a.partialG = h->d_partialG;
-	a.fcounters = h->d_fcounters;
-	for (int i = 0; i < 9; i++)
-		a.recip[i] = h->recip[i];
-	a.fscale = 2.0 / h->volume;
-	a.F_out = d_F;
-	a.gfrac_out = d_gfrac;
-	a.E_out = d_E;
-	a.bar = h->d_bar;
-	return launch_fused(h->d, mixed, a, grid, st);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -1033,21 +881,6 @@ int run_nufft(cc_handle *h, int64_t N, const double *d_frac, double *d_E, double
 	}
 }
 
-// A grid barrier of an earlier fused launch that ran out of time leaves its error word set: report it and reset.
-int check_barrier(cc_handle *h, bool always = false)
-{
-	if (!always && !h->fused_ran)
-		return CC_OK;
-	h->fused_ran = false;
-	unsigned w[3] = {0, 0, 0};
-	CC_CUDA(cudaMemcpy(w, h->d_bar, sizeof(w), cudaMemcpyDeviceToHost));
-	if (w[2] != 0u) {
-		CC_CUDA(cudaMemset(h->d_bar, 0, 3 * sizeof(unsigned)));
-		return fail(CC_ERR_TIMEOUT, "a grid barrier wait ran out in the fused evaluation kernel");
-	}
-	return CC_OK;
-}
-
 int check_handle(const cc_handle *h)
 {
 	if (!h)
@@ -1100,9 +933,7 @@ int create_common(int d, const double *basis, int64_t M, const int32_t *modes, c
 		return fail(CC_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
 	}
 	cc::Plan plan = cc::build_plan(d, M, modes, V, 8);
-	h->gspec = cc::global_spec(plan);
-	if ((rc = upload_kset(h->main, plan)) || (rc = dev_alloc(&h->d_E, 2)) || (rc = dev_alloc(&h->d_bar, 4)) ||
-	    (rc = (cudaMemset(h->d_bar, 0, 4 * sizeof(unsigned)) == cudaSuccess ? CC_OK : CC_ERR_CUDA))) {
+	if ((rc = upload_kset(h->main, plan)) || (rc = dev_alloc(&h->d_E, 2))) {
 		cc_destroy(h);
 		return rc;
 	}
@@ -1239,18 +1070,6 @@ int eval_device(cc_handle *h, int64_t N, const double *d_frac, double *d_E, doub
 		if (e2)
 			CC_CUDA(record_timing(e2, st));
 		int rc = run_nufft(h, N, d_frac, d_E, d_F, d_gfrac, want_rho_mode, st);
-		if (e3)
-			CC_CUDA(record_timing(e3, st));
-		return rc;
-	}
-	if (!want_rho_mode && h->use_fused && !h->d_skip && fused_eligible(h, N, mixed)) {
-		// one cooperative launch: the whole evaluation is reported as the force interval
-		if (e1)
-			CC_CUDA(record_timing(e1, st));
-		if (e2)
-			CC_CUDA(record_timing(e2, st));
-		int rc = run_fused(h, N, d_frac, d_E, d_F, d_gfrac, mixed, st);
-		h->fused_ran = true;
 		if (e3)
 			CC_CUDA(record_timing(e3, st));
 		return rc;
@@ -1544,13 +1363,6 @@ int cc_destroy(cc_handle *h)
 	cudaFree(h->d_rho_trial);
 	cudaFree(h->d_rho_cur);
 	cudaFree(h->d_mc_part);
-	cudaFree(h->d_tabP);
-	cudaFree(h->d_tabE);
-	cudaFree(h->d_bar);
-	cudaFree(h->d_eblockF);
-	cudaFree(h->d_partialF);
-	for (auto &kv : h->kstarts)
-		cudaFree(kv.second);
 	for (cudaEvent_t e : h->ev)
 		cudaEventDestroy(e);
 	for (auto &g : h->graphs)
@@ -1647,7 +1459,7 @@ int cc_energy_grad(cc_handle *h, double *E, double *F, int precision)
 	h->lastF_valid = false;
 	// E and F are written by the kernels straight into the mapped pinned result buffer
 	bool done = false;
-	if (!h->timing && !h->use_fused && !h->d_skip && N > 0 && h->main.plan.nslot > 0)
+	if (!h->timing && !h->d_skip && N > 0 && h->main.plan.nslot > 0)
 		if (int rc = launch_eval_graph(h, N, precision, forces, &done))
 			return rc;
 	if (!done) {
@@ -1663,8 +1475,6 @@ int cc_energy_grad(cc_handle *h, double *E, double *F, int precision)
 	}
 	CC_CUDA(cudaStreamSynchronize(h->stream));
 	h->in_pending = false;   // ev_in was recorded on this stream: the staging buffer is free again
-	if (int rc = check_barrier(h))
-		return rc;
 	*E = h->h_pin[0];
 	if (F && N > 0) {
 		std::memcpy(F, h->h_pin + 2, sizeof(double) * N * h->d);
@@ -1817,8 +1627,6 @@ int cc_objective(cc_handle *h, int64_t N, const double *x, double rescale, doubl
 		CC_CUDA(cudaMemcpyAsync(h->h_pin + 2, h->d_gfrac, sizeof(double) * N * d, cudaMemcpyDeviceToHost,
 		                        h->stream));
 	CC_CUDA(cudaStreamSynchronize(h->stream));
-	if (int rc = check_barrier(h))
-		return rc;
 	*f = h->h_pin[0];
 	if (grad)
 		for (int64_t i = 0; i < N * d; i++)
@@ -1895,11 +1703,10 @@ int cc_set_path(cc_handle *h, int path)
 {
 	if (int rc = check_handle(h))
 		return rc;
-	if (path != CC_PATH_SPLIT && path != CC_PATH_FUSED && path != CC_PATH_NUFFT && path != CC_PATH_AUTO)
-		return fail(CC_ERR_ARG, "path must be CC_PATH_SPLIT, CC_PATH_FUSED, CC_PATH_NUFFT or CC_PATH_AUTO");
+	if (path != CC_PATH_SPLIT && path != CC_PATH_NUFFT && path != CC_PATH_AUTO)
+		return fail(CC_ERR_ARG, "path must be CC_PATH_SPLIT, CC_PATH_NUFFT or CC_PATH_AUTO");
 	if (h->d_slotS0 && path == CC_PATH_NUFFT)
 		return fail(CC_ERR_ARG, "the NUFFT path evaluates the plain collective-coordinate form only");
-	h->use_fused = path == CC_PATH_FUSED;
 	h->use_nufft = path == CC_PATH_NUFFT;
 	h->auto_path = path == CC_PATH_AUTO;
 	g_alloc_gen++;   // captured evaluations hold the old path
@@ -1911,7 +1718,7 @@ int cc_check_device_error(cc_handle *h)
 	if (int rc = check_handle(h))
 		return rc;
 	CC_CUDA(cudaDeviceSynchronize());
-	return check_barrier(h, true);
+	return CC_OK;
 }
 
 int cc_set_timing(cc_handle *h, int on)
@@ -1975,11 +1782,8 @@ int cc_eval_path(cc_handle *h, int64_t N, int precision, int *path)
 		return rc;
 	if (!path || N < 0)
 		return fail(CC_ERR_ARG, "invalid cc_eval_path arguments");
-	const bool mixed = precision == CC_PREC_MIXED && !h->d_slotS0;
 	if (h->nsub <= 1 && (h->use_nufft || (h->auto_path && nufft_preferred(h, N))) && h->main.plan.nslot > 0)
 		*path = CC_PATH_NUFFT;
-	else if (h->nsub <= 1 && h->use_fused && fused_eligible(h, N, mixed))
-		*path = CC_PATH_FUSED;
 	else
 		*path = CC_PATH_SPLIT;
 	return CC_OK;

@@ -204,7 +204,6 @@ struct cc_handle {
 	cudaEvent_t ev_in = nullptr;    // recorded after the last copy out of h_in
 	bool in_pending = false;
 	bool lastF_valid = false;       // h_pin + 2 holds the forces of the bound positions
-	bool fused_ran = false;         // a fused launch ran since the barrier word was last read
 	bool upload_pending = false;    // h_in holds positions not yet copied to d_frac
 	double *d_pin = nullptr;        // device view of h_pin (mapped pinned memory): kernels write E and F there
 	// captured evaluations of cc_energy_grad (upload + kernels writing into h_pin), per (N, precision, forces)
@@ -218,17 +217,6 @@ struct cc_handle {
 	int64_t last_N = -1;            // key and generation of the last direct cc_energy_grad (captured when repeated)
 	int last_precision = -1, last_forces = -1;
 	unsigned long long last_gen = 0;
-	// fused (cooperative) path
-	cc::TabSpec gspec;
-	void *d_tabP = nullptr, *d_tabE = nullptr;
-	size_t tab_cap = 0;             // bytes of each table buffer
-	unsigned *d_bar = nullptr;      // grid barrier words (arrivals, generation, error)
-	double *d_eblockF = nullptr;
-	int eblockF_cap = 0;
-	double2 *d_partialF = nullptr;
-	size_t partialF_cap = 0;
-	std::vector<std::pair<int, int *> > kstarts;   // even segment splits per count
-	bool use_fused = false;         // cc_set_path
 	// S2 form (cc_create_s2): per-slot targets S0, E = sum V (|rho|^2 / N - S0)^2 + shift; split path only
 	double *d_slotS0 = nullptr;
 	// S2 over nsub sub-configurations (cc_create_s2_multiconfig): rho and u per sub-configuration, block partials

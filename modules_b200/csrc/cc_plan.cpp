@@ -194,19 +194,6 @@ Plan build_plan(int d, int64_t M, const int32_t *modes, const double *V, int L)
 	return p;
 }
 
-TabSpec global_spec(const Plan &p)
-{
-	Ranges r;
-	for (const Seg &s : p.segs)
-		if (s.len > 0)
-			r.add(p.d, s);
-	if (r.empty) {
-		Seg z = {0, 0, 0, 1};
-		r.add(p.d, z);
-	}
-	return make_spec(p.d, r);
-}
-
 ForceSplits force_splits(const Plan &p, int want)
 {
 	ForceSplits f;

@@ -68,10 +68,6 @@ constexpr int kFullMax = 48;       // prefix axes with a range up to this many i
 // Group M modes (M x d integers) into segments of L slots, in rho groups of 32 segments.
 Plan build_plan(int d, int64_t M, const int32_t *modes, const double *V, int L);
 
-// One table spec covering every segment of the plan (full tables for prefix axes up to kFullMax indices, coarse x
-// fine otherwise); its row may exceed kMaxRow.
-TabSpec global_spec(const Plan &p);
-
 // Cut the plan's segments into at least `want` force splits of similar size whose tables fit kMaxRow entries.
 ForceSplits force_splits(const Plan &p, int want);
 

@@ -1,6 +1,6 @@
 """Evaluate one synthetic stealthy configuration a few times (for profiling a single kernel launch sequence).
 
-    python -m modules_b200.evalcase --d 2 --N 20000 --chi 0.2 --evals 3 [--mixed] [--path split|fused|nufft|auto]
+    python -m modules_b200.evalcase --d 2 --N 20000 --chi 0.2 --evals 3 [--mixed] [--path split|nufft|auto]
     python -m modules_b200.evalcase --batch 512 --evals 3 [--mixed]
     python -m modules_b200.evalcase --serve 120
 
@@ -24,8 +24,7 @@ def main():
     ap.add_argument("--chi", type=float, default=0.2)
     ap.add_argument("--evals", type=int, default=3)
     ap.add_argument("--mixed", action="store_true")
-    ap.add_argument("--fused", action="store_true", help="same as --path fused")
-    ap.add_argument("--path", default="split", choices=["split", "fused", "nufft", "auto"])
+    ap.add_argument("--path", default="split", choices=["split", "nufft", "auto"])
     ap.add_argument("--batch", type=int, default=0, help="evaluate the seeded batch of this many instances")
     ap.add_argument("--serve", type=int, default=0, help="serve the seeded stream of this many requests")
     a = ap.parse_args()
@@ -48,8 +47,8 @@ def main():
     basis = np.eye(a.d) * a.N ** (1.0 / a.d)
     modes, V = cc.stealthy_kset(a.d, basis, a.N, a.chi)
     pot = cc.CCPotential(a.d, basis, modes, V)
-    paths = {"split": cc.PATH_SPLIT, "fused": cc.PATH_FUSED, "nufft": cc.PATH_NUFFT, "auto": cc.PATH_AUTO}
-    pot.set_path(cc.PATH_FUSED if a.fused else paths[a.path])
+    paths = {"split": cc.PATH_SPLIT, "nufft": cc.PATH_NUFFT, "auto": cc.PATH_AUTO}
+    pot.set_path(paths[a.path])
     pot.set_configuration(np.random.default_rng(1).random((a.N, a.d)))
     E = None
     for _ in range(a.evals):

@@ -107,24 +107,6 @@ int main()
 			CHECK(q1 > g * kGroupSegs);
 			check_spec(d, p.rspec[g], p.segs, g * kGroupSegs, q1);
 		}
-		{
-			std::vector<Seg> real;
-			for (const Seg &sg : p.segs)
-				if (sg.len > 0)
-					real.push_back(sg);
-			TabSpec g = global_spec(p);
-			CHECK(g.row > 0);
-			int items = 0, covered = 0;
-			for (int r = 0; r < g.nrun; r++) {
-				items += (g.run[r].count + 7) / 8;
-				covered += g.run[r].count;
-			}
-			CHECK(items == g.items && covered == g.row);
-			// the row limit does not apply to the global spec: check the lookups with a relaxed copy
-			TabSpec relaxed = g;
-			if (relaxed.row <= kMaxRow)
-				check_spec(d, relaxed, real, 0, (int)real.size());
-		}
 		CHECK(p.bstart.size() == p.bspec.size() + 1 && p.bstart.front() == 0 && p.bstart.back() == p.ngroups());
 		for (int b = 0; b < p.nbgroups(); b++) {
 			CHECK(p.bstart[b + 1] > p.bstart[b] && p.bstart[b + 1] - p.bstart[b] <= kBlockGroups);

@@ -135,9 +135,8 @@ def test_gpu_fp64_only_and_refusals(gpu):
     E, F = p.energy_and_forces()
     Em, Fm = p.energy_and_forces(precision=gpu.PREC_MIXED)   # evaluated in FP64 whatever the precision
     assert Em == E and np.array_equal(Fm, F)
-    p.set_path(gpu.PATH_FUSED)                                  # the fused kernel holds the plain form: split path
-    Ef, Ff = p.energy_and_forces()
-    assert Ef == E and np.array_equal(Ff, F)
+    with pytest.raises(gpu.CCError):
+        p.set_path(1)                                           # not a path (include/cc_gpu.h cc_set_path)
     with pytest.raises(gpu.CCError):
         p.set_path(gpu.PATH_NUFFT)
     with pytest.raises(gpu.CCError):
