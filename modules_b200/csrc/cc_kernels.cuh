@@ -581,10 +581,12 @@ __device__ __forceinline__ void reduce_body(const ReduceArgs &a, const int chunk
 	const int per = (a.nsplit + 7) >> 3;
 	cudaGridDependencySynchronize();
 	cudaTriggerProgrammaticLaunchCompletion();
-	if (eval_skipped(a.skip, a.stage, a.want_stage))
-		return;
+	// In the fused batch launch the wait comes first, also for a skipped instance: its last force item resets the
+	// instance's counts, which must not happen while one of its rho or reduce items is still to be counted.
 	if (a.ready)
 		wait_ready(a.ready, a.ready_need, a.err, a.ready_spins);
+	if (eval_skipped(a.skip, a.stage, a.want_stage))
+		return;
 	const int s0 = min(a.nsplit, c * per), s1 = min(a.nsplit, s0 + per);
 	double2 t = make_double2(0.0, 0.0);
 	if (slot < a.nslot) {
@@ -761,9 +763,14 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 	const int nvalid = min(32, a.N - pbase);
 	const int q0 = a.kstart[ks], q1 = a.kstart[ks + 1];
 	// The skip and stage words are written by kernels that completed before this evaluation's rho pass (whose
-	// completion this block's launch implies), like the positions: a finished instance builds no tables.
-	if (eval_skipped(a.skip, a.stage, a.want_stage))
+	// completion this block's launch implies), like the positions: a finished instance builds no tables. In the fused
+	// batch launch its force items still wait for its reduce items (which waited for its rho items), so that the last
+	// of them resets the instance's counts only once every item of the instance has been counted.
+	if (eval_skipped(a.skip, a.stage, a.want_stage)) {
+		if (a.ready)
+			wait_ready(a.ready, a.ready_need, a.err, a.ready_spins);
 		return;
+	}
 	if (threadIdx.x == 0)
 		sp = a.kspec[ks];
 	__syncthreads();
@@ -771,10 +778,10 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 	// while the reduce kernel still runs (programmatic dependent launch), before waiting for u.
 	build_tables<D, C>(sp, a.frac, pbase, 32, nvalid, tab, 1, 32, threadIdx.x, kForceThreads);
 	cudaGridDependencySynchronize();   // u of this step is complete
-	if (eval_skipped(a.skip, a.stage, a.want_stage))   // uniform over the instance
-		return;
 	if (a.ready)
 		wait_ready(a.ready, a.ready_need, a.err, a.ready_spins);
+	if (eval_skipped(a.skip, a.stage, a.want_stage))   // uniform over the instance
+		return;
 	if (a.E_out && pgroup == 0 && ks == 0 && warp == 0) {
 		// the energy, summed in the order of the reduce kernel's last block
 		double e = 0.0;

@@ -111,3 +111,21 @@ def test_batch_ground_states_against_reference(gpu, precision):
         # the stop rule is the GPU's E <= 1e-20 N; the reference's sum of the same configuration differs by rounding
         # (|rho| ~ 1e-10 near the ground state, its rounding ~1e-15: ~1e-5 relative in E)
         assert Er / n < 1.001e-20 and abs(e - Er) / n <= 1e-12
+
+
+def test_batch_counts_survive_finished_instances(gpu):
+    """A batched minimisation in which instances finish at very different times (skipped item by item while the others
+    run), then a second minimisation of the same batch from new starts: every instance ends where it ends alone. The
+    fused launch's per-instance counts must be zero again after every launch, whatever instances were skipped."""
+    specs = [(2, 64, 0.40, 0), (3, 700, 0.25, 3), (2, 250, 0.40, 3), (3, 120, 0.25, 0)]
+    pots, N, fracs = _instances(gpu, specs, seed=4)
+    batch = gpu.CCBatch(pots, N)
+    for seed in (4, 6):
+        rng = np.random.default_rng(seed)
+        starts = [rng.random((n, p.d)) for n, p in zip(N, pots)]
+        xs, E, evals, iters, status = batch.minimize(starts)
+        assert np.all(E / np.array(N) < 1e-20), (E / np.array(N), evals)
+        for k in range(len(pots)):
+            alone = gpu.CCBatch([pots[k]], [N[k]])
+            xa, Ea, ea, ia, sa = alone.minimize([starts[k]])
+            assert np.array_equal(xa[0], xs[k]) and Ea[0] == E[k] and ea[0] == evals[k]
