@@ -519,13 +519,19 @@ __device__ __forceinline__ void rho_body(const RhoArgs &a, const int bg, const i
 	const size_t out_row = (size_t)(split / cs) * a.nslot;
 	for (int e = rank * per + threadIdx.x; e < min(total, (rank + 1) * per); e += kRhoThreads) {
 		const int w = e / (L * 32), r = (e / 32) % L, ln = e & 31;
+		// the cluster's (at most 8) values are loaded together, then added in rank order
+		double2 v[8];
+#pragma unroll
+		for (int k = 0; k < 8; k++)
+			if (k < cs)
+				v[k] = cluster.map_shared_rank(red, k)[e];
 		double2 t = make_double2(0.0, 0.0);
-		for (int k = 0; k < cs; k++) {
-			const double2 *rs = cluster.map_shared_rank(red, k);
-			const double2 v = rs[e];
-			t.x += v.x;
-			t.y += v.y;
-		}
+#pragma unroll
+		for (int k = 0; k < 8; k++)
+			if (k < cs) {
+				t.x += v[k].x;
+				t.y += v[k].y;
+			}
 		a.partial[out_row + (size_t)r * a.nseg + (g0 + w) * 32 + ln] = t;
 	}
 	cluster.sync();
