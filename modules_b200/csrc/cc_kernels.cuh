@@ -310,6 +310,7 @@ struct BodyShared {
 	TabSpec sp;
 	Seg seg[kForceUChunk];
 	double2 red[8][32];
+	double pos[32 * 3];   // the force block's particles' coordinates (loaded together with its table spec)
 	int last;
 };
 __device__ __forceinline__ BodyShared &body_shared()
@@ -777,12 +778,16 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 			wait_ready(a.ready, a.ready_need, a.err, a.ready_spins);
 		return;
 	}
+	// the spec and the block's coordinates are loaded together (neither waits for the other)
+	double *pos = body_shared().pos;
 	if (threadIdx.x == 0)
 		sp = a.kspec[ks];
+	for (int t = threadIdx.x; t < nvalid * D; t += kForceThreads)
+		pos[t] = a.frac[(size_t)pbase * D + t];
 	__syncthreads();
 	// The tables need only the positions, which the rho pass of this evaluation has already read: they are built
 	// while the reduce kernel still runs (programmatic dependent launch), before waiting for u.
-	build_tables<D, C>(sp, a.frac, pbase, 32, nvalid, tab, 1, 32, threadIdx.x, kForceThreads);
+	build_tables<D, C>(sp, pos, 0, 32, nvalid, tab, 1, 32, threadIdx.x, kForceThreads);
 	cudaGridDependencySynchronize();   // u of this step is complete
 	if (a.ready)
 		wait_ready(a.ready, a.ready_need, a.err, a.ready_spins);
@@ -807,9 +812,12 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 	for (int c0 = q0; c0 < q1; c0 += kForceUChunk) {
 		const int nq = min(kForceUChunk, q1 - c0);
 		__syncthreads();   // tables complete (first chunk); the previous chunk's weights are no longer read
+		// FP64: slot-major (a warp's read of one weight is a broadcast); mixed: segment-major, a segment's 8 FP32
+		// weights contiguous (read as four 16-byte broadcasts)
 		for (int e = threadIdx.x; e < nq * L; e += kForceThreads) {
 			const int r = e / nq, qq = e - r * nq;
-			sh_u[r * kForceUChunk + qq] = to_c<C>(__ldcg(a.u_slot + (size_t)r * a.nseg + c0 + qq));
+			sh_u[MIXED ? qq * L + r : r * kForceUChunk + qq] =
+			    to_c<C>(__ldcg(a.u_slot + (size_t)r * a.nseg + c0 + qq));
 		}
 		for (int e = threadIdx.x; e < nq; e += kForceThreads)
 			sh_seg[e] = a.segs[c0 + e];
@@ -876,7 +884,7 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 				const Seg sgm = sh_seg[qq];
 				if (sgm.len == 0)   // padding segment of a rho group: weight 0, no table entries
 					continue;
-				const C *uu = sh_u + qq;
+				const float4 *uu = reinterpret_cast<const float4 *>(sh_u + qq * L);   // slot pairs (2r, 2r + 1)
 				const SeedIdx ix = seed_index<D>(sp, sgm);
 				const C z = seed_from<D, C>(tab + lane, 32, ix);
 				const C w = tab[ix.w * 32 + lane];
@@ -884,22 +892,26 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 				// error along)
 				const R c = (R)2 * w.x;
 				C p = z, q = cmul(z, w);
-				const C u0 = uu[0], u1 = uu[kForceUChunk];
-				R S0 = u0.x * p.y + u0.y * p.x, S1;
+				const float4 u01 = uu[0];
+				R S0 = u01.x * p.y + u01.y * p.x, S1;
 				{
-					const R t = u1.x * q.y + u1.y * q.x;
+					const R t = u01.z * q.y + u01.w * q.x;
 					S0 += t;
 					S1 = t;
 				}
 #pragma unroll
-				for (int r = 2; r < L; r++) {
+				for (int r = 2; r < L; r += 2) {
+					const float4 uv = uu[r / 2];
 					const C n = cheb_next(c, q, p);
-					const C u = uu[r * kForceUChunk];
-					const R t = u.x * n.y + u.y * n.x;
+					const R t = uv.x * n.y + uv.y * n.x;
 					S0 += t;
 					S1 = fma((R)r, t, S1);
-					p = q;
-					q = n;
+					const C n2 = cheb_next(c, n, q);
+					const R t2 = uv.z * n2.y + uv.w * n2.x;
+					S0 += t2;
+					S1 = fma((R)(r + 1), t2, S1);
+					p = n;
+					q = n2;
 				}
 				const double S0d = (double)S0;
 				if (D >= 2)

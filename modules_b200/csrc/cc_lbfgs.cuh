@@ -23,9 +23,9 @@ namespace cc {
 constexpr int kLbMaxHist = 64;
 // Restarts of a stalled FP64 minimisation (line search without decrease, or relative change below ftol) while the
 // energy is above the stop value: the history is dropped and the run continues from the last accepted point, up to
-// this many times, as the reference's driver restarts its optimiser in each of its three passes
-// (potential/StructureOptimization.cpp:1046-1072).
-constexpr int kLbRestarts = 2;
+// this many times (the reference's driver restarts its optimiser in each of its three passes,
+// potential/StructureOptimization.cpp:1046-1072; near chi = 1/2 some configurations need more).
+constexpr int kLbRestarts = 8;
 constexpr int kLbThreads = 256;
 
 enum LbStatus {
