@@ -5,7 +5,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libccgpu.so")
-SOURCES = ["csrc/cc_capi.cu", "csrc/cc_batch.cu", "csrc/cc_plan.cpp", "csrc/cc_noalloc.cu", "csrc/cc_serve.cu",
+SOURCES = ["csrc/cc_capi.cu", "csrc/cc_batch.cu", "csrc/cc_minimize.cu", "csrc/cc_plan.cpp", "csrc/cc_noalloc.cu", "csrc/cc_serve.cu",
            "csrc/cc_multi.cu"]
 HEADERS = ["csrc/cc_internal.h", "csrc/cc_kernels.cuh", "csrc/cc_lbfgs.cuh", "csrc/cc_plan.h", "csrc/cc_error.h", "csrc/cc_nufft.cuh", "csrc/cc_multi_launch.h", "../include/cc_gpu.h"]
 NVCC_FLAGS = [

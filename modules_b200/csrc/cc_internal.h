@@ -147,6 +147,21 @@ int sm_count();
 // CC_ERR_ARG unless precision is CC_PREC_FP64 or CC_PREC_MIXED.
 int check_prec(int precision);
 
+}  // namespace cci
+
+struct cc_handle;
+
+namespace cci {
+
+// CC_ERR_ARG for a null handle.
+int handle_check(const cc_handle *h);
+// The handle's per-particle buffers for N particles (positions, forces, gradients; grow-only).
+int handle_reserve(cc_handle *h, int64_t N);
+// One evaluation of the handle at device positions d_frac (N x d), enqueued on st: E (device), and F (Cartesian) and /
+// or gfrac (fractional gradient) where not null; want_rho_mode also fills rho in constraint order.
+int handle_eval(cc_handle *h, int64_t N, const double *d_frac, double *d_E, double *d_F, double *d_gfrac,
+                bool want_rho_mode, int precision, cudaStream_t st);
+
 constexpr size_t kRhoTabBudget = 48 * 1024;   // shared memory for one chunk of rho tables
 
 template <typename C> size_t rho_smem(int row, int chunk, int L)
