@@ -110,7 +110,7 @@ struct cc_batch {
 	cc::ReduceArgs *d_red[2] = {nullptr, nullptr};
 	cc::ForceArgs *d_force[2] = {nullptr, nullptr};
 	int *d_dim = nullptr;                    // B
-	int *d_pre = nullptr;                    // 3 x (B + 1): rho, reduce and force items per instance
+	int *d_pre = nullptr;                    // 4 x (B + 1): rho, reduce, force, reduce + force items per instance
 	int *d_shape = nullptr;                  // 3 x B
 	unsigned *d_queue = nullptr;             // 2 words
 	unsigned *d_count = nullptr;             // 3 x B completion counts + 1 error word
@@ -156,7 +156,7 @@ cc::MBatchArgs batch_args(const cc_batch *b, int set, int want_stage)
 int batch_build(cc_batch *b, int per_split, int segs_per_split)
 {
 	const int B = (int)b->order.size();
-	std::vector<int> pre(3 * (B + 1), 0), shape(3 * B, 0), dim(B, 0);
+	std::vector<int> pre(4 * (B + 1), 0), shape(3 * B, 0), dim(B, 0);
 	b->rho.clear();
 	b->red.clear();
 	b->force.clear();
@@ -205,6 +205,7 @@ int batch_build(cc_batch *b, int per_split, int segs_per_split)
 		fa.segs = h->main.segs;
 		fa.kstart = f->kstart;
 		fa.kspec = f->kspec;
+		fa.seed = f->seed;
 		fa.nksplit = f->host.count();
 		fa.u_slot = rr.u_slot;
 		fa.nseg = ra.nseg;
@@ -236,6 +237,9 @@ int batch_build(cc_batch *b, int per_split, int segs_per_split)
 	}
 	for (int ph = 0; ph < 3; ph++)
 		b->total[ph] = pre[ph * (B + 1) + B];
+	for (int k = 0; k < B; k++)   // each instance's reduce and force items, consecutive in the queue
+		pre[3 * (B + 1) + k + 1] = pre[3 * (B + 1) + k] + (pre[(B + 1) + k + 1] - pre[(B + 1) + k]) +
+		                           (pre[2 * (B + 1) + k + 1] - pre[2 * (B + 1) + k]);
 	int rc;
 	if ((rc = upload_into(b->d_rho[0], b->rho)) || (rc = upload_into(b->d_red[0], b->red)) ||
 	    (rc = upload_into(b->d_force[0], b->force)) || (rc = upload_into(b->d_pre, pre)) ||
@@ -342,7 +346,7 @@ int cc_batch_create(int count, cc_handle *const *handles, const int64_t *N, cc_b
 	const int B = count;
 	if ((rc = dev_alloc(&b->d_rho[0], B)) || (rc = dev_alloc(&b->d_red[0], B)) || (rc = dev_alloc(&b->d_force[0], B)) ||
 	    (rc = dev_alloc(&b->d_rho[1], B)) || (rc = dev_alloc(&b->d_red[1], B)) || (rc = dev_alloc(&b->d_force[1], B)) ||
-	    (rc = dev_alloc(&b->d_pre, 3 * (B + 1))) || (rc = dev_alloc(&b->d_shape, 3 * B)) ||
+	    (rc = dev_alloc(&b->d_pre, 4 * (B + 1))) || (rc = dev_alloc(&b->d_shape, 3 * B)) ||
 	    (rc = dev_alloc(&b->d_dim, B)) || (rc = dev_alloc(&b->d_queue, 2)) || (rc = dev_alloc(&b->d_count, 3 * B + 1)) ||
 	    (rc = (cudaMemset(b->d_queue, 0, 2 * sizeof(unsigned)) == cudaSuccess &&
 	                   cudaMemset(b->d_count, 0, (3 * B + 1) * sizeof(unsigned)) == cudaSuccess

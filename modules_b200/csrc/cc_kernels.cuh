@@ -173,11 +173,10 @@ __device__ __forceinline__ void build_tables(const TabSpec &sp, const double *__
 	}
 }
 
-// Table indices of a segment's seed: z_0 = prod_e T_e(index_e).
-struct SeedIdx {
-	int a[3], b[3];   // axis e: entry a[e] (full) or a[e] * b[e] (coarse x fine, b[e] >= 0)
-	int w;            // entry of the recurrence step exp(2 pi i s_last)
-};
+// Table indices of a segment's seed: z_0 = prod_e T_e(index_e) (cc_plan.h SegSeed: axis e is entry a[e], full, or
+// a[e] * b[e], coarse x fine with b[e] >= 0; w the entry of the recurrence step exp(2 pi i s_last)). The force pass
+// reads them precomputed on the host for its split's spec; the rho pass forms them once per lane.
+typedef SegSeed SeedIdx;
 
 template <int D>
 __device__ __forceinline__ SeedIdx seed_index(const TabSpec &sp, const Seg &g)
@@ -309,6 +308,7 @@ constexpr int kForceUChunk = 128;   // segments whose slot weights are staged in
 struct BodyShared {
 	TabSpec sp;
 	Seg seg[kForceUChunk];
+	SegSeed seed[kForceUChunk];   // the staged segments' seed indices (force pass)
 	double2 red[8][32];
 	double pos[32 * 3];   // the force block's particles' coordinates (loaded together with its table spec)
 	int last;
@@ -704,6 +704,7 @@ struct ForceArgs {
 	const Seg *segs;
 	const int *kstart;        // nksplit + 1: segment range of each split
 	const TabSpec *kspec;     // nksplit
+	const SegSeed *seed;      // per segment: its seed indices under the spec of its split
 	int nksplit;
 	const double2 *u_slot;    // [nslot], slot of (segment q, step r) = r * nseg + q
 	int nseg;
@@ -762,6 +763,7 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 	double *sh_g = reinterpret_cast<double *>(smem); // reused after the loop: kForceWarps x 32 x D
 	TabSpec &sp = body_shared().sp;
 	Seg *sh_seg = body_shared().seg;
+	SegSeed *sh_seed = body_shared().seed;
 	int &sh_last = body_shared().last;
 
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -819,8 +821,10 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 			sh_u[MIXED ? qq * L + r : r * kForceUChunk + qq] =
 			    to_c<C>(__ldcg(a.u_slot + (size_t)r * a.nseg + c0 + qq));
 		}
-		for (int e = threadIdx.x; e < nq; e += kForceThreads)
+		for (int e = threadIdx.x; e < nq; e += kForceThreads) {
 			sh_seg[e] = a.segs[c0 + e];
+			sh_seed[e] = a.seed[c0 + e];
+		}
 		__syncthreads();
 		if constexpr (!MIXED) {
 			// FP64: warp w takes a contiguous run of the chunk's segments; a segment that continues the previous one
@@ -846,7 +850,7 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 					z1 = cheb_next(c, z0, q);
 					run++;
 				} else {
-					const SeedIdx ix = seed_index<D>(sp, sgm);
+					const SeedIdx &ix = sh_seed[qq];
 					z0 = seed_from<D, double2>(tab + lane, 32, ix);
 					const double2 w = tab[ix.w * 32 + lane];
 					c = 2.0 * w.x;
@@ -885,7 +889,7 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 				if (sgm.len == 0)   // padding segment of a rho group: weight 0, no table entries
 					continue;
 				const float4 *uu = reinterpret_cast<const float4 *>(sh_u + qq * L);   // slot pairs (2r, 2r + 1)
-				const SeedIdx ix = seed_index<D>(sp, sgm);
+				const SeedIdx &ix = sh_seed[qq];
 				const C z = seed_from<D, C>(tab + lane, 32, ix);
 				const C w = tab[ix.w * 32 + lane];
 				// three-term recurrence along the segment (re-seeded per segment: in FP32 a longer run would carry its
@@ -982,8 +986,8 @@ __global__ void __launch_bounds__(kForceThreads, 3) cc_force_kernel(ForceArgs a)
 // fused batch evaluation: ONE persistent launch per batched energy + gradient step
 // ---------------------------------------------------------------------------------------------------------------
 // The rho, split-reduction and force items of every instance of a batch (every dimension) come from one work queue,
-// in that order: items [0, total[0]) are rho blocks, the next total[1] reduce chunks, the last total[2] force blocks,
-// each phase ordered by instance (instances by decreasing work). An item raises its instance's count of that phase
+// in this order: items [0, total[0]) are the rho blocks of every instance, then instance by instance its reduce chunks
+// followed by its force blocks (instances by decreasing work). An item raises its instance's count of that phase
 // when its results are visible; a reduce item waits (bounded) for its instance's rho count, a force item for its
 // reduce count, after building its tables. An item only waits for items taken from the queue before it, by blocks that
 // are running and never wait for later items, so the launch cannot deadlock whatever number of blocks is resident. The
@@ -994,7 +998,7 @@ struct MBatchArgs {
 	const ReduceArgs *red;
 	const ForceArgs *force;
 	const int *dim;       // B: dimension of each instance (1..3)
-	const int *pre;       // 3 x (B + 1): prefix sums of each instance's rho, reduce and force items
+	const int *pre;       // 4 x (B + 1): prefix sums of each instance's rho, reduce, force, and reduce + force items
 	const int *shape;     // 3 x B: rho block groups, reduce chunks, force particle groups
 	int B;
 	int total[3];
@@ -1070,16 +1074,27 @@ template <int MODE>
 __global__ void __launch_bounds__(kMBatchThreads, 3) cc_mbatch_kernel(MBatchArgs A)
 {
 	__shared__ int sh_item;
-	const int T0 = A.total[0], T1 = T0 + A.total[1], T = T1 + A.total[2];
+	const int T0 = A.total[0], T = T0 + A.total[1] + A.total[2];
 	// Under programmatic dependent launch this grid may be scheduled while the previous one still takes items from
 	// the same queue (its blocks trigger after their first item): wait for it to complete before taking any.
 	cudaGridDependencySynchronize();
 	for (int item; (item = queue_next(A.queue, &sh_item)) < T;) {
-		const int phase = item < T0 ? 0 : item < T1 ? 1 : 2;
+		// rho items first; then, instance by instance, its reduce items followed by its force items
+		int phase, b, local;
+		if (item < T0) {
+			phase = 0;
+			b = find_instance(A.pre, A.B, item);
+			local = item - __ldg(A.pre + b);
+		} else {
+			const int *prf = A.pre + 3 * (A.B + 1);
+			const int li = item - T0;
+			b = find_instance(prf, A.B, li);
+			const int within = li - __ldg(prf + b);
+			const int nred = __ldg(A.pre + (A.B + 1) + b + 1) - __ldg(A.pre + (A.B + 1) + b);
+			phase = within < nred ? 1 : 2;
+			local = within < nred ? within : within - nred;
+		}
 		const int *pre = A.pre + phase * (A.B + 1);
-		const int li = item - (phase == 0 ? 0 : phase == 1 ? T0 : T1);
-		const int b = find_instance(pre, A.B, li);
-		const int local = li - __ldg(pre + b);
 		const int d = __ldg(A.dim + b);
 		if (d == 3)
 			mbatch_item<3, MODE>(A, phase, b, local);

@@ -89,7 +89,7 @@ int serve_per_split(const cc::Plan &p)
 
 // Offsets of a request's arrays in its one allocation (see open_slot).
 struct SlotOffsets {
-	size_t segs, slotV, bstart, bspec, kstart, kspec, part, rho, u, ep, tk, pg, fc, x, g, d, xt, gt, S, Y, lp, st;
+	size_t segs, slotV, bstart, bspec, kstart, kspec, seed, part, rho, u, ep, tk, pg, fc, x, g, d, xt, gt, S, Y, lp, st;
 };
 
 int fill_slot(const cc_request &r, int idx, int m, const cc::Plan &p, const cc::ForceSplits &fs, double vol,
@@ -123,6 +123,7 @@ int open_slot(const cc_request &r, int idx, int m, int nblk_cap, cudaMemPool_t p
 	const size_t o_segs = c.take(sizeof(cc::Seg) * p.segs.size()), o_slotV = c.take(sizeof(double) * p.nslot),
 	             o_bstart = c.take(sizeof(int) * p.bstart.size()), o_bspec = c.take(sizeof(cc::TabSpec) * p.bspec.size()),
 	             o_kstart = c.take(sizeof(int) * fs.start.size()), o_kspec = c.take(sizeof(cc::TabSpec) * fs.spec.size()),
+	             o_seed = c.take(sizeof(cc::SegSeed) * fs.seed.size()),
 	             o_part = c.take(sizeof(double2) * (size_t)nsplit * p.nslot), o_rho = c.take(sizeof(double2) * p.nslot),
 	             o_u = c.take(sizeof(double2) * p.nslot), o_ep = c.take(sizeof(double) * nchunks),
 	             o_tk = c.take(sizeof(unsigned)), o_pg = c.take(sizeof(double) * (size_t)nks * n),
@@ -141,7 +142,7 @@ int open_slot(const cc_request &r, int idx, int m, int nblk_cap, cudaMemPool_t p
 		}
 	}
 	if (int rc = fill_slot(r, idx, m, p, fs, vol, recip, per_split, nsplit, nchunks, pgroups, nks, st,
-	                       {o_segs, o_slotV, o_bstart, o_bspec, o_kstart, o_kspec, o_part, o_rho, o_u, o_ep, o_tk,
+	                       {o_segs, o_slotV, o_bstart, o_bspec, o_kstart, o_kspec, o_seed, o_part, o_rho, o_u, o_ep, o_tk,
 	                        o_pg, o_fc, o_x, o_g, o_d, o_xt, o_gt, o_S, o_Y, o_lp, o_st},
 	                       s)) {
 		cudaFreeAsync(s.mem, st);
@@ -157,7 +158,7 @@ int fill_slot(const cc_request &r, int idx, int m, const cc::Plan &p, const cc::
               const SlotOffsets &off, Slot &s)
 {
 	const size_t o_segs = off.segs, o_slotV = off.slotV, o_bstart = off.bstart, o_bspec = off.bspec,
-	             o_kstart = off.kstart, o_kspec = off.kspec, o_part = off.part, o_rho = off.rho, o_u = off.u,
+	             o_kstart = off.kstart, o_kspec = off.kspec, o_seed = off.seed, o_part = off.part, o_rho = off.rho, o_u = off.u,
 	             o_ep = off.ep, o_tk = off.tk, o_pg = off.pg, o_fc = off.fc, o_x = off.x, o_g = off.g, o_d = off.d,
 	             o_xt = off.xt, o_gt = off.gt, o_S = off.S, o_Y = off.Y, o_lp = off.lp, o_st = off.st;
 	const int d = r.d;
@@ -171,6 +172,8 @@ int fill_slot(const cc_request &r, int idx, int m, const cc::Plan &p, const cc::
 	                        st));
 	SV_CUDA(cudaMemcpyAsync(b + o_kstart, fs.start.data(), sizeof(int) * fs.start.size(), cudaMemcpyHostToDevice, st));
 	SV_CUDA(cudaMemcpyAsync(b + o_kspec, fs.spec.data(), sizeof(cc::TabSpec) * fs.spec.size(), cudaMemcpyHostToDevice,
+	                        st));
+	SV_CUDA(cudaMemcpyAsync(b + o_seed, fs.seed.data(), sizeof(cc::SegSeed) * fs.seed.size(), cudaMemcpyHostToDevice,
 	                        st));
 	SV_CUDA(cudaMemsetAsync(b + o_tk, 0, sizeof(unsigned), st));
 	SV_CUDA(cudaMemsetAsync(b + o_fc, 0, sizeof(unsigned) * pgroups, st));
@@ -246,6 +249,7 @@ int fill_slot(const cc_request &r, int idx, int m, const cc::Plan &p, const cc::
 	fa.segs = ra.segs;
 	fa.kstart = reinterpret_cast<const int *>(b + o_kstart);
 	fa.kspec = reinterpret_cast<const cc::TabSpec *>(b + o_kspec);
+	fa.seed = reinterpret_cast<const cc::SegSeed *>(b + o_seed);
 	fa.nksplit = nks;
 	fa.u_slot = rr.u_slot;
 	fa.nseg = ra.nseg;
@@ -273,6 +277,9 @@ int fill_slot(const cc_request &r, int idx, int m, const cc::Plan &p, const cc::
 	return CC_OK;
 }
 
+// a request's reduce and force items in one fused launch
+int sl_items(const Slot &s) { return s.blocks[1] + s.blocks[2]; }
+
 // device bytes a request will need (the same carve as open_slot, with the k-set size estimated from chi N d)
 size_t estimate_bytes(const cc_request &r, int m, int nblk_cap)
 {
@@ -280,7 +287,7 @@ size_t estimate_bytes(const cc_request &r, int m, int nblk_cap)
 	const double nseg = M / 4 + 64, nslot = nseg * 8;
 	const double n = (double)r.N * r.d;
 	const double nsplit = std::ceil(r.N / (double)kServeMinPerSplit), nks = std::ceil(nseg / cc::kBatchSegsPerSplit) + 2;
-	const double bytes = 16 * nseg + 8 * nslot + 2 * 768 * (nseg / 256 + nks + 2) + 16 * nsplit * nslot + 32 * nslot +
+	const double bytes = 48 * nseg + 8 * nslot + 2 * 768 * (nseg / 256 + nks + 2) + 16 * nsplit * nslot + 32 * nslot +
 	                     8 * nks * n + 8 * n * (5 + 2 * m) + 8.0 * nblk_cap * cc::lb_ndots(m) + 16384;
 	return (size_t)bytes;
 }
@@ -351,7 +358,7 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 	SV_CUDA(cudaMalloc(&d_rr, sizeof(cc::ReduceArgs) * o.max_slots));
 	SV_CUDA(cudaMalloc(&d_fa, sizeof(cc::ForceArgs) * o.max_slots));
 	SV_CUDA(cudaMalloc(&d_li, sizeof(cc::LbInst) * o.max_slots));
-	SV_CUDA(cudaMalloc(&d_pre, sizeof(int) * 3 * (o.max_slots + 1)));
+	SV_CUDA(cudaMalloc(&d_pre, sizeof(int) * 4 * (o.max_slots + 1)));
 	SV_CUDA(cudaMalloc(&d_shape, sizeof(int) * 3 * o.max_slots));
 	SV_CUDA(cudaMalloc(&d_dim, sizeof(int) * o.max_slots));
 	SV_CUDA(cudaMalloc(&d_queue, sizeof(unsigned) * 2));
@@ -452,7 +459,7 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 		std::vector<cc::RhoArgs> ra(A);
 		std::vector<cc::ReduceArgs> rr(A);
 		std::vector<cc::ForceArgs> fa(A);
-		std::vector<int> pre(3 * (A + 1), 0), shape(3 * A, 0), dim(A, 0);
+		std::vector<int> pre(4 * (A + 1), 0), shape(3 * A, 0), dim(A, 0);
 		int rho_row = 1, force_row = 1, maxd = 1, maxn = 0;
 		for (int k = 0; k < A; k++) {
 			const Slot &sl = active[k];
@@ -470,6 +477,8 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 			maxd = std::max(maxd, sl.d);
 			maxn = std::max(maxn, sl.li.n);
 		}
+		for (int k = 0; k < A; k++)   // each request's reduce and force items, consecutive in the queue
+			pre[3 * (A + 1) + k + 1] = pre[3 * (A + 1) + k] + sl_items(active[k]);
 		SV_CUDA(cudaMemcpyAsync(d_ra, ra.data(), sizeof(cc::RhoArgs) * A, cudaMemcpyHostToDevice, st));
 		SV_CUDA(cudaMemcpyAsync(d_rr, rr.data(), sizeof(cc::ReduceArgs) * A, cudaMemcpyHostToDevice, st));
 		SV_CUDA(cudaMemcpyAsync(d_fa, fa.data(), sizeof(cc::ForceArgs) * A, cudaMemcpyHostToDevice, st));
