@@ -205,7 +205,6 @@ int batch_build(cc_batch *b, int per_split, int segs_per_split)
 		fa.segs = h->main.segs;
 		fa.kstart = f->kstart;
 		fa.kspec = f->kspec;
-		fa.seed = f->seed;
 		fa.nksplit = f->host.count();
 		fa.u_slot = rr.u_slot;
 		fa.nseg = ra.nseg;

@@ -82,8 +82,7 @@ int cci::get_splits(DevKSet &k, int want, const DevSplits **out)
 	f.want = want;
 	f.host = cc::force_splits(k.plan, want);
 	int rc;
-	if ((rc = upload(&f.kstart, f.host.start)) || (rc = upload(&f.kspec, f.host.spec)) ||
-	    (rc = upload(&f.seed, f.host.seed)))
+	if ((rc = upload(&f.kstart, f.host.start)) || (rc = upload(&f.kspec, f.host.spec)))
 		return rc;
 	k.splits.push_back(f);
 	*out = &k.splits.back();
@@ -610,7 +609,6 @@ int run_force(cc_handle *h, int64_t N, const double *d_frac, double *d_F, double
 	a.segs = h->main.segs;
 	a.kstart = f->kstart;
 	a.kspec = f->kspec;
-	a.seed = f->seed;
 	a.nksplit = nk;
 	a.u_slot = h->main.u_slot;
 	a.nseg = (int)p.segs.size();

@@ -36,7 +36,6 @@ struct DevSplits {
 	cc::ForceSplits host;
 	int *kstart = nullptr;
 	cc::TabSpec *kspec = nullptr;
-	cc::SegSeed *seed = nullptr;   // per segment, under its split's spec
 };
 
 struct DevKSet {
@@ -73,7 +72,6 @@ struct DevKSet {
 		for (DevSplits &f : splits) {
 			cudaFree(f.kstart);
 			cudaFree(f.kspec);
-			cudaFree(f.seed);
 		}
 		*this = DevKSet();
 	}

@@ -173,10 +173,11 @@ __device__ __forceinline__ void build_tables(const TabSpec &sp, const double *__
 	}
 }
 
-// Table indices of a segment's seed: z_0 = prod_e T_e(index_e) (cc_plan.h SegSeed: axis e is entry a[e], full, or
-// a[e] * b[e], coarse x fine with b[e] >= 0; w the entry of the recurrence step exp(2 pi i s_last)). The force pass
-// reads them precomputed on the host for its split's spec; the rho pass forms them once per lane.
-typedef SegSeed SeedIdx;
+// Table indices of a segment's seed: z_0 = prod_e T_e(index_e).
+struct SeedIdx {
+	int a[3], b[3];   // axis e: entry a[e] (full) or a[e] * b[e] (coarse x fine, b[e] >= 0)
+	int w;            // entry of the recurrence step exp(2 pi i s_last)
+};
 
 template <int D>
 __device__ __forceinline__ SeedIdx seed_index(const TabSpec &sp, const Seg &g)
@@ -308,7 +309,6 @@ constexpr int kForceUChunk = 128;   // segments whose slot weights are staged in
 struct BodyShared {
 	TabSpec sp;
 	Seg seg[kForceUChunk];
-	SegSeed seed[kForceUChunk];   // the staged segments' seed indices (force pass)
 	double2 red[8][32];
 	double pos[32 * 3];   // the force block's particles' coordinates (loaded together with its table spec)
 	int last;
@@ -704,7 +704,6 @@ struct ForceArgs {
 	const Seg *segs;
 	const int *kstart;        // nksplit + 1: segment range of each split
 	const TabSpec *kspec;     // nksplit
-	const SegSeed *seed;      // per segment: its seed indices under the spec of its split
 	int nksplit;
 	const double2 *u_slot;    // [nslot], slot of (segment q, step r) = r * nseg + q
 	int nseg;
@@ -763,7 +762,6 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 	double *sh_g = reinterpret_cast<double *>(smem); // reused after the loop: kForceWarps x 32 x D
 	TabSpec &sp = body_shared().sp;
 	Seg *sh_seg = body_shared().seg;
-	SegSeed *sh_seed = body_shared().seed;
 	int &sh_last = body_shared().last;
 
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -823,7 +821,6 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 		}
 		for (int e = threadIdx.x; e < nq; e += kForceThreads) {
 			sh_seg[e] = a.segs[c0 + e];
-			sh_seed[e] = a.seed[c0 + e];
 		}
 		__syncthreads();
 		if constexpr (!MIXED) {
@@ -850,7 +847,7 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 					z1 = cheb_next(c, z0, q);
 					run++;
 				} else {
-					const SeedIdx &ix = sh_seed[qq];
+					const SeedIdx ix = seed_index<D>(sp, sgm);
 					z0 = seed_from<D, double2>(tab + lane, 32, ix);
 					const double2 w = tab[ix.w * 32 + lane];
 					c = 2.0 * w.x;
@@ -889,7 +886,7 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 				if (sgm.len == 0)   // padding segment of a rho group: weight 0, no table entries
 					continue;
 				const float4 *uu = reinterpret_cast<const float4 *>(sh_u + qq * L);   // slot pairs (2r, 2r + 1)
-				const SeedIdx &ix = sh_seed[qq];
+				const SeedIdx ix = seed_index<D>(sp, sgm);
 				const C z = seed_from<D, C>(tab + lane, 32, ix);
 				const C w = tab[ix.w * 32 + lane];
 				// three-term recurrence along the segment (re-seeded per segment: in FP32 a longer run would carry its

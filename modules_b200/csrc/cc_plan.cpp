@@ -234,35 +234,7 @@ ForceSplits force_splits(const Plan &p, int want)
 		i = j;
 	}
 	f.start.push_back(nseg);
-	f.seed.assign(nseg, SegSeed());
-	for (int k = 0; k < f.count(); k++)
-		for (int q = f.start[k]; q < f.start[k + 1]; q++)
-			if (p.segs[q].len > 0)
-				f.seed[q] = seg_seed(p.d, f.spec[k], p.segs[q]);
 	return f;
-}
-
-SegSeed seg_seed(int d, const TabSpec &sp, const Seg &g)
-{
-	SegSeed x = {};
-	int v[3] = {g.p0, g.p1, 0};
-	v[d - 1] = g.start;
-	for (int e = 0; e < d; e++) {
-		const int m = v[e] - sp.lo[e];
-		if (sp.full[e]) {
-			x.a[e] = sp.offc[e] + m;
-			x.b[e] = -1;
-		} else {
-			x.a[e] = sp.offc[e] + (m >> 3);
-			x.b[e] = sp.offf[e] + (m & 7);
-		}
-	}
-	for (int e = d; e < 3; e++) {
-		x.a[e] = 0;
-		x.b[e] = -1;
-	}
-	x.w = sp.offf[d - 1] + 1;
-	return x;
 }
 
 bool cell_geometry(int d, const double *a, double *volume, double *recip)

@@ -53,20 +53,9 @@ struct Plan {
 };
 
 // A split of the segments for the force pass: segments [start[k], start[k+1]) share the table spec spec[k].
-// Table indices of a segment's seed z_0 = prod_e T_e(index_e) under a table spec: axis e is entry a[e] (full table)
-// or a[e] * b[e] (coarse x fine, b[e] >= 0); w is the entry of the recurrence step exp(2 pi i s_last).
-struct SegSeed {
-	int a[3], b[3];
-	int w, pad;
-};
-
-// The seed indices of segment g under spec sp (d dimensions).
-SegSeed seg_seed(int d, const TabSpec &sp, const Seg &g);
-
 struct ForceSplits {
 	std::vector<int> start;
 	std::vector<TabSpec> spec;
-	std::vector<SegSeed> seed;   // per segment, under the spec of its split (zeros for padding segments)
 	int max_row = 0;
 	int count() const { return (int)spec.size(); }
 };

@@ -89,7 +89,7 @@ int serve_per_split(const cc::Plan &p)
 
 // Offsets of a request's arrays in its one allocation (see open_slot).
 struct SlotOffsets {
-	size_t segs, slotV, bstart, bspec, kstart, kspec, seed, part, rho, u, ep, tk, pg, fc, x, g, d, xt, gt, S, Y, lp, st;
+	size_t segs, slotV, bstart, bspec, kstart, kspec, part, rho, u, ep, tk, pg, fc, x, g, d, xt, gt, S, Y, lp, st;
 };
 
 int fill_slot(const cc_request &r, int idx, int m, const cc::Plan &p, const cc::ForceSplits &fs, double vol,
@@ -123,7 +123,6 @@ int open_slot(const cc_request &r, int idx, int m, int nblk_cap, cudaMemPool_t p
 	const size_t o_segs = c.take(sizeof(cc::Seg) * p.segs.size()), o_slotV = c.take(sizeof(double) * p.nslot),
 	             o_bstart = c.take(sizeof(int) * p.bstart.size()), o_bspec = c.take(sizeof(cc::TabSpec) * p.bspec.size()),
 	             o_kstart = c.take(sizeof(int) * fs.start.size()), o_kspec = c.take(sizeof(cc::TabSpec) * fs.spec.size()),
-	             o_seed = c.take(sizeof(cc::SegSeed) * fs.seed.size()),
 	             o_part = c.take(sizeof(double2) * (size_t)nsplit * p.nslot), o_rho = c.take(sizeof(double2) * p.nslot),
 	             o_u = c.take(sizeof(double2) * p.nslot), o_ep = c.take(sizeof(double) * nchunks),
 	             o_tk = c.take(sizeof(unsigned)), o_pg = c.take(sizeof(double) * (size_t)nks * n),
@@ -142,7 +141,7 @@ int open_slot(const cc_request &r, int idx, int m, int nblk_cap, cudaMemPool_t p
 		}
 	}
 	if (int rc = fill_slot(r, idx, m, p, fs, vol, recip, per_split, nsplit, nchunks, pgroups, nks, st,
-	                       {o_segs, o_slotV, o_bstart, o_bspec, o_kstart, o_kspec, o_seed, o_part, o_rho, o_u, o_ep, o_tk,
+	                       {o_segs, o_slotV, o_bstart, o_bspec, o_kstart, o_kspec, o_part, o_rho, o_u, o_ep, o_tk,
 	                        o_pg, o_fc, o_x, o_g, o_d, o_xt, o_gt, o_S, o_Y, o_lp, o_st},
 	                       s)) {
 		cudaFreeAsync(s.mem, st);
@@ -158,7 +157,7 @@ int fill_slot(const cc_request &r, int idx, int m, const cc::Plan &p, const cc::
               const SlotOffsets &off, Slot &s)
 {
 	const size_t o_segs = off.segs, o_slotV = off.slotV, o_bstart = off.bstart, o_bspec = off.bspec,
-	             o_kstart = off.kstart, o_kspec = off.kspec, o_seed = off.seed, o_part = off.part, o_rho = off.rho, o_u = off.u,
+	             o_kstart = off.kstart, o_kspec = off.kspec, o_part = off.part, o_rho = off.rho, o_u = off.u,
 	             o_ep = off.ep, o_tk = off.tk, o_pg = off.pg, o_fc = off.fc, o_x = off.x, o_g = off.g, o_d = off.d,
 	             o_xt = off.xt, o_gt = off.gt, o_S = off.S, o_Y = off.Y, o_lp = off.lp, o_st = off.st;
 	const int d = r.d;
@@ -172,8 +171,6 @@ int fill_slot(const cc_request &r, int idx, int m, const cc::Plan &p, const cc::
 	                        st));
 	SV_CUDA(cudaMemcpyAsync(b + o_kstart, fs.start.data(), sizeof(int) * fs.start.size(), cudaMemcpyHostToDevice, st));
 	SV_CUDA(cudaMemcpyAsync(b + o_kspec, fs.spec.data(), sizeof(cc::TabSpec) * fs.spec.size(), cudaMemcpyHostToDevice,
-	                        st));
-	SV_CUDA(cudaMemcpyAsync(b + o_seed, fs.seed.data(), sizeof(cc::SegSeed) * fs.seed.size(), cudaMemcpyHostToDevice,
 	                        st));
 	SV_CUDA(cudaMemsetAsync(b + o_tk, 0, sizeof(unsigned), st));
 	SV_CUDA(cudaMemsetAsync(b + o_fc, 0, sizeof(unsigned) * pgroups, st));
@@ -249,7 +246,6 @@ int fill_slot(const cc_request &r, int idx, int m, const cc::Plan &p, const cc::
 	fa.segs = ra.segs;
 	fa.kstart = reinterpret_cast<const int *>(b + o_kstart);
 	fa.kspec = reinterpret_cast<const cc::TabSpec *>(b + o_kspec);
-	fa.seed = reinterpret_cast<const cc::SegSeed *>(b + o_seed);
 	fa.nksplit = nks;
 	fa.u_slot = rr.u_slot;
 	fa.nseg = ra.nseg;
@@ -287,7 +283,7 @@ size_t estimate_bytes(const cc_request &r, int m, int nblk_cap)
 	const double nseg = M / 4 + 64, nslot = nseg * 8;
 	const double n = (double)r.N * r.d;
 	const double nsplit = std::ceil(r.N / (double)kServeMinPerSplit), nks = std::ceil(nseg / cc::kBatchSegsPerSplit) + 2;
-	const double bytes = 48 * nseg + 8 * nslot + 2 * 768 * (nseg / 256 + nks + 2) + 16 * nsplit * nslot + 32 * nslot +
+	const double bytes = 16 * nseg + 8 * nslot + 2 * 768 * (nseg / 256 + nks + 2) + 16 * nsplit * nslot + 32 * nslot +
 	                     8 * nks * n + 8 * n * (5 + 2 * m) + 8.0 * nblk_cap * cc::lb_ndots(m) + 16384;
 	return (size_t)bytes;
 }
