@@ -169,7 +169,8 @@ int batch_build(cc_batch *b, int per_split, int segs_per_split)
 		const BatchBufs &q = b->bufs[i];
 		const int64_t n = b->N[i];
 		const int nsplit = (int)((n + per_split - 1) / per_split);
-		const int nchunks = (p.nslot + 31) / 32, pgroups = (int)((n + 31) / 32);
+		// reduce items of kWideSlots slots each (their energy terms are the force items' eblock entries)
+		const int nchunks = (p.nslot + cc::kWideSlots - 1) / cc::kWideSlots, pgroups = (int)((n + 31) / 32);
 		const DevSplits *f = nullptr;
 		const int want = (int)std::max<int64_t>(1, (p.real_segs + segs_per_split - 1) / segs_per_split);
 		if (int rc = get_splits(h->main, want, &f))

@@ -670,6 +670,72 @@ __device__ __forceinline__ void reduce_body(const ReduceArgs &a, const int chunk
 	}
 }
 
+// Item `item` (kWideSlots slots, one per thread) of the split reduction in the fused batch launch: every slot sums the
+// partial rows in row order, then the block's energy terms are added (lanes by a fixed tree, warps in order) into
+// eblock[item]. Wider than reduce_body's 32-slot chunks so that a batch's many small reductions cost few work items;
+// for up to 8 partial rows the sums equal reduce_body's bitwise (its 8 row chunks then hold one row each).
+constexpr int kWideSlots = 256;
+__device__ __forceinline__ void reduce_body_wide(const ReduceArgs &a, const int item)
+{
+	double2(&sh)[8][32] = body_shared().red;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	cudaGridDependencySynchronize();
+	cudaTriggerProgrammaticLaunchCompletion();
+	if (a.ready)
+		wait_ready(a.ready, a.ready_need, a.err, a.ready_spins);
+	if (eval_skipped(a.skip, a.stage, a.want_stage))
+		return;
+	const int slot = item * kWideSlots + threadIdx.x;
+	double e = 0.0;
+	if (slot < a.nslot) {
+		double2 t = make_double2(0.0, 0.0);
+		int sp = 0;
+		for (; sp + 4 <= a.nsplit; sp += 4) {
+			const double2 v0 = __ldcg(&a.partial[(size_t)sp * a.nslot + slot]);
+			const double2 v1 = __ldcg(&a.partial[(size_t)(sp + 1) * a.nslot + slot]);
+			const double2 v2 = __ldcg(&a.partial[(size_t)(sp + 2) * a.nslot + slot]);
+			const double2 v3 = __ldcg(&a.partial[(size_t)(sp + 3) * a.nslot + slot]);
+			t.x += v0.x;
+			t.y += v0.y;
+			t.x += v1.x;
+			t.y += v1.y;
+			t.x += v2.x;
+			t.y += v2.y;
+			t.x += v3.x;
+			t.y += v3.y;
+		}
+		for (; sp < a.nsplit; sp++) {
+			const double2 v = __ldcg(&a.partial[(size_t)sp * a.nslot + slot]);
+			t.x += v.x;
+			t.y += v.y;
+		}
+		t.x += a.rho_offset;
+		a.rho_slot[slot] = t;
+		double v = a.slotV[slot];
+		const double r2 = t.x * t.x + t.y * t.y;
+		if (a.slotS0) {
+			const double ds = r2 / a.npart - a.slotS0[slot];
+			v *= ds;
+			e = v * ds;
+		} else {
+			e = v * r2;
+		}
+		a.u_slot[slot] = make_double2(v * t.x, -v * t.y);
+	}
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1)
+		e += __shfl_down_sync(0xffffffffu, e, o);
+	if (lane == 0)
+		sh[0][warp].x = e;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double b = 0.0;
+		for (int w = 0; w < kRhoWarps; w++)
+			b += sh[0][w].x;
+		a.eblock[item] = b;
+	}
+}
+
 static __global__ void __launch_bounds__(kRedThreads) cc_reduce_kernel(ReduceArgs a)
 {
 	reduce_body(a, blockIdx.x, gridDim.x);
@@ -1041,7 +1107,7 @@ __device__ __forceinline__ void mbatch_item(const MBatchArgs &A, int phase, int 
 		r.ready_need = (unsigned)(__ldg(A.pre + b + 1) - __ldg(A.pre + b)) + (b == 0 ? A.phantom : 0u);
 		r.ready_spins = A.spins;
 		r.err = err;
-		reduce_body(r, local, __ldg(A.shape + A.B + b));
+		reduce_body_wide(r, local);
 	} else {
 		ForceArgs f = A.force[b];
 		bool mixed = MODE == 1;

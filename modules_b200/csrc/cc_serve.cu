@@ -117,7 +117,8 @@ int open_slot(const cc_request &r, int idx, int m, int nblk_cap, cudaMemPool_t p
 	const int n = (int)(N * d);
 	const int per_split = serve_per_split(p);
 	const int nsplit = (int)((N + per_split - 1) / per_split);
-	const int nchunks = (p.nslot + 31) / 32, pgroups = (int)((N + 31) / 32);
+	// reduce items of kWideSlots slots each in the fused launch (their energy terms are the force items' eblock)
+	const int nchunks = (p.nslot + cc::kWideSlots - 1) / cc::kWideSlots, pgroups = (int)((N + 31) / 32);
 	const int nks = fs.count();
 	Carve c;
 	const size_t o_segs = c.take(sizeof(cc::Seg) * p.segs.size()), o_slotV = c.take(sizeof(double) * p.nslot),
