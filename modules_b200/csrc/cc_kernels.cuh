@@ -102,10 +102,32 @@ __device__ __forceinline__ double2 cheb_next(double c, double2 q, double2 p)
 {
 	return make_double2(fma(c, q.x, -p.x), fma(c, q.y, -p.y));
 }
-// The same in FP32 (the mixed path): a segment of L = 8 slots stays within ~L^2/2 = 32 FP32 ulps of its seed's phase.
-__device__ __forceinline__ float2 cheb_next(float c, float2 q, float2 p)
+
+// acc += a + b (a, b: the same slot of two particles) and acc += a, component by component; the FP32 forms are packed
+// FP32x2 adds with the scalar adds' rounding, so both forms give the same sums.
+__device__ __forceinline__ void acc_add(double2 &acc, double2 a, double2 b)
 {
-	return make_float2(fmaf(c, q.x, -p.x), fmaf(c, q.y, -p.y));
+	acc.x += a.x + b.x;
+	acc.y += a.y + b.y;
+}
+__device__ __forceinline__ void acc_add(float2 &acc, float2 a, float2 b) { acc = __fadd2_rn(acc, __fadd2_rn(a, b)); }
+__device__ __forceinline__ void acc_add(double2 &acc, double2 a)
+{
+	acc.x += a.x;
+	acc.y += a.y;
+}
+__device__ __forceinline__ void acc_add(float2 &acc, float2 a) { acc = __fadd2_rn(acc, a); }
+
+// The FP32 recurrence (the mixed path; a segment of L = 8 slots stays within ~L^2/2 = 32 FP32 ulps of its seed's
+// phase), both components in one packed FP32x2 fused multiply-add (sm_100) rounded as fmaf, and written without a
+// negated addend: y_r = s_r z_r with s_r = -1 for r mod 4 in {2, 3} obeys
+// y_r = -c y_{r-1} + y_{r-2} for even r and y_r = c y_{r-1} + y_{r-2} for odd r. Negation is exact and commutes with
+// round-to-nearest, so y_r is s_r z_r bit for bit (and so are sums of y_r). cpos = (c, c), cneg = (-c, -c).
+__host__ __device__ constexpr bool slot_negated(int r) { return (r & 2) != 0; }
+// (called from fully unrolled loops, where r is a constant and the choice is made at compile time)
+__device__ __forceinline__ float2 seg_next(int r, float2 cpos, float2 cneg, float2 q, float2 p)
+{
+	return __ffma2_rn((r & 1) ? cpos : cneg, q, p);
 }
 
 // exp(2 pi i t): (cos, sin)
@@ -264,17 +286,9 @@ __device__ __forceinline__ bool eval_skipped(const int *skip, const int *stage, 
 	return (skip && *(volatile const int *)skip) || (stage && *(volatile const int *)stage != want_stage);
 }
 
-// Work queue of a persistent multi-instance launch: q[0] the next item, q[1] the blocks that found it empty. The last
-// block to leave resets both, so the next launch starts at item 0. Items are independent and write their own outputs,
-// so the order in which blocks take them does not change any result.
-__device__ __forceinline__ int queue_next(unsigned *q, int *sh_item)
-{
-	__syncthreads();   // the previous item's shared memory is no longer read
-	if (threadIdx.x == 0)
-		*sh_item = (int)atomicAdd(q, 1u);
-	__syncthreads();
-	return *sh_item;
-}
+// Work queue of a persistent multi-instance launch: q[0] the next item (taken with an atomic add), q[1] the blocks
+// that found it empty. The last block to leave resets both, so the next launch starts at item 0. Items write their
+// own outputs, so the order in which blocks take them does not change any result.
 
 __device__ __forceinline__ void queue_leave(unsigned *q)
 {
@@ -340,6 +354,19 @@ __device__ __forceinline__ void wait_ready(const unsigned *ready, unsigned need,
 	__syncthreads();
 }
 
+// The stage test and the bounded wait of one body call. The three-kernel launches pass their arguments' stage words
+// and no wait; the fused batch launch sets them per item, so that its bodies read the instances' descriptors from
+// global memory as they are and keep no modified copy in registers.
+struct ItemCtl {
+	const int *stage;
+	int want_stage;
+	// wait until *ready >= ready_need (the instance's items of the previous phase done) before reading their results;
+	// err is raised when that bounded wait runs out (after ready_spins polls, 0: kReadySpins). Null: no wait.
+	const unsigned *ready = nullptr;
+	unsigned ready_need = 0, ready_spins = 0;
+	unsigned *err = nullptr;
+};
+
 // ---------------------------------------------------------------------------------------------------------------
 // rho pass
 // ---------------------------------------------------------------------------------------------------------------
@@ -370,7 +397,7 @@ constexpr int kRhoThreads = kRhoWarps * 32;
 // Block (bg, split) of the rho pass. CLUSTER: the blocks of a thread-block cluster (consecutive splits) are added
 // through distributed shared memory into partial row split / cluster size; otherwise the block writes row `split`.
 template <int D, int L, bool MIXED, bool CLUSTER>
-__device__ __forceinline__ void rho_body(const RhoArgs &a, const int bg, const int split)
+__device__ __forceinline__ void rho_body(const RhoArgs &a, const int bg, const int split, const ItemCtl ctl)
 {
 	typedef typename std::conditional<MIXED, float2, double2>::type C;
 	constexpr int SUB = 16;
@@ -389,7 +416,7 @@ __device__ __forceinline__ void rho_body(const RhoArgs &a, const int bg, const i
 	const int j0 = min(a.N, split * a.per_split);
 	const int j1 = min(a.N, j0 + a.per_split);
 	cudaGridDependencySynchronize();   // inputs of this step are complete (programmatic dependent launch)
-	if (eval_skipped(a.skip, a.stage, a.want_stage))   // uniform over the instance: no block reaches a cluster barrier
+	if (eval_skipped(a.skip, ctl.stage, ctl.want_stage))   // uniform over the instance: no block reaches a cluster barrier
 		return;
 	if (a.frac_copy && bg == 0)
 		for (int t = threadIdx.x; t < (j1 - j0) * D; t += kRhoThreads)
@@ -431,19 +458,29 @@ __device__ __forceinline__ void rho_body(const RhoArgs &a, const int bg, const i
 			const C *r0 = tab + i * row, *r1 = r0 + row;
 			C z0 = seed_from<D, C>(r0, 1, ix), z1 = seed_from<D, C>(r1, 1, ix);
 			const C w0 = r0[ix.w], w1 = r1[ix.w];
-			{
-				// three-term recurrence along the segment
-				const R c0 = (R)2 * w0.x, c1 = (R)2 * w1.x;
-				C p0 = z0, p1 = z1, q0 = cmul(z0, w0), q1 = cmul(z1, w1);
-				accC[0].x += p0.x + p1.x;
-				accC[0].y += p0.y + p1.y;
-				accC[1].x += q0.x + q1.x;
-				accC[1].y += q0.y + q1.y;
+			// three-term recurrence along the segment
+			const R c0 = (R)2 * w0.x, c1 = (R)2 * w1.x;
+			C p0 = z0, p1 = z1, q0 = cmul(z0, w0), q1 = cmul(z1, w1);
+			acc_add(accC[0], p0, p1);
+			acc_add(accC[1], q0, q1);
+			if constexpr (MIXED) {
+				// sign-free form: accC[r] holds s_r times the slot's sum
+				const float2 c0p = make_float2(c0, c0), c0n = make_float2(-c0, -c0);
+				const float2 c1p = make_float2(c1, c1), c1n = make_float2(-c1, -c1);
+#pragma unroll
+				for (int r = 2; r < L; r++) {
+					const float2 n0 = seg_next(r, c0p, c0n, q0, p0), n1 = seg_next(r, c1p, c1n, q1, p1);
+					acc_add(accC[r], n0, n1);
+					p0 = q0;
+					q0 = n0;
+					p1 = q1;
+					q1 = n1;
+				}
+			} else {
 #pragma unroll
 				for (int r = 2; r < L; r++) {
 					const C n0 = cheb_next(c0, q0, p0), n1 = cheb_next(c1, q1, p1);
-					accC[r].x += n0.x + n1.x;
-					accC[r].y += n0.y + n1.y;
+					acc_add(accC[r], n0, n1);
 					p0 = q0;
 					q0 = n0;
 					p1 = q1;
@@ -454,8 +491,9 @@ __device__ __forceinline__ void rho_body(const RhoArgs &a, const int bg, const i
 				since_flush = 0;
 #pragma unroll
 				for (int r = 0; r < L; r++) {
-					acc[r].x += (double)accC[r].x;
-					acc[r].y += (double)accC[r].y;
+					const double sg = slot_negated(r) ? -1.0 : 1.0;
+					acc[r].x += sg * (double)accC[r].x;
+					acc[r].y += sg * (double)accC[r].y;
 					accC[r].x = 0;
 					accC[r].y = 0;
 				}
@@ -465,18 +503,24 @@ __device__ __forceinline__ void rho_body(const RhoArgs &a, const int bg, const i
 			const C *r0 = tab + i * row;
 			C z0 = seed_from<D, C>(r0, 1, ix);
 			const C w0 = r0[ix.w];
-			{
-				const R c0 = (R)2 * w0.x;
-				C p0 = z0, q0 = cmul(z0, w0);
-				accC[0].x += p0.x;
-				accC[0].y += p0.y;
-				accC[1].x += q0.x;
-				accC[1].y += q0.y;
+			const R c0 = (R)2 * w0.x;
+			C p0 = z0, q0 = cmul(z0, w0);
+			acc_add(accC[0], p0);
+			acc_add(accC[1], q0);
+			if constexpr (MIXED) {
+				const float2 c0p = make_float2(c0, c0), c0n = make_float2(-c0, -c0);
+#pragma unroll
+				for (int r = 2; r < L; r++) {
+					const float2 n0 = seg_next(r, c0p, c0n, q0, p0);
+					acc_add(accC[r], n0);
+					p0 = q0;
+					q0 = n0;
+				}
+			} else {
 #pragma unroll
 				for (int r = 2; r < L; r++) {
 					const C n0 = cheb_next(c0, q0, p0);
-					accC[r].x += n0.x;
-					accC[r].y += n0.y;
+					acc_add(accC[r], n0);
 					p0 = q0;
 					q0 = n0;
 				}
@@ -486,8 +530,9 @@ __device__ __forceinline__ void rho_body(const RhoArgs &a, const int bg, const i
 #pragma unroll
 	for (int r = 0; r < L; r++) {
 		if (MIXED) {
-			acc[r].x += (double)accC[r].x;
-			acc[r].y += (double)accC[r].y;
+			const double sg = slot_negated(r) ? -1.0 : 1.0;
+			acc[r].x += sg * (double)accC[r].x;
+			acc[r].y += sg * (double)accC[r].y;
 		} else {
 			acc[r].x = (double)accC[r].x;
 			acc[r].y = (double)accC[r].y;
@@ -545,7 +590,7 @@ __device__ __forceinline__ void rho_body(const RhoArgs &a, const int bg, const i
 template <int D, int L, bool MIXED>
 __global__ void __launch_bounds__(kRhoThreads, 3) cc_rho_kernel(RhoArgs a)
 {
-	rho_body<D, L, MIXED, true>(a, blockIdx.x, blockIdx.y);
+	rho_body<D, L, MIXED, true>(a, blockIdx.x, blockIdx.y, ItemCtl{a.stage, a.want_stage});
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -569,11 +614,6 @@ struct ReduceArgs {
 	// u = V (|rho|^2 / N - S0) conj(rho); npart = N
 	const double *slotS0;
 	double npart;
-	// fused batch launch: wait until *ready >= ready_need (the instance's rho items done) before reading partials;
-	// err is raised when that bounded wait runs out (after ready_spins polls, 0: kReadySpins). Null outside it.
-	const unsigned *ready;
-	unsigned ready_need, ready_spins;
-	unsigned *err;
 };
 
 constexpr int kRedThreads = 256;   // 32 slots x 8 split chunks
@@ -588,10 +628,6 @@ __device__ __forceinline__ void reduce_body(const ReduceArgs &a, const int chunk
 	const int per = (a.nsplit + 7) >> 3;
 	cudaGridDependencySynchronize();
 	cudaTriggerProgrammaticLaunchCompletion();
-	// In the fused batch launch the wait comes first, also for a skipped instance: its last force item resets the
-	// instance's counts, which must not happen while one of its rho or reduce items is still to be counted.
-	if (a.ready)
-		wait_ready(a.ready, a.ready_need, a.err, a.ready_spins);
 	if (eval_skipped(a.skip, a.stage, a.want_stage))
 		return;
 	const int s0 = min(a.nsplit, c * per), s1 = min(a.nsplit, s0 + per);
@@ -675,15 +711,17 @@ __device__ __forceinline__ void reduce_body(const ReduceArgs &a, const int chunk
 // eblock[item]. Wider than reduce_body's 32-slot chunks so that a batch's many small reductions cost few work items;
 // for up to 8 partial rows the sums equal reduce_body's bitwise (its 8 row chunks then hold one row each).
 constexpr int kWideSlots = 256;
-__device__ __forceinline__ void reduce_body_wide(const ReduceArgs &a, const int item)
+__device__ __forceinline__ void reduce_body_wide(const ReduceArgs &a, const int item, const ItemCtl ctl)
 {
 	double2(&sh)[8][32] = body_shared().red;
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	cudaGridDependencySynchronize();
 	cudaTriggerProgrammaticLaunchCompletion();
-	if (a.ready)
-		wait_ready(a.ready, a.ready_need, a.err, a.ready_spins);
-	if (eval_skipped(a.skip, a.stage, a.want_stage))
+	// The wait comes first, also for a skipped instance: its last force item resets the instance's counts, which must
+	// not happen while one of its rho or reduce items is still to be counted.
+	if (ctl.ready)
+		wait_ready(ctl.ready, ctl.ready_need, ctl.err, ctl.ready_spins);
+	if (eval_skipped(a.skip, ctl.stage, ctl.want_stage))
 		return;
 	const int slot = item * kWideSlots + threadIdx.x;
 	double e = 0.0;
@@ -786,11 +824,6 @@ struct ForceArgs {
 	const int *skip;
 	const int *stage;
 	int want_stage;
-	// fused batch launch: wait until *ready >= ready_need (the instance's reduce items done) before reading u; err is
-	// raised when that bounded wait runs out (after ready_spins polls, 0: kReadySpins). Null outside that launch.
-	const unsigned *ready;
-	unsigned ready_need, ready_spins;
-	unsigned *err;
 };
 
 constexpr int kForceWarps = 8;
@@ -818,7 +851,7 @@ template <typename C> __host__ __device__ constexpr size_t force_smem_bytes(int 
 // weights u of up to kForceUChunk segments at a time are staged in shared memory in the compute type (slot-major, so a
 // warp's read of one weight is a broadcast).
 template <int D, int L, bool MIXED>
-__device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup, const int ks)
+__device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup, const int ks, const ItemCtl ctl)
 {
 	typedef typename std::conditional<MIXED, float, double>::type R;
 	typedef typename std::conditional<MIXED, float2, double2>::type C;
@@ -839,9 +872,9 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 	// completion this block's launch implies), like the positions: a finished instance builds no tables. In the fused
 	// batch launch its force items still wait for its reduce items (which waited for its rho items), so that the last
 	// of them resets the instance's counts only once every item of the instance has been counted.
-	if (eval_skipped(a.skip, a.stage, a.want_stage)) {
-		if (a.ready)
-			wait_ready(a.ready, a.ready_need, a.err, a.ready_spins);
+	if (eval_skipped(a.skip, ctl.stage, ctl.want_stage)) {
+		if (ctl.ready)
+			wait_ready(ctl.ready, ctl.ready_need, ctl.err, ctl.ready_spins);
 		return;
 	}
 	// the spec and the block's coordinates are loaded together (neither waits for the other)
@@ -855,9 +888,9 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 	// while the reduce kernel still runs (programmatic dependent launch), before waiting for u.
 	build_tables<D, C>(sp, pos, 0, 32, nvalid, tab, 1, 32, threadIdx.x, kForceThreads);
 	cudaGridDependencySynchronize();   // u of this step is complete
-	if (a.ready)
-		wait_ready(a.ready, a.ready_need, a.err, a.ready_spins);
-	if (eval_skipped(a.skip, a.stage, a.want_stage))   // uniform over the instance
+	if (ctl.ready)
+		wait_ready(ctl.ready, ctl.ready_need, ctl.err, ctl.ready_spins);
+	if (eval_skipped(a.skip, ctl.stage, ctl.want_stage))   // uniform over the instance
 		return;
 	if (a.E_out && pgroup == 0 && ks == 0 && warp == 0) {
 		// the energy, summed in the order of the reduce kernel's last block
@@ -880,10 +913,17 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 		__syncthreads();   // tables complete (first chunk); the previous chunk's weights are no longer read
 		// FP64: slot-major (a warp's read of one weight is a broadcast); mixed: segment-major, a segment's 8 FP32
 		// weights contiguous (read as four 16-byte broadcasts)
+		// weights, mixed: (s_r u.y, s_r u.x) in FP32 for the sign-free recurrence's y_r = s_r z_r, so that the packed
+		// product with y_r is (u.y z.x, u.x z.y), whose sum is Im(u z)
 		for (int e = threadIdx.x; e < nq * L; e += kForceThreads) {
 			const int r = e / nq, qq = e - r * nq;
-			sh_u[MIXED ? qq * L + r : r * kForceUChunk + qq] =
-			    to_c<C>(__ldcg(a.u_slot + (size_t)r * a.nseg + c0 + qq));
+			const double2 u = __ldcg(a.u_slot + (size_t)r * a.nseg + c0 + qq);
+			if constexpr (MIXED) {
+				const float sg = slot_negated(r) ? -1.0f : 1.0f;
+				sh_u[qq * L + r] = make_float2(sg * (float)u.y, sg * (float)u.x);
+			} else {
+				sh_u[r * kForceUChunk + qq] = u;
+			}
 		}
 		for (int e = threadIdx.x; e < nq; e += kForceThreads) {
 			sh_seg[e] = a.segs[c0 + e];
@@ -955,31 +995,31 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 				const SeedIdx ix = seed_index<D>(sp, sgm);
 				const C z = seed_from<D, C>(tab + lane, 32, ix);
 				const C w = tab[ix.w * 32 + lane];
-				// three-term recurrence along the segment (re-seeded per segment: in FP32 a longer run would carry its
-				// error along)
-				const R c = (R)2 * w.x;
-				C p = z, q = cmul(z, w);
+				// sign-free three-term recurrence along the segment (re-seeded per segment: in FP32 a longer run would
+				// carry its error along), in packed FP32x2: A = sum_r P_r and B = sum_r r P_r of the products
+				// P_r = (s_r u_r) * y_r, whose two components add up to Im(u_r z_r)
+				const float c = 2.0f * w.x;
+				const float2 cp = make_float2(c, c), cn = make_float2(-c, -c);
+				float2 p = z, q = cmul(z, w);
 				const float4 u01 = uu[0];
-				R S0 = u01.x * p.y + u01.y * p.x, S1;
-				{
-					const R t = u01.z * q.y + u01.w * q.x;
-					S0 += t;
-					S1 = t;
-				}
+				float2 A = __fmul2_rn(make_float2(u01.x, u01.y), p);
+				float2 B = __fmul2_rn(make_float2(u01.z, u01.w), q);
+				A = __fadd2_rn(A, B);
 #pragma unroll
 				for (int r = 2; r < L; r += 2) {
 					const float4 uv = uu[r / 2];
-					const C n = cheb_next(c, q, p);
-					const R t = uv.x * n.y + uv.y * n.x;
-					S0 += t;
-					S1 = fma((R)r, t, S1);
-					const C n2 = cheb_next(c, n, q);
-					const R t2 = uv.z * n2.y + uv.w * n2.x;
-					S0 += t2;
-					S1 = fma((R)(r + 1), t2, S1);
+					const float2 n = seg_next(r, cp, cn, q, p);
+					const float2 P = __fmul2_rn(make_float2(uv.x, uv.y), n);
+					A = __fadd2_rn(A, P);
+					B = __ffma2_rn(make_float2((float)r, (float)r), P, B);
+					const float2 n2 = seg_next(r + 1, cp, cn, n, q);
+					const float2 P2 = __fmul2_rn(make_float2(uv.z, uv.w), n2);
+					A = __fadd2_rn(A, P2);
+					B = __ffma2_rn(make_float2((float)(r + 1), (float)(r + 1)), P2, B);
 					p = n;
 					q = n2;
 				}
+				const R S0 = A.x + A.y, S1 = B.x + B.y;
 				const double S0d = (double)S0;
 				if (D >= 2)
 					g[0] = fma(S0d, (double)sgm.p0, g[0]);
@@ -1040,9 +1080,9 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 }
 
 template <int D, int L, bool MIXED>
-__global__ void __launch_bounds__(kForceThreads, 3) cc_force_kernel(ForceArgs a)
+__global__ void __launch_bounds__(kForceThreads, MIXED ? 4 : 3) cc_force_kernel(ForceArgs a)
 {
-	force_body<D, L, MIXED>(a, blockIdx.x, blockIdx.y);
+	force_body<D, L, MIXED>(a, blockIdx.x, blockIdx.y, ItemCtl{a.stage, a.want_stage});
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -1077,98 +1117,99 @@ constexpr int kMBatchThreads = 256;
 template <int D, int MODE>
 __device__ __forceinline__ void mbatch_item(const MBatchArgs &A, int phase, int b, int local)
 {
-	// MODE 0: FP64, 1: mixed, 2: each instance at the precision of its stage word (mixed while it is 0)
-	unsigned *err = A.count + 3 * A.B;
+	// MODE 0: FP64, 1: mixed, 2: each instance at the precision of its stage word (mixed while it is 0). The
+	// instance's descriptors are read in place (global memory); the stage test and the waits come from `ctl`.
+	ItemCtl ctl;
+	ctl.err = A.count + 3 * A.B;
+	ctl.ready_spins = A.spins;
+	ctl.want_stage = A.want_stage;
 	if (phase == 0) {
-		RhoArgs r = A.rho[b];
-		bool mixed = MODE == 1;
-		if (MODE == 2) {
-			mixed = r.stage && *(volatile const int *)r.stage == 0;
-			r.stage = nullptr;
-		} else {
-			r.want_stage = A.want_stage;
-		}
+		const RhoArgs &r = A.rho[b];
+		const int *stage = r.stage;
+		const bool mixed = MODE == 1 || (MODE == 2 && stage && *(volatile const int *)stage == 0);
+		ctl.stage = MODE == 2 ? nullptr : stage;
 		const int ng = __ldg(A.shape + b);
 		if constexpr (MODE != 0) {
 			if (mixed) {
-				rho_body<D, 8, true, false>(r, local % ng, local / ng);
+				rho_body<D, 8, true, false>(r, local % ng, local / ng, ctl);
 				return;
 			}
 		}
 		if constexpr (MODE != 1)
-			rho_body<D, 8, false, false>(r, local % ng, local / ng);
+			rho_body<D, 8, false, false>(r, local % ng, local / ng, ctl);
 	} else if (phase == 1) {
-		ReduceArgs r = A.red[b];
-		if (MODE == 2)
-			r.stage = nullptr;
-		else
-			r.want_stage = A.want_stage;
-		r.ready = A.count + b;
-		r.ready_need = (unsigned)(__ldg(A.pre + b + 1) - __ldg(A.pre + b)) + (b == 0 ? A.phantom : 0u);
-		r.ready_spins = A.spins;
-		r.err = err;
-		reduce_body_wide(r, local);
+		const ReduceArgs &r = A.red[b];
+		ctl.stage = MODE == 2 ? nullptr : r.stage;
+		ctl.ready = A.count + b;
+		ctl.ready_need = (unsigned)(__ldg(A.pre + b + 1) - __ldg(A.pre + b)) + (b == 0 ? A.phantom : 0u);
+		reduce_body_wide(r, local, ctl);
 	} else {
-		ForceArgs f = A.force[b];
-		bool mixed = MODE == 1;
-		if (MODE == 2) {
-			mixed = f.stage && *(volatile const int *)f.stage == 0;
-			f.stage = nullptr;
-		} else {
-			f.want_stage = A.want_stage;
-		}
-		f.ready = A.count + A.B + b;
-		f.ready_need = (unsigned)(__ldg(A.pre + (A.B + 1) + b + 1) - __ldg(A.pre + (A.B + 1) + b));
-		f.ready_spins = A.spins;
-		f.err = err;
+		const ForceArgs &f = A.force[b];
+		const int *stage = f.stage;
+		const bool mixed = MODE == 1 || (MODE == 2 && stage && *(volatile const int *)stage == 0);
+		ctl.stage = MODE == 2 ? nullptr : stage;
+		ctl.ready = A.count + A.B + b;
+		ctl.ready_need = (unsigned)(__ldg(A.pre + (A.B + 1) + b + 1) - __ldg(A.pre + (A.B + 1) + b));
 		const int pg = __ldg(A.shape + 2 * A.B + b);
 		if constexpr (MODE != 0) {
 			if (mixed) {
-				force_body<D, 8, true>(f, local % pg, local / pg);
+				force_body<D, 8, true>(f, local % pg, local / pg, ctl);
 				return;
 			}
 		}
 		if constexpr (MODE != 1)
-			force_body<D, 8, false>(f, local % pg, local / pg);
+			force_body<D, 8, false>(f, local % pg, local / pg, ctl);
 	}
+}
+
+// Queue position -> (phase, instance, item within the instance's phase): rho items first; then, instance by instance,
+// its reduce items followed by its force items.
+__device__ __forceinline__ int4 mbatch_decode(const MBatchArgs &A, int item)
+{
+	const int T0 = A.total[0];
+	if (item < T0) {
+		const int b = find_instance(A.pre, A.B, item);
+		return make_int4(item, 0, b, item - __ldg(A.pre + b));
+	}
+	const int *prf = A.pre + 3 * (A.B + 1);
+	const int li = item - T0;
+	const int b = find_instance(prf, A.B, li);
+	const int within = li - __ldg(prf + b);
+	const int nred = __ldg(A.pre + (A.B + 1) + b + 1) - __ldg(A.pre + (A.B + 1) + b);
+	return within < nred ? make_int4(item, 1, b, within) : make_int4(item, 2, b, within - nred);
 }
 
 template <int MODE>
 __global__ void __launch_bounds__(kMBatchThreads, 3) cc_mbatch_kernel(MBatchArgs A)
 {
-	__shared__ int sh_item;
-	const int T0 = A.total[0], T = T0 + A.total[1] + A.total[2];
+	__shared__ int4 sh_item;   // the current item: (queue position, phase, instance, item within the phase)
+	const int T = A.total[0] + A.total[1] + A.total[2];
 	// Under programmatic dependent launch this grid may be scheduled while the previous one still takes items from
 	// the same queue (its blocks trigger after their first item): wait for it to complete before taking any.
 	cudaGridDependencySynchronize();
-	for (int item; (item = queue_next(A.queue, &sh_item)) < T;) {
-		// rho items first; then, instance by instance, its reduce items followed by its force items
-		int phase, b, local;
-		if (item < T0) {
-			phase = 0;
-			b = find_instance(A.pre, A.B, item);
-			local = item - __ldg(A.pre + b);
-		} else {
-			const int *prf = A.pre + 3 * (A.B + 1);
-			const int li = item - T0;
-			b = find_instance(prf, A.B, li);
-			const int within = li - __ldg(prf + b);
-			const int nred = __ldg(A.pre + (A.B + 1) + b + 1) - __ldg(A.pre + (A.B + 1) + b);
-			phase = within < nred ? 1 : 2;
-			local = within < nred ? within : within - nred;
+	for (;;) {
+		__syncthreads();   // the previous item's shared memory is no longer read
+		if (threadIdx.x == 0) {
+			const int item = (int)atomicAdd(A.queue, 1u);
+			sh_item = item < T ? mbatch_decode(A, item) : make_int4(item, 0, 0, 0);
 		}
-		const int *pre = A.pre + phase * (A.B + 1);
-		const int d = __ldg(A.dim + b);
+		__syncthreads();
+		const int4 it = sh_item;
+		if (it.x >= T)
+			break;
+		const int d = __ldg(A.dim + it.z);
 		if (d == 3)
-			mbatch_item<3, MODE>(A, phase, b, local);
+			mbatch_item<3, MODE>(A, it.y, it.z, it.w);
 		else if (d == 2)
-			mbatch_item<2, MODE>(A, phase, b, local);
+			mbatch_item<2, MODE>(A, it.y, it.z, it.w);
 		else
-			mbatch_item<1, MODE>(A, phase, b, local);
+			mbatch_item<1, MODE>(A, it.y, it.z, it.w);
 		// the item's results are visible before its count rises
 		__threadfence();
 		__syncthreads();
 		if (threadIdx.x == 0) {
+			const int phase = it.y, b = it.z;
+			const int *pre = A.pre + phase * (A.B + 1);
 			unsigned *cnt = A.count + phase * A.B + b;
 			const unsigned done = atomicAdd(cnt, 1u) + 1u;
 			if (phase == 2 && done == (unsigned)(__ldg(pre + b + 1) - __ldg(pre + b))) {
