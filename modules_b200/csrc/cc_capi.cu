@@ -173,6 +173,9 @@ Launch choose_launch(const cc::Plan &p, int64_t N, bool mixed)
 		}
 	}
 	l.per_split = (int)std::max<int64_t>(1, (N + l.nsplit - 1) / l.nsplit);
+	// no cluster of splits left without particles (N = 2000 over 192 splits of 11 fills only 182: 184 splits, one
+	// cluster wave fewer to place)
+	l.nsplit = (int)std::min<int64_t>(l.nsplit, ((N + l.per_split - 1) / l.per_split + l.csize - 1) / l.csize * l.csize);
 	// force: segment splits of every group of 32 particles, chosen the same way
 	const int64_t pg = std::max<int64_t>(1, (N + 31) / 32);
 	// (the tables of a split usually stay within 64 entries per particle)
