@@ -987,6 +987,12 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 				prev = sgm;
 			}
 		} else {
+			// the chunk's (at most kForceUChunk / kForceWarps) segment terms of each gradient component are added in
+			// FP32 and leave FP32 once per chunk
+			float gf[D];
+#pragma unroll
+			for (int e = 0; e < D; e++)
+				gf[e] = 0.0f;
 			for (int qq = warp; qq < nq; qq += kForceWarps) {
 				const Seg sgm = sh_seg[qq];
 				if (sgm.len == 0)   // padding segment of a rho group: weight 0, no table entries
@@ -1019,14 +1025,16 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 					p = n;
 					q = n2;
 				}
-				const R S0 = A.x + A.y, S1 = B.x + B.y;
-				const double S0d = (double)S0;
+				const float S0 = A.x + A.y, S1 = B.x + B.y;
 				if (D >= 2)
-					g[0] = fma(S0d, (double)sgm.p0, g[0]);
+					gf[0] = fmaf(S0, (float)sgm.p0, gf[0]);
 				if (D >= 3)
-					g[1] = fma(S0d, (double)sgm.p1, g[1]);
-				g[D - 1] = fma(S0d, (double)sgm.start, g[D - 1] + (double)S1);
+					gf[1] = fmaf(S0, (float)sgm.p1, gf[1]);
+				gf[D - 1] = fmaf(S0, (float)sgm.start, gf[D - 1] + S1);
 			}
+#pragma unroll
+			for (int e = 0; e < D; e++)
+				g[e] += (double)gf[e];
 		}
 	}
 
