@@ -836,6 +836,10 @@ __device__ __forceinline__ void write_force(const ForceArgs &a, int j, const dou
 }
 
 constexpr int kForceRun = 4;        // FP64 force pass: segments of a lattice line on one recurrence before a new seed
+// The same in the mixed path (FP32 recurrences). Measured at 2D N=1e5 chi=0.2 against the reference's FP64 forces:
+// runs of 1 / 2 / 4 segments give 1.0e-6 / 1.8e-6 / 7.9e-6 of max |F| (the energy is unchanged, 7e-9 relative) and a
+// 3.59 / 3.56 / 3.42 ms evaluation.
+constexpr int kForceRunMixed = 4;
 
 // Dynamic shared memory of the force kernel for tables of `row` entries: the staged weights, then the tables; the
 // per-warp sums reuse it after the loop.
@@ -993,20 +997,43 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 #pragma unroll
 			for (int e = 0; e < D; e++)
 				gf[e] = 0.0f;
-			for (int qq = warp; qq < nq; qq += kForceWarps) {
+			// as in FP64, warp w takes a contiguous run of the chunk's segments, and a segment that continues the
+			// previous one on its lattice line continues the (sign-free) recurrence, here for up to kForceRunMixed
+			// segments in a row; the sign pattern s_r and the coefficients' signs have period 4, which divides L, so
+			// the continuation's slots 0 and 1 are steps L and L + 1 of the same recurrence
+			const int per = (nq + kForceWarps - 1) / kForceWarps;
+			const int qa = min(nq, warp * per), qb = min(nq, qa + per);
+			float2 p = make_float2(0.0f, 0.0f), q = p, cp = p, cn = p;
+			int run = 0;
+			Seg prev = {0, 0, 0, 0};
+			for (int qq = qa; qq < qb; qq++) {
 				const Seg sgm = sh_seg[qq];
-				if (sgm.len == 0)   // padding segment of a rho group: weight 0, no table entries
+				if (sgm.len == 0) {   // padding segment of a rho group: weight 0, no table entries
+					run = 0;
 					continue;
+				}
 				const float4 *uu = reinterpret_cast<const float4 *>(sh_u + qq * L);   // slot pairs (2r, 2r + 1)
-				const SeedIdx ix = seed_index<D>(sp, sgm);
-				const C z = seed_from<D, C>(tab + lane, 32, ix);
-				const C w = tab[ix.w * 32 + lane];
-				// sign-free three-term recurrence along the segment (re-seeded per segment: in FP32 a longer run would
-				// carry its error along), in packed FP32x2: A = sum_r P_r and B = sum_r r P_r of the products
-				// P_r = (s_r u_r) * y_r, whose two components add up to Im(u_r z_r)
-				const float c = 2.0f * w.x;
-				const float2 cp = make_float2(c, c), cn = make_float2(-c, -c);
-				float2 p = z, q = cmul(z, w);
+				// packed FP32x2: A = sum_r P_r and B = sum_r r P_r of the products P_r = (s_r u_r) * y_r, whose two
+				// components add up to Im(u_r z_r)
+				float2 y0, y1;
+				if (run > 0 && run < kForceRunMixed && prev.len == L && sgm.p0 == prev.p0 && sgm.p1 == prev.p1 &&
+				    sgm.start == prev.start + L) {
+					y0 = seg_next(L, cp, cn, q, p);
+					y1 = seg_next(L + 1, cp, cn, y0, q);
+					run++;
+				} else {
+					const SeedIdx ix = seed_index<D>(sp, sgm);
+					const C z = seed_from<D, C>(tab + lane, 32, ix);
+					const C w = tab[ix.w * 32 + lane];
+					const float c = 2.0f * w.x;
+					cp = make_float2(c, c);
+					cn = make_float2(-c, -c);
+					y0 = z;
+					y1 = cmul(z, w);
+					run = 1;
+				}
+				p = y0;
+				q = y1;
 				const float4 u01 = uu[0];
 				float2 A = __fmul2_rn(make_float2(u01.x, u01.y), p);
 				float2 B = __fmul2_rn(make_float2(u01.z, u01.w), q);
@@ -1031,6 +1058,7 @@ __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup,
 				if (D >= 3)
 					gf[1] = fmaf(S0, (float)sgm.p1, gf[1]);
 				gf[D - 1] = fmaf(S0, (float)sgm.start, gf[D - 1] + S1);
+				prev = sgm;
 			}
 #pragma unroll
 			for (int e = 0; e < D; e++)
@@ -1122,17 +1150,42 @@ struct MBatchArgs {
 
 constexpr int kMBatchThreads = 256;
 
+// The fused batch kernel's current descriptor, copied into shared memory by the whole block at once (one round trip
+// to L2 for all its fields, instead of one per field as a body reads them, or a register copy that spills). One
+// variable of a non-template function, so the kernel holds one per block.
+union ItemDesc {
+	RhoArgs rho;
+	ReduceArgs red;
+	ForceArgs force;
+};
+__device__ __forceinline__ ItemDesc &item_desc()
+{
+	__shared__ ItemDesc s;
+	return s;
+}
+// (the previous item's body no longer reads the copy: every item ends at a block barrier)
+template <typename T> __device__ __forceinline__ const T &stage_desc(const T *src, T &dst)
+{
+	static_assert(sizeof(T) % 8 == 0 && alignof(T) >= 8, "descriptors are copied as 8-byte words");
+	const unsigned long long *s = reinterpret_cast<const unsigned long long *>(src);
+	unsigned long long *d = reinterpret_cast<unsigned long long *>(&dst);
+	for (int t = threadIdx.x; t < (int)(sizeof(T) / 8); t += blockDim.x)
+		d[t] = __ldg(s + t);
+	__syncthreads();
+	return dst;
+}
+
 template <int D, int MODE>
 __device__ __forceinline__ void mbatch_item(const MBatchArgs &A, int phase, int b, int local)
 {
 	// MODE 0: FP64, 1: mixed, 2: each instance at the precision of its stage word (mixed while it is 0). The
-	// instance's descriptors are read in place (global memory); the stage test and the waits come from `ctl`.
+	// instance's descriptor is read from its copy in shared memory; the stage test and the waits come from `ctl`.
 	ItemCtl ctl;
 	ctl.err = A.count + 3 * A.B;
 	ctl.ready_spins = A.spins;
 	ctl.want_stage = A.want_stage;
 	if (phase == 0) {
-		const RhoArgs &r = A.rho[b];
+		const RhoArgs &r = stage_desc(A.rho + b, item_desc().rho);
 		const int *stage = r.stage;
 		const bool mixed = MODE == 1 || (MODE == 2 && stage && *(volatile const int *)stage == 0);
 		ctl.stage = MODE == 2 ? nullptr : stage;
@@ -1146,13 +1199,13 @@ __device__ __forceinline__ void mbatch_item(const MBatchArgs &A, int phase, int 
 		if constexpr (MODE != 1)
 			rho_body<D, 8, false, false>(r, local % ng, local / ng, ctl);
 	} else if (phase == 1) {
-		const ReduceArgs &r = A.red[b];
+		const ReduceArgs &r = stage_desc(A.red + b, item_desc().red);
 		ctl.stage = MODE == 2 ? nullptr : r.stage;
 		ctl.ready = A.count + b;
 		ctl.ready_need = (unsigned)(__ldg(A.pre + b + 1) - __ldg(A.pre + b)) + (b == 0 ? A.phantom : 0u);
 		reduce_body_wide(r, local, ctl);
 	} else {
-		const ForceArgs &f = A.force[b];
+		const ForceArgs &f = stage_desc(A.force + b, item_desc().force);
 		const int *stage = f.stage;
 		const bool mixed = MODE == 1 || (MODE == 2 && stage && *(volatile const int *)stage == 0);
 		ctl.stage = MODE == 2 ? nullptr : stage;
