@@ -127,16 +127,22 @@ static __global__ void __launch_bounds__(kLbThreads) lb_dots_kernel(const LbInst
 			ssn[threadIdx.x] = sj;
 		}
 		__syncthreads();
-		for (int i = warp; i < count; i += kWarps) {
+		// two history pairs per step (i and i + kWarps): both pairs' loads are in flight together
+		for (int i = warp; i < count; i += 2 * kWarps) {
+			const int i2 = i + kWarps;
+			const bool two = i2 < count;
 			const double *s = in.S + (size_t)i * in.n + c0, *y = in.Y + (size_t)i * in.n + c0;
-			double si[kLbThreads / 32], yi[kLbThreads / 32];
+			const double *s2 = in.S + (size_t)(two ? i2 : i) * in.n + c0, *y2 = in.Y + (size_t)(two ? i2 : i) * in.n + c0;
+			double si[kLbThreads / 32], yi[kLbThreads / 32], si2[kLbThreads / 32], yi2[kLbThreads / 32];
 #pragma unroll
 			for (int e = 0; e < kLbThreads / 32; e++) {
 				const int k = lane + 32 * e;
 				si[e] = k < cn ? s[k] : 0.0;
 				yi[e] = k < cn ? y[k] : 0.0;
+				si2[e] = k < cn && two ? s2[k] : 0.0;
+				yi2[e] = k < cn && two ? y2[k] : 0.0;
 			}
-			double b[5] = {0, 0, 0, 0, 0};
+			double b[5] = {0, 0, 0, 0, 0}, b2[5] = {0, 0, 0, 0, 0};
 #pragma unroll
 			for (int e = 0; e < kLbThreads / 32; e++) {
 				const int k = lane + 32 * e;
@@ -146,15 +152,26 @@ static __global__ void __launch_bounds__(kLbThreads) lb_dots_kernel(const LbInst
 					b[2] += si[e] * syn[k];
 					b[3] += yi[e] * syn[k];
 					b[4] += yi[e] * ssn[k];
+					b2[0] += si2[e] * sgt[k];
+					b2[1] += yi2[e] * sgt[k];
+					b2[2] += si2[e] * syn[k];
+					b2[3] += yi2[e] * syn[k];
+					b2[4] += yi2[e] * ssn[k];
 				}
 			}
 #pragma unroll
 			for (int k = 0; k < 5; k++)
-				for (int o = 16; o > 0; o >>= 1)
+				for (int o = 16; o > 0; o >>= 1) {
 					b[k] += __shfl_down_sync(0xffffffffu, b[k], o);
-			if (lane == 0)
+					b2[k] += __shfl_down_sync(0xffffffffu, b2[k], o);
+				}
+			if (lane == 0) {
 				for (int k = 0; k < 5; k++)
 					pr[5 * i + k] += b[k];
+				if (two)
+					for (int k = 0; k < 5; k++)
+						pr[5 * i2 + k] += b2[k];
+			}
 		}
 	}
 #pragma unroll
@@ -192,9 +209,14 @@ __device__ __forceinline__ double lb_warp_sum(double v)
 
 constexpr int kLbSolveThreads = 256;
 
+// Dynamic shared memory of lb_solve_kernel: R (chronological) and the ring copies of S^T Y and Y^T Y.
+constexpr size_t kLbSolveSmem = 3 * sizeof(double) * kLbMaxHist * kLbMaxHist;
+
 // One block per instance: block totals of the dot products (parallel over the products, blocks summed in order),
 // accept / reject and the step length (thread 0), history matrices (parallel over slots), the triangular solves of
-// the compact form (warp 0, lanes split every inner sum), g.d of the new direction and the stop tests.
+// the compact form (warp 0, lanes split every inner sum), g.d of the new direction and the stop tests. The kernel is
+// a chain of dependent steps, so its global reads are issued together up front: the partial sums, the state's
+// scalars (thread 0) and the history matrices, which the block keeps in shared memory and updates there as well.
 static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const LbInst *insts, int cap)
 {
 	cudaGridDependencySynchronize();
@@ -203,28 +225,72 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 	if (st->status != kLbRunning)
 		return;
 	const int nblk = lb_blocks(in.n, cap);
+	extern __shared__ double lb_smem[];
+	double *sR = lb_smem;                              // R[a][b] = s_a . y_b (chronological, a <= b), k x k
+	double *shSY = sR + kLbMaxHist * kLbMaxHist;        // S^T Y by ring slots, m x m
+	double *shYY = shSY + kLbMaxHist * kLbMaxHist;      // Y^T Y by ring slots, m x m
 	__shared__ double tot[5 * kLbMaxHist + 6];
 	__shared__ double Sg[kLbMaxHist], Yg[kLbMaxHist], t[kLbMaxHist], q[kLbMaxHist], w1[kLbMaxHist];
-	__shared__ double sR[kLbMaxHist * kLbMaxHist];
 	__shared__ double rdiag[kLbMaxHist];
-	__shared__ int sh_accept, sh_newslot;
+	__shared__ int sh_accept, sh_newslot, sh_k, sh_head;
+	__shared__ double sh_gamma;
 	const int m = st->m, nd = lb_ndots(m);
+	const int count = st->count;
+	// thread 0's scalars of the state (in flight while the partial sums load)
+	double alpha = 0.0, E = 0.0, Et = 0.0, gd = 0.0, stopval = 0.0, gtol = 0.0, ftol = 0.0, switch_E = 0.0;
+	double gamma0 = 1.0;
+	int64_t evals = 0, max_evals = 0, iters = 0;
+	int head = 0, rejects = 0, small = 0, restarts = 0, stage = 0, sched = 0;
+	if (threadIdx.x == 0) {
+		alpha = st->alpha;
+		E = st->E;
+		Et = st->Et;
+		gd = st->gd;
+		stopval = st->stopval;
+		gtol = st->gtol;
+		ftol = st->ftol;
+		switch_E = st->switch_E;
+		gamma0 = st->gamma;
+		evals = st->evals;
+		max_evals = st->max_evals;
+		iters = st->iters;
+		head = st->head;
+		rejects = st->rejects;
+		small = st->small_steps;
+		restarts = st->restarts;
+		stage = st->stage;
+		sched = st->sched;
+	}
+	for (int e = threadIdx.x; e < m * m; e += kLbSolveThreads) {
+		shSY[e] = st->SY[e];
+		shYY[e] = st->YY[e];
+	}
+	// totals: the blocks' partials in block order, up to 16 blocks' loads in flight
 	for (int k = threadIdx.x; k < nd; k += kLbSolveThreads) {
+		const bool is_max = k == nd - 1;
 		double v = in.part[k];
-		for (int b = 1; b < nblk; b++)
-			v = (k == nd - 1) ? fmax(v, in.part[(size_t)b * nd + k]) : v + in.part[(size_t)b * nd + k];
+		for (int b0 = 1; b0 < nblk; b0 += 16) {
+			double pv[16];
+#pragma unroll
+			for (int u = 0; u < 16; u++)
+				pv[u] = b0 + u < nblk ? in.part[(size_t)(b0 + u) * nd + k] : 0.0;
+#pragma unroll
+			for (int u = 0; u < 16; u++)
+				if (b0 + u < nblk)
+					v = is_max ? fmax(v, pv[u]) : v + pv[u];
+		}
 		tot[k] = v;
 	}
 	__syncthreads();
 	const double gtd = tot[5 * m], gtgt = tot[5 * m + 1], sy = tot[5 * m + 2], yy = tot[5 * m + 3],
 	             ygt = tot[5 * m + 4], gtmax = tot[5 * m + 5];
-	const int count = st->count;
 	if (threadIdx.x == 0) {
-		st->evals++;
-		const double alpha = st->alpha, E = st->E, Et = st->Et, gd = st->gd;
+		evals++;
+		int status = kLbRunning;
 		const bool finite = isfinite(Et) && isfinite(gtgt);
 		const bool armijo = finite && Et <= E + 1e-4 * alpha * gd;
-		sh_accept = armijo;
+		int acc = armijo;
+		int k_new = count, head_new = head;
 		if (!armijo) {
 			// backtrack: safeguarded quadratic model of the energy along d
 			double a2 = 0.5 * alpha;
@@ -234,21 +300,21 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 					a2 = -gd * alpha * alpha / den;
 				a2 = fmin(fmax(a2, 0.1 * alpha), 0.5 * alpha);
 			}
-			st->alpha = a2;
+			rejects++;
+			if (rejects > 60 || a2 < 1e-300)
+				status = kLbLineSearch;
+			else if (evals >= max_evals)
+				status = kLbMaxEval;
+			const bool mixed_stage = sched && stage == 0;
+			st->evals = evals;
 			st->accepted = 0;
-			st->rejects++;
-			if (st->rejects > 60 || a2 < 1e-300)
-				st->status = kLbLineSearch;
-			else if (st->evals >= st->max_evals)
-				st->status = kLbMaxEval;
-			const bool mixed_stage = st->sched && st->stage == 0;
-			if (st->status == kLbLineSearch && (mixed_stage || (E > st->stopval && st->restarts < kLbRestarts))) {
+			if (status == kLbLineSearch && (mixed_stage || (E > stopval && restarts < kLbRestarts))) {
 				// the mixed stage stalled at its noise floor: continue in FP64 from x with a fresh history; an FP64
 				// run that stalled short of the stop value: restart from x with a fresh history
 				if (mixed_stage)
 					st->stage = 1;
 				else
-					st->restarts++;
+					st->restarts = restarts + 1;
 				st->status = kLbRunning;
 				st->count = 0;
 				st->head = 0;
@@ -256,97 +322,122 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 				st->alpha = 0.0;
 				st->rejects = 0;
 				st->small_steps = 0;
+			} else {
+				st->alpha = a2;
+				st->rejects = rejects;
+				st->status = status;
 			}
 		} else {
-			st->accepted = 1;
-			st->rejects = 0;
-			st->iters++;
+			iters++;
 			const double dE = E - Et;
-			st->small_steps = (isfinite(E) && dE <= st->ftol * fabs(E)) ? st->small_steps + 1 : 0;
+			small = (isfinite(E) && dE <= ftol * fabs(E)) ? small + 1 : 0;
 			const bool keep = sy > 1e-300 && yy > 0 && isfinite(sy) && isfinite(yy);
 			int newslot = -1;
+			double gamma = gamma0;
 			if (keep) {
-				newslot = count < m ? (st->head + count) % m : st->head;
+				newslot = count < m ? (head + count) % m : head;
 				if (count < m)
-					st->count = count + 1;
+					k_new = count + 1;
 				else
-					st->head = (st->head + 1) % m;
-				st->gamma = sy / yy;
+					head_new = (head + 1) % m;
+				gamma = sy / yy;
 			}
-			sh_newslot = newslot;
+			if (Et <= stopval && !(sched && stage == 0))
+				status = kLbStopval;
+			else if (gtmax <= gtol)
+				status = kLbGtol;
+			else if (small >= 3)
+				status = kLbFtol;
+			else if (evals >= max_evals)
+				status = kLbMaxEval;
+			if (sched && stage == 0 && (Et <= switch_E || status == kLbGtol || status == kLbFtol)) {
+				// switch to FP64: the accepted point is re-evaluated in FP64 as a fresh start (E = inf accepts it)
+				status = kLbRunning;
+				stage = 1;
+				small = 0;
+				acc = 2;
+			} else if (status == kLbFtol && Et > stopval && restarts < kLbRestarts) {
+				// stalled short of the stop value: restart from the accepted point with a fresh history
+				status = kLbRunning;
+				restarts++;
+				small = 0;
+				acc = 2;
+			}
+			st->evals = evals;
+			st->accepted = 1;
+			st->rejects = 0;
+			st->iters = iters;
+			st->small_steps = small;
+			st->count = k_new;
+			st->head = head_new;
+			st->gamma = gamma;
 			st->newslot = newslot;
 			st->E = Et;
 			st->gmax = gtmax;
 			st->gg = gtgt;
-			if (Et <= st->stopval && !(st->sched && st->stage == 0))
-				st->status = kLbStopval;
-			else if (gtmax <= st->gtol)
-				st->status = kLbGtol;
-			else if (st->small_steps >= 3)
-				st->status = kLbFtol;
-			else if (st->evals >= st->max_evals)
-				st->status = kLbMaxEval;
-			if (st->sched && st->stage == 0 &&
-			    (Et <= st->switch_E || st->status == kLbGtol || st->status == kLbFtol)) {
-				// switch to FP64: the accepted point is re-evaluated in FP64 as a fresh start (E = inf accepts it)
-				st->status = kLbRunning;
-				st->stage = 1;
-				st->small_steps = 0;
-				sh_accept = 2;
-			} else if (st->status == kLbFtol && Et > st->stopval && st->restarts < kLbRestarts) {
-				// stalled short of the stop value: restart from the accepted point with a fresh history
-				st->status = kLbRunning;
-				st->restarts++;
-				st->small_steps = 0;
-				sh_accept = 2;
-			}
+			st->status = status;
+			st->stage = stage;
+			st->restarts = restarts;
+			sh_newslot = newslot;
+			sh_k = k_new;
+			sh_head = head_new;
+			sh_gamma = gamma;
 		}
+		sh_accept = acc;
 	}
 	__syncthreads();
 	if (!sh_accept)
 		return;
 	const int newslot = sh_newslot;
-	// history products at the new point (ring slots), the new pair's rows and columns of S^T Y and Y^T Y
+	// history products at the new point (ring slots), the new pair's rows and columns of S^T Y and Y^T Y (in the
+	// state and in the block's copies)
 	for (int i = threadIdx.x; i < count; i += kLbSolveThreads) {
 		if (i == newslot)   // the oldest pair, replaced by the new one below
 			continue;
 		Sg[i] = tot[5 * i];
 		Yg[i] = tot[5 * i + 1];
 		if (newslot >= 0) {
-			st->SY[i * m + newslot] = tot[5 * i + 2];
-			st->SY[newslot * m + i] = tot[5 * i + 4];
-			st->YY[i * m + newslot] = tot[5 * i + 3];
-			st->YY[newslot * m + i] = tot[5 * i + 3];
+			const double a = tot[5 * i + 2], b = tot[5 * i + 4], c = tot[5 * i + 3];
+			st->SY[i * m + newslot] = a;
+			st->SY[newslot * m + i] = b;
+			st->YY[i * m + newslot] = c;
+			st->YY[newslot * m + i] = c;
+			shSY[i * m + newslot] = a;
+			shSY[newslot * m + i] = b;
+			shYY[i * m + newslot] = c;
+			shYY[newslot * m + i] = c;
 		}
 	}
 	if (threadIdx.x == 0 && newslot >= 0) {
 		st->SY[newslot * m + newslot] = sy;
 		st->YY[newslot * m + newslot] = yy;
-		Sg[newslot] = st->alpha * gtd;   // s'.gt with s' = alpha d (alpha of this accepted step)
+		shSY[newslot * m + newslot] = sy;
+		shYY[newslot * m + newslot] = yy;
+		Sg[newslot] = alpha * gtd;   // s'.gt with s' = alpha d (alpha of this accepted step)
 		Yg[newslot] = ygt;
 	}
 	__syncthreads();
-	const int k = st->count, head = st->head;
-	const double gam = k > 0 ? st->gamma : 1.0;
+	const int k = sh_k, head1 = sh_head;
+	const double gam = k > 0 ? sh_gamma : 1.0;
 	for (int i = threadIdx.x; i < k; i += kLbSolveThreads) {
 		st->Sg[i] = Sg[i];
 		st->Yg[i] = Yg[i];
 	}
-	// compact-form solves (chronological index a <-> ring slot (head + a) % m). R[a][b] = s_a . y_b (a <= b) goes to
-	// shared memory; the triangular solves run column by column on warp 0 (lane l owns rows l and l + 32: one
+	// compact-form solves (chronological index a <-> ring slot (head + a) % m). R goes to shared memory in
+	// chronological order; the triangular solves run column by column on warp 0 (lane l owns rows l and l + 32: one
 	// broadcast and two multiply-adds per column), the product with Y^T Y on all warps.
 	for (int e = threadIdx.x; e < k * k; e += kLbSolveThreads) {
 		const int a = e / k, b = e - a * k;
-		sR[e] = st->SY[((head + a) % m) * m + (head + b) % m];
+		sR[e] = shSY[((head1 + a) % m) * m + (head1 + b) % m];
 	}
 	// reciprocals of the diagonal s_a . y_a, formed in parallel (the solves then multiply)
 	for (int a = threadIdx.x; a < k; a += kLbSolveThreads)
-		rdiag[a] = 1.0 / st->SY[((head + a) % m) * m + (head + a) % m];
+		rdiag[a] = 1.0 / shSY[((head1 + a) % m) * m + (head1 + a) % m];
 	__syncthreads();
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	if (warp == 0) {
 		// t = R^-1 S^T g: backward substitution
-		double r0 = lane < k ? Sg[(head + lane) % m] : 0.0, r1 = lane + 32 < k ? Sg[(head + lane + 32) % m] : 0.0;
+		double r0 = lane < k ? Sg[(head1 + lane) % m] : 0.0, r1 = lane + 32 < k ? Sg[(head1 + lane + 32) % m] : 0.0;
 		for (int b = k - 1; b >= 0; b--) {
 			const double own = (b < 32 ? r0 : r1) * rdiag[b];
 			const double tb = __shfl_sync(0xffffffffu, own, b & 31);
@@ -361,10 +452,10 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 	__syncthreads();
 	// q = D t + gamma Y^T Y t - gamma Y^T g: row a on warp a mod 8, lanes over b, sums by a fixed tree
 	for (int a = warp; a < k; a += kLbSolveThreads / 32) {
-		const int ia = (head + a) % m;
+		const int ia = (head1 + a) % m;
 		double v = 0.0;
 		for (int b = lane; b < k; b += 32)
-			v += st->YY[ia * m + (head + b) % m] * t[b];
+			v += shYY[ia * m + (head1 + b) % m] * t[b];
 		v = lb_warp_sum(v);
 		if (lane == 0)
 			q[a] = sR[a * k + a] * t[a] + gam * v - gam * Yg[ia];
@@ -387,7 +478,7 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 		// store per ring slot: w[slot] = w1, w[kLbMaxHist + slot] = -gamma t; g.d of d = -(gamma g + S w1 + gamma Y w2)
 		double gdn = 0.0;
 		for (int a = lane; a < k; a += 32) {
-			const int ia = (head + a) % m;
+			const int ia = (head1 + a) % m;
 			st->w[ia] = w1[a];
 			st->w[kLbMaxHist + ia] = -gam * t[a];
 			gdn += w1[a] * Sg[ia] - gam * t[a] * Yg[ia];
@@ -424,57 +515,62 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 }
 
 // accept: insert the pair, move x and g; then d = -(gamma g + S w1 + gamma Y w2) and x_trial = x + alpha d.
-// reject: x_trial = x + alpha d.
+// reject: x_trial = x + alpha d. The state's scalars and the variable's values are loaded up front (the stores below
+// may alias them as far as the compiler knows, which would otherwise order every load after them).
 static __global__ void __launch_bounds__(kLbThreads) lb_update_kernel(const LbInst *insts)
 {
 	cudaGridDependencySynchronize();
 	const LbInst in = insts[blockIdx.y];
 	const LbState *st = in.st;
-	if (st->status != kLbRunning && !(st->accepted && st->status != kLbLineSearch))
+	const int status = st->status, accepted = st->accepted;
+	if (status != kLbRunning && !(accepted && status != kLbLineSearch))
 		return;
 	const int j = blockIdx.x * kLbThreads + threadIdx.x;
 	if (j >= in.n)
 		return;
-	const int m = st->m;
-	if (st->accepted) {
-		const int newslot = st->newslot;
-		const double gt = in.gt[j];
-		if (newslot >= 0 && st->status == kLbRunning) {
+	const int m = st->m, newslot = st->newslot, count = st->count, head = st->head;
+	const double gamma = st->gamma, alpha = st->alpha;
+	const double xj = in.x[j], xtj = in.xt[j];
+	if (accepted) {
+		const double gt = in.gt[j], gj = in.g[j];
+		if (newslot >= 0 && status == kLbRunning) {
 			// s = x_trial - x exactly as stepped; y = gt - g (a finished run stores no pair, so a repeated
 			// launch after the end only repeats the idempotent x = x_trial, g = gt)
-			in.S[(size_t)newslot * in.n + j] = in.xt[j] - in.x[j];
-			in.Y[(size_t)newslot * in.n + j] = gt - in.g[j];
+			in.S[(size_t)newslot * in.n + j] = xtj - xj;
+			in.Y[(size_t)newslot * in.n + j] = gt - gj;
 		}
-		in.x[j] = in.xt[j];
+		in.x[j] = xtj;
 		in.g[j] = gt;
-		if (st->status != kLbRunning)
+		if (status != kLbRunning)
 			return;
-		// the pairs' loads are issued four at a time; the sum runs over the pairs in order
-		const int count = st->count, head = st->head;
+		// the pairs' loads (and their weights) are issued eight at a time; the sum runs over the pairs in order
 		const double *__restrict__ S = in.S + j, *__restrict__ Y = in.Y + j, *__restrict__ w = st->w;
 		const size_t n = (size_t)in.n;
-		double v = st->gamma * gt;
+		double v = gamma * gt;
 		int c = 0;
-		for (; c + 4 <= count; c += 4) {
-			int i[4];
-			double sv[4], yv[4];
+		for (; c + 8 <= count; c += 8) {
+			double sv[8], yv[8], ws[8], wy[8];
 #pragma unroll
-			for (int u = 0; u < 4; u++) {
-				i[u] = (head + c + u) % m;
-				sv[u] = S[i[u] * n];
-				yv[u] = Y[i[u] * n];
+			for (int u = 0; u < 8; u++) {
+				const int i = (head + c + u) % m;
+				sv[u] = S[i * n];
+				yv[u] = Y[i * n];
+				ws[u] = w[i];
+				wy[u] = w[kLbMaxHist + i];
 			}
 #pragma unroll
-			for (int u = 0; u < 4; u++)
-				v += w[i[u]] * sv[u] + w[kLbMaxHist + i[u]] * yv[u];
+			for (int u = 0; u < 8; u++)
+				v += ws[u] * sv[u] + wy[u] * yv[u];
 		}
 		for (; c < count; c++) {
 			const int i = (head + c) % m;
 			v += w[i] * S[i * n] + w[kLbMaxHist + i] * Y[i * n];
 		}
 		in.d[j] = -v;
+		in.xt[j] = xtj + alpha * -v;
+		return;
 	}
-	in.xt[j] = in.x[j] + st->alpha * in.d[j];
+	in.xt[j] = xj + alpha * in.d[j];
 }
 
 static __global__ void lb_brief_kernel(const LbInst *insts, int count, LbBrief *out)
@@ -489,8 +585,12 @@ static __global__ void lb_brief_kernel(const LbInst *insts, int count, LbBrief *
 // The three kernels of one L-BFGS step on stream st for `count` instances (insts), at most `cap` dot-product blocks
 // per instance and `maxn` variables in the largest one. Each is launched with programmatic stream serialisation:
 // it is scheduled while the previous kernel drains and waits for it (cudaGridDependencySynchronize) before it reads.
-inline cudaError_t lb_step(const LbInst *insts, int count, int cap, int maxn, cudaStream_t st)
+static inline cudaError_t lb_step(const LbInst *insts, int count, int cap, int maxn, cudaStream_t st)
 {
+	static const cudaError_t smem_attr = cudaFuncSetAttribute(
+	    lb_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLbSolveSmem);
+	if (smem_attr != cudaSuccess)
+		return smem_attr;
 	cudaLaunchAttribute attr[1];
 	attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
 	attr[0].val.programmaticStreamSerializationAllowed = 1;
@@ -505,10 +605,12 @@ inline cudaError_t lb_step(const LbInst *insts, int count, int cap, int maxn, cu
 		return e;
 	cfg.gridDim = dim3(count);
 	cfg.blockDim = dim3(kLbSolveThreads);
+	cfg.dynamicSmemBytes = kLbSolveSmem;
 	if ((e = cudaLaunchKernelEx(&cfg, lb_solve_kernel, insts, cap)) != cudaSuccess)
 		return e;
 	cfg.gridDim = dim3((maxn + kLbThreads - 1) / kLbThreads, count);
 	cfg.blockDim = dim3(kLbThreads);
+	cfg.dynamicSmemBytes = 0;
 	return cudaLaunchKernelEx(&cfg, lb_update_kernel, insts);
 }
 

@@ -3,12 +3,15 @@
     python -m modules_b200.evalcase --d 2 --N 20000 --chi 0.2 --evals 3 [--mixed] [--path split|nufft|auto]
     python -m modules_b200.evalcase --batch 512 --evals 3 [--mixed]
     python -m modules_b200.evalcase --serve 120
+    python -m modules_b200.evalcase --d 3 --N 2000 --chi 0.45 --minimize [--mixed]
 
 The configuration: N uniform random points (seed 1) in a periodic cube of unit density, the CLI's Type 0 k-set.
 With --batch: the seeded batch of uneven instances of the benchmark (modules_b200.workloads.batched_workload),
 evaluated as one batch (the multi-instance kernels) with the default tile shape.
 With --serve: the seeded served stream of the benchmark (modules_b200.workloads.served_stream: arrivals at 60/s,
 N <= 4000, chi <= 0.40) through modules_b200.serve with 16 iterations per round.
+With --minimize: one L-BFGS minimisation of the configuration to Phi/N < 1e-20 (FP64, or with --mixed the precision
+schedule).
 """
 import argparse
 
@@ -27,6 +30,7 @@ def main():
     ap.add_argument("--path", default="split", choices=["split", "nufft", "auto"])
     ap.add_argument("--batch", type=int, default=0, help="evaluate the seeded batch of this many instances")
     ap.add_argument("--serve", type=int, default=0, help="serve the seeded stream of this many requests")
+    ap.add_argument("--minimize", action="store_true", help="minimise the configuration to its ground state")
     a = ap.parse_args()
     if a.serve > 0:
         from .workloads import served_stream
@@ -49,7 +53,13 @@ def main():
     pot = cc.CCPotential(a.d, basis, modes, V)
     paths = {"split": cc.PATH_SPLIT, "nufft": cc.PATH_NUFFT, "auto": cc.PATH_AUTO}
     pot.set_path(paths[a.path])
-    pot.set_configuration(np.random.default_rng(1).random((a.N, a.d)))
+    frac = np.random.default_rng(1).random((a.N, a.d))
+    if a.minimize:
+        prec = cc.PREC_SCHEDULE if a.mixed else cc.PREC_FP64
+        x, E, ev, it, st = pot.minimize(frac, stopval=1e-20 * a.N, precision=prec)
+        print(f"d={a.d} N={a.N} M={len(V)} minimised: E/N={E / a.N:.3e} evals={ev} iters={it} status={st}")
+        return
+    pot.set_configuration(frac)
     E = None
     for _ in range(a.evals):
         E, _F = pot.energy_and_forces(precision=cc.PREC_MIXED if a.mixed else cc.PREC_FP64)
