@@ -222,8 +222,6 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 	cudaGridDependencySynchronize();
 	const LbInst in = insts[blockIdx.x];
 	LbState *st = in.st;
-	if (st->status != kLbRunning)
-		return;
 	const int nblk = lb_blocks(in.n, cap);
 	extern __shared__ double lb_smem[];
 	double *sR = lb_smem;                              // R[a][b] = s_a . y_b (chronological, a <= b), k x k
@@ -234,9 +232,9 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 	__shared__ double rdiag[kLbMaxHist];
 	__shared__ int sh_accept, sh_newslot, sh_k, sh_head;
 	__shared__ double sh_gamma;
-	const int m = st->m, nd = lb_ndots(m);
+	const int status0 = st->status, m = st->m, nd = lb_ndots(m);
 	const int count = st->count;
-	// thread 0's scalars of the state (in flight while the partial sums load)
+	// thread 0's scalars of the state (loaded with the status word, and in flight while the partial sums load)
 	double alpha = 0.0, E = 0.0, Et = 0.0, gd = 0.0, stopval = 0.0, gtol = 0.0, ftol = 0.0, switch_E = 0.0;
 	double gamma0 = 1.0;
 	int64_t evals = 0, max_evals = 0, iters = 0;
@@ -261,9 +259,25 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 		stage = st->stage;
 		sched = st->sched;
 	}
-	for (int e = threadIdx.x; e < m * m; e += kLbSolveThreads) {
-		shSY[e] = st->SY[e];
-		shYY[e] = st->YY[e];
+	if (status0 != kLbRunning)
+		return;
+	// (eight elements of each matrix per thread in flight: a rolled loop would wait for each load before its store)
+	for (int e0 = threadIdx.x; e0 < m * m; e0 += 8 * kLbSolveThreads) {
+		double a[8], b[8];
+#pragma unroll
+		for (int u = 0; u < 8; u++) {
+			const int e = e0 + u * kLbSolveThreads;
+			a[u] = e < m * m ? st->SY[e] : 0.0;
+			b[u] = e < m * m ? st->YY[e] : 0.0;
+		}
+#pragma unroll
+		for (int u = 0; u < 8; u++) {
+			const int e = e0 + u * kLbSolveThreads;
+			if (e < m * m) {
+				shSY[e] = a[u];
+				shYY[e] = b[u];
+			}
+		}
 	}
 	// totals: the blocks' partials in block order, up to 16 blocks' loads in flight
 	for (int k = threadIdx.x; k < nd; k += kLbSolveThreads) {
@@ -543,11 +557,25 @@ static __global__ void __launch_bounds__(kLbThreads) lb_update_kernel(const LbIn
 		in.g[j] = gt;
 		if (status != kLbRunning)
 			return;
-		// the pairs' loads (and their weights) are issued eight at a time; the sum runs over the pairs in order
+		// the pairs' loads (and their weights) are issued sixteen at a time; the sum runs over the pairs in order
 		const double *__restrict__ S = in.S + j, *__restrict__ Y = in.Y + j, *__restrict__ w = st->w;
 		const size_t n = (size_t)in.n;
 		double v = gamma * gt;
 		int c = 0;
+		for (; c + 16 <= count; c += 16) {
+			double sv[16], yv[16], ws[16], wy[16];
+#pragma unroll
+			for (int u = 0; u < 16; u++) {
+				const int i = (head + c + u) % m;
+				sv[u] = S[i * n];
+				yv[u] = Y[i * n];
+				ws[u] = w[i];
+				wy[u] = w[kLbMaxHist + i];
+			}
+#pragma unroll
+			for (int u = 0; u < 16; u++)
+				v += ws[u] * sv[u] + wy[u] * yv[u];
+		}
 		for (; c + 8 <= count; c += 8) {
 			double sv[8], yv[8], ws[8], wy[8];
 #pragma unroll
