@@ -54,6 +54,7 @@ struct LbState {
 	double w[2 * kLbMaxHist];
 	double SY[kLbMaxHist * kLbMaxHist];   // SY[i * m + j] = s_i . y_j (ring slots)
 	double YY[kLbMaxHist * kLbMaxHist];   // YY[i * m + j] = y_i . y_j
+	double Ri[kLbMaxHist * kLbMaxHist];   // R^-1 by ring slots (upper triangle in chronological order)
 	double Sg[kLbMaxHist], Yg[kLbMaxHist];// S^T g, Y^T g at x (ring slots)
 };
 
@@ -209,14 +210,18 @@ __device__ __forceinline__ double lb_warp_sum(double v)
 
 constexpr int kLbSolveThreads = 256;
 
-// Dynamic shared memory of lb_solve_kernel: R (chronological) and the ring copies of S^T Y and Y^T Y.
+// Dynamic shared memory of lb_solve_kernel: the ring copies of S^T Y, Y^T Y and R^-1.
 constexpr size_t kLbSolveSmem = 3 * sizeof(double) * kLbMaxHist * kLbMaxHist;
 
 // One block per instance: block totals of the dot products (parallel over the products, blocks summed in order),
-// accept / reject and the step length (thread 0), history matrices (parallel over slots), the triangular solves of
-// the compact form (warp 0, lanes split every inner sum), g.d of the new direction and the stop tests. The kernel is
-// a chain of dependent steps, so its global reads are issued together up front: the partial sums, the state's
-// scalars (thread 0) and the history matrices, which the block keeps in shared memory and updates there as well.
+// accept / reject and the step length (thread 0), history matrices (parallel over slots), the products with R^-1 of
+// the compact form, g.d of the new direction and the stop tests. R^-1 is kept with the history instead of solving
+// with R each iteration: dropping the oldest pair keeps the trailing block of the inverse of an upper triangular
+// matrix, and a new (newest) pair adds one column, -R^-1 r / rho with r_a = s_a . y_new and rho = s_new . y_new; so
+// both triangular solves become matrix-vector products spread over the warps, where substitution was a chain of k
+// dependent steps. The kernel is a chain of dependent phases, so its global reads are issued together up front: the
+// partial sums, the state's scalars (thread 0) and the history matrices, which the block keeps in shared memory and
+// updates there as well.
 static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const LbInst *insts, int cap)
 {
 	cudaGridDependencySynchronize();
@@ -224,12 +229,12 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 	LbState *st = in.st;
 	const int nblk = lb_blocks(in.n, cap);
 	extern __shared__ double lb_smem[];
-	double *sR = lb_smem;                              // R[a][b] = s_a . y_b (chronological, a <= b), k x k
-	double *shSY = sR + kLbMaxHist * kLbMaxHist;        // S^T Y by ring slots, m x m
+	double *shSY = lb_smem;                             // S^T Y by ring slots, m x m
 	double *shYY = shSY + kLbMaxHist * kLbMaxHist;      // Y^T Y by ring slots, m x m
+	double *shRi = shYY + kLbMaxHist * kLbMaxHist;      // R^-1 by ring slots, m x m
 	__shared__ double tot[5 * kLbMaxHist + 6];
 	__shared__ double Sg[kLbMaxHist], Yg[kLbMaxHist], t[kLbMaxHist], q[kLbMaxHist], w1[kLbMaxHist];
-	__shared__ double rdiag[kLbMaxHist];
+	__shared__ int slot[kLbMaxHist];
 	__shared__ int sh_accept, sh_newslot, sh_k, sh_head;
 	__shared__ double sh_gamma;
 	const int status0 = st->status, m = st->m, nd = lb_ndots(m);
@@ -263,12 +268,13 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 		return;
 	// (eight elements of each matrix per thread in flight: a rolled loop would wait for each load before its store)
 	for (int e0 = threadIdx.x; e0 < m * m; e0 += 8 * kLbSolveThreads) {
-		double a[8], b[8];
+		double a[8], b[8], c[8];
 #pragma unroll
 		for (int u = 0; u < 8; u++) {
 			const int e = e0 + u * kLbSolveThreads;
 			a[u] = e < m * m ? st->SY[e] : 0.0;
 			b[u] = e < m * m ? st->YY[e] : 0.0;
+			c[u] = e < m * m ? st->Ri[e] : 0.0;
 		}
 #pragma unroll
 		for (int u = 0; u < 8; u++) {
@@ -276,6 +282,7 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 			if (e < m * m) {
 				shSY[e] = a[u];
 				shYY[e] = b[u];
+				shRi[e] = c[u];
 			}
 		}
 	}
@@ -436,63 +443,86 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 	for (int i = threadIdx.x; i < k; i += kLbSolveThreads) {
 		st->Sg[i] = Sg[i];
 		st->Yg[i] = Yg[i];
+		slot[i] = head1 + i < m ? head1 + i : head1 + i - m;   // chronological index -> ring slot
 	}
-	// compact-form solves (chronological index a <-> ring slot (head + a) % m). R goes to shared memory in
-	// chronological order; the triangular solves run column by column on warp 0 (lane l owns rows l and l + 32: one
-	// broadcast and two multiply-adds per column), the product with Y^T Y on all warps.
-	for (int e = threadIdx.x; e < k * k; e += kLbSolveThreads) {
-		const int a = e / k, b = e - a * k;
-		sR[e] = shSY[((head1 + a) % m) * m + (head1 + b) % m];
-	}
-	// reciprocals of the diagonal s_a . y_a, formed in parallel (the solves then multiply)
-	for (int a = threadIdx.x; a < k; a += kLbSolveThreads)
-		rdiag[a] = 1.0 / shSY[((head1 + a) % m) * m + (head1 + a) % m];
 	__syncthreads();
+	// compact form (chronological index a <-> ring slot slot[a]). Every product with a k x k matrix runs on the whole
+	// block at once: four lanes per row (64 rows, kLbMaxHist), each taking every fourth term in order, then a fixed
+	// two-step tree (the four lanes of a row are adjacent lanes of one warp; rows beyond k add nothing)
+	static_assert(kLbSolveThreads == 4 * kLbMaxHist, "four lanes per history row");
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	if (warp == 0) {
-		// t = R^-1 S^T g: backward substitution
-		double r0 = lane < k ? Sg[(head1 + lane) % m] : 0.0, r1 = lane + 32 < k ? Sg[(head1 + lane + 32) % m] : 0.0;
-		for (int b = k - 1; b >= 0; b--) {
-			const double own = (b < 32 ? r0 : r1) * rdiag[b];
-			const double tb = __shfl_sync(0xffffffffu, own, b & 31);
-			if (lane == 0)
-				t[b] = tb;
-			if (lane < b)
-				r0 -= sR[lane * k + b] * tb;
-			if (lane + 32 < b)
-				r1 -= sR[(lane + 32) * k + b] * tb;
-		}
-	}
-	__syncthreads();
-	// q = D t + gamma Y^T Y t - gamma Y^T g: row a on warp a mod 8, lanes over b, sums by a fixed tree
-	for (int a = warp; a < k; a += kLbSolveThreads / 32) {
-		const int ia = (head1 + a) % m;
+	const int row = threadIdx.x >> 2, sub = threadIdx.x & 3;
+	auto row_sum = [](double v) {
+		v += __shfl_xor_sync(0xffffffffu, v, 1);
+		return v + __shfl_xor_sync(0xffffffffu, v, 2);
+	};
+	if (newslot >= 0) {
+		// the new pair's column of R^-1 (the new pair is the newest, chronological index k - 1)
 		double v = 0.0;
-		for (int b = lane; b < k; b += 32)
-			v += shYY[ia * m + (head1 + b) % m] * t[b];
-		v = lb_warp_sum(v);
-		if (lane == 0)
-			q[a] = sR[a * k + a] * t[a] + gam * v - gam * Yg[ia];
+		if (row < k - 1) {
+			const int ia = slot[row];
+			for (int b = row + sub; b < k - 1; b += 4)
+				v += shRi[ia * m + slot[b]] * shSY[slot[b] * m + newslot];
+		}
+		v = row_sum(v);
+		if (row < k - 1 && sub == 0) {
+			const double c = -v / sy;
+			shRi[slot[row] * m + newslot] = c;
+			st->Ri[slot[row] * m + newslot] = c;
+		}
+		if (threadIdx.x == 0) {
+			const double c = 1.0 / sy;
+			shRi[newslot * m + newslot] = c;
+			st->Ri[newslot * m + newslot] = c;
+		}
+		__syncthreads();
+	}
+	// t = R^-1 S^T g
+	{
+		double v = 0.0;
+		if (row < k) {
+			const int ia = slot[row];
+			for (int b = row + sub; b < k; b += 4)
+				v += shRi[ia * m + slot[b]] * Sg[slot[b]];
+		}
+		v = row_sum(v);
+		if (row < k && sub == 0)
+			t[row] = v;
+	}
+	__syncthreads();
+	// q = D t + gamma Y^T Y t - gamma Y^T g
+	{
+		double v = 0.0;
+		if (row < k) {
+			const int ia = slot[row];
+			for (int b = sub; b < k; b += 4)
+				v += shYY[ia * m + slot[b]] * t[b];
+		}
+		v = row_sum(v);
+		if (row < k && sub == 0) {
+			const int ia = slot[row];
+			q[row] = shSY[ia * m + ia] * t[row] + gam * v - gam * Yg[ia];
+		}
+	}
+	__syncthreads();
+	// w1 = R^-T q
+	{
+		double v = 0.0;
+		if (row < k) {
+			const int ib = slot[row];
+			for (int a = sub; a <= row; a += 4)
+				v += shRi[slot[a] * m + ib] * q[a];
+		}
+		v = row_sum(v);
+		if (row < k && sub == 0)
+			w1[row] = v;
 	}
 	__syncthreads();
 	if (warp == 0) {
-		// w1 = R^-T q: forward substitution
-		double r0 = lane < k ? q[lane] : 0.0, r1 = lane + 32 < k ? q[lane + 32] : 0.0;
-		for (int b = 0; b < k; b++) {
-			const double own = (b < 32 ? r0 : r1) * rdiag[b];
-			const double wb = __shfl_sync(0xffffffffu, own, b & 31);
-			if (lane == 0)
-				w1[b] = wb;
-			if (lane > b && lane < k)
-				r0 -= sR[b * k + lane] * wb;
-			if (lane + 32 > b && lane + 32 < k)
-				r1 -= sR[b * k + lane + 32] * wb;
-		}
-		__syncwarp();
 		// store per ring slot: w[slot] = w1, w[kLbMaxHist + slot] = -gamma t; g.d of d = -(gamma g + S w1 + gamma Y w2)
 		double gdn = 0.0;
 		for (int a = lane; a < k; a += 32) {
-			const int ia = (head1 + a) % m;
+			const int ia = slot[a];
 			st->w[ia] = w1[a];
 			st->w[kLbMaxHist + ia] = -gam * t[a];
 			gdn += w1[a] * Sg[ia] - gam * t[a] * Yg[ia];
@@ -544,9 +574,8 @@ static __global__ void __launch_bounds__(kLbThreads) lb_update_kernel(const LbIn
 		return;
 	const int m = st->m, newslot = st->newslot, count = st->count, head = st->head;
 	const double gamma = st->gamma, alpha = st->alpha;
-	const double xj = in.x[j], xtj = in.xt[j];
+	const double xj = in.x[j], xtj = in.xt[j], gt = in.gt[j], gj = in.g[j];
 	if (accepted) {
-		const double gt = in.gt[j], gj = in.g[j];
 		if (newslot >= 0 && status == kLbRunning) {
 			// s = x_trial - x exactly as stepped; y = gt - g (a finished run stores no pair, so a repeated
 			// launch after the end only repeats the idempotent x = x_trial, g = gt)
@@ -566,7 +595,7 @@ static __global__ void __launch_bounds__(kLbThreads) lb_update_kernel(const LbIn
 			double sv[16], yv[16], ws[16], wy[16];
 #pragma unroll
 			for (int u = 0; u < 16; u++) {
-				const int i = (head + c + u) % m;
+				const int i = head + c + u < m ? head + c + u : head + c + u - m;
 				sv[u] = S[i * n];
 				yv[u] = Y[i * n];
 				ws[u] = w[i];
@@ -580,7 +609,7 @@ static __global__ void __launch_bounds__(kLbThreads) lb_update_kernel(const LbIn
 			double sv[8], yv[8], ws[8], wy[8];
 #pragma unroll
 			for (int u = 0; u < 8; u++) {
-				const int i = (head + c + u) % m;
+				const int i = head + c + u < m ? head + c + u : head + c + u - m;
 				sv[u] = S[i * n];
 				yv[u] = Y[i * n];
 				ws[u] = w[i];
@@ -591,7 +620,7 @@ static __global__ void __launch_bounds__(kLbThreads) lb_update_kernel(const LbIn
 				v += ws[u] * sv[u] + wy[u] * yv[u];
 		}
 		for (; c < count; c++) {
-			const int i = (head + c) % m;
+			const int i = head + c < m ? head + c : head + c - m;
 			v += w[i] * S[i * n] + w[kLbMaxHist + i] * Y[i * n];
 		}
 		in.d[j] = -v;
