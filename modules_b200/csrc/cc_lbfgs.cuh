@@ -91,7 +91,8 @@ constexpr int kLbMaxBlocks = 64;   // cap of the batched minimisation and the se
 // w + 16, ... over the chunk (every lane up to 8 variables, loads issued together), so the pairs' loads run in
 // parallel across warps instead of one pair after another. Sums have a fixed order (lanes by a fixed tree, chunks in
 // order, warps in order for the non-pair products), so a run repeats bitwise.
-static __global__ void __launch_bounds__(kLbThreads) lb_dots_kernel(const LbInst *insts, int cap)
+constexpr int kLbDotsThreads = 2 * kLbThreads;   // a chunk of kLbThreads variables; twice as many warps over the pairs
+static __global__ void __launch_bounds__(kLbDotsThreads) lb_dots_kernel(const LbInst *insts, int cap)
 {
 	cudaGridDependencySynchronize();   // launched early (programmatic dependent launch): the evaluation is complete
 	const LbInst in = insts[blockIdx.y];
@@ -99,7 +100,7 @@ static __global__ void __launch_bounds__(kLbThreads) lb_dots_kernel(const LbInst
 	const int nblk = lb_blocks(in.n, cap);
 	if (st->status != kLbRunning || (int)blockIdx.x >= nblk)
 		return;
-	constexpr int kWarps = kLbThreads / 32;
+	constexpr int kWarps = kLbDotsThreads / 32;
 	const int m = st->m, nd = lb_ndots(m);
 	const int per = (in.n + nblk - 1) / nblk;
 	const int j0 = blockIdx.x * per, j1 = min(in.n, j0 + per);
@@ -109,7 +110,7 @@ static __global__ void __launch_bounds__(kLbThreads) lb_dots_kernel(const LbInst
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	const int count = st->count;
 	double a[6] = {0, 0, 0, 0, 0, 0};
-	for (int k = threadIdx.x; k < 5 * count; k += kLbThreads)
+	for (int k = threadIdx.x; k < 5 * count; k += kLbDotsThreads)
 		pr[k] = 0.0;
 	for (int c0 = j0; c0 < j1; c0 += kLbThreads) {
 		const int cn = min(kLbThreads, j1 - c0);
@@ -186,7 +187,7 @@ static __global__ void __launch_bounds__(kLbThreads) lb_dots_kernel(const LbInst
 			red[warp][k] = a[k];
 	__syncthreads();
 	double *out = in.part + (size_t)blockIdx.x * nd;
-	for (int k = threadIdx.x; k < nd; k += kLbThreads) {
+	for (int k = threadIdx.x; k < nd; k += kLbDotsThreads) {
 		if (k < 5 * m) {
 			out[k] = k / 5 < count ? pr[k] : 0.0;
 			continue;
@@ -222,7 +223,7 @@ constexpr size_t kLbSolveSmem = 3 * sizeof(double) * kLbMaxHist * kLbMaxHist;
 // dependent steps. The kernel is a chain of dependent phases, so its global reads are issued together up front: the
 // partial sums, the state's scalars (thread 0) and the history matrices, which the block keeps in shared memory and
 // updates there as well.
-static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const LbInst *insts, int cap)
+static __global__ void __launch_bounds__(kLbSolveThreads, 2) lb_solve_kernel(const LbInst *insts, int cap)
 {
 	cudaGridDependencySynchronize();
 	const LbInst in = insts[blockIdx.x];
@@ -235,29 +236,24 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 	__shared__ double tot[5 * kLbMaxHist + 6];
 	__shared__ double Sg[kLbMaxHist], Yg[kLbMaxHist], t[kLbMaxHist], q[kLbMaxHist], w1[kLbMaxHist];
 	__shared__ int slot[kLbMaxHist];
-	__shared__ int sh_accept, sh_newslot, sh_k, sh_head;
-	__shared__ double sh_gamma;
+	__shared__ int sh_accept;
 	const int status0 = st->status, m = st->m, nd = lb_ndots(m);
 	const int count = st->count;
-	// thread 0's scalars of the state (loaded with the status word, and in flight while the partial sums load)
-	double alpha = 0.0, E = 0.0, Et = 0.0, gd = 0.0, stopval = 0.0, gtol = 0.0, ftol = 0.0, switch_E = 0.0;
-	double gamma0 = 1.0;
+	// the state's scalars (loaded with the status word, and in flight while the partial sums load): every thread
+	// takes the acceptance test and the new pair's slot, thread 0 the rest of the bookkeeping
+	const double alpha = st->alpha, E = st->E, Et = st->Et, gd = st->gd, gamma0 = st->gamma;
+	const int head = st->head;
+	double stopval = 0.0, gtol = 0.0, ftol = 0.0, switch_E = 0.0;
 	int64_t evals = 0, max_evals = 0, iters = 0;
-	int head = 0, rejects = 0, small = 0, restarts = 0, stage = 0, sched = 0;
+	int rejects = 0, small = 0, restarts = 0, stage = 0, sched = 0;
 	if (threadIdx.x == 0) {
-		alpha = st->alpha;
-		E = st->E;
-		Et = st->Et;
-		gd = st->gd;
 		stopval = st->stopval;
 		gtol = st->gtol;
 		ftol = st->ftol;
 		switch_E = st->switch_E;
-		gamma0 = st->gamma;
 		evals = st->evals;
 		max_evals = st->max_evals;
 		iters = st->iters;
-		head = st->head;
 		rejects = st->rejects;
 		small = st->small_steps;
 		restarts = st->restarts;
@@ -287,32 +283,30 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 		}
 	}
 	// totals: the blocks' partials in block order, up to 16 blocks' loads in flight
-	for (int k = threadIdx.x; k < nd; k += kLbSolveThreads) {
-		const bool is_max = k == nd - 1;
-		double v = in.part[k];
+	for (int p = threadIdx.x; p < nd; p += kLbSolveThreads) {
+		const bool is_max = p == nd - 1;
+		double v = in.part[p];
 		for (int b0 = 1; b0 < nblk; b0 += 16) {
 			double pv[16];
 #pragma unroll
 			for (int u = 0; u < 16; u++)
-				pv[u] = b0 + u < nblk ? in.part[(size_t)(b0 + u) * nd + k] : 0.0;
+				pv[u] = b0 + u < nblk ? in.part[(size_t)(b0 + u) * nd + p] : 0.0;
 #pragma unroll
 			for (int u = 0; u < 16; u++)
 				if (b0 + u < nblk)
 					v = is_max ? fmax(v, pv[u]) : v + pv[u];
 		}
-		tot[k] = v;
+		tot[p] = v;
 	}
 	__syncthreads();
 	const double gtd = tot[5 * m], gtgt = tot[5 * m + 1], sy = tot[5 * m + 2], yy = tot[5 * m + 3],
 	             ygt = tot[5 * m + 4], gtmax = tot[5 * m + 5];
-	if (threadIdx.x == 0) {
-		evals++;
-		int status = kLbRunning;
-		const bool finite = isfinite(Et) && isfinite(gtgt);
-		const bool armijo = finite && Et <= E + 1e-4 * alpha * gd;
-		int acc = armijo;
-		int k_new = count, head_new = head;
-		if (!armijo) {
+	const bool finite = isfinite(Et) && isfinite(gtgt);
+	const bool armijo = finite && Et <= E + 1e-4 * alpha * gd;
+	if (!armijo) {
+		if (threadIdx.x == 0) {
+			evals++;
+			int status = kLbRunning;
 			// backtrack: safeguarded quadratic model of the energy along d
 			double a2 = 0.5 * alpha;
 			if (finite) {
@@ -348,68 +342,65 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 				st->rejects = rejects;
 				st->status = status;
 			}
-		} else {
-			iters++;
-			const double dE = E - Et;
-			small = (isfinite(E) && dE <= ftol * fabs(E)) ? small + 1 : 0;
-			const bool keep = sy > 1e-300 && yy > 0 && isfinite(sy) && isfinite(yy);
-			int newslot = -1;
-			double gamma = gamma0;
-			if (keep) {
-				newslot = count < m ? (head + count) % m : head;
-				if (count < m)
-					k_new = count + 1;
-				else
-					head_new = (head + 1) % m;
-				gamma = sy / yy;
-			}
-			if (Et <= stopval && !(sched && stage == 0))
-				status = kLbStopval;
-			else if (gtmax <= gtol)
-				status = kLbGtol;
-			else if (small >= 3)
-				status = kLbFtol;
-			else if (evals >= max_evals)
-				status = kLbMaxEval;
-			if (sched && stage == 0 && (Et <= switch_E || status == kLbGtol || status == kLbFtol)) {
-				// switch to FP64: the accepted point is re-evaluated in FP64 as a fresh start (E = inf accepts it)
-				status = kLbRunning;
-				stage = 1;
-				small = 0;
-				acc = 2;
-			} else if (status == kLbFtol && Et > stopval && restarts < kLbRestarts) {
-				// stalled short of the stop value: restart from the accepted point with a fresh history
-				status = kLbRunning;
-				restarts++;
-				small = 0;
-				acc = 2;
-			}
-			st->evals = evals;
-			st->accepted = 1;
-			st->rejects = 0;
-			st->iters = iters;
-			st->small_steps = small;
-			st->count = k_new;
-			st->head = head_new;
-			st->gamma = gamma;
-			st->newslot = newslot;
-			st->E = Et;
-			st->gmax = gtmax;
-			st->gg = gtgt;
-			st->status = status;
-			st->stage = stage;
-			st->restarts = restarts;
-			sh_newslot = newslot;
-			sh_k = k_new;
-			sh_head = head_new;
-			sh_gamma = gamma;
 		}
-		sh_accept = acc;
-	}
-	__syncthreads();
-	if (!sh_accept)
 		return;
-	const int newslot = sh_newslot;
+	}
+	// accepted: the new pair enters the history if s.y > 0
+	const bool keep = sy > 1e-300 && yy > 0 && isfinite(sy) && isfinite(yy);
+	int newslot = -1, k = count, head1 = head;
+	double gamma = gamma0;
+	if (keep) {
+		newslot = count < m ? (head + count) % m : head;
+		if (count < m)
+			k = count + 1;
+		else
+			head1 = (head + 1) % m;
+		gamma = sy / yy;
+	}
+	if (threadIdx.x == 0) {
+		int status = kLbRunning, acc = 1;
+		evals++;
+		iters++;
+		const double dE = E - Et;
+		small = (isfinite(E) && dE <= ftol * fabs(E)) ? small + 1 : 0;
+		if (Et <= stopval && !(sched && stage == 0))
+			status = kLbStopval;
+		else if (gtmax <= gtol)
+			status = kLbGtol;
+		else if (small >= 3)
+			status = kLbFtol;
+		else if (evals >= max_evals)
+			status = kLbMaxEval;
+		if (sched && stage == 0 && (Et <= switch_E || status == kLbGtol || status == kLbFtol)) {
+			// switch to FP64: the accepted point is re-evaluated in FP64 as a fresh start (E = inf accepts it)
+			status = kLbRunning;
+			stage = 1;
+			small = 0;
+			acc = 2;
+		} else if (status == kLbFtol && Et > stopval && restarts < kLbRestarts) {
+			// stalled short of the stop value: restart from the accepted point with a fresh history
+			status = kLbRunning;
+			restarts++;
+			small = 0;
+			acc = 2;
+		}
+		st->evals = evals;
+		st->accepted = 1;
+		st->rejects = 0;
+		st->iters = iters;
+		st->small_steps = small;
+		st->count = k;
+		st->head = head1;
+		st->gamma = gamma;
+		st->newslot = newslot;
+		st->E = Et;
+		st->gmax = gtmax;
+		st->gg = gtgt;
+		st->status = status;
+		st->stage = stage;
+		st->restarts = restarts;
+		sh_accept = acc;   // read after the barriers below
+	}
 	// history products at the new point (ring slots), the new pair's rows and columns of S^T Y and Y^T Y (in the
 	// state and in the block's copies)
 	for (int i = threadIdx.x; i < count; i += kLbSolveThreads) {
@@ -438,8 +429,7 @@ static __global__ void __launch_bounds__(kLbSolveThreads) lb_solve_kernel(const 
 		Yg[newslot] = ygt;
 	}
 	__syncthreads();
-	const int k = sh_k, head1 = sh_head;
-	const double gam = k > 0 ? sh_gamma : 1.0;
+	const double gam = k > 0 ? gamma : 1.0;
 	for (int i = threadIdx.x; i < k; i += kLbSolveThreads) {
 		st->Sg[i] = Sg[i];
 		st->Yg[i] = Yg[i];
@@ -656,7 +646,7 @@ static inline cudaError_t lb_step(const LbInst *insts, int count, int cap, int m
 	cfg.attrs = attr;
 	cfg.numAttrs = 1;
 	cfg.gridDim = dim3(cap, count);
-	cfg.blockDim = dim3(kLbThreads);
+	cfg.blockDim = dim3(kLbDotsThreads);
 	cudaError_t e = cudaLaunchKernelEx(&cfg, lb_dots_kernel, insts, cap);
 	if (e != cudaSuccess)
 		return e;
