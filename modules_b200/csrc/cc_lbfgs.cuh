@@ -549,75 +549,114 @@ static __global__ void __launch_bounds__(kLbSolveThreads, 2) lb_solve_kernel(con
 }
 
 // accept: insert the pair, move x and g; then d = -(gamma g + S w1 + gamma Y w2) and x_trial = x + alpha d.
-// reject: x_trial = x + alpha d. The state's scalars and the variable's values are loaded up front (the stores below
-// may alias them as far as the compiler knows, which would otherwise order every load after them).
-static __global__ void __launch_bounds__(kLbThreads) lb_update_kernel(const LbInst *insts)
+// reject: x_trial = x + alpha d. The history sum is taken in quarters of the pairs: quarter q's terms in order (the
+// first quarter starting from gamma g), then (P0 + P1) + (P2 + P3). LANES = 4 gives each quarter its own lane (all
+// of a lane's pairs loaded at once, the tree through two shuffles: the single-instance launch, whose time is latency);
+// LANES = 1 takes the four quarters on one thread (the multi-instance launches, which have parallelism to spare). Both
+// do the same arithmetic, so an instance's result does not depend on the launch it runs in. The state's scalars and
+// the variable's values are loaded up front (the stores below may alias them as far as the compiler knows, which
+// would otherwise order every load after them).
+constexpr int kLbUpdPairs = kLbMaxHist / 4;   // pairs per quarter at most
+template <int LANES>
+__device__ __forceinline__ double lb_quarter(const double *__restrict__ S, const double *__restrict__ Y,
+                                             const double *__restrict__ w, size_t n, int head, int m, int count,
+                                             int q, double v)
+{
+	const int per = (count + 3) / 4, c0 = q * per;
+	double sv[kLbUpdPairs], yv[kLbUpdPairs], ws[kLbUpdPairs], wy[kLbUpdPairs];
+#pragma unroll
+	for (int u = 0; u < kLbUpdPairs; u++) {
+		const int c = c0 + u;
+		const bool on = u < per && c < count;
+		const int i = !on ? 0 : head + c < m ? head + c : head + c - m;
+		sv[u] = on ? S[i * n] : 0.0;
+		yv[u] = on ? Y[i * n] : 0.0;
+		ws[u] = on ? w[i] : 0.0;
+		wy[u] = on ? w[kLbMaxHist + i] : 0.0;
+	}
+#pragma unroll
+	for (int u = 0; u < kLbUpdPairs; u++)
+		if (u < per && c0 + u < count)
+			v = fma(wy[u], yv[u], fma(ws[u], sv[u], v));
+	return v;
+}
+template <int LANES>
+static __global__ void __launch_bounds__(kLbThreads, LANES == 1 ? 4 : 2) lb_update_kernel(const LbInst *insts)
 {
 	cudaGridDependencySynchronize();
 	const LbInst in = insts[blockIdx.y];
 	const LbState *st = in.st;
 	const int status = st->status, accepted = st->accepted;
 	if (status != kLbRunning && !(accepted && status != kLbLineSearch))
+		return;   // (the whole block: one instance)
+	const int sub = threadIdx.x & (LANES - 1);
+	const int j = blockIdx.x * (kLbThreads / LANES) + threadIdx.x / LANES;
+	const bool mine = j < in.n && sub == 0;   // the lane that stores the variable's results
+	if (LANES == 1 && j >= in.n)
 		return;
-	const int j = blockIdx.x * kLbThreads + threadIdx.x;
-	if (j >= in.n)
-		return;
+	const int jj = j < in.n ? j : 0;          // lanes past the end read variable 0 and store nothing
 	const int m = st->m, newslot = st->newslot, count = st->count, head = st->head;
 	const double gamma = st->gamma, alpha = st->alpha;
-	const double xj = in.x[j], xtj = in.xt[j], gt = in.gt[j], gj = in.g[j];
+	const double xj = in.x[jj], xtj = in.xt[jj], gt = in.gt[jj], gj = in.g[jj];
 	if (accepted) {
-		if (newslot >= 0 && status == kLbRunning) {
-			// s = x_trial - x exactly as stepped; y = gt - g (a finished run stores no pair, so a repeated
-			// launch after the end only repeats the idempotent x = x_trial, g = gt)
-			in.S[(size_t)newslot * in.n + j] = xtj - xj;
-			in.Y[(size_t)newslot * in.n + j] = gt - gj;
+		if (mine) {
+			if (newslot >= 0 && status == kLbRunning) {
+				// s = x_trial - x exactly as stepped; y = gt - g (a finished run stores no pair, so a repeated
+				// launch after the end only repeats the idempotent x = x_trial, g = gt)
+				in.S[(size_t)newslot * in.n + j] = xtj - xj;
+				in.Y[(size_t)newslot * in.n + j] = gt - gj;
+			}
+			in.x[j] = xtj;
+			in.g[j] = gt;
 		}
-		in.x[j] = xtj;
-		in.g[j] = gt;
 		if (status != kLbRunning)
 			return;
-		// the pairs' loads (and their weights) are issued sixteen at a time; the sum runs over the pairs in order
-		const double *__restrict__ S = in.S + j, *__restrict__ Y = in.Y + j, *__restrict__ w = st->w;
+		const double *S = in.S + jj, *Y = in.Y + jj, *w = st->w;
 		const size_t n = (size_t)in.n;
-		double v = gamma * gt;
-		int c = 0;
-		for (; c + 16 <= count; c += 16) {
-			double sv[16], yv[16], ws[16], wy[16];
+		double v;
+		if constexpr (LANES == 4) {
+			v = lb_quarter<4>(S, Y, w, n, head, m, count, sub, sub == 0 ? gamma * gt : 0.0);
+			v += __shfl_xor_sync(0xffffffffu, v, 1);
+			v += __shfl_xor_sync(0xffffffffu, v, 2);
+		} else {
+			// the same four quarter sums, one after another, each in batches of four pairs' loads
+			const int per = (count + 3) / 4;
+			double p[4];
+#pragma unroll 1
+			for (int q = 0; q < 4; q++) {
+				double a = q == 0 ? gamma * gt : 0.0;
+				const int c1 = min(count, (q + 1) * per);
+				int c = q * per;
+				for (; c + 4 <= c1; c += 4) {
+					double sv[4], yv[4], ws[4], wy[4];
 #pragma unroll
-			for (int u = 0; u < 16; u++) {
-				const int i = head + c + u < m ? head + c + u : head + c + u - m;
-				sv[u] = S[i * n];
-				yv[u] = Y[i * n];
-				ws[u] = w[i];
-				wy[u] = w[kLbMaxHist + i];
+					for (int u = 0; u < 4; u++) {
+						const int i = head + c + u < m ? head + c + u : head + c + u - m;
+						sv[u] = S[i * n];
+						yv[u] = Y[i * n];
+						ws[u] = w[i];
+						wy[u] = w[kLbMaxHist + i];
+					}
+#pragma unroll
+					for (int u = 0; u < 4; u++)
+						a = fma(wy[u], yv[u], fma(ws[u], sv[u], a));
+				}
+				for (; c < c1; c++) {
+					const int i = head + c < m ? head + c : head + c - m;
+					a = fma(w[kLbMaxHist + i], Y[i * n], fma(w[i], S[i * n], a));
+				}
+				p[q] = a;
 			}
-#pragma unroll
-			for (int u = 0; u < 16; u++)
-				v += ws[u] * sv[u] + wy[u] * yv[u];
+			v = (p[0] + p[1]) + (p[2] + p[3]);
 		}
-		for (; c + 8 <= count; c += 8) {
-			double sv[8], yv[8], ws[8], wy[8];
-#pragma unroll
-			for (int u = 0; u < 8; u++) {
-				const int i = head + c + u < m ? head + c + u : head + c + u - m;
-				sv[u] = S[i * n];
-				yv[u] = Y[i * n];
-				ws[u] = w[i];
-				wy[u] = w[kLbMaxHist + i];
-			}
-#pragma unroll
-			for (int u = 0; u < 8; u++)
-				v += ws[u] * sv[u] + wy[u] * yv[u];
+		if (mine) {
+			in.d[j] = -v;
+			in.xt[j] = xtj + alpha * -v;
 		}
-		for (; c < count; c++) {
-			const int i = head + c < m ? head + c : head + c - m;
-			v += w[i] * S[i * n] + w[kLbMaxHist + i] * Y[i * n];
-		}
-		in.d[j] = -v;
-		in.xt[j] = xtj + alpha * -v;
 		return;
 	}
-	in.xt[j] = xj + alpha * in.d[j];
+	if (mine)
+		in.xt[j] = xj + alpha * in.d[j];
 }
 
 static __global__ void lb_brief_kernel(const LbInst *insts, int count, LbBrief *out)
@@ -655,10 +694,14 @@ static inline cudaError_t lb_step(const LbInst *insts, int count, int cap, int m
 	cfg.dynamicSmemBytes = kLbSolveSmem;
 	if ((e = cudaLaunchKernelEx(&cfg, lb_solve_kernel, insts, cap)) != cudaSuccess)
 		return e;
-	cfg.gridDim = dim3((maxn + kLbThreads - 1) / kLbThreads, count);
 	cfg.blockDim = dim3(kLbThreads);
 	cfg.dynamicSmemBytes = 0;
-	return cudaLaunchKernelEx(&cfg, lb_update_kernel, insts);
+	if (count == 1) {
+		cfg.gridDim = dim3((maxn + kLbThreads / 4 - 1) / (kLbThreads / 4), 1);
+		return cudaLaunchKernelEx(&cfg, lb_update_kernel<4>, insts);
+	}
+	cfg.gridDim = dim3((maxn + kLbThreads - 1) / kLbThreads, count);
+	return cudaLaunchKernelEx(&cfg, lb_update_kernel<1>, insts);
 }
 
 }  // namespace cc
