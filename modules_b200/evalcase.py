@@ -1,13 +1,14 @@
 """Evaluate one synthetic stealthy configuration a few times (for profiling a single kernel launch sequence).
 
     python -m modules_b200.evalcase --d 2 --N 20000 --chi 0.2 --evals 3 [--mixed] [--path split|nufft|auto]
-    python -m modules_b200.evalcase --batch 512 --evals 3 [--mixed]
+    python -m modules_b200.evalcase --batch 512 --evals 3 [--mixed] [--autotune]
     python -m modules_b200.evalcase --serve 120
     python -m modules_b200.evalcase --d 3 --N 2000 --chi 0.45 --minimize [--mixed]
 
 The configuration: N uniform random points (seed 1) in a periodic cube of unit density, the CLI's Type 0 k-set.
 With --batch: the seeded batch of uneven instances of the benchmark (modules_b200.workloads.batched_workload),
-evaluated as one batch (the multi-instance kernels) with the default tile shape.
+evaluated as one batch (the fused batch kernel) with the default tile shape, or with --autotune the shape the
+autotuner picks (as the benchmark does).
 With --serve: the seeded served stream of the benchmark (modules_b200.workloads.served_stream: arrivals at 60/s,
 N <= 4000, chi <= 0.40) through modules_b200.serve with 16 iterations per round.
 With --minimize: one L-BFGS minimisation of the configuration to Phi/N < 1e-20 (FP64, or with --mixed the precision
@@ -31,6 +32,7 @@ def main():
     ap.add_argument("--batch", type=int, default=0, help="evaluate the seeded batch of this many instances")
     ap.add_argument("--serve", type=int, default=0, help="serve the seeded stream of this many requests")
     ap.add_argument("--minimize", action="store_true", help="minimise the configuration to its ground state")
+    ap.add_argument("--autotune", action="store_true", help="with --batch: autotune the tile shape first")
     a = ap.parse_args()
     if a.serve > 0:
         from .workloads import served_stream
@@ -44,6 +46,8 @@ def main():
         pots, Ns, fracs, pairs = batched_workload(cc, a.batch)
         batch = cc.CCBatch(pots, Ns)
         batch.set_positions(fracs)
+        if a.autotune:
+            print("tile", batch.autotune(reps=2))
         for _ in range(a.evals):
             E, _F = batch.energy_and_forces(precision=cc.PREC_MIXED if a.mixed else cc.PREC_FP64)
         print(f"batch of {a.batch}: {pairs} particle-k pairs, sum E={float(np.sum(E)):.12e}")
