@@ -565,6 +565,7 @@ int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opt
 		const size_t n = (size_t)b->N[i] * b->h[i]->d;
 		cc::LbInst &l = lbi[i];
 		l.n = (int)n;
+		l.m = m;
 		l.x = ar.at<double>(ox[i]);
 		l.g = ar.at<double>(og[i]);
 		l.d = ar.at<double>(od[i]);

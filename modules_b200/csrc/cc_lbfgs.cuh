@@ -67,6 +67,7 @@ struct LbBrief {
 
 struct LbInst {
 	int n;                  // variables
+	int m;                  // history size (the state's m, here as well so that kernels know it one load earlier)
 	double *x, *g, *d, *xt, *gt;
 	double *S, *Y;          // [m][n] ring
 	double *part;           // [nblk][kLbDots]
@@ -98,17 +99,29 @@ static __global__ void __launch_bounds__(kLbDotsThreads) lb_dots_kernel(const Lb
 	const LbInst in = insts[blockIdx.y];
 	const LbState *st = in.st;
 	const int nblk = lb_blocks(in.n, cap);
-	if (st->status != kLbRunning || (int)blockIdx.x >= nblk)
+	if ((int)blockIdx.x >= nblk)
 		return;
 	constexpr int kWarps = kLbDotsThreads / 32;
-	const int m = st->m, nd = lb_ndots(m);
+	const int m = in.m, nd = lb_ndots(m);
 	const int per = (in.n + nblk - 1) / nblk;
 	const int j0 = blockIdx.x * per, j1 = min(in.n, j0 + per);
 	__shared__ double sgt[kLbThreads], syn[kLbThreads], ssn[kLbThreads];
 	__shared__ double pr[5 * kLbMaxHist];
 	__shared__ double red[kWarps][6];
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	const int count = st->count;
+	// the state's words and the first chunk's values go out together (the values' addresses do not depend on them)
+	const int status = st->status, count = st->count;
+	double v_gt = 0.0, v_g = 0.0, v_xt = 0.0, v_x = 0.0, v_d = 0.0;
+	if (threadIdx.x < min(kLbThreads, j1 - j0)) {
+		const int j = j0 + threadIdx.x;
+		v_gt = in.gt[j];
+		v_g = in.g[j];
+		v_xt = in.xt[j];
+		v_x = in.x[j];
+		v_d = in.d[j];
+	}
+	if (status != kLbRunning)
+		return;
 	double a[6] = {0, 0, 0, 0, 0, 0};
 	for (int k = threadIdx.x; k < 5 * count; k += kLbDotsThreads)
 		pr[k] = 0.0;
@@ -117,8 +130,15 @@ static __global__ void __launch_bounds__(kLbDotsThreads) lb_dots_kernel(const Lb
 		__syncthreads();   // the previous chunk is no longer read
 		if (threadIdx.x < cn) {
 			const int j = c0 + threadIdx.x;
-			const double gt = in.gt[j], yj = gt - in.g[j], sj = in.xt[j] - in.x[j];
-			a[0] += gt * in.d[j];
+			if (c0 != j0) {
+				v_gt = in.gt[j];
+				v_g = in.g[j];
+				v_xt = in.xt[j];
+				v_x = in.x[j];
+				v_d = in.d[j];
+			}
+			const double gt = v_gt, yj = gt - v_g, sj = v_xt - v_x;
+			a[0] += gt * v_d;
 			a[1] += gt * gt;
 			a[2] += sj * yj;
 			a[3] += yj * yj;
@@ -237,7 +257,7 @@ static __global__ void __launch_bounds__(kLbSolveThreads, 2) lb_solve_kernel(con
 	__shared__ double Sg[kLbMaxHist], Yg[kLbMaxHist], t[kLbMaxHist], q[kLbMaxHist], w1[kLbMaxHist];
 	__shared__ int slot[kLbMaxHist];
 	__shared__ int sh_accept;
-	const int status0 = st->status, m = st->m, nd = lb_ndots(m);
+	const int status0 = st->status, m = in.m, nd = lb_ndots(m);
 	const int count = st->count;
 	// the state's scalars (loaded with the status word, and in flight while the partial sums load): every thread
 	// takes the acceptance test and the new pair's slot, thread 0 the rest of the bookkeeping
@@ -260,8 +280,8 @@ static __global__ void __launch_bounds__(kLbSolveThreads, 2) lb_solve_kernel(con
 		stage = st->stage;
 		sched = st->sched;
 	}
-	if (status0 != kLbRunning)
-		return;
+	// The history matrices and the partial sums are loaded before the status word is tested: their addresses do not
+	// depend on it, so all of these loads are in flight together (a finished instance loads them for nothing).
 	// (eight elements of each matrix per thread in flight: a rolled loop would wait for each load before its store)
 	for (int e0 = threadIdx.x; e0 < m * m; e0 += 8 * kLbSolveThreads) {
 		double a[8], b[8], c[8];
@@ -298,6 +318,8 @@ static __global__ void __launch_bounds__(kLbSolveThreads, 2) lb_solve_kernel(con
 		}
 		tot[p] = v;
 	}
+	if (status0 != kLbRunning)
+		return;
 	__syncthreads();
 	const double gtd = tot[5 * m], gtgt = tot[5 * m + 1], sy = tot[5 * m + 2], yy = tot[5 * m + 3],
 	             ygt = tot[5 * m + 4], gtmax = tot[5 * m + 5];

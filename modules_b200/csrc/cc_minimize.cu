@@ -133,6 +133,7 @@ int cc_minimize(cc_handle *h, int64_t N, double *frac, const cc_lbfgs_opts *opts
 	CC_CUDA(cudaMemset(b.d, 0, sizeof(double) * n));
 	cc::LbInst inst;
 	inst.n = n;
+	inst.m = m;
 	inst.x = b.x;
 	inst.g = b.g;
 	inst.d = b.d;

@@ -201,6 +201,7 @@ int fill_slot(const cc_request &r, int idx, int m, const cc::Plan &p, const cc::
 	s.N = N;
 	cc::LbInst &l = s.li;
 	l.n = n;
+	l.m = m;
 	l.x = reinterpret_cast<double *>(b + o_x);
 	l.g = reinterpret_cast<double *>(b + o_g);
 	l.d = reinterpret_cast<double *>(b + o_d);
