@@ -369,6 +369,33 @@ def run_extras(args, cc, torch):
                       "pairs_per_s": pairs / (ms / 1e3), "launches_per_step": 1,
                       "autotuned_tile": {"particles_per_rho_block": tile[0], "segments_per_force_block": tile[1]}}
     del batch
+    # the headline configuration (3D N=2000, chi=0.45) through the same fused batch launch: 128 distinct
+    # configurations of the step's pool per launch (an ensemble evaluated together: independent minimisations or
+    # Monte Carlo chains), positions resident; the headline itself evaluates one configuration after another
+    hbasis = np.eye(D) * SIDE
+    hmodes, hV = cc.stealthy_kset(D, hbasis, N, CHI)
+    HB = 128
+    hb = cc.CCBatch([cc.CCPotential(D, hbasis, hmodes, hV) for _ in range(HB)], [N] * HB)
+    hb.set_positions(list(pool_positions(HB)))
+    htile = hb.autotune(reps=2)
+    with torch.cuda.stream(st):
+        for _ in range(3):
+            hb.eval_device(stream=st.cuda_stream)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(st):
+        a.record(st)
+        for _ in range(reps):
+            hb.eval_device(stream=st.cuda_stream)
+        b.record(st)
+    torch.cuda.synchronize()
+    hms = a.elapsed_time(b) / reps
+    out["batched_headline_config"] = {
+        "workload": f"{HB} configurations of the headline workload (3D N={N} chi={CHI} M={len(hV)}) per fused batch "
+                    "launch, positions resident, FP64",
+        "ms_per_launch": hms, "evals_per_s": HB / (hms / 1e3), "pairs_per_s": HB * N * len(hV) / (hms / 1e3),
+        "autotuned_tile": {"particles_per_rho_block": htile[0], "segments_per_force_block": htile[1]}}
+    del hb
     # ground states per second: the plain single-configuration FP64 path, one instance after another, against the
     # batched minimisation of the same instances (mixed precision until E/N <= 1e-10, then FP64)
     rng = np.random.default_rng(77)
