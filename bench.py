@@ -37,7 +37,10 @@ METRIC = "CC energy+grad evals/s"
 UNIT = "evals/s"
 # DRAM bytes (read + write) per launch of the kernels on this workload, from one ncu capture
 # (profiles/cc_kernels_3d_n2000_ncu.md: dram__bytes_read.sum + dram__bytes_write.sum)
-NCU_TRAFFIC_BYTES = {"cc_force_kernel": 0.144e6, "cc_rho_kernel": 0.078e6, "cc_reduce_kernel": 1.418e6}
+# DRAM bytes (read + write) per launch at this workload from ncu captures with ncu's default cache flush before each
+# pass (cold); with warm caches (--cache-control none) each of the three kernels reads about 256 bytes of DRAM
+NCU_TRAFFIC_BYTES = {"cc_force_kernel": 0.149e6, "cc_rho_kernel": 0.028e6, "cc_reduce_kernel": 1.418e6}
+NCU_L2_BYTES_WARM = {"cc_force_kernel": 5.45e6, "cc_rho_kernel": 3.24e6, "cc_reduce_kernel": 2.23e6}
 WORKLOAD = "3D stealthy CC ground-state evaluation: N=2000 uniform in a periodic cube (unit density), chi=0.45, " \
            "M=2724 half-space k (v=1), FP64 energy + Cartesian forces"
 DATA = "synthetic (seeded uniform positions; k-set of the reference CLI's Type 0 rule)"
@@ -629,7 +632,8 @@ def run_ours(args):
                              "peak_source": "measured in this run: FMA-chain probe kernel (cc_probe_fma_peak); "
                                             "MEASURED_PEAKS.json has no FP64 figure",
                              "flops_per_launch": fl, "launch_ms": tk, "traffic": NCU_TRAFFIC_BYTES.get(dom),
-                             "traffic_unit": "bytes per launch (ncu capture)", "kernel_ms": kernel_ms,
+                             "traffic_unit": "DRAM bytes per launch (ncu capture, cold caches; warm: ~256 B)",
+                             "l2_bytes_warm": NCU_L2_BYTES_WARM.get(dom), "kernel_ms": kernel_ms,
                              "timing": "CUDA events around each kernel inside a replayed graph; under programmatic "
                                        "dependent launch consecutive kernels overlap, so the intervals overlap and "
                                        "sum to more than the evaluation",
