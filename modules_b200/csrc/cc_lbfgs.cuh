@@ -11,8 +11,9 @@
 //
 // One iteration on the device (every instance of a batch at once, blockIdx.y = instance):
 //   evaluation at x_trial -> E_t, g_t;  lb_dots: block partials of the dot products;
-//   lb_solve (one block per instance): totals in block order, accept / reject, history matrices, the small solves,
-//     the next step length and the stop tests;  lb_update: history insert, x, g, the new direction and x_trial.
+//   lb_solve (one block per instance): totals in block order, accept / reject, history matrices and R^-1 (kept
+//     with the history: a column per new pair), the products of the compact form, the next step length and the stop
+//     tests;  lb_update: history insert, x, g, the new direction and x_trial.
 // Every sum has a fixed order, so a run repeats bitwise.
 #pragma once
 #include <cuda_runtime.h>
