@@ -623,7 +623,7 @@ int cc_batch_minimize(cc_batch *b, double *const *frac, const cc_lbfgs_opts *opt
 		for (int it = 0; it < o.iters_per_check; it++) {
 			if (int r2 = batch_eval(b, 1, prec, st))
 				return r2;
-			CC_CUDA(cc::lb_step(b->d_lb, count, nblk, maxn, st));
+			CC_CUDA(cc::lb_step(b->d_lb, count, nblk, maxn, st, count == 1 ? &lbo[0] : nullptr));
 			CC_CUDA(cudaGetLastError());
 		}
 		return CC_OK;

@@ -123,6 +123,7 @@ struct LbBuffers {
 	double *part = nullptr;
 	cc::LbState *st = nullptr;
 	cc::LbInst *inst = nullptr;
+	cc::LbInst host_inst{};   // the host copy of *inst (passed in the L-BFGS kernels' parameters)
 	void release()
 	{
 		cudaFree(x);

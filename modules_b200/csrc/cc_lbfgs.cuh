@@ -94,10 +94,10 @@ constexpr int kLbMaxBlocks = 64;   // cap of the batched minimisation and the se
 // parallel across warps instead of one pair after another. Sums have a fixed order (lanes by a fixed tree, chunks in
 // order, warps in order for the non-pair products), so a run repeats bitwise.
 constexpr int kLbDotsThreads = 2 * kLbThreads;   // a chunk of kLbThreads variables; twice as many warps over the pairs
-static __global__ void __launch_bounds__(kLbDotsThreads) lb_dots_kernel(const LbInst *insts, int cap)
+static __global__ void __launch_bounds__(kLbDotsThreads) lb_dots_kernel(const LbInst *insts, int cap, LbInst one)
 {
 	cudaGridDependencySynchronize();   // launched early (programmatic dependent launch): the evaluation is complete
-	const LbInst in = insts[blockIdx.y];
+	const LbInst in = insts ? insts[blockIdx.y] : one;
 	const LbState *st = in.st;
 	const int nblk = lb_blocks(in.n, cap);
 	if ((int)blockIdx.x >= nblk)
@@ -244,10 +244,10 @@ constexpr size_t kLbSolveSmem = 3 * sizeof(double) * kLbMaxHist * kLbMaxHist;
 // dependent steps. The kernel is a chain of dependent phases, so its global reads are issued together up front: the
 // partial sums, the state's scalars (thread 0) and the history matrices, which the block keeps in shared memory and
 // updates there as well.
-static __global__ void __launch_bounds__(kLbSolveThreads, 2) lb_solve_kernel(const LbInst *insts, int cap)
+static __global__ void __launch_bounds__(kLbSolveThreads, 2) lb_solve_kernel(const LbInst *insts, int cap, LbInst one)
 {
 	cudaGridDependencySynchronize();
-	const LbInst in = insts[blockIdx.x];
+	const LbInst in = insts ? insts[blockIdx.x] : one;
 	LbState *st = in.st;
 	const int nblk = lb_blocks(in.n, cap);
 	extern __shared__ double lb_smem[];
@@ -604,10 +604,10 @@ __device__ __forceinline__ double lb_quarter(const double *__restrict__ S, const
 	return v;
 }
 template <int LANES>
-static __global__ void __launch_bounds__(kLbThreads, LANES == 1 ? 4 : 2) lb_update_kernel(const LbInst *insts)
+static __global__ void __launch_bounds__(kLbThreads, LANES == 1 ? 4 : 2) lb_update_kernel(const LbInst *insts, LbInst one)
 {
 	cudaGridDependencySynchronize();
-	const LbInst in = insts[blockIdx.y];
+	const LbInst in = insts ? insts[blockIdx.y] : one;
 	const LbState *st = in.st;
 	const int status = st->status, accepted = st->accepted;
 	if (status != kLbRunning && !(accepted && status != kLbLineSearch))
@@ -694,8 +694,14 @@ static __global__ void lb_brief_kernel(const LbInst *insts, int count, LbBrief *
 // The three kernels of one L-BFGS step on stream st for `count` instances (insts), at most `cap` dot-product blocks
 // per instance and `maxn` variables in the largest one. Each is launched with programmatic stream serialisation:
 // it is scheduled while the previous kernel drains and waits for it (cudaGridDependencySynchronize) before it reads.
-static inline cudaError_t lb_step(const LbInst *insts, int count, int cap, int maxn, cudaStream_t st)
+// With one instance and its descriptor on the host (`one`), the descriptor goes in the kernels' parameters instead
+// of being read from device memory (one dependent load fewer at the start of each kernel).
+static inline cudaError_t lb_step(const LbInst *insts, int count, int cap, int maxn, cudaStream_t st,
+                                  const LbInst *one = nullptr)
 {
+	const LbInst o = one && count == 1 ? *one : LbInst{};
+	if (one && count == 1)
+		insts = nullptr;
 	static const cudaError_t smem_attr = cudaFuncSetAttribute(
 	    lb_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLbSolveSmem);
 	if (smem_attr != cudaSuccess)
@@ -709,22 +715,22 @@ static inline cudaError_t lb_step(const LbInst *insts, int count, int cap, int m
 	cfg.numAttrs = 1;
 	cfg.gridDim = dim3(cap, count);
 	cfg.blockDim = dim3(kLbDotsThreads);
-	cudaError_t e = cudaLaunchKernelEx(&cfg, lb_dots_kernel, insts, cap);
+	cudaError_t e = cudaLaunchKernelEx(&cfg, lb_dots_kernel, insts, cap, o);
 	if (e != cudaSuccess)
 		return e;
 	cfg.gridDim = dim3(count);
 	cfg.blockDim = dim3(kLbSolveThreads);
 	cfg.dynamicSmemBytes = kLbSolveSmem;
-	if ((e = cudaLaunchKernelEx(&cfg, lb_solve_kernel, insts, cap)) != cudaSuccess)
+	if ((e = cudaLaunchKernelEx(&cfg, lb_solve_kernel, insts, cap, o)) != cudaSuccess)
 		return e;
 	cfg.blockDim = dim3(kLbThreads);
 	cfg.dynamicSmemBytes = 0;
 	if (count == 1) {
 		cfg.gridDim = dim3((maxn + kLbThreads / 4 - 1) / (kLbThreads / 4), 1);
-		return cudaLaunchKernelEx(&cfg, lb_update_kernel<4>, insts);
+		return cudaLaunchKernelEx(&cfg, lb_update_kernel<4>, insts, o);
 	}
 	cfg.gridDim = dim3((maxn + kLbThreads - 1) / kLbThreads, count);
-	return cudaLaunchKernelEx(&cfg, lb_update_kernel<1>, insts);
+	return cudaLaunchKernelEx(&cfg, lb_update_kernel<1>, insts, o);
 }
 
 }  // namespace cc

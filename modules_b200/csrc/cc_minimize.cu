@@ -37,7 +37,7 @@ int lb_iteration(cc_handle *h, int64_t N, LbBuffers &b, int n, int nblk, int pre
 {
 	if (int rc = handle_eval(h, N, b.xt, &b.st->Et, nullptr, b.gt, false, prec, st))
 		return rc;
-	CC_CUDA(cc::lb_step(b.inst, 1, nblk, n, st));
+	CC_CUDA(cc::lb_step(b.inst, 1, nblk, n, st, &b.host_inst));
 	CC_CUDA(cudaGetLastError());
 	return CC_OK;
 }
@@ -144,6 +144,7 @@ int cc_minimize(cc_handle *h, int64_t N, double *frac, const cc_lbfgs_opts *opts
 	inst.part = b.part;
 	inst.st = b.st;
 	CC_CUDA(cudaMemcpy(b.inst, &inst, sizeof(inst), cudaMemcpyHostToDevice));
+	b.host_inst = inst;
 	// warm-up evaluations allocate the evaluation's work buffers before any capture
 	const bool sched = o.precision == CC_PREC_SCHEDULE;
 	const int prec0 = (o.precision == CC_PREC_FP64) ? CC_PREC_FP64 : CC_PREC_MIXED;

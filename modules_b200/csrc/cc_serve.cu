@@ -507,7 +507,7 @@ extern "C" int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *
 				s_err = std::string("serve: ") + cc_last_error();
 				break;
 			}
-			if (cc::lb_step(d_li, A, nblk, maxn, st) != cudaSuccess)
+			if (cc::lb_step(d_li, A, nblk, maxn, st, A == 1 ? &li[0] : nullptr) != cudaSuccess)
 				rc = sfail(CC_ERR_CUDA, "serve: kernel launch failed");
 		}
 		if (rc)
