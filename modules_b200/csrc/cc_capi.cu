@@ -1094,8 +1094,9 @@ int eval_device(cc_handle *h, int64_t N, const double *d_frac, double *d_E, doub
 }
 
 // cc_energy_grad as one CUDA graph: the rho / reduce / force kernels (the rho kernel reading the staged positions from
-// mapped pinned memory) writing E and F into mapped pinned memory. A key is captured on its second consecutive use with no allocation in between (the first,
-// direct evaluation makes every allocation the launch needs); *done tells whether the graph ran.
+// mapped pinned memory) writing E and F into mapped pinned memory. A key is captured on its second consecutive use
+// with no allocation in between (the first, direct evaluation makes every allocation the launch needs); *done tells
+// whether the graph ran.
 int launch_eval_graph(cc_handle *h, int64_t N, int precision, int forces, bool *done)
 {
 	*done = false;

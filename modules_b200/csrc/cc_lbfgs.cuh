@@ -580,7 +580,7 @@ static __global__ void __launch_bounds__(kLbSolveThreads, 2) lb_solve_kernel(con
 // the variable's values are loaded up front (the stores below may alias them as far as the compiler knows, which
 // would otherwise order every load after them).
 constexpr int kLbUpdPairs = kLbMaxHist / 4;   // pairs per quarter at most
-template <int LANES>
+// quarter q of the history sum on one lane, all of its pairs' loads at once
 __device__ __forceinline__ double lb_quarter(const double *__restrict__ S, const double *__restrict__ Y,
                                              const double *__restrict__ w, size_t n, int head, int m, int count,
                                              int q, double v)
@@ -604,7 +604,8 @@ __device__ __forceinline__ double lb_quarter(const double *__restrict__ S, const
 	return v;
 }
 template <int LANES>
-static __global__ void __launch_bounds__(kLbThreads, LANES == 1 ? 4 : 2) lb_update_kernel(const LbInst *insts, LbInst one)
+static __global__ void __launch_bounds__(kLbThreads, LANES == 1 ? 4 : 2)
+    lb_update_kernel(const LbInst *insts, LbInst one)
 {
 	cudaGridDependencySynchronize();
 	const LbInst in = insts ? insts[blockIdx.y] : one;
@@ -638,7 +639,7 @@ static __global__ void __launch_bounds__(kLbThreads, LANES == 1 ? 4 : 2) lb_upda
 		const size_t n = (size_t)in.n;
 		double v;
 		if constexpr (LANES == 4) {
-			v = lb_quarter<4>(S, Y, w, n, head, m, count, sub, sub == 0 ? gamma * gt : 0.0);
+			v = lb_quarter(S, Y, w, n, head, m, count, sub, sub == 0 ? gamma * gt : 0.0);
 			v += __shfl_xor_sync(0xffffffffu, v, 1);
 			v += __shfl_xor_sync(0xffffffffu, v, 2);
 		} else {
