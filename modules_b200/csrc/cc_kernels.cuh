@@ -850,10 +850,11 @@ template <typename C> __host__ __device__ constexpr size_t force_smem_bytes(int 
 	           : (size_t)kForceWarps * 32 * d * sizeof(double);
 }
 
-// Grid (ceil(N/32), nksplit). Block = 32 particles (lanes) x 8 warps striding over the split's segments; the tables of
-// the block's particles for the split are built once (entry-major, so a warp reads 32 consecutive entries). The slot
-// weights u of up to kForceUChunk segments at a time are staged in shared memory in the compute type (slot-major, so a
-// warp's read of one weight is a broadcast).
+// Grid (ceil(N/32), nksplit). Block = 32 particles (lanes) x 8 warps, each warp on a contiguous run of the split's
+// segments; the tables of the block's particles for the split are built once (entry-major, so a warp reads 32
+// consecutive entries). The slot weights u of up to kForceUChunk segments at a time are staged in shared memory in the
+// compute type (a warp's read of one weight is a broadcast): FP64 slot-major, mixed segment-major with each pair of
+// components swapped and signed for the sign-free FP32 recurrence.
 template <int D, int L, bool MIXED>
 __device__ __forceinline__ void force_body(const ForceArgs &a, const int pgroup, const int ks, const ItemCtl ctl)
 {
