@@ -74,3 +74,33 @@ def test_precision_schedule_reaches_ground_state(gpu):
                                             precision=gpu.PREC_SCHEDULE, switch_energy_per_particle=1e-10)
     print(f"3D N=2000 schedule: E={E:.3e} evals={evals} iters={iters} status={status}")
     assert E / N < 1e-20
+
+
+@pytest.mark.parametrize("history", [3, 64])
+def test_ground_state_history_sizes(gpu, history):
+    """The history at its smallest sizes (the ring wraps every few iterations) and at its largest (64 pairs, four
+    full quarters of the update's history sum): alone and in a batch the configuration reaches its ground state,
+    the reference's FP64 energy of the result agrees, and the batch of one ends bitwise where the mixed batch does
+    (one instance takes the four-lane update, a batch the one-lane one: the same arithmetic)."""
+    r = load_golden("stealthy_2d_n100")
+    mref = load_golden("min_2d_n100")
+    N = 100
+    p = gpu.CCPotential(2, r["basis"], r["modes"], r["V"])
+    x, E, evals, iters, status = p.minimize(mref["frac0"], stopval=1e-20 * N, history=history)
+    print(f"history {history}: E={E:.3e} evals={evals} status={status}")
+    assert E / N < 1e-20
+    ref = oracle.Ref(2, r["basis"], r["V"], modes=r["modes"])
+    ref.set_positions(x)
+    Eref, _, _, _ = ref.eval(forces=False)
+    assert Eref / N < 1e-20
+    # in a batch with another instance, and alone in a batch of one
+    basis2 = np.eye(3) * 300 ** (1.0 / 3.0)
+    modes2, V2 = gpu.stealthy_kset(3, basis2, 300, 0.2, 3)
+    other = gpu.CCPotential(3, basis2, modes2, V2)
+    f2 = np.random.default_rng(4).random((300, 3))
+    mix = gpu.CCBatch([p, other], [N, 300])
+    xs, Es, es, its, sts = mix.minimize([mref["frac0"], f2], history=history)
+    assert np.all(Es / np.array([N, 300]) < 1e-20)
+    one = gpu.CCBatch([p], [N])
+    xa, Ea, ea, ia, sa = one.minimize([mref["frac0"]], history=history)
+    assert np.array_equal(xa[0], xs[0]) and Ea[0] == Es[0] and ea[0] == es[0]
