@@ -35,6 +35,30 @@ def test_batch_matches_each_instance(gpu):
         assert np.abs(fb - f1).max() <= 1e-10 * np.abs(f1).max()
 
 
+def test_batch_ensemble_of_one_potential(gpu):
+    """Many configurations of one potential in one fused launch (the ensemble form of the benchmark's
+    configuration): each instance's energy and forces equal those of the same instance in a batch of one, bitwise,
+    and agree with the three-kernel evaluation of the potential to rounding."""
+    d, n, chi = 3, 400, 0.40
+    basis = np.eye(d) * n ** (1.0 / d)
+    modes, V = gpu.stealthy_kset(d, basis, n, chi)
+    B = 24
+    pots = [gpu.CCPotential(d, basis, modes, V) for _ in range(B)]
+    fracs = list(np.random.default_rng(21).random((B, n, d)))
+    ens = gpu.CCBatch(pots, [n] * B)
+    ens.set_positions(fracs)
+    E, F = ens.energy_and_forces()
+    for k in (0, 7, B - 1):
+        one = gpu.CCBatch([pots[k]], [n])
+        one.set_positions([fracs[k]])
+        e1, f1 = one.energy_and_forces()
+        assert e1[0] == E[k] and np.array_equal(f1[0], F[k])
+        pots[k].set_configuration(fracs[k])
+        e2, f2 = pots[k].energy_and_forces()
+        assert abs(E[k] - e2) <= 1e-10 * abs(e2)
+        assert np.abs(F[k] - f2).max() <= 1e-10 * np.abs(f2).max()
+
+
 def test_batch_golden_parity(gpu):
     """A batch of the golden cases (1D-3D, skew cells, repeated modes) against the reference's results."""
     names = ["lattice_1d", "lattice_2d_skew", "lattice_3d_skew", "weighted_3d_n300", "stealthy_3d_n2000"]
