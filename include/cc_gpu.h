@@ -339,6 +339,15 @@ int cc_set_path(cc_handle *h, int path);
  * handle under its current cc_set_path choice. */
 int cc_eval_path(cc_handle *h, int64_t N, int precision, int *path);
 
+/* on = 1: the caller promises that the positions given to cc_energy_grad_device on this handle were complete before
+ * the kernel enqueued just before the call on its stream, and that no work in flight writes them (for example a pool
+ * of resident configurations evaluated one after another). The rho kernel of such an evaluation then runs its
+ * tables and phase sums while the previous kernel on the stream drains, and waits for that kernel only before it
+ * writes its partial rows. Results are bitwise those of on = 0 (the default, for positions that a kernel just before
+ * the call produced, such as an optimiser's update). Only the split path's rho kernel of cc_energy_grad_device
+ * uses it; every other entry point ignores it. No counterpart in the reference (one evaluation per call there). */
+int cc_set_independent_positions(cc_handle *h, int on);
+
 /* Synchronise the device and report a CUDA error of an earlier device-path evaluation (no kernel of a handle waits
  * on another block, so there is no timeout to report here). */
 int cc_check_device_error(cc_handle *h);

@@ -97,6 +97,7 @@ _SIGS = {
     "cc_isotropic_structure_factor": (_i, [_i, _i64, _vp, _vp, _vp, _d, _d, _d, _d, _i, _d, _vp, _i64,
                                            ctypes.POINTER(_i64)]),
     "cc_set_timing": (_i, [_vp, _i]),
+    "cc_set_independent_positions": (_i, [_vp, _i]),
     "cc_get_timing": (_i, [_vp, ctypes.POINTER(_d), ctypes.POINTER(_d), ctypes.POINTER(_d), ctypes.POINTER(_i64)]),
     "cc_plan_info": (_i, [_vp, _i64, ctypes.POINTER(_i), ctypes.POINTER(_i64), ctypes.POINTER(_i),
                           ctypes.POINTER(_i)]),
@@ -437,6 +438,12 @@ class CCPotential:
 
     def check_device_error(self):
         _check(self._lib.cc_check_device_error(self._h))
+
+    def set_independent_positions(self, on=True):
+        """Promise that positions given to energy_grad_device were complete before the kernel enqueued just before
+        each call and that nothing in flight writes them (a pool of resident configurations): the rho kernel then
+        overlaps its phase sums with the previous kernel's tail. Results are bitwise those of the default (off)."""
+        _check(self._lib.cc_set_independent_positions(self._h, 1 if on else 0))
 
     def set_timing(self, on):
         _check(self._lib.cc_set_timing(self._h, 1 if on else 0))

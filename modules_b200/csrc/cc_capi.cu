@@ -544,6 +544,7 @@ int run_rho(cc_handle *h, DevKSet &k, int64_t N, const double *d_frac, double *d
 	a.partial = k.partial;
 	a.skip = h->d_skip;
 	a.frac_copy = (&k == &h->main) ? h->rho_copy : nullptr;
+	a.early = (h->early_call && &k == &h->main && !a.skip && !a.frac_copy) ? 1 : 0;
 	if (int rc = launch_rho(h->d, a, mixed, p.nbgroups(), nsplit, csize, p.block_max_row, st))
 		return rc;
 	if (after_rho)
@@ -1509,7 +1510,10 @@ int cc_energy_grad_device(cc_handle *h, int64_t N, const double *d_frac, double 
 		if (int rc = ensure_particles(h, N))
 			return rc;
 	cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : h->stream;
-	return eval_device(h, N, d_frac, d_E, d_F, d_gfrac, false, precision, st);
+	h->early_call = h->independent;
+	const int rc = eval_device(h, N, d_frac, d_E, d_F, d_gfrac, false, precision, st);
+	h->early_call = false;
+	return rc;
 }
 
 int cc_rho(cc_handle *h, double *re, double *im, int precision)
@@ -1741,6 +1745,14 @@ int cc_set_timing(cc_handle *h, int on)
 	h->timing = on != 0;
 	if (on)
 		h->ev_used = 0;   // switching on starts a new record; switching off keeps it for cc_get_timing
+	return CC_OK;
+}
+
+int cc_set_independent_positions(cc_handle *h, int on)
+{
+	if (int rc = check_handle(h))
+		return rc;
+	h->independent = on != 0;
 	return CC_OK;
 }
 

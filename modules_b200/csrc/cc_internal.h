@@ -260,6 +260,8 @@ struct cc_handle {
 	bool mc_valid = false, mc_pending = false;
 	const int *d_skip = nullptr;    // evaluations do nothing while *d_skip != 0 (set by cc_minimize)
 	bool timing = false;            // cc_set_timing
+	bool independent = false;       // cc_set_independent_positions
+	bool early_call = false;        // set for the duration of a cc_energy_grad_device call when independent
 	// cc_minimize's state, kept between calls so that a minimisation makes no allocation call into the CUDA driver
 	// once the handle has run one of its size: FP64 / mixed buffers (capacities n variables, m pairs, nblk dot
 	// blocks) and the batch of one that runs the precision schedule (for sched_N particles)

@@ -385,6 +385,9 @@ struct RhoArgs {
 	int want_stage;
 	double *frac_copy;        // if not null, the blocks of block group 0 also store their particles' coordinates
 	                          // there (frac is then host memory the kernels that follow do not read)
+	int early;                // nonzero: frac was complete before the previous kernel on the stream was enqueued and
+	                          // nothing in flight writes it, so the blocks run their main loop before waiting for
+	                          // that kernel (skip, stage and frac_copy are then null)
 };
 
 constexpr int kRhoWarps = 8;
@@ -415,7 +418,9 @@ __device__ __forceinline__ void rho_body(const RhoArgs &a, const int bg, const i
 	const Seg sg = a.segs[q];
 	const int j0 = min(a.N, split * a.per_split);
 	const int j1 = min(a.N, j0 + a.per_split);
-	cudaGridDependencySynchronize();   // inputs of this step are complete (programmatic dependent launch)
+	// inputs of this step are complete (programmatic dependent launch); with a.early only the partial rows wait
+	if (!a.early)
+		cudaGridDependencySynchronize();
 	if (eval_skipped(a.skip, ctl.stage, ctl.want_stage))   // uniform over the instance: no block reaches a cluster barrier
 		return;
 	if (a.frac_copy && bg == 0)
@@ -538,6 +543,10 @@ __device__ __forceinline__ void rho_body(const RhoArgs &a, const int bg, const i
 			acc[r].y = (double)accC[r].y;
 		}
 	}
+	// Early mode: the sums above read only positions and the k-set; the partial rows below are still read by the
+	// previous evaluation's reduce kernel until the previous kernel on the stream has completed.
+	if (a.early)
+		cudaGridDependencySynchronize();
 	cudaTriggerProgrammaticLaunchCompletion();   // the next kernel may be scheduled; it waits for this grid
 
 	if constexpr (!CLUSTER) {

@@ -201,6 +201,52 @@ def test_device_path_matches_host(gpu):
     assert np.abs(d_g.cpu().numpy() - gref).max() <= 1e-12 * np.abs(gref).max()
 
 
+def test_independent_positions_bitwise(gpu):
+    """A pool of resident configurations evaluated back to back with cc_set_independent_positions (the rho kernel
+    runs its phase sums before waiting for the previous kernel on the stream), eagerly and replayed from a CUDA
+    graph, gives bitwise the energies and forces of one synchronised evaluation at a time without it."""
+    torch = pytest.importorskip("torch")
+    r = load_golden("stealthy_3d_n2000")
+    p = make_pot(gpu, r)
+    n, d = r["frac"].shape
+    rng = np.random.default_rng(5)
+    pool_h = [np.mod(r["frac"] + rng.normal(0.0, 0.02, r["frac"].shape), 1.0) for _ in range(6)]
+    pool = [torch.tensor(x, dtype=torch.float64, device="cuda") for x in pool_h]
+    P = len(pool)
+    E = torch.zeros(3, P, dtype=torch.float64, device="cuda")
+    F = torch.zeros(3, P, n, d, dtype=torch.float64, device="cuda")
+    st = torch.cuda.Stream()
+
+    def run(rnd, i):
+        p.energy_grad_device(n, pool[i].data_ptr(), E[rnd, i:i + 1].data_ptr(), F[rnd, i].data_ptr(),
+                             stream=torch.cuda.current_stream().cuda_stream)
+
+    with torch.cuda.stream(st):
+        for i in range(P):   # one at a time, default ordering
+            run(0, i)
+            torch.cuda.synchronize()
+        p.set_independent_positions(True)
+        for i in range(P):   # back to back, early rho
+            run(1, i)
+        for i in range(P):
+            run(1, i)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=st):
+        for i in range(P):
+            run(2, i)
+    for _ in range(3):
+        g.replay()
+    torch.cuda.synchronize()
+    del g
+    p.set_independent_positions(False)
+    assert torch.equal(E[1], E[0]) and torch.equal(F[1], F[0])
+    assert torch.equal(E[2], E[0]) and torch.equal(F[2], F[0])
+    p.set_configuration(pool_h[0])
+    E0, F0 = p.energy_and_forces()
+    assert E[1, 0].item() == E0 and np.array_equal(F[1, 0].cpu().numpy(), F0)
+
+
 def test_mixed_precision_error(gpu):
     """Mixed path (FP32 seeds and recurrences, FP64 partials) against the FP64 path: report and bound the error."""
     r = load_golden("stealthy_3d_n2000")
