@@ -240,6 +240,17 @@ typedef struct {
 int cc_serve(const cc_request *reqs, int count, const cc_serve_opts *opts, cc_request_result *results, double *wall_s);
 const char *cc_serve_last_error(void);
 
+/* Many configurations from host memory in one call: frac (P x N x d fractional coordinates, host), E (P energies,
+ * host) and F (P x N x d Cartesian forces, host, may be NULL). The same results, bitwise, as P calls of
+ * cc_set_positions + cc_energy_grad (coordinates outside [0,1) are wrapped the same way; a non-finite one fails the
+ * call with CC_ERR_ARG). The positions go to the device in chunks of 64 configurations on a second stream while
+ * earlier chunks are evaluated, and the evaluations follow one another without host synchronisation (each rho kernel
+ * overlaps the previous evaluation's force kernel); pinned host buffers (cudaHostAlloc, cudaHostRegister) let the
+ * copies overlap. The call returns when E and F are written. Every configuration of a call is resident on the
+ * device at once (2 P N d doubles). Replaces a loop of the reference's SetConfiguration + Energy + AllForce over
+ * configurations (potential/CollectiveCoordinatePotential.h:1351-1448). */
+int cc_energy_grad_many(cc_handle *h, int64_t P, int64_t N, const double *frac, double *E, double *F, int precision);
+
 /* Device-resident evaluation: d_frac (N x d, device), outputs d_E (1 double) and d_F (N x d Cartesian, may be
  * NULL) and d_gfrac (N x d gradient of the energy with respect to the fractional coordinates, may be NULL), all on
  * the device, enqueued on `stream` (a cudaStream_t; NULL = the handle's stream). No host synchronisation. */

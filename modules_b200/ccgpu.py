@@ -87,6 +87,7 @@ _SIGS = {
     "cc_structure_factor": (_i, [_vp, _i64, _vp, _vp, _i]),
     "cc_objective": (_i, [_vp, _i64, _vp, _d, ctypes.POINTER(_d), _vp, _i]),
     "cc_energy_grad_device": (_i, [_vp, _i64, _vp, _vp, _vp, _vp, _i, _vp]),
+    "cc_energy_grad_many": (_i, [_vp, _i64, _i64, _vp, _vp, _vp, _i]),
     "cc_kset_stealthy": (_i, [_i, _vp, _i64, _d, _i, _i64, _vp, _vp, ctypes.POINTER(_i64)]),
     "cc_kset_isotropic": (_i, [_i, _vp, _d, _d, _d, _d, _i64, _vp, _vp, ctypes.POINTER(_i64)]),
     "cc_multi_create": (_i, [_i, _vp, _i, _vp, _vp, _vp, _d, _d, ctypes.POINTER(_vp)]),
@@ -459,6 +460,25 @@ class CCPotential:
         _check(self._lib.cc_plan_info(self._h, int(N), ctypes.byref(L), ctypes.byref(nseg), ctypes.byref(ns),
                                       ctypes.byref(nk)))
         return dict(L=L.value, nseg=nseg.value, nsplit=ns.value, nksplit=nk.value)
+
+    def energy_grad_many(self, frac, E=None, F=None, precision=PREC_FP64, forces=True):
+        """Energies and forces of many configurations from host memory in one call: frac is (P, N, d). E (P,) and F
+        (P, N, d) are filled when given (pass arrays in pinned memory, e.g. numpy views of pinned torch tensors, for
+        copies that overlap the evaluations), else allocated. Bitwise the results of P set_configuration +
+        energy_and_forces calls. Returns (E, F)."""
+        if frac.dtype != np.float64 or not frac.flags.c_contiguous:
+            frac = np.ascontiguousarray(frac, dtype=np.float64)
+        P, N = frac.shape[0], frac.shape[1]
+        if E is None:
+            E = np.empty(P)
+        if forces and F is None:
+            F = np.empty((P, N, self.d))
+        for a, n in ((E, P), (F if forces else None, P * N * self.d)):
+            if a is not None and (a.dtype != np.float64 or not a.flags.c_contiguous or a.size != n):
+                raise ValueError("E must be a contiguous float64 array of P values and F of P x N x d")
+        _check(self._lib.cc_energy_grad_many(self._h, P, N, _ptr(frac), _ptr(E), _ptr(F) if forces else None,
+                                             precision))
+        return E, (F if forces else None)
 
     def energy_grad_device(self, N, d_frac, d_E, d_F=None, d_gfrac=None, precision=PREC_FP64, stream=None):
         """Enqueue one evaluation on device pointers (ints); no synchronisation."""

@@ -1387,6 +1387,16 @@ int cc_destroy(cc_handle *h)
 		cufftDestroy(h->nu_p2);
 	for (void *b : h->nu_bufs)
 		cudaFree(b);
+	if (h->copy_stream)
+		cudaStreamSynchronize(h->copy_stream);
+	cudaFree(h->d_many_in);
+	cudaFree(h->d_many_F);
+	cudaFree(h->d_many_E);
+	cudaFree(h->d_many_bad);
+	for (cudaEvent_t e : h->many_ev)
+		cudaEventDestroy(e);
+	if (h->copy_stream)
+		cudaStreamDestroy(h->copy_stream);
 	if (h->stream)
 		cudaStreamDestroy(h->stream);
 	delete h;
@@ -1514,6 +1524,133 @@ int cc_energy_grad_device(cc_handle *h, int64_t N, const double *d_frac, double 
 	const int rc = eval_device(h, N, d_frac, d_E, d_F, d_gfrac, false, precision, st);
 	h->early_call = false;
 	return rc;
+}
+
+// Positions of cc_energy_grad_many brought into [0, 1) with cc_set_positions' operations (so the results are the
+// same bitwise); a non-finite coordinate is replaced by 0, so that no kernel sees it, and reported through *bad.
+static __global__ void cc_wrap_many_kernel(double *x, int64_t n, int *bad)
+{
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+		const double v = x[i];
+		if (v >= 0.0 && v < 1.0)
+			continue;
+		if (!isfinite(v)) {
+			x[i] = 0.0;
+			*bad = 1;
+			continue;
+		}
+		double w = v - floor(v);
+		w -= floor(w);
+		x[i] = w;
+	}
+}
+
+constexpr int64_t kManyChunk = 64;   // configurations per host<->device copy of cc_energy_grad_many
+
+static int many_buffers(cc_handle *h, int64_t P, size_t total, int64_t nch)
+{
+	if (total > h->many_cap) {
+		cudaFree(h->d_many_in);
+		cudaFree(h->d_many_F);
+		h->d_many_in = h->d_many_F = nullptr;
+		h->many_cap = 0;
+		if (int rc = dev_alloc(&h->d_many_in, total))
+			return rc;
+		if (int rc = dev_alloc(&h->d_many_F, total))
+			return rc;
+		h->many_cap = total;
+	}
+	if ((size_t)P > h->many_ecap) {
+		cudaFree(h->d_many_E);
+		h->d_many_E = nullptr;
+		h->many_ecap = 0;
+		if (int rc = dev_alloc(&h->d_many_E, (size_t)P))
+			return rc;
+		h->many_ecap = (size_t)P;
+	}
+	if (!h->d_many_bad)
+		if (int rc = dev_alloc(&h->d_many_bad, 1))
+			return rc;
+	if (!h->copy_stream)
+		CC_CUDA(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+	while ((int64_t)h->many_ev.size() < 2 * nch) {
+		cudaEvent_t e = nullptr;
+		CC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+		h->many_ev.push_back(e);
+	}
+	return CC_OK;
+}
+
+int cc_energy_grad_many(cc_handle *h, int64_t P, int64_t N, const double *frac, double *E, double *F, int precision)
+{
+	if (int rc = check_handle(h))
+		return rc;
+	if (int rc = check_prec(precision))
+		return rc;
+	if (P < 0 || N < 0 || N > ((int64_t)1 << 31) - 64 || (P > 0 && (!E || (N > 0 && !frac))))
+		return fail(CC_ERR_ARG, "invalid configuration count, particle count or buffers");
+	if (N % h->nsub)
+		return fail(CC_ERR_ARG, "the particle count is not a multiple of the number of sub-configurations");
+	if (P == 0)
+		return CC_OK;
+	const size_t per = (size_t)N * h->d, total = (size_t)P * per;
+	const int64_t nch = (P + kManyChunk - 1) / kManyChunk;
+	if ((size_t)std::max<int64_t>(N, 1) > h->ncap)
+		if (int rc = ensure_particles(h, N))
+			return rc;
+	if (int rc = many_buffers(h, P, total, nch))
+		return rc;
+	cudaStream_t st = h->stream, cp = h->copy_stream;
+	CC_CUDA(cudaMemsetAsync(h->d_many_bad, 0, sizeof(int), st));
+	// the copy stream starts after the handle's earlier work (which may still read these buffers)
+	CC_CUDA(cudaEventRecord(h->many_ev[1], st));
+	CC_CUDA(cudaStreamWaitEvent(cp, h->many_ev[1], 0));
+	int rc = CC_OK;
+	for (int64_t c = 0; c < nch && rc == CC_OK; c++) {
+		const int64_t p0 = c * kManyChunk, p1 = std::min(P, p0 + kManyChunk);
+		const size_t n = (size_t)(p1 - p0) * per;
+		cudaEvent_t in = h->many_ev[2 * c], done = h->many_ev[2 * c + 1];
+		if (n)
+			CC_CUDA(cudaMemcpyAsync(h->d_many_in + p0 * per, frac + p0 * per, n * sizeof(double), cudaMemcpyHostToDevice,
+			                        cp));
+		CC_CUDA(cudaEventRecord(in, cp));
+		CC_CUDA(cudaStreamWaitEvent(st, in, 0));
+		if (n) {
+			const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 4 * 148);
+			cc_wrap_many_kernel<<<blocks, 256, 0, st>>>(h->d_many_in + p0 * per, (int64_t)n, h->d_many_bad);
+			CC_CUDA(cudaGetLastError());
+		}
+		for (int64_t p = p0; p < p1 && rc == CC_OK; p++) {
+			// after the chunk's first evaluation (which waits for the wrap kernel) the positions are complete before
+			// the kernel just before each rho kernel: the rho kernels may overlap the previous evaluation
+			h->early_call = p > p0;
+			rc = eval_device(h, N, h->d_many_in + p * per, h->d_many_E + p, (F && N > 0) ? h->d_many_F + p * per : nullptr,
+			                 nullptr, false, precision, st);
+			h->early_call = false;
+		}
+		CC_CUDA(cudaEventRecord(done, st));
+	}
+	// Results go out after every evaluation is enqueued: a copy into pageable memory returns only when it is done,
+	// and must not hold back the enqueueing of later chunks.
+	for (int64_t c = 0; c < nch && rc == CC_OK; c++) {
+		const int64_t p0 = c * kManyChunk, p1 = std::min(P, p0 + kManyChunk);
+		const size_t n = (size_t)(p1 - p0) * per;
+		CC_CUDA(cudaStreamWaitEvent(cp, h->many_ev[2 * c + 1], 0));
+		if (F && n)
+			CC_CUDA(cudaMemcpyAsync(F + p0 * per, h->d_many_F + p0 * per, n * sizeof(double), cudaMemcpyDeviceToHost, cp));
+	}
+	int bad = 0;
+	if (rc == CC_OK) {
+		CC_CUDA(cudaMemcpyAsync(E, h->d_many_E, (size_t)P * sizeof(double), cudaMemcpyDeviceToHost, cp));
+		CC_CUDA(cudaMemcpyAsync(&bad, h->d_many_bad, sizeof(int), cudaMemcpyDeviceToHost, cp));
+	}
+	CC_CUDA(cudaStreamSynchronize(cp));
+	CC_CUDA(cudaStreamSynchronize(st));
+	if (rc != CC_OK)
+		return rc;
+	if (bad)
+		return fail(CC_ERR_ARG, "non-finite fractional coordinate");
+	return CC_OK;
 }
 
 int cc_rho(cc_handle *h, double *re, double *im, int precision)

@@ -261,6 +261,12 @@ struct cc_handle {
 	const int *d_skip = nullptr;    // evaluations do nothing while *d_skip != 0 (set by cc_minimize)
 	bool timing = false;            // cc_set_timing
 	bool independent = false;       // cc_set_independent_positions
+	// cc_energy_grad_many: every configuration of a call resident at once, so that its copies overlap the evaluations
+	double *d_many_in = nullptr, *d_many_F = nullptr, *d_many_E = nullptr;
+	int *d_many_bad = nullptr;          // set by the wrap kernel on a non-finite coordinate
+	size_t many_cap = 0, many_ecap = 0; // doubles of d_many_in / d_many_F and of d_many_E
+	cudaStream_t copy_stream = nullptr;
+	std::vector<cudaEvent_t> many_ev;   // two per chunk: positions in, results done
 	bool early_call = false;        // set for the duration of a cc_energy_grad_device call when independent
 	// cc_minimize's state, kept between calls so that a minimisation makes no allocation call into the CUDA driver
 	// once the handle has run one of its size: FP64 / mixed buffers (capacities n variables, m pairs, nblk dot

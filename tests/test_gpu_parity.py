@@ -247,6 +247,40 @@ def test_independent_positions_bitwise(gpu):
     assert E[1, 0].item() == E0 and np.array_equal(F[1, 0].cpu().numpy(), F0)
 
 
+def test_energy_grad_many_matches_single(gpu):
+    """cc_energy_grad_many over 70 configurations (two copy chunks), from pageable and from pinned host memory, with
+    coordinates outside [0, 1) in some of them, equals bitwise one set_configuration + energy_and_forces call per
+    configuration; a non-finite coordinate fails the call with CC_ERR_ARG and leaves the handle usable."""
+    torch = pytest.importorskip("torch")
+    r = load_golden("stealthy_3d_n2000")
+    p = make_pot(gpu, r)
+    n, d = r["frac"].shape
+    rng = np.random.default_rng(11)
+    pool = np.stack([np.mod(r["frac"] + rng.normal(0.0, 0.05, r["frac"].shape), 1.0) for _ in range(70)])
+    pool[3] += 1.0
+    pool[5, :40] -= 1.25
+    pool[7, 0, 0] = 1.0
+    E, F = p.energy_grad_many(pool)
+    pin_in = torch.empty(pool.shape, dtype=torch.float64, pin_memory=True).numpy()
+    pin_in[:] = pool
+    pin_E = torch.empty(len(pool), dtype=torch.float64, pin_memory=True).numpy()
+    pin_F = torch.empty(pool.shape, dtype=torch.float64, pin_memory=True).numpy()
+    p.energy_grad_many(pin_in, pin_E, pin_F)
+    E2, _ = p.energy_grad_many(pool, forces=False)
+    for i in range(len(pool)):
+        p.set_configuration(pool[i])
+        Ei, Fi = p.energy_and_forces()
+        assert E[i] == Ei and pin_E[i] == Ei and E2[i] == Ei, i
+        assert np.array_equal(F[i], Fi) and np.array_equal(pin_F[i], Fi), i
+    bad = pool[:3].copy()
+    bad[1, 5, 0] = np.nan
+    with pytest.raises(gpu.CCError) as e:
+        p.energy_grad_many(bad)
+    assert e.value.code == -1
+    E3, F3 = p.energy_grad_many(pool[:3])
+    assert np.array_equal(E3, E[:3]) and np.array_equal(F3, F[:3])
+
+
 def test_mixed_precision_error(gpu):
     """Mixed path (FP32 seeds and recurrences, FP64 partials) against the FP64 path: report and bound the error."""
     r = load_golden("stealthy_3d_n2000")
