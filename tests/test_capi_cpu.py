@@ -43,6 +43,7 @@ def test_argument_errors(ccgpu):
     assert lib.cc_energy_grad(None, ctypes.byref(E), None, 0) == -1
     assert "null" in lib.cc_last_error().decode()
     assert lib.cc_set_independent_positions(None, 1) == -1
+    assert lib.cc_energy_grad_many(None, 1, 1, None, ctypes.byref(E), None, 0) == -1
 
 
 def test_nonlattice_k_rejected(ccgpu):
